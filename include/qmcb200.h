@@ -1,0 +1,211 @@
+/*
+ * qmcb200.h -- C ABI of the B200 Slater-Jastrow walker-evaluation library
+ * (libqmcb200.so).
+ *
+ * The library replaces QMcBeaver's wavefunction-evaluation hot path:
+ *   QMCFunctions::evaluate(Array1D<QMCWalkerData*>&, Array1D<Array2D<double>*>&, int)
+ *     (QMcBeaver/include/QMCFunctions.h:67-70), implemented by
+ *   QMCSCFJastrow::evaluate (QMcBeaver/src/QMCSCFJastrow.cpp:91-181)
+ * and the single-electron Metropolis / DMC step around it
+ *   QMCRun::propagateWalkers + QMCWalker::{initialize,process}Propagation
+ *     (QMcBeaver/src/QMCRun.cpp:28-87, QMcBeaver/src/QMCWalker.cpp:179-282).
+ *
+ * Conventions
+ *   - Plain C types only; every function returns 0 on success and a positive
+ *     QMCB_E_* code on failure; qmcb_last_error() gives the message.
+ *   - Electrons are ordered alpha [0, n_alpha) then beta
+ *     (QMcBeaver/src/QMCSCFJastrow.cpp:68-76); positions are [N][3] doubles.
+ *   - Per-walker state (inverse Slater matrices, Slater rows and derivative
+ *     rows, Jastrow gradients, energies) lives in device memory, addressed by
+ *     a walker slot in [0, max_walkers).  This is the state QMCWalkerData
+ *     carries in the reference (QMcBeaver/src/QMCWalkerData.cpp:56-161).
+ *   - One handle = one CUDA stream; a handle is not thread safe.
+ */
+#ifndef QMCB200_H
+#define QMCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QMCB_PADE_MAX 8
+
+/* error codes */
+#define QMCB_OK 0
+#define QMCB_E_ARG 1      /* bad argument / size */
+#define QMCB_E_CUDA 2     /* CUDA runtime error */
+#define QMCB_E_NOMEM 3    /* device allocation failed */
+#define QMCB_E_STATE 4    /* call order (e.g. evaluate one electron before a full evaluation) */
+#define QMCB_E_LIMIT 5    /* size beyond a compiled limit */
+
+/* per-walker status bits written by evaluate / steps */
+#define QMCB_ST_SINGULAR 1 /* Slater matrix singular or psi ratio 0 (wd->singular) */
+#define QMCB_ST_NAN 2      /* NaN in gradient / energy */
+
+/* run types, samplers, quantum-force modifications (QMcBeaver/src/QMCFlags.cpp) */
+#define QMCB_VMC 0
+#define QMCB_DMC 1
+#define QMCB_NO_IMPORTANCE_SAMPLING 0
+#define QMCB_IMPORTANCE_SAMPLING 1
+#define QMCB_QF_NONE 0
+#define QMCB_QF_UMRIGAR93_EQUAL 1
+#define QMCB_QF_UMRIGAR93_UNEQUAL 2
+#define QMCB_EMOD_NONE 0
+#define QMCB_EMOD_UMRIGAR93 1
+#define QMCB_EMOD_MODIFIED_UMRIGAR93 2
+#define QMCB_RW_SIMPLE_SYMMETRIC 0
+#define QMCB_RW_SIMPLE_ASYMMETRIC 1
+#define QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED 2
+
+/* arithmetic of the orbital contraction and Slater updates */
+#define QMCB_PREC_FP64 0  /* plain FP64 everywhere (parity path) */
+#define QMCB_PREC_MIXED 1 /* FP32 orbital rows / SM update, FP64 refresh and accumulators */
+
+/*
+ * Molecular system: what QMCInput reads from the .ckmf &geometry, &basis,
+ * &wavefunction and &Jastrow sections for one restricted determinant with
+ * Pade two-body Jastrows.
+ */
+typedef struct qmcb_system_desc {
+  int n_nuclei;                 /* M */
+  const double *nuc_xyz;        /* [M][3] bohr */
+  const double *nuc_charge;     /* [M] Z (Zeff) */
+  int n_alpha, n_beta;          /* electrons per spin */
+  int n_basis;                  /* K contracted Cartesian Gaussians */
+  const int *bf_atom;           /* [K] centre of function k */
+  const int *bf_powers;         /* [K][3] Cartesian powers a, b, c */
+  const int *bf_nprim;          /* [K] primitives of function k */
+  const int *bf_prim_offset;    /* [K] first primitive of function k */
+  int n_prim_total;
+  const double *prim_exponent;  /* [n_prim_total] */
+  const double *prim_coeff;     /* [n_prim_total] raw contraction coefficients */
+  const double *mo_alpha;       /* [n_alpha][K] occupied orbital rows (AlphaCoeffs) */
+  const double *mo_beta;        /* [n_beta][K] (BetaCoeffs) */
+  int n_pade;                   /* Pade functions u = P(r)/Q(r) */
+  const double *pade_num;       /* [n_pade][QMCB_PADE_MAX] P coefficients, P[0] = 0 */
+  const double *pade_den;       /* [n_pade][QMCB_PADE_MAX] Q coefficients, Q[0] = 1 */
+  const int *pade_nnum;         /* [n_pade] used length of P */
+  const int *pade_nden;         /* [n_pade] used length of Q */
+  int ee_pade[3];               /* up-down, up-up, down-down function (-1 = none) */
+  const int *en_pade_up;        /* [M] up electron - nucleus function (-1 = none) */
+  const int *en_pade_dn;        /* [M] down electron - nucleus function */
+} qmcb_system_desc;
+
+/* Sampling / DMC parameters (the QMCFlags fields the path reads). */
+typedef struct qmcb_run_params {
+  int run_type;              /* QMCB_VMC | QMCB_DMC (run_type) */
+  int sampling;              /* sampling_method */
+  int qf_modification;       /* QF_modification_type */
+  double qf_equal_a;         /* umrigar93_equalelectrons_parameter */
+  double dt;                 /* dt */
+  double dt_effective;       /* dt_effective (reweighting exponent) */
+  int energy_modification;   /* energy_modification_type */
+  int reweighting;           /* walker_reweighting_method */
+  double energy_trial;       /* E_T */
+  double energy_estimated;   /* E_est */
+  double branching_threshold;
+  double fusion_threshold;
+  int old_walker_acceptance; /* old_walker_acceptance_parameter */
+  int refresh_interval;      /* steps between full LU refreshes, 0 = never */
+  int precision;             /* QMCB_PREC_* */
+  uint64_t seed;             /* Philox key for device random numbers */
+} qmcb_run_params;
+
+/* Ensemble sums over one call of qmcb_run_steps (for E_est / E_T and error bars). */
+typedef struct qmcb_step_stats {
+  double sum_weight;         /* sum over walker-steps of weight */
+  double sum_weight_energy;  /* sum of weight * E_L (observable, p/q weighted) */
+  double sum_weight_energy2; /* sum of weight * E_L^2 */
+  double sum_accept;         /* sum of acceptance probabilities */
+  double n_moves;            /* walker-moves performed */
+  double final_weight;       /* total weight after the last step */
+  int n_walkers;             /* walkers alive after the last step */
+  int n_singular;            /* rejected singular / NaN proposals */
+} qmcb_step_stats;
+
+typedef struct qmcb_handle qmcb_handle;
+
+/* Library version string. */
+const char *qmcb_version(void);
+
+/* Message of the last failure on this handle (or of the last failed create
+ * when h is NULL). */
+const char *qmcb_last_error(const qmcb_handle *h);
+
+/* Builds device tables for the system and allocates state for max_walkers
+ * slots on the current CUDA device.  Replaces QMCSCFJastrow::initialize
+ * (QMcBeaver/src/QMCSCFJastrow.cpp:61-89) + QMCWalkerData::initialize
+ * (QMcBeaver/src/QMCWalkerData.cpp:56-161). */
+int qmcb_create(const qmcb_system_desc *sys, int max_walkers, qmcb_handle **out);
+int qmcb_destroy(qmcb_handle *h);
+int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p);
+int qmcb_get_params(const qmcb_handle *h, qmcb_run_params *p);
+int qmcb_num_electrons(const qmcb_handle *h);
+int qmcb_max_walkers(const qmcb_handle *h);
+
+/*
+ * QMCFunctions::evaluate(walkerData[], xData[], num) for the walkers in
+ * slots[0..num), all with the same which_e (QMcBeaver/src/QMCSCFJastrow.cpp:91-181):
+ *   which_e = -1: full evaluation (LU inverse, all Slater rows, all Jastrow
+ *                 pairs), as for walker initialisation / all-electron moves;
+ *   which_e = e : electron e moved; Sherman-Morrison row update of that
+ *                 spin's inverse (QMcBeaver/include/Array2D.h:1567-1610) and
+ *                 incremental Jastrow update (QMcBeaver/src/QMCJastrowElectronElectron.cpp:68-147).
+ * The state of each slot is updated unconditionally, as the reference does.
+ * R: host [num][N][3].  Outputs (host, any may be NULL):
+ *   log_abs_psi[num], sign[num]            psi = sign * exp(log_abs_psi)
+ *   grad[num][N][3]                        gradPsiRatio
+ *   mod_grad[num][N][3]                    modifiedGradPsiRatio
+ *   lap[num]                               lap(psi)/psi
+ *   e_local[num]                           localEnergy
+ *   pe[num][3]                             potentialEnergy, neEnergy, eeEnergy
+ *   status[num]                            QMCB_ST_* bits (wd->singular)
+ */
+int qmcb_evaluate(qmcb_handle *h, int which_e, const int *slots, int num, const double *R,
+                  double *log_abs_psi, double *sign, double *grad, double *mod_grad, double *lap,
+                  double *e_local, double *pe, unsigned char *status);
+
+/* Same as qmcb_evaluate with every pointer in device memory and no
+ * host synchronisation; stream NULL = the handle's stream. */
+int qmcb_evaluate_device(qmcb_handle *h, int which_e, const int *d_slots, int num, const double *d_R,
+                         double *d_log_abs_psi, double *d_sign, double *d_grad, double *d_mod_grad,
+                         double *d_lap, double *d_e_local, double *d_pe, unsigned char *d_status,
+                         void *stream);
+
+/* Uploads positions of walkers [0, n) from host R[n][N][3] into slots 0..n-1
+ * and runs the full evaluation on them (QMCWalker::initializeWalkerPosition,
+ * QMcBeaver/src/QMCWalker.cpp:2006-2034). Sets weight 1, age 0. */
+int qmcb_init_walkers(qmcb_handle *h, int n, const double *R);
+
+/*
+ * n_steps single-electron Metropolis steps (VMC) or DMC steps on the live
+ * walkers (QMCRun::step, QMcBeaver/src/QMCRun.cpp:1179-1236): step s moves
+ * electron (first_step + s) % N of every walker (QMcBeaver/src/QMCWalker.cpp:186-190),
+ * accepts or rejects, reweights when that electron is 0 (DMC), and branches
+ * after such steps (nonunit weight branching, QMcBeaver/src/QMCRun.cpp:740-814).
+ * Full LU refresh every refresh_interval steps.  Stats are accumulated.
+ */
+int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats *stats);
+
+/* Live walker count and per-walker read back (host buffers, any may be NULL). */
+int qmcb_num_walkers(const qmcb_handle *h);
+int qmcb_get_walkers(qmcb_handle *h, int n, double *R, double *weight, double *e_local,
+                     double *log_abs_psi, double *sign);
+
+/* Copies the full device state of walker slot src into dst (branching,
+ * QMcBeaver/src/QMCRun.cpp:758). */
+int qmcb_copy_slot(qmcb_handle *h, int src, int dst);
+
+/* Blocks until the handle's stream is idle. */
+int qmcb_synchronize(qmcb_handle *h);
+
+/* The CUDA stream of the handle (cudaStream_t as void*). */
+void *qmcb_stream(qmcb_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QMCB200_H */

@@ -1,0 +1,192 @@
+"""ctypes front ends of the oracle (C restatement) and of the reference build.
+
+TEST INFRASTRUCTURE ONLY.  Both expose the same calls:
+
+    ev = OracleEvaluator(system, qf_mod=..., dt=...)   # or ReferenceEvaluator
+    ws = ev.new_walkers(n)
+    ev.evaluate(ws, R, which_e)          # QMCSCFJastrow::evaluate
+    out = ev.results(ws)                 # dict of numpy arrays
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from qmcbeaver_b200.desc import PackedSystem, QMCB_QF_NONE
+from qmcbeaver_b200.system import MolecularSystem
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libqmcref.so")
+REF_EXE = os.path.join(HERE, "_ref", "QMcBeaver.x")
+REFERENCE_TREE = os.environ.get("QMCB_REFERENCE_TREE", "/root/reference/QMcBeaver")
+
+SCALARS = ["e_local", "kinetic", "potential", "ne", "ee", "U", "U_xx", "D_xx", "det_a", "det_b", "singular",
+           "log_abs_psi", "sign", "psi"]
+
+QF_NAMES = {0: "none", 1: "umrigar93_equalelectrons", 2: "umrigar93_unequalelectrons"}
+
+
+def build_port() -> str:
+    """Compiles oracle/qmc_oracle.c (gcc) if the library is missing or stale."""
+    src = os.path.join(HERE, "qmc_oracle.c")
+    if not os.path.exists(PORT_SO) or os.path.getmtime(PORT_SO) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", HERE, "port", "CXX=g++"])
+    return PORT_SO
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO) or os.path.isdir(os.path.join(REFERENCE_TREE, "src"))
+
+
+def build_reference() -> str:
+    if not os.path.exists(REF_SO):
+        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", "CXX=/usr/bin/g++",
+                               f"REF={REFERENCE_TREE}"])
+    return REF_SO
+
+
+class _Base:
+    N: int
+
+    def results(self, walkers) -> Dict[str, np.ndarray]:
+        n = len(walkers)
+        sc = np.zeros((n, 14))
+        g = np.zeros((n, self.N, 3))
+        mg = np.zeros((n, self.N, 3))
+        buf = np.zeros(14)
+        gb = np.zeros((self.N, 3))
+        mb = np.zeros((self.N, 3))
+        for i, w in enumerate(walkers):
+            self._get(w, buf.ctypes.data_as(C.c_void_p), gb.ctypes.data_as(C.c_void_p),
+                      mb.ctypes.data_as(C.c_void_p))
+            sc[i] = buf
+            g[i] = gb
+            mg[i] = mb
+        out = {k: sc[:, i].copy() for i, k in enumerate(SCALARS)}
+        out["grad"] = g
+        out["mod_grad"] = mg
+        out["lap"] = -2.0 * out["kinetic"]
+        return out
+
+
+class OracleEvaluator(_Base):
+    """The C restatement (oracle/qmc_oracle.c)."""
+
+    def __init__(self, system: MolecularSystem, qf_mod: int = QMCB_QF_NONE, qf_a: float = 0.5, dt: float = 0.09):
+        self.lib = C.CDLL(build_port())
+        L = self.lib
+        L.orc_system_new.restype = C.c_void_p
+        L.orc_system_new.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+        L.orc_walker_new.restype = C.c_void_p
+        L.orc_walker_new.argtypes = [C.c_void_p]
+        L.orc_walker_clone.restype = C.c_void_p
+        L.orc_walker_clone.argtypes = [C.c_void_p]
+        L.orc_walker_copy.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_walker_free.argtypes = [C.c_void_p]
+        L.orc_evaluate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.orc_walker_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_walker_inverse.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_basis_at.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        self.packed = PackedSystem(system)
+        self.system = system
+        self.N = system.n_electrons
+        self.sys = L.orc_system_new(C.byref(self.packed.desc), qf_mod, qf_a, dt)
+
+    def new_walkers(self, n: int) -> List[int]:
+        return [self.lib.orc_walker_new(self.sys) for _ in range(n)]
+
+    def clone(self, w):
+        return self.lib.orc_walker_clone(w)
+
+    def copy(self, dst, src):
+        self.lib.orc_walker_copy(dst, src)
+
+    def free(self, ws):
+        for w in ws:
+            self.lib.orc_walker_free(w)
+
+    def evaluate(self, walkers, R: np.ndarray, which_e: int) -> None:
+        R = np.ascontiguousarray(R, np.float64)
+        arr = (C.c_void_p * len(walkers))(*walkers)
+        self.lib.orc_evaluate(self.sys, arr, R.ctypes.data_as(C.c_void_p), len(walkers), which_e)
+
+    def _get(self, w, a, b, c):
+        self.lib.orc_walker_get(w, a, b, c)
+
+    def inverse(self, w, beta: int) -> np.ndarray:
+        n = self.system.n_beta if beta else self.system.n_alpha
+        out = np.zeros((n, n))
+        self.lib.orc_walker_inverse(w, beta, out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def basis_at(self, r) -> np.ndarray:
+        out = np.zeros((5, self.system.n_basis))
+        r = np.ascontiguousarray(r, np.float64)
+        self.lib.orc_basis_at(self.sys, r.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p))
+        return out
+
+
+class ReferenceEvaluator(_Base):
+    """The reference QMcBeaver code itself (oracle/_ref/libqmcref.so), driven
+    through its own QMCSCFJastrow::evaluate.  One system per process: the
+    reference keeps its input in a global."""
+
+    _loaded: Optional[str] = None
+
+    def __init__(self, system: MolecularSystem, qf_mod: int = QMCB_QF_NONE, qf_a: float = 0.5, dt: float = 0.09,
+                 max_batch: int = 256):
+        if ReferenceEvaluator._loaded is not None:
+            raise RuntimeError("the reference library holds one system per process")
+        self.lib = C.CDLL(build_reference())
+        L = self.lib
+        L.ref_init.argtypes = [C.c_char_p]
+        L.ref_walker_new.restype = C.c_void_p
+        L.ref_walker_clone.restype = C.c_void_p
+        L.ref_walker_clone.argtypes = [C.c_void_p]
+        L.ref_walker_free.argtypes = [C.c_void_p]
+        L.ref_evaluate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        L.ref_walker_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_walker_inverse.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        self.system = system
+        self.N = system.n_electrons
+        self.max_batch = max_batch
+        fd, path = tempfile.mkstemp(suffix=".ckmf")
+        os.close(fd)
+        system.to_ckmf(path, {"walkers_per_pass": max_batch, "number_of_walkers": max_batch,
+                              "QF_modification_type": QF_NAMES[qf_mod],
+                              "umrigar93_equalelectrons_parameter": float(qf_a), "dt": float(dt)})
+        L.ref_init(path.encode())
+        os.unlink(path)
+        ReferenceEvaluator._loaded = path
+
+    def new_walkers(self, n: int) -> List[int]:
+        return [self.lib.ref_walker_new() for _ in range(n)]
+
+    def clone(self, w):
+        return self.lib.ref_walker_clone(w)
+
+    def free(self, ws):
+        for w in ws:
+            self.lib.ref_walker_free(w)
+
+    def evaluate(self, walkers, R: np.ndarray, which_e: int) -> None:
+        R = np.ascontiguousarray(R, np.float64)
+        for s in range(0, len(walkers), self.max_batch):
+            chunk = walkers[s:s + self.max_batch]
+            arr = (C.c_void_p * len(chunk))(*chunk)
+            self.lib.ref_evaluate(arr, R[s:s + len(chunk)].ctypes.data_as(C.c_void_p), len(chunk), which_e)
+
+    def _get(self, w, a, b, c):
+        self.lib.ref_walker_get(w, a, b, c)
+
+    def inverse(self, w, beta: int) -> np.ndarray:
+        n = self.system.n_beta if beta else self.system.n_alpha
+        out = np.zeros((n, n))
+        self.lib.ref_walker_inverse(w, beta, out.ctypes.data_as(C.c_void_p))
+        return out

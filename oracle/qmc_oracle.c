@@ -1,0 +1,808 @@
+/*
+ * qmc_oracle.c -- CPU restatement of QMcBeaver's Slater-Jastrow walker
+ * evaluation.  TEST INFRASTRUCTURE ONLY (the checker for the CUDA path).
+ *
+ * Each routine follows the reference function named beside it, with the
+ * same loop orders and operation order, including the long double
+ * accumulators of the LU decomposition, so that it reproduces the reference
+ * to the last bits on the same inputs.  Pinned by tests/test_oracle.py
+ * against the reference built from its own sources (oracle/_ref) and the
+ * committed golden vectors.
+ */
+#include "qmc_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+struct orc_system {
+  int M, na, nb, N, K;
+  double *nuc_xyz, *nuc_z;
+  int *bf_atom, *bf_pow, *bf_nprim, *bf_off;
+  double *pexp, *pcoef;
+  int *atom_first, *atom_nbf, *atom_lmax; /* per atom function ranges */
+  double *mo_a, *mo_b;                    /* [n][K] */
+  int npade;
+  double *pnum, *pden;
+  int *pnn, *pnd;
+  int ee[3];
+  int *en_up, *en_dn;
+  double Pnn;
+  int qf_mod;
+  double qf_a, dt;
+};
+
+struct orc_walker {
+  const orc_system *s;
+  double *inv[2];     /* [n][n] inv[o*n+e] (Dc_invA / Dc_invB) */
+  double *Dx[2][3];   /* [n][n] derivative rows, row = electron (D_xA) */
+  double *Dxx[2];     /* [n][n] (D_xxA) */
+  double det[2];      /* DcA, DcB */
+  double *rDx[2];     /* [N][3] grad ratios (rDc_xA) */
+  double rDxx[2];     /* rDc_xxA */
+  int sing[2];
+  double *rij, *rij_uvec, *riA, *riA_uvec;
+  double *Uij, *Uij_x, *Uij_xx, *UiA, *UiA_x, *UiA_xx;
+  double U, U_xx;
+  double *U_x;
+  double D_xx;
+  double *D_x, *grad, *mgrad;
+  double E_L, KE, PE, neE, eeE, lap;
+  int singular;
+  double logpsi, sign;
+};
+
+static double *dup_d(const double *p, size_t n)
+{
+  double *q = (double *)malloc(sizeof(double) * (n ? n : 1));
+  if (n) memcpy(q, p, sizeof(double) * n);
+  return q;
+}
+static int *dup_i(const int *p, size_t n)
+{
+  int *q = (int *)malloc(sizeof(int) * (n ? n : 1));
+  if (n) memcpy(q, p, sizeof(int) * n);
+  return q;
+}
+
+orc_system *orc_system_new(const qmcb_system_desc *d, int qf_mod, double qf_a, double dt)
+{
+  orc_system *s = (orc_system *)calloc(1, sizeof(orc_system));
+  s->M = d->n_nuclei;
+  s->na = d->n_alpha;
+  s->nb = d->n_beta;
+  s->N = s->na + s->nb;
+  s->K = d->n_basis;
+  s->nuc_xyz = dup_d(d->nuc_xyz, 3 * s->M);
+  s->nuc_z = dup_d(d->nuc_charge, s->M);
+  s->bf_atom = dup_i(d->bf_atom, s->K);
+  s->bf_pow = dup_i(d->bf_powers, 3 * s->K);
+  s->bf_nprim = dup_i(d->bf_nprim, s->K);
+  s->bf_off = dup_i(d->bf_prim_offset, s->K);
+  s->pexp = dup_d(d->prim_exponent, d->n_prim_total);
+  s->pcoef = dup_d(d->prim_coeff, d->n_prim_total);
+  s->mo_a = dup_d(d->mo_alpha, (size_t)s->na * s->K);
+  s->mo_b = dup_d(d->mo_beta, (size_t)s->nb * s->K);
+  s->npade = d->n_pade;
+  s->pnum = dup_d(d->pade_num, (size_t)s->npade * QMCB_PADE_MAX);
+  s->pden = dup_d(d->pade_den, (size_t)s->npade * QMCB_PADE_MAX);
+  s->pnn = dup_i(d->pade_nnum, s->npade);
+  s->pnd = dup_i(d->pade_nden, s->npade);
+  for (int i = 0; i < 3; i++) s->ee[i] = d->ee_pade[i];
+  s->en_up = dup_i(d->en_pade_up, s->M);
+  s->en_dn = dup_i(d->en_pade_dn, s->M);
+  s->atom_first = (int *)calloc(s->M, sizeof(int));
+  s->atom_nbf = (int *)calloc(s->M, sizeof(int));
+  s->atom_lmax = (int *)calloc(s->M, sizeof(int));
+  for (int a = 0; a < s->M; a++) s->atom_first[a] = -1;
+  for (int k = 0; k < s->K; k++) {
+    int a = s->bf_atom[k];
+    if (s->atom_first[a] < 0) s->atom_first[a] = k;
+    s->atom_nbf[a]++;
+    int l = s->bf_pow[3 * k] + s->bf_pow[3 * k + 1] + s->bf_pow[3 * k + 2];
+    if (l > s->atom_lmax[a]) s->atom_lmax[a] = l;
+  }
+  /* calc_P_nn, QMcBeaver/src/QMCPotential_Energy.cpp:285-307 */
+  s->Pnn = 0.0;
+  for (int i = 0; i < s->M; i++)
+    for (int j = i + 1; j < s->M; j++) {
+      const double *a = s->nuc_xyz + 3 * i, *b = s->nuc_xyz + 3 * j;
+      double r = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) +
+                      (a[2] - b[2]) * (a[2] - b[2]));
+      s->Pnn += (s->nuc_z[i] * s->nuc_z[j]) / r;
+    }
+  s->qf_mod = qf_mod;
+  s->qf_a = qf_a;
+  s->dt = dt;
+  return s;
+}
+
+void orc_system_free(orc_system *s)
+{
+  if (!s) return;
+  free(s->nuc_xyz); free(s->nuc_z); free(s->bf_atom); free(s->bf_pow); free(s->bf_nprim);
+  free(s->bf_off); free(s->pexp); free(s->pcoef); free(s->mo_a); free(s->mo_b); free(s->pnum);
+  free(s->pden); free(s->pnn); free(s->pnd); free(s->en_up); free(s->en_dn);
+  free(s->atom_first); free(s->atom_nbf); free(s->atom_lmax);
+  free(s);
+}
+
+int orc_num_electrons(const orc_system *s) { return s->N; }
+
+/* ------------------------------------------------------------ walker state */
+#define NFIELDS 29
+static void walker_alloc(orc_walker *w, const orc_system *s)
+{
+  int N = s->N, M = s->M;
+  w->s = s;
+  for (int sp = 0; sp < 2; sp++) {
+    int n = sp ? s->nb : s->na;
+    size_t nn = (size_t)(n ? n * n : 1);
+    w->inv[sp] = (double *)calloc(nn, sizeof(double));
+    for (int d = 0; d < 3; d++) w->Dx[sp][d] = (double *)calloc(nn, sizeof(double));
+    w->Dxx[sp] = (double *)calloc(nn, sizeof(double));
+    w->rDx[sp] = (double *)calloc((size_t)N * 3, sizeof(double));
+  }
+  w->rij = (double *)calloc((size_t)N * N, sizeof(double));
+  w->rij_uvec = (double *)calloc((size_t)N * N * 3, sizeof(double));
+  w->riA = (double *)calloc((size_t)N * M + 1, sizeof(double));
+  w->riA_uvec = (double *)calloc((size_t)N * M * 3 + 1, sizeof(double));
+  w->Uij = (double *)calloc((size_t)N * N, sizeof(double));
+  w->Uij_x = (double *)calloc((size_t)N * N * 3, sizeof(double));
+  w->Uij_xx = (double *)calloc((size_t)N * N, sizeof(double));
+  w->UiA = (double *)calloc((size_t)N * M + 1, sizeof(double));
+  w->UiA_x = (double *)calloc((size_t)N * M * 3 + 1, sizeof(double));
+  w->UiA_xx = (double *)calloc((size_t)N * M + 1, sizeof(double));
+  w->U_x = (double *)calloc((size_t)N * 3, sizeof(double));
+  w->D_x = (double *)calloc((size_t)N * 3, sizeof(double));
+  w->grad = (double *)calloc((size_t)N * 3, sizeof(double));
+  w->mgrad = (double *)calloc((size_t)N * 3, sizeof(double));
+}
+
+orc_walker *orc_walker_new(const orc_system *s)
+{
+  orc_walker *w = (orc_walker *)calloc(1, sizeof(orc_walker));
+  walker_alloc(w, s);
+  w->det[0] = w->det[1] = 1.0;
+  return w;
+}
+
+void orc_walker_free(orc_walker *w)
+{
+  if (!w) return;
+  for (int sp = 0; sp < 2; sp++) {
+    free(w->inv[sp]);
+    for (int d = 0; d < 3; d++) free(w->Dx[sp][d]);
+    free(w->Dxx[sp]);
+    free(w->rDx[sp]);
+  }
+  free(w->rij); free(w->rij_uvec); free(w->riA); free(w->riA_uvec); free(w->Uij); free(w->Uij_x);
+  free(w->Uij_xx); free(w->UiA); free(w->UiA_x); free(w->UiA_xx); free(w->U_x); free(w->D_x);
+  free(w->grad); free(w->mgrad);
+  free(w);
+}
+
+void orc_walker_copy(orc_walker *dst, const orc_walker *src)
+{
+  const orc_system *s = src->s;
+  int N = s->N, M = s->M;
+  for (int sp = 0; sp < 2; sp++) {
+    int n = sp ? s->nb : s->na;
+    size_t nn = (size_t)(n ? n * n : 1);
+    memcpy(dst->inv[sp], src->inv[sp], nn * sizeof(double));
+    for (int d = 0; d < 3; d++) memcpy(dst->Dx[sp][d], src->Dx[sp][d], nn * sizeof(double));
+    memcpy(dst->Dxx[sp], src->Dxx[sp], nn * sizeof(double));
+    memcpy(dst->rDx[sp], src->rDx[sp], (size_t)N * 3 * sizeof(double));
+    dst->det[sp] = src->det[sp];
+    dst->rDxx[sp] = src->rDxx[sp];
+    dst->sing[sp] = src->sing[sp];
+  }
+  memcpy(dst->rij, src->rij, (size_t)N * N * sizeof(double));
+  memcpy(dst->rij_uvec, src->rij_uvec, (size_t)N * N * 3 * sizeof(double));
+  memcpy(dst->riA, src->riA, ((size_t)N * M + 1) * sizeof(double));
+  memcpy(dst->riA_uvec, src->riA_uvec, ((size_t)N * M * 3 + 1) * sizeof(double));
+  memcpy(dst->Uij, src->Uij, (size_t)N * N * sizeof(double));
+  memcpy(dst->Uij_x, src->Uij_x, (size_t)N * N * 3 * sizeof(double));
+  memcpy(dst->Uij_xx, src->Uij_xx, (size_t)N * N * sizeof(double));
+  memcpy(dst->UiA, src->UiA, ((size_t)N * M + 1) * sizeof(double));
+  memcpy(dst->UiA_x, src->UiA_x, ((size_t)N * M * 3 + 1) * sizeof(double));
+  memcpy(dst->UiA_xx, src->UiA_xx, ((size_t)N * M + 1) * sizeof(double));
+  memcpy(dst->U_x, src->U_x, (size_t)N * 3 * sizeof(double));
+  memcpy(dst->D_x, src->D_x, (size_t)N * 3 * sizeof(double));
+  memcpy(dst->grad, src->grad, (size_t)N * 3 * sizeof(double));
+  memcpy(dst->mgrad, src->mgrad, (size_t)N * 3 * sizeof(double));
+  dst->U = src->U; dst->U_xx = src->U_xx; dst->D_xx = src->D_xx;
+  dst->E_L = src->E_L; dst->KE = src->KE; dst->PE = src->PE; dst->neE = src->neE; dst->eeE = src->eeE;
+  dst->lap = src->lap; dst->singular = src->singular; dst->logpsi = src->logpsi; dst->sign = src->sign;
+}
+
+orc_walker *orc_walker_clone(const orc_walker *w)
+{
+  orc_walker *c = orc_walker_new(w->s);
+  orc_walker_copy(c, w);
+  return c;
+}
+
+/* ------------------------------------------------------- distances (a8) */
+/* QMCWalkerData::updateDistances, QMcBeaver/src/QMCWalkerData.cpp:302-344 */
+static double dist(const double *a, const double *b)
+{
+  return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+}
+
+static void update_distances(const orc_system *s, orc_walker *w, const double *R, int whichE)
+{
+  int N = s->N, M = s->M;
+  if (whichE == -1) {
+    for (int i = 0; i < N; i++) {
+      for (int j = 0; j < i; j++) {
+        double r = dist(R + 3 * i, R + 3 * j);
+        w->rij[i * N + j] = r;
+        for (int x = 0; x < 3; x++) w->rij_uvec[(i * N + j) * 3 + x] = (R[3 * i + x] - R[3 * j + x]) / r;
+      }
+      for (int j = 0; j < M; j++) {
+        double r = dist(R + 3 * i, s->nuc_xyz + 3 * j);
+        w->riA[i * M + j] = r;
+        for (int x = 0; x < 3; x++) w->riA_uvec[(i * M + j) * 3 + x] = (R[3 * i + x] - s->nuc_xyz[3 * j + x]) / r;
+      }
+    }
+  } else {
+    for (int j = 0; j < N; j++) {
+      if (j == whichE) continue;
+      double r = dist(R + 3 * j, R + 3 * whichE);
+      int e1 = whichE > j ? whichE : j;
+      int e2 = whichE < j ? whichE : j;
+      w->rij[e1 * N + e2] = r;
+      for (int x = 0; x < 3; x++) w->rij_uvec[(e1 * N + e2) * 3 + x] = (R[3 * e1 + x] - R[3 * e2 + x]) / r;
+    }
+    for (int j = 0; j < M; j++) {
+      w->riA[whichE * M + j] = dist(R + 3 * whichE, s->nuc_xyz + 3 * j);
+      for (int x = 0; x < 3; x++)
+        w->riA_uvec[(whichE * M + j) * 3 + x] = (R[3 * whichE + x] - s->nuc_xyz[3 * j + x]) / w->riA[whichE * M + j];
+    }
+  }
+}
+
+/* ------------------------------------------------------------ basis (a2) */
+/* QMCBasisFunction::evaluateBasisFunctions, QMcBeaver/src/QMCBasisFunction.cpp:287-403,
+ * including the exponent cache keyed on the previous primitive (:310,372-379). */
+static void basis_eval(const orc_system *s, const double *R, int start, int stop, double *chi /* [nUP][5][K] */)
+{
+  int K = s->K;
+  double temp1 = 0, temp2 = 0, temp3x = 0, temp3y = 0, temp3z = 0;
+  int el = 0;
+  for (int idx = start; idx <= stop; idx++) {
+    int bf = 0;
+    double p0 = 0.0;
+    for (int atom = 0; atom < s->M; atom++) {
+      double Xc[3];
+      for (int x = 0; x < 3; x++) Xc[x] = R[3 * idx + x] - s->nuc_xyz[3 * atom + x];
+      const int numl = s->atom_lmax[atom] + 1;
+      const int numn = numl > 3 ? numl : 3;
+      double xyz_abc[3][16][3];
+      for (int x = 0; x < 3; x++) {
+        xyz_abc[x][0][0] = 1.0;
+        xyz_abc[x][1][0] = Xc[x];
+        for (int abc = 2; abc < numn; abc++) xyz_abc[x][abc][0] = xyz_abc[x][1][0] * xyz_abc[x][abc - 1][0];
+        xyz_abc[x][0][1] = 0.0;
+        xyz_abc[x][0][2] = 0.0;
+        for (int abc = 1; abc < numn; abc++) {
+          xyz_abc[x][abc][1] = abc / xyz_abc[x][1][0];
+          xyz_abc[x][abc][2] = abc * (abc - 1.0) / xyz_abc[x][2][0];
+        }
+      }
+      double r_sq = xyz_abc[0][2][0] + xyz_abc[1][2][0] + xyz_abc[2][2][0];
+      int nbf = s->atom_nbf[atom];
+      int f0 = s->atom_first[atom];
+      for (int j = 0; j < nbf; j++) {
+        int k = f0 + j;
+        int a = s->bf_pow[3 * k], b = s->bf_pow[3 * k + 1], c = s->bf_pow[3 * k + 2];
+        double xyzA0 = xyz_abc[0][a][0] * xyz_abc[1][b][0] * xyz_abc[2][c][0];
+        double xyzA1 = 4.0 * (a + b + c) + 6.0;
+        double x_val = 0, x_grx = 0, x_gry = 0, x_grz = 0, x_lap = 0;
+        int np = s->bf_nprim[k];
+        const double *ex = s->pexp + s->bf_off[k];
+        const double *co = s->pcoef + s->bf_off[k];
+        for (int i = 0; i < np; i++) {
+          if (fabs(p0 - ex[i]) > 1e-10) {
+            p0 = ex[i];
+            temp1 = exp(-p0 * r_sq);
+            temp2 = 4.0 * r_sq * p0 * p0;
+            temp3x = -2.0 * p0 * xyz_abc[0][1][0];
+            temp3y = -2.0 * p0 * xyz_abc[1][1][0];
+            temp3z = -2.0 * p0 * xyz_abc[2][1][0];
+          }
+          double exp_term = temp1 * co[i] * xyzA0;
+          x_val += exp_term;
+          x_grx += exp_term * (xyz_abc[0][a][1] + temp3x);
+          x_gry += exp_term * (xyz_abc[1][b][1] + temp3y);
+          x_grz += exp_term * (xyz_abc[2][c][1] + temp3z);
+          x_lap += exp_term * (xyz_abc[0][a][2] + xyz_abc[1][b][2] + xyz_abc[2][c][2] - p0 * xyzA1 + temp2);
+        }
+        double *o = chi + (size_t)el * 5 * K;
+        o[0 * K + bf] = x_val;
+        o[1 * K + bf] = x_grx;
+        o[2 * K + bf] = x_gry;
+        o[3 * K + bf] = x_grz;
+        o[4 * K + bf] = x_lap;
+        bf++;
+      }
+    }
+    el++;
+  }
+}
+
+void orc_basis_at(const orc_system *s, const double *r, double *out)
+{
+  /* evaluate a single position as electron 0 */
+  double *R = (double *)malloc(sizeof(double) * 3);
+  R[0] = r[0]; R[1] = r[1]; R[2] = r[2];
+  basis_eval(s, R, 0, 0, out);
+  free(R);
+}
+
+/* ----------------------------------------------------- contraction (a3) */
+/* Array2D::gemm with rhsIsTransposed (QMcBeaver/include/Array2D.h:473-485):
+ * D[e][o] = sum_k chi[e][k] * C[o][k], k ascending. */
+static void contract(const orc_system *s, const double *chi, int nUP, const double *C, int n, double *D /* [5][nUP][n] */)
+{
+  int K = s->K;
+  for (int q = 0; q < 5; q++)
+    for (int e = 0; e < nUP; e++)
+      for (int o = 0; o < n; o++) {
+        const double *A = chi + ((size_t)e * 5 + q) * K;
+        const double *B = C + (size_t)o * K;
+        double cij = 0;
+        for (int k = 0; k < K; k++) cij += A[k] * B[k];
+        D[((size_t)q * nUP + e) * n + o] = cij;
+      }
+}
+
+/* ---------------------------------------------------------- LU (a4) */
+/* Array2D::ludcmp (QMcBeaver/include/Array2D.h:1204-1340), Crout with implicit
+ * row scaling and long double accumulators. a is n x n row-major, destroyed. */
+static void ludcmp(double *a, int n, int *indx, double *d, int *calcOK)
+{
+  int imax = -1;
+  long double big, dum, temp, sum;
+  double *vv = (double *)malloc(sizeof(double) * (n ? n : 1));
+  *calcOK = 1;
+  *d = 1.0;
+  for (int i = 0; i < n; i++) {
+    big = 0.0L;
+    for (int j = 0; j < n; j++)
+      if ((temp = (double)fabs(a[i * n + j])) > big) big = temp;
+    if (big == 0.0L) {
+      *calcOK = 0;
+      free(vv);
+      return;
+    }
+    vv[i] = (double)(1.0L / big);
+  }
+  for (int j = 0; j < n; j++) {
+    for (int i = 0; i < j; i++) {
+      sum = -1.0 * a[i * n + j];
+      for (int k = 0; k < i; k++) sum += a[i * n + k] * a[k * n + j];
+      a[i * n + j] = (double)(-1.0 * sum);
+    }
+    big = 0.0L;
+    for (int i = j; i < n; i++) {
+      sum = -1.0 * a[i * n + j];
+      for (int k = 0; k < j; k++) sum += a[i * n + k] * a[k * n + j];
+      a[i * n + j] = (double)(-1.0 * sum);
+      if ((dum = vv[i] * (double)(fabs((double)sum))) >= big) {
+        big = dum;
+        imax = i;
+      }
+    }
+    if (j != imax) {
+      for (int k = 0; k < n; k++) {
+        dum = a[imax * n + k];
+        a[imax * n + k] = a[j * n + k];
+        a[j * n + k] = (double)dum;
+      }
+      *d = -(*d);
+      vv[imax] = vv[j];
+    }
+    indx[j] = imax;
+    if (a[j * n + j] == 0.0) a[j * n + j] = 1e-300;
+    if (j != n) {
+      dum = 1.0L / (a[j * n + j]);
+      for (int i = j + 1; i < n; i++) a[i * n + j] *= (double)dum;
+    }
+  }
+  free(vv);
+}
+
+/* Array2D::lubksb (QMcBeaver/include/Array2D.h:1352-1421) */
+static void lubksb(const double *a, int n, const int *indx, double *b)
+{
+  int ii = -1, ip;
+  long double sum;
+  for (int i = 0; i < n; i++) {
+    ip = indx[i];
+    sum = -1.0 * b[ip];
+    b[ip] = b[i];
+    if (ii >= 0) {
+      for (int j = ii; j <= i - 1; j++) sum += a[i * n + j] * b[j];
+    } else if (sum) {
+      ii = i;
+    }
+    b[i] = (double)(-1.0 * sum);
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    sum = -1.0 * b[i];
+    for (int j = i + 1; j < n; j++) sum += a[i * n + j] * b[j];
+    b[i] = (double)(-1.0 * sum / a[i * n + i]);
+  }
+}
+
+/* Array2D::determinant_and_inverse, NR branch (QMcBeaver/include/Array2D.h:1521-1548).
+ * inv[i*n+j] = (A^-1)(i,j). */
+static void det_and_inverse(double *a, int n, double *inv, double *det, int *calcOK)
+{
+  double d;
+  int *indx = (int *)malloc(sizeof(int) * (n ? n : 1));
+  double *col = (double *)malloc(sizeof(double) * (n ? n : 1));
+  ludcmp(a, n, indx, &d, calcOK);
+  if (*calcOK) {
+    for (int j = 0; j < n; j++) {
+      for (int i = 0; i < n; i++) col[i] = 0.0;
+      col[j] = 1.0;
+      lubksb(a, n, indx, col);
+      for (int i = 0; i < n; i++) inv[i * n + j] = col[i];
+    }
+  }
+  for (int i = 0; i < n; i++) d *= a[i * n + i];
+  *det = d;
+  free(indx);
+  free(col);
+}
+
+/* Array2D::inverseUpdateOneRow (QMcBeaver/include/Array2D.h:1567-1610): inv is
+ * n x n, row = replaced electron, v = the new Slater row. Returns det ratio. */
+static double inverse_update_row(double *inv, int n, int row, const double *v)
+{
+  double detRatio = 0;
+  for (int r = 0; r < n; r++) detRatio += v[r] * inv[r * n + row];
+  double q = 1.0 / detRatio;
+  for (int c = 0; c < n; c++) {
+    if (c == row) continue;
+    double val = 0.0;
+    for (int l = 0; l < n; l++) val += v[l] * inv[l * n + c];
+    val *= q;
+    for (int r = 0; r < n; r++) inv[r * n + c] -= val * inv[r * n + row];
+  }
+  for (int r = 0; r < n; r++) inv[r * n + row] *= q;
+  return detRatio;
+}
+
+/* ---------------------------------------------------- Slater spin (a2-a4) */
+/* QMCSlater::evaluate (QMcBeaver/src/QMCSlater.cpp:828-884) followed by
+ * update_Ds (:390-541) and calculate_DerivativeRatios (:648-764) for one spin. */
+static void slater_spin(const orc_system *s, orc_walker *w, int sp, const double *R, int whichE)
+{
+  int n = sp ? s->nb : s->na;
+  int Start = sp ? s->na : 0;
+  int Stop = Start + n - 1;
+  if (n == 0) return;
+  if (whichE != -1 && (whichE < Start || whichE > Stop)) return;
+  int start = whichE == -1 ? Start : whichE;
+  int stop = whichE == -1 ? Stop : whichE;
+  int nUP = stop - start + 1;
+  int K = s->K;
+  const double *C = sp ? s->mo_b : s->mo_a;
+  double *chi = (double *)malloc(sizeof(double) * (size_t)nUP * 5 * K);
+  double *D = (double *)malloc(sizeof(double) * (size_t)5 * nUP * n);
+  basis_eval(s, R, start, stop, chi);
+  contract(s, chi, nUP, C, n, D);
+  /* splice new derivative rows into D_x / D_xx (QMcBeaver/src/QMCSlater.cpp:465-491) */
+  int iEl = whichE == -1 ? 0 : whichE - Start;
+  for (int e = 0; e < nUP; e++)
+    for (int o = 0; o < n; o++) {
+      for (int d = 0; d < 3; d++) w->Dx[sp][d][(iEl + e) * n + o] = D[((size_t)(1 + d) * nUP + e) * n + o];
+      w->Dxx[sp][(iEl + e) * n + o] = D[((size_t)4 * nUP + e) * n + o];
+    }
+  int calcOK = 1;
+  if (whichE == -1) {
+    det_and_inverse(D, n, w->inv[sp], &w->det[sp], &calcOK);
+  } else {
+    double ratio = inverse_update_row(w->inv[sp], n, whichE - Start, D);
+    if (ratio != 0.0)
+      w->det[sp] *= ratio;
+    else
+      calcOK = 0;
+  }
+  w->sing[sp] = !calcOK;
+  if (calcOK) {
+    double lap_PR = 0.0;
+    double *g = w->rDx[sp];
+    for (int e = 0; e < n; e++) g[3 * e] = g[3 * e + 1] = g[3 * e + 2] = 0.0;
+    const double *inv = w->inv[sp];
+    for (int o = 0; o < n; o++)
+      for (int e = 0; e < n; e++) {
+        double inv_v = inv[o * n + e];
+        lap_PR += w->Dxx[sp][e * n + o] * inv_v;
+        g[3 * e + 0] += w->Dx[sp][0][e * n + o] * inv_v;
+        g[3 * e + 1] += w->Dx[sp][1][e * n + o] * inv_v;
+        g[3 * e + 2] += w->Dx[sp][2][e * n + o] * inv_v;
+      }
+    w->rDxx[sp] = lap_PR;
+  }
+  free(chi);
+  free(D);
+}
+
+/* ------------------------------------------------------------ Jastrow (a6) */
+/* FixedCuspPadeCorrelationFunction::evaluate (QMcBeaver/src/FixedCuspPadeCorrelationFunction.cpp:89-111)
+ * with Polynomial::evaluateAll (QMcBeaver/src/Polynomial.cpp:127-148). */
+static void poly_all(const double *c, int len, double x, double *f, double *df, double *d2f)
+{
+  int n = len - 1;
+  *f = c[n];
+  *df = 0.0;
+  *d2f = 0.0;
+  for (int i = n - 1; i >= 0; i--) {
+    *d2f = *d2f * x + *df;
+    *df = *df * x + *f;
+    *f = *f * x + c[i];
+  }
+  *d2f *= 2;
+}
+
+static void pade(const orc_system *s, int idx, double r, double *u, double *du, double *d2u)
+{
+  double a, ap, app, b, bp, bpp;
+  poly_all(s->pnum + idx * QMCB_PADE_MAX, s->pnn[idx], r, &a, &ap, &app);
+  poly_all(s->pden + idx * QMCB_PADE_MAX, s->pnd[idx], r, &b, &bp, &bpp);
+  double aDIVb = a / b;
+  double bpDIVb = bp / b;
+  double apDIVb = ap / b;
+  *u = aDIVb;
+  *du = apDIVb - bpDIVb * aDIVb;
+  *d2u = (app - bpp * aDIVb) / b - 2 * bpDIVb * (*du);
+}
+
+/* QMCJastrowElectronElectron::collectForPair (QMcBeaver/src/QMCJastrowElectronElectron.cpp:221-268) */
+static void collect_pair(const orc_system *s, orc_walker *w, int E1, int E2, int f)
+{
+  int N = s->N;
+  double r = w->rij[E1 * N + E2];
+  double u, du, d2u;
+  pade(s, f, r, &u, &du, &d2u);
+  double Uij = u, Uij_x = du, Uij_xx = 2.0 * (2.0 / r * Uij_x + d2u);
+  w->U -= w->Uij[E1 * N + E2];
+  w->U += Uij;
+  w->Uij[E1 * N + E2] = Uij;
+  for (int i = 0; i < 3; i++) {
+    double temp = w->Uij_x[(E1 * N + E2) * 3 + i];
+    w->U_x[E1 * 3 + i] -= temp;
+    w->U_x[E2 * 3 + i] += temp;
+    temp = Uij_x * w->rij_uvec[(E1 * N + E2) * 3 + i];
+    w->Uij_x[(E1 * N + E2) * 3 + i] = temp;
+    w->U_x[E1 * 3 + i] += temp;
+    w->U_x[E2 * 3 + i] -= temp;
+  }
+  w->U_xx -= w->Uij_xx[E1 * N + E2];
+  w->U_xx += Uij_xx;
+  w->Uij_xx[E1 * N + E2] = Uij_xx;
+}
+
+/* QMCJastrowElectronElectron::updateOne / updateAll (:68-219) */
+static void jastrow_ee(const orc_system *s, orc_walker *w, int whichE)
+{
+  int na = s->na, nb = s->nb, N = s->N;
+  int fA = (na > 0 && nb > 0) ? s->ee[0] : -1;
+  int fUU = na > 1 ? s->ee[1] : -1;
+  int fDD = nb > 1 ? s->ee[2] : -1;
+  if (whichE != -1) {
+    int E = whichE;
+    int isAlpha = E < na;
+    if (fA >= 0) {
+      if (isAlpha)
+        for (int EB = na; EB < N; EB++) collect_pair(s, w, EB, E, fA);
+      else
+        for (int EA = 0; EA < na; EA++) collect_pair(s, w, E, EA, fA);
+    }
+    if (fUU >= 0 && isAlpha) {
+      for (int EA = 0; EA < E; EA++) collect_pair(s, w, E, EA, fUU);
+      for (int EA = E + 1; EA < na; EA++) collect_pair(s, w, EA, E, fUU);
+    }
+    if (fDD >= 0 && !isAlpha) {
+      for (int EB = na; EB < E; EB++) collect_pair(s, w, E, EB, fDD);
+      for (int EB = E + 1; EB < N; EB++) collect_pair(s, w, EB, E, fDD);
+    }
+  } else {
+    if (fA >= 0)
+      for (int E1 = 0; E1 < na; E1++)
+        for (int E2 = na; E2 < N; E2++) collect_pair(s, w, E2, E1, fA);
+    if (fUU >= 0)
+      for (int E1 = 0; E1 < na; E1++)
+        for (int E2 = 0; E2 < E1; E2++) collect_pair(s, w, E1, E2, fUU);
+    if (fDD >= 0)
+      for (int E1 = na; E1 < N; E1++)
+        for (int E2 = na; E2 < E1; E2++) collect_pair(s, w, E1, E2, fDD);
+  }
+}
+
+/* QMCJastrowElectronNuclear::evaluate (QMcBeaver/src/QMCJastrowElectronNuclear.cpp:54-187) */
+static void jastrow_en(const orc_system *s, orc_walker *w, int whichE)
+{
+  int M = s->M, N = s->N, na = s->na;
+  for (int nuc = 0; nuc < M; nuc++) {
+    for (int e = 0; e < N; e++) {
+      if (whichE != e && whichE != -1) continue;
+      int f = e < na ? s->en_up[nuc] : s->en_dn[nuc];
+      if (f < 0) continue;
+      double r = w->riA[e * M + nuc];
+      double u, du, d2u;
+      pade(s, f, r, &u, &du, &d2u);
+      double UiA = u, UiA_x = du, UiA_xx = 2.0 / r * UiA_x + d2u;
+      w->U -= w->UiA[e * M + nuc];
+      w->U += UiA;
+      w->UiA[e * M + nuc] = UiA;
+      w->U_xx -= w->UiA_xx[e * M + nuc];
+      w->U_xx += UiA_xx;
+      w->UiA_xx[e * M + nuc] = UiA_xx;
+      for (int i = 0; i < 3; i++) {
+        double temp = w->UiA_x[(e * M + nuc) * 3 + i];
+        w->U_x[e * 3 + i] -= temp;
+        temp = UiA_x * w->riA_uvec[(e * M + nuc) * 3 + i];
+        w->UiA_x[(e * M + nuc) * 3 + i] = temp;
+        w->U_x[e * 3 + i] += temp;
+      }
+    }
+  }
+}
+
+/* -------------------------------------------------------- potential (a7) */
+/* QMCPotential_Energy::evaluate / calc_P_en / calc_P_ee (QMcBeaver/src/QMCPotential_Energy.cpp:242-333) */
+static void potential(const orc_system *s, orc_walker *w)
+{
+  int M = s->M, N = s->N;
+  double Pen = 0.0;
+  for (int nuc = 0; nuc < M; nuc++) {
+    double Zeff = s->nuc_z[nuc];
+    for (int el = 0; el < N; el++) Pen -= Zeff / w->riA[el * M + nuc];
+  }
+  double Pee = 0.0;
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < i; j++) Pee += (-1.0 * -1.0) / w->rij[i * N + j];
+  w->PE = s->Pnn + Pee + Pen;
+  w->neE = Pen;
+  w->eeE = Pee;
+}
+
+/* ------------------------------------------------------- psi quantities (a5) */
+/* QMCSCFJastrow::calculate_Psi_quantities / update_SCF / calculate_Modified_Grad_PsiRatio
+ * (QMcBeaver/src/QMCSCFJastrow.cpp:196-472) and calculate_E_Local (QMcBeaver/include/QMCSCFJastrow.h:311-314). */
+static void psi_quantities(const orc_system *s, orc_walker *w, const double *R)
+{
+  int N = s->N, na = s->na, nb = s->nb, M = s->M;
+  if (w->sing[0] || w->sing[1]) {
+    w->singular = 1;
+  } else {
+    w->D_xx = 0.0;
+    for (int i = 0; i < 3 * N; i++) w->D_x[i] = 0.0;
+    double termPR = 1.0;
+    if (na > 0) w->D_xx += termPR * w->rDxx[0];
+    if (nb > 0) w->D_xx += termPR * w->rDxx[1];
+    for (int e = 0; e < na; e++)
+      for (int k = 0; k < 3; k++) w->D_x[e * 3 + k] += termPR * w->rDx[0][e * 3 + k];
+    for (int e = 0; e < nb; e++)
+      for (int k = 0; k < 3; k++) w->D_x[(e + na) * 3 + k] += termPR * w->rDx[1][e * 3 + k];
+    double L = w->D_xx + w->U_xx;
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < 3; j++) {
+        w->grad[i * 3 + j] = w->D_x[i * 3 + j] + w->U_x[i * 3 + j];
+        L += w->U_x[i * 3 + j] * w->D_x[i * 3 + j] * 2.0;
+        L += w->U_x[i * 3 + j] * w->U_x[i * 3 + j];
+      }
+    w->lap = L;
+  }
+  /* modified quantum force */
+  if (s->qf_mod == QMCB_QF_NONE) {
+    for (int i = 0; i < 3 * N; i++) w->mgrad[i] = w->grad[i];
+  } else if (s->qf_mod == QMCB_QF_UMRIGAR93_EQUAL) {
+    double a = s->qf_a;
+    double magsq = 0.0;
+    for (int i = 0; i < 3 * N; i++) magsq += w->grad[i] * w->grad[i];
+    double factor = (-1.0 + sqrt(1.0 + 2 * a * magsq * s->dt)) / (a * magsq * s->dt);
+    for (int i = 0; i < 3 * N; i++) w->mgrad[i] = w->grad[i] * factor;
+  } else {
+    for (int i = 0; i < N; i++) {
+      /* QMCMolecule::findClosestNucleusIndex: smallest riA, first on ties */
+      int cn = 0;
+      for (int j = 1; j < M; j++)
+        if (w->riA[i * M + j] < w->riA[i * M + cn]) cn = j;
+      double Zc = s->nuc_z[cn];
+      double nv[3], ev[3], d2 = 0.0, temp;
+      for (int x = 0; x < 3; x++) {
+        temp = R[3 * i + x] - s->nuc_xyz[3 * cn + x];
+        nv[x] = temp;
+        d2 += temp * temp;
+      }
+      double inv_len = 1.0 / sqrt(d2);
+      for (int x = 0; x < 3; x++) nv[x] *= inv_len;
+      for (int x = 0; x < 3; x++) ev[x] = w->grad[3 * i + x];
+      double ev2 = ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2];
+      if (fabs(ev2) < 1e-10) {
+        for (int x = 0; x < 3; x++) ev[x] *= 0.0;
+      } else {
+        double sc = 1.0 / sqrt(ev2);
+        for (int x = 0; x < 3; x++) ev[x] *= sc;
+      }
+      temp = Zc * Zc * d2;
+      double dotp = 0;
+      for (int x = 0; x < 3; x++) dotp += nv[x] * ev[x];
+      double a = 0.5 * (1.0 + dotp) + temp / (10.0 * (4.0 + temp));
+      double factor;
+      if (fabs(ev2) < 1e-10)
+        factor = 1.0;
+      else
+        factor = (-1.0 + sqrt(1.0 + 2.0 * a * ev2 * s->dt)) / (a * ev2 * s->dt);
+      for (int x = 0; x < 3; x++) w->mgrad[3 * i + x] = w->grad[3 * i + x] * factor;
+    }
+  }
+  double lm = 0.0, lu = 0.0;
+  for (int i = 0; i < 3 * N; i++) {
+    lm += w->mgrad[i] * w->mgrad[i];
+    lu += w->grad[i] * w->grad[i];
+  }
+  lm = sqrt(lm);
+  lu = sqrt(lu);
+  if (isnan(lm) || isnan(lu) || isnan(lm / lu) || lu == 0) w->singular = 1;
+  w->KE = -0.5 * w->lap;
+  w->E_L = -0.5 * w->lap + w->PE;
+  w->logpsi = log(fabs(w->det[0])) + log(fabs(w->det[1])) + w->U;
+  w->sign = (w->det[0] * w->det[1] < 0) ? -1.0 : 1.0;
+}
+
+/* --------------------------------------------------------- evaluate (a1) */
+int orc_evaluate(const orc_system *s, orc_walker **walkers, const double *R, int num, int whichE)
+{
+  int N = s->N;
+  for (int wi = 0; wi < num; wi++) {
+    orc_walker *w = walkers[wi];
+    const double *Rw = R + (size_t)wi * N * 3;
+    w->singular = 0;
+    update_distances(s, w, Rw, whichE);
+    /* QMCJastrow::evaluate: e-n then e-e (QMcBeaver/src/QMCJastrow.cpp:134-151) */
+    jastrow_en(s, w, whichE);
+    jastrow_ee(s, w, whichE);
+    slater_spin(s, w, 0, Rw, whichE);
+    slater_spin(s, w, 1, Rw, whichE);
+    potential(s, w);
+    psi_quantities(s, w, Rw);
+  }
+  return 0;
+}
+
+void orc_walker_get(const orc_walker *w, double *sc, double *grad, double *mgrad)
+{
+  int N = w->s->N;
+  sc[0] = w->E_L;
+  sc[1] = w->KE;
+  sc[2] = w->PE;
+  sc[3] = w->neE;
+  sc[4] = w->eeE;
+  sc[5] = w->U;
+  sc[6] = w->U_xx;
+  sc[7] = w->D_xx;
+  sc[8] = w->s->na > 0 ? w->det[0] : 1.0;
+  sc[9] = w->s->nb > 0 ? w->det[1] : 1.0;
+  sc[10] = w->singular ? 1.0 : 0.0;
+  sc[11] = w->logpsi;
+  sc[12] = w->sign;
+  sc[13] = w->sign * exp(w->logpsi);
+  for (int i = 0; i < 3 * N; i++) {
+    if (grad) grad[i] = w->grad[i];
+    if (mgrad) mgrad[i] = w->mgrad[i];
+  }
+}
+
+void orc_walker_inverse(const orc_walker *w, int beta, double *out)
+{
+  int n = beta ? w->s->nb : w->s->na;
+  memcpy(out, w->inv[beta ? 1 : 0], sizeof(double) * n * n);
+}

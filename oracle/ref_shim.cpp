@@ -1,0 +1,130 @@
+// ref_shim.cpp -- C entry points into the reference QMcBeaver CPU code.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is compiled together with the
+// reference's own sources (read-only tree, see oracle/Makefile) into
+// oracle/_ref/libqmcref.so.  It is used by tests/golden/make_golden.py to
+// produce golden vectors and by tests that pin the C restatement
+// (oracle/qmc_oracle.c) to the reference.  Nothing in the product links it.
+//
+// It drives the reference exactly the way QMCWalker / QMCRun do:
+//   * QMCWalkerData::initialize(3,-1,-1)        QMcBeaver/src/QMCWalkerData.cpp:56
+//   * QMCWalkerData::updateDistances(R)         QMcBeaver/src/QMCWalkerData.cpp:302
+//   * QMCSCFJastrow::evaluate(wd[], R[], num)   QMcBeaver/src/QMCSCFJastrow.cpp:91
+// with whichE = -1 for a full (LU) evaluation and whichE = e for a single
+// electron update (Sherman-Morrison path, requires one_e_per_iter 1 in the
+// input file, QMcBeaver/src/QMCSlater.cpp:700-711).
+
+#include "QMCInput.h"
+#include "QMCSCFJastrow.h"
+#include "QMCWalkerData.h"
+#include "Array1D.h"
+#include "Array2D.h"
+#include <cmath>
+#include <vector>
+
+// The reference defines these globals next to main() in QMcBeaver.cpp,
+// which is left out of the library; they are defined here instead.
+QMCInput globalInput;
+int argc = 0;
+char **argv = 0;
+
+static QMCSCFJastrow *g_qmf = 0;
+static int g_nel = 0;
+
+extern "C" {
+
+int ref_init(const char *ckmf)
+{
+  globalInput.read(std::string(ckmf));
+  g_nel = globalInput.WF.getNumberElectrons();
+  g_qmf = new QMCSCFJastrow();
+  g_qmf->initialize(&globalInput, 0);
+  return g_nel;
+}
+
+int ref_num_electrons(void) { return g_nel; }
+int ref_num_alpha(void) { return globalInput.WF.getNumberElectrons(true); }
+int ref_num_basis(void) { return globalInput.WF.getNumberBasisFunctions(); }
+
+void *ref_walker_new(void)
+{
+  QMCWalkerData *wd = new QMCWalkerData();
+  wd->initialize(3, -1, -1);
+  return wd;
+}
+
+void ref_walker_free(void *w) { delete (QMCWalkerData *)w; }
+
+void *ref_walker_clone(void *w)
+{
+  QMCWalkerData *src = (QMCWalkerData *)w;
+  QMCWalkerData *dst = new QMCWalkerData();
+  dst->initialize(3, -1, -1);
+  *dst = *src;
+  return dst;
+}
+
+// Evaluates `num` walkers at positions R[num][N][3] with a uniform whichE,
+// as QMCRun::propagateWalkers does (QMcBeaver/src/QMCRun.cpp:43-55).
+int ref_evaluate(void **walkers, const double *R, int num, int whichE)
+{
+  std::vector<Array2D<double> > Rs(num);
+  Array1D<Array2D<double> *> rp(num);
+  Array1D<QMCWalkerData *> wp(num);
+  for (int w = 0; w < num; w++) {
+    Rs[w].allocate(g_nel, 3);
+    for (int e = 0; e < g_nel; e++)
+      for (int d = 0; d < 3; d++) Rs[w](e, d) = R[(w * g_nel + e) * 3 + d];
+    QMCWalkerData *wd = (QMCWalkerData *)walkers[w];
+    wd->whichE = whichE;
+    wd->singular = false;
+    wd->updateDistances(Rs[w]);
+    rp(w) = &Rs[w];
+    wp(w) = wd;
+  }
+  g_qmf->evaluate(wp, rp, num);
+  return 0;
+}
+
+// scalars: [0] E_L, [1] kinetic, [2] potential, [3] e-n potential,
+// [4] e-e potential, [5] ln Jastrow U, [6] lap(lnJ) U_xx, [7] lap(D)/D D_xx,
+// [8] alpha determinant, [9] beta determinant, [10] singular flag,
+// [11] ln|psi| (= ln|detA detB| + U), [12] sign(psi), [13] (double)psi
+// grad[N][3]: gradPsiRatio; mgrad[N][3]: modifiedGradPsiRatio
+void ref_walker_get(void *w, double *scalars, double *grad, double *mgrad)
+{
+  QMCWalkerData *wd = (QMCWalkerData *)w;
+  scalars[0] = wd->localEnergy;
+  scalars[1] = wd->kineticEnergy;
+  scalars[2] = wd->potentialEnergy;
+  scalars[3] = wd->neEnergy;
+  scalars[4] = wd->eeEnergy;
+  scalars[5] = wd->U;
+  scalars[6] = wd->U_xx;
+  scalars[7] = wd->D_xx;
+  double da = wd->DcA.dim1() > 0 ? wd->DcA(0) : 1.0;
+  double db = wd->DcB.dim1() > 0 ? wd->DcB(0) : 1.0;
+  scalars[8] = da;
+  scalars[9] = db;
+  scalars[10] = wd->singular ? 1.0 : 0.0;
+  scalars[11] = std::log(std::fabs(da)) + std::log(std::fabs(db)) + wd->U;
+  scalars[12] = (da * db < 0) ? -1.0 : 1.0;
+  scalars[13] = (double)wd->psi;
+  for (int e = 0; e < g_nel; e++)
+    for (int d = 0; d < 3; d++) {
+      if (grad) grad[e * 3 + d] = wd->gradPsiRatio(e, d);
+      if (mgrad) mgrad[e * 3 + d] = wd->modifiedGradPsiRatio(e, d);
+    }
+}
+
+// The alpha / beta inverse Slater matrices as stored by the reference
+// (Dc_invA(0)(o,e), QMcBeaver/src/QMCWalkerData.cpp:69-76).
+void ref_walker_inverse(void *w, int beta, double *out)
+{
+  QMCWalkerData *wd = (QMCWalkerData *)w;
+  Array2D<double> &inv = beta ? wd->Dc_invB(0) : wd->Dc_invA(0);
+  for (int i = 0; i < inv.dim1(); i++)
+    for (int j = 0; j < inv.dim2(); j++) out[i * inv.dim2() + j] = inv(i, j);
+}
+
+} // extern "C"

@@ -1,0 +1,133 @@
+"""ctypes mirror of the C-ABI structs in include/qmcb200.h and the packing of
+a :class:`~qmcbeaver_b200.system.MolecularSystem` into ``qmcb_system_desc``."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .system import PADE_MAX, MolecularSystem
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+# constants of include/qmcb200.h
+QMCB_VMC, QMCB_DMC = 0, 1
+QMCB_NO_IMPORTANCE_SAMPLING, QMCB_IMPORTANCE_SAMPLING = 0, 1
+QMCB_QF_NONE, QMCB_QF_UMRIGAR93_EQUAL, QMCB_QF_UMRIGAR93_UNEQUAL = 0, 1, 2
+QMCB_EMOD_NONE, QMCB_EMOD_UMRIGAR93, QMCB_EMOD_MODIFIED_UMRIGAR93 = 0, 1, 2
+QMCB_RW_SIMPLE_SYMMETRIC, QMCB_RW_SIMPLE_ASYMMETRIC, QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED = 0, 1, 2
+QMCB_PREC_FP64, QMCB_PREC_MIXED = 0, 1
+QMCB_ST_SINGULAR, QMCB_ST_NAN = 1, 2
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [
+        ("n_nuclei", C.c_int), ("nuc_xyz", _dp), ("nuc_charge", _dp),
+        ("n_alpha", C.c_int), ("n_beta", C.c_int),
+        ("n_basis", C.c_int), ("bf_atom", _ip), ("bf_powers", _ip), ("bf_nprim", _ip), ("bf_prim_offset", _ip),
+        ("n_prim_total", C.c_int), ("prim_exponent", _dp), ("prim_coeff", _dp),
+        ("mo_alpha", _dp), ("mo_beta", _dp),
+        ("n_pade", C.c_int), ("pade_num", _dp), ("pade_den", _dp), ("pade_nnum", _ip), ("pade_nden", _ip),
+        ("ee_pade", C.c_int * 3), ("en_pade_up", _ip), ("en_pade_dn", _ip),
+    ]
+
+
+class RunParams(C.Structure):
+    _fields_ = [
+        ("run_type", C.c_int), ("sampling", C.c_int), ("qf_modification", C.c_int), ("qf_equal_a", C.c_double),
+        ("dt", C.c_double), ("dt_effective", C.c_double), ("energy_modification", C.c_int),
+        ("reweighting", C.c_int), ("energy_trial", C.c_double), ("energy_estimated", C.c_double),
+        ("branching_threshold", C.c_double), ("fusion_threshold", C.c_double),
+        ("old_walker_acceptance", C.c_int), ("refresh_interval", C.c_int), ("precision", C.c_int),
+        ("seed", C.c_uint64),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [
+        ("sum_weight", C.c_double), ("sum_weight_energy", C.c_double), ("sum_weight_energy2", C.c_double),
+        ("sum_accept", C.c_double), ("n_moves", C.c_double), ("final_weight", C.c_double),
+        ("n_walkers", C.c_int), ("n_singular", C.c_int),
+    ]
+
+
+def run_params(**kw) -> RunParams:
+    p = RunParams()
+    p.run_type = QMCB_VMC
+    p.sampling = QMCB_NO_IMPORTANCE_SAMPLING
+    p.qf_modification = QMCB_QF_NONE
+    p.qf_equal_a = 0.5
+    p.dt = 0.09
+    p.dt_effective = -1.0
+    p.energy_modification = QMCB_EMOD_NONE
+    p.reweighting = QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED
+    p.energy_trial = 0.0
+    p.energy_estimated = 0.0
+    p.branching_threshold = 2.0
+    p.fusion_threshold = 0.45
+    p.old_walker_acceptance = 50
+    p.refresh_interval = 0
+    p.precision = QMCB_PREC_FP64
+    p.seed = 12345
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    if p.dt_effective < 0:
+        p.dt_effective = p.dt
+    return p
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a: np.ndarray):
+    return a.ctypes.data_as(_ip)
+
+
+class PackedSystem:
+    """Owns the numpy buffers a ``qmcb_system_desc`` points into."""
+
+    def __init__(self, s: MolecularSystem):
+        self.system = s
+        atom, pw, nprim, off, ex, co = s.flat_basis()
+        npade, num, den, nn, nd, ee, en_up, en_dn = s.pade_tables()
+        self._keep = dict(
+            nuc_xyz=np.ascontiguousarray(s.coords, np.float64),
+            nuc_z=np.ascontiguousarray(s.Z, np.float64),
+            atom=atom, pw=np.ascontiguousarray(pw), nprim=nprim, off=off, ex=ex, co=co,
+            mo_a=np.ascontiguousarray(s.mo_alpha(), np.float64),
+            mo_b=np.ascontiguousarray(s.mo_beta(), np.float64) if s.n_beta else np.zeros((1, s.n_basis)),
+            num=np.ascontiguousarray(num), den=np.ascontiguousarray(den), nn=nn, nd=nd,
+            en_up=en_up, en_dn=en_dn,
+        )
+        k = self._keep
+        d = SystemDesc()
+        d.n_nuclei = s.n_nuclei
+        d.nuc_xyz = _d(k["nuc_xyz"])
+        d.nuc_charge = _d(k["nuc_z"])
+        d.n_alpha = s.n_alpha
+        d.n_beta = s.n_beta
+        d.n_basis = s.n_basis
+        d.bf_atom = _i(k["atom"])
+        d.bf_powers = _i(k["pw"])
+        d.bf_nprim = _i(k["nprim"])
+        d.bf_prim_offset = _i(k["off"])
+        d.n_prim_total = len(k["ex"])
+        d.prim_exponent = _d(k["ex"])
+        d.prim_coeff = _d(k["co"])
+        d.mo_alpha = _d(k["mo_a"])
+        d.mo_beta = _d(k["mo_b"])
+        d.n_pade = npade
+        d.pade_num = _d(k["num"])
+        d.pade_den = _d(k["den"])
+        d.pade_nnum = _i(k["nn"])
+        d.pade_nden = _i(k["nd"])
+        for i in range(3):
+            d.ee_pade[i] = int(ee[i])
+        d.en_pade_up = _i(k["en_up"])
+        d.en_pade_dn = _i(k["en_dn"])
+        self.desc = d
+        assert PADE_MAX == 8

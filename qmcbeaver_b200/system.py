@@ -1,0 +1,533 @@
+"""Molecular system description for the Slater-Jastrow walker path.
+
+A :class:`MolecularSystem` holds exactly what QMcBeaver reads from the
+``&geometry``, ``&basis``, ``&wavefunction`` and ``&Jastrow`` sections of a
+``.ckmf`` input for a single-determinant, restricted, all-electron
+calculation with Pade two-body Jastrows:
+
+* nuclei: label, charge Z, position  (QMcBeaver/src/QMCMolecule.cpp, readGeometry)
+* contracted Cartesian Gaussians per atom: type string (``s``, ``px``,
+  ``dxy`` ...), primitive exponents and raw contraction coefficients
+  (QMcBeaver/src/QMCBasisFunctionCoefficients.cpp:84-127; the coefficients
+  are used as given, QMcBeaver/src/QMCBasisFunction.cpp:381, so any
+  normalisation is folded in here)
+* MO coefficients, orbital rows x basis columns, and the occupied orbitals of
+  each spin (QMcBeaver/src/QMCWavefunction.cpp:873-905)
+* Pade correlation functions u(r) = P(r) / Q(r), P(0) = 0, Q(0) = 1, for the
+  up-down, up-up, down-down electron pairs and for each nucleus type
+  (QMcBeaver/src/FixedCuspPadeCorrelationFunction.cpp:34-77)
+
+It also generates the seeded synthetic molecules the benchmark and tests run
+(:func:`make_system`) and writes them as ``.ckmf`` text so the reference CPU
+code reads bit-identical doubles (``%.17g``).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+ELEMENT = {1: "H", 2: "He", 3: "Li", 4: "Be", 5: "B", 6: "C", 7: "N", 8: "O", 9: "F", 10: "Ne"}
+
+SHELL_TYPES = {
+    "s": ["s"],
+    "p": ["px", "py", "pz"],
+    "d": ["dxx", "dyy", "dzz", "dxy", "dxz", "dyz"],
+}
+
+PADE_MAX = 8  # coefficients per polynomial (degree <= 7), matches qmcb200.h
+
+
+def type_to_powers(t: str) -> Tuple[int, int, int]:
+    """Cartesian powers of a basis type string, as type_to_xyz
+    (QMcBeaver/src/QMCBasisFunctionCoefficients.cpp:39-82)."""
+    t = t.lower()
+    lnames = "spdfghi"
+    l = lnames.index(t[0])
+    if len(t) - 1 != l:
+        raise ValueError(f"basis type {t!r} does not have angular momentum {l}")
+    return (t.count("x"), t.count("y"), t.count("z"))
+
+
+@dataclasses.dataclass
+class BasisFunction:
+    type: str
+    exponents: np.ndarray  # (P,)
+    coefficients: np.ndarray  # (P,) raw, normalisation folded in
+
+    @property
+    def powers(self) -> Tuple[int, int, int]:
+        return type_to_powers(self.type)
+
+
+@dataclasses.dataclass
+class Pade:
+    """u(r) = sum_i num[i] r^i / sum_i den[i] r^i with num[0] = 0, den[0] = 1."""
+    num: Sequence[float]
+    den: Sequence[float]
+
+    @staticmethod
+    def fixed_cusp(cusp: float, b: float) -> "Pade":
+        # FixedCuspPade with one numerator constant and one denominator
+        # parameter: numerator [0, cusp], denominator [1, b]
+        # (QMcBeaver/src/FixedCuspPadeCorrelationFunction.cpp:56-72).
+        return Pade(num=[0.0, float(cusp)], den=[1.0, float(b)])
+
+    def evaluate(self, r: float) -> Tuple[float, float, float]:
+        """(u, u', u'') with the reference's operation order
+        (QMcBeaver/src/FixedCuspPadeCorrelationFunction.cpp:89-111,
+        QMcBeaver/src/Polynomial.cpp:127-148)."""
+        a, ap, app = _poly_all(self.num, r)
+        b, bp, bpp = _poly_all(self.den, r)
+        aDIVb = a / b
+        bpDIVb = bp / b
+        apDIVb = ap / b
+        f = aDIVb
+        df = apDIVb - bpDIVb * aDIVb
+        d2f = (app - bpp * aDIVb) / b - 2 * bpDIVb * df
+        return f, df, d2f
+
+
+def _poly_all(c: Sequence[float], x: float) -> Tuple[float, float, float]:
+    n = len(c) - 1
+    f = c[n]
+    df = 0.0
+    d2f = 0.0
+    for i in range(n - 1, -1, -1):
+        d2f = d2f * x + df
+        df = df * x + f
+        f = f * x + c[i]
+    return f, df, 2 * d2f
+
+
+@dataclasses.dataclass
+class MolecularSystem:
+    labels: List[str]
+    Z: np.ndarray  # (M,) float charges
+    coords: np.ndarray  # (M,3)
+    basis: List[List[BasisFunction]]  # per atom
+    mo: np.ndarray  # (n_orb, K), orbital rows
+    n_alpha: int
+    n_beta: int
+    alpha_occ: np.ndarray  # indices of occupied orbitals (alpha)
+    beta_occ: np.ndarray
+    ee_anti: Optional[Pade]
+    ee_para_up: Optional[Pade]
+    ee_para_dn: Optional[Pade]
+    en_up: Dict[str, Pade]  # by nucleus label
+    en_dn: Dict[str, Pade]
+    name: str = "synthetic"
+
+    # ------------------------------------------------------------------ sizes
+    @property
+    def n_nuclei(self) -> int:
+        return len(self.labels)
+
+    @property
+    def n_electrons(self) -> int:
+        return self.n_alpha + self.n_beta
+
+    @property
+    def n_basis(self) -> int:
+        return sum(len(fs) for fs in self.basis)
+
+    @property
+    def charge(self) -> int:
+        return int(round(float(self.Z.sum()))) - self.n_electrons
+
+    def flat_basis(self):
+        """Flattened basis tables in the reference's function order
+        (atoms in geometry order, functions in file order;
+        QMcBeaver/src/QMCBasisFunction.cpp:177-201)."""
+        atom, pw, nprim, off, ex, co = [], [], [], [], [], []
+        for a, fs in enumerate(self.basis):
+            for f in fs:
+                atom.append(a)
+                pw.append(f.powers)
+                nprim.append(len(f.exponents))
+                off.append(len(ex))
+                ex.extend(float(v) for v in f.exponents)
+                co.extend(float(v) for v in f.coefficients)
+        return (np.asarray(atom, np.int32), np.asarray(pw, np.int32).reshape(-1, 3),
+                np.asarray(nprim, np.int32), np.asarray(off, np.int32),
+                np.asarray(ex, np.float64), np.asarray(co, np.float64))
+
+    def mo_alpha(self) -> np.ndarray:
+        return np.ascontiguousarray(self.mo[self.alpha_occ])
+
+    def mo_beta(self) -> np.ndarray:
+        return np.ascontiguousarray(self.mo[self.beta_occ])
+
+    def pade_tables(self):
+        """Pade table + indices: ee[3] = (anti, up-up, dn-dn), en_up[M], en_dn[M];
+        -1 means no correlation function for that pair."""
+        funcs: List[Pade] = []
+
+        def add(p: Optional[Pade]) -> int:
+            if p is None:
+                return -1
+            funcs.append(p)
+            return len(funcs) - 1
+
+        ee = [add(self.ee_anti), add(self.ee_para_up), add(self.ee_para_dn)]
+        en_up = [add(self.en_up.get(l)) for l in self.labels]
+        en_dn = [add(self.en_dn.get(l)) for l in self.labels]
+        nfun = max(1, len(funcs))
+        num = np.zeros((nfun, PADE_MAX))
+        den = np.zeros((nfun, PADE_MAX))
+        nn = np.zeros(nfun, np.int32)
+        nd = np.zeros(nfun, np.int32)
+        for i, p in enumerate(funcs):
+            if len(p.num) > PADE_MAX or len(p.den) > PADE_MAX:
+                raise ValueError("Pade polynomial too long")
+            num[i, : len(p.num)] = p.num
+            den[i, : len(p.den)] = p.den
+            nn[i] = len(p.num)
+            nd[i] = len(p.den)
+        return (len(funcs), num, den, nn, nd, np.asarray(ee, np.int32),
+                np.asarray(en_up, np.int32), np.asarray(en_dn, np.int32))
+
+    def nuclear_repulsion(self) -> float:
+        """V_nn as calc_P_nn (QMcBeaver/src/QMCPotential_Energy.cpp:285-307)."""
+        v = 0.0
+        M = self.n_nuclei
+        for i in range(M):
+            for j in range(i + 1, M):
+                d = self.coords[i] - self.coords[j]
+                r = math.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+                v += (self.Z[i] * self.Z[j]) / r
+        return float(v)
+
+    def check_exponent_cache(self) -> None:
+        """The reference reuses exp(-a r^2) when consecutive primitives share an
+        exponent, and the cache is not reset between atoms
+        (QMcBeaver/src/QMCBasisFunction.cpp:310,372-379).  A system where the
+        last exponent of one atom equals the first exponent of the next would
+        make the reference reuse a stale value; refuse such systems."""
+        prev_last = None
+        for fs in self.basis:
+            if not fs:
+                continue
+            first = float(fs[0].exponents[0])
+            if prev_last is not None and abs(prev_last - first) <= 1e-10:
+                raise ValueError("exponent shared across atom boundary (stale exp cache in reference)")
+            prev_last = float(fs[-1].exponents[-1])
+
+    # ------------------------------------------------------------ positions
+    def initial_positions(self, n_walkers: int, seed: int = 1, sigma: float = 0.8) -> np.ndarray:
+        """Electrons placed by Gaussians around nuclei, electron e on nucleus
+        e-th in a charge-weighted round robin.  Returns (W, N, 3) float64."""
+        rng = np.random.default_rng(seed)
+        order: List[int] = []
+        zs = [max(1, int(round(z))) for z in self.Z]
+        left = list(zs)
+        while len(order) < self.n_electrons:
+            progressed = False
+            for a in range(self.n_nuclei):
+                if left[a] > 0 and len(order) < self.n_electrons:
+                    order.append(a)
+                    left[a] -= 1
+                    progressed = True
+            if not progressed:
+                left = list(zs)
+        # alternate spins over nuclei: alpha electrons take even slots
+        a_slots = order[0::2][: self.n_alpha]
+        b_slots = order[1::2][: self.n_beta]
+        while len(a_slots) < self.n_alpha:
+            a_slots.append(order[len(a_slots) % len(order)])
+        while len(b_slots) < self.n_beta:
+            b_slots.append(order[len(b_slots) % len(order)])
+        centers = self.coords[np.asarray(a_slots + b_slots)]
+        R = centers[None, :, :] + sigma * rng.standard_normal((n_walkers, self.n_electrons, 3))
+        return np.ascontiguousarray(R, dtype=np.float64)
+
+    # ------------------------------------------------------------ ckmf text
+    def to_ckmf(self, path: str, flags: Optional[Dict[str, object]] = None) -> None:
+        """Writes a QMcBeaver input with the sections the reference parses:
+        &flags (key line / value line, QMcBeaver/src/QMCFlags.cpp:198-206),
+        &geometry, &basis, &wavefunction, &Jastrow."""
+        f = dict(DEFAULT_FLAGS)
+        f.update({
+            "atoms": self.n_nuclei,
+            "charge": self.charge,
+            "norbitals": self.mo.shape[0],
+            "nbasisfunc": self.n_basis,
+            "ndeterminants": 1,
+            "trial_function_type": "restricted",
+        })
+        if flags:
+            f.update(flags)
+        g = "%.17g"
+        out: List[str] = ["# synthetic system " + self.name, "", "&flags"]
+        for k, v in f.items():
+            out.append(k)
+            out.append(" " + (g % v if isinstance(v, float) else str(v)))
+        out.append("&")
+        out.append("&geometry")
+        for l, z, c in zip(self.labels, self.Z, self.coords):
+            out.append(f"{l} {int(round(z))} {g % c[0]} {g % c[1]} {g % c[2]}")
+        out.append("&")
+        out.append("&basis")
+        for l, fs in zip(self.labels, self.basis):
+            maxg = max(len(b.exponents) for b in fs)
+            out.append(f"{l} {len(fs)} {maxg}")
+            for b in fs:
+                out.append(f"  {len(b.exponents)} {b.type}")
+                for e, c in zip(b.exponents, b.coefficients):
+                    out.append(f"    {g % e} {g % c}")
+        out.append("&")
+        out.append("&wavefunction")
+        for row in self.mo:
+            out.append(" ".join(g % v for v in row))
+        out.append("")
+        occ_a = np.zeros(self.mo.shape[0], int)
+        occ_a[self.alpha_occ] = 1
+        occ_b = np.zeros(self.mo.shape[0], int)
+        occ_b[self.beta_occ] = 1
+        out.append("Alpha Occupation")
+        out.append(" ".join(str(v) for v in occ_a))
+        out.append("")
+        out.append("Beta Occupation")
+        out.append(" ".join(str(v) for v in occ_b))
+        out.append("")
+        out.append("CI Coeffs")
+        out.append("1")
+        out.append("")
+        out.append("&")
+        out.append("")
+        out.append("&Jastrow")
+
+        def block(p1: str, p2: str, p: Pade) -> None:
+            # FixedCuspPade: numerator constants first then parameters,
+            # denominator parameters; this writer only emits the
+            # [0, cusp] / [1, b...] form the configs use.
+            if len(p.num) != 2 or p.num[0] != 0.0 or p.den[0] != 1.0:
+                raise ValueError("ckmf writer supports u = a r / (1 + b1 r + ...)")
+            dparams = list(p.den[1:])
+            out.append(f"ParticleTypes:\t{p1}\t{p2}")
+            out.append("CorrelationFunctionType:\tFixedCuspPade")
+            out.append("NumberOfParameterTypes:\t2")
+            out.append(f"NumberOfParametersOfEachType:\t0\t{len(dparams)}")
+            out.append("Parameters:\t" + "\t".join(g % v for v in dparams))
+            out.append("NumberOfConstantTypes:\t1")
+            out.append("NumberOfConstantsOfEachType:\t1")
+            out.append("Constants:\t" + g % p.num[1])
+            out.append("")
+
+        if self.ee_anti is not None and self.n_alpha > 0 and self.n_beta > 0:
+            block("Electron_up", "Electron_down", self.ee_anti)
+        if self.ee_para_up is not None and self.n_alpha > 1:
+            block("Electron_up", "Electron_up", self.ee_para_up)
+        if self.ee_para_dn is not None and self.n_beta > 1:
+            block("Electron_down", "Electron_down", self.ee_para_dn)
+        for l in dict.fromkeys(self.labels):
+            if l in self.en_up:
+                block("Electron_up", l, self.en_up[l])
+            if l in self.en_dn and self.n_beta > 0:
+                block("Electron_down", l, self.en_dn[l])
+        out.append("&Jastrow")
+        out.append("")
+        with open(path, "w") as fh:
+            fh.write("\n".join(out))
+
+
+DEFAULT_FLAGS: Dict[str, object] = {
+    "run_type": "variational",
+    "dt": 0.09,
+    "number_of_walkers": 1,
+    "max_time_steps": 10,
+    "max_time": -1,
+    "one_e_per_iter": 1,
+    "warn_verbosity": 0,
+    "sampling_method": "no_importance_sampling",
+    "QF_modification_type": "none",
+    "energy_modification_type": "none",
+    "energy_cutoff_type": "none",
+    "walker_reweighting_method": "umrigar93_probability_weighted",
+    "branching_method": "nonunit_weight_branching",
+    "branching_threshold": 2.0,
+    "fusion_threshold": 0.45,
+    "equilibration_steps": 0,
+    "walker_initialization_method": "dans_walker_initialization",
+    "replace_electron_nucleus_cusps": 0,
+    "use_three_body_jastrow": 0,
+    "link_Jastrow_parameters": 1,
+    "optimize_Psi": 0,
+    "iseed": -1000,
+    "walkers_per_pass": 1,
+    "output_interval": 100,
+    "energy": -1.0,
+    "chip_and_mike_are_cool": "Yea_Baby!",
+}
+
+
+# ----------------------------------------------------------------- generator
+def _double_factorial(n: int) -> int:
+    r = 1
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
+def _overlap_1d(m: int, p: float) -> float:
+    # int x^(2m) exp(-p x^2) dx
+    return _double_factorial(2 * m - 1) / (2.0 * p) ** m * math.sqrt(math.pi / p)
+
+
+def _self_overlap(powers, ea: float, eb: float) -> float:
+    p = ea + eb
+    s = 1.0
+    for m in powers:
+        s *= _overlap_1d(m, p)
+    return s
+
+
+def _contracted(rng: np.random.Generator, t: str, exps: np.ndarray, raw: np.ndarray) -> BasisFunction:
+    """Primitive normalisation folded into the coefficients, then the
+    contraction normalised to unit self-overlap."""
+    pw = type_to_powers(t)
+    c = np.array([raw[i] / math.sqrt(_self_overlap(pw, exps[i], exps[i])) for i in range(len(exps))])
+    s = 0.0
+    for i in range(len(exps)):
+        for j in range(len(exps)):
+            s += c[i] * c[j] * _self_overlap(pw, exps[i], exps[j])
+    c = c / math.sqrt(s)
+    return BasisFunction(t, exps.copy(), c)
+
+
+def _shell(rng: np.random.Generator, kind: str, nprim: int) -> List[BasisFunction]:
+    exps = np.sort(10.0 ** rng.uniform(-1.0, 2.0, nprim))[::-1].copy()
+    raw = rng.standard_normal(nprim)
+    return [_contracted(rng, t, exps, raw) for t in SHELL_TYPES[kind]]
+
+
+def _place_nuclei(rng: np.random.Generator, M: int, box: float, min_sep: float) -> np.ndarray:
+    pts: List[np.ndarray] = []
+    tries = 0
+    while len(pts) < M:
+        tries += 1
+        if tries > 200000:
+            raise RuntimeError("cannot place nuclei")
+        p = rng.uniform(-box / 2, box / 2, 3)
+        if all(np.linalg.norm(p - q) >= min_sep for q in pts):
+            pts.append(p)
+    return np.asarray(pts)
+
+
+def _distribute_basis(rng: np.random.Generator, Z: Sequence[int], K: int, nprim: int) -> List[List[BasisFunction]]:
+    """Round robin over atoms adding shells until exactly K functions exist.
+    Heavy atoms cycle s, p, s, d, p ...; hydrogen cycles s, p, s, s, p."""
+    heavy = ["s", "p", "s", "d", "p", "s", "d", "p"]
+    light = ["s", "p", "s", "s", "p"]
+    size = {"s": 1, "p": 3, "d": 6}
+    basis: List[List[BasisFunction]] = [[] for _ in Z]
+    idx = [0] * len(Z)
+    left = K
+    while left > 0:
+        for a, z in enumerate(Z):
+            if left == 0:
+                break
+            pat = heavy if z > 2 else light
+            kind = pat[idx[a] % len(pat)]
+            idx[a] += 1
+            if size[kind] > left:
+                kind = "s"
+            basis[a].extend(_shell(rng, kind, nprim))
+            left -= size[kind]
+    return basis
+
+
+def _random_mo(rng: np.random.Generator, K: int, n: int) -> np.ndarray:
+    A = rng.normal(0.0, 1.0 / math.sqrt(K), (K, K))
+    Q, _ = np.linalg.qr(A)
+    return np.ascontiguousarray(Q[:, :n].T)  # orbital rows
+
+
+def _jastrows(labels: Sequence[str], Z: Sequence[float]):
+    ee_anti = Pade.fixed_cusp(0.5, 1.0)
+    ee_para = Pade.fixed_cusp(0.25, 1.0)
+    en = {l: Pade.fixed_cusp(-float(z), 1.5) for l, z in zip(labels, Z)}
+    return ee_anti, ee_para, en
+
+
+def _assemble(name, Zs, coords, basis, n_alpha, n_beta, rng, jastrow=True) -> MolecularSystem:
+    labels = [ELEMENT[int(z)] for z in Zs]
+    K = sum(len(b) for b in basis)
+    n_orb = max(n_alpha, n_beta)
+    mo = _random_mo(rng, K, n_orb)
+    if jastrow:
+        ee_anti, ee_para, en = _jastrows(labels, Zs)
+    else:
+        ee_anti = ee_para = None
+        en = {}
+    sysm = MolecularSystem(
+        labels=labels, Z=np.asarray(Zs, np.float64), coords=np.asarray(coords, np.float64),
+        basis=basis, mo=mo, n_alpha=n_alpha, n_beta=n_beta,
+        alpha_occ=np.arange(n_alpha), beta_occ=np.arange(n_beta),
+        ee_anti=ee_anti, ee_para_up=ee_para, ee_para_dn=ee_para,
+        en_up=dict(en), en_dn=dict(en), name=name)
+    sysm.check_exponent_cache()
+    return sysm
+
+
+def make_water_like(seed: int = 1, jastrow: bool = True) -> MolecularSystem:
+    """The small VMC system: O at the origin, H at (+-1.43, 1.11, 0) bohr,
+    5 up + 5 down electrons, 24 contracted Cartesian Gaussians with 3
+    primitives (O: 2 s + 2 p + 1 d shell = 14; each H: 2 s + 1 p = 5)."""
+    rng = np.random.default_rng(seed)
+    Zs = [8, 1, 1]
+    coords = [[0.0, 0.0, 0.0], [1.43, 1.11, 0.0], [-1.43, 1.11, 0.0]]
+    basis = []
+    for z in Zs:
+        fs: List[BasisFunction] = []
+        kinds = ["s", "s", "p", "p", "d"] if z == 8 else ["s", "s", "p"]
+        for k in kinds:
+            fs.extend(_shell(rng, k, 3))
+        basis.append(fs)
+    return _assemble("water-like C1 (3 nuclei, 10 e, 24 bf)", Zs, coords, basis, 5, 5, rng, jastrow)
+
+
+def make_random_molecule(n_elec: int, n_nuclei: int, n_basis: int, box: float, z_choices: Sequence[int],
+                         seed: int = 1, min_sep: float = 1.8, jastrow: bool = True,
+                         name: Optional[str] = None) -> MolecularSystem:
+    """Synthetic molecule: nuclei uniform in a cube (minimum separation),
+    Z drawn from z_choices (the draw whose total charge is closest to the
+    electron count is kept), n_elec/2 up and n_elec/2 down electrons,
+    n_basis contracted Cartesian Gaussians with 3 primitives each."""
+    rng = np.random.default_rng(seed)
+    best = None
+    for _ in range(256):
+        Zs = list(rng.choice(z_choices, n_nuclei))
+        d = abs(sum(Zs) - n_elec)
+        if best is None or d < best[0]:
+            best = (d, Zs)
+        if d == 0:
+            break
+    Zs = [int(z) for z in best[1]]
+    coords = _place_nuclei(rng, n_nuclei, box, min_sep)
+    basis = _distribute_basis(rng, Zs, n_basis, 3)
+    na = n_elec - n_elec // 2
+    nb = n_elec // 2
+    return _assemble(name or f"synthetic ({n_nuclei} nuclei, {n_elec} e, {n_basis} bf)",
+                     Zs, coords, basis, na, nb, rng, jastrow)
+
+
+# The benchmark / parity workloads, named by what they are.
+WORKLOADS = {
+    "vmc_water_10e": dict(kind="water", walkers=100, run="vmc", dt=0.09, importance=False),
+    "dmc_6nuc_30e": dict(kind="random", n_elec=30, n_nuclei=6, n_basis=120, box=6.0, z=(1, 6, 7, 8),
+                         walkers=16384, run="dmc", dt=0.01, importance=True, refresh=50),
+    "mixed_20nuc_100e": dict(kind="random", n_elec=100, n_nuclei=20, n_basis=400, box=12.0, z=(1, 6, 8),
+                             walkers=65536, run="dmc", dt=0.01, importance=True, refresh=50),
+}
+
+
+def make_system(workload: str, seed: int = 1, jastrow: bool = True) -> MolecularSystem:
+    w = WORKLOADS[workload]
+    if w["kind"] == "water":
+        return make_water_like(seed, jastrow)
+    return make_random_molecule(w["n_elec"], w["n_nuclei"], w["n_basis"], w["box"], w["z"], seed=seed,
+                                jastrow=jastrow, name=workload)
