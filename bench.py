@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 walker path: walker-moves/s of plain-FP64 DMC on the
+30-electron synthetic molecule (6 nuclei, 120 contracted Gaussians, 16,384
+walkers, tau = 0.01, drift-diffusion single-electron moves, nonunit-weight
+branching, full LU refresh every 50 steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one single-electron move (propose, evaluate, accept/reject) of
+every live walker, plus the DMC reweight / branching on the steps that move
+electron 0.  Under torchrun each rank runs an independent walker population
+(walkers shard with no data-path collective; weak scaling); the timed region
+is bracketed by barriers and the max time over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "dmc_6nuc_30e"
+DEFAULT_WALKERS = 16384
+
+
+def bytes_per_move(n: int, N: int) -> int:
+    """Algorithmic HBM bytes of one FP64 walker-move: the moved spin's inverse
+    read + written (2 n^2 8), its gradient / Laplacian rows read for the ratio
+    sums (4 n^2 8), the four new derivative rows written (4 n 8), positions
+    read (24 N), Jastrow gradients read + written (48 N), new gradients
+    written (24 N) and the scalars (24)."""
+    return 2 * n * n * 8 + 4 * n * n * 8 + 4 * n * 8 + 24 * N + 48 * N + 24 * N + 24
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic(workload: str):
+    """Per-walker-move DRAM bytes of the move kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    v = d.get(workload, {}).get("dram_bytes_per_walker_move")
+    return float(v) if v is not None else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dmc_params(seed: int, e0: float):
+    from qmcbeaver_b200.desc import (QMCB_DMC, QMCB_EMOD_UMRIGAR93, QMCB_IMPORTANCE_SAMPLING,
+                                     QMCB_QF_UMRIGAR93_UNEQUAL, run_params)
+    return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
+                      energy_modification=QMCB_EMOD_UMRIGAR93, dt=0.01, refresh_interval=50, reweight_start_step=0,
+                      energy_trial=e0, energy_estimated=e0, seed=seed)
+
+
+def cpu_reference_sample(system, walkers: int, steps: int, procs: int, e0: float):
+    """The reference CPU program on this workload: its DMC when the population
+    survives, else its drift-diffusion VMC steps (same per-move path)."""
+    from oracle import refrun
+    if not refrun.available():
+        return None
+    r = refrun.run_reference(system, "dmc", 0.01, walkers, steps, procs, energy=e0)
+    if not r["ok"]:
+        r = refrun.run_reference(system, "vmc_drift", 0.01, walkers, steps, procs, energy=e0)
+        r["note"] = "reference DMC population collapsed on this trial function; timed its drift-diffusion VMC moves"
+    return r
+
+
+def run_reference_arm(args, rank: int):
+    if rank != 0:
+        return
+    from qmcbeaver_b200.system import make_system
+    from oracle import refrun
+    system = make_system(WORKLOAD, seed=1)
+    procs = os.cpu_count() or 1
+    if not refrun.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/QMcBeaver.x not built (reference tree absent at build time)"}))
+        return
+    vals = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_sample(system, walkers=8, steps=60, procs=procs, e0=-150.0)
+        if r is None:
+            break
+        if i >= args.warmup:
+            vals.append(r["moves_per_s"])
+        last = r
+        if i >= args.warmup and len(vals) >= max(1, min(args.steps, 3)):
+            break
+    v = float(np.mean(vals)) if vals else 0.0
+    sample = (f"{procs} processes x {last['walkers']} walkers x {last['steps']} steps of the reference's "
+              f"{last['mode']} ({last.get('note', 'full DMC')})")
+    out = {"metric": "walker-moves/s", "value": v, "unit": "walker-moves/s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": len(vals), "warmup": args.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "walkers_per_process": last["walkers"], "processes": procs},
+           "cpu_baseline": {"value": v, "unit": "walker-moves/s", "cores": procs, "kind": "reference",
+                            "sample": sample},
+           "e2e": {"value": v, "unit": "walker-moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--warmup", type=int, default=60)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--walkers", type=int, default=DEFAULT_WALKERS)
+    ap.add_argument("--e2e-steps", type=int, default=120)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    from qmcbeaver_b200.api import QMCB200Functions
+    from qmcbeaver_b200.system import make_system
+
+    system = make_system(WORKLOAD, seed=1)
+    W = args.walkers
+    N, n = system.n_electrons, system.n_alpha
+    R0 = system.initial_positions(W, seed=1000 + rank)
+    f = QMCB200Functions(system, 2 * W, dmc_params(seed=77 + rank, e0=0.0))
+    f.init_walkers(R0)
+    e0 = float(np.mean(f.get_walkers()["e_local"]))
+    f.set_params(dmc_params(seed=77 + rank, e0=e0))
+    f.init_walkers(R0)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up
+    f.run_steps(0, args.warmup)
+    stream = torch.cuda.ExternalStream(f.stream)
+    f.set_profiling(True)
+    f.kernel_stats(reset=True)
+    barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t_start.record(stream)
+        st = f.run_steps(args.warmup, args.steps)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = t_start.elapsed_time(t_end)
+    ks = f.kernel_stats(reset=True)
+    f.set_profiling(False)
+    moves = st.n_moves
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        m = torch.tensor([moves], device="cuda", dtype=torch.float64)
+        dist.all_reduce(m, op=dist.ReduceOp.SUM)
+        ms, moves = float(t.item()), float(m.item())
+    value = moves / (ms / 1e3)
+
+    # roofline of the move kernel (dominant): algorithmic bytes per launch / launch time
+    mv = ks["move"]
+    avg_ms = mv["ms"] / max(mv["launches"], 1)
+    walkers_per_launch = st.n_moves / max(mv["launches"], 1)
+    bpm = bytes_per_move(n, N)
+    achieved = bpm * walkers_per_launch / (avg_ms / 1e3) / 1e9
+    peak, peak_kind = read_peaks()
+    tr = read_traffic(WORKLOAD)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tr * walkers_per_launch) if tr is not None else None,
+                "peak_kind": peak_kind, "kernel": "k_move", "algorithmic_bytes_per_walker_move": bpm,
+                "walkers_per_launch": walkers_per_launch, "avg_launch_ms": avg_ms}
+    launches = int(sum(v["launches"] for v in ks.values()))
+
+    # end to end through the public API: one qmcb_run_steps call per step, with
+    # the host's trial energy uploaded before and the step statistics read back after
+    from qmcbeaver_b200.desc import RunParams, StepStats
+    import ctypes
+    barrier()
+    p = dmc_params(seed=77 + rank, e0=e0)
+    e_est = e0
+    sw = swe = 0.0
+    step0 = args.warmup + args.steps
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_moves = 0.0
+    for s in range(args.e2e_steps):
+        f.set_params(p)
+        st2 = f.run_steps(step0 + s, 1)
+        e2e_moves += st2.n_moves
+        if st2.sum_weight > 0:
+            sw += st2.sum_weight
+            swe += st2.sum_weight_energy
+            e_est = swe / sw
+        if st2.final_weight > 0:
+            p.energy_estimated = e_est
+            p.energy_trial = e_est - p.population_control * np.log(st2.final_weight / W)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        m = torch.tensor([e2e_moves], device="cuda", dtype=torch.float64)
+        dist.all_reduce(m, op=dist.ReduceOp.SUM)
+        e2e_s, e2e_moves = float(t.item()), float(m.item())
+    e2e = {"value": e2e_moves / e2e_s, "unit": "walker-moves/s", "h2d_bytes_per_step": ctypes.sizeof(RunParams),
+           "d2h_bytes_per_step": ctypes.sizeof(StepStats) + 16,
+           "api": "qmcb_set_params + qmcb_run_steps(step, 1) per step (host E_T in, step statistics out)"}
+
+    # reference-facing evaluate (QMCFunctions::evaluate shape) with host buffers
+    slots = np.arange(min(W, 4096), dtype=np.int32)
+    Rh = np.ascontiguousarray(R0[: len(slots)])
+    f2 = QMCB200Functions(system, len(slots), dmc_params(seed=1, e0=e0))
+    f2.evaluate(slots, Rh, -1)
+    rng = np.random.default_rng(5)
+    t0 = time.perf_counter()
+    n_eval = 2 * N
+    for s in range(n_eval):
+        e = s % N
+        Rh[:, e] += 0.1 * rng.standard_normal((len(slots), 3))
+        f2.evaluate(slots, Rh, e)
+    ev_s = time.perf_counter() - t0
+    f2.close()
+    e2e_eval = {"value": len(slots) * n_eval / ev_s, "unit": "walker-moves/s", "walkers": len(slots),
+                "h2d_bytes_per_step": len(slots) * (3 * N * 8 + 4),
+                "d2h_bytes_per_step": len(slots) * (6 * N * 8 + 7 * 8 + 1),
+                "api": "qmcb_evaluate(which_e, host R[num][N][3]) per step, no Markov chain"}
+
+    out = {"metric": "walker-moves/s", "value": value, "unit": "walker-moves/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "walkers_per_gpu": W, "electrons": N, "nuclei": system.n_nuclei,
+                      "basis_functions": system.n_basis, "tau": 0.01, "refresh_interval": 50,
+                      "walker_moves": moves, "final_walkers": st.n_walkers,
+                      "parallelism": f"replicas{world}" if world > 1 else "single",
+                      "l2": "walker state > L2 (%.0f MB per GPU)" % (2 * W * f.lay_bytes() / 1e6)
+                      if hasattr(f, "lay_bytes") else "walker state larger than L2"},
+           "roofline": roofline, "gpu_launches": launches, "kernels": ks, "e2e": e2e, "e2e_evaluate_api": e2e_eval,
+           "energy": {"mean_weighted_E_L": st.sum_weight_energy / st.sum_weight if st.sum_weight > 0 else None,
+                      "acceptance": st.sum_accept / max(st.n_moves, 1), "singular": st.n_singular}}
+    clocks = clk.summary()
+    if clocks is not None:
+        out["clocks"] = clocks
+    f.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_sample(system, walkers=8, steps=60, procs=os.cpu_count() or 1, e0=e0)
+        if r is not None:
+            out["cpu_baseline"] = {"value": r["moves_per_s"], "unit": "walker-moves/s", "cores": r["procs"],
+                                   "kind": "reference",
+                                   "sample": f"{r['procs']} processes x {r['walkers']} walkers x {r['steps']} steps "
+                                             f"of the reference's {r['mode']} ({r.get('note', 'full DMC')})"}
+    if rank == 0:
+        print(json.dumps(out))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -112,6 +112,9 @@ typedef struct qmcb_run_params {
   int refresh_interval;      /* steps between full LU refreshes, 0 = never */
   int precision;             /* QMCB_PREC_* */
   uint64_t seed;             /* Philox key for device random numbers */
+  double population_control; /* population_control_parameter (E_T feedback) */
+  int target_walkers;        /* W0 of updateTrialEnergy; 0 = walkers at init */
+  int reweight_start_step;   /* steps below this keep dW = 1 (QMCWalker.cpp:1071) */
 } qmcb_run_params;
 
 /* Ensemble sums over one call of qmcb_run_steps (for E_est / E_T and error bars). */
@@ -198,6 +201,28 @@ int qmcb_get_walkers(qmcb_handle *h, int n, double *R, double *weight, double *e
 /* Copies the full device state of walker slot src into dst (branching,
  * QMcBeaver/src/QMCRun.cpp:758). */
 int qmcb_copy_slot(qmcb_handle *h, int src, int dst);
+
+/* Overwrites the weights of the first n live walkers (host w[n]); for
+ * drivers that manage the population themselves (QMCWalker::setWeight). */
+int qmcb_set_walker_weights(qmcb_handle *h, int n, const double *w);
+
+/* One nonunit-weight branching pass over the live walkers
+ * (QMCRun::branchWalkers / nonunitWeightBranching,
+ * QMcBeaver/src/QMCRun.cpp:89-127,740-814); `step` selects the random
+ * stream of the fusion draws.  Returns the new live count in *n_live. */
+int qmcb_branch(qmcb_handle *h, int step, int *n_live);
+
+/* Kernel timing: when enabled, qmcb_run_steps records CUDA events around
+ * every launch on the handle's stream and accumulates per-kernel totals.
+ * out[2*k] = total ms, out[2*k+1] = launches for k = QMCB_KERNEL_*. */
+#define QMCB_KERNEL_MOVE 0
+#define QMCB_KERNEL_BRANCH 1
+#define QMCB_KERNEL_COPY 2
+#define QMCB_KERNEL_ENERGY 3
+#define QMCB_KERNEL_REFRESH 4
+#define QMCB_KERNEL_COUNT 5
+int qmcb_set_profiling(qmcb_handle *h, int enable);
+int qmcb_get_kernel_stats(qmcb_handle *h, double *out, int reset);
 
 /* Blocks until the handle's stream is idle. */
 int qmcb_synchronize(qmcb_handle *h);

@@ -1,0 +1,263 @@
+// device_common.cuh -- device-side building blocks of the walker path.
+//
+// Layout conventions (HBM):
+//   * per-walker state is one contiguous block of `stride` doubles per slot
+//     (walker-major), so one warp reads a walker's arrays with unit stride;
+//   * Slater values Dv[e][o] are stored electron-major (rows = electrons, as
+//     the reference's Slater matrix), the derivative matrices transposed,
+//     DgT[d][o][e] and DlT[o][e], so the per-move ratio sums read them with
+//     consecutive lanes on consecutive electrons;
+//   * inverse Inv[o][e] = (D^-1)(o,e), the reference's Dc_inv layout
+//     (QMcBeaver/src/QMCWalkerData.cpp:69-76).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define QMCB_FULL_MASK 0xffffffffu
+
+namespace qmcb {
+
+constexpr int kPadeMax = 8;
+
+// Scalars kept per walker (offsets inside the SC block of a walker).
+enum Sc {
+  SC_U = 0,        // ln Jastrow
+  SC_UXX,          // lap ln J
+  SC_LAPR_A,       // lap(D_a)/D_a  (rDc_xxA)
+  SC_LAPR_B,
+  SC_LOGDET_A,     // ln |det D_a|
+  SC_LOGDET_B,
+  SC_SIGN_A,       // sign det D_a
+  SC_SIGN_B,
+  SC_VEN,          // e-n potential
+  SC_VEE,          // e-e potential
+  SC_PE,           // total potential (incl. V_nn)
+  SC_EL,           // local energy
+  SC_LAP,          // lap(psi)/psi
+  SC_WEIGHT,       // DMC weight
+  SC_AGE,          // steps since the last accepted move
+  SC_STATUS,       // QMCB_ST_* bits
+  SC_MODRATIO,     // |modified grad| / |grad|
+  SC_AGE_MOVED,    // age when the walker last moved
+  SC_COUNT
+};
+constexpr int kScalars = 24;  // padded
+
+struct DevSys {
+  int M, na, nb, N, K, npade;
+  int ee[3];
+  double Pnn;
+  const double4 *nuc;    // [M] x, y, z, Z
+  const int4 *bf;        // [K] atom, a | b<<8 | c<<16, nprim, prim offset
+  const double2 *prim;   // [P] exponent, coefficient
+  const double *ct[2];   // [K][n_s] MO coefficients, transposed
+  const double *pade;    // [npade][2][kPadeMax] numerator, denominator
+  const int2 *pade_len;  // [npade] numerator length, denominator length
+  const int *en[2];      // [M] e-n function per spin
+};
+
+// Offsets (in doubles) of each array in a walker block.
+struct Layout {
+  int stride;
+  int R;         // [N][3]
+  int Dv[2];     // [n][n]  electron-major Slater values
+  int DgT[2];    // [3][n][n] orbital-major gradients
+  int DlT[2];    // [n][n]    orbital-major laplacians
+  int Inv[2];    // [n][n]    Inv[o][e]
+  int gradD;     // [N][3] grad(D)/D per electron (rDc_x of its spin)
+  int Ux;        // [N][3] grad ln J
+  int grad;      // [N][3] gradPsiRatio
+  int mgrad;     // [N][3] modifiedGradPsiRatio
+  int sc;        // [kScalars]
+};
+
+struct RunCfg {
+  int run_type, sampling, qf_mod, emod, reweighting, old_walker_acceptance;
+  double qf_a, dt, dt_eff;
+  double branching_threshold, fusion_threshold;
+  uint64_t seed;
+};
+
+// ------------------------------------------------------------------ warp
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(QMCB_FULL_MASK, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(QMCB_FULL_MASK, v, o));
+  return v;
+}
+
+// ------------------------------------------------------------------ RNG
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11), written from the
+// published round function: two 32x32->64 multiplies per round with the
+// Weyl key schedule.
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox_round(U4 c, uint32_t k0, uint32_t k1)
+{
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+  uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+  U4 r;
+  r.x = hi1 ^ c.y ^ k0;
+  r.y = lo1;
+  r.z = hi0 ^ c.w ^ k1;
+  r.w = lo0;
+  return r;
+}
+
+__device__ __forceinline__ U4 philox4x32(U4 c, uint64_t key)
+{
+  uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+#pragma unroll
+  for (int i = 0; i < 10; i++) {
+    c = philox_round(c, k0, k1);
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// uniform double in (0, 1] from 53 random bits
+__device__ __forceinline__ double u01(uint32_t a, uint32_t b)
+{
+  uint64_t v = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
+  return ((double)v + 1.0) * (1.0 / 9007199254740992.0);
+}
+
+// Four uniforms for (walker identity, step, purpose).
+__device__ __forceinline__ void rng_uniform4(uint64_t seed, uint32_t walker, uint32_t step, uint32_t purpose,
+                                             double u[4])
+{
+  U4 c{walker, step, purpose, 0x51ED2701u};
+  U4 r1 = philox4x32(c, seed);
+  c.w = 0x51ED2702u;
+  U4 r2 = philox4x32(c, seed);
+  u[0] = u01(r1.x, r1.y);
+  u[1] = u01(r1.z, r1.w);
+  u[2] = u01(r2.x, r2.y);
+  u[3] = u01(r2.z, r2.w);
+}
+
+// ------------------------------------------------------------------ Pade
+// u = P(r)/Q(r) with u', u'' in the operation order of
+// FixedCuspPadeCorrelationFunction::evaluate (QMcBeaver/src/FixedCuspPadeCorrelationFunction.cpp:89-111)
+// and Polynomial::evaluateAll (QMcBeaver/src/Polynomial.cpp:127-148).
+__device__ __forceinline__ void poly_all(const double *c, int len, double x, double &f, double &df, double &d2f)
+{
+  int n = len - 1;
+  f = c[n];
+  df = 0.0;
+  d2f = 0.0;
+  for (int i = n - 1; i >= 0; i--) {
+    d2f = d2f * x + df;
+    df = df * x + f;
+    f = f * x + c[i];
+  }
+  d2f *= 2.0;
+}
+
+__device__ __forceinline__ void pade_eval(const DevSys &S, int f, double r, double &u, double &du, double &d2u)
+{
+  const double *P = S.pade + (size_t)f * 2 * kPadeMax;
+  int2 L = S.pade_len[f];
+  double a, ap, app, b, bp, bpp;
+  poly_all(P, L.x, r, a, ap, app);
+  poly_all(P + kPadeMax, L.y, r, b, bp, bpp);
+  double aDIVb = a / b, bpDIVb = bp / b, apDIVb = ap / b;
+  u = aDIVb;
+  du = apDIVb - bpDIVb * aDIVb;
+  d2u = (app - bpp * aDIVb) / b - 2.0 * bpDIVb * du;
+}
+
+// e-e correlation function index for electrons i, j
+__device__ __forceinline__ int ee_func(const DevSys &S, int i, int j)
+{
+  bool ai = i < S.na, aj = j < S.na;
+  if (ai != aj) return S.ee[0];
+  return ai ? S.ee[1] : S.ee[2];
+}
+
+// ------------------------------------------------------------------ basis
+// Contracted Cartesian Gaussian k with value, gradient and Laplacian, the
+// formulas of QMCBasisFunction::evaluateBasisFunctions
+// (QMcBeaver/src/QMCBasisFunction.cpp:287-403):
+//   f = sum_i c_i x^a y^b z^c exp(-alpha_i r^2)
+//   df/dx = f_i (a/x - 2 alpha_i x) ...
+//   lap f = f_i (a(a-1)/x^2 + b(b-1)/y^2 + c(c-1)/z^2 - alpha_i (4L+6) + 4 alpha_i^2 r^2)
+__device__ __forceinline__ double ipow(double x, int a)
+{
+  double r = 1.0;
+  for (int i = 0; i < a; i++) r *= x;
+  return r;
+}
+
+__device__ __forceinline__ void basis_one(const DevSys &S, int k, const double r[3], double out[5])
+{
+  int4 info = __ldg(&S.bf[k]);
+  int a = info.y & 0xff, b = (info.y >> 8) & 0xff, c = (info.y >> 16) & 0xff;
+  double4 A = S.nuc[info.x];
+  double x = r[0] - A.x, y = r[1] - A.y, z = r[2] - A.z;
+  double x2 = x * x, y2 = y * y, z2 = z * z;
+  double r_sq = x2 + y2 + z2;
+  double poly = ipow(x, a) * ipow(y, b) * ipow(z, c);
+  double ax = a ? a / x : 0.0, by = b ? b / y : 0.0, cz = c ? c / z : 0.0;
+  double axx = a > 1 ? a * (a - 1.0) / x2 : 0.0;
+  double byy = b > 1 ? b * (b - 1.0) / y2 : 0.0;
+  double czz = c > 1 ? c * (c - 1.0) / z2 : 0.0;
+  double L46 = 4.0 * (a + b + c) + 6.0;
+  double v = 0, gx = 0, gy = 0, gz = 0, l = 0;
+  for (int i = 0; i < info.z; i++) {
+    double2 p = __ldg(&S.prim[info.w + i]);
+    double al = p.x;
+    double e = exp(-al * r_sq) * p.y * poly;
+    double t3 = -2.0 * al;
+    v += e;
+    gx += e * (ax + t3 * x);
+    gy += e * (by + t3 * y);
+    gz += e * (cz + t3 * z);
+    l += e * (axx + byy + czz - al * L46 + 4.0 * r_sq * al * al);
+  }
+  out[0] = v;
+  out[1] = gx;
+  out[2] = gy;
+  out[3] = gz;
+  out[4] = l;
+}
+
+// All K functions at position r; chi[q*ldc + k], q = val, gx, gy, gz, lap.
+__device__ __forceinline__ void basis_warp(const DevSys &S, const double r[3], double *chi, int ldc)
+{
+  for (int k = lane_id(); k < S.K; k += 32) {
+    double o[5];
+    basis_one(S, k, r, o);
+#pragma unroll
+    for (int q = 0; q < 5; q++) chi[q * ldc + k] = o[q];
+  }
+}
+
+// D[q][o] = sum_k chi[q][k] * Ct[k][o] for q < 5, o < n  (the orbital
+// contraction of QMCSlater::evaluate, QMcBeaver/src/QMCSlater.cpp:856-862).
+__device__ __forceinline__ void contract_warp(const double *chi, int ldc, const double *Ct, int n, int K,
+                                              double *D)
+{
+  for (int t = lane_id(); t < 5 * n; t += 32) {
+    int q = t / n, o = t - q * n;
+    const double *cq = chi + q * ldc;
+    double acc = 0.0;
+    for (int k = 0; k < K; k++) acc = fma(cq[k], Ct[k * n + o], acc);
+    D[t] = acc;
+  }
+}
+
+}  // namespace qmcb

@@ -1,0 +1,1014 @@
+// kernels.cuh -- the walker-path kernels (sm_100a, FP64 parity arithmetic).
+//
+// One warp owns one walker for the duration of a kernel; several warps (one
+// walker each) share a CTA.  Per-warp scratch lives in dynamic shared
+// memory; per-walker state lives in HBM as one contiguous block per slot.
+//
+//   k_full      full evaluation (whichE = -1) or LU refresh of stored Slater
+//               values; QMCSCFJastrow::evaluate with all electrons
+//   k_move      one single-electron move of every walker: proposal (or the
+//               caller's position), basis + orbital rows, Sherman-Morrison
+//               inverse update, ratio sums, incremental Jastrow and
+//               potential, psi quantities, Metropolis test, DMC reweight and
+//               observables, commit on accept
+//   k_branch    nonunit-weight branching of the live list (single CTA)
+//   k_copy      state copies for split walkers
+//   k_energy    E_est / E_T update after a branching step
+#pragma once
+
+#include "device_common.cuh"
+
+namespace qmcb {
+
+// Output pointers of the evaluate entry points (device memory, may be null).
+struct EvalOut {
+  double *log_abs_psi, *sign, *grad, *mgrad, *lap, *e_local, *pe;
+  unsigned char *status;
+};
+
+// Device accumulators of one qmcb_run_steps call.
+enum StatIdx {
+  ST_SUM_W = 0,
+  ST_SUM_WE,
+  ST_SUM_WE2,
+  ST_SUM_ACC,
+  ST_MOVES,
+  ST_FINAL_W,
+  ST_SINGULAR,
+  ST_RUN_SUM_W,   // running sums for E_est (kept across calls)
+  ST_RUN_SUM_WE,
+  ST_COUNT
+};
+
+// E_T, E_est, population target (device copies so device-side updates are
+// seen by the following launches without a host round trip).
+struct EnergyCtl {
+  double e_trial, e_est, target_weight, pop_control;
+};
+
+// Shared-memory doubles needed by one warp.
+__host__ __device__ inline int move_scratch_doubles(int N, int K, int nmax)
+{
+  return 5 * (K + 1) + 5 * nmax + nmax * nmax + nmax + 5 * 3 * N + 8;
+}
+__host__ __device__ inline int full_scratch_doubles(int N, int K, int nmax)
+{
+  return 5 * (K + 1) + 5 * nmax + 2 * nmax * nmax + 2 * nmax + 3 * N + 8;
+}
+
+// ------------------------------------------------------------------------
+// Modified quantum force, QMCSCFJastrow::calculate_Modified_Grad_PsiRatio
+// (QMcBeaver/src/QMCSCFJastrow.cpp:329-472).  gr, mg, R: [N][3] (shared).
+// Returns |mg| / |gr|; sets *bad when the reference flags the walker singular.
+__device__ inline double qf_modify_warp(const DevSys &S, const RunCfg &cfg, const double *R, const double *gr,
+                                        double *mg, bool *bad)
+{
+  const int lane = lane_id(), N = S.N;
+  if (cfg.qf_mod == 1) {
+    double part = 0.0;
+    for (int t = lane; t < 3 * N; t += 32) part += gr[t] * gr[t];
+    double magsq = warp_sum(part);
+    double a = cfg.qf_a;
+    double factor = (-1.0 + sqrt(1.0 + 2 * a * magsq * cfg.dt)) / (a * magsq * cfg.dt);
+    for (int t = lane; t < 3 * N; t += 32) mg[t] = gr[t] * factor;
+  } else if (cfg.qf_mod == 2) {
+    for (int i = lane; i < N; i += 32) {
+      int cn = 0;
+      double cd = 1e100;
+      for (int A = 0; A < S.M; A++) {
+        double4 P = S.nuc[A];
+        double dx = R[3 * i] - P.x, dy = R[3 * i + 1] - P.y, dz = R[3 * i + 2] - P.z;
+        double r = sqrt(dx * dx + dy * dy + dz * dz);
+        if (r < cd) {
+          cd = r;
+          cn = A;
+        }
+      }
+      double4 P = S.nuc[cn];
+      double nv[3] = {R[3 * i] - P.x, R[3 * i + 1] - P.y, R[3 * i + 2] - P.z};
+      double d2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
+      double il = 1.0 / sqrt(d2);
+      double ev[3] = {gr[3 * i], gr[3 * i + 1], gr[3 * i + 2]};
+      double ev2 = ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2];
+      double sc = fabs(ev2) < 1e-10 ? 0.0 : 1.0 / sqrt(ev2);
+      double dotp = 0.0;
+      for (int x = 0; x < 3; x++) dotp += (nv[x] * il) * (ev[x] * sc);
+      double temp = P.w * P.w * d2;
+      double a = 0.5 * (1.0 + dotp) + temp / (10.0 * (4.0 + temp));
+      double factor = fabs(ev2) < 1e-10 ? 1.0 : (-1.0 + sqrt(1.0 + 2.0 * a * ev2 * cfg.dt)) / (a * ev2 * cfg.dt);
+      for (int x = 0; x < 3; x++) mg[3 * i + x] = gr[3 * i + x] * factor;
+    }
+  } else {
+    for (int t = lane; t < 3 * N; t += 32) mg[t] = gr[t];
+  }
+  __syncwarp();
+  double pm = 0.0, pu = 0.0;
+  for (int t = lane; t < 3 * N; t += 32) {
+    pm += mg[t] * mg[t];
+    pu += gr[t] * gr[t];
+  }
+  double lm = sqrt(warp_sum(pm)), lu = sqrt(warp_sum(pu));
+  double ratio = lm / lu;
+  if (isnan(lm) || isnan(lu) || isnan(ratio) || lu == 0.0) *bad = true;
+  return ratio;
+}
+
+// ------------------------------------------------------------------------
+// Warp LU with the reference's implicitly scaled partial pivoting
+// (Array2D::ludcmp, QMcBeaver/include/Array2D.h:1204-1340) and the inverse
+// by forward / back substitution of the identity (lubksb :1352-1421).
+// A: [n][n] row-major (destroyed), X: [n][n] receives A^-1 in X[o][e],
+// vv / piv scratch of n doubles.  Returns false when singular.
+__device__ inline bool lu_inverse_warp(double *A, double *X, double *vv, double *piv, int n, double &logdet,
+                                       double &sign)
+{
+  const int lane = lane_id();
+  bool sing = false;
+  for (int i = lane; i < n; i += 32) {
+    double big = 0.0;
+    for (int j = 0; j < n; j++) big = fmax(big, fabs(A[i * n + j]));
+    if (big == 0.0) sing = true;
+    vv[i] = big == 0.0 ? 0.0 : 1.0 / big;
+  }
+  sing = __any_sync(QMCB_FULL_MASK, sing);
+  __syncwarp();
+  if (sing) {
+    logdet = -INFINITY;
+    sign = 0.0;
+    return false;
+  }
+  double sg = 1.0, ld = 0.0;
+  for (int j = 0; j < n; j++) {
+    double best = -1.0;
+    int bi = -1;
+    for (int i = j + lane; i < n; i += 32) {
+      double v = vv[i] * fabs(A[i * n + j]);
+      if (v >= best) {
+        best = v;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(QMCB_FULL_MASK, best, o);
+      int oi = __shfl_xor_sync(QMCB_FULL_MASK, bi, o);
+      if (ob > best || (ob == best && oi > bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (bi != j) {
+      for (int k = lane; k < n; k += 32) {
+        double t = A[bi * n + k];
+        A[bi * n + k] = A[j * n + k];
+        A[j * n + k] = t;
+      }
+      __syncwarp();
+      if (lane == 0) vv[bi] = vv[j];
+      sg = -sg;
+    }
+    if (lane == 0) piv[j] = (double)bi;
+    __syncwarp();
+    double p = A[j * n + j];
+    if (p == 0.0) {
+      sing = true;
+      break;
+    }
+    double dum = 1.0 / p;
+    ld += log(fabs(p));
+    if (p < 0) sg = -sg;
+    for (int i = j + 1 + lane; i < n; i += 32) A[i * n + j] *= dum;
+    __syncwarp();
+    int m = n - j - 1;
+    for (int t = lane; t < m * m; t += 32) {
+      int i = j + 1 + t / m, c = j + 1 + t % m;
+      A[i * n + c] -= A[i * n + j] * A[j * n + c];
+    }
+    __syncwarp();
+  }
+  if (sing) {
+    logdet = -INFINITY;
+    sign = 0.0;
+    return false;
+  }
+  logdet = ld;
+  sign = sg;
+  // inverse: column jc of X solves A x = e_jc
+  for (int jc = lane; jc < n; jc += 32) {
+    for (int i = 0; i < n; i++) X[i * n + jc] = (i == jc) ? 1.0 : 0.0;
+    for (int i = 0; i < n; i++) {
+      int ip = (int)piv[i];
+      double s = X[ip * n + jc];
+      X[ip * n + jc] = X[i * n + jc];
+      for (int k = 0; k < i; k++) s -= A[i * n + k] * X[k * n + jc];
+      X[i * n + jc] = s;
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double s = X[i * n + jc];
+      for (int k = i + 1; k < n; k++) s -= A[i * n + k] * X[k * n + jc];
+      X[i * n + jc] = s / A[i * n + i];
+    }
+  }
+  __syncwarp();
+  return true;
+}
+
+// ------------------------------------------------------------------------
+// Jastrow and potential from scratch for all electrons (updateAll order of
+// pairs is irrelevant here: totals are summed fresh, not incrementally).
+// Writes Ux[N][3] to `ux`, returns U, U_xx, V_ee, V_en through refs.
+__device__ inline void jastrow_pe_full_warp(const DevSys &S, const double *R, double *ux, double &U, double &Uxx,
+                                            double &Vee, double &Ven)
+{
+  const int lane = lane_id(), N = S.N;
+  double pu = 0, pxx = 0, pee = 0, pen = 0;
+  for (int i = lane; i < N; i += 32) {
+    double xi = R[3 * i], yi = R[3 * i + 1], zi = R[3 * i + 2];
+    double gx = 0, gy = 0, gz = 0;
+    for (int j = 0; j < N; j++) {
+      if (j == i) continue;
+      double dx = xi - R[3 * j], dy = yi - R[3 * j + 1], dz = zi - R[3 * j + 2];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      if (j < i) pee += 1.0 / r;
+      int f = ee_func(S, i, j);
+      if (f < 0) continue;
+      double u, du, d2u;
+      pade_eval(S, f, r, u, du, d2u);
+      gx += du * (dx / r);
+      gy += du * (dy / r);
+      gz += du * (dz / r);
+      if (j < i) {
+        pu += u;
+        pxx += 2.0 * (2.0 / r * du + d2u);
+      }
+    }
+    int sp = i < S.na ? 0 : 1;
+    for (int A = 0; A < S.M; A++) {
+      double4 P = S.nuc[A];
+      double dx = xi - P.x, dy = yi - P.y, dz = zi - P.z;
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      pen -= P.w / r;
+      int f = S.en[sp][A];
+      if (f < 0) continue;
+      double u, du, d2u;
+      pade_eval(S, f, r, u, du, d2u);
+      gx += du * (dx / r);
+      gy += du * (dy / r);
+      gz += du * (dz / r);
+      pu += u;
+      pxx += 2.0 / r * du + d2u;
+    }
+    ux[3 * i] = gx;
+    ux[3 * i + 1] = gy;
+    ux[3 * i + 2] = gz;
+  }
+  U = warp_sum(pu);
+  Uxx = warp_sum(pxx);
+  Vee = warp_sum(pee);
+  Ven = warp_sum(pen);
+}
+
+// Psi quantities (QMCSCFJastrow::calculate_Psi_quantities / update_SCF,
+// QMcBeaver/src/QMCSCFJastrow.cpp:196-327): gr = gD + Ux and
+// lap = Dxx + U_xx + sum(2 Ux.gD + Ux.Ux).
+__device__ inline double psi_lap_warp(int N, const double *gD, const double *Ux, double *gr, double Dxx, double Uxx)
+{
+  const int lane = lane_id();
+  double part = 0.0;
+  for (int i = lane; i < N; i += 32) {
+    for (int d = 0; d < 3; d++) {
+      double dx = gD[3 * i + d], u = Ux[3 * i + d];
+      gr[3 * i + d] = dx + u;
+      part += u * dx * 2.0;
+      part += u * u;
+    }
+  }
+  return Dxx + Uxx + warp_sum(part);
+}
+
+// ------------------------------------------------------------------------
+// Full evaluation (do_basis = true: QMCSCFJastrow::evaluate with whichE = -1)
+// or refresh from the stored Slater values (do_basis = false).
+// R_in: [num][N][3] positions to store first (null: use the stored ones).
+__global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+                                              int num, const int *d_num, const double *R_in, int do_basis,
+                                              EvalOut out)
+{
+  extern __shared__ double smem[];
+  const int lane = lane_id(), warp = threadIdx.x >> 5;
+  const int nw = d_num ? *d_num : num;
+  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (wi >= nw) return;
+  const int N = S.N, K = S.K, nmax = max(S.na, S.nb);
+  const int slot = slots ? slots[wi] : wi;
+  double *blk = state + (size_t)slot * L.stride;
+  double *sm = smem + (size_t)warp * full_scratch_doubles(N, K, nmax);
+  const int ldc = K + 1;
+  double *chi = sm;
+  double *Dn = chi + 5 * ldc;
+  double *A = Dn + 5 * nmax;
+  double *X = A + nmax * nmax;
+  double *vv = X + nmax * nmax;
+  double *piv = vv + nmax;
+  double *Rs = piv + nmax;
+  double *R = blk + L.R;
+  double *sc = blk + L.sc;
+
+  if (R_in) {
+    for (int t = lane; t < 3 * N; t += 32) R[t] = R_in[(size_t)wi * 3 * N + t];
+  }
+  for (int t = lane; t < 3 * N; t += 32) Rs[t] = R[t];
+  __syncwarp();
+
+  bool bad = false;
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? S.nb : S.na, base = sp ? S.na : 0;
+    if (n == 0) {
+      sc[SC_LAPR_A + sp] = 0.0;
+      sc[SC_LOGDET_A + sp] = 0.0;
+      sc[SC_SIGN_A + sp] = 1.0;
+      continue;
+    }
+    double *Dv = blk + L.Dv[sp], *DgT = blk + L.DgT[sp], *DlT = blk + L.DlT[sp];
+    if (do_basis) {
+      for (int e = 0; e < n; e++) {
+        double r[3] = {Rs[3 * (base + e)], Rs[3 * (base + e) + 1], Rs[3 * (base + e) + 2]};
+        basis_warp(S, r, chi, ldc);
+        __syncwarp();
+        contract_warp(chi, ldc, S.ct[sp], n, K, Dn);
+        __syncwarp();
+        for (int o = lane; o < n; o += 32) {
+          Dv[e * n + o] = Dn[o];
+          DgT[(0 * n + o) * n + e] = Dn[n + o];
+          DgT[(1 * n + o) * n + e] = Dn[2 * n + o];
+          DgT[(2 * n + o) * n + e] = Dn[3 * n + o];
+          DlT[o * n + e] = Dn[4 * n + o];
+        }
+        __syncwarp();
+      }
+    }
+    for (int t = lane; t < n * n; t += 32) A[t] = Dv[t];
+    __syncwarp();
+    double logdet, sign;
+    bool ok = lu_inverse_warp(A, X, vv, piv, n, logdet, sign);
+    if (!ok) bad = true;
+    double *Inv = blk + L.Inv[sp];
+    for (int t = lane; t < n * n; t += 32) Inv[t] = X[t];
+    // ratio sums (QMcBeaver/src/QMCSlater.cpp:741-762)
+    double lp = 0.0;
+    for (int e = lane; e < n; e += 32) {
+      double gx = 0, gy = 0, gz = 0;
+      for (int o = 0; o < n; o++) {
+        double iv = X[o * n + e];
+        lp += DlT[o * n + e] * iv;
+        gx += DgT[(0 * n + o) * n + e] * iv;
+        gy += DgT[(1 * n + o) * n + e] * iv;
+        gz += DgT[(2 * n + o) * n + e] * iv;
+      }
+      blk[L.gradD + 3 * (base + e)] = gx;
+      blk[L.gradD + 3 * (base + e) + 1] = gy;
+      blk[L.gradD + 3 * (base + e) + 2] = gz;
+    }
+    lp = warp_sum(lp);
+    if (lane == 0) {
+      sc[SC_LAPR_A + sp] = lp;
+      sc[SC_LOGDET_A + sp] = logdet;
+      sc[SC_SIGN_A + sp] = sign;
+    }
+    __syncwarp();
+  }
+
+  double U, Uxx, Vee, Ven;
+  double *ux = blk + L.Ux;
+  jastrow_pe_full_warp(S, Rs, ux, U, Uxx, Vee, Ven);
+  __syncwarp();
+  double *gD = blk + L.gradD, *gr = blk + L.grad, *mg = blk + L.mgrad;
+  double Dxx = 0.0;
+  if (S.na > 0) Dxx += sc[SC_LAPR_A];
+  if (S.nb > 0) Dxx += sc[SC_LAPR_B];
+  double lap = psi_lap_warp(N, gD, ux, gr, Dxx, Uxx);
+  __syncwarp();
+  double modratio = qf_modify_warp(S, cfg, Rs, gr, mg, &bad);
+  double PE = S.Pnn + Vee + Ven;
+  double EL = -0.5 * lap + PE;
+  unsigned st = bad ? 1u : 0u;
+  if (isnan(EL) || isnan(lap)) st |= 2u;
+  if (lane == 0) {
+    sc[SC_U] = U;
+    sc[SC_UXX] = Uxx;
+    sc[SC_VEE] = Vee;
+    sc[SC_VEN] = Ven;
+    sc[SC_PE] = PE;
+    sc[SC_EL] = EL;
+    sc[SC_LAP] = lap;
+    sc[SC_MODRATIO] = modratio;
+    sc[SC_STATUS] = (double)st;
+    if (R_in) {
+      sc[SC_WEIGHT] = 1.0;
+      sc[SC_AGE] = 0.0;
+      sc[SC_AGE_MOVED] = 0.0;
+    }
+    if (out.log_abs_psi) out.log_abs_psi[wi] = sc[SC_LOGDET_A] + sc[SC_LOGDET_B] + U;
+    if (out.sign) out.sign[wi] = sc[SC_SIGN_A] * sc[SC_SIGN_B];
+    if (out.lap) out.lap[wi] = lap;
+    if (out.e_local) out.e_local[wi] = EL;
+    if (out.pe) {
+      out.pe[3 * wi] = PE;
+      out.pe[3 * wi + 1] = Ven;
+      out.pe[3 * wi + 2] = Vee;
+    }
+    if (out.status) out.status[wi] = (unsigned char)st;
+  }
+  __syncwarp();
+  if (out.grad)
+    for (int t = lane; t < 3 * N; t += 32) out.grad[(size_t)wi * 3 * N + t] = gr[t];
+  if (out.mgrad)
+    for (int t = lane; t < 3 * N; t += 32) out.mgrad[(size_t)wi * 3 * N + t] = mg[t];
+}
+
+// ------------------------------------------------------------------------
+// One single-electron move of electron e for every walker in the list.
+// kMetropolis = false: the caller's positions R_in[wi] are taken and the
+// new state is committed unconditionally (QMCFunctions::evaluate with
+// whichE = e).  kMetropolis = true: proposal from the walker's own random
+// stream, acceptance test, DMC reweight when do_reweight, commit on accept
+// (QMCWalker::initializePropagation / processPropagation,
+// QMcBeaver/src/QMCWalker.cpp:179-282).
+struct MoveArgs {
+  int e;             // moved electron
+  int step;          // global step number (random stream position)
+  int do_reweight;   // this step reweights / collects observables (whichE == 0)
+  int reweight_on;   // step >= reweight_start_step
+};
+
+template <bool kMetropolis>
+__global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+                                              int num, const int *d_num, const double *R_in, MoveArgs mv,
+                                              const EnergyCtl *ectl, double *stats, EvalOut out)
+{
+  extern __shared__ double smem[];
+  const int lane = lane_id(), warp = threadIdx.x >> 5;
+  const int nw = d_num ? *d_num : num;
+  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (wi >= nw) return;
+  const int N = S.N, K = S.K, nmax = max(S.na, S.nb);
+  const int e = mv.e;
+  const int sp = e < S.na ? 0 : 1;
+  const int n = sp ? S.nb : S.na, base = sp ? S.na : 0, el = e - base;
+  const int slot = slots ? slots[wi] : wi;
+  double *blk = state + (size_t)slot * L.stride;
+  double *sm = smem + (size_t)warp * move_scratch_doubles(N, K, nmax);
+  const int ldc = K + 1;
+  double *chi = sm;
+  double *Dn = chi + 5 * ldc;
+  double *Inv = Dn + 5 * nmax;
+  double *valc = Inv + nmax * nmax;
+  double *Ux = valc + nmax;
+  double *gD = Ux + 3 * N;
+  double *gr = gD + 3 * N;
+  double *mg = gr + 3 * N;
+  double *Rn = mg + 3 * N;
+  double *sc = blk + L.sc;
+  const double *Rold = blk + L.R;
+
+  for (int t = lane; t < 3 * N; t += 32) Rn[t] = Rold[t];
+  __syncwarp();
+  const double ro[3] = {Rn[3 * e], Rn[3 * e + 1], Rn[3 * e + 2]};
+  double rn[3];
+  double g_fwd = 0.0, u_acc = 0.5;
+  if (kMetropolis) {
+    double u[4];
+    rng_uniform4(cfg.seed, (uint32_t)slot, (uint32_t)mv.step, 0u, u);
+    double u2[4];
+    rng_uniform4(cfg.seed, (uint32_t)slot, (uint32_t)mv.step, 1u, u2);
+    const double two_pi = 6.283185307179586;
+    double rad0 = sqrt(-2.0 * log(u[0])), rad1 = sqrt(-2.0 * log(u[2]));
+    double z[3] = {rad0 * cos(two_pi * u[1]), rad0 * sin(two_pi * u[1]), rad1 * cos(two_pi * u[3])};
+    u_acc = u2[0];
+    double sigma = sqrt(cfg.dt);
+    const double *mgo = blk + L.mgrad;
+    for (int d = 0; d < 3; d++) {
+      double drift = sigma * z[d];
+      double disp = drift;
+      if (cfg.sampling == 1) disp += cfg.dt * mgo[3 * e + d];
+      rn[d] = ro[d] + disp;
+      g_fwd += drift * drift;
+    }
+    if (cfg.sampling == 1) {
+      double part = 0.0;
+      for (int t = lane; t < 3 * N; t += 32) {
+        if (t / 3 == e) continue;
+        double dd = cfg.dt * mgo[t];
+        part += dd * dd;
+      }
+      g_fwd += warp_sum(part);
+    }
+  } else {
+    for (int d = 0; d < 3; d++) rn[d] = R_in[(size_t)wi * 3 * N + 3 * e + d];
+  }
+  __syncwarp();
+  if (lane == 0)
+    for (int d = 0; d < 3; d++) Rn[3 * e + d] = rn[d];
+
+  // ---- incremental Jastrow + potential (QMCJastrowElectronElectron::updateOne,
+  //      QMCJastrowElectronNuclear::evaluate, QMCPotential_Energy::evaluate)
+  double dU = 0, dUxx = 0, ge[3] = {0, 0, 0}, dVee = 0, dVen = 0;
+  const double *Uxo = blk + L.Ux;
+  for (int j = lane; j < N; j += 32) {
+    double uj[3] = {Uxo[3 * j], Uxo[3 * j + 1], Uxo[3 * j + 2]};
+    if (j != e) {
+      double Rj[3] = {Rold[3 * j], Rold[3 * j + 1], Rold[3 * j + 2]};
+      double dxo = ro[0] - Rj[0], dyo = ro[1] - Rj[1], dzo = ro[2] - Rj[2];
+      double dxn = rn[0] - Rj[0], dyn = rn[1] - Rj[1], dzn = rn[2] - Rj[2];
+      double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
+      double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
+      dVee += 1.0 / r_n - 1.0 / r_o;
+      int f = ee_func(S, e, j);
+      if (f >= 0) {
+        double uo, duo, d2uo, un, dun, d2un;
+        pade_eval(S, f, r_o, uo, duo, d2uo);
+        pade_eval(S, f, r_n, un, dun, d2un);
+        dU += un - uo;
+        dUxx += 2.0 * (2.0 / r_n * dun + d2un) - 2.0 * (2.0 / r_o * duo + d2uo);
+        double vx = dun * (dxn / r_n) - duo * (dxo / r_o);
+        double vy = dun * (dyn / r_n) - duo * (dyo / r_o);
+        double vz = dun * (dzn / r_n) - duo * (dzo / r_o);
+        ge[0] += vx;
+        ge[1] += vy;
+        ge[2] += vz;
+        uj[0] -= vx;
+        uj[1] -= vy;
+        uj[2] -= vz;
+      }
+    }
+    Ux[3 * j] = uj[0];
+    Ux[3 * j + 1] = uj[1];
+    Ux[3 * j + 2] = uj[2];
+  }
+  for (int A = lane; A < S.M; A += 32) {
+    double4 P = S.nuc[A];
+    double dxo = ro[0] - P.x, dyo = ro[1] - P.y, dzo = ro[2] - P.z;
+    double dxn = rn[0] - P.x, dyn = rn[1] - P.y, dzn = rn[2] - P.z;
+    double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
+    double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
+    dVen -= P.w * (1.0 / r_n - 1.0 / r_o);
+    int f = S.en[sp][A];
+    if (f >= 0) {
+      double uo, duo, d2uo, un, dun, d2un;
+      pade_eval(S, f, r_o, uo, duo, d2uo);
+      pade_eval(S, f, r_n, un, dun, d2un);
+      dU += un - uo;
+      dUxx += (2.0 / r_n * dun + d2un) - (2.0 / r_o * duo + d2uo);
+      ge[0] += dun * (dxn / r_n) - duo * (dxo / r_o);
+      ge[1] += dun * (dyn / r_n) - duo * (dyo / r_o);
+      ge[2] += dun * (dzn / r_n) - duo * (dzo / r_o);
+    }
+  }
+  dU = warp_sum(dU);
+  dUxx = warp_sum(dUxx);
+  dVee = warp_sum(dVee);
+  dVen = warp_sum(dVen);
+  for (int d = 0; d < 3; d++) ge[d] = warp_sum(ge[d]);
+  __syncwarp();
+  if (lane == 0)
+    for (int d = 0; d < 3; d++) Ux[3 * e + d] = Uxo[3 * e + d] + ge[d];
+
+  // ---- basis at the new position and the new Slater / derivative rows
+  basis_warp(S, rn, chi, ldc);
+  __syncwarp();
+  contract_warp(chi, ldc, S.ct[sp], n, K, Dn);
+  const double *InvG = blk + L.Inv[sp];
+  for (int t = lane; t < n * n; t += 32) Inv[t] = InvG[t];
+  __syncwarp();
+
+  // ---- Sherman-Morrison row replacement (Array2D::inverseUpdateOneRow,
+  //      QMcBeaver/include/Array2D.h:1567-1610)
+  double part = 0.0;
+  for (int o = lane; o < n; o += 32) part += Dn[o] * Inv[o * n + el];
+  const double ratio = warp_sum(part);
+  bool bad = !(ratio != 0.0) || !isfinite(ratio);
+  const double q = 1.0 / ratio;
+  for (int c = lane; c < n; c += 32) {
+    if (c == el) continue;
+    double val = 0.0;
+    for (int l = 0; l < n; l++) val += Dn[l] * Inv[l * n + c];
+    valc[c] = val * q;
+  }
+  __syncwarp();
+  for (int t = lane; t < n * n; t += 32) {
+    int r = t / n, c = t - r * n;
+    if (c != el) Inv[t] -= valc[c] * Inv[r * n + el];
+  }
+  __syncwarp();
+  for (int r = lane; r < n; r += 32) Inv[r * n + el] *= q;
+  __syncwarp();
+
+  // ---- ratio sums of the moved spin (QMcBeaver/src/QMCSlater.cpp:741-762)
+  const double *DgT = blk + L.DgT[sp], *DlT = blk + L.DlT[sp];
+  double lp = 0.0;
+  for (int e2 = lane; e2 < n; e2 += 32) {
+    double gx = 0, gy = 0, gz = 0;
+    if (e2 == el) {
+      for (int o = 0; o < n; o++) {
+        double iv = Inv[o * n + el];
+        gx += Dn[n + o] * iv;
+        gy += Dn[2 * n + o] * iv;
+        gz += Dn[3 * n + o] * iv;
+        lp += Dn[4 * n + o] * iv;
+      }
+    } else {
+      for (int o = 0; o < n; o++) {
+        double iv = Inv[o * n + e2];
+        gx += DgT[(0 * n + o) * n + e2] * iv;
+        gy += DgT[(1 * n + o) * n + e2] * iv;
+        gz += DgT[(2 * n + o) * n + e2] * iv;
+        lp += DlT[o * n + e2] * iv;
+      }
+    }
+    gD[3 * (base + e2)] = gx;
+    gD[3 * (base + e2) + 1] = gy;
+    gD[3 * (base + e2) + 2] = gz;
+  }
+  const double lapR = warp_sum(lp);
+  {
+    const int obase = sp ? 0 : S.na, on = sp ? S.na : S.nb;
+    for (int t = lane; t < 3 * on; t += 32) gD[3 * obase + t] = blk[L.gradD + 3 * obase + t];
+  }
+  __syncwarp();
+
+  // ---- psi quantities, quantum force, local energy
+  const double U_new = sc[SC_U] + dU, Uxx_new = sc[SC_UXX] + dUxx;
+  double lapA = sp == 0 ? lapR : sc[SC_LAPR_A];
+  double lapB = sp == 1 ? lapR : sc[SC_LAPR_B];
+  double Dxx = 0.0;
+  if (S.na > 0) Dxx += lapA;
+  if (S.nb > 0) Dxx += lapB;
+  const double lap = psi_lap_warp(N, gD, Ux, gr, Dxx, Uxx_new);
+  __syncwarp();
+  const double modratio = qf_modify_warp(S, cfg, Rn, gr, mg, &bad);
+  const double Vee = sc[SC_VEE] + dVee, Ven = sc[SC_VEN] + dVen;
+  const double PE = S.Pnn + Vee + Ven;
+  const double EL = -0.5 * lap + PE;
+  if (isnan(EL)) bad = true;
+  const double logdet_new = sc[SC_LOGDET_A + sp] + log(fabs(ratio));
+  const double sign_new = sc[SC_SIGN_A + sp] * (ratio < 0 ? -1.0 : 1.0);
+
+  bool accept = true;
+  double p = 1.0;
+  if (kMetropolis) {
+    // acceptance (QMCWalker::calculateMoveAcceptanceProbability, :1578-1654)
+    double log_g = 0.0;
+    if (cfg.sampling == 1) {
+      double pr = 0.0;
+      for (int t = lane; t < 3 * N; t += 32) {
+        double tt = Rold[t] - Rn[t] - cfg.dt * mg[t];
+        pr += tt * tt;
+      }
+      double g_rev = warp_sum(pr);
+      log_g = -(g_rev - g_fwd) / (2.0 * cfg.dt);
+    }
+    double lpr = log(fabs(ratio)) + dU;
+    p = exp(2.0 * lpr + log_g);
+    const double age = sc[SC_AGE];
+    const double over = age - cfg.old_walker_acceptance;
+    if (!isnan(p)) {
+      if (over > 500)
+        p = 1.0;
+      else if (over > 0)
+        p *= pow(1.1, over);
+    } else {
+      p = 0.0;
+    }
+    if (bad) p = 0.0;
+    if (cfg.run_type == 1 && ratio < 0) p = 0.0;
+    if (p > 1.0) p = 1.0;
+    accept = p > u_acc;
+    double new_age = accept ? 0.0 : age + 1.0;
+    double w = sc[SC_WEIGHT];
+    // reweight (QMCWalker::reweight_walker, :1060-1185), observables (:2096-2123, 2306-2387)
+    if (mv.do_reweight) {
+      if (cfg.run_type == 1 && mv.reweight_on) {
+        const double ET = ectl->e_trial, Eest = ectl->e_est;
+        const double Eo = sc[SC_EL], mo = sc[SC_MODRATIO];
+        const double Et = bad ? Eo : EL;
+        double St, So;
+        if (cfg.emod == 0) {
+          St = ET - Et;
+          So = ET - Eo;
+        } else if (cfg.emod == 2) {
+          St = (ET - Et) * (bad ? mo : modratio);
+          So = (ET - Eo) * mo;
+        } else {
+          St = (ET - Eest) + (Eest - Et) * (bad ? mo : modratio);
+          So = (ET - Eest) + (Eest - Eo) * mo;
+        }
+        double rw;
+        if (cfg.reweighting == 0)
+          rw = 0.5 * (St + So);
+        else if (cfg.reweighting == 1)
+          rw = accept ? 0.5 * (St + So) : So;
+        else
+          rw = p * 0.5 * (So + St) + (1.0 - p) * So;
+        double dW = exp(rw * cfg.dt_eff);
+        if (new_age - cfg.old_walker_acceptance > 0)
+          w *= 0.9;
+        else
+          w *= dW;
+      }
+      double Eobs = p * (bad ? 0.0 : EL) + (1.0 - p) * sc[SC_EL];
+      if (lane == 0 && w > 0.0) {
+        atomicAdd(&stats[ST_SUM_W], w);
+        atomicAdd(&stats[ST_SUM_WE], w * Eobs);
+        atomicAdd(&stats[ST_SUM_WE2], w * Eobs * Eobs);
+        atomicAdd(&stats[ST_RUN_SUM_W], w);
+        atomicAdd(&stats[ST_RUN_SUM_WE], w * Eobs);
+      }
+    }
+    if (lane == 0) {
+      atomicAdd(&stats[ST_SUM_ACC], p);
+      atomicAdd(&stats[ST_MOVES], 1.0);
+      if (bad) atomicAdd(&stats[ST_SINGULAR], 1.0);
+      sc[SC_WEIGHT] = w;
+      sc[SC_AGE] = new_age;
+      if (accept) sc[SC_AGE_MOVED] = age;
+    }
+  }
+  __syncwarp();
+
+  if (accept) {
+    double *Rw = blk + L.R;
+    if (lane < 3) Rw[3 * e + lane] = rn[lane];
+    double *InvW = blk + L.Inv[sp];
+    for (int t = lane; t < n * n; t += 32) InvW[t] = Inv[t];
+    double *Dv = blk + L.Dv[sp], *DgW = blk + L.DgT[sp], *DlW = blk + L.DlT[sp];
+    for (int o = lane; o < n; o += 32) {
+      Dv[el * n + o] = Dn[o];
+      DgW[(0 * n + o) * n + el] = Dn[n + o];
+      DgW[(1 * n + o) * n + el] = Dn[2 * n + o];
+      DgW[(2 * n + o) * n + el] = Dn[3 * n + o];
+      DlW[o * n + el] = Dn[4 * n + o];
+    }
+    for (int t = lane; t < 3 * N; t += 32) {
+      blk[L.gradD + t] = gD[t];
+      blk[L.Ux + t] = Ux[t];
+      blk[L.grad + t] = gr[t];
+      blk[L.mgrad + t] = mg[t];
+    }
+    if (lane == 0) {
+      sc[SC_U] = U_new;
+      sc[SC_UXX] = Uxx_new;
+      sc[SC_LAPR_A + sp] = lapR;
+      sc[SC_LOGDET_A + sp] = logdet_new;
+      sc[SC_SIGN_A + sp] = sign_new;
+      sc[SC_VEE] = Vee;
+      sc[SC_VEN] = Ven;
+      sc[SC_PE] = PE;
+      sc[SC_EL] = EL;
+      sc[SC_LAP] = lap;
+      sc[SC_MODRATIO] = modratio;
+      sc[SC_STATUS] = bad ? 1.0 : 0.0;
+    }
+  }
+  if (!kMetropolis) {
+    if (lane == 0) {
+      const double la = sp == 0 ? logdet_new : sc[SC_LOGDET_A];
+      const double lb = sp == 1 ? logdet_new : sc[SC_LOGDET_B];
+      const double sa = sp == 0 ? sign_new : sc[SC_SIGN_A];
+      const double sb = sp == 1 ? sign_new : sc[SC_SIGN_B];
+      unsigned st = bad ? 1u : 0u;
+      if (isnan(EL) || isnan(lap)) st |= 2u;
+      if (out.log_abs_psi) out.log_abs_psi[wi] = la + lb + U_new;
+      if (out.sign) out.sign[wi] = sa * sb;
+      if (out.lap) out.lap[wi] = lap;
+      if (out.e_local) out.e_local[wi] = EL;
+      if (out.pe) {
+        out.pe[3 * wi] = PE;
+        out.pe[3 * wi + 1] = Ven;
+        out.pe[3 * wi + 2] = Vee;
+      }
+      if (out.status) out.status[wi] = (unsigned char)st;
+    }
+    if (out.grad)
+      for (int t = lane; t < 3 * N; t += 32) out.grad[(size_t)wi * 3 * N + t] = gr[t];
+    if (out.mgrad)
+      for (int t = lane; t < 3 * N; t += 32) out.mgrad[(size_t)wi * 3 * N + t] = mg[t];
+  }
+}
+
+// ------------------------------------------------------------------------
+// Nonunit-weight branching (QMCRun::nonunitWeightBranching,
+// QMcBeaver/src/QMCRun.cpp:740-814) on the live slot list, one CTA of
+// 1024 threads.  Walkers above the branching threshold split in two with
+// half the weight each (the copy is appended to the list), walkers below
+// 0.01 die, walkers below the fusion threshold are paired in list order and
+// one of each pair survives with the sum of the weights (probability
+// w1 / (w1 + w2) for the first).  Dead slots go on the free stack; copies
+// take slots from it and are written to the copy list for k_copy.
+// ctl: [0] n_live, [1] n_free, [2] n_copies.
+__global__ void __launch_bounds__(1024) k_branch(double *state, Layout L, int *live, int *live_tmp, int *free_stack,
+                                                 int *ctl, int2 *copies, double thr_split, double thr_fuse,
+                                                 uint64_t seed, int step, double *stats)
+{
+  __shared__ int s_warp[32];
+  __shared__ int s_base[4];
+  __shared__ double s_wsum[32];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int n = ctl[0];
+  int nfree = ctl[1];
+  // pass 1: pair fusion candidates in list order and decide
+  int cand_base = 0;
+  for (int c0 = 0; c0 < n; c0 += 1024) {
+    int i = c0 + tid;
+    int slot = i < n ? live[i] : -1;
+    double w = slot >= 0 ? state[(size_t)slot * L.stride + L.sc + SC_WEIGHT] : 0.0;
+    int is_c = (slot >= 0 && w <= thr_split && w >= 0.01 && w < thr_fuse) ? 1 : 0;
+    // block exclusive scan of is_c
+    unsigned b = __ballot_sync(QMCB_FULL_MASK, is_c);
+    int wpre = __popc(b & ((1u << lane) - 1));
+    if (lane == 31) s_warp[wid] = wpre + is_c;
+    __syncthreads();
+    if (wid == 0) {
+      int v = s_warp[lane], x = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(QMCB_FULL_MASK, x, o);
+        if (lane >= o) x += y;
+      }
+      s_warp[lane] = x - v;
+      if (lane == 31) s_base[0] = x;
+    }
+    __syncthreads();
+    int rank = cand_base + s_warp[wid] + wpre;  // global candidate rank
+    int total = s_base[0];
+    // candidate ranks are global over the whole list, so pairs (0,1), (2,3)
+    // ... may straddle chunk boundaries.
+    if (is_c) live_tmp[rank] = i;
+    __syncthreads();
+    cand_base += total;
+  }
+  __syncthreads();
+  // decide pairs: candidate 2m and 2m+1
+  for (int m = tid; 2 * m + 1 < cand_base; m += 1024) {
+    int ia = live_tmp[2 * m], ib = live_tmp[2 * m + 1];
+    int sa = live[ia], sb = live[ib];
+    double *wa = &state[(size_t)sa * L.stride + L.sc + SC_WEIGHT];
+    double *wb = &state[(size_t)sb * L.stride + L.sc + SC_WEIGHT];
+    double w1 = *wa, w2 = *wb, w3 = w1 + w2;
+    double u[4];
+    rng_uniform4(seed, (uint32_t)sa, (uint32_t)step, 7u, u);
+    if (u[0] < w1 / w3) {
+      *wa = w3;
+      *wb = -1.0;  // marked dead
+    } else {
+      *wb = w3;
+      *wa = -1.0;
+    }
+  }
+  __syncthreads();
+  // pass 2: survivors keep list order; dead slots to the free stack; splits append copies
+  int out_base = 0, split_base = 0;
+  // first count survivors + kills to know where split copies go and how many slots free
+  for (int c0 = 0; c0 < n; c0 += 1024) {
+    int i = c0 + tid;
+    int slot = i < n ? live[i] : -1;
+    double w = slot >= 0 ? state[(size_t)slot * L.stride + L.sc + SC_WEIGHT] : 0.0;
+    int dead = (slot >= 0 && w < 0.01) ? 1 : 0;
+    int keep = (slot >= 0 && !dead) ? 1 : 0;
+    unsigned bk = __ballot_sync(QMCB_FULL_MASK, keep), bd = __ballot_sync(QMCB_FULL_MASK, dead);
+    int pk = __popc(bk & ((1u << lane) - 1)), pd = __popc(bd & ((1u << lane) - 1));
+    if (lane == 31) s_warp[wid] = ((pk + keep) << 16) | (pd + dead);
+    __syncthreads();
+    if (wid == 0) {
+      int v = s_warp[lane];
+      int vk = v >> 16, vd = v & 0xffff, xk = vk, xd = vd;
+      for (int o = 1; o < 32; o <<= 1) {
+        int yk = __shfl_up_sync(QMCB_FULL_MASK, xk, o), yd = __shfl_up_sync(QMCB_FULL_MASK, xd, o);
+        if (lane >= o) {
+          xk += yk;
+          xd += yd;
+        }
+      }
+      s_warp[lane] = ((xk - vk) << 16) | (xd - vd);
+      if (lane == 31) {
+        s_base[1] = xk;
+        s_base[2] = xd;
+      }
+    }
+    __syncthreads();
+    int ok = s_warp[wid] >> 16, od = s_warp[wid] & 0xffff;
+    if (keep) live_tmp[out_base + ok + pk] = slot;
+    if (dead) free_stack[nfree + od + pd] = slot;
+    int tk = s_base[1], td = s_base[2];
+    __syncthreads();
+    out_base += tk;
+    nfree += td;
+  }
+  __syncthreads();
+  // splits among survivors (in new list order), appended at the end
+  int n_keep = out_base;
+  double wsum_part = 0.0;
+  for (int c0 = 0; c0 < n_keep; c0 += 1024) {
+    int i = c0 + tid;
+    int slot = i < n_keep ? live_tmp[i] : -1;
+    double *wp = slot >= 0 ? &state[(size_t)slot * L.stride + L.sc + SC_WEIGHT] : nullptr;
+    double w = wp ? *wp : 0.0;
+    int sp = (slot >= 0 && w > thr_split) ? 1 : 0;
+    unsigned bs = __ballot_sync(QMCB_FULL_MASK, sp);
+    int ps = __popc(bs & ((1u << lane) - 1));
+    if (lane == 31) s_warp[wid] = ps + sp;
+    __syncthreads();
+    if (wid == 0) {
+      int v = s_warp[lane], x = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(QMCB_FULL_MASK, x, o);
+        if (lane >= o) x += y;
+      }
+      s_warp[lane] = x - v;
+      if (lane == 31) s_base[3] = x;
+    }
+    __syncthreads();
+    int r = split_base + s_warp[wid] + ps;
+    if (sp) {
+      if (r < nfree) {
+        int dst = free_stack[nfree - 1 - r];
+        *wp = w * 0.5;
+        copies[r] = make_int2(slot, dst);
+        live_tmp[n_keep + r] = dst;
+        wsum_part += w;  // both halves
+      } else {
+        wsum_part += w;  // no free slot: keep the walker whole
+      }
+    } else if (slot >= 0) {
+      wsum_part += w;
+    }
+    int ts = s_base[3];
+    __syncthreads();
+    split_base += ts;
+  }
+  int n_split = min(split_base, nfree);
+  __syncthreads();
+  for (int i = tid; i < n_keep + n_split; i += 1024) live[i] = live_tmp[i];
+  double ws = warp_sum(wsum_part);
+  if (lane == 0) s_wsum[wid] = ws;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int k = 0; k < 32; k++) t += s_wsum[k];
+    stats[ST_FINAL_W] = t;
+    ctl[0] = n_keep + n_split;
+    ctl[1] = nfree - n_split;
+    ctl[2] = n_split;
+  }
+}
+
+// Copies whole walker blocks for the splits recorded by k_branch; the copy
+// keeps the halved weight already written to the source.
+__global__ void k_copy(double *state, Layout L, const int2 *copies, const int *ctl)
+{
+  const int nc = ctl[2];
+  for (int c = blockIdx.x; c < nc; c += gridDim.x) {
+    int2 p = copies[c];
+    const double *src = state + (size_t)p.x * L.stride;
+    double *dst = state + (size_t)p.y * L.stride;
+    for (int t = threadIdx.x; t < L.stride; t += blockDim.x) dst[t] = src[t];
+  }
+}
+
+// E_est from the running weighted energy average and
+// E_T = E_est - c ln(W / W0) (QMCManager::updateEstimatedEnergy /
+// updateTrialEnergy, QMcBeaver/src/QMCManager.cpp:2247-2310).
+__global__ void k_energy(EnergyCtl *ectl, const double *stats, int min_samples_ok)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double sw = stats[ST_RUN_SUM_W];
+  if (min_samples_ok && sw > 0.0) ectl->e_est = stats[ST_RUN_SUM_WE] / sw;
+  double ratio = stats[ST_FINAL_W] / ectl->target_weight;
+  double lr = ratio > 1e-250 ? log(ratio) : 0.0;
+  ectl->e_trial = ectl->e_est - ectl->pop_control * lr;
+}
+
+// Packs R, weight, E_L, log|psi|, sign of the first n live walkers into
+// out[n][3N + 4] for one device-to-host copy.
+__global__ void k_gather(const double *state, Layout L, int N, const int *live, int n, double *out)
+{
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = lane_id();
+  if (w >= n) return;
+  const double *blk = state + (size_t)live[w] * L.stride;
+  double *o = out + (size_t)w * (3 * N + 4);
+  for (int t = lane; t < 3 * N; t += 32) o[t] = blk[L.R + t];
+  if (lane == 0) {
+    const double *sc = blk + L.sc;
+    o[3 * N] = sc[SC_WEIGHT];
+    o[3 * N + 1] = sc[SC_EL];
+    o[3 * N + 2] = sc[SC_LOGDET_A] + sc[SC_LOGDET_B] + sc[SC_U];
+    o[3 * N + 3] = sc[SC_SIGN_A] * sc[SC_SIGN_B];
+  }
+}
+
+// Sets the weights of the first n live walkers.
+__global__ void k_set_weights(double *state, Layout L, const int *live, int n, const double *w)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    state[(size_t)live[i] * L.stride + L.sc + SC_WEIGHT] = w[i];
+}
+
+}  // namespace qmcb

@@ -1,0 +1,683 @@
+// qmcb200.cu -- C ABI of the B200 Slater-Jastrow walker library.
+//
+// Host side of include/qmcb200.h: device tables for the molecular system,
+// the per-walker state blocks, the live-walker list used by DMC branching,
+// and the launch sequence of one Monte Carlo step.  Kernels are in
+// kernels.cuh.  No CPU fallback: every entry point fails with QMCB_E_CUDA
+// when no CUDA device is usable.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/qmcb200.h"
+#include "kernels.cuh"
+
+using namespace qmcb;
+
+namespace {
+
+const int kWarpsPerBlock = 4;
+
+std::string g_create_error;
+
+}  // namespace
+
+struct qmcb_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevSys sys{};
+  Layout lay{};
+  int N = 0, K = 0, nmax = 0, max_walkers = 0;
+  qmcb_run_params params{};
+  // device buffers
+  double4 *d_nuc = nullptr;
+  int4 *d_bf = nullptr;
+  double2 *d_prim = nullptr;
+  double *d_ct[2] = {nullptr, nullptr};
+  double *d_pade = nullptr;
+  int2 *d_pade_len = nullptr;
+  int *d_en[2] = {nullptr, nullptr};
+  double *d_state = nullptr;
+  int *d_live = nullptr, *d_live_tmp = nullptr, *d_free = nullptr, *d_ctl = nullptr;
+  int2 *d_copies = nullptr;
+  double *d_stats = nullptr;
+  EnergyCtl *d_ectl = nullptr;
+  // staging for the host-pointer evaluate
+  int *d_slots = nullptr;
+  double *d_R = nullptr, *d_out = nullptr;
+  unsigned char *d_status = nullptr;
+  int n_live_host = 0;
+  double target_weight = 0.0;
+  size_t smem_move = 0, smem_full = 0;
+  bool evaluated_once = false;
+  // kernel timing (qmcb_set_profiling)
+  bool prof = false;
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<int> prof_kind;
+  size_t prof_used = 0;
+  double prof_ms[QMCB_KERNEL_COUNT] = {0};
+  double prof_n[QMCB_KERNEL_COUNT] = {0};
+  std::string err;
+};
+
+// Event pair around one launch when profiling is on.
+struct ProfScope {
+  qmcb_handle *h;
+  size_t idx;
+  ProfScope(qmcb_handle *hh, int kind, cudaStream_t st) : h(hh), idx((size_t)-1)
+  {
+    if (!h->prof) return;
+    if (h->prof_used + 2 > h->prof_ev.size()) {
+      size_t grow = std::max<size_t>(256, h->prof_ev.size());
+      for (size_t i = 0; i < grow; i++) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        h->prof_ev.push_back(e);
+      }
+    }
+    idx = h->prof_used;
+    h->prof_used += 2;
+    h->prof_kind.push_back(kind);
+    cudaEventRecord(h->prof_ev[idx], st);
+  }
+  void end(cudaStream_t st)
+  {
+    if (idx != (size_t)-1) cudaEventRecord(h->prof_ev[idx + 1], st);
+  }
+};
+
+// Folds the recorded event pairs into the totals (stream must be idle).
+static void prof_collect(qmcb_handle *h)
+{
+  for (size_t i = 0; i + 1 < h->prof_used && i / 2 < h->prof_kind.size(); i += 2) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->prof_ev[i], h->prof_ev[i + 1]) == cudaSuccess) {
+      int k = h->prof_kind[i / 2];
+      h->prof_ms[k] += ms;
+      h->prof_n[k] += 1.0;
+    }
+  }
+  h->prof_used = 0;
+  h->prof_kind.clear();
+}
+
+static int fail(qmcb_handle *h, int code, const std::string &msg)
+{
+  if (h)
+    h->err = msg;
+  else
+    g_create_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(h, QMCB_E_CUDA, std::string(#call ": ") + cudaGetErrorString(e_));   \
+  } while (0)
+
+static RunCfg make_cfg(const qmcb_run_params &p)
+{
+  RunCfg c{};
+  c.run_type = p.run_type;
+  c.sampling = p.sampling;
+  c.qf_mod = p.qf_modification;
+  c.emod = p.energy_modification;
+  c.reweighting = p.reweighting;
+  c.old_walker_acceptance = p.old_walker_acceptance;
+  c.qf_a = p.qf_equal_a;
+  c.dt = p.dt;
+  c.dt_eff = p.dt_effective;
+  c.branching_threshold = p.branching_threshold;
+  c.fusion_threshold = p.fusion_threshold;
+  c.seed = p.seed;
+  return c;
+}
+
+static void default_params(qmcb_run_params *p)
+{
+  std::memset(p, 0, sizeof(*p));
+  p->run_type = QMCB_VMC;
+  p->sampling = QMCB_NO_IMPORTANCE_SAMPLING;
+  p->qf_modification = QMCB_QF_NONE;
+  p->qf_equal_a = 0.5;
+  p->dt = 0.09;
+  p->dt_effective = 0.09;
+  p->energy_modification = QMCB_EMOD_NONE;
+  p->reweighting = QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED;
+  p->branching_threshold = 2.0;
+  p->fusion_threshold = 0.45;
+  p->old_walker_acceptance = 50;
+  p->refresh_interval = 0;
+  p->precision = QMCB_PREC_FP64;
+  p->seed = 12345;
+  p->population_control = 1.0;
+  p->target_walkers = 0;
+  p->reweight_start_step = 100;
+}
+
+template <typename T>
+static cudaError_t upload(T **d, const std::vector<T> &v)
+{
+  cudaError_t e = cudaMalloc((void **)d, sizeof(T) * std::max<size_t>(v.size(), 1));
+  if (e != cudaSuccess) return e;
+  if (!v.empty()) e = cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+  return e;
+}
+
+extern "C" {
+
+const char *qmcb_version(void) { return "qmcb200 0.1 (sm_100a, FP64 parity path)"; }
+
+const char *qmcb_last_error(const qmcb_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
+{
+  qmcb_handle *h = nullptr;
+  if (!d || !out || max_walkers <= 0) return fail(nullptr, QMCB_E_ARG, "qmcb_create: null argument or max_walkers <= 0");
+  *out = nullptr;
+  const int M = d->n_nuclei, na = d->n_alpha, nb = d->n_beta, K = d->n_basis;
+  if (M <= 0 || na < 0 || nb < 0 || na + nb <= 0 || K <= 0 || d->n_pade < 0)
+    return fail(nullptr, QMCB_E_ARG, "qmcb_create: bad sizes");
+  if (na > 256 || nb > 256 || K > 4096 || M > 1024)
+    return fail(nullptr, QMCB_E_LIMIT, "qmcb_create: n_alpha/n_beta <= 256, n_basis <= 4096, n_nuclei <= 1024");
+  int ndev = 0;
+  cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess || ndev == 0)
+    return fail(nullptr, QMCB_E_CUDA, std::string("qmcb_create: no CUDA device: ") + cudaGetErrorString(ce));
+
+  h = new (std::nothrow) qmcb_handle();
+  if (!h) return fail(nullptr, QMCB_E_NOMEM, "qmcb_create: out of host memory");
+  cudaGetDevice(&h->device);
+  h->N = na + nb;
+  h->K = K;
+  h->nmax = std::max(na, nb);
+  h->max_walkers = max_walkers;
+  default_params(&h->params);
+
+  // ---- system tables
+  std::vector<double4> nuc(M);
+  for (int a = 0; a < M; a++)
+    nuc[a] = make_double4(d->nuc_xyz[3 * a], d->nuc_xyz[3 * a + 1], d->nuc_xyz[3 * a + 2], d->nuc_charge[a]);
+  std::vector<int4> bf(K);
+  for (int k = 0; k < K; k++) {
+    int a = d->bf_powers[3 * k], b = d->bf_powers[3 * k + 1], c = d->bf_powers[3 * k + 2];
+    if (d->bf_atom[k] < 0 || d->bf_atom[k] >= M || a < 0 || b < 0 || c < 0 || a > 15 || b > 15 || c > 15 ||
+        d->bf_nprim[k] <= 0 || d->bf_prim_offset[k] < 0 ||
+        d->bf_prim_offset[k] + d->bf_nprim[k] > d->n_prim_total) {
+      delete h;
+      return fail(nullptr, QMCB_E_ARG, "qmcb_create: bad basis function table");
+    }
+    bf[k] = make_int4(d->bf_atom[k], a | (b << 8) | (c << 16), d->bf_nprim[k], d->bf_prim_offset[k]);
+  }
+  std::vector<double2> prim(d->n_prim_total);
+  for (int i = 0; i < d->n_prim_total; i++) prim[i] = make_double2(d->prim_exponent[i], d->prim_coeff[i]);
+  std::vector<double> ct[2];
+  for (int sp = 0; sp < 2; sp++) {
+    int n = sp ? nb : na;
+    const double *mo = sp ? d->mo_beta : d->mo_alpha;
+    ct[sp].assign((size_t)K * std::max(n, 1), 0.0);
+    for (int o = 0; o < n; o++)
+      for (int k = 0; k < K; k++) ct[sp][(size_t)k * n + o] = mo[(size_t)o * K + k];
+  }
+  std::vector<double> pade((size_t)std::max(d->n_pade, 1) * 2 * kPadeMax, 0.0);
+  std::vector<int2> plen(std::max(d->n_pade, 1), make_int2(1, 1));
+  for (int f = 0; f < d->n_pade; f++) {
+    int ln = d->pade_nnum[f], ld = d->pade_nden[f];
+    if (ln < 1 || ln > kPadeMax || ld < 1 || ld > kPadeMax) {
+      delete h;
+      return fail(nullptr, QMCB_E_ARG, "qmcb_create: Pade polynomial length out of range");
+    }
+    for (int i = 0; i < kPadeMax; i++) {
+      pade[(size_t)f * 2 * kPadeMax + i] = d->pade_num[f * kPadeMax + i];
+      pade[(size_t)f * 2 * kPadeMax + kPadeMax + i] = d->pade_den[f * kPadeMax + i];
+    }
+    plen[f] = make_int2(ln, ld);
+  }
+  for (int i = 0; i < 3; i++)
+    if (d->ee_pade[i] >= d->n_pade) {
+      delete h;
+      return fail(nullptr, QMCB_E_ARG, "qmcb_create: ee_pade index out of range");
+    }
+  std::vector<int> en[2];
+  for (int sp = 0; sp < 2; sp++) {
+    const int *src = sp ? d->en_pade_dn : d->en_pade_up;
+    en[sp].assign(M, -1);
+    for (int a = 0; a < M; a++) {
+      en[sp][a] = src ? src[a] : -1;
+      if (en[sp][a] >= d->n_pade) {
+        delete h;
+        return fail(nullptr, QMCB_E_ARG, "qmcb_create: en_pade index out of range");
+      }
+    }
+  }
+  double Pnn = 0.0;
+  for (int i = 0; i < M; i++)
+    for (int j = i + 1; j < M; j++) {
+      double dx = nuc[i].x - nuc[j].x, dy = nuc[i].y - nuc[j].y, dz = nuc[i].z - nuc[j].z;
+      Pnn += (nuc[i].w * nuc[j].w) / std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+
+#define CKC(call)                                                                           \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) {                                                                \
+      std::string m_ = std::string("qmcb_create: " #call ": ") + cudaGetErrorString(e_);    \
+      qmcb_destroy(h);                                                                      \
+      return fail(nullptr, e_ == cudaErrorMemoryAllocation ? QMCB_E_NOMEM : QMCB_E_CUDA, m_); \
+    }                                                                                       \
+  } while (0)
+  CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CKC(upload(&h->d_nuc, nuc));
+  CKC(upload(&h->d_bf, bf));
+  CKC(upload(&h->d_prim, prim));
+  CKC(upload(&h->d_ct[0], ct[0]));
+  CKC(upload(&h->d_ct[1], ct[1]));
+  CKC(upload(&h->d_pade, pade));
+  CKC(upload(&h->d_pade_len, plen));
+  CKC(upload(&h->d_en[0], en[0]));
+  CKC(upload(&h->d_en[1], en[1]));
+
+  DevSys &S = h->sys;
+  S.M = M;
+  S.na = na;
+  S.nb = nb;
+  S.N = h->N;
+  S.K = K;
+  S.npade = d->n_pade;
+  for (int i = 0; i < 3; i++) S.ee[i] = d->ee_pade[i];
+  S.Pnn = Pnn;
+  S.nuc = h->d_nuc;
+  S.bf = h->d_bf;
+  S.prim = h->d_prim;
+  S.ct[0] = h->d_ct[0];
+  S.ct[1] = h->d_ct[1];
+  S.pade = h->d_pade;
+  S.pade_len = h->d_pade_len;
+  S.en[0] = h->d_en[0];
+  S.en[1] = h->d_en[1];
+
+  // ---- per-walker block layout (offsets in doubles, arrays 32-byte aligned)
+  Layout &L = h->lay;
+  int off = 0;
+  auto take = [&](int count) {
+    int o = off;
+    off += (count + 3) & ~3;
+    return o;
+  };
+  L.R = take(3 * h->N);
+  for (int sp = 0; sp < 2; sp++) {
+    int n = sp ? nb : na;
+    L.Dv[sp] = take(n * n);
+    L.DgT[sp] = take(3 * n * n);
+    L.DlT[sp] = take(n * n);
+    L.Inv[sp] = take(n * n);
+  }
+  L.gradD = take(3 * h->N);
+  L.Ux = take(3 * h->N);
+  L.grad = take(3 * h->N);
+  L.mgrad = take(3 * h->N);
+  L.sc = take(kScalars);
+  L.stride = (off + 31) & ~31;  // 256-byte aligned blocks
+
+  size_t bytes = (size_t)max_walkers * L.stride * sizeof(double);
+  CKC(cudaMalloc(&h->d_state, bytes));
+  CKC(cudaMemset(h->d_state, 0, bytes));
+  CKC(cudaMalloc(&h->d_live, sizeof(int) * max_walkers));
+  CKC(cudaMalloc(&h->d_live_tmp, sizeof(int) * max_walkers));
+  CKC(cudaMalloc(&h->d_free, sizeof(int) * max_walkers));
+  CKC(cudaMalloc(&h->d_ctl, sizeof(int) * 4));
+  CKC(cudaMalloc(&h->d_copies, sizeof(int2) * max_walkers));
+  CKC(cudaMalloc(&h->d_stats, sizeof(double) * ST_COUNT));
+  CKC(cudaMemset(h->d_stats, 0, sizeof(double) * ST_COUNT));
+  CKC(cudaMalloc(&h->d_ectl, sizeof(EnergyCtl)));
+  CKC(cudaMalloc(&h->d_slots, sizeof(int) * max_walkers));
+  CKC(cudaMalloc(&h->d_R, sizeof(double) * (size_t)max_walkers * 3 * h->N));
+  CKC(cudaMalloc(&h->d_out, sizeof(double) * (size_t)max_walkers * (6 * h->N + 8)));
+  CKC(cudaMalloc(&h->d_status, max_walkers));
+
+  h->smem_move = sizeof(double) * (size_t)kWarpsPerBlock * move_scratch_doubles(h->N, K, h->nmax);
+  h->smem_full = sizeof(double) * (size_t)kWarpsPerBlock * full_scratch_doubles(h->N, K, h->nmax);
+  int max_optin = 0;
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  if ((int)h->smem_move > max_optin || (int)h->smem_full > max_optin) {
+    qmcb_destroy(h);
+    return fail(nullptr, QMCB_E_LIMIT, "qmcb_create: system too large for the per-walker shared-memory scratch");
+  }
+  CKC(cudaFuncSetAttribute(k_move<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
+  CKC(cudaFuncSetAttribute(k_move<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
+  CKC(cudaFuncSetAttribute(k_full, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_full));
+#undef CKC
+  *out = h;
+  return QMCB_OK;
+}
+
+int qmcb_destroy(qmcb_handle *h)
+{
+  if (!h) return QMCB_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  void *ptrs[] = {h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
+                  h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
+                  h->d_copies, h->d_stats, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return QMCB_OK;
+}
+
+int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
+{
+  if (!h || !p) return fail(h, QMCB_E_ARG, "qmcb_set_params: null argument");
+  if (!(p->dt > 0)) return fail(h, QMCB_E_ARG, "qmcb_set_params: dt must be positive");
+  if (p->qf_modification == QMCB_QF_UMRIGAR93_EQUAL && (p->qf_equal_a > 1 || p->qf_equal_a <= 0))
+    return fail(h, QMCB_E_ARG, "qmcb_set_params: umrigar93_equalelectrons_parameter must be in (0, 1]");
+  if (p->run_type < 0 || p->run_type > 1 || p->sampling < 0 || p->sampling > 1 || p->qf_modification < 0 ||
+      p->qf_modification > 2 || p->energy_modification < 0 || p->energy_modification > 2 || p->reweighting < 0 ||
+      p->reweighting > 2)
+    return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");
+  if (p->precision != QMCB_PREC_FP64) return fail(h, QMCB_E_ARG, "qmcb_set_params: only QMCB_PREC_FP64 in this build");
+  h->params = *p;
+  if (h->n_live_host > 0) {
+    // the host's E_T / E_est feed the next steps (QMCManager::updateTrialEnergy)
+    EnergyCtl ec{};
+    ec.e_trial = p->energy_trial;
+    ec.e_est = p->energy_estimated;
+    ec.target_weight = p->target_walkers > 0 ? p->target_walkers : h->target_weight;
+    ec.pop_control = p->population_control;
+    CK(cudaMemcpyAsync(h->d_ectl, &ec, sizeof(ec), cudaMemcpyHostToDevice, h->stream));
+  }
+  return QMCB_OK;
+}
+
+int qmcb_get_params(const qmcb_handle *h, qmcb_run_params *p)
+{
+  if (!h || !p) return QMCB_E_ARG;
+  *p = h->params;
+  return QMCB_OK;
+}
+
+int qmcb_num_electrons(const qmcb_handle *h) { return h ? h->N : -1; }
+int qmcb_max_walkers(const qmcb_handle *h) { return h ? h->max_walkers : -1; }
+void *qmcb_stream(qmcb_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int qmcb_synchronize(qmcb_handle *h)
+{
+  if (!h) return QMCB_E_ARG;
+  CK(cudaStreamSynchronize(h->stream));
+  return QMCB_OK;
+}
+
+static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num, const double *d_R, EvalOut o,
+                       cudaStream_t st)
+{
+  RunCfg cfg = make_cfg(h->params);
+  int blocks = (num + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (which_e < 0) {
+    k_full<<<blocks, 32 * kWarpsPerBlock, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
+                                                              nullptr, d_R, 1, o);
+  } else {
+    MoveArgs mv{which_e, 0, 0, 0};
+    k_move<false><<<blocks, 32 * kWarpsPerBlock, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
+                                                                     num, nullptr, d_R, mv, h->d_ectl,
+                                                                     h->d_stats, o);
+  }
+  CK(cudaGetLastError());
+  return QMCB_OK;
+}
+
+int qmcb_evaluate_device(qmcb_handle *h, int which_e, const int *d_slots, int num, const double *d_R,
+                         double *d_log_abs_psi, double *d_sign, double *d_grad, double *d_mod_grad, double *d_lap,
+                         double *d_e_local, double *d_pe, unsigned char *d_status, void *stream)
+{
+  if (!h) return QMCB_E_ARG;
+  if (num < 0 || num > h->max_walkers || which_e < -1 || which_e >= h->N || !d_R || (num > 0 && !d_slots))
+    return fail(h, QMCB_E_ARG, "qmcb_evaluate_device: bad argument");
+  if (which_e >= 0 && !h->evaluated_once)
+    return fail(h, QMCB_E_STATE, "qmcb_evaluate_device: one-electron update before any full evaluation");
+  if (num == 0) return QMCB_OK;
+  EvalOut o{d_log_abs_psi, d_sign, d_grad, d_mod_grad, d_lap, d_e_local, d_pe, d_status};
+  int rc = launch_eval(h, which_e, d_slots, num, d_R, o, stream ? (cudaStream_t)stream : h->stream);
+  if (rc == QMCB_OK && which_e < 0) h->evaluated_once = true;
+  return rc;
+}
+
+int qmcb_evaluate(qmcb_handle *h, int which_e, const int *slots, int num, const double *R, double *log_abs_psi,
+                  double *sign, double *grad, double *mod_grad, double *lap, double *e_local, double *pe,
+                  unsigned char *status)
+{
+  if (!h) return QMCB_E_ARG;
+  if (num < 0 || num > h->max_walkers || which_e < -1 || which_e >= h->N || !R || !slots)
+    return fail(h, QMCB_E_ARG, "qmcb_evaluate: bad argument");
+  for (int i = 0; i < num; i++)
+    if (slots[i] < 0 || slots[i] >= h->max_walkers) return fail(h, QMCB_E_ARG, "qmcb_evaluate: slot out of range");
+  if (which_e >= 0 && !h->evaluated_once)
+    return fail(h, QMCB_E_STATE, "qmcb_evaluate: one-electron update before any full evaluation");
+  if (num == 0) return QMCB_OK;
+  const int N = h->N;
+  cudaStream_t st = h->stream;
+  CK(cudaMemcpyAsync(h->d_slots, slots, sizeof(int) * num, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->d_R, R, sizeof(double) * (size_t)num * 3 * N, cudaMemcpyHostToDevice, st));
+  double *base = h->d_out;
+  double *o_lp = base, *o_sg = o_lp + num, *o_lap = o_sg + num, *o_el = o_lap + num, *o_pe = o_el + num;
+  double *o_g = o_pe + 3 * (size_t)num, *o_mg = o_g + 3 * (size_t)N * num;
+  EvalOut o{o_lp, o_sg, o_g, o_mg, o_lap, o_el, o_pe, h->d_status};
+  int rc = launch_eval(h, which_e, h->d_slots, num, h->d_R, o, st);
+  if (rc) return rc;
+  if (which_e < 0) h->evaluated_once = true;
+  if (log_abs_psi) CK(cudaMemcpyAsync(log_abs_psi, o_lp, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
+  if (sign) CK(cudaMemcpyAsync(sign, o_sg, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
+  if (lap) CK(cudaMemcpyAsync(lap, o_lap, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
+  if (e_local) CK(cudaMemcpyAsync(e_local, o_el, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
+  if (pe) CK(cudaMemcpyAsync(pe, o_pe, sizeof(double) * 3 * num, cudaMemcpyDeviceToHost, st));
+  if (grad) CK(cudaMemcpyAsync(grad, o_g, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
+  if (mod_grad)
+    CK(cudaMemcpyAsync(mod_grad, o_mg, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
+  if (status) CK(cudaMemcpyAsync(status, h->d_status, num, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return QMCB_OK;
+}
+
+int qmcb_init_walkers(qmcb_handle *h, int n, const double *R)
+{
+  if (!h) return QMCB_E_ARG;
+  if (n <= 0 || n > h->max_walkers || !R) return fail(h, QMCB_E_ARG, "qmcb_init_walkers: bad argument");
+  cudaStream_t st = h->stream;
+  std::vector<int> live(h->max_walkers), fr(h->max_walkers);
+  for (int i = 0; i < n; i++) live[i] = i;
+  // free stack: popped from the top, so store the highest slots first
+  int nf = h->max_walkers - n;
+  for (int i = 0; i < nf; i++) fr[i] = h->max_walkers - 1 - i;
+  CK(cudaMemcpyAsync(h->d_live, live.data(), sizeof(int) * h->max_walkers, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->d_free, fr.data(), sizeof(int) * h->max_walkers, cudaMemcpyHostToDevice, st));
+  int ctl[4] = {n, nf, 0, 0};
+  CK(cudaMemcpyAsync(h->d_ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->d_R, R, sizeof(double) * (size_t)n * 3 * h->N, cudaMemcpyHostToDevice, st));
+  EvalOut o{};
+  int rc = launch_eval(h, -1, h->d_live, n, h->d_R, o, st);
+  if (rc) return rc;
+  h->evaluated_once = true;
+  EnergyCtl ec{};
+  ec.e_trial = h->params.energy_trial;
+  ec.e_est = h->params.energy_estimated;
+  ec.target_weight = h->params.target_walkers > 0 ? h->params.target_walkers : n;
+  ec.pop_control = h->params.population_control;
+  h->target_weight = ec.target_weight;
+  CK(cudaMemcpyAsync(h->d_ectl, &ec, sizeof(ec), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(h->d_stats, 0, sizeof(double) * ST_COUNT, st));
+  CK(cudaStreamSynchronize(st));
+  h->n_live_host = n;
+  return QMCB_OK;
+}
+
+int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats *stats)
+{
+  if (!h) return QMCB_E_ARG;
+  if (n_steps < 0 || first_step < 0) return fail(h, QMCB_E_ARG, "qmcb_run_steps: bad step range");
+  if (!h->evaluated_once || h->n_live_host <= 0)
+    return fail(h, QMCB_E_STATE, "qmcb_run_steps: call qmcb_init_walkers first");
+  cudaStream_t st = h->stream;
+  RunCfg cfg = make_cfg(h->params);
+  // per-call sums; the running E_est sums persist across calls
+  CK(cudaMemsetAsync(h->d_stats, 0, sizeof(double) * ST_RUN_SUM_W, st));
+  const int blocks = (h->max_walkers + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const bool dmc = h->params.run_type == QMCB_DMC;
+  for (int s = 0; s < n_steps; s++) {
+    int step = first_step + s;
+    MoveArgs mv;
+    mv.e = step % h->N;
+    mv.step = step;
+    mv.do_reweight = mv.e == 0;
+    mv.reweight_on = step >= h->params.reweight_start_step;
+    EvalOut o{};
+    {
+      ProfScope ps(h, QMCB_KERNEL_MOVE, st);
+      k_move<true><<<blocks, 32 * kWarpsPerBlock, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live,
+                                                                      0, h->d_ctl, nullptr, mv, h->d_ectl,
+                                                                      h->d_stats, o);
+      ps.end(st);
+    }
+    if (dmc && mv.e == 0) {
+      {
+        ProfScope ps(h, QMCB_KERNEL_BRANCH, st);
+        k_branch<<<1, 1024, 0, st>>>(h->d_state, h->lay, h->d_live, h->d_live_tmp, h->d_free, h->d_ctl,
+                                     h->d_copies, h->params.branching_threshold, h->params.fusion_threshold,
+                                     h->params.seed, step, h->d_stats);
+        ps.end(st);
+      }
+      {
+        ProfScope ps(h, QMCB_KERNEL_COPY, st);
+        k_copy<<<592, 256, 0, st>>>(h->d_state, h->lay, h->d_copies, h->d_ctl);
+        ps.end(st);
+      }
+      {
+        ProfScope ps(h, QMCB_KERNEL_ENERGY, st);
+        k_energy<<<1, 32, 0, st>>>(h->d_ectl, h->d_stats, 1);
+        ps.end(st);
+      }
+    }
+    if (h->params.refresh_interval > 0 && (step + 1) % h->params.refresh_interval == 0) {
+      EvalOut o2{};
+      ProfScope ps(h, QMCB_KERNEL_REFRESH, st);
+      k_full<<<blocks, 32 * kWarpsPerBlock, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live, 0,
+                                                                h->d_ctl, nullptr, 0, o2);
+      ps.end(st);
+    }
+  }
+  CK(cudaGetLastError());
+  double sv[ST_COUNT];
+  int ctl[4];
+  CK(cudaMemcpyAsync(sv, h->d_stats, sizeof(sv), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(ctl, h->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (h->prof) prof_collect(h);
+  h->n_live_host = ctl[0];
+  if (stats) {
+    stats->sum_weight = sv[ST_SUM_W];
+    stats->sum_weight_energy = sv[ST_SUM_WE];
+    stats->sum_weight_energy2 = sv[ST_SUM_WE2];
+    stats->sum_accept = sv[ST_SUM_ACC];
+    stats->n_moves = sv[ST_MOVES];
+    stats->final_weight = sv[ST_FINAL_W];
+    stats->n_walkers = ctl[0];
+    stats->n_singular = (int)sv[ST_SINGULAR];
+  }
+  return QMCB_OK;
+}
+
+int qmcb_num_walkers(const qmcb_handle *h) { return h ? h->n_live_host : -1; }
+
+int qmcb_get_walkers(qmcb_handle *h, int n, double *R, double *weight, double *e_local, double *log_abs_psi,
+                     double *sign)
+{
+  if (!h) return QMCB_E_ARG;
+  if (n < 0 || n > h->n_live_host) return fail(h, QMCB_E_ARG, "qmcb_get_walkers: n beyond live walkers");
+  if (n == 0) return QMCB_OK;
+  cudaStream_t st = h->stream;
+  const int N = h->N, rec = 3 * N + 4;
+  k_gather<<<(n + 3) / 4, 128, 0, st>>>(h->d_state, h->lay, N, h->d_live, n, h->d_out);
+  CK(cudaGetLastError());
+  std::vector<double> buf((size_t)n * rec);
+  CK(cudaMemcpyAsync(buf.data(), h->d_out, sizeof(double) * buf.size(), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int i = 0; i < n; i++) {
+    const double *o = buf.data() + (size_t)i * rec;
+    if (R) std::memcpy(R + (size_t)i * 3 * N, o, sizeof(double) * 3 * N);
+    if (weight) weight[i] = o[3 * N];
+    if (e_local) e_local[i] = o[3 * N + 1];
+    if (log_abs_psi) log_abs_psi[i] = o[3 * N + 2];
+    if (sign) sign[i] = o[3 * N + 3];
+  }
+  return QMCB_OK;
+}
+
+int qmcb_set_walker_weights(qmcb_handle *h, int n, const double *w)
+{
+  if (!h) return QMCB_E_ARG;
+  if (n < 0 || n > h->n_live_host || (n > 0 && !w)) return fail(h, QMCB_E_ARG, "qmcb_set_walker_weights: bad n");
+  if (n == 0) return QMCB_OK;
+  cudaStream_t st = h->stream;
+  CK(cudaMemcpyAsync(h->d_out, w, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+  k_set_weights<<<(n + 255) / 256, 256, 0, st>>>(h->d_state, h->lay, h->d_live, n, h->d_out);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(st));
+  return QMCB_OK;
+}
+
+int qmcb_branch(qmcb_handle *h, int step, int *n_live)
+{
+  if (!h) return QMCB_E_ARG;
+  if (!h->evaluated_once || h->n_live_host <= 0) return fail(h, QMCB_E_STATE, "qmcb_branch: no live walkers");
+  cudaStream_t st = h->stream;
+  k_branch<<<1, 1024, 0, st>>>(h->d_state, h->lay, h->d_live, h->d_live_tmp, h->d_free, h->d_ctl, h->d_copies,
+                               h->params.branching_threshold, h->params.fusion_threshold, h->params.seed, step,
+                               h->d_stats);
+  k_copy<<<592, 256, 0, st>>>(h->d_state, h->lay, h->d_copies, h->d_ctl);
+  CK(cudaGetLastError());
+  int ctl[4];
+  CK(cudaMemcpyAsync(ctl, h->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  h->n_live_host = ctl[0];
+  if (n_live) *n_live = ctl[0];
+  return QMCB_OK;
+}
+
+int qmcb_set_profiling(qmcb_handle *h, int enable)
+{
+  if (!h) return QMCB_E_ARG;
+  h->prof = enable != 0;
+  return QMCB_OK;
+}
+
+int qmcb_get_kernel_stats(qmcb_handle *h, double *out, int reset)
+{
+  if (!h || !out) return QMCB_E_ARG;
+  for (int k = 0; k < QMCB_KERNEL_COUNT; k++) {
+    out[2 * k] = h->prof_ms[k];
+    out[2 * k + 1] = h->prof_n[k];
+    if (reset) h->prof_ms[k] = h->prof_n[k] = 0.0;
+  }
+  return QMCB_OK;
+}
+
+int qmcb_copy_slot(qmcb_handle *h, int src, int dst)
+{
+  if (!h) return QMCB_E_ARG;
+  if (src < 0 || dst < 0 || src >= h->max_walkers || dst >= h->max_walkers)
+    return fail(h, QMCB_E_ARG, "qmcb_copy_slot: slot out of range");
+  if (src == dst) return QMCB_OK;
+  size_t b = sizeof(double) * h->lay.stride;
+  CK(cudaMemcpyAsync(h->d_state + (size_t)dst * h->lay.stride, h->d_state + (size_t)src * h->lay.stride, b,
+                     cudaMemcpyDeviceToDevice, h->stream));
+  return QMCB_OK;
+}
+
+}  // extern "C"

@@ -40,7 +40,8 @@ class RunParams(C.Structure):
         ("reweighting", C.c_int), ("energy_trial", C.c_double), ("energy_estimated", C.c_double),
         ("branching_threshold", C.c_double), ("fusion_threshold", C.c_double),
         ("old_walker_acceptance", C.c_int), ("refresh_interval", C.c_int), ("precision", C.c_int),
-        ("seed", C.c_uint64),
+        ("seed", C.c_uint64), ("population_control", C.c_double), ("target_walkers", C.c_int),
+        ("reweight_start_step", C.c_int),
     ]
 
 
@@ -70,6 +71,9 @@ def run_params(**kw) -> RunParams:
     p.refresh_interval = 0
     p.precision = QMCB_PREC_FP64
     p.seed = 12345
+    p.population_control = 1.0
+    p.target_walkers = 0
+    p.reweight_start_step = 100
     for k, v in kw.items():
         if not hasattr(p, k):
             raise AttributeError(k)

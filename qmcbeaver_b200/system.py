@@ -531,3 +531,64 @@ def make_system(workload: str, seed: int = 1, jastrow: bool = True) -> Molecular
         return make_water_like(seed, jastrow)
     return make_random_molecule(w["n_elec"], w["n_nuclei"], w["n_basis"], w["box"], w["z"], seed=seed,
                                 jastrow=jastrow, name=workload)
+
+
+# ------------------------------------------------------------ serialisation
+def system_to_arrays(s: MolecularSystem) -> Dict[str, np.ndarray]:
+    """Flat arrays (npz friendly) that rebuild the system exactly."""
+    types, atom, nprim, ex, co = [], [], [], [], []
+    for a, fs in enumerate(s.basis):
+        for f in fs:
+            types.append(f.type)
+            atom.append(a)
+            nprim.append(len(f.exponents))
+            ex.extend(float(v) for v in f.exponents)
+            co.extend(float(v) for v in f.coefficients)
+
+    def pade_arr(p: Optional[Pade]) -> np.ndarray:
+        out = np.full((2, PADE_MAX + 1), np.nan)
+        if p is not None:
+            out[0, 0] = len(p.num)
+            out[0, 1:1 + len(p.num)] = p.num
+            out[1, 0] = len(p.den)
+            out[1, 1:1 + len(p.den)] = p.den
+        return out
+
+    return dict(
+        labels=np.array(s.labels), Z=s.Z, coords=s.coords, bf_type=np.array(types), bf_atom=np.array(atom),
+        bf_nprim=np.array(nprim), prim_exp=np.array(ex), prim_coef=np.array(co), mo=s.mo,
+        n_alpha=np.array(s.n_alpha), n_beta=np.array(s.n_beta), alpha_occ=s.alpha_occ, beta_occ=s.beta_occ,
+        ee_anti=pade_arr(s.ee_anti), ee_para_up=pade_arr(s.ee_para_up), ee_para_dn=pade_arr(s.ee_para_dn),
+        en_up=np.stack([pade_arr(s.en_up.get(l)) for l in s.labels]),
+        en_dn=np.stack([pade_arr(s.en_dn.get(l)) for l in s.labels]),
+        name=np.array(s.name))
+
+
+def system_from_arrays(d) -> MolecularSystem:
+    def pade_of(a) -> Optional[Pade]:
+        a = np.asarray(a)
+        if np.isnan(a[0, 0]):
+            return None
+        nn, nd = int(a[0, 0]), int(a[1, 0])
+        return Pade(num=list(a[0, 1:1 + nn]), den=list(a[1, 1:1 + nd]))
+
+    labels = [str(x) for x in d["labels"]]
+    basis: List[List[BasisFunction]] = [[] for _ in labels]
+    p = 0
+    for t, a, n in zip(d["bf_type"], d["bf_atom"], d["bf_nprim"]):
+        basis[int(a)].append(BasisFunction(str(t), np.array(d["prim_exp"][p:p + n]), np.array(d["prim_coef"][p:p + n])))
+        p += int(n)
+    en_up = {}
+    en_dn = {}
+    for i, l in enumerate(labels):
+        pu, pd = pade_of(d["en_up"][i]), pade_of(d["en_dn"][i])
+        if pu is not None:
+            en_up[l] = pu
+        if pd is not None:
+            en_dn[l] = pd
+    return MolecularSystem(
+        labels=labels, Z=np.array(d["Z"], np.float64), coords=np.array(d["coords"], np.float64), basis=basis,
+        mo=np.array(d["mo"], np.float64), n_alpha=int(d["n_alpha"]), n_beta=int(d["n_beta"]),
+        alpha_occ=np.array(d["alpha_occ"]), beta_occ=np.array(d["beta_occ"]),
+        ee_anti=pade_of(d["ee_anti"]), ee_para_up=pade_of(d["ee_para_up"]), ee_para_dn=pade_of(d["ee_para_dn"]),
+        en_up=en_up, en_dn=en_dn, name=str(d["name"]))

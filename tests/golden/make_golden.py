@@ -1,0 +1,80 @@
+"""Generates the golden vectors in tests/golden/*.npz from the reference
+QMcBeaver CPU code itself (built from its sources by oracle/Makefile into
+oracle/_ref/libqmcref.so and driven through QMCSCFJastrow::evaluate).
+
+Each case: a synthetic system, walker positions, then a sequence of
+evaluate calls -- a full evaluation (whichE = -1) followed by single-electron
+moves (whichE = e, Sherman-Morrison path), including moves that put an
+electron back where it was (the reference's rejection path,
+QMcBeaver/src/QMCWalker.cpp:254-266).  Recorded per call: log|psi|, sign,
+grad(psi)/psi, modified quantum force, lap(psi)/psi, E_L, potentials,
+singular flag.
+
+Run:  python tests/golden/make_golden.py      (needs the reference tree)
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+CASES = {
+    # name: (workload, qf_mod, dt, walkers, moves, step sigma, revert every)
+    "water_vmc": ("vmc_water_10e", 0, 0.09, 8, 24, 0.3, 5),
+    "dmc30_unequal": ("dmc_6nuc_30e", 2, 0.01, 4, 34, 0.15, 7),
+    "dmc30_equal": ("dmc_6nuc_30e", 1, 0.01, 2, 8, 0.15, 0),
+}
+
+
+def run_case(name: str) -> None:
+    from qmcbeaver_b200.system import make_system, system_to_arrays
+    from oracle.evaluators import ReferenceEvaluator
+    workload, qf, dt, W, moves, sigma, revert = CASES[name]
+    s = make_system(workload, seed=1)
+    ref = ReferenceEvaluator(s, qf_mod=qf, dt=dt)
+    rng = np.random.default_rng(2024)
+    R = s.initial_positions(W, seed=11)
+    N = s.n_electrons
+    ws = ref.new_walkers(W)
+    whichE, Rseq, outs = [], [], []
+
+    def call(e, Rnow):
+        ref.evaluate(ws, Rnow, e)
+        o = ref.results(ws)
+        whichE.append(e)
+        Rseq.append(Rnow.copy())
+        outs.append(o)
+
+    call(-1, R)
+    prev = None
+    for m in range(moves):
+        e = m % N
+        if revert and m % revert == revert - 1 and prev is not None:
+            # put the last moved electron back (the reference's rollback)
+            pe, pr = prev
+            R[:, pe] = pr
+            call(pe, R)
+            prev = None
+            continue
+        old = R[:, e].copy()
+        R[:, e] = R[:, e] + sigma * rng.standard_normal((W, 3))
+        call(e, R)
+        prev = (e, old)
+    keys = ["log_abs_psi", "sign", "grad", "mod_grad", "lap", "e_local", "potential", "ne", "ee", "singular"]
+    data = {k: np.stack([o[k] for o in outs]) for k in keys}
+    data.update(whichE=np.array(whichE), R=np.stack(Rseq), qf_mod=np.array(qf), dt=np.array(dt))
+    data.update({"sys_" + k: v for k, v in system_to_arrays(s).items()})
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)
+    print(name, "calls", len(whichE), "walkers", W, "N", N)
+
+
+if __name__ == "__main__":
+    if len(sys.argv) > 1:
+        run_case(sys.argv[1])
+    else:
+        for c in CASES:  # one process per case: the reference keeps its input in globals
+            subprocess.check_call([sys.executable, os.path.abspath(__file__), c])

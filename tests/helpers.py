@@ -1,0 +1,58 @@
+"""Shared test helpers: golden cases, replay of evaluate sequences, tolerances."""
+import glob
+import os
+
+import numpy as np
+
+from qmcbeaver_b200.system import system_from_arrays
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GOLDEN_CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+
+# Per-call parity of the plain FP64 path against the reference: 1e-10 relative
+# (psi ratio via log|psi|, drift, E_L).
+PARITY_RTOL = 1e-10
+
+
+def load_golden(name):
+    d = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+    sysd = {k[4:]: d[k] for k in d.files if k.startswith("sys_")}
+    return system_from_arrays(sysd), d
+
+
+def rel_err(a, b, floor=1.0):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))) if a.size else 0.0
+
+
+def compare(out, ref, rtol, label=""):
+    """Checks one evaluate call's outputs against reference outputs."""
+    ok = ref["singular"] == 0 if "singular" in ref else np.ones(len(ref["e_local"]), bool)
+    msgs = []
+    for k, floor in (("e_local", 1.0), ("lap", 1.0), ("potential", 1.0)):
+        e = rel_err(out[k][ok], ref[k][ok], floor)
+        if e > rtol:
+            msgs.append(f"{k} {e:.3e}")
+    # psi ratio: |d log psi| is the relative error of psi
+    e = float(np.max(np.abs(out["log_abs_psi"][ok] - ref["log_abs_psi"][ok]))) if ok.any() else 0.0
+    if e > rtol:
+        msgs.append(f"log_abs_psi {e:.3e}")
+    if not np.array_equal(out["sign"][ok], ref["sign"][ok]):
+        msgs.append("sign")
+    for k in ("grad", "mod_grad"):
+        a, b = out[k][ok], ref[k][ok]
+        scale = np.maximum(np.linalg.norm(b, axis=-1, keepdims=True), 1.0)
+        e = float(np.max(np.abs(a - b) / scale)) if a.size else 0.0
+        if e > rtol:
+            msgs.append(f"{k} {e:.3e}")
+    assert not msgs, f"{label}: " + ", ".join(msgs)
+
+
+def replay(ev_eval, d, rtol, label):
+    """Feeds the golden call sequence through ev_eval(which_e, R) -> outputs."""
+    for i, e in enumerate(d["whichE"]):
+        out = ev_eval(int(e), d["R"][i])
+        ref = {k: d[k][i] for k in ("log_abs_psi", "sign", "grad", "mod_grad", "lap", "e_local", "potential",
+                                     "singular")}
+        compare(out, ref, rtol, f"{label} call {i} whichE={e}")

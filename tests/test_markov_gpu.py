@@ -1,0 +1,165 @@
+"""The device Markov chain (qmcb_run_steps) against the oracle-driven chain:
+same algorithm, different random streams, so energies must agree within the
+combined statistical error; and DMC branching against a restatement of
+QMCRun::nonunitWeightBranching with the same device random draws."""
+import numpy as np
+import pytest
+
+from philox import uniform4
+from qmcbeaver_b200.api import QMCB200Functions
+from qmcbeaver_b200.desc import QMCB_DMC, QMCB_IMPORTANCE_SAMPLING, QMCB_QF_UMRIGAR93_UNEQUAL, run_params
+from qmcbeaver_b200.system import make_system
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_vmc(s, W, sweeps, dt, seed, warm):
+    """Single-electron Metropolis with the oracle (QMCWalker, no importance
+    sampling): R' = R + sqrt(dt) g, p = |psi'/psi|^2; observables p E' + q E
+    on the steps that move electron 0."""
+    from oracle.evaluators import OracleEvaluator
+    orc = OracleEvaluator(s, qf_mod=0, dt=dt)
+    rng = np.random.default_rng(seed)
+    N = s.n_electrons
+    R = s.initial_positions(W, seed=seed)
+    cur = orc.new_walkers(W)
+    trial = orc.new_walkers(W)
+    orc.evaluate(cur, R, -1)
+    for t, c in zip(trial, cur):
+        orc.copy(t, c)
+    res = orc.results(cur)
+    E, lp = res["e_local"].copy(), res["log_abs_psi"].copy()
+    samples = []
+    for step in range(sweeps * N):
+        e = step % N
+        Rt = R.copy()
+        Rt[:, e] += np.sqrt(dt) * rng.standard_normal((W, 3))
+        orc.evaluate(trial, Rt, e)
+        r = orc.results(trial)
+        p = np.minimum(1.0, np.exp(2 * (r["log_abs_psi"] - lp)))
+        p[r["singular"] != 0] = 0.0
+        acc = p > rng.random(W)
+        if e == 0 and step >= warm * N:
+            samples.append(np.mean(p * r["e_local"] + (1 - p) * E))
+        for i in range(W):
+            if acc[i]:
+                orc.copy(cur[i], trial[i])
+            else:
+                orc.copy(trial[i], cur[i])
+        R[acc] = Rt[acc]
+        E[acc] = r["e_local"][acc]
+        lp[acc] = r["log_abs_psi"][acc]
+    return np.array(samples)
+
+
+def block_stats(x, nblocks=20):
+    b = np.array_split(np.asarray(x), nblocks)
+    m = np.array([bb.mean() for bb in b])
+    return m.mean(), m.std(ddof=1) / np.sqrt(len(m))
+
+
+def test_vmc_energy_agrees_with_oracle_chain():
+    s = make_system("vmc_water_10e", seed=1)
+    W, sweeps, warm, dt = 100, 220, 20, 0.09
+    ref = oracle_vmc(s, W, sweeps, dt, seed=7, warm=warm)
+    f = QMCB200Functions(s, W, run_params(dt=dt, seed=99))
+    f.init_walkers(s.initial_positions(W, seed=7))
+    N = s.n_electrons
+    f.run_steps(1, warm * N)
+    gpu = []
+    acc = 0.0
+    for k in range(sweeps - warm):
+        st = f.run_steps(1 + (warm + k) * N, N)
+        gpu.append(st.sum_weight_energy / st.sum_weight)
+        acc += st.sum_accept / st.n_moves
+    m1, e1 = block_stats(ref)
+    m2, e2 = block_stats(gpu)
+    z = abs(m1 - m2) / np.hypot(e1, e2)
+    assert z < 4.0, (m1, e1, m2, e2)
+    assert 0.2 < acc / (sweeps - warm) < 0.99
+
+
+def branch_restatement(w, slots, thr, fuse, seed, step):
+    """QMCRun::nonunitWeightBranching (QMcBeaver/src/QMCRun.cpp:740-814) over
+    the live list with the device's fusion draws."""
+    w = list(w)
+    keep = [True] * len(w)
+    pend = None
+    for i in range(len(w)):
+        if w[i] > thr or w[i] < 0.01:
+            if w[i] < 0.01:
+                keep[i] = False
+            continue
+        if w[i] < fuse:
+            if pend is None:
+                pend = i
+            else:
+                w1, w2 = w[pend], w[i]
+                w3 = w1 + w2
+                if uniform4(seed, slots[pend], step, 7)[0] < w1 / w3:
+                    w[pend] = w3
+                    keep[i] = False
+                else:
+                    w[i] = w3
+                    keep[pend] = False
+                pend = None
+    out = [w[i] for i in range(len(w)) if keep[i]]
+    adds = []
+    for j in range(len(out)):
+        if out[j] > thr:
+            out[j] = out[j] / 2
+            adds.append(out[j])
+    return out + adds
+
+
+def test_branching_matches_reference_rule():
+    s = make_system("vmc_water_10e", seed=1)
+    W = 3000
+    f = QMCB200Functions(s, 2 * W, run_params(run_type=QMCB_DMC, seed=4242))
+    f.init_walkers(s.initial_positions(W, seed=1))
+    rng = np.random.default_rng(3)
+    w = np.exp(rng.normal(0.0, 1.2, W))
+    w[rng.random(W) < 0.05] = 0.005
+    f.set_walker_weights(w)
+    n = f.branch(step=77)
+    expect = branch_restatement(w, list(range(W)), 2.0, 0.45, 4242, 77)
+    got = f.get_walkers()["weight"]
+    assert n == len(expect)
+    np.testing.assert_allclose(got, expect, rtol=0, atol=0)
+    assert abs(got.sum() - sum(expect)) < 1e-9
+
+
+def test_branching_copies_walker_state():
+    s = make_system("vmc_water_10e", seed=1)
+    W = 40
+    f = QMCB200Functions(s, 2 * W, run_params(run_type=QMCB_DMC))
+    f.init_walkers(s.initial_positions(W, seed=2))
+    w = np.ones(W)
+    w[3] = 3.0
+    f.set_walker_weights(w)
+    before = f.get_walkers()
+    n = f.branch(step=1)
+    after = f.get_walkers()
+    assert n == W + 1
+    np.testing.assert_array_equal(after["R"][-1], before["R"][3])
+    assert after["weight"][3] == after["weight"][-1] == 1.5
+    assert after["e_local"][-1] == before["e_local"][3]
+
+
+def test_dmc_population_stays_controlled():
+    s = make_system("dmc_6nuc_30e", seed=1)
+    W = 2048
+    p = run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
+                   dt=0.01, refresh_interval=50, reweight_start_step=0, seed=5)
+    f = QMCB200Functions(s, 4 * W, p)
+    R = s.initial_positions(W, seed=3)
+    f.init_walkers(R)
+    e0 = float(np.mean(f.get_walkers()["e_local"]))
+    p.energy_trial = p.energy_estimated = e0
+    f.set_params(p)
+    f.init_walkers(R)
+    st = f.run_steps(0, 30 * 10)
+    assert st.n_moves > 0.5 * 300 * W
+    assert 0.3 * W < st.n_walkers < 3 * W
+    assert np.isfinite(st.sum_weight_energy / st.sum_weight)
+    assert st.n_singular < 0.01 * st.n_moves

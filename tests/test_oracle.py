@@ -1,0 +1,84 @@
+"""The oracle (C restatement of the reference algorithm) against the golden
+vectors produced by the reference itself, and -- where the reference tree is
+present -- against the reference build call for call."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN_CASES, load_golden, replay
+from oracle.evaluators import OracleEvaluator, reference_available
+
+ORACLE_RTOL = 1e-12
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_oracle_reproduces_reference_golden(case):
+    s, d = load_golden(case)
+    ev = OracleEvaluator(s, qf_mod=int(d["qf_mod"]), dt=float(d["dt"]))
+    W = d["R"].shape[1]
+    ws = ev.new_walkers(W)
+
+    def run(e, R):
+        ev.evaluate(ws, R, e)
+        return ev.results(ws)
+
+    replay(run, d, ORACLE_RTOL, f"oracle/{case}")
+
+
+def test_golden_cases_present():
+    assert {"water_vmc", "dmc30_unequal", "dmc30_equal"} <= set(GOLDEN_CASES)
+
+
+def test_golden_sequences_cover_rollback_and_both_spins():
+    s, d = load_golden("dmc30_unequal")
+    e = d["whichE"]
+    assert e[0] == -1
+    assert (e[1:] < s.n_alpha).any() and (e[1:] >= s.n_alpha).any()
+    # a rollback call repeats the electron of the call before it
+    assert any(e[i] == e[i - 1] for i in range(2, len(e)))
+
+
+_CHILD = r"""
+import sys, numpy as np
+sys.path.insert(0, {root!r})
+from qmcbeaver_b200.system import make_random_molecule
+from oracle.evaluators import OracleEvaluator, ReferenceEvaluator
+s = make_random_molecule({ne}, {nn}, {nb}, 5.0, (1, 6, 7, 8), seed={seed})
+qf, dt = {qf}, 0.02
+ref = ReferenceEvaluator(s, qf_mod=qf, dt=dt); orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
+W = 5
+R = s.initial_positions(W, seed=3)
+wr, wo = ref.new_walkers(W), orc.new_walkers(W)
+rng = np.random.default_rng(9)
+worst = 0.0
+for step in range(-1, 2 * s.n_electrons):
+    e = -1 if step < 0 else step % s.n_electrons
+    if e >= 0:
+        R[:, e] += 0.2 * rng.standard_normal((W, 3))
+    ref.evaluate(wr, R, e); orc.evaluate(wo, R, e)
+    a, b = ref.results(wr), orc.results(wo)
+    for k in ("e_local", "lap", "potential", "log_abs_psi"):
+        worst = max(worst, float(np.max(np.abs(a[k] - b[k]) / np.maximum(np.abs(a[k]), 1.0))))
+    for k in ("grad", "mod_grad"):
+        worst = max(worst, float(np.max(np.abs(a[k] - b[k]) / np.maximum(np.abs(a[k]), 1.0))))
+    assert np.array_equal(a["sign"], b["sign"])
+print("WORST", worst)
+"""
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference tree / build not present")
+# n_alpha == n_beta with every orbital row occupied: the reference's one-electron
+# path copies derivative rows with the full orbital-row width
+# (QMcBeaver/src/QMCWalkerData.cpp:80-93, QMcBeaver/include/Array2D.h:986), so it
+# reads past its rows whenever the beta spin occupies fewer orbitals.
+@pytest.mark.parametrize("ne,nn,nb,seed,qf", [(6, 2, 16, 3, 0), (10, 3, 30, 4, 2), (14, 4, 40, 5, 1)])
+def test_oracle_matches_reference_call_for_call(ne, nn, nb, seed, qf):
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = _CHILD.format(root=root, ne=ne, nn=nn, nb=nb, seed=seed, qf=qf)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    worst = float([l for l in r.stdout.splitlines() if l.startswith("WORST")][0].split()[1])
+    assert worst < 1e-11, worst

@@ -1,0 +1,109 @@
+"""Per-call parity of the CUDA path (through the C ABI) with the reference:
+golden vectors recorded from the reference itself, and the oracle on fresh
+seeded configurations.  Plain FP64 path: 1e-10 relative."""
+import numpy as np
+import pytest
+
+from helpers import GOLDEN_CASES, PARITY_RTOL, compare, load_golden, replay
+from qmcbeaver_b200.api import QMCB200Functions
+from qmcbeaver_b200.system import make_random_molecule, make_system
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_gpu_reproduces_reference_golden(case):
+    s, d = load_golden(case)
+    W = d["R"].shape[1]
+    f = QMCB200Functions(s, W, qf_modification=int(d["qf_mod"]), dt=float(d["dt"]))
+    slots = np.arange(W)
+    replay(lambda e, R: f.evaluate(slots, R, e), d, PARITY_RTOL, f"gpu/{case}")
+    f.close()
+
+
+def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0):
+    from oracle.evaluators import OracleEvaluator
+    orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
+    f = QMCB200Functions(s, W + slots_offset, qf_modification=qf, dt=dt)
+    slots = np.arange(W) + slots_offset
+    ws = orc.new_walkers(W)
+    R = s.initial_positions(W, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    N = s.n_electrons
+    calls = [(-1, None)] + [(m % N, None) for m in range(sweeps * N)]
+    for i, (e, _) in enumerate(calls):
+        if e >= 0:
+            R[:, e] += sigma * rng.standard_normal((W, 3))
+        orc.evaluate(ws, R, e)
+        ref = orc.results(ws)
+        out = f.evaluate(slots, R, e)
+        compare(out, ref, PARITY_RTOL, f"{s.name} call {i} whichE={e}")
+    f.close()
+
+
+@pytest.mark.parametrize("wl,W,qf,dt,sweeps", [("vmc_water_10e", 100, 0, 0.09, 3),
+                                              ("dmc_6nuc_30e", 64, 2, 0.01, 2),
+                                              ("dmc_6nuc_30e", 16, 1, 0.01, 1)])
+def test_gpu_matches_oracle_workloads(wl, W, qf, dt, sweeps):
+    _oracle_sequence(make_system(wl, seed=3), W, qf, dt, sweeps, 0.2, seed=21, slots_offset=5)
+
+
+def test_gpu_matches_oracle_100_electrons():
+    # the 100-electron / 400-function system in FP64
+    s = make_system("mixed_20nuc_100e", seed=2)
+    _oracle_sequence(s, 4, 2, 0.01, 1, 0.1, seed=5)
+
+
+@pytest.mark.parametrize("ne,nn,nb,seed", [(2, 1, 5, 1), (4, 2, 12, 2), (7, 2, 20, 3), (70, 8, 160, 4)])
+def test_gpu_matches_oracle_shapes(ne, nn, nb, seed):
+    # odd electron counts (n_alpha != n_beta), one-electron spins, n > 32
+    s = make_random_molecule(ne, nn, nb, 5.0, (1, 6, 7, 8), seed=seed)
+    _oracle_sequence(s, 6, 2, 0.02, 1, 0.2, seed=seed)
+
+
+def test_sherman_morrison_consistent_with_full_refresh():
+    # after many single-electron updates the stored state equals a fresh full
+    # evaluation at the same positions (no periodic refresh in between)
+    s = make_system("dmc_6nuc_30e", seed=4)
+    W = 512
+    f = QMCB200Functions(s, 2 * W, qf_modification=2, dt=0.01)
+    R = s.initial_positions(W, seed=8)
+    a = np.arange(W)
+    f.evaluate(a, R, -1)
+    rng = np.random.default_rng(4)
+    for m in range(3 * s.n_electrons):
+        e = m % s.n_electrons
+        R[:, e] += 0.15 * rng.standard_normal((W, 3))
+        last = f.evaluate(a, R, e)
+    fresh = f.evaluate(a + W, R, -1)
+    ok = (last["status"] == 0) & (fresh["status"] == 0)
+    assert ok.mean() > 0.95
+    for k in ("e_local", "log_abs_psi"):
+        err = np.abs(last[k][ok] - fresh[k][ok]) / np.maximum(np.abs(fresh[k][ok]), 1.0)
+        assert np.max(err) < 1e-8, (k, np.max(err))
+    g = np.max(np.abs(last["grad"][ok] - fresh["grad"][ok]) / np.maximum(np.abs(fresh["grad"][ok]), 1.0))
+    assert g < 1e-7
+
+
+def test_copy_slot_clones_state():
+    s = make_system("vmc_water_10e", seed=1)
+    f = QMCB200Functions(s, 8)
+    R = s.initial_positions(2, seed=2)
+    f.evaluate([0, 1], R, -1)
+    f.copy_slot(0, 5)
+    R2 = R.copy()
+    R2[:, 3] += 0.1
+    a = f.evaluate([0], R2[:1], 3)
+    b = f.evaluate([5], R2[:1], 3)
+    for k in ("log_abs_psi", "e_local", "grad"):
+        np.testing.assert_array_equal(a[k], b[k])
+
+
+def test_one_electron_update_needs_full_evaluation_first():
+    from qmcbeaver_b200.api import QMCBError
+    s = make_system("vmc_water_10e", seed=1)
+    f = QMCB200Functions(s, 4)
+    with pytest.raises(QMCBError, match="before any full evaluation"):
+        f.evaluate([0], s.initial_positions(1), 2)
+    with pytest.raises(QMCBError, match="slot out of range"):
+        f.evaluate([9], s.initial_positions(1), -1)
