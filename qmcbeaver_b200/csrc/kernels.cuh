@@ -714,6 +714,9 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
           w *= 0.9;
         else
           w *= dW;
+        // a non-finite weight (NaN energy or exp overflow) removes the walker
+        // at the next branching instead of poisoning the ensemble sums
+        if (!isfinite(w)) w = 0.0;
       }
       double Eobs = p * (bad ? 0.0 : EL) + (1.0 - p) * sc[SC_EL];
       if (lane == 0 && w > 0.0) {

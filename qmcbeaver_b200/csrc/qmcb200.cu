@@ -22,7 +22,7 @@ using namespace qmcb;
 
 namespace {
 
-const int kWarpsPerBlock = 4;
+const int kMaxWarpsPerBlock = 4;
 
 std::string g_create_error;
 
@@ -55,6 +55,7 @@ struct qmcb_handle {
   int n_live_host = 0;
   double target_weight = 0.0;
   size_t smem_move = 0, smem_full = 0;
+  int wpb_move = 1, wpb_full = 1;  // warps (walkers) per CTA of k_move / k_full
   bool evaluated_once = false;
   // kernel timing (qmcb_set_profiling)
   bool prof = false;
@@ -343,14 +344,18 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(cudaMalloc(&h->d_out, sizeof(double) * (size_t)max_walkers * (6 * h->N + 8)));
   CKC(cudaMalloc(&h->d_status, max_walkers));
 
-  h->smem_move = sizeof(double) * (size_t)kWarpsPerBlock * move_scratch_doubles(h->N, K, h->nmax);
-  h->smem_full = sizeof(double) * (size_t)kWarpsPerBlock * full_scratch_doubles(h->N, K, h->nmax);
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-  if ((int)h->smem_move > max_optin || (int)h->smem_full > max_optin) {
+  const size_t per_move = sizeof(double) * (size_t)move_scratch_doubles(h->N, K, h->nmax);
+  const size_t per_full = sizeof(double) * (size_t)full_scratch_doubles(h->N, K, h->nmax);
+  if (per_move > (size_t)max_optin || per_full > (size_t)max_optin) {
     qmcb_destroy(h);
     return fail(nullptr, QMCB_E_LIMIT, "qmcb_create: system too large for the per-walker shared-memory scratch");
   }
+  h->wpb_move = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_move);
+  h->wpb_full = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_full);
+  h->smem_move = per_move * h->wpb_move;
+  h->smem_full = per_full * h->wpb_full;
   CKC(cudaFuncSetAttribute(k_move<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
   CKC(cudaFuncSetAttribute(k_move<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
   CKC(cudaFuncSetAttribute(k_full, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_full));
@@ -420,13 +425,14 @@ static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num,
                        cudaStream_t st)
 {
   RunCfg cfg = make_cfg(h->params);
-  int blocks = (num + kWarpsPerBlock - 1) / kWarpsPerBlock;
   if (which_e < 0) {
-    k_full<<<blocks, 32 * kWarpsPerBlock, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
+    int blocks = (num + h->wpb_full - 1) / h->wpb_full;
+    k_full<<<blocks, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
                                                               nullptr, d_R, 1, o);
   } else {
     MoveArgs mv{which_e, 0, 0, 0};
-    k_move<false><<<blocks, 32 * kWarpsPerBlock, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
+    int blocks = (num + h->wpb_move - 1) / h->wpb_move;
+    k_move<false><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
                                                                      num, nullptr, d_R, mv, h->d_ectl,
                                                                      h->d_stats, o);
   }
@@ -522,13 +528,14 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
 {
   if (!h) return QMCB_E_ARG;
   if (n_steps < 0 || first_step < 0) return fail(h, QMCB_E_ARG, "qmcb_run_steps: bad step range");
-  if (!h->evaluated_once || h->n_live_host <= 0)
-    return fail(h, QMCB_E_STATE, "qmcb_run_steps: call qmcb_init_walkers first");
+  if (!h->evaluated_once) return fail(h, QMCB_E_STATE, "qmcb_run_steps: call qmcb_init_walkers first");
+  if (h->n_live_host <= 0) return fail(h, QMCB_E_STATE, "qmcb_run_steps: no live walkers (population died out)");
   cudaStream_t st = h->stream;
   RunCfg cfg = make_cfg(h->params);
   // per-call sums; the running E_est sums persist across calls
   CK(cudaMemsetAsync(h->d_stats, 0, sizeof(double) * ST_RUN_SUM_W, st));
-  const int blocks = (h->max_walkers + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const int blocks = (h->max_walkers + h->wpb_move - 1) / h->wpb_move;
+  const int blocks_full = (h->max_walkers + h->wpb_full - 1) / h->wpb_full;
   const bool dmc = h->params.run_type == QMCB_DMC;
   for (int s = 0; s < n_steps; s++) {
     int step = first_step + s;
@@ -540,7 +547,7 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
     EvalOut o{};
     {
       ProfScope ps(h, QMCB_KERNEL_MOVE, st);
-      k_move<true><<<blocks, 32 * kWarpsPerBlock, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live,
+      k_move<true><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live,
                                                                       0, h->d_ctl, nullptr, mv, h->d_ectl,
                                                                       h->d_stats, o);
       ps.end(st);
@@ -567,7 +574,7 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
     if (h->params.refresh_interval > 0 && (step + 1) % h->params.refresh_interval == 0) {
       EvalOut o2{};
       ProfScope ps(h, QMCB_KERNEL_REFRESH, st);
-      k_full<<<blocks, 32 * kWarpsPerBlock, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live, 0,
+      k_full<<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live, 0,
                                                                 h->d_ctl, nullptr, 0, o2);
       ps.end(st);
     }

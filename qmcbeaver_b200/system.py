@@ -446,6 +446,97 @@ def _random_mo(rng: np.random.Generator, K: int, n: int) -> np.ndarray:
     return np.ascontiguousarray(Q[:, :n].T)  # orbital rows
 
 
+def _overlap_1d_table(imax: int, jmax: int, a, b, A, B) -> np.ndarray:
+    """Obara-Saika table of 1D overlaps <(x-A)^i e^{-a(x-A)^2} | (x-B)^j e^{-b(x-B)^2}>
+    for i <= imax, j <= jmax (Obara & Saika, J. Chem. Phys. 84, 3963 (1986)),
+    vectorised over arrays of exponent / centre pairs."""
+    p = a + b
+    P = (a * A + b * B) / p
+    XPA, XPB = P - A, P - B
+    S = np.zeros(np.broadcast(a, b, A, B).shape + (imax + 1, jmax + 1))
+    S[..., 0, 0] = np.sqrt(np.pi / p) * np.exp(-a * b / p * (A - B) ** 2)
+    o = 1.0 / (2.0 * p)
+    for i in range(imax + 1):
+        for j in range(jmax + 1):
+            if i == 0 and j == 0:
+                continue
+            if i > 0:
+                v = XPA * S[..., i - 1, j]
+                if i > 1:
+                    v = v + (i - 1) * o * S[..., i - 2, j]
+                if j > 0:
+                    v = v + j * o * S[..., i - 1, j - 1]
+            else:
+                v = XPB * S[..., i, j - 1]
+                if j > 1:
+                    v = v + (j - 1) * o * S[..., i, j - 2]
+            S[..., i, j] = v
+    return S
+
+
+def core_hamiltonian_orbitals(s: "MolecularSystem", n: int, block: int = 256) -> np.ndarray:
+    """Lowest n orbitals of an approximate core Hamiltonian in the system's
+    basis: exact overlap S and kinetic T (Obara-Saika), nuclear attraction in
+    the Mulliken approximation V_ab = S_ab (v_a + v_b) / 2 with v_a = -sum_C
+    Z_C <1/r_C>_a (own centre: the radial expectation of the contraction;
+    other centres: the point value 1/R).  Solves T + V = S C e.
+    Returns the orbital rows (n, K)."""
+    atom, pw, nprim, off, ex, co = s.flat_basis()
+    K = len(atom)
+    pf = np.repeat(np.arange(K), nprim)
+    Pn = len(ex)
+    Ac = s.coords[atom[pf]]
+    pa = pw[pf]
+    S = np.zeros((K, K))
+    T = np.zeros((K, K))
+    jj_all = np.arange(Pn)
+    for r0 in range(0, Pn, block):
+        ii = np.arange(r0, min(Pn, r0 + block))[:, None]
+        jj = jj_all[None, :]
+        a, b = np.broadcast_arrays(ex[ii], ex[jj])
+        Sd, Td = [], []
+        for d in range(3):
+            tab = _overlap_1d_table(2 if pa[:, d].max() <= 2 else pa[:, d].max(), pa[:, d].max() + 2,
+                                    a, b, Ac[ii, d], Ac[jj, d])
+            i_ = np.broadcast_to(pa[ii, d], a.shape)
+            j_ = np.broadcast_to(pa[jj, d], a.shape)
+            row = np.take_along_axis(tab, i_[..., None, None], -2)[..., 0, :]
+            s0 = np.take_along_axis(row, j_[..., None], -1)[..., 0]
+            sp2 = np.take_along_axis(row, (j_ + 2)[..., None], -1)[..., 0]
+            sm2 = np.take_along_axis(row, np.maximum(j_ - 2, 0)[..., None], -1)[..., 0]
+            t = -2.0 * b * b * sp2 + b * (2 * j_ + 1) * s0 - 0.5 * j_ * (j_ - 1) * np.where(j_ >= 2, sm2, 0.0)
+            Sd.append(s0)
+            Td.append(t)
+        cc = co[ii] * co[jj]
+        sp = cc * Sd[0] * Sd[1] * Sd[2]
+        tp = cc * (Td[0] * Sd[1] * Sd[2] + Sd[0] * Td[1] * Sd[2] + Sd[0] * Sd[1] * Td[2])
+        fi = np.broadcast_to(pf[ii], a.shape)
+        fj = np.broadcast_to(pf[jj], a.shape)
+        np.add.at(S, (fi, fj), sp)
+        np.add.at(T, (fi, fj), tp)
+    v = np.zeros(K)
+    for k in range(K):
+        L = int(pw[k].sum())
+        sl = slice(off[k], off[k] + nprim[k])
+        e_, c_ = ex[sl], co[sl]
+        pij = e_[:, None] + e_[None, :]
+        cij = c_[:, None] * c_[None, :]
+        num = np.sum(cij * math.gamma(L + 1) / (2 * pij ** (L + 1)))
+        den = np.sum(cij * math.gamma(L + 1.5) / (2 * pij ** (L + 1.5)))
+        for C in range(s.n_nuclei):
+            if C == atom[k]:
+                v[k] -= s.Z[C] * num / den
+            else:
+                v[k] -= s.Z[C] / np.linalg.norm(s.coords[C] - s.coords[atom[k]])
+    H = T + 0.5 * S * (v[:, None] + v[None, :])
+    w, U = np.linalg.eigh(S)
+    keep = w > 1e-8 * w.max()
+    X = U[:, keep] / np.sqrt(w[keep])
+    _, Cp = np.linalg.eigh(X.T @ H @ X)
+    C = X @ Cp
+    return np.ascontiguousarray(C[:, :n].T)
+
+
 def _jastrows(labels: Sequence[str], Z: Sequence[float]):
     ee_anti = Pade.fixed_cusp(0.5, 1.0)
     ee_para = Pade.fixed_cusp(0.25, 1.0)
@@ -453,7 +544,7 @@ def _jastrows(labels: Sequence[str], Z: Sequence[float]):
     return ee_anti, ee_para, en
 
 
-def _assemble(name, Zs, coords, basis, n_alpha, n_beta, rng, jastrow=True) -> MolecularSystem:
+def _assemble(name, Zs, coords, basis, n_alpha, n_beta, rng, jastrow=True, orbitals="random") -> MolecularSystem:
     labels = [ELEMENT[int(z)] for z in Zs]
     K = sum(len(b) for b in basis)
     n_orb = max(n_alpha, n_beta)
@@ -469,6 +560,8 @@ def _assemble(name, Zs, coords, basis, n_alpha, n_beta, rng, jastrow=True) -> Mo
         alpha_occ=np.arange(n_alpha), beta_occ=np.arange(n_beta),
         ee_anti=ee_anti, ee_para_up=ee_para, ee_para_dn=ee_para,
         en_up=dict(en), en_dn=dict(en), name=name)
+    if orbitals == "core":
+        sysm.mo = core_hamiltonian_orbitals(sysm, n_orb)
     sysm.check_exponent_cache()
     return sysm
 
@@ -492,11 +585,14 @@ def make_water_like(seed: int = 1, jastrow: bool = True) -> MolecularSystem:
 
 def make_random_molecule(n_elec: int, n_nuclei: int, n_basis: int, box: float, z_choices: Sequence[int],
                          seed: int = 1, min_sep: float = 1.8, jastrow: bool = True,
-                         name: Optional[str] = None) -> MolecularSystem:
+                         name: Optional[str] = None, orbitals: str = "core") -> MolecularSystem:
     """Synthetic molecule: nuclei uniform in a cube (minimum separation),
     Z drawn from z_choices (the draw whose total charge is closest to the
     electron count is kept), n_elec/2 up and n_elec/2 down electrons,
-    n_basis contracted Cartesian Gaussians with 3 primitives each."""
+    n_basis contracted Cartesian Gaussians with 3 primitives each.
+    orbitals = "core": lowest orbitals of the approximate core Hamiltonian
+    (a trial function whose local energy is tame enough for DMC population
+    control); "random": QR-orthonormalised Gaussian coefficients."""
     rng = np.random.default_rng(seed)
     best = None
     for _ in range(256):
@@ -512,7 +608,7 @@ def make_random_molecule(n_elec: int, n_nuclei: int, n_basis: int, box: float, z
     na = n_elec - n_elec // 2
     nb = n_elec // 2
     return _assemble(name or f"synthetic ({n_nuclei} nuclei, {n_elec} e, {n_basis} bf)",
-                     Zs, coords, basis, na, nb, rng, jastrow)
+                     Zs, coords, basis, na, nb, rng, jastrow, orbitals)
 
 
 # The benchmark / parity workloads, named by what they are.

@@ -26,9 +26,12 @@ def rel_err(a, b, floor=1.0):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))) if a.size else 0.0
 
 
-def compare(out, ref, rtol, label=""):
-    """Checks one evaluate call's outputs against reference outputs."""
+def compare(out, ref, rtol, label="", mask=None):
+    """Checks one evaluate call's outputs against reference outputs (walkers
+    in `mask`, default all non-singular ones)."""
     ok = ref["singular"] == 0 if "singular" in ref else np.ones(len(ref["e_local"]), bool)
+    if mask is not None:
+        ok = ok & mask
     msgs = []
     for k, floor in (("e_local", 1.0), ("lap", 1.0), ("potential", 1.0)):
         e = rel_err(out[k][ok], ref[k][ok], floor)
@@ -56,3 +59,19 @@ def replay(ev_eval, d, rtol, label):
         ref = {k: d[k][i] for k in ("log_abs_psi", "sign", "grad", "mod_grad", "lap", "e_local", "potential",
                                      "singular")}
         compare(out, ref, rtol, f"{label} call {i} whichE={e}")
+
+
+# Rounding differences between two FP64 implementations grow with the
+# condition number of the Slater matrix carried through Sherman-Morrison
+# updates; the 1e-10 bar applies to walkers whose matrices stayed below this
+# condition number (a walker that once exceeded it stays excluded).
+COND_LIMIT = 1e5
+
+
+def slater_conditions(orc, walkers, system):
+    c = np.zeros(len(walkers))
+    for i, w in enumerate(walkers):
+        for beta, n in ((0, system.n_alpha), (1, system.n_beta)):
+            if n > 0:
+                c[i] = max(c[i], np.linalg.cond(orc.inverse(w, beta)))
+    return c

@@ -4,7 +4,7 @@ seeded configurations.  Plain FP64 path: 1e-10 relative."""
 import numpy as np
 import pytest
 
-from helpers import GOLDEN_CASES, PARITY_RTOL, compare, load_golden, replay
+from helpers import COND_LIMIT, GOLDEN_CASES, PARITY_RTOL, compare, load_golden, replay, slater_conditions
 from qmcbeaver_b200.api import QMCB200Functions
 from qmcbeaver_b200.system import make_random_molecule, make_system
 
@@ -31,14 +31,18 @@ def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0):
     rng = np.random.default_rng(seed + 1)
     N = s.n_electrons
     calls = [(-1, None)] + [(m % N, None) for m in range(sweeps * N)]
+    good = np.ones(W, bool)
     for i, (e, _) in enumerate(calls):
         if e >= 0:
             R[:, e] += sigma * rng.standard_normal((W, 3))
         orc.evaluate(ws, R, e)
         ref = orc.results(ws)
+        good &= slater_conditions(orc, ws, s) < COND_LIMIT
         out = f.evaluate(slots, R, e)
-        compare(out, ref, PARITY_RTOL, f"{s.name} call {i} whichE={e}")
+        compare(out, ref, PARITY_RTOL, f"{s.name} call {i} whichE={e}", mask=good)
     f.close()
+    assert good.mean() >= 0.5, f"only {good.sum()} of {W} walkers stayed well conditioned"
+    return good.mean()
 
 
 @pytest.mark.parametrize("wl,W,qf,dt,sweeps", [("vmc_water_10e", 100, 0, 0.09, 3),
