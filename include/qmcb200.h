@@ -115,6 +115,9 @@ typedef struct qmcb_run_params {
   double population_control; /* population_control_parameter (E_T feedback) */
   int target_walkers;        /* W0 of updateTrialEnergy; 0 = walkers at init */
   int reweight_start_step;   /* steps below this keep dW = 1 (QMCWalker.cpp:1071) */
+  double energy_original;    /* energy_estimated_original (input energy); 0 = energy_estimated */
+  double rel_cutoff;         /* observables with |E - E_orig| / |E_orig| >= rel_cutoff are left out */
+  int limit_branching;       /* QMCWalker::branchRecommended rules on splits (QMCWalker.cpp) */
 } qmcb_run_params;
 
 /* Ensemble sums over one call of qmcb_run_steps (for E_est / E_T and error bars). */

@@ -40,6 +40,7 @@ enum Sc {
   SC_STATUS,       // QMCB_ST_* bits
   SC_MODRATIO,     // |modified grad| / |grad|
   SC_AGE_MOVED,    // age when the walker last moved
+  SC_DW,           // weight factor of the last reweight
   SC_COUNT
 };
 constexpr int kScalars = 24;  // padded
@@ -73,9 +74,10 @@ struct Layout {
 };
 
 struct RunCfg {
-  int run_type, sampling, qf_mod, emod, reweighting, old_walker_acceptance;
+  int run_type, sampling, qf_mod, emod, reweighting, old_walker_acceptance, limit_branching;
   double qf_a, dt, dt_eff;
   double branching_threshold, fusion_threshold;
+  double e_orig, rel_cutoff;
   uint64_t seed;
 };
 

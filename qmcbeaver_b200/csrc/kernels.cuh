@@ -37,6 +37,7 @@ enum StatIdx {
   ST_SINGULAR,
   ST_RUN_SUM_W,   // running sums for E_est (kept across calls)
   ST_RUN_SUM_WE,
+  ST_RUN_COUNT,   // samples in the running sums
   ST_COUNT
 };
 
@@ -407,6 +408,7 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
       sc[SC_WEIGHT] = 1.0;
       sc[SC_AGE] = 0.0;
       sc[SC_AGE_MOVED] = 0.0;
+      sc[SC_DW] = 1.0;
     }
     if (out.log_abs_psi) out.log_abs_psi[wi] = sc[SC_LOGDET_A] + sc[SC_LOGDET_B] + U;
     if (out.sign) out.sign[wi] = sc[SC_SIGN_A] * sc[SC_SIGN_B];
@@ -714,17 +716,21 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
           w *= 0.9;
         else
           w *= dW;
+        if (lane == 0) sc[SC_DW] = dW;
         // a non-finite weight (NaN energy or exp overflow) removes the walker
         // at the next branching instead of poisoning the ensemble sums
         if (!isfinite(w)) w = 0.0;
       }
       double Eobs = p * (bad ? 0.0 : EL) + (1.0 - p) * sc[SC_EL];
-      if (lane == 0 && w > 0.0) {
+      // rel_cutoff filter of QMCWalker::calculateObservables (QMcBeaver/src/QMCWalker.cpp:2336-2351)
+      const bool in_avg = fabs((Eobs - cfg.e_orig) / cfg.e_orig) < cfg.rel_cutoff;
+      if (lane == 0 && w > 0.0 && in_avg) {
         atomicAdd(&stats[ST_SUM_W], w);
         atomicAdd(&stats[ST_SUM_WE], w * Eobs);
         atomicAdd(&stats[ST_SUM_WE2], w * Eobs * Eobs);
         atomicAdd(&stats[ST_RUN_SUM_W], w);
         atomicAdd(&stats[ST_RUN_SUM_WE], w * Eobs);
+        atomicAdd(&stats[ST_RUN_COUNT], 1.0);
       }
     }
     if (lane == 0) {
@@ -808,9 +814,29 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
 // w1 / (w1 + w2) for the first).  Dead slots go on the free stack; copies
 // take slots from it and are written to the copy list for k_copy.
 // ctl: [0] n_live, [1] n_free, [2] n_copies.
+// QMCWalker::branchRecommended (limit_branching): no split for a walker that
+// has not moved for more than 4 steps, whose weight grows too fast
+// (dW^(age+1) > 5), that is heavy (> 100) and still growing (> 1.5), or whose
+// local energy is more than 100x off the input energy.
+__device__ __forceinline__ bool branch_recommended(const double *sc, double e_orig, int limit)
+{
+  if (!limit) return true;
+  const double age = sc[SC_AGE], W = sc[SC_WEIGHT], dW = sc[SC_DW];
+  const double growth = pow(dW, age + 1.0);
+  bool ok = true;
+  if (age > 4.0) ok = false;
+  if (growth > 5.0)
+    ok = false;
+  else if (W > 100.0 && growth > 1.5)
+    ok = false;
+  if (fabs((sc[SC_EL] - e_orig) / e_orig) > 100.0) ok = false;
+  return ok;
+}
+
 __global__ void __launch_bounds__(1024) k_branch(double *state, Layout L, int *live, int *live_tmp, int *free_stack,
                                                  int *ctl, int2 *copies, double thr_split, double thr_fuse,
-                                                 uint64_t seed, int step, double *stats)
+                                                 uint64_t seed, int step, double *stats, double e_orig,
+                                                 int limit_branching)
 {
   __shared__ int s_warp[32];
   __shared__ int s_base[4];
@@ -914,7 +940,8 @@ __global__ void __launch_bounds__(1024) k_branch(double *state, Layout L, int *l
     int slot = i < n_keep ? live_tmp[i] : -1;
     double *wp = slot >= 0 ? &state[(size_t)slot * L.stride + L.sc + SC_WEIGHT] : nullptr;
     double w = wp ? *wp : 0.0;
-    int sp = (slot >= 0 && w > thr_split) ? 1 : 0;
+    int sp = (slot >= 0 && w > thr_split &&
+              branch_recommended(state + (size_t)slot * L.stride + L.sc, e_orig, limit_branching)) ? 1 : 0;
     unsigned bs = __ballot_sync(QMCB_FULL_MASK, sp);
     int ps = __popc(bs & ((1u << lane) - 1));
     if (lane == 31) s_warp[wid] = ps + sp;
@@ -983,7 +1010,9 @@ __global__ void k_energy(EnergyCtl *ectl, const double *stats, int min_samples_o
 {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double sw = stats[ST_RUN_SUM_W];
-  if (min_samples_ok && sw > 0.0) ectl->e_est = stats[ST_RUN_SUM_WE] / sw;
+  // E_est follows the running average once it holds 100 samples
+  // (QMCManager::updateEstimatedEnergy, QMcBeaver/src/QMCManager.cpp:2247-2261)
+  if (min_samples_ok && sw > 0.0 && stats[ST_RUN_COUNT] >= 100.0) ectl->e_est = stats[ST_RUN_SUM_WE] / sw;
   double ratio = stats[ST_FINAL_W] / ectl->target_weight;
   double lr = ratio > 1e-250 ? log(ratio) : 0.0;
   ectl->e_trial = ectl->e_est - ectl->pop_control * lr;

@@ -139,6 +139,9 @@ static RunCfg make_cfg(const qmcb_run_params &p)
   c.branching_threshold = p.branching_threshold;
   c.fusion_threshold = p.fusion_threshold;
   c.seed = p.seed;
+  c.limit_branching = p.limit_branching;
+  c.e_orig = p.energy_original != 0.0 ? p.energy_original : (p.energy_estimated != 0.0 ? p.energy_estimated : -1.0);
+  c.rel_cutoff = p.rel_cutoff > 0 ? p.rel_cutoff : 1e300;
   return c;
 }
 
@@ -162,6 +165,9 @@ static void default_params(qmcb_run_params *p)
   p->population_control = 1.0;
   p->target_walkers = 0;
   p->reweight_start_step = 100;
+  p->energy_original = 0.0;
+  p->rel_cutoff = 100.0;
+  p->limit_branching = 1;
 }
 
 template <typename T>
@@ -557,7 +563,7 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
         ProfScope ps(h, QMCB_KERNEL_BRANCH, st);
         k_branch<<<1, 1024, 0, st>>>(h->d_state, h->lay, h->d_live, h->d_live_tmp, h->d_free, h->d_ctl,
                                      h->d_copies, h->params.branching_threshold, h->params.fusion_threshold,
-                                     h->params.seed, step, h->d_stats);
+                                     h->params.seed, step, h->d_stats, cfg.e_orig, cfg.limit_branching);
         ps.end(st);
       }
       {
@@ -644,9 +650,10 @@ int qmcb_branch(qmcb_handle *h, int step, int *n_live)
   if (!h) return QMCB_E_ARG;
   if (!h->evaluated_once || h->n_live_host <= 0) return fail(h, QMCB_E_STATE, "qmcb_branch: no live walkers");
   cudaStream_t st = h->stream;
+  RunCfg cfg = make_cfg(h->params);
   k_branch<<<1, 1024, 0, st>>>(h->d_state, h->lay, h->d_live, h->d_live_tmp, h->d_free, h->d_ctl, h->d_copies,
                                h->params.branching_threshold, h->params.fusion_threshold, h->params.seed, step,
-                               h->d_stats);
+                               h->d_stats, cfg.e_orig, cfg.limit_branching);
   k_copy<<<592, 256, 0, st>>>(h->d_state, h->lay, h->d_copies, h->d_ctl);
   CK(cudaGetLastError());
   int ctl[4];

@@ -41,7 +41,8 @@ class RunParams(C.Structure):
         ("branching_threshold", C.c_double), ("fusion_threshold", C.c_double),
         ("old_walker_acceptance", C.c_int), ("refresh_interval", C.c_int), ("precision", C.c_int),
         ("seed", C.c_uint64), ("population_control", C.c_double), ("target_walkers", C.c_int),
-        ("reweight_start_step", C.c_int),
+        ("reweight_start_step", C.c_int), ("energy_original", C.c_double), ("rel_cutoff", C.c_double),
+        ("limit_branching", C.c_int),
     ]
 
 
@@ -74,6 +75,9 @@ def run_params(**kw) -> RunParams:
     p.population_control = 1.0
     p.target_walkers = 0
     p.reweight_start_step = 100
+    p.energy_original = 0.0
+    p.rel_cutoff = 100.0
+    p.limit_branching = 1
     for k, v in kw.items():
         if not hasattr(p, k):
             raise AttributeError(k)

@@ -115,7 +115,7 @@ def branch_restatement(w, slots, thr, fuse, seed, step):
 def test_branching_matches_reference_rule():
     s = make_system("vmc_water_10e", seed=1)
     W = 3000
-    f = QMCB200Functions(s, 2 * W, run_params(run_type=QMCB_DMC, seed=4242))
+    f = QMCB200Functions(s, 2 * W, run_params(run_type=QMCB_DMC, seed=4242, limit_branching=0))
     f.init_walkers(s.initial_positions(W, seed=1))
     rng = np.random.default_rng(3)
     w = np.exp(rng.normal(0.0, 1.2, W))
@@ -132,7 +132,7 @@ def test_branching_matches_reference_rule():
 def test_branching_copies_walker_state():
     s = make_system("vmc_water_10e", seed=1)
     W = 40
-    f = QMCB200Functions(s, 2 * W, run_params(run_type=QMCB_DMC))
+    f = QMCB200Functions(s, 2 * W, run_params(run_type=QMCB_DMC, limit_branching=0))
     f.init_walkers(s.initial_positions(W, seed=2))
     w = np.ones(W)
     w[3] = 3.0
