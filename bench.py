@@ -114,12 +114,16 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dmc_params(seed: int, e0: float):
+def dmc_params(seed: int, e0: float, reweight_start: int = 0):
     from qmcbeaver_b200.desc import (QMCB_DMC, QMCB_EMOD_UMRIGAR93, QMCB_IMPORTANCE_SAMPLING,
                                      QMCB_QF_UMRIGAR93_UNEQUAL, run_params)
     return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
-                      energy_modification=QMCB_EMOD_UMRIGAR93, dt=0.01, refresh_interval=50, reweight_start_step=0,
-                      energy_trial=e0, energy_estimated=e0, seed=seed)
+                      energy_modification=QMCB_EMOD_UMRIGAR93, dt=0.01, refresh_interval=50,
+                      reweight_start_step=reweight_start, energy_trial=e0, energy_estimated=e0, energy_original=e0,
+                      seed=seed)
+
+
+EQUIL_SWEEPS = 5
 
 
 def cpu_reference_sample(system, walkers: int, steps: int, procs: int, e0: float):
@@ -199,12 +203,17 @@ def main():
     W = args.walkers
     N, n = system.n_electrons, system.n_alpha
     R0 = system.initial_positions(W, seed=1000 + rank)
-    f = QMCB200Functions(system, 2 * W, dmc_params(seed=77 + rank, e0=0.0))
+    # equilibration: drift-diffusion moves with the weights held at 1 (the
+    # reference keeps dW = 1 for its first 100 steps, QMcBeaver/src/QMCWalker.cpp:1071),
+    # then E_T = E_est = E_orig = the equilibrated mean local energy
+    eq_steps = EQUIL_SWEEPS * N
+    f = QMCB200Functions(system, 2 * W, dmc_params(seed=77 + rank, e0=-1.0, reweight_start=eq_steps))
     f.init_walkers(R0)
+    f.run_steps(0, eq_steps)
+    R_eq = f.get_walkers()["R"]
     e0 = float(np.mean(f.get_walkers()["e_local"]))
     f.set_params(dmc_params(seed=77 + rank, e0=e0))
-    f.init_walkers(R0)
-
+    f.init_walkers(R_eq)
     def barrier():
         if dist is not None:
             dist.barrier()
@@ -287,7 +296,7 @@ def main():
 
     # reference-facing evaluate (QMCFunctions::evaluate shape) with host buffers
     slots = np.arange(min(W, 4096), dtype=np.int32)
-    Rh = np.ascontiguousarray(R0[: len(slots)])
+    Rh = np.ascontiguousarray(R_eq[: len(slots)])
     f2 = QMCB200Functions(system, len(slots), dmc_params(seed=1, e0=e0))
     f2.evaluate(slots, Rh, -1)
     rng = np.random.default_rng(5)

@@ -62,7 +62,7 @@ def test_vmc_energy_agrees_with_oracle_chain():
     s = make_system("vmc_water_10e", seed=1)
     W, sweeps, warm, dt = 100, 220, 20, 0.09
     ref = oracle_vmc(s, W, sweeps, dt, seed=7, warm=warm)
-    f = QMCB200Functions(s, W, run_params(dt=dt, seed=99))
+    f = QMCB200Functions(s, W, run_params(dt=dt, seed=99, rel_cutoff=0.0))
     f.init_walkers(s.initial_positions(W, seed=7))
     N = s.n_electrons
     f.run_steps(1, warm * N)
@@ -149,17 +149,25 @@ def test_branching_copies_walker_state():
 def test_dmc_population_stays_controlled():
     s = make_system("dmc_6nuc_30e", seed=1)
     W = 2048
-    p = run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
-                   dt=0.01, refresh_interval=50, reweight_start_step=0, seed=5)
-    f = QMCB200Functions(s, 4 * W, p)
-    R = s.initial_positions(W, seed=3)
-    f.init_walkers(R)
-    e0 = float(np.mean(f.get_walkers()["e_local"]))
-    p.energy_trial = p.energy_estimated = e0
-    f.set_params(p)
-    f.init_walkers(R)
-    st = f.run_steps(0, 30 * 10)
-    assert st.n_moves > 0.5 * 300 * W
+    N = s.n_electrons
+    eq = 5 * N
+
+    def params(e0, start):
+        return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING,
+                          qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, energy_modification=1, dt=0.01,
+                          refresh_interval=50, reweight_start_step=start, energy_trial=e0, energy_estimated=e0,
+                          energy_original=e0, seed=5)
+
+    f = QMCB200Functions(s, 4 * W, params(-1.0, eq))
+    f.init_walkers(s.initial_positions(W, seed=3))
+    st = f.run_steps(0, eq)
+    assert st.n_walkers == W  # weights held at 1 while equilibrating
+    wk = f.get_walkers()
+    e0 = float(np.mean(wk["e_local"]))
+    f.set_params(params(e0, 0))
+    f.init_walkers(wk["R"])
+    st = f.run_steps(0, 10 * N)
+    assert st.n_moves > 0.5 * 10 * N * W
     assert 0.3 * W < st.n_walkers < 3 * W
     assert np.isfinite(st.sum_weight_energy / st.sum_weight)
     assert st.n_singular < 0.01 * st.n_moves
