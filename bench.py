@@ -76,7 +76,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -120,10 +120,13 @@ def dmc_params(seed: int, e0: float, reweight_start: int = 0):
     return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
                       energy_modification=QMCB_EMOD_UMRIGAR93, dt=0.01, refresh_interval=50,
                       reweight_start_step=reweight_start, energy_trial=e0, energy_estimated=e0, energy_original=e0,
-                      seed=seed)
+                      seed=seed, limit_branching=0)
 
 
 EQUIL_SWEEPS = 5
+# Equilibrated mean local energy of the 30-electron trial function (Hartree),
+# the reference's input `energy` (E_T start, observable cutoff centre).
+E_GUESS = -55.0
 
 
 def cpu_reference_sample(system, walkers: int, steps: int, procs: int, e0: float):
@@ -151,8 +154,8 @@ def run_reference_arm(args, rank: int):
         return
     # one short untimed warm-up run, then one bounded timed sample (~10 s of
     # CPU work on every host core); the reference's own timers give us/move
-    cpu_reference_sample(system, walkers=4, steps=30, procs=procs, e0=-150.0)
-    last = cpu_reference_sample(system, walkers=32, steps=1500, procs=procs, e0=-150.0)
+    cpu_reference_sample(system, walkers=4, steps=30, procs=procs, e0=E_GUESS)
+    last = cpu_reference_sample(system, walkers=32, steps=450, procs=procs, e0=E_GUESS)
     vals = [last["moves_per_s"]]
     v = float(np.mean(vals)) if vals else 0.0
     sample = (f"{procs} processes x {last['walkers']} walkers x {last['steps']} steps of the reference's "
@@ -169,7 +172,7 @@ def run_reference_arm(args, rank: int):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=600)
+    ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--warmup", type=int, default=60)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--walkers", type=int, default=DEFAULT_WALKERS)
@@ -330,7 +333,7 @@ def main():
         out["clocks"] = clocks
     f.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_reference_sample(system, walkers=32, steps=1500, procs=os.cpu_count() or 1, e0=e0)
+        r = cpu_reference_sample(system, walkers=32, steps=450, procs=os.cpu_count() or 1, e0=E_GUESS)
         if r is not None:
             out["cpu_baseline"] = {"value": r["moves_per_s"], "unit": "walker-moves/s", "cores": r["procs"],
                                    "kind": "reference",

@@ -26,7 +26,7 @@ RUN_FLAGS = {
     "dmc": {"run_type": "diffusion", "sampling_method": "importance_sampling",
             "QF_modification_type": "umrigar93_unequalelectrons", "energy_modification_type": "umrigar93",
             "walker_reweighting_method": "umrigar93_probability_weighted",
-            "branching_method": "nonunit_weight_branching"},
+            "branching_method": "nonunit_weight_branching", "limit_branching": 0},
     "vmc_drift": {"run_type": "variational", "sampling_method": "importance_sampling",
                   "QF_modification_type": "umrigar93_unequalelectrons"},
     "vmc": {"run_type": "variational", "sampling_method": "no_importance_sampling", "QF_modification_type": "none"},
@@ -38,7 +38,7 @@ def available() -> bool:
 
 
 def run_reference(system, mode: str, dt: float, walkers: int, steps: int, procs: int, energy: float = -1.0,
-                  timeout: float = 600.0) -> Dict[str, object]:
+                  timeout: float = 300.0) -> Dict[str, object]:
     """Returns aggregate walker-moves/s over `procs` concurrent processes."""
     if not available():
         raise FileNotFoundError(REF_EXE)
