@@ -115,12 +115,12 @@ class ClockSampler:
 
 
 def dmc_params(seed: int, e0: float, reweight_start: int = 0):
-    from qmcbeaver_b200.desc import (QMCB_DMC, QMCB_EMOD_UMRIGAR93, QMCB_IMPORTANCE_SAMPLING,
+    from qmcbeaver_b200.desc import (QMCB_DMC, QMCB_ECUT_BDJM_PUSH88, QMCB_EMOD_UMRIGAR93, QMCB_IMPORTANCE_SAMPLING,
                                      QMCB_QF_UMRIGAR93_UNEQUAL, run_params)
     return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
                       energy_modification=QMCB_EMOD_UMRIGAR93, dt=0.01, refresh_interval=50,
                       reweight_start_step=reweight_start, energy_trial=e0, energy_estimated=e0, energy_original=e0,
-                      seed=seed, limit_branching=0)
+                      seed=seed, energy_cutoff=QMCB_ECUT_BDJM_PUSH88, population_control=1.0 / 0.01)
 
 
 EQUIL_SWEEPS = 5
@@ -155,7 +155,7 @@ def run_reference_arm(args, rank: int):
     # one short untimed warm-up run, then one bounded timed sample (~10 s of
     # CPU work on every host core); the reference's own timers give us/move
     cpu_reference_sample(system, walkers=4, steps=30, procs=procs, e0=E_GUESS)
-    last = cpu_reference_sample(system, walkers=32, steps=450, procs=procs, e0=E_GUESS)
+    last = cpu_reference_sample(system, walkers=64, steps=1500, procs=procs, e0=E_GUESS)
     vals = [last["moves_per_s"]]
     v = float(np.mean(vals)) if vals else 0.0
     sample = (f"{procs} processes x {last['walkers']} walkers x {last['steps']} steps of the reference's "
@@ -285,6 +285,8 @@ def main():
         if st2.final_weight > 0:
             p.energy_estimated = e_est
             p.energy_trial = e_est - p.population_control * np.log(st2.final_weight / W)
+        elif st2.n_walkers > 0:
+            p.energy_trial = e_est
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if dist is not None:
@@ -333,7 +335,7 @@ def main():
         out["clocks"] = clocks
     f.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_reference_sample(system, walkers=32, steps=450, procs=os.cpu_count() or 1, e0=E_GUESS)
+        r = cpu_reference_sample(system, walkers=64, steps=1500, procs=os.cpu_count() or 1, e0=E_GUESS)
         if r is not None:
             out["cpu_baseline"] = {"value": r["moves_per_s"], "unit": "walker-moves/s", "cores": r["procs"],
                                    "kind": "reference",

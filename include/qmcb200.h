@@ -118,7 +118,13 @@ typedef struct qmcb_run_params {
   double energy_original;    /* energy_estimated_original (input energy); 0 = energy_estimated */
   double rel_cutoff;         /* observables with |E - E_orig| / |E_orig| >= rel_cutoff are left out */
   int limit_branching;       /* QMCWalker::branchRecommended rules on splits (QMCWalker.cpp) */
+  int energy_cutoff;         /* QMCB_ECUT_*: local energy used in the reweighting exponent */
 } qmcb_run_params;
+
+/* energy_cutoff_type (QMCWalkerData::getModifiedLocalEnergy, QMcBeaver/src/QMCWalkerData.cpp:163-205) */
+#define QMCB_ECUT_NONE 0
+#define QMCB_ECUT_UMRIGAR93 1    /* E_L * |modified drift| / |drift| */
+#define QMCB_ECUT_BDJM_PUSH88 2  /* E_L clamped to E_orig +- 2 / sqrt(dt) */
 
 /* Ensemble sums over one call of qmcb_run_steps (for E_est / E_T and error bars). */
 typedef struct qmcb_step_stats {

@@ -26,7 +26,7 @@ RUN_FLAGS = {
     "dmc": {"run_type": "diffusion", "sampling_method": "importance_sampling",
             "QF_modification_type": "umrigar93_unequalelectrons", "energy_modification_type": "umrigar93",
             "walker_reweighting_method": "umrigar93_probability_weighted",
-            "branching_method": "nonunit_weight_branching", "limit_branching": 0},
+            "branching_method": "nonunit_weight_branching", "population_control_parameter": 100.0},
     "vmc_drift": {"run_type": "variational", "sampling_method": "importance_sampling",
                   "QF_modification_type": "umrigar93_unequalelectrons"},
     "vmc": {"run_type": "variational", "sampling_method": "no_importance_sampling", "QF_modification_type": "none"},

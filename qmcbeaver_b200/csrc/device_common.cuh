@@ -74,7 +74,7 @@ struct Layout {
 };
 
 struct RunCfg {
-  int run_type, sampling, qf_mod, emod, reweighting, old_walker_acceptance, limit_branching;
+  int run_type, sampling, qf_mod, emod, reweighting, old_walker_acceptance, limit_branching, ecut;
   double qf_a, dt, dt_eff;
   double branching_threshold, fusion_threshold;
   double e_orig, rel_cutoff;

@@ -691,8 +691,18 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
     if (mv.do_reweight) {
       if (cfg.run_type == 1 && mv.reweight_on) {
         const double ET = ectl->e_trial, Eest = ectl->e_est;
-        const double Eo = sc[SC_EL], mo = sc[SC_MODRATIO];
-        const double Et = bad ? Eo : EL;
+        const double mo = sc[SC_MODRATIO];
+        double Eo = sc[SC_EL];
+        double Et = bad ? Eo : EL;
+        if (cfg.ecut == 1) {
+          Et *= bad ? mo : modratio;
+          Eo *= mo;
+        } else if (cfg.ecut == 2) {
+          // DePasquale, Rothstein, Vrbik (1988) cutoff |E_L - E_orig| <= 2 / sqrt(dt)
+          const double cut = 2.0 / sqrt(cfg.dt);
+          Et = fmin(fmax(Et, cfg.e_orig - cut), cfg.e_orig + cut);
+          Eo = fmin(fmax(Eo, cfg.e_orig - cut), cfg.e_orig + cut);
+        }
         double St, So;
         if (cfg.emod == 0) {
           St = ET - Et;

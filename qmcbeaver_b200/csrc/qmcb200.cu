@@ -140,6 +140,7 @@ static RunCfg make_cfg(const qmcb_run_params &p)
   c.fusion_threshold = p.fusion_threshold;
   c.seed = p.seed;
   c.limit_branching = p.limit_branching;
+  c.ecut = p.energy_cutoff;
   c.e_orig = p.energy_original != 0.0 ? p.energy_original : (p.energy_estimated != 0.0 ? p.energy_estimated : -1.0);
   c.rel_cutoff = p.rel_cutoff > 0 ? p.rel_cutoff : 1e300;
   return c;
@@ -168,6 +169,7 @@ static void default_params(qmcb_run_params *p)
   p->energy_original = 0.0;
   p->rel_cutoff = 100.0;
   p->limit_branching = 1;
+  p->energy_cutoff = QMCB_ECUT_NONE;
 }
 
 template <typename T>
@@ -393,7 +395,7 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: umrigar93_equalelectrons_parameter must be in (0, 1]");
   if (p->run_type < 0 || p->run_type > 1 || p->sampling < 0 || p->sampling > 1 || p->qf_modification < 0 ||
       p->qf_modification > 2 || p->energy_modification < 0 || p->energy_modification > 2 || p->reweighting < 0 ||
-      p->reweighting > 2)
+      p->reweighting > 2 || p->energy_cutoff < 0 || p->energy_cutoff > 2)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");
   if (p->precision != QMCB_PREC_FP64) return fail(h, QMCB_E_ARG, "qmcb_set_params: only QMCB_PREC_FP64 in this build");
   h->params = *p;

@@ -19,6 +19,7 @@ QMCB_EMOD_NONE, QMCB_EMOD_UMRIGAR93, QMCB_EMOD_MODIFIED_UMRIGAR93 = 0, 1, 2
 QMCB_RW_SIMPLE_SYMMETRIC, QMCB_RW_SIMPLE_ASYMMETRIC, QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED = 0, 1, 2
 QMCB_PREC_FP64, QMCB_PREC_MIXED = 0, 1
 QMCB_ST_SINGULAR, QMCB_ST_NAN = 1, 2
+QMCB_ECUT_NONE, QMCB_ECUT_UMRIGAR93, QMCB_ECUT_BDJM_PUSH88 = 0, 1, 2
 
 
 class SystemDesc(C.Structure):
@@ -42,7 +43,7 @@ class RunParams(C.Structure):
         ("old_walker_acceptance", C.c_int), ("refresh_interval", C.c_int), ("precision", C.c_int),
         ("seed", C.c_uint64), ("population_control", C.c_double), ("target_walkers", C.c_int),
         ("reweight_start_step", C.c_int), ("energy_original", C.c_double), ("rel_cutoff", C.c_double),
-        ("limit_branching", C.c_int),
+        ("limit_branching", C.c_int), ("energy_cutoff", C.c_int),
     ]
 
 
@@ -78,6 +79,7 @@ def run_params(**kw) -> RunParams:
     p.energy_original = 0.0
     p.rel_cutoff = 100.0
     p.limit_branching = 1
+    p.energy_cutoff = QMCB_ECUT_NONE
     for k, v in kw.items():
         if not hasattr(p, k):
             raise AttributeError(k)

@@ -156,7 +156,7 @@ def test_dmc_population_stays_controlled():
         return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING,
                           qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, energy_modification=1, dt=0.01,
                           refresh_interval=50, reweight_start_step=start, energy_trial=e0, energy_estimated=e0,
-                          energy_original=e0, seed=5, limit_branching=0)
+                          energy_original=e0, seed=5, energy_cutoff=2, population_control=100.0)
 
     f = QMCB200Functions(s, 4 * W, params(-1.0, eq))
     f.init_walkers(s.initial_positions(W, seed=3))
@@ -168,6 +168,6 @@ def test_dmc_population_stays_controlled():
     f.init_walkers(wk["R"])
     st = f.run_steps(0, 10 * N)
     assert st.n_moves > 0.5 * 10 * N * W
-    assert 0.3 * W < st.n_walkers < 3 * W
+    assert 0.7 * W < st.n_walkers < 1.5 * W
     assert np.isfinite(st.sum_weight_energy / st.sum_weight)
     assert st.n_singular < 0.01 * st.n_moves
