@@ -144,7 +144,7 @@ typedef struct qmcb_handle qmcb_handle;
 const char *qmcb_version(void);
 
 /* Message of the last failure on this handle (or of the last failed create
- * when h is NULL). */
+ * or handle-free call when h is NULL). */
 const char *qmcb_last_error(const qmcb_handle *h);
 
 /* Builds device tables for the system and allocates state for max_walkers
@@ -238,6 +238,34 @@ int qmcb_synchronize(qmcb_handle *h);
 
 /* The CUDA stream of the handle (cudaStream_t as void*). */
 void *qmcb_stream(qmcb_handle *h);
+
+/*
+ * Allocation-free branching pass (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory at call time: drivers that
+ * hand every byte of HBM to their own memory pool up front (a serving process
+ * with a pre-reserved arena), or that must not trigger the device-wide
+ * synchronisation cudaMalloc / cudaFree imply in the middle of an
+ * asynchronous step sequence.  It needs no handle and calls no allocator: its
+ * scratch is a static device array inside the library.
+ *
+ * Same decisions as qmcb_branch on a plain list of n walker weights (split
+ * above branching_threshold, die below 0.01, fuse pairs below
+ * fusion_threshold in list order, the draw of a pair keyed by (seed, index of
+ * its first member, step)), without the branch-recommendation rules.
+ * Outputs: d_weight_out / d_parent_out (room for 2n entries each) receive the
+ * new list -- survivors in order, split copies appended -- with each entry's
+ * source index; *d_n_out the new count.  All pointers are device memory;
+ * launched on `stream` (NULL = legacy default stream), not synchronised.
+ * Limits: n <= QMCB_NOALLOC_MAX_WALKERS, else QMCB_E_LIMIT.  Every call shares
+ * the one static scratch array, so calls that overlap on the GPU race; keep
+ * them on one stream.  The first call on a device looks up the array's
+ * device address; make that call before any stream capture.
+ */
+#define QMCB_NOALLOC_MAX_WALKERS 65536
+int qmcb_branch_weights_noalloc(const double *d_weight_in, int n, double branching_threshold,
+                                double fusion_threshold, uint64_t seed, int step, double *d_weight_out,
+                                int *d_parent_out, int *d_n_out, void *stream);
 
 #ifdef __cplusplus
 }

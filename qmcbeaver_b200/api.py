@@ -28,6 +28,7 @@ EXPORTS = [
     "qmcb_num_electrons", "qmcb_max_walkers", "qmcb_evaluate", "qmcb_evaluate_device", "qmcb_init_walkers",
     "qmcb_run_steps", "qmcb_num_walkers", "qmcb_get_walkers", "qmcb_copy_slot", "qmcb_synchronize",
     "qmcb_stream", "qmcb_set_walker_weights", "qmcb_branch", "qmcb_set_profiling", "qmcb_get_kernel_stats",
+    "qmcb_branch_weights_noalloc",
 ]
 
 KERNELS = ["move", "branch", "copy", "energy", "refresh"]
@@ -71,6 +72,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.qmcb_branch.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
     L.qmcb_set_profiling.argtypes = [vp, C.c_int]
     L.qmcb_get_kernel_stats.argtypes = [vp, vp, C.c_int]
+    L.qmcb_branch_weights_noalloc.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, vp, vp, vp,
+                                              vp]
     _lib = L
     return L
 

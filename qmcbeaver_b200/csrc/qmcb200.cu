@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -180,6 +181,115 @@ static cudaError_t upload(T **d, const std::vector<T> &v)
   if (!v.empty()) e = cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
   return e;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free branching pass over a caller's weight list.
+//
+// The working weights and the index lists live in these file-scope device
+// arrays instead of memory the library would allocate; every GPU that loads
+// the library holds them (768 KB) until the process exits.  All calls share
+// them, so calls that overlap on the GPU race.
+static __device__ __align__(256) double g_noalloc_weight[QMCB_NOALLOC_MAX_WALKERS];
+static __device__ __align__(256) int g_noalloc_index[QMCB_NOALLOC_MAX_WALKERS];
+
+// Same decisions as k_branch (nonunit-weight branching, fusion pairs in list
+// order, random stream of a pair keyed by its first member's list index),
+// on plain arrays: survivors keep their order, split copies are appended.
+// w_out / parent_out need room for 2 n entries.
+__global__ void __launch_bounds__(1024) k_branch_list(const double *w_in, int n, double thr_split, double thr_fuse,
+                                                      uint64_t seed, int step, double *w_work, int *idx,
+                                                      double *w_out, int *parent_out, int *n_out)
+{
+  __shared__ int s_warp[32];
+  __shared__ int s_tot;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  // every working element read below is written here first in this call
+  for (int i = tid; i < n; i += 1024) w_work[i] = w_in[i];
+  __syncthreads();
+  auto block_scan = [&](int flag, int &excl, int &total) {
+    unsigned b = __ballot_sync(QMCB_FULL_MASK, flag);
+    int pre = __popc(b & ((1u << lane) - 1));
+    if (lane == 31) s_warp[wid] = pre + flag;
+    __syncthreads();
+    if (wid == 0) {
+      int v = s_warp[lane], x = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(QMCB_FULL_MASK, x, o);
+        if (lane >= o) x += y;
+      }
+      s_warp[lane] = x - v;
+      if (lane == 31) s_tot = x;
+    }
+    __syncthreads();
+    excl = s_warp[wid] + pre;
+    total = s_tot;
+    __syncthreads();
+  };
+  // fusion candidates in list order
+  int nc = 0;
+  for (int c0 = 0; c0 < n; c0 += 1024) {
+    int i = c0 + tid;
+    double w = i < n ? w_work[i] : 0.0;
+    int is_c = (i < n && w <= thr_split && w >= 0.01 && w < thr_fuse) ? 1 : 0;
+    int ex, tot;
+    block_scan(is_c, ex, tot);
+    if (is_c) idx[nc + ex] = i;
+    nc += tot;
+  }
+  __syncthreads();
+  for (int m = tid; 2 * m + 1 < nc; m += 1024) {
+    int ia = idx[2 * m], ib = idx[2 * m + 1];
+    double w1 = w_work[ia], w2 = w_work[ib], w3 = w1 + w2;
+    double u[4];
+    rng_uniform4(seed, (uint32_t)ia, (uint32_t)step, 7u, u);
+    if (u[0] < w1 / w3) {
+      w_work[ia] = w3;
+      w_work[ib] = -1.0;
+    } else {
+      w_work[ib] = w3;
+      w_work[ia] = -1.0;
+    }
+  }
+  __syncthreads();
+  // survivors in order
+  int nk = 0;
+  for (int c0 = 0; c0 < n; c0 += 1024) {
+    int i = c0 + tid;
+    int keep = (i < n && w_work[i] >= 0.01) ? 1 : 0;
+    int ex, tot;
+    block_scan(keep, ex, tot);
+    if (keep) idx[nk + ex] = i;
+    nk += tot;
+  }
+  __syncthreads();
+  // splits appended after the survivors
+  int ns = 0;
+  for (int c0 = 0; c0 < nk; c0 += 1024) {
+    int j = c0 + tid;
+    int src = j < nk ? idx[j] : -1;
+    double w = src >= 0 ? w_work[src] : 0.0;
+    int sp = (src >= 0 && w > thr_split) ? 1 : 0;
+    int ex, tot;
+    block_scan(sp, ex, tot);
+    if (src >= 0) {
+      double wk = sp ? 0.5 * w : w;
+      w_out[j] = wk;
+      parent_out[j] = src;
+      if (sp) {
+        w_out[nk + ns + ex] = wk;
+        parent_out[nk + ns + ex] = src;
+      }
+    }
+    ns += tot;
+  }
+  if (tid == 0) *n_out = nk + ns;
+}
+
+namespace {
+std::mutex g_noalloc_mu;
+void *g_noalloc_w_addr[64];
+void *g_noalloc_i_addr[64];
+}  // namespace
 
 extern "C" {
 
@@ -693,6 +803,49 @@ int qmcb_copy_slot(qmcb_handle *h, int src, int dst)
   size_t b = sizeof(double) * h->lay.stride;
   CK(cudaMemcpyAsync(h->d_state + (size_t)dst * h->lay.stride, h->d_state + (size_t)src * h->lay.stride, b,
                      cudaMemcpyDeviceToDevice, h->stream));
+  return QMCB_OK;
+}
+
+int qmcb_branch_weights_noalloc(const double *d_weight_in, int n, double branching_threshold,
+                                double fusion_threshold, uint64_t seed, int step, double *d_weight_out,
+                                int *d_parent_out, int *d_n_out, void *stream)
+{
+  if (n < 0 || (n > 0 && (!d_weight_in || !d_weight_out || !d_parent_out)) || !d_n_out)
+    return fail(nullptr, QMCB_E_ARG, "qmcb_branch_weights_noalloc: null buffer or negative n");
+  if (n > QMCB_NOALLOC_MAX_WALKERS)
+    return fail(nullptr, QMCB_E_LIMIT,
+                "qmcb_branch_weights_noalloc: n exceeds QMCB_NOALLOC_MAX_WALKERS (65536)");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64)
+    return fail(nullptr, QMCB_E_CUDA, std::string("qmcb_branch_weights_noalloc: no CUDA device: ") +
+                                          cudaGetErrorString(e));
+  void *pw = nullptr, *pi = nullptr;
+  {
+    // once per device, with that device current: the device addresses of
+    // the static scratch arrays (their host-side names are not device addresses)
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_w_addr[dev] || !g_noalloc_i_addr[dev]) {
+      e = cudaGetSymbolAddress(&pw, g_noalloc_weight);
+      if (e != cudaSuccess)
+        return fail(nullptr, QMCB_E_CUDA, std::string("qmcb_branch_weights_noalloc: cudaGetSymbolAddress: ") +
+                                              cudaGetErrorString(e));
+      e = cudaGetSymbolAddress(&pi, g_noalloc_index);
+      if (e != cudaSuccess)
+        return fail(nullptr, QMCB_E_CUDA, std::string("qmcb_branch_weights_noalloc: cudaGetSymbolAddress: ") +
+                                              cudaGetErrorString(e));
+      g_noalloc_w_addr[dev] = pw;
+      g_noalloc_i_addr[dev] = pi;
+    }
+    pw = g_noalloc_w_addr[dev];
+    pi = g_noalloc_i_addr[dev];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  k_branch_list<<<1, 1024, 0, st>>>(d_weight_in, n, branching_threshold, fusion_threshold, seed, step, (double *)pw,
+                                    (int *)pi, d_weight_out, d_parent_out, d_n_out);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail(nullptr, QMCB_E_CUDA, std::string("qmcb_branch_weights_noalloc: launch: ") + cudaGetErrorString(e));
   return QMCB_OK;
 }
 
