@@ -45,13 +45,19 @@ enum Sc {
 };
 constexpr int kScalars = 24;  // padded
 
+constexpr int kShellPrim = 6;  // primitives kept in registers per shell
+
 struct DevSys {
-  int M, na, nb, N, K, npade;
+  int M, na, nb, N, K, npade, nshell;
   int ee[3];
   double Pnn;
   const double4 *nuc;    // [M] x, y, z, Z
   const int4 *bf;        // [K] atom, a | b<<8 | c<<16, nprim, prim offset
   const double2 *prim;   // [P] exponent, coefficient
+  const int4 *shell;     // [nshell] atom, first function, nmem | L<<8 | nprim<<16, exponent offset
+  const int2 *fn;        // [K] a | b<<8 | c<<16, coefficient offset
+  const double *pexp;    // [P] exponents
+  const double *pcoef;   // [P] coefficients
   const double *ct[2];   // [K][n_s] MO coefficients, transposed
   const double *pade;    // [npade][2][kPadeMax] numerator, denominator
   const int2 *pade_len;  // [npade] numerator length, denominator length
@@ -176,10 +182,11 @@ __device__ __forceinline__ void pade_eval(const DevSys &S, int f, double r, doub
   double a, ap, app, b, bp, bpp;
   poly_all(P, L.x, r, a, ap, app);
   poly_all(P + kPadeMax, L.y, r, b, bp, bpp);
-  double aDIVb = a / b, bpDIVb = bp / b, apDIVb = ap / b;
+  const double ib = 1.0 / b;
+  double aDIVb = a * ib, bpDIVb = bp * ib, apDIVb = ap * ib;
   u = aDIVb;
   du = apDIVb - bpDIVb * aDIVb;
-  d2u = (app - bpp * aDIVb) / b - 2.0 * bpDIVb * du;
+  d2u = (app - bpp * aDIVb) * ib - 2.0 * bpDIVb * du;
 }
 
 // e-e correlation function index for electrons i, j
@@ -245,6 +252,140 @@ __device__ __forceinline__ void basis_warp(const DevSys &S, const double r[3], d
     basis_one(S, k, r, o);
 #pragma unroll
     for (int q = 0; q < 5; q++) chi[q * ldc + k] = o[q];
+  }
+}
+
+// Basis functions of all shells at position r (lanes over shells).  A shell
+// is a run of functions on one centre sharing their exponents; exp(-a r^2)
+// is evaluated once per primitive and shell.  With P = x^a y^b z^c and
+// E_m = sum_i c_i a_i^m exp(-a_i r^2) (m = 0, 1, 2) the reference's formulas
+// (QMcBeaver/src/QMCBasisFunction.cpp:370-391) become
+//   f = E0 P,  df/dx = E0 dP/dx - 2 x P E1,
+//   lap f = E0 lap P + P sum_i c_i e_i (4 r^2 a_i^2 - (4L + 6) a_i),
+// polynomial derivatives instead of the reference's a/x and a(a-1)/x^2
+// factors (same values, no division by a coordinate).
+__device__ __forceinline__ void shell_members(const DevSys &S, int4 sh, double x, double y, double z, double r2,
+                                              const double *ex, const double *al, double *chi, int ldc)
+{
+  const int nmem = sh.z & 0xff, L = (sh.z >> 8) & 0xff, np = sh.z >> 16;
+  const double Lf = 4.0 * L + 6.0;
+  for (int m = 0; m < nmem; m++) {
+    const int k = sh.y + m;
+    const int2 f = __ldg(&S.fn[k]);
+    const int a = f.x & 0xff, b = (f.x >> 8) & 0xff, c = (f.x >> 16) & 0xff;
+    const double *co = S.pcoef + f.y;
+    // E0 = sum c e, E1 = sum c a e, El = sum c e (4 r^2 a^2 - (4L+6) a): the
+    // Laplacian factor is combined per primitive, as the reference does, so
+    // its cancellation happens before the sum
+    double E0 = 0.0, E1 = 0.0, El = 0.0;
+    const double r2x4 = 4.0 * r2;
+    if (np <= kShellPrim) {
+#pragma unroll
+      for (int i = 0; i < kShellPrim; i++) {
+        if (i < np) {
+          const double e = __ldg(&co[i]) * ex[i];
+          E0 += e;
+          E1 = fma(e, al[i], E1);
+          El = fma(e, al[i] * fma(r2x4, al[i], -Lf), El);
+        }
+      }
+    } else {
+      for (int i = 0; i < np; i++) {
+        const double ai = __ldg(&S.pexp[sh.w + i]);
+        const double e = __ldg(&co[i]) * exp(-ai * r2);
+        E0 += e;
+        E1 = fma(e, ai, E1);
+        El = fma(e, ai * fma(r2x4, ai, -Lf), El);
+      }
+    }
+    const double xa = ipow(x, a), yb = ipow(y, b), zc = ipow(z, c);
+    const double P = xa * yb * zc;
+    const double Px = a ? a * ipow(x, a - 1) * yb * zc : 0.0;
+    const double Py = b ? b * xa * ipow(y, b - 1) * zc : 0.0;
+    const double Pz = c ? c * xa * yb * ipow(z, c - 1) : 0.0;
+    double Pl = 0.0;
+    if (a > 1) Pl += a * (a - 1.0) * ipow(x, a - 2) * yb * zc;
+    if (b > 1) Pl += b * (b - 1.0) * xa * ipow(y, b - 2) * zc;
+    if (c > 1) Pl += c * (c - 1.0) * xa * yb * ipow(z, c - 2);
+    const double PE1 = P * E1;
+    chi[0 * ldc + k] = E0 * P;
+    chi[1 * ldc + k] = fma(E0, Px, -2.0 * x * PE1);
+    chi[2 * ldc + k] = fma(E0, Py, -2.0 * y * PE1);
+    chi[3 * ldc + k] = fma(E0, Pz, -2.0 * z * PE1);
+    chi[4 * ldc + k] = fma(E0, Pl, P * El);
+  }
+}
+
+__device__ __forceinline__ void basis_shells_warp(const DevSys &S, const double r[3], double *chi, int ldc)
+{
+  for (int si = lane_id(); si < S.nshell; si += 32) {
+    const int4 sh = __ldg(&S.shell[si]);
+    const double4 A = S.nuc[sh.x];
+    const double x = r[0] - A.x, y = r[1] - A.y, z = r[2] - A.z;
+    const double r2 = x * x + y * y + z * z;
+    const int np = sh.z >> 16;
+    double ex[kShellPrim], al[kShellPrim];
+#pragma unroll
+    for (int i = 0; i < kShellPrim; i++) {
+      al[i] = 0.0;
+      ex[i] = 0.0;
+      if (i < np && np <= kShellPrim) {
+        al[i] = __ldg(&S.pexp[sh.w + i]);
+        ex[i] = exp(-al[i] * r2);
+      }
+    }
+    shell_members(S, sh, x, y, z, r2, ex, al, chi, ldc);
+  }
+}
+
+// D[q][o] = sum_k chi[q][k] Ct[k][o] with lanes split into K-slices of n
+// orbitals each (n <= 32): every lane keeps five independent accumulators;
+// the slices' partial sums meet in `part` (5 * 32 doubles).
+__device__ __forceinline__ void contract_slices_warp(const double *chi, int ldc, const double *__restrict__ Ct, int n,
+                                                     int K, double *D, double *part)
+{
+  const int lane = lane_id();
+  if (n <= 32) {
+    const int S = 32 / n, s = lane / n, o = lane - s * n;
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (s < S) {
+      const int k0 = (K * s) / S, k1 = (K * (s + 1)) / S;
+      for (int k = k0; k < k1; k++) {
+        const double cf = __ldg(&Ct[k * n + o]);
+#pragma unroll
+        for (int q = 0; q < 5; q++) acc[q] = fma(chi[q * ldc + k], cf, acc[q]);
+      }
+    }
+    if (S == 1) {
+      if (s < S)
+#pragma unroll
+        for (int q = 0; q < 5; q++) D[q * n + o] = acc[q];
+    } else {
+      __syncwarp();  // part may alias chi: every lane is done reading it
+      if (s < S)
+#pragma unroll
+        for (int q = 0; q < 5; q++) part[(s * 5 + q) * n + o] = acc[q];
+      __syncwarp();
+      if (lane < n) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+          double t = 0.0;
+          for (int ss = 0; ss < S; ss++) t += part[(ss * 5 + q) * n + lane];
+          D[q * n + lane] = t;
+        }
+      }
+    }
+  } else {
+    for (int o = lane; o < n; o += 32) {
+      double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int k = 0; k < K; k++) {
+        const double cf = __ldg(&Ct[k * n + o]);
+#pragma unroll
+        for (int q = 0; q < 5; q++) acc[q] = fma(chi[q * ldc + k], cf, acc[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 5; q++) D[q * n + o] = acc[q];
+    }
   }
 }
 

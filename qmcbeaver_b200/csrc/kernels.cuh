@@ -48,13 +48,18 @@ struct EnergyCtl {
 };
 
 // Shared-memory doubles needed by one warp.
+constexpr int kPart = 160;  // 5 quantities x 32 lanes of slice partial sums
+// Move-kernel scratch: region A holds the basis values chi[5][K]; once the
+// contraction has consumed them it is reused for the slice partial sums and
+// the new drift / modified drift (gr, mg).
+__host__ __device__ inline int move_region_a(int N, int K) { return max(5 * K, kPart + 6 * N); }
 __host__ __device__ inline int move_scratch_doubles(int N, int K, int nmax)
 {
-  return 5 * (K + 1) + 5 * nmax + nmax * nmax + nmax + 5 * 3 * N + 8;
+  return move_region_a(N, K) + 5 * nmax + nmax * nmax + nmax + 3 * 3 * N + 8;
 }
 __host__ __device__ inline int full_scratch_doubles(int N, int K, int nmax)
 {
-  return 5 * (K + 1) + 5 * nmax + 2 * nmax * nmax + 2 * nmax + 3 * N + 8;
+  return 5 * (K + 1) + 5 * nmax + 2 * nmax * nmax + 2 * nmax + 3 * N + kPart + 8;
 }
 
 // ------------------------------------------------------------------------
@@ -74,14 +79,16 @@ __device__ inline double qf_modify_warp(const DevSys &S, const RunCfg &cfg, cons
     for (int t = lane; t < 3 * N; t += 32) mg[t] = gr[t] * factor;
   } else if (cfg.qf_mod == 2) {
     for (int i = lane; i < N; i += 32) {
+      // closest nucleus (QMCMolecule::findClosestNucleusIndex): smallest
+      // distance, first index on ties -- compared on squared distances
       int cn = 0;
-      double cd = 1e100;
+      double cd = 1e300;
       for (int A = 0; A < S.M; A++) {
         double4 P = S.nuc[A];
         double dx = R[3 * i] - P.x, dy = R[3 * i + 1] - P.y, dz = R[3 * i + 2] - P.z;
-        double r = sqrt(dx * dx + dy * dy + dz * dz);
-        if (r < cd) {
-          cd = r;
+        double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < cd) {
+          cd = d2;
           cn = A;
         }
       }
@@ -312,6 +319,7 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
   double *vv = X + nmax * nmax;
   double *piv = vv + nmax;
   double *Rs = piv + nmax;
+  double *part = Rs + 3 * N;
   double *R = blk + L.R;
   double *sc = blk + L.sc;
 
@@ -334,9 +342,9 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
     if (do_basis) {
       for (int e = 0; e < n; e++) {
         double r[3] = {Rs[3 * (base + e)], Rs[3 * (base + e) + 1], Rs[3 * (base + e) + 2]};
-        basis_warp(S, r, chi, ldc);
+        basis_shells_warp(S, r, chi, ldc);
         __syncwarp();
-        contract_warp(chi, ldc, S.ct[sp], n, K, Dn);
+        contract_slices_warp(chi, ldc, S.ct[sp], n, K, Dn, part);
         __syncwarp();
         for (int o = lane; o < n; o += 32) {
           Dv[e * n + o] = Dn[o];
@@ -444,7 +452,7 @@ struct MoveArgs {
 };
 
 template <bool kMetropolis>
-__global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+__global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, MoveArgs mv,
                                               const EnergyCtl *ectl, double *stats, EvalOut out)
 {
@@ -460,16 +468,17 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
   const int slot = slots ? slots[wi] : wi;
   double *blk = state + (size_t)slot * L.stride;
   double *sm = smem + (size_t)warp * move_scratch_doubles(N, K, nmax);
-  const int ldc = K + 1;
+  const int ldc = K;
   double *chi = sm;
-  double *Dn = chi + 5 * ldc;
+  double *part = sm;                   // after the contraction's k loop
+  double *gr = sm + kPart;             // after the contraction
+  double *mg = gr + 3 * N;
+  double *Dn = sm + move_region_a(N, K);
   double *Inv = Dn + 5 * nmax;
   double *valc = Inv + nmax * nmax;
   double *Ux = valc + nmax;
   double *gD = Ux + 3 * N;
-  double *gr = gD + 3 * N;
-  double *mg = gr + 3 * N;
-  double *Rn = mg + 3 * N;
+  double *Rn = gD + 3 * N;
   double *sc = blk + L.sc;
   const double *Rold = blk + L.R;
 
@@ -524,17 +533,19 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
       double dxn = rn[0] - Rj[0], dyn = rn[1] - Rj[1], dzn = rn[2] - Rj[2];
       double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
       double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
-      dVee += 1.0 / r_n - 1.0 / r_o;
+      const double io = 1.0 / r_o, in_ = 1.0 / r_n;
+      dVee += in_ - io;
       int f = ee_func(S, e, j);
       if (f >= 0) {
         double uo, duo, d2uo, un, dun, d2un;
         pade_eval(S, f, r_o, uo, duo, d2uo);
         pade_eval(S, f, r_n, un, dun, d2un);
         dU += un - uo;
-        dUxx += 2.0 * (2.0 / r_n * dun + d2un) - 2.0 * (2.0 / r_o * duo + d2uo);
-        double vx = dun * (dxn / r_n) - duo * (dxo / r_o);
-        double vy = dun * (dyn / r_n) - duo * (dyo / r_o);
-        double vz = dun * (dzn / r_n) - duo * (dzo / r_o);
+        dUxx += 2.0 * (2.0 * in_ * dun + d2un) - 2.0 * (2.0 * io * duo + d2uo);
+        const double sn = dun * in_, so = duo * io;
+        double vx = sn * dxn - so * dxo;
+        double vy = sn * dyn - so * dyo;
+        double vz = sn * dzn - so * dzo;
         ge[0] += vx;
         ge[1] += vy;
         ge[2] += vz;
@@ -553,17 +564,19 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
     double dxn = rn[0] - P.x, dyn = rn[1] - P.y, dzn = rn[2] - P.z;
     double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
     double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
-    dVen -= P.w * (1.0 / r_n - 1.0 / r_o);
+    const double io = 1.0 / r_o, in_ = 1.0 / r_n;
+    dVen -= P.w * (in_ - io);
     int f = S.en[sp][A];
     if (f >= 0) {
       double uo, duo, d2uo, un, dun, d2un;
       pade_eval(S, f, r_o, uo, duo, d2uo);
       pade_eval(S, f, r_n, un, dun, d2un);
       dU += un - uo;
-      dUxx += (2.0 / r_n * dun + d2un) - (2.0 / r_o * duo + d2uo);
-      ge[0] += dun * (dxn / r_n) - duo * (dxo / r_o);
-      ge[1] += dun * (dyn / r_n) - duo * (dyo / r_o);
-      ge[2] += dun * (dzn / r_n) - duo * (dzo / r_o);
+      dUxx += (2.0 * in_ * dun + d2un) - (2.0 * io * duo + d2uo);
+      const double sn = dun * in_, so = duo * io;
+      ge[0] += sn * dxn - so * dxo;
+      ge[1] += sn * dyn - so * dyo;
+      ge[2] += sn * dzn - so * dzo;
     }
   }
   dU = warp_sum(dU);
@@ -576,18 +589,18 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
     for (int d = 0; d < 3; d++) Ux[3 * e + d] = Uxo[3 * e + d] + ge[d];
 
   // ---- basis at the new position and the new Slater / derivative rows
-  basis_warp(S, rn, chi, ldc);
+  basis_shells_warp(S, rn, chi, ldc);
   __syncwarp();
-  contract_warp(chi, ldc, S.ct[sp], n, K, Dn);
+  contract_slices_warp(chi, ldc, S.ct[sp], n, K, Dn, part);
   const double *InvG = blk + L.Inv[sp];
   for (int t = lane; t < n * n; t += 32) Inv[t] = InvG[t];
   __syncwarp();
 
   // ---- Sherman-Morrison row replacement (Array2D::inverseUpdateOneRow,
   //      QMcBeaver/include/Array2D.h:1567-1610)
-  double part = 0.0;
-  for (int o = lane; o < n; o += 32) part += Dn[o] * Inv[o * n + el];
-  const double ratio = warp_sum(part);
+  double rpart = 0.0;
+  for (int o = lane; o < n; o += 32) rpart += Dn[o] * Inv[o * n + el];
+  const double ratio = warp_sum(rpart);
   bool bad = !(ratio != 0.0) || !isfinite(ratio);
   const double q = 1.0 / ratio;
   for (int c = lane; c < n; c += 32) {
@@ -597,9 +610,18 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
     valc[c] = val * q;
   }
   __syncwarp();
-  for (int t = lane; t < n * n; t += 32) {
-    int r = t / n, c = t - r * n;
-    if (c != el) Inv[t] -= valc[c] * Inv[r * n + el];
+  if (n <= 32) {
+    const int rpp = 32 / n, r0 = lane / n, c = lane - r0 * n;
+    if (r0 < rpp && c != el) {
+      const double vc = valc[c];
+      for (int r = r0; r < n; r += rpp) Inv[r * n + c] -= vc * Inv[r * n + el];
+    }
+  } else {
+    for (int c = lane; c < n; c += 32) {
+      if (c == el) continue;
+      const double vc = valc[c];
+      for (int r = 0; r < n; r++) Inv[r * n + c] -= vc * Inv[r * n + el];
+    }
   }
   __syncwarp();
   for (int r = lane; r < n; r += 32) Inv[r * n + el] *= q;
@@ -608,28 +630,56 @@ __global__ void __launch_bounds__(128) k_move(DevSys S, Layout L, RunCfg cfg, do
   // ---- ratio sums of the moved spin (QMcBeaver/src/QMCSlater.cpp:741-762)
   const double *DgT = blk + L.DgT[sp], *DlT = blk + L.DlT[sp];
   double lp = 0.0;
-  for (int e2 = lane; e2 < n; e2 += 32) {
-    double gx = 0, gy = 0, gz = 0;
-    if (e2 == el) {
-      for (int o = 0; o < n; o++) {
-        double iv = Inv[o * n + el];
-        gx += Dn[n + o] * iv;
-        gy += Dn[2 * n + o] * iv;
-        gz += Dn[3 * n + o] * iv;
-        lp += Dn[4 * n + o] * iv;
+  {
+    // lanes = (o-slice, electron): S2 slices of the orbital sum for n <= 16
+    const int S2 = n <= 32 ? 32 / n : 1;
+    const int s2 = n <= 32 ? lane / n : 0;
+    const int o0 = (n * s2) / S2, o1 = (n * (s2 + 1)) / S2;
+    for (int e2 = (n <= 32 ? lane - s2 * n : lane); e2 < n && s2 < S2; e2 += (n <= 32 ? n : 32)) {
+      double gx = 0, gy = 0, gz = 0, ll = 0;
+      const int oa = n <= 32 ? o0 : 0, ob = n <= 32 ? o1 : n;
+      if (e2 == el) {
+        for (int o = oa; o < ob; o++) {
+          const double iv = Inv[o * n + el];
+          gx = fma(Dn[n + o], iv, gx);
+          gy = fma(Dn[2 * n + o], iv, gy);
+          gz = fma(Dn[3 * n + o], iv, gz);
+          ll = fma(Dn[4 * n + o], iv, ll);
+        }
+      } else {
+        for (int o = oa; o < ob; o++) {
+          const double iv = Inv[o * n + e2];
+          gx = fma(DgT[(0 * n + o) * n + e2], iv, gx);
+          gy = fma(DgT[(1 * n + o) * n + e2], iv, gy);
+          gz = fma(DgT[(2 * n + o) * n + e2], iv, gz);
+          ll = fma(DlT[o * n + e2], iv, ll);
+        }
       }
-    } else {
-      for (int o = 0; o < n; o++) {
-        double iv = Inv[o * n + e2];
-        gx += DgT[(0 * n + o) * n + e2] * iv;
-        gy += DgT[(1 * n + o) * n + e2] * iv;
-        gz += DgT[(2 * n + o) * n + e2] * iv;
-        lp += DlT[o * n + e2] * iv;
+      lp += ll;
+      if (S2 == 1) {
+        gD[3 * (base + e2)] = gx;
+        gD[3 * (base + e2) + 1] = gy;
+        gD[3 * (base + e2) + 2] = gz;
+      } else {
+        part[(s2 * 3 + 0) * n + e2] = gx;
+        part[(s2 * 3 + 1) * n + e2] = gy;
+        part[(s2 * 3 + 2) * n + e2] = gz;
       }
     }
-    gD[3 * (base + e2)] = gx;
-    gD[3 * (base + e2) + 1] = gy;
-    gD[3 * (base + e2) + 2] = gz;
+    if (S2 > 1) {
+      __syncwarp();
+      for (int e2 = lane; e2 < n; e2 += 32) {
+        double gx = 0, gy = 0, gz = 0;
+        for (int ss = 0; ss < S2; ss++) {
+          gx += part[(ss * 3 + 0) * n + e2];
+          gy += part[(ss * 3 + 1) * n + e2];
+          gz += part[(ss * 3 + 2) * n + e2];
+        }
+        gD[3 * (base + e2)] = gx;
+        gD[3 * (base + e2) + 1] = gy;
+        gD[3 * (base + e2) + 2] = gz;
+      }
+    }
   }
   const double lapR = warp_sum(lp);
   {

@@ -43,6 +43,9 @@ struct qmcb_handle {
   double *d_ct[2] = {nullptr, nullptr};
   double *d_pade = nullptr;
   int2 *d_pade_len = nullptr;
+  int4 *d_shell = nullptr;
+  int2 *d_fn = nullptr;
+  double *d_pexp = nullptr, *d_pcoef = nullptr;
   int *d_en[2] = {nullptr, nullptr};
   double *d_state = nullptr;
   int *d_live = nullptr, *d_live_tmp = nullptr, *d_free = nullptr, *d_ctl = nullptr;
@@ -338,6 +341,39 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   }
   std::vector<double2> prim(d->n_prim_total);
   for (int i = 0; i < d->n_prim_total; i++) prim[i] = make_double2(d->prim_exponent[i], d->prim_coeff[i]);
+  // shells: runs of consecutive functions on one centre with the same angular
+  // momentum and identical exponent lists (their exps are shared)
+  std::vector<double> pexp(d->prim_exponent, d->prim_exponent + d->n_prim_total);
+  std::vector<double> pcoef(d->prim_coeff, d->prim_coeff + d->n_prim_total);
+  std::vector<int2> fn(K);
+  std::vector<int4> shells;
+  for (int k = 0; k < K;) {
+    const int atom = d->bf_atom[k], np = d->bf_nprim[k], off = d->bf_prim_offset[k];
+    const int L = d->bf_powers[3 * k] + d->bf_powers[3 * k + 1] + d->bf_powers[3 * k + 2];
+    const int maxmem = (L + 1) * (L + 2) / 2;
+    int m = 1;
+    while (k + m < K && m < maxmem && m < 255 && np <= kShellPrim) {
+      const int k2 = k + m;
+      const int L2 = d->bf_powers[3 * k2] + d->bf_powers[3 * k2 + 1] + d->bf_powers[3 * k2 + 2];
+      if (d->bf_atom[k2] != atom || d->bf_nprim[k2] != np || L2 != L) break;
+      bool same = true;
+      for (int i = 0; i < np; i++)
+        if (d->prim_exponent[d->bf_prim_offset[k2] + i] != d->prim_exponent[off + i]) same = false;
+      if (!same) break;
+      m++;
+    }
+    shells.push_back(make_int4(atom, k, m | (L << 8) | (np << 16), off));
+    k += m;
+  }
+  for (int k = 0; k < K; k++) {
+    int a = d->bf_powers[3 * k], b = d->bf_powers[3 * k + 1], c = d->bf_powers[3 * k + 2];
+    fn[k] = make_int2(a | (b << 8) | (c << 16), d->bf_prim_offset[k]);
+  }
+  // lanes of a warp take consecutive shells: order them by angular momentum
+  // and size so neighbouring lanes run the same member loop
+  std::stable_sort(shells.begin(), shells.end(), [](const int4 &x, const int4 &y) {
+    return (x.z & 0xffff) < (y.z & 0xffff);
+  });
   std::vector<double> ct[2];
   for (int sp = 0; sp < 2; sp++) {
     int n = sp ? nb : na;
@@ -397,6 +433,10 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(upload(&h->d_nuc, nuc));
   CKC(upload(&h->d_bf, bf));
   CKC(upload(&h->d_prim, prim));
+  CKC(upload(&h->d_shell, shells));
+  CKC(upload(&h->d_fn, fn));
+  CKC(upload(&h->d_pexp, pexp));
+  CKC(upload(&h->d_pcoef, pcoef));
   CKC(upload(&h->d_ct[0], ct[0]));
   CKC(upload(&h->d_ct[1], ct[1]));
   CKC(upload(&h->d_pade, pade));
@@ -416,6 +456,11 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   S.nuc = h->d_nuc;
   S.bf = h->d_bf;
   S.prim = h->d_prim;
+  S.nshell = (int)shells.size();
+  S.shell = h->d_shell;
+  S.fn = h->d_fn;
+  S.pexp = h->d_pexp;
+  S.pcoef = h->d_pcoef;
   S.ct[0] = h->d_ct[0];
   S.ct[1] = h->d_ct[1];
   S.pade = h->d_pade;
@@ -486,7 +531,7 @@ int qmcb_destroy(qmcb_handle *h)
 {
   if (!h) return QMCB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *ptrs[] = {h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
+  void *ptrs[] = {h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
                   h->d_copies, h->d_stats, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
   for (void *p : ptrs)

@@ -63,9 +63,11 @@ def replay(ev_eval, d, rtol, label):
 
 # Rounding differences between two FP64 implementations grow with the
 # condition number of the Slater matrix carried through Sherman-Morrison
-# updates; the 1e-10 bar applies to walkers whose matrices stayed below this
-# condition number (a walker that once exceeded it stays excluded).
-COND_LIMIT = 1e5
+# updates (measured: about 1.1e-15 * cond).  The 1e-10 bar applies to walkers
+# whose matrices stayed below COND_LIMIT; beyond it the bound is
+# COND_SLOPE * cond (a walker that once exceeded the limit stays there).
+COND_SLOPE = 2e-15
+COND_LIMIT = 5e4
 
 
 def slater_conditions(orc, walkers, system):

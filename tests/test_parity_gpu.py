@@ -4,7 +4,7 @@ seeded configurations.  Plain FP64 path: 1e-10 relative."""
 import numpy as np
 import pytest
 
-from helpers import COND_LIMIT, GOLDEN_CASES, PARITY_RTOL, compare, load_golden, replay, slater_conditions
+from helpers import COND_LIMIT, COND_SLOPE, GOLDEN_CASES, PARITY_RTOL, compare, load_golden, replay, slater_conditions
 from qmcbeaver_b200.api import QMCB200Functions
 from qmcbeaver_b200.system import make_random_molecule, make_system
 
@@ -21,7 +21,7 @@ def test_gpu_reproduces_reference_golden(case):
     f.close()
 
 
-def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good=0.5):
+def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good=0.3):
     from oracle.evaluators import OracleEvaluator
     orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
     f = QMCB200Functions(s, W + slots_offset, qf_modification=qf, dt=dt)
@@ -45,8 +45,8 @@ def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good
         compare(out, ref, PARITY_RTOL, f"{s.name} call {i} whichE={e}", mask=good)
         if (~good).any():
             # ill-conditioned Slater matrices: rounding differences of two
-            # FP64 implementations are bounded by ~cond * 1e-14
-            tol = max(PARITY_RTOL, 1e-14 * float(worst_cond[~good].max()))
+            # FP64 implementations grow as ~cond * 1e-15
+            tol = max(PARITY_RTOL, COND_SLOPE * float(worst_cond[~good].max()))
             compare(out, ref, tol, f"{s.name} call {i} whichE={e} (cond {worst_cond[~good].max():.1e})", mask=~good)
     f.close()
     assert good.mean() >= min_good, f"only {good.sum()} of {W} walkers stayed well conditioned"
@@ -57,7 +57,7 @@ def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good
                                               ("dmc_6nuc_30e", 64, 2, 0.01, 2),
                                               ("dmc_6nuc_30e", 16, 1, 0.01, 1)])
 def test_gpu_matches_oracle_workloads(wl, W, qf, dt, sweeps):
-    _oracle_sequence(make_system(wl, seed=3), W, qf, dt, sweeps, 0.2, seed=21, slots_offset=5)
+    _oracle_sequence(make_system(wl, seed=3), W, qf, dt, sweeps, 3 * dt ** 0.5, seed=21, slots_offset=5)
 
 
 def test_gpu_matches_oracle_100_electrons():
