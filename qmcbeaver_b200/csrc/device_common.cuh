@@ -62,6 +62,8 @@ struct DevSys {
   const double *pade;    // [npade][2][kPadeMax] numerator, denominator
   const int2 *pade_len;  // [npade] numerator length, denominator length
   const int *en[2];      // [M] e-n function per spin
+  const double2 *pade_ab; // [npade] (a, b) when every function is a r / (1 + b r)
+  int pade_simple;
 };
 
 // Offsets (in doubles) of each array in a walker block.
@@ -177,6 +179,18 @@ __device__ __forceinline__ void poly_all(const double *c, int len, double x, dou
 
 __device__ __forceinline__ void pade_eval(const DevSys &S, int f, double r, double &u, double &du, double &d2u)
 {
+  if (S.pade_simple) {
+    // u = a r / (1 + b r): u' = a q^2, u'' = -2 a b q^3 with q = 1 / (1 + b r)
+    // (the FixedCuspPade form of the workloads; same values as the general
+    // quotient-rule evaluation below up to rounding)
+    const double2 ab = __ldg(&S.pade_ab[f]);
+    const double q = 1.0 / fma(ab.y, r, 1.0);
+    const double aq = ab.x * q;
+    u = aq * r;
+    du = aq * q;
+    d2u = -2.0 * ab.y * du * q;
+    return;
+  }
   const double *P = S.pade + (size_t)f * 2 * kPadeMax;
   int2 L = S.pade_len[f];
   double a, ap, app, b, bp, bpp;
@@ -385,6 +399,51 @@ __device__ __forceinline__ void contract_slices_warp(const double *chi, int ldc,
       }
 #pragma unroll
       for (int q = 0; q < 5; q++) D[q * n + o] = acc[q];
+    }
+  }
+}
+
+// FP64 tensor-core tile D(8x8) += A(8x4) B(4x8), mma.sync m8n8k4 (row.col).
+// Fragments: a = A[lane/4][lane%4], b = B[lane%4][lane/4],
+// d0,d1 = D[lane/4][2(lane%4)], D[lane/4][2(lane%4)+1].
+__device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// D[q][o] = sum_k chi[q][k] Ct[k][o] on the FP64 tensor pipe: rows q = the
+// five basis quantities (padded to 8), columns = orbitals in tiles of 8,
+// k in steps of 4; two column tiles in flight for latency hiding.
+__device__ __forceinline__ void contract_dmma_warp(const double *chi, int ldc, const double *__restrict__ Ct, int n,
+                                                   int K, double *D)
+{
+  const int lane = lane_id(), r = lane >> 2, c4 = lane & 3;
+  const int ntiles = (n + 7) >> 3;
+  for (int t0 = 0; t0 < ntiles; t0 += 2) {
+    const bool two = t0 + 1 < ntiles;
+    const int o0 = t0 * 8 + r, o1 = o0 + 8;
+    double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const int k = k0 + c4;
+      const bool kin = k < K;
+      const double a = (r < 5 && kin) ? chi[r * ldc + k] : 0.0;
+      const double b0 = (kin && o0 < n) ? __ldg(&Ct[k * n + o0]) : 0.0;
+      dmma_m8n8k4(d00, d01, a, b0);
+      if (two) {
+        const double b1 = (kin && o1 < n) ? __ldg(&Ct[k * n + o1]) : 0.0;
+        dmma_m8n8k4(d10, d11, a, b1);
+      }
+    }
+    if (r < 5) {
+      const int oc = t0 * 8 + 2 * c4;
+      if (oc < n) D[r * n + oc] = d00;
+      if (oc + 1 < n) D[r * n + oc + 1] = d01;
+      if (two) {
+        if (oc + 8 < n) D[r * n + oc + 8] = d10;
+        if (oc + 9 < n) D[r * n + oc + 9] = d11;
+      }
     }
   }
 }

@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
         double r[3] = {Rs[3 * (base + e)], Rs[3 * (base + e) + 1], Rs[3 * (base + e) + 2]};
         basis_shells_warp(S, r, chi, ldc);
         __syncwarp();
-        contract_slices_warp(chi, ldc, S.ct[sp], n, K, Dn, part);
+        contract_dmma_warp(chi, ldc, S.ct[sp], n, K, Dn);
         __syncwarp();
         for (int o = lane; o < n; o += 32) {
           Dv[e * n + o] = Dn[o];
@@ -488,14 +488,25 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
   double rn[3];
   double g_fwd = 0.0, u_acc = 0.5;
   if (kMetropolis) {
-    double u[4];
-    rng_uniform4(cfg.seed, (uint32_t)slot, (uint32_t)mv.step, 0u, u);
-    double u2[4];
-    rng_uniform4(cfg.seed, (uint32_t)slot, (uint32_t)mv.step, 1u, u2);
-    const double two_pi = 6.283185307179586;
-    double rad0 = sqrt(-2.0 * log(u[0])), rad1 = sqrt(-2.0 * log(u[2]));
-    double z[3] = {rad0 * cos(two_pi * u[1]), rad0 * sin(two_pi * u[1]), rad1 * cos(two_pi * u[3])};
-    u_acc = u2[0];
+    // lanes 0-2 draw the three Gaussian displacements, lane 3 the acceptance
+    // uniform, each from its own Philox counter; one round trip for the warp
+    double zr, z[3];
+    {
+      const U4 c = philox4x32(U4{(uint32_t)slot, (uint32_t)mv.step, (uint32_t)(lane & 3), 0x51ED2701u}, cfg.seed);
+      // Box-Muller in single precision: the proposal only needs a Gaussian
+      // sample, not a particular one (the random streams differ from the
+      // reference's ran1 in any case)
+      const float u1 = ((float)(c.x >> 8) + 0.5f) * (1.0f / 16777216.0f);
+      const float u2 = (float)(c.y >> 8) * (1.0f / 16777216.0f);
+      const float rad = sqrtf(-2.0f * __logf(u1));
+      float sn, cs;
+      __sincosf(6.2831853f * u2, &sn, &cs);
+      zr = (lane & 3) == 3 ? u01(c.z, c.w) : (double)(rad * cs);
+    }
+    z[0] = __shfl_sync(QMCB_FULL_MASK, zr, 0);
+    z[1] = __shfl_sync(QMCB_FULL_MASK, zr, 1);
+    z[2] = __shfl_sync(QMCB_FULL_MASK, zr, 2);
+    u_acc = __shfl_sync(QMCB_FULL_MASK, zr, 3);
     double sigma = sqrt(cfg.dt);
     const double *mgo = blk + L.mgrad;
     for (int d = 0; d < 3; d++) {
@@ -591,7 +602,7 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
   // ---- basis at the new position and the new Slater / derivative rows
   basis_shells_warp(S, rn, chi, ldc);
   __syncwarp();
-  contract_slices_warp(chi, ldc, S.ct[sp], n, K, Dn, part);
+  contract_dmma_warp(chi, ldc, S.ct[sp], n, K, Dn);
   const double *InvG = blk + L.Inv[sp];
   for (int t = lane; t < n * n; t += 32) Inv[t] = InvG[t];
   __syncwarp();
@@ -817,11 +828,13 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
       DgW[(2 * n + o) * n + el] = Dn[3 * n + o];
       DlW[o * n + el] = Dn[4 * n + o];
     }
+    for (int t = lane; t < 3 * n; t += 32) blk[L.gradD + 3 * base + t] = gD[3 * base + t];
     for (int t = lane; t < 3 * N; t += 32) {
-      blk[L.gradD + t] = gD[t];
       blk[L.Ux + t] = Ux[t];
-      blk[L.grad + t] = gr[t];
       blk[L.mgrad + t] = mg[t];
+      // gradPsiRatio itself is an evaluate output; the chain needs only the
+      // modified drift (its length ratio is kept as a scalar)
+      if (!kMetropolis) blk[L.grad + t] = gr[t];
     }
     if (lane == 0) {
       sc[SC_U] = U_new;

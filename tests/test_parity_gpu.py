@@ -21,7 +21,7 @@ def test_gpu_reproduces_reference_golden(case):
     f.close()
 
 
-def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good=0.3):
+def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good=0.2):
     from oracle.evaluators import OracleEvaluator
     orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
     f = QMCB200Functions(s, W + slots_offset, qf_modification=qf, dt=dt)
