@@ -79,6 +79,9 @@ struct Layout {
   int grad;      // [N][3] gradPsiRatio
   int mgrad;     // [N][3] modifiedGradPsiRatio
   int sc;        // [kScalars]
+  // move-kernel scratch (doubles, even counts): region A, rows, factors,
+  // staged positions, staged per-electron tail, staged spin block, stride
+  int mv_region_a, mv_dn, mv_valc, mv_r, mv_tail, mv_spin[2], mv_stride;
 };
 
 struct RunCfg {
@@ -104,6 +107,26 @@ __device__ __forceinline__ double warp_max(double v)
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(QMCB_FULL_MASK, v, o));
   return v;
+}
+
+// ------------------------------------------------------------------ async copy
+// 16-byte global -> shared copies that complete in the background
+// (cp.async, LDGSTS); the warp waits on its commit groups before reading.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
+{
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int Pending>
+__device__ __forceinline__ void cp_async_wait()
+{
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(Pending) : "memory");
+}
+// `count` doubles (even; both addresses 16-byte aligned), lanes stride by 2.
+__device__ __forceinline__ void warp_copy_async(double *dst, const double *src, int count)
+{
+  for (int c = 2 * lane_id(); c < count; c += 64) cp_async16(dst + c, src + c);
 }
 
 // ------------------------------------------------------------------ RNG
@@ -421,19 +444,26 @@ __device__ __forceinline__ void contract_dmma_warp(const double *chi, int ldc, c
 {
   const int lane = lane_id(), r = lane >> 2, c4 = lane & 3;
   const int ntiles = (n + 7) >> 3;
+  constexpr int U = 4;  // k-steps whose operands are loaded before their mma
   for (int t0 = 0; t0 < ntiles; t0 += 2) {
     const bool two = t0 + 1 < ntiles;
     const int o0 = t0 * 8 + r, o1 = o0 + 8;
+    const bool in0 = o0 < n, in1 = two && o1 < n;
     double d00 = 0.0, d01 = 0.0, d10 = 0.0, d11 = 0.0;
-    for (int k0 = 0; k0 < K; k0 += 4) {
-      const int k = k0 + c4;
-      const bool kin = k < K;
-      const double a = (r < 5 && kin) ? chi[r * ldc + k] : 0.0;
-      const double b0 = (kin && o0 < n) ? __ldg(&Ct[k * n + o0]) : 0.0;
-      dmma_m8n8k4(d00, d01, a, b0);
-      if (two) {
-        const double b1 = (kin && o1 < n) ? __ldg(&Ct[k * n + o1]) : 0.0;
-        dmma_m8n8k4(d10, d11, a, b1);
+    for (int k0 = 0; k0 < K; k0 += 4 * U) {
+      double a[U], b0[U], b1[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int k = k0 + 4 * u + c4;
+        const bool kin = k < K;
+        a[u] = (r < 5 && kin) ? chi[r * ldc + k] : 0.0;
+        b0[u] = (kin && in0) ? __ldg(&Ct[k * n + o0]) : 0.0;
+        b1[u] = (kin && in1) ? __ldg(&Ct[k * n + o1]) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        dmma_m8n8k4(d00, d01, a[u], b0[u]);
+        if (two) dmma_m8n8k4(d10, d11, a[u], b1[u]);
       }
     }
     if (r < 5) {

@@ -49,14 +49,14 @@ struct EnergyCtl {
 
 // Shared-memory doubles needed by one warp.
 constexpr int kPart = 160;  // 5 quantities x 32 lanes of slice partial sums
-// Move-kernel scratch: region A holds the basis values chi[5][K]; once the
-// contraction has consumed them it is reused for the slice partial sums and
-// the new drift / modified drift (gr, mg).
-__host__ __device__ inline int move_region_a(int N, int K) { return max(5 * K, kPart + 6 * N); }
-__host__ __device__ inline int move_scratch_doubles(int N, int K, int nmax)
-{
-  return move_region_a(N, K) + 5 * nmax + nmax * nmax + nmax + 3 * 3 * N + 8;
-}
+// Move-kernel scratch per warp (sizes in Layout::mv_*, set by the host):
+// region A holds the basis values chi[5][K]; once the contraction has
+// consumed them it is reused for the slice partial sums and the new drift /
+// modified drift; then the new rows, the Sherman-Morrison factors, and the
+// staged copies of the walker's positions, per-electron arrays and the moved
+// spin's derivative rows and inverse.
+__host__ __device__ inline int even(int x) { return (x + 1) & ~1; }
+__host__ __device__ inline int move_region_a(int N, int K) { return even(max(5 * K, kPart + 6 * N)); }
 __host__ __device__ inline int full_scratch_doubles(int N, int K, int nmax)
 {
   return 5 * (K + 1) + 5 * nmax + 2 * nmax * nmax + 2 * nmax + 3 * N + kPart + 8;
@@ -452,7 +452,7 @@ struct MoveArgs {
 };
 
 template <bool kMetropolis>
-__global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+__global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, MoveArgs mv,
                                               const EnergyCtl *ectl, double *stats, EvalOut out)
 {
@@ -461,32 +461,48 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
   const int nw = d_num ? *d_num : num;
   const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
   if (wi >= nw) return;
-  const int N = S.N, K = S.K, nmax = max(S.na, S.nb);
+  const int N = S.N, K = S.K;
   const int e = mv.e;
   const int sp = e < S.na ? 0 : 1;
   const int n = sp ? S.nb : S.na, base = sp ? S.na : 0, el = e - base;
   const int slot = slots ? slots[wi] : wi;
   double *blk = state + (size_t)slot * L.stride;
-  double *sm = smem + (size_t)warp * move_scratch_doubles(N, K, nmax);
-  const int ldc = K;
-  double *chi = sm;
-  double *part = sm;                   // after the contraction's k loop
-  double *gr = sm + kPart;             // after the contraction
-  double *mg = gr + 3 * N;
-  double *Dn = sm + move_region_a(N, K);
-  double *Inv = Dn + 5 * nmax;
-  double *valc = Inv + nmax * nmax;
-  double *Ux = valc + nmax;
-  double *gD = Ux + 3 * N;
-  double *Rn = gD + 3 * N;
-  double *sc = blk + L.sc;
-  const double *Rold = blk + L.R;
 
-  for (int t = lane; t < 3 * N; t += 32) Rn[t] = Rold[t];
+  // ---- scratch of this warp (offsets in doubles, all even: 16-byte aligned)
+  double *sm = smem + (size_t)warp * L.mv_stride;
+  const int ldc = K;
+  double *chi = sm;                    // region A: basis values ...
+  double *part = sm;                   // ... then slice partial sums
+  double *gr = sm + kPart;             // ... and the new drift / modified drift
+  double *mg = gr + 3 * N;
+  double *Dn = sm + L.mv_region_a;     // new Slater / derivative rows [5][n]
+  double *valc = Dn + L.mv_dn;         // Sherman-Morrison column factors [n]
+  double *sR = valc + L.mv_valc;       // positions (electron e updated in place)
+  double *sT = sR + L.mv_r;            // gradD, Ux, grad, mgrad, scalars (prefetched copy)
+  double *sS = sT + L.mv_tail;         // inverse of the moved spin (prefetched copy)
+  double *gD = sT;                     // grad(D)/D, updated in place for the moved spin
+  double *Ux = sT + (L.Ux - L.gradD);  // grad ln J, updated in place
+  const double *mgo = sT + (L.mgrad - L.gradD);
+  const double *sc0 = sT + (L.sc - L.gradD);
+  const double *DgT = blk + L.DgT[sp];  // read once per move by the ratio sums
+  const double *DlT = blk + L.DlT[sp];
+  double *Inv = sS;
+  double *sc = blk + L.sc;
+
+  // ---- stage the walker's state: positions and the per-electron arrays
+  //      first, the moved spin's inverse as a second group that lands while
+  //      the basis and orbital rows are computed
+  warp_copy_async(sR, blk + L.R, L.mv_r);
+  warp_copy_async(sT, blk + L.gradD, L.mv_tail);
+  cp_async_commit();
+  warp_copy_async(sS, blk + L.Inv[sp], L.mv_spin[sp]);
+  cp_async_commit();
+  cp_async_wait<1>();
   __syncwarp();
-  const double ro[3] = {Rn[3 * e], Rn[3 * e + 1], Rn[3 * e + 2]};
+
+  const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3];
-  double g_fwd = 0.0, u_acc = 0.5;
+  double g_fwd = 0.0, g_unmoved = 0.0, u_acc = 0.5;
   if (kMetropolis) {
     // lanes 0-2 draw the three Gaussian displacements, lane 3 the acceptance
     // uniform, each from its own Philox counter; one round trip for the warp
@@ -507,77 +523,71 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
     z[1] = __shfl_sync(QMCB_FULL_MASK, zr, 1);
     z[2] = __shfl_sync(QMCB_FULL_MASK, zr, 2);
     u_acc = __shfl_sync(QMCB_FULL_MASK, zr, 3);
-    double sigma = sqrt(cfg.dt);
-    const double *mgo = blk + L.mgrad;
+    const double sigma = sqrt(cfg.dt);
     for (int d = 0; d < 3; d++) {
-      double drift = sigma * z[d];
+      const double drift = sigma * z[d];
       double disp = drift;
       if (cfg.sampling == 1) disp += cfg.dt * mgo[3 * e + d];
       rn[d] = ro[d] + disp;
       g_fwd += drift * drift;
     }
     if (cfg.sampling == 1) {
-      double part = 0.0;
+      // G(R -> R') includes the drift of the electrons that do not move
+      // (QMcBeaver/src/QMCWalker.cpp:383-388)
+      double prt = 0.0;
       for (int t = lane; t < 3 * N; t += 32) {
         if (t / 3 == e) continue;
-        double dd = cfg.dt * mgo[t];
-        part += dd * dd;
+        const double dd = cfg.dt * mgo[t];
+        prt += dd * dd;
       }
-      g_fwd += warp_sum(part);
+      g_unmoved = warp_sum(prt);
+      g_fwd += g_unmoved;
     }
   } else {
     for (int d = 0; d < 3; d++) rn[d] = R_in[(size_t)wi * 3 * N + 3 * e + d];
   }
-  __syncwarp();
-  if (lane == 0)
-    for (int d = 0; d < 3; d++) Rn[3 * e + d] = rn[d];
 
   // ---- incremental Jastrow + potential (QMCJastrowElectronElectron::updateOne,
-  //      QMCJastrowElectronNuclear::evaluate, QMCPotential_Energy::evaluate)
+  //      QMCJastrowElectronNuclear::evaluate, QMCPotential_Energy::evaluate);
+  //      lane j updates its own U_x[j] in place, U_x[e] is reduced afterwards
   double dU = 0, dUxx = 0, ge[3] = {0, 0, 0}, dVee = 0, dVen = 0;
-  const double *Uxo = blk + L.Ux;
+  const double uxe[3] = {Ux[3 * e], Ux[3 * e + 1], Ux[3 * e + 2]};
+  __syncwarp();
   for (int j = lane; j < N; j += 32) {
-    double uj[3] = {Uxo[3 * j], Uxo[3 * j + 1], Uxo[3 * j + 2]};
-    if (j != e) {
-      double Rj[3] = {Rold[3 * j], Rold[3 * j + 1], Rold[3 * j + 2]};
-      double dxo = ro[0] - Rj[0], dyo = ro[1] - Rj[1], dzo = ro[2] - Rj[2];
-      double dxn = rn[0] - Rj[0], dyn = rn[1] - Rj[1], dzn = rn[2] - Rj[2];
-      double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
-      double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
-      const double io = 1.0 / r_o, in_ = 1.0 / r_n;
-      dVee += in_ - io;
-      int f = ee_func(S, e, j);
-      if (f >= 0) {
-        double uo, duo, d2uo, un, dun, d2un;
-        pade_eval(S, f, r_o, uo, duo, d2uo);
-        pade_eval(S, f, r_n, un, dun, d2un);
-        dU += un - uo;
-        dUxx += 2.0 * (2.0 * in_ * dun + d2un) - 2.0 * (2.0 * io * duo + d2uo);
-        const double sn = dun * in_, so = duo * io;
-        double vx = sn * dxn - so * dxo;
-        double vy = sn * dyn - so * dyo;
-        double vz = sn * dzn - so * dzo;
-        ge[0] += vx;
-        ge[1] += vy;
-        ge[2] += vz;
-        uj[0] -= vx;
-        uj[1] -= vy;
-        uj[2] -= vz;
-      }
+    if (j == e) continue;
+    const double Rj[3] = {sR[3 * j], sR[3 * j + 1], sR[3 * j + 2]};
+    const double dxo = ro[0] - Rj[0], dyo = ro[1] - Rj[1], dzo = ro[2] - Rj[2];
+    const double dxn = rn[0] - Rj[0], dyn = rn[1] - Rj[1], dzn = rn[2] - Rj[2];
+    const double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
+    const double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
+    const double io = 1.0 / r_o, in_ = 1.0 / r_n;
+    dVee += in_ - io;
+    const int f = ee_func(S, e, j);
+    if (f >= 0) {
+      double uo, duo, d2uo, un, dun, d2un;
+      pade_eval(S, f, r_o, uo, duo, d2uo);
+      pade_eval(S, f, r_n, un, dun, d2un);
+      dU += un - uo;
+      dUxx += 2.0 * (2.0 * in_ * dun + d2un) - 2.0 * (2.0 * io * duo + d2uo);
+      const double sn = dun * in_, so = duo * io;
+      const double vx = sn * dxn - so * dxo, vy = sn * dyn - so * dyo, vz = sn * dzn - so * dzo;
+      ge[0] += vx;
+      ge[1] += vy;
+      ge[2] += vz;
+      Ux[3 * j] -= vx;
+      Ux[3 * j + 1] -= vy;
+      Ux[3 * j + 2] -= vz;
     }
-    Ux[3 * j] = uj[0];
-    Ux[3 * j + 1] = uj[1];
-    Ux[3 * j + 2] = uj[2];
   }
   for (int A = lane; A < S.M; A += 32) {
-    double4 P = S.nuc[A];
-    double dxo = ro[0] - P.x, dyo = ro[1] - P.y, dzo = ro[2] - P.z;
-    double dxn = rn[0] - P.x, dyn = rn[1] - P.y, dzn = rn[2] - P.z;
-    double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
-    double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
+    const double4 P = S.nuc[A];
+    const double dxo = ro[0] - P.x, dyo = ro[1] - P.y, dzo = ro[2] - P.z;
+    const double dxn = rn[0] - P.x, dyn = rn[1] - P.y, dzn = rn[2] - P.z;
+    const double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
+    const double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
     const double io = 1.0 / r_o, in_ = 1.0 / r_n;
     dVen -= P.w * (in_ - io);
-    int f = S.en[sp][A];
+    const int f = S.en[sp][A];
     if (f >= 0) {
       double uo, duo, d2uo, un, dun, d2un;
       pade_eval(S, f, r_o, uo, duo, d2uo);
@@ -597,18 +607,20 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
   for (int d = 0; d < 3; d++) ge[d] = warp_sum(ge[d]);
   __syncwarp();
   if (lane == 0)
-    for (int d = 0; d < 3; d++) Ux[3 * e + d] = Uxo[3 * e + d] + ge[d];
+    for (int d = 0; d < 3; d++) {
+      Ux[3 * e + d] = uxe[d] + ge[d];
+      sR[3 * e + d] = rn[d];
+    }
 
   // ---- basis at the new position and the new Slater / derivative rows
   basis_shells_warp(S, rn, chi, ldc);
   __syncwarp();
   contract_dmma_warp(chi, ldc, S.ct[sp], n, K, Dn);
-  const double *InvG = blk + L.Inv[sp];
-  for (int t = lane; t < n * n; t += 32) Inv[t] = InvG[t];
+  cp_async_wait<0>();
   __syncwarp();
 
   // ---- Sherman-Morrison row replacement (Array2D::inverseUpdateOneRow,
-  //      QMcBeaver/include/Array2D.h:1567-1610)
+  //      QMcBeaver/include/Array2D.h:1567-1610), in place on the staged inverse
   double rpart = 0.0;
   for (int o = lane; o < n; o += 32) rpart += Dn[o] * Inv[o * n + el];
   const double ratio = warp_sum(rpart);
@@ -617,7 +629,7 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
   for (int c = lane; c < n; c += 32) {
     if (c == el) continue;
     double val = 0.0;
-    for (int l = 0; l < n; l++) val += Dn[l] * Inv[l * n + c];
+    for (int l = 0; l < n; l++) val = fma(Dn[l], Inv[l * n + c], val);
     valc[c] = val * q;
   }
   __syncwarp();
@@ -639,16 +651,14 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
   __syncwarp();
 
   // ---- ratio sums of the moved spin (QMcBeaver/src/QMCSlater.cpp:741-762)
-  const double *DgT = blk + L.DgT[sp], *DlT = blk + L.DlT[sp];
+  //      lanes = (orbital slice, electron) for n <= 16
   double lp = 0.0;
   {
-    // lanes = (o-slice, electron): S2 slices of the orbital sum for n <= 16
     const int S2 = n <= 32 ? 32 / n : 1;
     const int s2 = n <= 32 ? lane / n : 0;
-    const int o0 = (n * s2) / S2, o1 = (n * (s2 + 1)) / S2;
+    const int oa = n <= 32 ? (n * s2) / S2 : 0, ob = n <= 32 ? (n * (s2 + 1)) / S2 : n;
     for (int e2 = (n <= 32 ? lane - s2 * n : lane); e2 < n && s2 < S2; e2 += (n <= 32 ? n : 32)) {
       double gx = 0, gy = 0, gz = 0, ll = 0;
-      const int oa = n <= 32 ? o0 : 0, ob = n <= 32 ? o1 : n;
       if (e2 == el) {
         for (int o = oa; o < ob; o++) {
           const double iv = Inv[o * n + el];
@@ -658,12 +668,34 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
           ll = fma(Dn[4 * n + o], iv, ll);
         }
       } else {
-        for (int o = oa; o < ob; o++) {
+        // the walker's rows stream from HBM once per move: load four
+        // orbitals' worth before using them, evict-first so the system
+        // tables keep the L1
+        int o = oa;
+        for (; o + 4 <= ob; o += 4) {
+          double g0[4], g1[4], g2[4], gl[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            g0[u] = __ldcs(&DgT[(0 * n + o + u) * n + e2]);
+            g1[u] = __ldcs(&DgT[(1 * n + o + u) * n + e2]);
+            g2[u] = __ldcs(&DgT[(2 * n + o + u) * n + e2]);
+            gl[u] = __ldcs(&DlT[(o + u) * n + e2]);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const double iv = Inv[(o + u) * n + e2];
+            gx = fma(g0[u], iv, gx);
+            gy = fma(g1[u], iv, gy);
+            gz = fma(g2[u], iv, gz);
+            ll = fma(gl[u], iv, ll);
+          }
+        }
+        for (; o < ob; o++) {
           const double iv = Inv[o * n + e2];
-          gx = fma(DgT[(0 * n + o) * n + e2], iv, gx);
-          gy = fma(DgT[(1 * n + o) * n + e2], iv, gy);
-          gz = fma(DgT[(2 * n + o) * n + e2], iv, gz);
-          ll = fma(DlT[o * n + e2], iv, ll);
+          gx = fma(__ldcs(&DgT[(0 * n + o) * n + e2]), iv, gx);
+          gy = fma(__ldcs(&DgT[(1 * n + o) * n + e2]), iv, gy);
+          gz = fma(__ldcs(&DgT[(2 * n + o) * n + e2]), iv, gz);
+          ll = fma(__ldcs(&DlT[o * n + e2]), iv, ll);
         }
       }
       lp += ll;
@@ -693,46 +725,43 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
     }
   }
   const double lapR = warp_sum(lp);
-  {
-    const int obase = sp ? 0 : S.na, on = sp ? S.na : S.nb;
-    for (int t = lane; t < 3 * on; t += 32) gD[3 * obase + t] = blk[L.gradD + 3 * obase + t];
-  }
   __syncwarp();
 
   // ---- psi quantities, quantum force, local energy
-  const double U_new = sc[SC_U] + dU, Uxx_new = sc[SC_UXX] + dUxx;
-  double lapA = sp == 0 ? lapR : sc[SC_LAPR_A];
-  double lapB = sp == 1 ? lapR : sc[SC_LAPR_B];
+  const double U_new = sc0[SC_U] + dU, Uxx_new = sc0[SC_UXX] + dUxx;
+  const double lapA = sp == 0 ? lapR : sc0[SC_LAPR_A];
+  const double lapB = sp == 1 ? lapR : sc0[SC_LAPR_B];
   double Dxx = 0.0;
   if (S.na > 0) Dxx += lapA;
   if (S.nb > 0) Dxx += lapB;
   const double lap = psi_lap_warp(N, gD, Ux, gr, Dxx, Uxx_new);
   __syncwarp();
-  const double modratio = qf_modify_warp(S, cfg, Rn, gr, mg, &bad);
-  const double Vee = sc[SC_VEE] + dVee, Ven = sc[SC_VEN] + dVen;
+  const double modratio = qf_modify_warp(S, cfg, sR, gr, mg, &bad);
+  const double Vee = sc0[SC_VEE] + dVee, Ven = sc0[SC_VEN] + dVen;
   const double PE = S.Pnn + Vee + Ven;
   const double EL = -0.5 * lap + PE;
   if (isnan(EL)) bad = true;
-  const double logdet_new = sc[SC_LOGDET_A + sp] + log(fabs(ratio));
-  const double sign_new = sc[SC_SIGN_A + sp] * (ratio < 0 ? -1.0 : 1.0);
+  const double logdet_new = sc0[SC_LOGDET_A + sp] + log(fabs(ratio));
+  const double sign_new = sc0[SC_SIGN_A + sp] * (ratio < 0 ? -1.0 : 1.0);
 
   bool accept = true;
   double p = 1.0;
   if (kMetropolis) {
-    // acceptance (QMCWalker::calculateMoveAcceptanceProbability, :1578-1654)
+    // acceptance (QMCWalker::calculateMoveAcceptanceProbability, :1578-1654);
+    // G(R' -> R): only electron e moved, the others contribute (dt v'_i)^2
     double log_g = 0.0;
     if (cfg.sampling == 1) {
       double pr = 0.0;
       for (int t = lane; t < 3 * N; t += 32) {
-        double tt = Rold[t] - Rn[t] - cfg.dt * mg[t];
+        const double tt = (t / 3 == e) ? (ro[t - 3 * e] - rn[t - 3 * e] - cfg.dt * mg[t]) : (cfg.dt * mg[t]);
         pr += tt * tt;
       }
-      double g_rev = warp_sum(pr);
+      const double g_rev = warp_sum(pr);
       log_g = -(g_rev - g_fwd) / (2.0 * cfg.dt);
     }
-    double lpr = log(fabs(ratio)) + dU;
+    const double lpr = log(fabs(ratio)) + dU;
     p = exp(2.0 * lpr + log_g);
-    const double age = sc[SC_AGE];
+    const double age = sc0[SC_AGE];
     const double over = age - cfg.old_walker_acceptance;
     if (!isnan(p)) {
       if (over > 500)
@@ -746,14 +775,14 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
     if (cfg.run_type == 1 && ratio < 0) p = 0.0;
     if (p > 1.0) p = 1.0;
     accept = p > u_acc;
-    double new_age = accept ? 0.0 : age + 1.0;
-    double w = sc[SC_WEIGHT];
+    const double new_age = accept ? 0.0 : age + 1.0;
+    double w = sc0[SC_WEIGHT];
     // reweight (QMCWalker::reweight_walker, :1060-1185), observables (:2096-2123, 2306-2387)
     if (mv.do_reweight) {
       if (cfg.run_type == 1 && mv.reweight_on) {
         const double ET = ectl->e_trial, Eest = ectl->e_est;
-        const double mo = sc[SC_MODRATIO];
-        double Eo = sc[SC_EL];
+        const double mo = sc0[SC_MODRATIO];
+        double Eo = sc0[SC_EL];
         double Et = bad ? Eo : EL;
         if (cfg.ecut == 1) {
           Et *= bad ? mo : modratio;
@@ -782,7 +811,7 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
           rw = accept ? 0.5 * (St + So) : So;
         else
           rw = p * 0.5 * (So + St) + (1.0 - p) * So;
-        double dW = exp(rw * cfg.dt_eff);
+        const double dW = exp(rw * cfg.dt_eff);
         if (new_age - cfg.old_walker_acceptance > 0)
           w *= 0.9;
         else
@@ -792,7 +821,7 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
         // at the next branching instead of poisoning the ensemble sums
         if (!isfinite(w)) w = 0.0;
       }
-      double Eobs = p * (bad ? 0.0 : EL) + (1.0 - p) * sc[SC_EL];
+      const double Eobs = p * (bad ? 0.0 : EL) + (1.0 - p) * sc0[SC_EL];
       // rel_cutoff filter of QMCWalker::calculateObservables (QMcBeaver/src/QMCWalker.cpp:2336-2351)
       const bool in_avg = fabs((Eobs - cfg.e_orig) / cfg.e_orig) < cfg.rel_cutoff;
       if (lane == 0 && w > 0.0 && in_avg) {
@@ -853,10 +882,10 @@ __global__ void __launch_bounds__(128, 6) k_move(DevSys S, Layout L, RunCfg cfg,
   }
   if (!kMetropolis) {
     if (lane == 0) {
-      const double la = sp == 0 ? logdet_new : sc[SC_LOGDET_A];
-      const double lb = sp == 1 ? logdet_new : sc[SC_LOGDET_B];
-      const double sa = sp == 0 ? sign_new : sc[SC_SIGN_A];
-      const double sb = sp == 1 ? sign_new : sc[SC_SIGN_B];
+      const double la = sp == 0 ? logdet_new : sc0[SC_LOGDET_A];
+      const double lb = sp == 1 ? logdet_new : sc0[SC_LOGDET_B];
+      const double sa = sp == 0 ? sign_new : sc0[SC_SIGN_A];
+      const double sb = sp == 1 ? sign_new : sc0[SC_SIGN_B];
       unsigned st = bad ? 1u : 0u;
       if (isnan(EL) || isnan(lap)) st |= 2u;
       if (out.log_abs_psi) out.log_abs_psi[wi] = la + lb + U_new;

@@ -504,6 +504,24 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   L.mgrad = take(3 * h->N);
   L.sc = take(kScalars);
   L.stride = (off + 31) & ~31;  // 256-byte aligned blocks
+  // move-kernel scratch: staged copies read whole padded ranges of the block
+  // (all inside the block: arrays start on 32-byte boundaries, the block is
+  // padded to 256 bytes)
+  L.mv_region_a = move_region_a(h->N, K);
+  L.mv_dn = even(5 * h->nmax);
+  L.mv_valc = even(h->nmax);
+  L.mv_r = even(3 * h->N);
+  L.mv_tail = even(L.sc + kScalars - L.gradD);
+  for (int sp = 0; sp < 2; sp++) {
+    int n = sp ? nb : na;
+    L.mv_spin[sp] = even(n * n);
+  }
+  L.mv_stride = L.mv_region_a + L.mv_dn + L.mv_valc + L.mv_r + L.mv_tail + std::max(L.mv_spin[0], L.mv_spin[1]) + 2;
+  if (L.R + L.mv_r > L.stride || L.gradD + L.mv_tail > L.stride || L.Inv[0] + L.mv_spin[0] > L.stride ||
+      L.Inv[1] + L.mv_spin[1] > L.stride) {
+    qmcb_destroy(h);
+    return fail(nullptr, QMCB_E_ARG, "qmcb_create: internal layout error (staged ranges exceed the walker block)");
+  }
 
   size_t bytes = (size_t)max_walkers * L.stride * sizeof(double);
   CKC(cudaMalloc(&h->d_state, bytes));
@@ -523,7 +541,7 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
 
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-  const size_t per_move = sizeof(double) * (size_t)move_scratch_doubles(h->N, K, h->nmax);
+  const size_t per_move = sizeof(double) * (size_t)L.mv_stride;
   const size_t per_full = sizeof(double) * (size_t)full_scratch_doubles(h->N, K, h->nmax);
   if (per_move > (size_t)max_optin || per_full > (size_t)max_optin) {
     qmcb_destroy(h);
