@@ -200,6 +200,7 @@ def main():
     import torch
     torch.cuda.set_device(local)
     from qmcbeaver_b200.api import QMCB200Functions
+    from qmcbeaver_b200.replicas import aggregate_timing, reduce_energy, replica_seed
     from qmcbeaver_b200.system import make_system
 
     system = make_system(WORKLOAD, seed=1)
@@ -210,12 +211,12 @@ def main():
     # reference keeps dW = 1 for its first 100 steps, QMcBeaver/src/QMCWalker.cpp:1071),
     # then E_T = E_est = E_orig = the equilibrated mean local energy
     eq_steps = EQUIL_SWEEPS * N
-    f = QMCB200Functions(system, 2 * W, dmc_params(seed=77 + rank, e0=-1.0, reweight_start=eq_steps))
+    f = QMCB200Functions(system, 2 * W, dmc_params(seed=replica_seed(77, rank), e0=-1.0, reweight_start=eq_steps))
     f.init_walkers(R0)
     f.run_steps(0, eq_steps)
     R_eq = f.get_walkers()["R"]
     e0 = float(np.mean(f.get_walkers()["e_local"]))
-    f.set_params(dmc_params(seed=77 + rank, e0=e0))
+    f.set_params(dmc_params(seed=replica_seed(77, rank), e0=e0))
     f.init_walkers(R_eq)
     def barrier():
         if dist is not None:
@@ -239,14 +240,10 @@ def main():
     ms = t_start.elapsed_time(t_end)
     ks = f.kernel_stats(reset=True)
     f.set_profiling(False)
-    moves = st.n_moves
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        m = torch.tensor([moves], device="cuda", dtype=torch.float64)
-        dist.all_reduce(m, op=dist.ReduceOp.SUM)
-        ms, moves = float(t.item()), float(m.item())
+    ms, moves = aggregate_timing(ms, st.n_moves)
     value = moves / (ms / 1e3)
+    ensemble = reduce_energy(st.sum_weight, st.sum_weight_energy, st.sum_weight_energy2, st.n_walkers,
+                             st.final_weight)
 
     # roofline of the move kernel (dominant): algorithmic bytes per launch / launch time
     mv = ks["move"]
@@ -267,7 +264,7 @@ def main():
     from qmcbeaver_b200.desc import RunParams, StepStats
     import ctypes
     barrier()
-    p = dmc_params(seed=77 + rank, e0=e0)
+    p = dmc_params(seed=replica_seed(77, rank), e0=e0)
     e_est = e0
     sw = swe = 0.0
     step0 = args.warmup + args.steps
@@ -289,12 +286,7 @@ def main():
             p.energy_trial = e_est
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        m = torch.tensor([e2e_moves], device="cuda", dtype=torch.float64)
-        dist.all_reduce(m, op=dist.ReduceOp.SUM)
-        e2e_s, e2e_moves = float(t.item()), float(m.item())
+    e2e_s, e2e_moves = aggregate_timing(e2e_s, e2e_moves)
     e2e = {"value": e2e_moves / e2e_s, "unit": "walker-moves/s", "h2d_bytes_per_step": ctypes.sizeof(RunParams),
            "d2h_bytes_per_step": ctypes.sizeof(StepStats) + 16,
            "api": "qmcb_set_params + qmcb_run_steps(step, 1) per step (host E_T in, step statistics out)"}
@@ -328,7 +320,7 @@ def main():
                       "l2": "walker state > L2 (%.0f MB per GPU)" % (2 * W * f.lay_bytes() / 1e6)
                       if hasattr(f, "lay_bytes") else "walker state larger than L2"},
            "roofline": roofline, "gpu_launches": launches, "kernels": ks, "e2e": e2e, "e2e_evaluate_api": e2e_eval,
-           "energy": {"mean_weighted_E_L": st.sum_weight_energy / st.sum_weight if st.sum_weight > 0 else None,
+           "energy": {"mean_weighted_E_L": ensemble["energy"], "walkers_all_ranks": ensemble["walkers"],
                       "acceptance": st.sum_accept / max(st.n_moves, 1), "singular": st.n_singular}}
     clocks = clk.summary()
     if clocks is not None:
