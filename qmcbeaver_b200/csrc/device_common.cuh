@@ -59,6 +59,7 @@ struct DevSys {
   const double *pexp;    // [P] exponents
   const double *pcoef;   // [P] coefficients
   const double *ct[2];   // [K][n_s] MO coefficients, transposed
+  const float *ctf[2];   // the same in FP32 (mixed-precision path)
   const double *pade;    // [npade][2][kPadeMax] numerator, denominator
   const int2 *pade_len;  // [npade] numerator length, denominator length
   const int *en[2];      // [M] e-n function per spin
@@ -248,48 +249,11 @@ __device__ __forceinline__ double ipow(double x, int a)
   return r;
 }
 
-__device__ __forceinline__ void basis_one(const DevSys &S, int k, const double r[3], double out[5])
+__device__ __forceinline__ float ipowf(float x, int a)
 {
-  int4 info = __ldg(&S.bf[k]);
-  int a = info.y & 0xff, b = (info.y >> 8) & 0xff, c = (info.y >> 16) & 0xff;
-  double4 A = S.nuc[info.x];
-  double x = r[0] - A.x, y = r[1] - A.y, z = r[2] - A.z;
-  double x2 = x * x, y2 = y * y, z2 = z * z;
-  double r_sq = x2 + y2 + z2;
-  double poly = ipow(x, a) * ipow(y, b) * ipow(z, c);
-  double ax = a ? a / x : 0.0, by = b ? b / y : 0.0, cz = c ? c / z : 0.0;
-  double axx = a > 1 ? a * (a - 1.0) / x2 : 0.0;
-  double byy = b > 1 ? b * (b - 1.0) / y2 : 0.0;
-  double czz = c > 1 ? c * (c - 1.0) / z2 : 0.0;
-  double L46 = 4.0 * (a + b + c) + 6.0;
-  double v = 0, gx = 0, gy = 0, gz = 0, l = 0;
-  for (int i = 0; i < info.z; i++) {
-    double2 p = __ldg(&S.prim[info.w + i]);
-    double al = p.x;
-    double e = exp(-al * r_sq) * p.y * poly;
-    double t3 = -2.0 * al;
-    v += e;
-    gx += e * (ax + t3 * x);
-    gy += e * (by + t3 * y);
-    gz += e * (cz + t3 * z);
-    l += e * (axx + byy + czz - al * L46 + 4.0 * r_sq * al * al);
-  }
-  out[0] = v;
-  out[1] = gx;
-  out[2] = gy;
-  out[3] = gz;
-  out[4] = l;
-}
-
-// All K functions at position r; chi[q*ldc + k], q = val, gx, gy, gz, lap.
-__device__ __forceinline__ void basis_warp(const DevSys &S, const double r[3], double *chi, int ldc)
-{
-  for (int k = lane_id(); k < S.K; k += 32) {
-    double o[5];
-    basis_one(S, k, r, o);
-#pragma unroll
-    for (int q = 0; q < 5; q++) chi[q * ldc + k] = o[q];
-  }
+  float r = 1.0f;
+  for (int i = 0; i < a; i++) r *= x;
+  return r;
 }
 
 // Basis functions of all shells at position r (lanes over shells).  A shell
@@ -375,57 +339,6 @@ __device__ __forceinline__ void basis_shells_warp(const DevSys &S, const double 
   }
 }
 
-// D[q][o] = sum_k chi[q][k] Ct[k][o] with lanes split into K-slices of n
-// orbitals each (n <= 32): every lane keeps five independent accumulators;
-// the slices' partial sums meet in `part` (5 * 32 doubles).
-__device__ __forceinline__ void contract_slices_warp(const double *chi, int ldc, const double *__restrict__ Ct, int n,
-                                                     int K, double *D, double *part)
-{
-  const int lane = lane_id();
-  if (n <= 32) {
-    const int S = 32 / n, s = lane / n, o = lane - s * n;
-    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (s < S) {
-      const int k0 = (K * s) / S, k1 = (K * (s + 1)) / S;
-      for (int k = k0; k < k1; k++) {
-        const double cf = __ldg(&Ct[k * n + o]);
-#pragma unroll
-        for (int q = 0; q < 5; q++) acc[q] = fma(chi[q * ldc + k], cf, acc[q]);
-      }
-    }
-    if (S == 1) {
-      if (s < S)
-#pragma unroll
-        for (int q = 0; q < 5; q++) D[q * n + o] = acc[q];
-    } else {
-      __syncwarp();  // part may alias chi: every lane is done reading it
-      if (s < S)
-#pragma unroll
-        for (int q = 0; q < 5; q++) part[(s * 5 + q) * n + o] = acc[q];
-      __syncwarp();
-      if (lane < n) {
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-          double t = 0.0;
-          for (int ss = 0; ss < S; ss++) t += part[(ss * 5 + q) * n + lane];
-          D[q * n + lane] = t;
-        }
-      }
-    }
-  } else {
-    for (int o = lane; o < n; o += 32) {
-      double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-      for (int k = 0; k < K; k++) {
-        const double cf = __ldg(&Ct[k * n + o]);
-#pragma unroll
-        for (int q = 0; q < 5; q++) acc[q] = fma(chi[q * ldc + k], cf, acc[q]);
-      }
-#pragma unroll
-      for (int q = 0; q < 5; q++) D[q * n + o] = acc[q];
-    }
-  }
-}
-
 // FP64 tensor-core tile D(8x8) += A(8x4) B(4x8), mma.sync m8n8k4 (row.col).
 // Fragments: a = A[lane/4][lane%4], b = B[lane%4][lane/4],
 // d0,d1 = D[lane/4][2(lane%4)], D[lane/4][2(lane%4)+1].
@@ -478,17 +391,140 @@ __device__ __forceinline__ void contract_dmma_warp(const double *chi, int ldc, c
   }
 }
 
-// D[q][o] = sum_k chi[q][k] * Ct[k][o] for q < 5, o < n  (the orbital
-// contraction of QMCSlater::evaluate, QMcBeaver/src/QMCSlater.cpp:856-862).
-__device__ __forceinline__ void contract_warp(const double *chi, int ldc, const double *Ct, int n, int K,
-                                              double *D)
+// ------------------------------------------------------------------ FP32
+// Single-precision basis for the mixed-precision path: the same shell
+// formulas as basis_shells_warp with exp on the special-function unit.
+__device__ __forceinline__ void basis_shells_warp_f(const DevSys &S, const double r[3], float *chi, int ldc)
 {
-  for (int t = lane_id(); t < 5 * n; t += 32) {
-    int q = t / n, o = t - q * n;
-    const double *cq = chi + q * ldc;
-    double acc = 0.0;
-    for (int k = 0; k < K; k++) acc = fma(cq[k], Ct[k * n + o], acc);
-    D[t] = acc;
+  for (int si = lane_id(); si < S.nshell; si += 32) {
+    const int4 sh = __ldg(&S.shell[si]);
+    const double4 A = S.nuc[sh.x];
+    const float x = (float)(r[0] - A.x), y = (float)(r[1] - A.y), z = (float)(r[2] - A.z);
+    const float r2 = x * x + y * y + z * z;
+    const int nmem = sh.z & 0xff, L = (sh.z >> 8) & 0xff, np = sh.z >> 16;
+    const float Lf = 4.0f * L + 6.0f, r2x4 = 4.0f * r2;
+    // exp(-a r^2) with the exponent formed in FP64 and split into an
+    // integer power of two and a fraction in [0, 1): FP32 rounding of a large
+    // argument a r^2 would otherwise cost |a r^2| * 6e-8 relative accuracy
+    const double r2d = (r[0] - A.x) * (r[0] - A.x) + (r[1] - A.y) * (r[1] - A.y) + (r[2] - A.z) * (r[2] - A.z);
+    float ex[kShellPrim], al[kShellPrim];
+#pragma unroll
+    for (int i = 0; i < kShellPrim; i++) {
+      al[i] = 0.0f;
+      ex[i] = 0.0f;
+      if (i < np && np <= kShellPrim) {
+        const double ad = __ldg(&S.pexp[sh.w + i]);
+        al[i] = (float)ad;
+        const double t = -ad * r2d * 1.4426950408889634;  // log2(e)
+        const double fl = floor(t);
+        ex[i] = fl < -150.0 ? 0.0f : ldexpf(exp2f((float)(t - fl)), (int)fl);
+      }
+    }
+    for (int m = 0; m < nmem; m++) {
+      const int k = sh.y + m;
+      const int2 f = __ldg(&S.fn[k]);
+      const int a = f.x & 0xff, b = (f.x >> 8) & 0xff, c = (f.x >> 16) & 0xff;
+      const double *co = S.pcoef + f.y;
+      float E0 = 0.0f, E1 = 0.0f, El = 0.0f;
+      if (np <= kShellPrim) {
+#pragma unroll
+        for (int i = 0; i < kShellPrim; i++) {
+          if (i < np) {
+            const float e = (float)__ldg(&co[i]) * ex[i];
+            E0 += e;
+            E1 = fmaf(e, al[i], E1);
+            El = fmaf(e, al[i] * fmaf(r2x4, al[i], -Lf), El);
+          }
+        }
+      } else {
+        for (int i = 0; i < np; i++) {
+          const float ai = (float)__ldg(&S.pexp[sh.w + i]);
+          const float e = (float)__ldg(&co[i]) * __expf(-ai * r2);
+          E0 += e;
+          E1 = fmaf(e, ai, E1);
+          El = fmaf(e, ai * fmaf(r2x4, ai, -Lf), El);
+        }
+      }
+      const float xa = ipowf(x, a), yb = ipowf(y, b), zc = ipowf(z, c);
+      const float P = xa * yb * zc;
+      const float Px = a ? a * ipowf(x, a - 1) * yb * zc : 0.0f;
+      const float Py = b ? b * xa * ipowf(y, b - 1) * zc : 0.0f;
+      const float Pz = c ? c * xa * yb * ipowf(z, c - 1) : 0.0f;
+      float Pl = 0.0f;
+      if (a > 1) Pl += a * (a - 1.0f) * ipowf(x, a - 2) * yb * zc;
+      if (b > 1) Pl += b * (b - 1.0f) * xa * ipowf(y, b - 2) * zc;
+      if (c > 1) Pl += c * (c - 1.0f) * xa * yb * ipowf(z, c - 2);
+      const float PE1 = P * E1;
+      chi[0 * ldc + k] = E0 * P;
+      chi[1 * ldc + k] = fmaf(E0, Px, -2.0f * x * PE1);
+      chi[2 * ldc + k] = fmaf(E0, Py, -2.0f * y * PE1);
+      chi[3 * ldc + k] = fmaf(E0, Pz, -2.0f * z * PE1);
+      chi[4 * ldc + k] = fmaf(E0, Pl, P * El);
+    }
+  }
+}
+
+// D[q][o] = sum_k chi[q][k] Ct[k][o] in FP32 with lanes split into K-slices
+// of n orbitals (n <= 32), five independent accumulators per lane; the
+// slices' partial sums meet in `part` (5 * 32 floats).
+__device__ __forceinline__ void contract_slices_warp_f(const float *chi, int ldc, const float *__restrict__ Ct, int n,
+                                                       int K, float *D, float *part)
+{
+  // FP32 operands, FP64 accumulation: each product of two FP32 values is
+  // exact in FP64, so the sum carries no cancellation loss
+  const int lane = lane_id();
+  double *dpart = (double *)part;
+  if (n <= 32) {
+    const int S = 32 / n, s = lane / n, o = lane - s * n;
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (s < S) {
+      const int k0 = (K * s) / S, k1 = (K * (s + 1)) / S;
+      int k = k0;
+      for (; k + 4 <= k1; k += 4) {
+        float cf[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) cf[u] = __ldg(&Ct[(k + u) * n + o]);
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+          for (int q = 0; q < 5; q++) acc[q] = fma((double)chi[q * ldc + k + u], (double)cf[u], acc[q]);
+      }
+      for (; k < k1; k++) {
+        const double cf = (double)__ldg(&Ct[k * n + o]);
+#pragma unroll
+        for (int q = 0; q < 5; q++) acc[q] = fma((double)chi[q * ldc + k], cf, acc[q]);
+      }
+    }
+    __syncwarp();  // part may alias chi
+    if (S == 1) {
+      if (s < S)
+#pragma unroll
+        for (int q = 0; q < 5; q++) D[q * n + o] = (float)acc[q];
+    } else {
+      if (s < S)
+#pragma unroll
+        for (int q = 0; q < 5; q++) dpart[(s * 5 + q) * n + o] = acc[q];
+      __syncwarp();
+      if (lane < n) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+          double t = 0.0;
+          for (int ss = 0; ss < S; ss++) t += dpart[(ss * 5 + q) * n + lane];
+          D[q * n + lane] = (float)t;
+        }
+      }
+    }
+  } else {
+    for (int o = lane; o < n; o += 32) {
+      double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int k = 0; k < K; k++) {
+        const double cf = (double)__ldg(&Ct[k * n + o]);
+#pragma unroll
+        for (int q = 0; q < 5; q++) acc[q] = fma((double)chi[q * ldc + k], cf, acc[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 5; q++) D[q * n + o] = (float)acc[q];
+    }
   }
 }
 

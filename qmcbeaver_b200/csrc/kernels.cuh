@@ -298,6 +298,7 @@ __device__ inline double psi_lap_warp(int N, const double *gD, const double *Ux,
 // Full evaluation (do_basis = true: QMCSCFJastrow::evaluate with whichE = -1)
 // or refresh from the stored Slater values (do_basis = false).
 // R_in: [num][N][3] positions to store first (null: use the stored ones).
+template <typename TS, typename TI>
 __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, int do_basis,
                                               EvalOut out)
@@ -338,7 +339,9 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
       sc[SC_SIGN_A + sp] = 1.0;
       continue;
     }
-    double *Dv = blk + L.Dv[sp], *DgT = blk + L.DgT[sp], *DlT = blk + L.DlT[sp];
+    // stored Slater rows in the state precision TS; the basis, LU and ratio
+    // sums here always run in FP64 (this is the refresh of the mixed path)
+    TS *Dv = (TS *)(blk + L.Dv[sp]), *DgT = (TS *)(blk + L.DgT[sp]), *DlT = (TS *)(blk + L.DlT[sp]);
     if (do_basis) {
       for (int e = 0; e < n; e++) {
         double r[3] = {Rs[3 * (base + e)], Rs[3 * (base + e) + 1], Rs[3 * (base + e) + 2]};
@@ -347,32 +350,32 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
         contract_dmma_warp(chi, ldc, S.ct[sp], n, K, Dn);
         __syncwarp();
         for (int o = lane; o < n; o += 32) {
-          Dv[e * n + o] = Dn[o];
-          DgT[(0 * n + o) * n + e] = Dn[n + o];
-          DgT[(1 * n + o) * n + e] = Dn[2 * n + o];
-          DgT[(2 * n + o) * n + e] = Dn[3 * n + o];
-          DlT[o * n + e] = Dn[4 * n + o];
+          Dv[e * n + o] = (TS)Dn[o];
+          DgT[(0 * n + o) * n + e] = (TS)Dn[n + o];
+          DgT[(1 * n + o) * n + e] = (TS)Dn[2 * n + o];
+          DgT[(2 * n + o) * n + e] = (TS)Dn[3 * n + o];
+          DlT[o * n + e] = (TS)Dn[4 * n + o];
         }
         __syncwarp();
       }
     }
-    for (int t = lane; t < n * n; t += 32) A[t] = Dv[t];
+    for (int t = lane; t < n * n; t += 32) A[t] = (double)Dv[t];
     __syncwarp();
     double logdet, sign;
     bool ok = lu_inverse_warp(A, X, vv, piv, n, logdet, sign);
     if (!ok) bad = true;
-    double *Inv = blk + L.Inv[sp];
-    for (int t = lane; t < n * n; t += 32) Inv[t] = X[t];
+    TI *Inv = (TI *)(blk + L.Inv[sp]);
+    for (int t = lane; t < n * n; t += 32) Inv[t] = (TI)X[t];
     // ratio sums (QMcBeaver/src/QMCSlater.cpp:741-762)
     double lp = 0.0;
     for (int e = lane; e < n; e += 32) {
       double gx = 0, gy = 0, gz = 0;
       for (int o = 0; o < n; o++) {
         double iv = X[o * n + e];
-        lp += DlT[o * n + e] * iv;
-        gx += DgT[(0 * n + o) * n + e] * iv;
-        gy += DgT[(1 * n + o) * n + e] * iv;
-        gz += DgT[(2 * n + o) * n + e] * iv;
+        lp += (double)DlT[o * n + e] * iv;
+        gx += (double)DgT[(0 * n + o) * n + e] * iv;
+        gy += (double)DgT[(1 * n + o) * n + e] * iv;
+        gz += (double)DgT[(2 * n + o) * n + e] * iv;
       }
       blk[L.gradD + 3 * (base + e)] = gx;
       blk[L.gradD + 3 * (base + e) + 1] = gy;
@@ -451,7 +454,7 @@ struct MoveArgs {
   int reweight_on;   // step >= reweight_start_step
 };
 
-template <bool kMetropolis>
+template <bool kMetropolis, typename TS, typename TI>
 __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, MoveArgs mv,
                                               const EnergyCtl *ectl, double *stats, EvalOut out)
@@ -471,23 +474,25 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
   // ---- scratch of this warp (offsets in doubles, all even: 16-byte aligned)
   double *sm = smem + (size_t)warp * L.mv_stride;
   const int ldc = K;
-  double *chi = sm;                    // region A: basis values ...
-  double *part = sm;                   // ... then slice partial sums
+  TS *chi = (TS *)sm;                  // region A: basis values ...
+  TS *cpart = (TS *)sm;                // ... then contraction slice sums
+  double *part = sm;                   // ... then ratio-sum slice sums
   double *gr = sm + kPart;             // ... and the new drift / modified drift
   double *mg = gr + 3 * N;
-  double *Dn = sm + L.mv_region_a;     // new Slater / derivative rows [5][n]
-  double *valc = Dn + L.mv_dn;         // Sherman-Morrison column factors [n]
-  double *sR = valc + L.mv_valc;       // positions (electron e updated in place)
+  TS *Dn = (TS *)(sm + L.mv_region_a); // new Slater / derivative rows [5][n]
+  TI *valc = (TI *)(sm + L.mv_region_a + L.mv_dn);  // Sherman-Morrison factors [n]
+  double *sR = sm + L.mv_region_a + L.mv_dn + L.mv_valc;  // positions (electron e updated in place)
   double *sT = sR + L.mv_r;            // gradD, Ux, grad, mgrad, scalars (prefetched copy)
   double *sS = sT + L.mv_tail;         // inverse of the moved spin (prefetched copy)
   double *gD = sT;                     // grad(D)/D, updated in place for the moved spin
   double *Ux = sT + (L.Ux - L.gradD);  // grad ln J, updated in place
   const double *mgo = sT + (L.mgrad - L.gradD);
   const double *sc0 = sT + (L.sc - L.gradD);
-  const double *DgT = blk + L.DgT[sp];  // read once per move by the ratio sums
-  const double *DlT = blk + L.DlT[sp];
-  double *Inv = sS;
+  const TS *DgT = (const TS *)(blk + L.DgT[sp]);  // read once per move by the ratio sums
+  const TS *DlT = (const TS *)(blk + L.DlT[sp]);
+  TI *Inv = (TI *)sS;
   double *sc = blk + L.sc;
+  const int inv_d = even((n * n * (int)sizeof(TI) + 7) / 8);
 
   // ---- stage the walker's state: positions and the per-electron arrays
   //      first, the moved spin's inverse as a second group that lands while
@@ -495,7 +500,7 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
   warp_copy_async(sR, blk + L.R, L.mv_r);
   warp_copy_async(sT, blk + L.gradD, L.mv_tail);
   cp_async_commit();
-  warp_copy_async(sS, blk + L.Inv[sp], L.mv_spin[sp]);
+  warp_copy_async(sS, blk + L.Inv[sp], inv_d);
   cp_async_commit();
   cp_async_wait<1>();
   __syncwarp();
@@ -613,41 +618,49 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
     }
 
   // ---- basis at the new position and the new Slater / derivative rows
-  basis_shells_warp(S, rn, chi, ldc);
-  __syncwarp();
-  contract_dmma_warp(chi, ldc, S.ct[sp], n, K, Dn);
+  if constexpr (sizeof(TS) == 8) {
+    basis_shells_warp(S, rn, (double *)chi, ldc);
+    __syncwarp();
+    contract_dmma_warp((const double *)chi, ldc, S.ct[sp], n, K, (double *)Dn);
+  } else {
+    basis_shells_warp_f(S, rn, (float *)chi, ldc);
+    __syncwarp();
+    contract_slices_warp_f((const float *)chi, ldc, S.ctf[sp], n, K, (float *)Dn, (float *)cpart);
+  }
   cp_async_wait<0>();
   __syncwarp();
 
   // ---- Sherman-Morrison row replacement (Array2D::inverseUpdateOneRow,
   //      QMcBeaver/include/Array2D.h:1567-1610), in place on the staged inverse
+  // determinant ratio accumulated in FP64; the inverse update itself runs
+  // in the state precision TS
   double rpart = 0.0;
-  for (int o = lane; o < n; o += 32) rpart += Dn[o] * Inv[o * n + el];
+  for (int o = lane; o < n; o += 32) rpart = fma((double)Dn[o], (double)Inv[o * n + el], rpart);
   const double ratio = warp_sum(rpart);
   bool bad = !(ratio != 0.0) || !isfinite(ratio);
   const double q = 1.0 / ratio;
   for (int c = lane; c < n; c += 32) {
     if (c == el) continue;
-    double val = 0.0;
-    for (int l = 0; l < n; l++) val = fma(Dn[l], Inv[l * n + c], val);
-    valc[c] = val * q;
+    TI val = (TI)0;
+    for (int l = 0; l < n; l++) val = fma((TI)Dn[l], Inv[l * n + c], val);
+    valc[c] = (TI)(val * q);
   }
   __syncwarp();
   if (n <= 32) {
     const int rpp = 32 / n, r0 = lane / n, c = lane - r0 * n;
     if (r0 < rpp && c != el) {
-      const double vc = valc[c];
+      const TI vc = valc[c];
       for (int r = r0; r < n; r += rpp) Inv[r * n + c] -= vc * Inv[r * n + el];
     }
   } else {
     for (int c = lane; c < n; c += 32) {
       if (c == el) continue;
-      const double vc = valc[c];
+      const TI vc = valc[c];
       for (int r = 0; r < n; r++) Inv[r * n + c] -= vc * Inv[r * n + el];
     }
   }
   __syncwarp();
-  for (int r = lane; r < n; r += 32) Inv[r * n + el] *= q;
+  for (int r = lane; r < n; r += 32) Inv[r * n + el] = (TI)(Inv[r * n + el] * q);
   __syncwarp();
 
   // ---- ratio sums of the moved spin (QMcBeaver/src/QMCSlater.cpp:741-762)
@@ -661,11 +674,11 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
       double gx = 0, gy = 0, gz = 0, ll = 0;
       if (e2 == el) {
         for (int o = oa; o < ob; o++) {
-          const double iv = Inv[o * n + el];
-          gx = fma(Dn[n + o], iv, gx);
-          gy = fma(Dn[2 * n + o], iv, gy);
-          gz = fma(Dn[3 * n + o], iv, gz);
-          ll = fma(Dn[4 * n + o], iv, ll);
+          const double iv = (double)Inv[o * n + el];
+          gx = fma((double)Dn[n + o], iv, gx);
+          gy = fma((double)Dn[2 * n + o], iv, gy);
+          gz = fma((double)Dn[3 * n + o], iv, gz);
+          ll = fma((double)Dn[4 * n + o], iv, ll);
         }
       } else {
         // the walker's rows stream from HBM once per move: load four
@@ -673,7 +686,7 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
         // tables keep the L1
         int o = oa;
         for (; o + 4 <= ob; o += 4) {
-          double g0[4], g1[4], g2[4], gl[4];
+          TS g0[4], g1[4], g2[4], gl[4];
 #pragma unroll
           for (int u = 0; u < 4; u++) {
             g0[u] = __ldcs(&DgT[(0 * n + o + u) * n + e2]);
@@ -683,19 +696,19 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
           }
 #pragma unroll
           for (int u = 0; u < 4; u++) {
-            const double iv = Inv[(o + u) * n + e2];
-            gx = fma(g0[u], iv, gx);
-            gy = fma(g1[u], iv, gy);
-            gz = fma(g2[u], iv, gz);
-            ll = fma(gl[u], iv, ll);
+            const double iv = (double)Inv[(o + u) * n + e2];
+            gx = fma((double)g0[u], iv, gx);
+            gy = fma((double)g1[u], iv, gy);
+            gz = fma((double)g2[u], iv, gz);
+            ll = fma((double)gl[u], iv, ll);
           }
         }
         for (; o < ob; o++) {
-          const double iv = Inv[o * n + e2];
-          gx = fma(__ldcs(&DgT[(0 * n + o) * n + e2]), iv, gx);
-          gy = fma(__ldcs(&DgT[(1 * n + o) * n + e2]), iv, gy);
-          gz = fma(__ldcs(&DgT[(2 * n + o) * n + e2]), iv, gz);
-          ll = fma(__ldcs(&DlT[o * n + e2]), iv, ll);
+          const double iv = (double)Inv[o * n + e2];
+          gx = fma((double)__ldcs(&DgT[(0 * n + o) * n + e2]), iv, gx);
+          gy = fma((double)__ldcs(&DgT[(1 * n + o) * n + e2]), iv, gy);
+          gz = fma((double)__ldcs(&DgT[(2 * n + o) * n + e2]), iv, gz);
+          ll = fma((double)__ldcs(&DlT[o * n + e2]), iv, ll);
         }
       }
       lp += ll;
@@ -847,9 +860,9 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
   if (accept) {
     double *Rw = blk + L.R;
     if (lane < 3) Rw[3 * e + lane] = rn[lane];
-    double *InvW = blk + L.Inv[sp];
+    TI *InvW = (TI *)(blk + L.Inv[sp]);
     for (int t = lane; t < n * n; t += 32) InvW[t] = Inv[t];
-    double *Dv = blk + L.Dv[sp], *DgW = blk + L.DgT[sp], *DlW = blk + L.DlT[sp];
+    TS *Dv = (TS *)(blk + L.Dv[sp]), *DgW = (TS *)(blk + L.DgT[sp]), *DlW = (TS *)(blk + L.DlT[sp]);
     for (int o = lane; o < n; o += 32) {
       Dv[el * n + o] = Dn[o];
       DgW[(0 * n + o) * n + el] = Dn[n + o];

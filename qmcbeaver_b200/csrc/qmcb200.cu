@@ -21,6 +21,12 @@
 
 using namespace qmcb;
 
+// Mixed precision: FP32 basis values, orbital rows and contraction; the
+// inverse and its Sherman-Morrison update in MIXED_TI.
+#ifndef MIXED_TI
+#define MIXED_TI double
+#endif
+
 namespace {
 
 const int kMaxWarpsPerBlock = 4;
@@ -41,6 +47,7 @@ struct qmcb_handle {
   int4 *d_bf = nullptr;
   double2 *d_prim = nullptr;
   double *d_ct[2] = {nullptr, nullptr};
+  float *d_ctf[2] = {nullptr, nullptr};
   double *d_pade = nullptr;
   int2 *d_pade_len = nullptr;
   double2 *d_pade_ab = nullptr;
@@ -62,6 +69,7 @@ struct qmcb_handle {
   size_t smem_move = 0, smem_full = 0;
   int wpb_move = 1, wpb_full = 1;  // warps (walkers) per CTA of k_move / k_full
   bool evaluated_once = false;
+  int state_prec = -1;  // precision the stored walker state was written in
   // kernel timing (qmcb_set_profiling)
   bool prof = false;
   std::vector<cudaEvent_t> prof_ev;
@@ -450,6 +458,10 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(upload(&h->d_pcoef, pcoef));
   CKC(upload(&h->d_ct[0], ct[0]));
   CKC(upload(&h->d_ct[1], ct[1]));
+  for (int sp = 0; sp < 2; sp++) {
+    std::vector<float> cf(ct[sp].begin(), ct[sp].end());
+    CKC(upload(&h->d_ctf[sp], cf));
+  }
   CKC(upload(&h->d_pade, pade));
   CKC(upload(&h->d_pade_len, plen));
   CKC(upload(&h->d_pade_ab, pade_ab));
@@ -475,6 +487,8 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   S.pcoef = h->d_pcoef;
   S.ct[0] = h->d_ct[0];
   S.ct[1] = h->d_ct[1];
+  S.ctf[0] = h->d_ctf[0];
+  S.ctf[1] = h->d_ctf[1];
   S.pade = h->d_pade;
   S.pade_len = h->d_pade_len;
   S.pade_ab = h->d_pade_ab;
@@ -551,9 +565,12 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   h->wpb_full = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_full);
   h->smem_move = per_move * h->wpb_move;
   h->smem_full = per_full * h->wpb_full;
-  CKC(cudaFuncSetAttribute(k_move<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
-  CKC(cudaFuncSetAttribute(k_move<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
-  CKC(cudaFuncSetAttribute(k_full, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_full));
+  CKC(cudaFuncSetAttribute(k_move<true, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
+  CKC(cudaFuncSetAttribute(k_move<false, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
+  CKC(cudaFuncSetAttribute(k_move<true, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
+  CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
+  CKC(cudaFuncSetAttribute(k_full<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_full));
+  CKC(cudaFuncSetAttribute(k_full<float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_full));
 #undef CKC
   *out = h;
   return QMCB_OK;
@@ -563,7 +580,7 @@ int qmcb_destroy(qmcb_handle *h)
 {
   if (!h) return QMCB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *ptrs[] = {h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
+  void *ptrs[] = {h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
                   h->d_copies, h->d_stats, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
   for (void *p : ptrs)
@@ -584,7 +601,8 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
       p->qf_modification > 2 || p->energy_modification < 0 || p->energy_modification > 2 || p->reweighting < 0 ||
       p->reweighting > 2 || p->energy_cutoff < 0 || p->energy_cutoff > 2)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");
-  if (p->precision != QMCB_PREC_FP64) return fail(h, QMCB_E_ARG, "qmcb_set_params: only QMCB_PREC_FP64 in this build");
+  if (p->precision != QMCB_PREC_FP64 && p->precision != QMCB_PREC_MIXED)
+    return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown precision");
   h->params = *p;
   if (h->n_live_host > 0) {
     // the host's E_T / E_est feed the next steps (QMCManager::updateTrialEnergy)
@@ -620,18 +638,31 @@ static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num,
                        cudaStream_t st)
 {
   RunCfg cfg = make_cfg(h->params);
+  const bool mixed = h->params.precision == QMCB_PREC_MIXED;
   if (which_e < 0) {
     int blocks = (num + h->wpb_full - 1) / h->wpb_full;
-    k_full<<<blocks, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
-                                                              nullptr, d_R, 1, o);
+    if (mixed)
+      k_full<float, MIXED_TI><<<blocks, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
+                                                                    nullptr, d_R, 1, o);
+    else
+      k_full<double, double><<<blocks, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
+                                                                     nullptr, d_R, 1, o);
   } else {
+    if (h->state_prec != h->params.precision)
+      return fail(h, QMCB_E_STATE, "evaluate: walker state was written in another precision; evaluate all electrons first");
     MoveArgs mv{which_e, 0, 0, 0};
     int blocks = (num + h->wpb_move - 1) / h->wpb_move;
-    k_move<false><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
-                                                                     num, nullptr, d_R, mv, h->d_ectl,
-                                                                     h->d_stats, o);
+    if (mixed)
+      k_move<false, float, MIXED_TI><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
+                                                                          num, nullptr, d_R, mv, h->d_ectl,
+                                                                          h->d_stats, o);
+    else
+      k_move<false, double, double><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
+                                                                           num, nullptr, d_R, mv, h->d_ectl,
+                                                                           h->d_stats, o);
   }
   CK(cudaGetLastError());
+  if (which_e < 0) h->state_prec = h->params.precision;
   return QMCB_OK;
 }
 
@@ -724,6 +755,9 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
   if (!h) return QMCB_E_ARG;
   if (n_steps < 0 || first_step < 0) return fail(h, QMCB_E_ARG, "qmcb_run_steps: bad step range");
   if (!h->evaluated_once) return fail(h, QMCB_E_STATE, "qmcb_run_steps: call qmcb_init_walkers first");
+  if (h->state_prec != h->params.precision)
+    return fail(h, QMCB_E_STATE, "qmcb_run_steps: walker state was written in another precision; call qmcb_init_walkers");
+  const bool mixed = h->params.precision == QMCB_PREC_MIXED;
   if (h->n_live_host <= 0) return fail(h, QMCB_E_STATE, "qmcb_run_steps: no live walkers (population died out)");
   cudaStream_t st = h->stream;
   RunCfg cfg = make_cfg(h->params);
@@ -742,9 +776,14 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
     EvalOut o{};
     {
       ProfScope ps(h, QMCB_KERNEL_MOVE, st);
-      k_move<true><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live,
-                                                                      0, h->d_ctl, nullptr, mv, h->d_ectl,
-                                                                      h->d_stats, o);
+      if (mixed)
+        k_move<true, float, MIXED_TI><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state,
+                                                                            h->d_live, 0, h->d_ctl, nullptr, mv,
+                                                                            h->d_ectl, h->d_stats, o);
+      else
+        k_move<true, double, double><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state,
+                                                                             h->d_live, 0, h->d_ctl, nullptr, mv,
+                                                                             h->d_ectl, h->d_stats, o);
       ps.end(st);
     }
     if (dmc && mv.e == 0) {
@@ -769,8 +808,12 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
     if (h->params.refresh_interval > 0 && (step + 1) % h->params.refresh_interval == 0) {
       EvalOut o2{};
       ProfScope ps(h, QMCB_KERNEL_REFRESH, st);
-      k_full<<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live, 0,
-                                                                h->d_ctl, nullptr, 0, o2);
+      if (mixed)
+        k_full<float, MIXED_TI><<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state,
+                                                                           h->d_live, 0, h->d_ctl, nullptr, 0, o2);
+      else
+        k_full<double, double><<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state,
+                                                                            h->d_live, 0, h->d_ctl, nullptr, 0, o2);
       ps.end(st);
     }
   }
