@@ -202,6 +202,19 @@ int qmcb_init_walkers(qmcb_handle *h, int n, const double *R);
  */
 int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats *stats);
 
+/* Asynchronous form for drivers that keep several handles busy at once
+ * (one stream per handle; kernels of different handles overlap on the GPU):
+ * qmcb_run_steps_async enqueues the steps and returns; qmcb_steps_done
+ * returns 1 when they finished (0 while running, negative on error);
+ * qmcb_steps_collect waits and returns the statistics.  One batch in
+ * flight per handle. */
+int qmcb_run_steps_async(qmcb_handle *h, int first_step, int n_steps);
+int qmcb_steps_done(qmcb_handle *h);
+int qmcb_steps_collect(qmcb_handle *h, qmcb_step_stats *stats);
+
+/* Device bytes of the walker state of a handle (admission control). */
+size_t qmcb_state_bytes(const qmcb_handle *h);
+
 /* Live walker count and per-walker read back (host buffers, any may be NULL). */
 int qmcb_num_walkers(const qmcb_handle *h);
 int qmcb_get_walkers(qmcb_handle *h, int n, double *R, double *weight, double *e_local,

@@ -28,7 +28,8 @@ EXPORTS = [
     "qmcb_num_electrons", "qmcb_max_walkers", "qmcb_evaluate", "qmcb_evaluate_device", "qmcb_init_walkers",
     "qmcb_run_steps", "qmcb_num_walkers", "qmcb_get_walkers", "qmcb_copy_slot", "qmcb_synchronize",
     "qmcb_stream", "qmcb_set_walker_weights", "qmcb_branch", "qmcb_set_profiling", "qmcb_get_kernel_stats",
-    "qmcb_branch_weights_noalloc",
+    "qmcb_branch_weights_noalloc", "qmcb_run_steps_async", "qmcb_steps_done", "qmcb_steps_collect",
+    "qmcb_state_bytes",
 ]
 
 KERNELS = ["move", "branch", "copy", "energy", "refresh"]
@@ -72,6 +73,11 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.qmcb_branch.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
     L.qmcb_set_profiling.argtypes = [vp, C.c_int]
     L.qmcb_get_kernel_stats.argtypes = [vp, vp, C.c_int]
+    L.qmcb_run_steps_async.argtypes = [vp, C.c_int, C.c_int]
+    L.qmcb_steps_done.argtypes = [vp]
+    L.qmcb_steps_collect.argtypes = [vp, vp]
+    L.qmcb_state_bytes.argtypes = [vp]
+    L.qmcb_state_bytes.restype = C.c_size_t
     L.qmcb_branch_weights_noalloc.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, vp, vp, vp,
                                               vp]
     _lib = L
@@ -151,6 +157,23 @@ class QMCB200Functions:
         st = StepStats()
         self._check(self.lib.qmcb_run_steps(self.h, int(first_step), int(n_steps), C.byref(st)), "qmcb_run_steps")
         return st
+
+    def run_steps_async(self, first_step: int, n_steps: int) -> None:
+        self._check(self.lib.qmcb_run_steps_async(self.h, int(first_step), int(n_steps)), "qmcb_run_steps_async")
+
+    def steps_done(self) -> bool:
+        r = self.lib.qmcb_steps_done(self.h)
+        if r < 0:
+            self._check(-r, "qmcb_steps_done")
+        return r == 1
+
+    def steps_collect(self) -> StepStats:
+        st = StepStats()
+        self._check(self.lib.qmcb_steps_collect(self.h, C.byref(st)), "qmcb_steps_collect")
+        return st
+
+    def state_bytes(self) -> int:
+        return int(self.lib.qmcb_state_bytes(self.h))
 
     def num_walkers(self) -> int:
         return int(self.lib.qmcb_num_walkers(self.h))

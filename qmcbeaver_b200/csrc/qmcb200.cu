@@ -70,6 +70,11 @@ struct qmcb_handle {
   int wpb_move = 1, wpb_full = 1;  // warps (walkers) per CTA of k_move / k_full
   bool evaluated_once = false;
   int state_prec = -1;  // precision the stored walker state was written in
+  // asynchronous step batches (qmcb_run_steps_async)
+  double *h_stats = nullptr;  // pinned
+  int *h_ctl = nullptr;       // pinned
+  cudaEvent_t done_ev = nullptr;
+  bool in_flight = false;
   // kernel timing (qmcb_set_profiling)
   bool prof = false;
   std::vector<cudaEvent_t> prof_ev;
@@ -552,6 +557,9 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(cudaMalloc(&h->d_R, sizeof(double) * (size_t)max_walkers * 3 * h->N));
   CKC(cudaMalloc(&h->d_out, sizeof(double) * (size_t)max_walkers * (6 * h->N + 8)));
   CKC(cudaMalloc(&h->d_status, max_walkers));
+  CKC(cudaMallocHost(&h->h_stats, sizeof(double) * ST_COUNT));
+  CKC(cudaMallocHost(&h->h_ctl, sizeof(int) * 4));
+  CKC(cudaEventCreateWithFlags(&h->done_ev, cudaEventDisableTiming));
 
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
@@ -565,12 +573,15 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   h->wpb_full = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_full);
   h->smem_move = per_move * h->wpb_move;
   h->smem_full = per_full * h->wpb_full;
-  CKC(cudaFuncSetAttribute(k_move<true, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
-  CKC(cudaFuncSetAttribute(k_move<false, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
-  CKC(cudaFuncSetAttribute(k_move<true, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
-  CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_move));
-  CKC(cudaFuncSetAttribute(k_full<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_full));
-  CKC(cudaFuncSetAttribute(k_full<float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_full));
+  // the dynamic shared-memory limit is a per-kernel, process-wide attribute:
+  // raise it to the device maximum once, so handles of different systems
+  // (each launching with its own size) never undercut one another
+  CKC(cudaFuncSetAttribute(k_move<true, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<false, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<true, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_full<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_full<float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
 #undef CKC
   *out = h;
   return QMCB_OK;
@@ -586,6 +597,9 @@ int qmcb_destroy(qmcb_handle *h)
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
+  if (h->done_ev) cudaEventDestroy(h->done_ev);
+  if (h->h_stats) cudaFreeHost(h->h_stats);
+  if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return QMCB_OK;
@@ -750,13 +764,15 @@ int qmcb_init_walkers(qmcb_handle *h, int n, const double *R)
   return QMCB_OK;
 }
 
-int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats *stats)
+// Enqueues n_steps Monte Carlo steps and the copy of the step statistics
+// into the handle's pinned buffer, then records the completion event.
+static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps)
 {
-  if (!h) return QMCB_E_ARG;
   if (n_steps < 0 || first_step < 0) return fail(h, QMCB_E_ARG, "qmcb_run_steps: bad step range");
   if (!h->evaluated_once) return fail(h, QMCB_E_STATE, "qmcb_run_steps: call qmcb_init_walkers first");
   if (h->state_prec != h->params.precision)
     return fail(h, QMCB_E_STATE, "qmcb_run_steps: walker state was written in another precision; call qmcb_init_walkers");
+  if (h->in_flight) return fail(h, QMCB_E_STATE, "qmcb_run_steps: a batch of steps is still in flight on this handle");
   const bool mixed = h->params.precision == QMCB_PREC_MIXED;
   if (h->n_live_host <= 0) return fail(h, QMCB_E_STATE, "qmcb_run_steps: no live walkers (population died out)");
   cudaStream_t st = h->stream;
@@ -818,13 +834,22 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
     }
   }
   CK(cudaGetLastError());
-  double sv[ST_COUNT];
-  int ctl[4];
-  CK(cudaMemcpyAsync(sv, h->d_stats, sizeof(sv), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(ctl, h->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
+  CK(cudaMemcpyAsync(h->h_stats, h->d_stats, sizeof(double) * ST_COUNT, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(h->done_ev, st));
+  h->in_flight = true;
+  return QMCB_OK;
+}
+
+// Waits for the batch in flight and converts the pinned statistics.
+static int finish_steps(qmcb_handle *h, qmcb_step_stats *stats)
+{
+  if (!h->in_flight) return fail(h, QMCB_E_STATE, "qmcb_steps_collect: no batch in flight");
+  CK(cudaEventSynchronize(h->done_ev));
+  h->in_flight = false;
   if (h->prof) prof_collect(h);
-  h->n_live_host = ctl[0];
+  const double *sv = h->h_stats;
+  h->n_live_host = h->h_ctl[0];
   if (stats) {
     stats->sum_weight = sv[ST_SUM_W];
     stats->sum_weight_energy = sv[ST_SUM_WE];
@@ -832,10 +857,46 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
     stats->sum_accept = sv[ST_SUM_ACC];
     stats->n_moves = sv[ST_MOVES];
     stats->final_weight = sv[ST_FINAL_W];
-    stats->n_walkers = ctl[0];
+    stats->n_walkers = h->h_ctl[0];
     stats->n_singular = (int)sv[ST_SINGULAR];
   }
   return QMCB_OK;
+}
+
+int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats *stats)
+{
+  if (!h) return QMCB_E_ARG;
+  int rc = enqueue_steps(h, first_step, n_steps);
+  if (rc) return rc;
+  return finish_steps(h, stats);
+}
+
+int qmcb_run_steps_async(qmcb_handle *h, int first_step, int n_steps)
+{
+  if (!h) return QMCB_E_ARG;
+  return enqueue_steps(h, first_step, n_steps);
+}
+
+int qmcb_steps_done(qmcb_handle *h)
+{
+  if (!h) return -QMCB_E_ARG;
+  if (!h->in_flight) return 1;
+  cudaError_t e = cudaEventQuery(h->done_ev);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) return 0;
+  fail(h, QMCB_E_CUDA, std::string("qmcb_steps_done: ") + cudaGetErrorString(e));
+  return -QMCB_E_CUDA;
+}
+
+int qmcb_steps_collect(qmcb_handle *h, qmcb_step_stats *stats)
+{
+  if (!h) return QMCB_E_ARG;
+  return finish_steps(h, stats);
+}
+
+size_t qmcb_state_bytes(const qmcb_handle *h)
+{
+  return h ? (size_t)h->max_walkers * h->lay.stride * sizeof(double) : 0;
 }
 
 int qmcb_num_walkers(const qmcb_handle *h) { return h ? h->n_live_host : -1; }

@@ -1,0 +1,54 @@
+"""Serving loop: jobs admitted by device footprint, run concurrently (one
+stream per job), each job's energies the same alone and in the mix."""
+import numpy as np
+import pytest
+
+from qmcbeaver_b200.serving import Job, Server, blocked_error, make_jobs, state_footprint
+
+pytestmark = pytest.mark.gpu
+
+
+def test_jobs_complete_and_report_latency():
+    jobs = make_jobs(6, rate=50.0, seed=3, electrons=(4, 20), walkers=(256, 512), target_error=0.5, max_sweeps=40)
+    out = Server(max_active=4).run(jobs)
+    assert out["jobs"] == 6
+    assert out["latency_p50_s"] is not None and out["latency_p99_s"] >= out["latency_p50_s"]
+    for j in jobs:
+        assert j.finished is not None and np.isfinite(j.energy)
+        assert len(j.energies) >= j.min_blocks
+
+
+def test_result_same_alone_and_in_mix():
+    def fresh():
+        js = make_jobs(5, rate=1e3, seed=5, electrons=(6, 16), walkers=(256, 512), target_error=0.0, max_sweeps=24)
+        for j in js:
+            j.arrival = 0.0
+        return js
+    mix = fresh()
+    Server(max_active=5).run(mix)
+    alone = fresh()[2]
+    Server(max_active=1).run([alone])
+    assert len(alone.energies) == len(mix[2].energies) == 24
+    np.testing.assert_allclose(alone.energies, mix[2].energies, rtol=1e-10, atol=0)
+
+
+def test_admission_respects_footprint_budget():
+    jobs = make_jobs(4, rate=1e3, seed=7, electrons=(10, 10), walkers=(512, 512), target_error=0.0, max_sweeps=4)
+    need = state_footprint(jobs[0].system, 512)
+    srv = Server(hbm_budget=int(need * 1.5), max_active=8)   # room for one job at a time
+    out = srv.run(jobs)
+    assert out["jobs"] == 4
+    # with room for one job only, each job is admitted after the previous finished
+    order = sorted(jobs, key=lambda j: j.admitted)
+    for a, b in zip(order, order[1:]):
+        assert b.admitted >= a.finished - 1e-6
+
+
+def test_footprint_matches_library():
+    from qmcbeaver_b200.api import QMCB200Functions
+    from qmcbeaver_b200.system import make_system
+    for wl in ("vmc_water_10e", "dmc_6nuc_30e"):
+        s = make_system(wl)
+        f = QMCB200Functions(s, 2 * 300)
+        assert f.state_bytes() == state_footprint(s, 300)
+        f.close()
