@@ -142,6 +142,82 @@ def cpu_reference_sample(system, walkers: int, steps: int, procs: int, e0: float
     return r
 
 
+def mixed_section(system, W, e0, rank, args):
+    """The same DMC workload with the mixed-precision path (FP32 basis and
+    orbital rows, FP64 inverse / ratios / refresh / energies) and its local
+    energy error against the FP64 path on identical configurations."""
+    import torch
+    from qmcbeaver_b200.api import QMCB200Functions
+    from qmcbeaver_b200.desc import QMCB_PREC_FP64, QMCB_PREC_MIXED, run_params
+    from qmcbeaver_b200.replicas import aggregate_timing, replica_seed
+    N = system.n_electrons
+    p = dmc_params(seed=replica_seed(91, rank), e0=-1.0, reweight_start=EQUIL_SWEEPS * N)
+    p.precision = QMCB_PREC_MIXED
+    f = QMCB200Functions(system, 2 * W, p)
+    f.init_walkers(system.initial_positions(W, seed=2000 + rank))
+    f.run_steps(0, EQUIL_SWEEPS * N)
+    R_eq = f.get_walkers()["R"]
+    p = dmc_params(seed=replica_seed(91, rank), e0=e0)
+    p.precision = QMCB_PREC_MIXED
+    f.set_params(p)
+    f.init_walkers(R_eq)
+    f.run_steps(0, args.warmup)
+    steps = max(args.steps // 4, 3 * N)
+    torch.cuda.synchronize()
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.ExternalStream(f.stream)
+    s_ev.record(stream)
+    st = f.run_steps(args.warmup, steps)
+    e_ev.record(stream)
+    torch.cuda.synchronize()
+    ms, moves = aggregate_timing(s_ev.elapsed_time(e_ev), st.n_moves)
+    f.close()
+    # local-energy error on identical configurations (256 walkers, 2 sweeps of moves)
+    Wc = 256
+    a = QMCB200Functions(system, Wc, run_params(precision=QMCB_PREC_FP64, qf_modification=2, dt=0.01))
+    b = QMCB200Functions(system, Wc, run_params(precision=QMCB_PREC_MIXED, qf_modification=2, dt=0.01))
+    R = np.ascontiguousarray(R_eq[:Wc])
+    sl = np.arange(Wc)
+    a.evaluate(sl, R, -1)
+    b.evaluate(sl, R, -1)
+    rng = np.random.default_rng(3)
+    errs = []
+    for m in range(2 * N):
+        e = m % N
+        R[:, e] += 0.1 * rng.standard_normal((Wc, 3))
+        x, y = a.evaluate(sl, R, e), b.evaluate(sl, R, e)
+        ok = (x["status"] == 0) & (y["status"] == 0)
+        errs.append(np.abs(x["e_local"] - y["e_local"])[ok])
+    a.close()
+    b.close()
+    err = np.concatenate(errs)
+    return {"value": moves / (ms / 1e3), "unit": "walker-moves/s", "steps": steps,
+            "el_error_vs_fp64_ha": {"median": float(np.median(err)), "p90": float(np.percentile(err, 90)),
+                                    "p99": float(np.percentile(err, 99))},
+            "note": "FP32 basis and orbital rows (FP64 accumulation), FP64 inverse, determinant ratio, ratio sums, "
+                    "LU refresh and energies"}
+
+
+def serving_section(args):
+    """Poisson arrivals of VMC energy jobs (molecules drawn like the
+    uneven-batching workload, 4-40 electrons), run concurrently with
+    footprint admission, next to the same jobs solved one after another."""
+    from qmcbeaver_b200.serving import Server, make_jobs
+    kw = dict(electrons=(4, 40), walkers=(256, 2048), target_error=0.2, max_sweeps=200)
+    mix = make_jobs(args.serve_jobs, rate=args.serve_rate, seed=11, **kw)
+    res = Server(max_active=16).run(mix)
+    seq = make_jobs(args.serve_jobs, rate=args.serve_rate, seed=11, **kw)
+    ref = Server(max_active=1).run(seq)
+    same = all(abs(a.energy - b.energy) <= 1e-9 * max(1.0, abs(b.energy)) for a, b in zip(mix, seq)
+               if len(a.energies) == len(b.energies))
+    return {"jobs": res["jobs"], "arrival_rate_per_s": args.serve_rate, "target_error_ha": kw["target_error"],
+            "latency_p50_s": res["latency_p50_s"], "latency_p99_s": res["latency_p99_s"],
+            "walker_moves_per_s": res["walker_moves_per_s"],
+            "sequential": {"latency_p50_s": ref["latency_p50_s"], "latency_p99_s": ref["latency_p99_s"],
+                           "walker_moves_per_s": ref["walker_moves_per_s"]},
+            "same_results_alone_and_mixed": bool(same)}
+
+
 def run_reference_arm(args, rank: int):
     if rank != 0:
         return
@@ -178,6 +254,9 @@ def main():
     ap.add_argument("--walkers", type=int, default=DEFAULT_WALKERS)
     ap.add_argument("--e2e-steps", type=int, default=120)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and serving sections")
+    ap.add_argument("--serve-jobs", type=int, default=24)
+    ap.add_argument("--serve-rate", type=float, default=20.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -326,6 +405,10 @@ def main():
     if clocks is not None:
         out["clocks"] = clocks
     f.close()
+    if not args.no_extras:
+        out["mixed"] = mixed_section(system, W, e0, rank, args)
+        if world == 1:
+            out["serving"] = serving_section(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_sample(system, walkers=64, steps=1500, procs=os.cpu_count() or 1, e0=E_GUESS)
         if r is not None:
