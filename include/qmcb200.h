@@ -31,7 +31,11 @@
 extern "C" {
 #endif
 
-#define QMCB_PADE_MAX 8
+#define QMCB_PADE_MAX 16
+
+/* two-body correlation function forms (QMcBeaver/src/QMCCorrelationFunctionFactory.cpp) */
+#define QMCB_CORR_PADE 0        /* P(r)/Q(r): Pade and FixedCuspPade */
+#define QMCB_CORR_CAMBRIDGE2 1  /* (fL r - 1)^C alpha(fL r) for fL r < 1, else 0 */
 
 /* error codes */
 #define QMCB_OK 0
@@ -84,11 +88,14 @@ typedef struct qmcb_system_desc {
   const double *prim_coeff;     /* [n_prim_total] raw contraction coefficients */
   const double *mo_alpha;       /* [n_alpha][K] occupied orbital rows (AlphaCoeffs) */
   const double *mo_beta;        /* [n_beta][K] (BetaCoeffs) */
-  int n_pade;                   /* Pade functions u = P(r)/Q(r) */
-  const double *pade_num;       /* [n_pade][QMCB_PADE_MAX] P coefficients, P[0] = 0 */
-  const double *pade_den;       /* [n_pade][QMCB_PADE_MAX] Q coefficients, Q[0] = 1 */
-  const int *pade_nnum;         /* [n_pade] used length of P */
+  int n_pade;                   /* two-body correlation functions */
+  const double *pade_num;       /* [n_pade][QMCB_PADE_MAX] Pade: P coefficients, P[0] = 0;
+                                   Cambridge2: polynomial alpha coefficients */
+  const double *pade_den;       /* [n_pade][QMCB_PADE_MAX] Pade: Q coefficients, Q[0] = 1 */
+  const int *pade_nnum;         /* [n_pade] used length of the first table */
   const int *pade_nden;         /* [n_pade] used length of Q */
+  const int *corr_type;         /* [n_pade] QMCB_CORR_* (NULL: all Pade) */
+  const double *corr_param;     /* [n_pade][4] Cambridge2: fL, C, active (1/0), unused */
   int ee_pade[3];               /* up-down, up-up, down-down function (-1 = none) */
   const int *en_pade_up;        /* [M] up electron - nucleus function (-1 = none) */
   const int *en_pade_dn;        /* [M] down electron - nucleus function */

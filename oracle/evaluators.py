@@ -140,7 +140,12 @@ class ReferenceEvaluator(_Base):
     _loaded: Optional[str] = None
 
     def __init__(self, system: MolecularSystem, qf_mod: int = QMCB_QF_NONE, qf_a: float = 0.5, dt: float = 0.09,
-                 max_batch: int = 256):
+                 max_batch: int = 256, ckmf_text: Optional[str] = None, one_e_per_iter: int = 1):
+        """`ckmf_text`: run this input (a reference .ckmf, flags patched for
+        the batch size, the QF options and dt) instead of one written from
+        `system`; `system` must then be the same input read by
+        qmcbeaver_b200.ckmf.  `one_e_per_iter` = 0 selects the reference's
+        all-electron evaluation path (full evaluations only)."""
         if ReferenceEvaluator._loaded is not None:
             raise RuntimeError("the reference library holds one system per process")
         self.lib = C.CDLL(build_reference())
@@ -158,9 +163,20 @@ class ReferenceEvaluator(_Base):
         self.max_batch = max_batch
         fd, path = tempfile.mkstemp(suffix=".ckmf")
         os.close(fd)
-        system.to_ckmf(path, {"walkers_per_pass": max_batch, "number_of_walkers": max_batch,
-                              "QF_modification_type": QF_NAMES[qf_mod],
-                              "umrigar93_equalelectrons_parameter": float(qf_a), "dt": float(dt)})
+        flags = {"walkers_per_pass": max_batch, "number_of_walkers": max_batch,
+                 "QF_modification_type": QF_NAMES[qf_mod],
+                 "umrigar93_equalelectrons_parameter": float(qf_a), "dt": float(dt),
+                 # read_flags starts the run at dt_equilibration (QMcBeaver/src/QMCFlags.cpp:915-916)
+                 "dt_equilibration": float(dt)}
+        if ckmf_text is None:
+            system.to_ckmf(path, flags)
+        else:
+            from qmcbeaver_b200.ckmf import patch_flags, strip_three_body
+            flags.update({"replace_electron_nucleus_cusps": 0, "use_three_body_jastrow": 0,
+                          "one_e_per_iter": int(one_e_per_iter),
+                          "print_configs": 0, "optimize_Psi": 0})
+            with open(path, "w") as fh:
+                fh.write(patch_flags(strip_three_body(ckmf_text), flags))
         L.ref_init(path.encode())
         os.unlink(path)
         ReferenceEvaluator._loaded = path

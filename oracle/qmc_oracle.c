@@ -25,6 +25,8 @@ struct orc_system {
   int npade;
   double *pnum, *pden;
   int *pnn, *pnd;
+  int *ctype;
+  double *cparam;
   int ee[3];
   int *en_up, *en_dn;
   double Pnn;
@@ -88,6 +90,13 @@ orc_system *orc_system_new(const qmcb_system_desc *d, int qf_mod, double qf_a, d
   s->pden = dup_d(d->pade_den, (size_t)s->npade * QMCB_PADE_MAX);
   s->pnn = dup_i(d->pade_nnum, s->npade);
   s->pnd = dup_i(d->pade_nden, s->npade);
+  s->ctype = (int *)calloc(s->npade ? s->npade : 1, sizeof(int));
+  s->cparam = (double *)calloc(4 * (s->npade ? s->npade : 1), sizeof(double));
+  for (int f = 0; f < s->npade; f++) {
+    s->ctype[f] = d->corr_type ? d->corr_type[f] : QMCB_CORR_PADE;
+    if (d->corr_param)
+      for (int i = 0; i < 4; i++) s->cparam[4 * f + i] = d->corr_param[4 * f + i];
+  }
   for (int i = 0; i < 3; i++) s->ee[i] = d->ee_pade[i];
   s->en_up = dup_i(d->en_pade_up, s->M);
   s->en_dn = dup_i(d->en_pade_dn, s->M);
@@ -122,7 +131,7 @@ void orc_system_free(orc_system *s)
   if (!s) return;
   free(s->nuc_xyz); free(s->nuc_z); free(s->bf_atom); free(s->bf_pow); free(s->bf_nprim);
   free(s->bf_off); free(s->pexp); free(s->pcoef); free(s->mo_a); free(s->mo_b); free(s->pnum);
-  free(s->pden); free(s->pnn); free(s->pnd); free(s->en_up); free(s->en_dn);
+  free(s->pden); free(s->pnn); free(s->pnd); free(s->ctype); free(s->cparam); free(s->en_up); free(s->en_dn);
   free(s->atom_first); free(s->atom_nbf); free(s->atom_lmax);
   free(s);
 }
@@ -552,6 +561,26 @@ static void poly_all(const double *c, int len, double x, double *f, double *df, 
 
 static void pade(const orc_system *s, int idx, double r, double *u, double *du, double *d2u)
 {
+  if (s->ctype[idx] == QMCB_CORR_CAMBRIDGE2) {
+    /* Cambridge2CorrelationFunction::evaluate (QMcBeaver/src/Cambridge2CorrelationFunction.cpp) */
+    const double *cp = s->cparam + 4 * idx;
+    double fL = cp[0];
+    int C = (int)cp[1];
+    *u = *du = *d2u = 0.0;
+    if (cp[2] == 0.0) return;
+    double d = fL * r - 1.0;
+    if (d > 0.0) return;
+    double a, ap, app;
+    poly_all(s->pnum + idx * QMCB_PADE_MAX, s->pnn[idx], fL * r, &a, &ap, &app);
+    double P = a, dP_r = fL * ap, dP_rr = fL * fL * app;
+    double dpc = pow(d, C);
+    double dpc_r = C * fL * dpc / d;
+    double dpc_rr = (C - 1.0) * fL * dpc_r / d;
+    *u = dpc * P;
+    *du = dpc_r * P + dpc * dP_r;
+    *d2u = dpc_rr * P + dpc_r * dP_r * 2.0 + dpc * dP_rr;
+    return;
+  }
   double a, ap, app, b, bp, bpp;
   poly_all(s->pnum + idx * QMCB_PADE_MAX, s->pnn[idx], r, &a, &ap, &app);
   poly_all(s->pden + idx * QMCB_PADE_MAX, s->pnd[idx], r, &b, &bp, &bpp);

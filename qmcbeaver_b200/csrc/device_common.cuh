@@ -18,7 +18,7 @@
 
 namespace qmcb {
 
-constexpr int kPadeMax = 8;
+constexpr int kPadeMax = 16;
 
 // Scalars kept per walker (offsets inside the SC block of a walker).
 enum Sc {
@@ -65,6 +65,8 @@ struct DevSys {
   const int *en[2];      // [M] e-n function per spin
   const double2 *pade_ab; // [npade] (a, b) when every function is a r / (1 + b r)
   int pade_simple;
+  const int *ctype;       // [npade] QMCB_CORR_*
+  const double4 *cparam;  // [npade] Cambridge2: fL, C, active
 };
 
 // Offsets (in doubles) of each array in a walker block.
@@ -217,6 +219,28 @@ __device__ __forceinline__ void pade_eval(const DevSys &S, int f, double r, doub
   }
   const double *P = S.pade + (size_t)f * 2 * kPadeMax;
   int2 L = S.pade_len[f];
+  if (S.ctype[f] == 1) {
+    // Cambridge2 (Cambridge2CorrelationFunction::evaluate,
+    // QMcBeaver/src/Cambridge2CorrelationFunction.cpp): u = d^C alpha(fL r),
+    // d = fL r - 1, zero for d > 0 or an inactive function
+    const double4 cp = S.cparam[f];
+    u = du = d2u = 0.0;
+    const double fL = cp.x;
+    const int C = (int)cp.y;
+    const double d = fL * r - 1.0;
+    if (cp.z == 0.0 || d > 0.0) return;
+    double a, ap, app;
+    poly_all(P, L.x, fL * r, a, ap, app);
+    const double dP_r = fL * ap, dP_rr = fL * fL * app;
+    double dpc = 1.0;
+    for (int i = 0; i < C; i++) dpc *= d;
+    const double dpc_r = C * fL * dpc / d;
+    const double dpc_rr = (C - 1.0) * fL * dpc_r / d;
+    u = dpc * a;
+    du = dpc_r * a + dpc * dP_r;
+    d2u = dpc_rr * a + dpc_r * dP_r * 2.0 + dpc * dP_rr;
+    return;
+  }
   double a, ap, app, b, bp, bpp;
   poly_all(P, L.x, r, a, ap, app);
   poly_all(P + kPadeMax, L.y, r, b, bp, bpp);

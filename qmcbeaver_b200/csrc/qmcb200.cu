@@ -51,6 +51,8 @@ struct qmcb_handle {
   double *d_pade = nullptr;
   int2 *d_pade_len = nullptr;
   double2 *d_pade_ab = nullptr;
+  int *d_ctype = nullptr;
+  double4 *d_cparam = nullptr;
   int4 *d_shell = nullptr;
   int2 *d_fn = nullptr;
   double *d_pexp = nullptr, *d_pcoef = nullptr;
@@ -410,12 +412,33 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
     }
     plen[f] = make_int2(ln, ld);
   }
+  std::vector<int> ctype(std::max(d->n_pade, 1), 0);
+  std::vector<double4> cparam(std::max(d->n_pade, 1), make_double4(0.0, 0.0, 0.0, 0.0));
+  for (int f = 0; f < d->n_pade; f++) {
+    ctype[f] = d->corr_type ? d->corr_type[f] : QMCB_CORR_PADE;
+    if (ctype[f] != QMCB_CORR_PADE && ctype[f] != QMCB_CORR_CAMBRIDGE2) {
+      delete h;
+      return fail(nullptr, QMCB_E_ARG, "qmcb_create: unknown correlation function type");
+    }
+    if (ctype[f] == QMCB_CORR_CAMBRIDGE2) {
+      if (!d->corr_param) {
+        delete h;
+        return fail(nullptr, QMCB_E_ARG, "qmcb_create: Cambridge2 function without corr_param");
+      }
+      const double *cp = d->corr_param + 4 * f;
+      if (cp[1] < 1.0 || cp[1] > 16.0) {
+        delete h;
+        return fail(nullptr, QMCB_E_ARG, "qmcb_create: Cambridge2 exponent C out of range");
+      }
+      cparam[f] = make_double4(cp[0], cp[1], cp[2], cp[3]);
+    }
+  }
   // every function of the form a r / (1 + b r) takes the closed-form path
   std::vector<double2> pade_ab(std::max(d->n_pade, 1), make_double2(0.0, 0.0));
   bool pade_simple = d->n_pade > 0;
   for (int f = 0; f < d->n_pade; f++) {
     const double *nu = d->pade_num + f * kPadeMax, *de = d->pade_den + f * kPadeMax;
-    if (d->pade_nnum[f] == 2 && d->pade_nden[f] == 2 && nu[0] == 0.0 && de[0] == 1.0)
+    if (ctype[f] == QMCB_CORR_PADE && d->pade_nnum[f] == 2 && d->pade_nden[f] == 2 && nu[0] == 0.0 && de[0] == 1.0)
       pade_ab[f] = make_double2(nu[1], de[1]);
     else
       pade_simple = false;
@@ -470,6 +493,8 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(upload(&h->d_pade, pade));
   CKC(upload(&h->d_pade_len, plen));
   CKC(upload(&h->d_pade_ab, pade_ab));
+  CKC(upload(&h->d_ctype, ctype));
+  CKC(upload(&h->d_cparam, cparam));
   CKC(upload(&h->d_en[0], en[0]));
   CKC(upload(&h->d_en[1], en[1]));
 
@@ -498,6 +523,8 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   S.pade_len = h->d_pade_len;
   S.pade_ab = h->d_pade_ab;
   S.pade_simple = pade_simple ? 1 : 0;
+  S.ctype = h->d_ctype;
+  S.cparam = h->d_cparam;
   S.en[0] = h->d_en[0];
   S.en[1] = h->d_en[1];
 
@@ -591,7 +618,7 @@ int qmcb_destroy(qmcb_handle *h)
 {
   if (!h) return QMCB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *ptrs[] = {h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
+  void *ptrs[] = {h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
                   h->d_copies, h->d_stats, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
   for (void *p : ptrs)

@@ -30,6 +30,7 @@ class SystemDesc(C.Structure):
         ("n_prim_total", C.c_int), ("prim_exponent", _dp), ("prim_coeff", _dp),
         ("mo_alpha", _dp), ("mo_beta", _dp),
         ("n_pade", C.c_int), ("pade_num", _dp), ("pade_den", _dp), ("pade_nnum", _ip), ("pade_nden", _ip),
+        ("corr_type", _ip), ("corr_param", _dp),
         ("ee_pade", C.c_int * 3), ("en_pade_up", _ip), ("en_pade_dn", _ip),
     ]
 
@@ -103,7 +104,7 @@ class PackedSystem:
     def __init__(self, s: MolecularSystem):
         self.system = s
         atom, pw, nprim, off, ex, co = s.flat_basis()
-        npade, num, den, nn, nd, ee, en_up, en_dn = s.pade_tables()
+        npade, num, den, nn, nd, ee, en_up, en_dn, ctype, cparam = s.pade_tables()
         self._keep = dict(
             nuc_xyz=np.ascontiguousarray(s.coords, np.float64),
             nuc_z=np.ascontiguousarray(s.Z, np.float64),
@@ -111,7 +112,8 @@ class PackedSystem:
             mo_a=np.ascontiguousarray(s.mo_alpha(), np.float64),
             mo_b=np.ascontiguousarray(s.mo_beta(), np.float64) if s.n_beta else np.zeros((1, s.n_basis)),
             num=np.ascontiguousarray(num), den=np.ascontiguousarray(den), nn=nn, nd=nd,
-            en_up=en_up, en_dn=en_dn,
+            en_up=en_up, en_dn=en_dn, ctype=np.ascontiguousarray(ctype, np.int32),
+            cparam=np.ascontiguousarray(cparam, np.float64),
         )
         k = self._keep
         d = SystemDesc()
@@ -135,9 +137,11 @@ class PackedSystem:
         d.pade_den = _d(k["den"])
         d.pade_nnum = _i(k["nn"])
         d.pade_nden = _i(k["nd"])
+        d.corr_type = _i(k["ctype"])
+        d.corr_param = _d(k["cparam"])
         for i in range(3):
             d.ee_pade[i] = int(ee[i])
         d.en_pade_up = _i(k["en_up"])
         d.en_pade_dn = _i(k["en_dn"])
         self.desc = d
-        assert PADE_MAX == 8
+        assert PADE_MAX == 16

@@ -37,7 +37,8 @@ SHELL_TYPES = {
     "d": ["dxx", "dyy", "dzz", "dxy", "dxz", "dyz"],
 }
 
-PADE_MAX = 8  # coefficients per polynomial (degree <= 7), matches qmcb200.h
+PADE_MAX = 16  # coefficients per polynomial (degree <= 15), matches qmcb200.h
+CORR_PADE, CORR_CAMBRIDGE2 = 0, 1
 
 
 def type_to_powers(t: str) -> Tuple[int, int, int]:
@@ -88,6 +89,61 @@ class Pade:
         df = apDIVb - bpDIVb * aDIVb
         d2f = (app - bpp * aDIVb) / b - 2 * bpDIVb * df
         return f, df, d2f
+
+
+@dataclasses.dataclass
+class Cambridge2:
+    """u(r) = (fL r - 1)^C alpha(fL r) for fL r <= 1, zero beyond, with alpha
+    the polynomial of Cambridge2CorrelationFunction::initializeParameters
+    (QMcBeaver/src/Cambridge2CorrelationFunction.cpp): alpha_0 = p[1],
+    alpha_1 = g / (-1)^C / fL + alpha_0 C (g the cusp constant), alpha_i = p[i]."""
+    fL: float
+    C: int
+    alpha: Sequence[float]
+    active: bool = True
+    # the input's own parameters (L, cusp constant g, scale f), kept for
+    # writing the function back out; derived from fL / alpha when zero
+    L: float = 0.0
+    g: float = 0.0
+    f: float = 1.0
+
+    def input_parameters(self) -> Tuple[List[float], List[float]]:
+        """(Parameters, Constants) of a ckmf block giving this function."""
+        if self.L > 0.0 or not self.active:
+            L, g, f = self.L, self.g, self.f
+        else:
+            L, f = self.fL, 1.0
+            g = (self.alpha[1] - self.alpha[0] * self.C) * (-1.0) ** self.C * self.fL
+        return [L, self.alpha[0]] + list(self.alpha[2:]), [g, float(self.C), 0.0, f]
+
+    @staticmethod
+    def from_parameters(params: Sequence[float], constants: Sequence[float], a_diag: float = -1e-5) -> "Cambridge2":
+        g = float(constants[0])
+        C = int(constants[1])
+        f = float(constants[3]) if len(constants) >= 4 else 1.0
+        L = float(params[0])
+        fL = f * L
+        active = not (L <= 0.0 or fL > 100.0)
+        if not active and a_diag >= 0.0:
+            raise ValueError(f"Cambridge2 with L = {L}")
+        a0 = float(params[1])
+        # an inactive function is never evaluated; its alpha_1 is left at 0
+        a1 = g / (-1.0) ** C / fL + a0 * C if fL != 0.0 else 0.0
+        a = [a0, a1] + [float(x) for x in params[2:]]
+        return Cambridge2(fL=fL, C=C, alpha=a, active=active, L=L, g=g, f=f)
+
+    def evaluate(self, r: float) -> Tuple[float, float, float]:
+        if not self.active:
+            return 0.0, 0.0, 0.0
+        d = self.fL * r - 1.0
+        if d > 0.0:
+            return 0.0, 0.0, 0.0
+        P, ap, app = _poly_all(self.alpha, self.fL * r)
+        dP_r, dP_rr = self.fL * ap, self.fL * self.fL * app
+        dpc = d ** self.C
+        dpc_r = self.C * self.fL * dpc / d
+        dpc_rr = (self.C - 1.0) * self.fL * dpc_r / d
+        return dpc * P, dpc_r * P + dpc * dP_r, dpc_rr * P + dpc_r * dP_r * 2.0 + dpc * dP_rr
 
 
 def _poly_all(c: Sequence[float], x: float) -> Tuple[float, float, float]:
@@ -161,11 +217,12 @@ class MolecularSystem:
         return np.ascontiguousarray(self.mo[self.beta_occ])
 
     def pade_tables(self):
-        """Pade table + indices: ee[3] = (anti, up-up, dn-dn), en_up[M], en_dn[M];
-        -1 means no correlation function for that pair."""
-        funcs: List[Pade] = []
+        """Correlation-function table + indices: ee[3] = (anti, up-up, dn-dn),
+        en_up[M], en_dn[M]; -1 means no correlation function for that pair.
+        Returns (n, num, den, nnum, nden, ee, en_up, en_dn, ctype, cparam)."""
+        funcs: List[object] = []
 
-        def add(p: Optional[Pade]) -> int:
+        def add(p) -> int:
             if p is None:
                 return -1
             funcs.append(p)
@@ -179,15 +236,27 @@ class MolecularSystem:
         den = np.zeros((nfun, PADE_MAX))
         nn = np.zeros(nfun, np.int32)
         nd = np.zeros(nfun, np.int32)
+        ctype = np.zeros(nfun, np.int32)
+        cparam = np.zeros((nfun, 4))
         for i, p in enumerate(funcs):
-            if len(p.num) > PADE_MAX or len(p.den) > PADE_MAX:
-                raise ValueError("Pade polynomial too long")
-            num[i, : len(p.num)] = p.num
-            den[i, : len(p.den)] = p.den
-            nn[i] = len(p.num)
-            nd[i] = len(p.den)
+            if isinstance(p, Cambridge2):
+                if len(p.alpha) > PADE_MAX:
+                    raise ValueError("Cambridge2 polynomial too long")
+                num[i, : len(p.alpha)] = p.alpha
+                nn[i] = len(p.alpha)
+                den[i, 0] = 1.0
+                nd[i] = 1
+                ctype[i] = CORR_CAMBRIDGE2
+                cparam[i] = (p.fL, float(p.C), 1.0 if p.active else 0.0, 0.0)
+            else:
+                if len(p.num) > PADE_MAX or len(p.den) > PADE_MAX:
+                    raise ValueError("Pade polynomial too long")
+                num[i, : len(p.num)] = p.num
+                den[i, : len(p.den)] = p.den
+                nn[i] = len(p.num)
+                nd[i] = len(p.den)
         return (len(funcs), num, den, nn, nd, np.asarray(ee, np.int32),
-                np.asarray(en_up, np.int32), np.asarray(en_dn, np.int32))
+                np.asarray(en_up, np.int32), np.asarray(en_dn, np.int32), ctype, cparam)
 
     def nuclear_repulsion(self) -> float:
         """V_nn as calc_P_nn (QMcBeaver/src/QMCPotential_Energy.cpp:285-307)."""
@@ -249,7 +318,12 @@ class MolecularSystem:
         &flags (key line / value line, QMcBeaver/src/QMCFlags.cpp:198-206),
         &geometry, &basis, &wavefunction, &Jastrow."""
         f = dict(DEFAULT_FLAGS)
+        # up and down electrons share parameters only when their functions
+        # agree (QMcBeaver/src/QMCJastrowParameters.cpp:880-900)
+        linked = (self.ee_para_dn == self.ee_para_up or self.n_beta < 2) and \
+            (self.n_beta == 0 or self.en_dn == self.en_up)
         f.update({
+            "link_Jastrow_parameters": 1 if linked else 0,
             "atoms": self.n_nuclei,
             "charge": self.charge,
             "norbitals": self.mo.shape[0],
@@ -299,18 +373,28 @@ class MolecularSystem:
         out.append("")
         out.append("&Jastrow")
 
-        def block(p1: str, p2: str, p: Pade) -> None:
-            # FixedCuspPade: numerator constants first then parameters,
-            # denominator parameters; this writer only emits the
-            # [0, cusp] / [1, b...] form the configs use.
-            if len(p.num) != 2 or p.num[0] != 0.0 or p.den[0] != 1.0:
-                raise ValueError("ckmf writer supports u = a r / (1 + b1 r + ...)")
-            dparams = list(p.den[1:])
+        def block(p1: str, p2: str, p) -> None:
             out.append(f"ParticleTypes:\t{p1}\t{p2}")
+            if isinstance(p, Cambridge2):
+                params, consts = p.input_parameters()
+                out.append("CorrelationFunctionType:\tCambridge2")
+                out.append("NumberOfParameterTypes:\t2")
+                out.append(f"NumberOfParametersOfEachType:\t1\t{len(params) - 1}")
+                out.append("Parameters:\t" + "\t".join(g % v for v in params))
+                out.append("NumberOfConstantTypes:\t4")
+                out.append("NumberOfConstantsOfEachType:\t1\t1\t1\t1")
+                out.append("Constants:\t" + "\t".join(g % v for v in consts))
+                out.append("")
+                return
+            # FixedCuspPade: numerator [0, constant, parameters of type 0],
+            # denominator [1, parameters of type 1]
+            if len(p.num) < 2 or p.num[0] != 0.0 or p.den[0] != 1.0:
+                raise ValueError("ckmf writer needs u = (c r + ...) / (1 + ...)")
+            nparams, dparams = list(p.num[2:]), list(p.den[1:])
             out.append("CorrelationFunctionType:\tFixedCuspPade")
             out.append("NumberOfParameterTypes:\t2")
-            out.append(f"NumberOfParametersOfEachType:\t0\t{len(dparams)}")
-            out.append("Parameters:\t" + "\t".join(g % v for v in dparams))
+            out.append(f"NumberOfParametersOfEachType:\t{len(nparams)}\t{len(dparams)}")
+            out.append("Parameters:\t" + "\t".join(g % v for v in nparams + dparams))
             out.append("NumberOfConstantTypes:\t1")
             out.append("NumberOfConstantsOfEachType:\t1")
             out.append("Constants:\t" + g % p.num[1])
@@ -566,6 +650,27 @@ def _assemble(name, Zs, coords, basis, n_alpha, n_beta, rng, jastrow=True, orbit
     return sysm
 
 
+def with_cambridge2(s: MolecularSystem, seed: int = 1) -> MolecularSystem:
+    """The same molecule with Cambridge2 two-body functions of the shape the
+    reference's inputs use (QMcBeaver/test/oepi.ckmf &Jastrow): e-e cusp
+    constants 1/2 (up-down) and 1/4 (parallel), e-n cusp constant 0,
+    C = 3 (C = 2 for the down-down pair), L in [0.13, 0.25] so each
+    function reaches 4 to 8 bohr, 8 to 12 alpha coefficients; the last
+    nucleus type's down-electron function is inactive (L = 0)."""
+    rng = np.random.default_rng(seed)
+
+    def fn(g: float, C: int, n: int, active: bool = True) -> Cambridge2:
+        L = float(rng.uniform(0.13, 0.25)) if active else 0.0
+        a = rng.normal(0.0, 1.5, n).tolist()
+        return Cambridge2.from_parameters([L] + a, [g, C])
+
+    types = list(dict.fromkeys(s.labels))
+    en_up = {l: fn(0.0, 3, 8 + (i % 5)) for i, l in enumerate(types)}
+    en_dn = {l: fn(0.0, 3, 8, active=(i != len(types) - 1)) for i, l in enumerate(types)}
+    return dataclasses.replace(s, ee_anti=fn(0.5, 3, 8), ee_para_up=fn(0.25, 3, 9), ee_para_dn=fn(0.25, 2, 8),
+                               en_up=en_up, en_dn=en_dn, name=s.name + " cambridge2")
+
+
 def make_water_like(seed: int = 1, jastrow: bool = True) -> MolecularSystem:
     """The small VMC system: O at the origin, H at (+-1.43, 1.11, 0) bohr,
     5 up + 5 down electrons, 24 contracted Cartesian Gaussians with 3
@@ -618,6 +723,10 @@ WORKLOADS = {
                          walkers=16384, run="dmc", dt=0.01, importance=True, refresh=50),
     "mixed_20nuc_100e": dict(kind="random", n_elec=100, n_nuclei=20, n_basis=400, box=12.0, z=(1, 6, 8),
                              walkers=65536, run="dmc", dt=0.01, importance=True, refresh=50),
+    # Cambridge2 two-body Jastrow (the form of the reference's own test inputs)
+    "vmc_cambridge2_16e": dict(kind="random", n_elec=16, n_nuclei=4, n_basis=64, box=5.0, z=(1, 6, 7, 8),
+                               walkers=4096, run="vmc", dt=0.01, importance=True, refresh=50,
+                               correlation="cambridge2"),
 }
 
 
@@ -625,8 +734,12 @@ def make_system(workload: str, seed: int = 1, jastrow: bool = True) -> Molecular
     w = WORKLOADS[workload]
     if w["kind"] == "water":
         return make_water_like(seed, jastrow)
-    return make_random_molecule(w["n_elec"], w["n_nuclei"], w["n_basis"], w["box"], w["z"], seed=seed,
-                                jastrow=jastrow, name=workload)
+    s = make_random_molecule(w["n_elec"], w["n_nuclei"], w["n_basis"], w["box"], w["z"], seed=seed,
+                             jastrow=jastrow, name=workload)
+    if jastrow and w.get("correlation") == "cambridge2":
+        s = with_cambridge2(s, seed=seed + 1)
+        s.name = workload
+    return s
 
 
 # ------------------------------------------------------------ serialisation
@@ -641,9 +754,16 @@ def system_to_arrays(s: MolecularSystem) -> Dict[str, np.ndarray]:
             ex.extend(float(v) for v in f.exponents)
             co.extend(float(v) for v in f.coefficients)
 
-    def pade_arr(p: Optional[Pade]) -> np.ndarray:
+    def pade_arr(p) -> np.ndarray:
+        # row 0: [len, numerator...], row 1: [len, denominator...]; a
+        # Cambridge2 function is stored as row 0 = [-len, alpha...],
+        # row 1 = [fL, C, active, ...]
         out = np.full((2, PADE_MAX + 1), np.nan)
-        if p is not None:
+        if isinstance(p, Cambridge2):
+            out[0, 0] = -len(p.alpha)
+            out[0, 1:1 + len(p.alpha)] = p.alpha
+            out[1, 0:3] = (p.fL, p.C, 1.0 if p.active else 0.0)
+        elif p is not None:
             out[0, 0] = len(p.num)
             out[0, 1:1 + len(p.num)] = p.num
             out[1, 0] = len(p.den)
@@ -661,10 +781,13 @@ def system_to_arrays(s: MolecularSystem) -> Dict[str, np.ndarray]:
 
 
 def system_from_arrays(d) -> MolecularSystem:
-    def pade_of(a) -> Optional[Pade]:
+    def pade_of(a):
         a = np.asarray(a)
         if np.isnan(a[0, 0]):
             return None
+        if a[0, 0] < 0:
+            n = int(-a[0, 0])
+            return Cambridge2(fL=float(a[1, 0]), C=int(a[1, 1]), alpha=list(a[0, 1:1 + n]), active=bool(a[1, 2]))
         nn, nd = int(a[0, 0]), int(a[1, 0])
         return Pade(num=list(a[0, 1:1 + nn]), den=list(a[1, 1:1 + nd]))
 

@@ -27,6 +27,8 @@ CASES = {
     "water_vmc": ("vmc_water_10e", 0, 0.09, 8, 24, 0.3, 5),
     "dmc30_unequal": ("dmc_6nuc_30e", 2, 0.01, 4, 34, 0.15, 7),
     "dmc30_equal": ("dmc_6nuc_30e", 1, 0.01, 2, 8, 0.15, 0),
+    # Cambridge2 two-body Jastrow with C = 2 and C = 3 and an inactive function
+    "cambridge2_vmc": ("vmc_cambridge2_16e", 2, 0.01, 6, 40, 0.2, 6),
 }
 
 

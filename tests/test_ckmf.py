@@ -1,0 +1,283 @@
+"""The .ckmf reader and writer (config I/O), and -- where the reference tree
+is present -- the oracle against the reference run on the reference's own
+input files (two-body Jastrows; cusp replacement and three-body blocks
+left out, as the walker path evaluates neither)."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from oracle.evaluators import reference_available
+from qmcbeaver_b200.ckmf import CkmfError, patch_flags, read_ckmf, strip_three_body
+from qmcbeaver_b200.system import Cambridge2, Pade, make_system, with_cambridge2
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_INPUTS = "/root/reference/QMcBeaver"
+
+
+def _same_tables(a, b):
+    ta, tb = a.pade_tables(), b.pade_tables()
+    for x, y in zip(ta, tb):
+        np.testing.assert_array_equal(np.asarray(x), np.asarray(y))
+
+
+@pytest.mark.parametrize("workload,cambridge", [("vmc_water_10e", False), ("dmc_6nuc_30e", True),
+                                                ("vmc_cambridge2_16e", False)])
+def test_writer_reader_round_trip(tmp_path, workload, cambridge):
+    s = make_system(workload, seed=1)
+    if cambridge:
+        s = with_cambridge2(s, seed=4)
+    p = tmp_path / "sys.ckmf"
+    s.to_ckmf(str(p))
+    c = read_ckmf(str(p))
+    assert c.n_alpha == s.n_alpha and c.n_beta == s.n_beta and c.n_determinants == 1
+    t = c.to_system()
+    np.testing.assert_array_equal(t.coords, s.coords)
+    np.testing.assert_array_equal(t.Z, s.Z)
+    np.testing.assert_array_equal(t.mo_alpha(), s.mo_alpha())
+    np.testing.assert_array_equal(t.mo_beta(), s.mo_beta())
+    for x, y in zip(t.flat_basis(), s.flat_basis()):
+        np.testing.assert_array_equal(x, y)
+    _same_tables(t, s)
+
+
+def test_cambridge2_parameters_and_evaluation():
+    # alpha_1 = g / (-1)^C / fL + alpha_0 C (Cambridge2CorrelationFunction::initializeParameters)
+    f = Cambridge2.from_parameters([0.2, 1.5, -0.7, 0.3], [0.5, 3, 0, 2.0])
+    assert f.fL == pytest.approx(0.4) and f.C == 3 and f.active
+    assert f.alpha[1] == pytest.approx(0.5 / -1.0 / 0.4 + 1.5 * 3)
+    # u' at r = 0 equals the cusp constant g for any alpha
+    _, du, _ = f.evaluate(0.0)
+    assert du == pytest.approx(0.5, rel=1e-12)
+    # zero beyond the cutoff 1 / fL, and the first derivatives by differences
+    assert f.evaluate(2.6) == (0.0, 0.0, 0.0)
+    r, h = 0.9, 1e-5
+    u0, d1, d2 = f.evaluate(r)
+    up, um = f.evaluate(r + h)[0], f.evaluate(r - h)[0]
+    assert d1 == pytest.approx((up - um) / (2 * h), rel=1e-7)
+    assert d2 == pytest.approx((up - 2 * u0 + um) / h ** 2, rel=1e-4)
+    assert not Cambridge2.from_parameters([0.0, 1.0], [0.0, 3]).active
+    with pytest.raises(ValueError):
+        Cambridge2.from_parameters([0.0, 1.0], [0.0, 3], a_diag=0.1)
+    # writing out and reading back keeps every coefficient
+    params, consts = f.input_parameters()
+    g = Cambridge2.from_parameters(params, consts)
+    assert (g.fL, g.C, list(g.alpha)) == (f.fL, f.C, list(f.alpha))
+
+
+_TEXT = """# a two-electron input written for the reader tests
+&flags
+atoms
+ 1
+charge
+ 0
+norbitals
+ 2
+nbasisfunc
+ 2
+ndeterminants
+ {ndet}
+# comment lines are skipped where a key is expected
+dt
+ 0.02
+{extra}
+&
+&geometry
+he 2 0.0 0.0 0.1
+&
+&basis
+HE 2 2
+  2 s
+    3.0 0.5
+    0.5 0.7
+  1 px
+    1.0 0.9
+&
+&wavefunction
+0.9 0.1
+0.2 -0.8
+Alpha Occupation
+{aocc}
+Beta Occupation
+{bocc}
+CI Coeffs
+{ci}
+&
+
+&Jastrow
+ParticleTypes: Electron_Down Electron_UP
+CorrelationFunctionType: Pade
+NumberOfParameterTypes: 2
+NumberOfParametersOfEachType: 2 1
+Parameters: 0.5 0.1 2.0
+NumberOfConstantTypes: 0
+NumberOfConstantsOfEachType:
+Constants:
+
+ParticleTypes: Electron_up He
+CorrelationFunctionType: FixedCuspPade
+NumberOfParameterTypes: 2
+NumberOfParametersOfEachType: 1 2
+Parameters: 0.3 1.5 0.25
+NumberOfConstantTypes: 1
+NumberOfConstantsOfEachType: 1
+Constants: -2
+
+ParticleTypes: Electron_down He
+CorrelationFunctionType: Cambridge2
+NumberOfParameterTypes: 2
+NumberOfParametersOfEachType: 1 3
+Parameters: 0.25 0.4 -0.2 0.1
+NumberOfConstantTypes: 2
+NumberOfConstantsOfEachType: 1 1
+Constants: 0 2
+
+ParticleTypes: He Electron_up Electron_down
+threeBodyCorrelationFunctionType: Cambridge
+NumberOfParameterTypes: 2
+&Jastrow
+"""
+
+
+def _text(ndet=1, extra="", aocc="1 0", bocc="1 0", ci="1.0"):
+    return _TEXT.format(ndet=ndet, extra=extra, aocc=aocc, bocc=bocc, ci=ci)
+
+
+def test_reader_sections_and_function_layouts():
+    c = read_ckmf("t", _text(extra="replace_electron_nucleus_cusps\n 0\nlink_Jastrow_parameters\n 0"))
+    assert c.labels == ["He"] and c.flag("dt", kind=float) == 0.02
+    assert [f.type for f in c.basis[0]] == ["s", "px"]
+    assert c.three_body_blocks == 1
+    with pytest.raises(CkmfError, match="three-body"):
+        c.to_system()
+    s = c.to_system(allow_three_body=True)
+    # Pade: numerator [0, type-0 parameters], denominator [1, the rest]
+    assert isinstance(s.ee_anti, Pade)
+    assert list(s.ee_anti.num) == [0.0, 0.5, 0.1] and list(s.ee_anti.den) == [1.0, 2.0]
+    # FixedCuspPade: numerator [0, constant, type-0 parameters], denominator [1, type-1 parameters]
+    up = s.en_up["He"]
+    assert list(up.num) == [0.0, -2.0, 0.3] and list(up.den) == [1.0, 1.5, 0.25]
+    # unlinked: the down electrons keep their own (Cambridge2) function
+    dn = s.en_dn["He"]
+    assert isinstance(dn, Cambridge2) and dn.C == 2 and dn.fL == 0.25
+    # linked (the reference's default): down electrons take the up functions
+    s2 = read_ckmf("t", _text(extra="replace_electron_nucleus_cusps\n 0")).to_system(allow_three_body=True)
+    assert s2.en_dn["He"] is s2.en_up["He"]
+
+
+def test_reader_refusals_and_constraints():
+    with pytest.raises(CkmfError, match="replace_electron_nucleus_cusps"):
+        read_ckmf("t", _text()).to_system(allow_three_body=True)
+    c = read_ckmf("t", _text(ndet=2, aocc="1 0\n0 1", bocc="1 0\n1 0", ci="0.9 c 0 -0.5"))
+    assert c.n_determinants == 2
+    np.testing.assert_allclose(c.ci_coeffs, [0.9, -0.45])
+    with pytest.raises(CkmfError, match="determinants"):
+        c.to_system(allow_cusp_replacement=True, allow_three_body=True)
+    with pytest.raises(CkmfError, match="electrons"):
+        read_ckmf("t", _text(aocc="1 1"))
+    with pytest.raises(CkmfError, match="walker path"):
+        read_ckmf("t", _text(extra="sampling_method\n umrigar93_accelerated_sampling")).run_params()
+
+
+def test_run_params_from_flags():
+    from qmcbeaver_b200 import desc as D
+    c = read_ckmf("t", _text(extra="run_type\n diffusion\nsampling_method\n importance_sampling\n"
+                                   "energy_cutoff_type\n bdjm-push88\npopulation_control_parameter\n 100"))
+    p = c.run_params()
+    assert p.run_type == D.QMCB_DMC and p.sampling == D.QMCB_IMPORTANCE_SAMPLING
+    assert p.energy_cutoff == D.QMCB_ECUT_BDJM_PUSH88 and p.population_control == 100.0
+    assert p.dt == 0.02 and p.dt_effective == 0.02
+    assert p.qf_modification == D.QMCB_QF_UMRIGAR93_UNEQUAL   # the reference's default
+
+
+def test_patch_flags_and_strip_three_body():
+    t = patch_flags(_text(), {"dt": 0.5, "one_e_per_iter": 1})
+    c = read_ckmf("t", t)
+    assert c.flags["dt"] == "0.5" and c.flags["one_e_per_iter"] == "1"
+    s = strip_three_body(_text())
+    assert "threeBodyCorrelationFunctionType:" not in s
+    assert read_ckmf("t", s).three_body_blocks == 0 and len(read_ckmf("t", s).jastrow) == 3
+
+
+# ------------------------------------------------------------ the reference
+# Every input the reference ships, with what the reader makes of it.  Two of
+# them the reference itself rejects or this path does not evaluate.
+_EXPECT_ERROR = {"examples/HMX_fast.ckmf": "nuclear charge", "test/ecp.ckmf": "pseudopotentials"}
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_INPUTS), reason="reference tree not present")
+def test_reader_reads_every_reference_input():
+    import glob
+    paths = sorted(glob.glob(REF_INPUTS + "/test/*.ckmf") + glob.glob(REF_INPUTS + "/examples/*.ckmf"))
+    assert len(paths) >= 20
+    for p in paths:
+        rel = os.path.relpath(p, REF_INPUTS)
+        if rel in _EXPECT_ERROR:
+            with pytest.raises(CkmfError, match=_EXPECT_ERROR[rel]):
+                read_ckmf(p)
+            continue
+        c = read_ckmf(p)
+        if c.n_determinants == 1:
+            s = c.to_system(allow_cusp_replacement=True, allow_three_body=True)
+            assert s.n_electrons == int(round(s.Z.sum())) - int(c.flags.get("charge", 0))
+
+
+_CHILD = r"""
+import sys, numpy as np
+sys.path.insert(0, {root!r}); sys.path.insert(0, {root!r} + "/tests")
+from qmcbeaver_b200.ckmf import read_ckmf
+from oracle.evaluators import OracleEvaluator, ReferenceEvaluator
+from helpers import slater_conditions
+path, one_e = {path!r}, {one_e}
+text = open(path).read()
+s = read_ckmf(path).to_system(allow_cusp_replacement=True, allow_three_body=True)
+W, qf, dt = 3, 2, 0.01
+ref = ReferenceEvaluator(s, qf_mod=qf, dt=dt, ckmf_text=text, one_e_per_iter=one_e)
+orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
+R = s.initial_positions(W, seed=5)
+wr, wo = ref.new_walkers(W), orc.new_walkers(W)
+rng = np.random.default_rng(0)
+worst = 0.0
+steps = range(-1, min(2 * s.n_electrons, 40)) if one_e else [-1]
+for step in steps:
+    e = -1 if step < 0 else step % s.n_electrons
+    if e >= 0:
+        R[:, e] += 0.2 * rng.standard_normal((W, 3))
+    ref.evaluate(wr, R, e); orc.evaluate(wo, R, e)
+    a, b = ref.results(wr), orc.results(wo)
+    assert not a["singular"].any()
+    # the all-electron path leaves the per-spin determinants the shim reads
+    # log|psi| and the sign from unset, so those two are compared on the
+    # one-electron path only
+    keys = ["e_local", "lap", "potential", "grad", "mod_grad"]
+    if one_e:
+        assert np.array_equal(a["sign"], b["sign"])
+        keys.append("log_abs_psi")
+    scale = np.maximum(1.0, 2e-15 * slater_conditions(orc, wo, s) / 1e-11)
+    for k in keys:
+        d = np.abs(a[k] - b[k]) / np.maximum(np.abs(a[k]), 1.0)
+        d = d.reshape(W, -1).max(axis=1) / scale
+        worst = max(worst, float(d.max()))
+print("WORST", worst)
+"""
+
+
+# one_e_per_iter = 0 for HMX: the reference's one-electron path copies
+# derivative rows with the full orbital-row width
+# (QMcBeaver/src/QMCWalkerData.cpp:80-93, QMcBeaver/include/Array2D.h:986),
+# which breaks its gradients whenever more orbitals are listed than occupied
+# (HMX lists 516, occupies 76); its all-electron path is the one to compare.
+@pytest.mark.skipif(not reference_available() or not os.path.isdir(REF_INPUTS),
+                    reason="reference tree / build not present")
+@pytest.mark.parametrize("rel,one_e", [
+    ("test/oepi.ckmf", 1), ("test/he.ckmf", 1), ("test/bare.ckmf", 1), ("examples/h2o.ckmf", 1),
+    ("examples/ne0.ckmf", 1), ("examples/ne0P.ckmf", 1), ("examples/H2_hf_631Gss-vmc.ckmf", 1),
+    ("examples/10_Annulene-heart-DZd_CCSDT.HF_CC-PVDZ.DMC.ckmf", 1), ("test/hmx.ckmf", 0)])
+def test_oracle_matches_reference_on_reference_inputs(rel, one_e):
+    code = _CHILD.format(root=ROOT, path=os.path.join(REF_INPUTS, rel), one_e=one_e)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    worst = float([l for l in r.stdout.splitlines() if l.startswith("WORST")][0].split()[1])
+    assert worst < 1e-11, worst

@@ -53,11 +53,15 @@ def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good
     return good.mean()
 
 
-@pytest.mark.parametrize("wl,W,qf,dt,sweeps", [("vmc_water_10e", 100, 0, 0.09, 3),
-                                              ("dmc_6nuc_30e", 64, 2, 0.01, 2),
-                                              ("dmc_6nuc_30e", 16, 1, 0.01, 1)])
-def test_gpu_matches_oracle_workloads(wl, W, qf, dt, sweeps):
-    _oracle_sequence(make_system(wl, seed=3), W, qf, dt, sweeps, 3 * dt ** 0.5, seed=21, slots_offset=5)
+# min_good: the share of walkers that must keep every Slater matrix below
+# the condition limit of the 1e-10 check (the rest are checked at 2e-15 cond)
+@pytest.mark.parametrize("wl,W,qf,dt,sweeps,min_good", [("vmc_water_10e", 100, 0, 0.09, 3, 0.2),
+                                                       ("dmc_6nuc_30e", 64, 2, 0.01, 2, 0.2),
+                                                       ("dmc_6nuc_30e", 16, 1, 0.01, 1, 0.2),
+                                                       ("vmc_cambridge2_16e", 64, 2, 0.01, 3, 0.1)])
+def test_gpu_matches_oracle_workloads(wl, W, qf, dt, sweeps, min_good):
+    _oracle_sequence(make_system(wl, seed=3), W, qf, dt, sweeps, 3 * dt ** 0.5, seed=21, slots_offset=5,
+                     min_good=min_good)
 
 
 def test_gpu_matches_oracle_100_electrons():
