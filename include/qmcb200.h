@@ -70,8 +70,8 @@ extern "C" {
 
 /*
  * Molecular system: what QMCInput reads from the .ckmf &geometry, &basis,
- * &wavefunction and &Jastrow sections for one restricted determinant with
- * Pade two-body Jastrows.
+ * &wavefunction and &Jastrow sections: one or several determinants of
+ * restricted or unrestricted orbitals, Pade / Cambridge2 two-body Jastrows.
  */
 typedef struct qmcb_system_desc {
   int n_nuclei;                 /* M */
@@ -99,6 +99,18 @@ typedef struct qmcb_system_desc {
   int ee_pade[3];               /* up-down, up-up, down-down function (-1 = none) */
   const int *en_pade_up;        /* [M] up electron - nucleus function (-1 = none) */
   const int *en_pade_dn;        /* [M] down electron - nucleus function */
+  /* Several determinants, psi_D = sum_c ci_coeff[c] det_alpha(c) det_beta(c)
+     (QMCWavefunction with Ndeterminants > 1, QMcBeaver/src/QMCWavefunction.cpp:
+     311-472, 873-977; QMCSCFJastrow::update_SCF, QMcBeaver/src/QMCSCFJastrow.cpp:
+     284-327).  n_det <= 1: one determinant of all the mo_alpha / mo_beta rows
+     and the fields below are ignored.  n_det > 1: mo_alpha / mo_beta hold the
+     n_act_alpha / n_act_beta active orbital rows of each spin and every
+     determinant lists the rows of its columns in increasing order. */
+  int n_det;
+  int n_act_alpha, n_act_beta;
+  const int *det_occ_alpha;     /* [n_det][n_alpha] */
+  const int *det_occ_beta;      /* [n_det][n_beta] */
+  const double *ci_coeff;       /* [n_det] */
 } qmcb_system_desc;
 
 /* Sampling / DMC parameters (the QMCFlags fields the path reads). */

@@ -92,6 +92,9 @@ class OracleEvaluator(_Base):
         L.orc_evaluate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.orc_walker_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_walker_inverse.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_walker_inverse_det.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.orc_walker_kappa.argtypes = [C.c_void_p]
+        L.orc_walker_kappa.restype = C.c_double
         L.orc_basis_at.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         self.packed = PackedSystem(system)
         self.system = system
@@ -119,11 +122,18 @@ class OracleEvaluator(_Base):
     def _get(self, w, a, b, c):
         self.lib.orc_walker_get(w, a, b, c)
 
-    def inverse(self, w, beta: int) -> np.ndarray:
+    def inverse(self, w, beta: int, det: int = 0) -> np.ndarray:
+        """Inverse Slater matrix of determinant `det` of one spin."""
         n = self.system.n_beta if beta else self.system.n_alpha
         out = np.zeros((n, n))
-        self.lib.orc_walker_inverse(w, beta, out.ctypes.data_as(C.c_void_p))
+        self.lib.orc_walker_inverse_det(w, beta, det, out.ctypes.data_as(C.c_void_p))
         return out
+
+    def kappa(self, walkers) -> np.ndarray:
+        """Per walker: sum_c |termPR_c lap_c| / max(|lap(D)/D|, 1), the factor
+        by which the determinant-weighted laplacian sum amplifies rounding
+        (1 or less for one determinant)."""
+        return np.array([self.lib.orc_walker_kappa(w) for w in walkers])
 
     def basis_at(self, r) -> np.ndarray:
         out = np.zeros((5, self.system.n_basis))

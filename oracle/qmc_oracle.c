@@ -21,7 +21,11 @@ struct orc_system {
   int *bf_atom, *bf_pow, *bf_nprim, *bf_off;
   double *pexp, *pcoef;
   int *atom_first, *atom_nbf, *atom_lmax; /* per atom function ranges */
-  double *mo_a, *mo_b;                    /* [n][K] */
+  double *mo_a, *mo_b;                    /* [nact][K] orbital rows of each spin */
+  int ndet, nact[2];
+  int *occ[2];                            /* [ndet][n] active row of each column */
+  int *swaps[2];                          /* [ndet][n] columns replaced from det ci-1, -1 ends */
+  double *ci;                             /* [ndet] */
   int npade;
   double *pnum, *pden;
   int *pnn, *pnd;
@@ -36,13 +40,14 @@ struct orc_system {
 
 struct orc_walker {
   const orc_system *s;
-  double *inv[2];     /* [n][n] inv[o*n+e] (Dc_invA / Dc_invB) */
-  double *Dx[2][3];   /* [n][n] derivative rows, row = electron (D_xA) */
-  double *Dxx[2];     /* [n][n] (D_xxA) */
-  double det[2];      /* DcA, DcB */
-  double *rDx[2];     /* [N][3] grad ratios (rDc_xA) */
-  double rDxx[2];     /* rDc_xxA */
-  int sing[2];
+  double *inv[2];     /* [ndet][n][n] inv[o*n+e] per determinant (Dc_invA(ci) / Dc_invB(ci)) */
+  double *Dx[2][3];   /* [n][nact] derivative rows, row = electron (D_xA) */
+  double *Dxx[2];     /* [n][nact] (D_xxA) */
+  double *Dv[2];      /* [n][nact] orbital values (Dw) */
+  double *det[2];     /* [ndet] DcA(ci), DcB(ci) */
+  double *rDx[2];     /* [ndet][n][3] grad ratios (rDc_xA(ci)) */
+  double *rDxx[2];    /* [ndet] rDc_xxA(ci) */
+  int *sing[2];       /* [ndet] */
   double *rij, *rij_uvec, *riA, *riA_uvec;
   double *Uij, *Uij_x, *Uij_xx, *UiA, *UiA_x, *UiA_xx;
   double U, U_xx;
@@ -52,6 +57,7 @@ struct orc_walker {
   double E_L, KE, PE, neE, eeE, lap;
   int singular;
   double logpsi, sign;
+  double kappa;       /* condition number of the determinant-weighted laplacian sum */
 };
 
 static double *dup_d(const double *p, size_t n)
@@ -65,6 +71,40 @@ static int *dup_i(const int *p, size_t n)
   int *q = (int *)malloc(sizeof(int) * (n ? n : 1));
   if (n) memcpy(q, p, sizeof(int) * n);
   return q;
+}
+
+/* The order in which determinant ci's columns are swapped in from
+ * determinant ci-1 so that no intermediate matrix holds one orbital twice
+ * (QMCWavefunction::makeCoefficients, QMcBeaver/src/QMCWavefunction.cpp:924-976).
+ * idx: [ndet][n] active rows; swaps: [ndet][n] receives the columns, -1 ends.
+ * (The reference loops until no blocked swap is left; sorted occupation
+ * lists never block for good, the loop here stops after n passes.) */
+static void make_swaps(const int *idx, int ndet, int n, int *swaps)
+{
+  int *iu = dup_i(idx, (size_t)ndet * n);
+  for (int t = 0; t < ndet * n; t++) swaps[t] = -1;
+  for (int ci = 1; ci < ndet; ci++) {
+    int swap = 0, bad, pass = 0;
+    do {
+      bad = 0;
+      for (int o = 0; o < n; o++) {
+        if (iu[ci * n + o] == iu[(ci - 1) * n + o]) continue;
+        int good = 1;
+        for (int o2 = 0; o2 < n; o2++)
+          if (o != o2 && iu[ci * n + o] == iu[(ci - 1) * n + o2]) {
+            bad = 1;
+            good = 0;
+            break;
+          }
+        if (good) {
+          iu[(ci - 1) * n + o] = iu[ci * n + o];
+          swaps[ci * n + swap] = o;
+          swap++;
+        }
+      }
+    } while (bad && ++pass <= n);
+  }
+  free(iu);
 }
 
 orc_system *orc_system_new(const qmcb_system_desc *d, int qf_mod, double qf_a, double dt)
@@ -83,8 +123,22 @@ orc_system *orc_system_new(const qmcb_system_desc *d, int qf_mod, double qf_a, d
   s->bf_off = dup_i(d->bf_prim_offset, s->K);
   s->pexp = dup_d(d->prim_exponent, d->n_prim_total);
   s->pcoef = dup_d(d->prim_coeff, d->n_prim_total);
-  s->mo_a = dup_d(d->mo_alpha, (size_t)s->na * s->K);
-  s->mo_b = dup_d(d->mo_beta, (size_t)s->nb * s->K);
+  s->ndet = d->n_det > 1 ? d->n_det : 1;
+  s->nact[0] = d->n_det > 1 ? d->n_act_alpha : s->na;
+  s->nact[1] = d->n_det > 1 ? d->n_act_beta : s->nb;
+  s->mo_a = dup_d(d->mo_alpha, (size_t)s->nact[0] * s->K);
+  s->mo_b = dup_d(d->mo_beta, (size_t)s->nact[1] * s->K);
+  s->ci = (double *)malloc(sizeof(double) * s->ndet);
+  for (int c = 0; c < s->ndet; c++) s->ci[c] = d->n_det > 1 ? d->ci_coeff[c] : 1.0;
+  for (int sp = 0; sp < 2; sp++) {
+    int n = sp ? s->nb : s->na;
+    const int *src = sp ? d->det_occ_beta : d->det_occ_alpha;
+    s->occ[sp] = (int *)malloc(sizeof(int) * (size_t)s->ndet * (n ? n : 1));
+    s->swaps[sp] = (int *)malloc(sizeof(int) * (size_t)s->ndet * (n ? n : 1));
+    for (int c = 0; c < s->ndet; c++)
+      for (int o = 0; o < n; o++) s->occ[sp][c * n + o] = d->n_det > 1 ? src[c * n + o] : o;
+    make_swaps(s->occ[sp], s->ndet, n, s->swaps[sp]);
+  }
   s->npade = d->n_pade;
   s->pnum = dup_d(d->pade_num, (size_t)s->npade * QMCB_PADE_MAX);
   s->pden = dup_d(d->pade_den, (size_t)s->npade * QMCB_PADE_MAX);
@@ -133,24 +187,30 @@ void orc_system_free(orc_system *s)
   free(s->bf_off); free(s->pexp); free(s->pcoef); free(s->mo_a); free(s->mo_b); free(s->pnum);
   free(s->pden); free(s->pnn); free(s->pnd); free(s->ctype); free(s->cparam); free(s->en_up); free(s->en_dn);
   free(s->atom_first); free(s->atom_nbf); free(s->atom_lmax);
+  free(s->ci);
+  for (int sp = 0; sp < 2; sp++) { free(s->occ[sp]); free(s->swaps[sp]); }
   free(s);
 }
 
 int orc_num_electrons(const orc_system *s) { return s->N; }
 
 /* ------------------------------------------------------------ walker state */
-#define NFIELDS 29
 static void walker_alloc(orc_walker *w, const orc_system *s)
 {
-  int N = s->N, M = s->M;
+  int N = s->N, M = s->M, nd = s->ndet;
   w->s = s;
   for (int sp = 0; sp < 2; sp++) {
-    int n = sp ? s->nb : s->na;
-    size_t nn = (size_t)(n ? n * n : 1);
-    w->inv[sp] = (double *)calloc(nn, sizeof(double));
-    for (int d = 0; d < 3; d++) w->Dx[sp][d] = (double *)calloc(nn, sizeof(double));
-    w->Dxx[sp] = (double *)calloc(nn, sizeof(double));
-    w->rDx[sp] = (double *)calloc((size_t)N * 3, sizeof(double));
+    int n = sp ? s->nb : s->na, a = s->nact[sp];
+    size_t nn = (size_t)(n ? n * n : 1), na_ = (size_t)(n && a ? n * a : 1);
+    w->inv[sp] = (double *)calloc(nn * nd, sizeof(double));
+    for (int d = 0; d < 3; d++) w->Dx[sp][d] = (double *)calloc(na_, sizeof(double));
+    w->Dxx[sp] = (double *)calloc(na_, sizeof(double));
+    w->Dv[sp] = (double *)calloc(na_, sizeof(double));
+    w->det[sp] = (double *)calloc(nd, sizeof(double));
+    w->rDx[sp] = (double *)calloc((size_t)nd * N * 3, sizeof(double));
+    w->rDxx[sp] = (double *)calloc(nd, sizeof(double));
+    w->sing[sp] = (int *)calloc(nd, sizeof(int));
+    for (int c = 0; c < nd; c++) w->det[sp][c] = 1.0;
   }
   w->rij = (double *)calloc((size_t)N * N, sizeof(double));
   w->rij_uvec = (double *)calloc((size_t)N * N * 3, sizeof(double));
@@ -172,7 +232,6 @@ orc_walker *orc_walker_new(const orc_system *s)
 {
   orc_walker *w = (orc_walker *)calloc(1, sizeof(orc_walker));
   walker_alloc(w, s);
-  w->det[0] = w->det[1] = 1.0;
   return w;
 }
 
@@ -183,7 +242,11 @@ void orc_walker_free(orc_walker *w)
     free(w->inv[sp]);
     for (int d = 0; d < 3; d++) free(w->Dx[sp][d]);
     free(w->Dxx[sp]);
+    free(w->Dv[sp]);
+    free(w->det[sp]);
     free(w->rDx[sp]);
+    free(w->rDxx[sp]);
+    free(w->sing[sp]);
   }
   free(w->rij); free(w->rij_uvec); free(w->riA); free(w->riA_uvec); free(w->Uij); free(w->Uij_x);
   free(w->Uij_xx); free(w->UiA); free(w->UiA_x); free(w->UiA_xx); free(w->U_x); free(w->D_x);
@@ -194,17 +257,18 @@ void orc_walker_free(orc_walker *w)
 void orc_walker_copy(orc_walker *dst, const orc_walker *src)
 {
   const orc_system *s = src->s;
-  int N = s->N, M = s->M;
+  int N = s->N, M = s->M, nd = s->ndet;
   for (int sp = 0; sp < 2; sp++) {
-    int n = sp ? s->nb : s->na;
-    size_t nn = (size_t)(n ? n * n : 1);
-    memcpy(dst->inv[sp], src->inv[sp], nn * sizeof(double));
-    for (int d = 0; d < 3; d++) memcpy(dst->Dx[sp][d], src->Dx[sp][d], nn * sizeof(double));
-    memcpy(dst->Dxx[sp], src->Dxx[sp], nn * sizeof(double));
-    memcpy(dst->rDx[sp], src->rDx[sp], (size_t)N * 3 * sizeof(double));
-    dst->det[sp] = src->det[sp];
-    dst->rDxx[sp] = src->rDxx[sp];
-    dst->sing[sp] = src->sing[sp];
+    int n = sp ? s->nb : s->na, a = s->nact[sp];
+    size_t nn = (size_t)(n ? n * n : 1), na_ = (size_t)(n && a ? n * a : 1);
+    memcpy(dst->inv[sp], src->inv[sp], nn * nd * sizeof(double));
+    for (int d = 0; d < 3; d++) memcpy(dst->Dx[sp][d], src->Dx[sp][d], na_ * sizeof(double));
+    memcpy(dst->Dxx[sp], src->Dxx[sp], na_ * sizeof(double));
+    memcpy(dst->Dv[sp], src->Dv[sp], na_ * sizeof(double));
+    memcpy(dst->det[sp], src->det[sp], nd * sizeof(double));
+    memcpy(dst->rDx[sp], src->rDx[sp], (size_t)nd * N * 3 * sizeof(double));
+    memcpy(dst->rDxx[sp], src->rDxx[sp], nd * sizeof(double));
+    memcpy(dst->sing[sp], src->sing[sp], nd * sizeof(int));
   }
   memcpy(dst->rij, src->rij, (size_t)N * N * sizeof(double));
   memcpy(dst->rij_uvec, src->rij_uvec, (size_t)N * N * 3 * sizeof(double));
@@ -486,9 +550,31 @@ static double inverse_update_row(double *inv, int n, int row, const double *v)
   return detRatio;
 }
 
+/* Array2D::inverseUpdateOneColumn (QMcBeaver/include/Array2D.h:1628-1671): the
+ * column `col` of the matrix becomes column `col` of newD (n x n, row-major
+ * [e][o]); inv[o*n+e]. Returns the determinant ratio. */
+static double inverse_update_col(double *inv, int n, int col, const double *newD)
+{
+  double detRatio = 0;
+  for (int c = 0; c < n; c++) detRatio += newD[c * n + col] * inv[col * n + c];
+  double q = 1.0 / detRatio;
+  for (int r = 0; r < n; r++) {
+    if (r == col) continue;
+    double val = 0.0;
+    for (int l = 0; l < n; l++) val += newD[l * n + col] * inv[r * n + l];
+    val *= q;
+    for (int c = 0; c < n; c++) inv[r * n + c] -= val * inv[col * n + c];
+  }
+  for (int c = 0; c < n; c++) inv[col * n + c] *= q;
+  return detRatio;
+}
+
 /* ---------------------------------------------------- Slater spin (a2-a4) */
 /* QMCSlater::evaluate (QMcBeaver/src/QMCSlater.cpp:828-884) followed by
- * update_Ds (:390-541) and calculate_DerivativeRatios (:648-764) for one spin. */
+ * update_Ds (:390-541) and calculate_DerivativeRatios (:648-764) for one spin,
+ * every determinant: the first one by LU (all electrons) or a row update
+ * (one electron), the others by column swaps from the previous determinant
+ * (all electrons) or their own row update (one electron). */
 static void slater_spin(const orc_system *s, orc_walker *w, int sp, const double *R, int whichE)
 {
   int n = sp ? s->nb : s->na;
@@ -499,47 +585,74 @@ static void slater_spin(const orc_system *s, orc_walker *w, int sp, const double
   int start = whichE == -1 ? Start : whichE;
   int stop = whichE == -1 ? Stop : whichE;
   int nUP = stop - start + 1;
-  int K = s->K;
+  int K = s->K, a = s->nact[sp], nd = s->ndet;
   const double *C = sp ? s->mo_b : s->mo_a;
   double *chi = (double *)malloc(sizeof(double) * (size_t)nUP * 5 * K);
-  double *D = (double *)malloc(sizeof(double) * (size_t)5 * nUP * n);
+  double *D = (double *)malloc(sizeof(double) * (size_t)5 * nUP * a);
+  double *ciDet = (double *)malloc(sizeof(double) * (size_t)nUP * n);
   basis_eval(s, R, start, stop, chi);
-  contract(s, chi, nUP, C, n, D);
-  /* splice new derivative rows into D_x / D_xx (QMcBeaver/src/QMCSlater.cpp:465-491) */
+  contract(s, chi, nUP, C, a, D);
+  /* splice new rows into D_x / D_xx (QMcBeaver/src/QMCSlater.cpp:465-491) */
   int iEl = whichE == -1 ? 0 : whichE - Start;
   for (int e = 0; e < nUP; e++)
-    for (int o = 0; o < n; o++) {
-      for (int d = 0; d < 3; d++) w->Dx[sp][d][(iEl + e) * n + o] = D[((size_t)(1 + d) * nUP + e) * n + o];
-      w->Dxx[sp][(iEl + e) * n + o] = D[((size_t)4 * nUP + e) * n + o];
+    for (int o = 0; o < a; o++) {
+      w->Dv[sp][(iEl + e) * a + o] = D[(size_t)e * a + o];
+      for (int d = 0; d < 3; d++) w->Dx[sp][d][(iEl + e) * a + o] = D[((size_t)(1 + d) * nUP + e) * a + o];
+      w->Dxx[sp][(iEl + e) * a + o] = D[((size_t)4 * nUP + e) * a + o];
     }
-  int calcOK = 1;
-  if (whichE == -1) {
-    det_and_inverse(D, n, w->inv[sp], &w->det[sp], &calcOK);
-  } else {
-    double ratio = inverse_update_row(w->inv[sp], n, whichE - Start, D);
-    if (ratio != 0.0)
-      w->det[sp] *= ratio;
-    else
-      calcOK = 0;
-  }
-  w->sing[sp] = !calcOK;
-  if (calcOK) {
-    double lap_PR = 0.0;
-    double *g = w->rDx[sp];
-    for (int e = 0; e < n; e++) g[3 * e] = g[3 * e + 1] = g[3 * e + 2] = 0.0;
-    const double *inv = w->inv[sp];
-    for (int o = 0; o < n; o++)
-      for (int e = 0; e < n; e++) {
-        double inv_v = inv[o * n + e];
-        lap_PR += w->Dxx[sp][e * n + o] * inv_v;
-        g[3 * e + 0] += w->Dx[sp][0][e * n + o] * inv_v;
-        g[3 * e + 1] += w->Dx[sp][1][e * n + o] * inv_v;
-        g[3 * e + 2] += w->Dx[sp][2][e * n + o] * inv_v;
+  for (int ci = 0; ci < nd; ci++) {
+    const int *occ = s->occ[sp] + ci * n;
+    double *inv = w->inv[sp] + (size_t)ci * n * n;
+    /* QMCWavefunction::getDataForCI: the columns of determinant ci */
+    for (int e = 0; e < nUP; e++)
+      for (int o = 0; o < n; o++) ciDet[e * n + o] = D[(size_t)e * a + occ[o]];
+    int calcOK = 1;
+    if (whichE == -1) {
+      if (ci == 0) {
+        det_and_inverse(ciDet, n, inv, &w->det[sp][0], &calcOK);
+      } else {
+        memcpy(inv, inv - (size_t)n * n, sizeof(double) * n * n);
+        w->det[sp][ci] = w->det[sp][ci - 1];
+        for (int o = 0; o < n; o++) {
+          int so = s->swaps[sp][ci * n + o];
+          if (so < 0) break;
+          double ratio = inverse_update_col(inv, n, so, ciDet);
+          w->det[sp][ci] *= ratio;
+          if (ratio == 0) break;
+        }
+        if (w->det[sp][ci] == 0) {
+          calcOK = 0;
+          det_and_inverse(ciDet, n, inv, &w->det[sp][ci], &calcOK);
+        }
       }
-    w->rDxx[sp] = lap_PR;
+    } else {
+      double ratio = inverse_update_row(inv, n, whichE - Start, ciDet);
+      if (ratio != 0.0)
+        w->det[sp][ci] *= ratio;
+      else
+        calcOK = 0;
+    }
+    w->sing[sp][ci] = !calcOK;
+    if (calcOK) {
+      double lap_PR = 0.0;
+      double *g = w->rDx[sp] + (size_t)ci * s->N * 3;
+      for (int e = 0; e < n; e++) g[3 * e] = g[3 * e + 1] = g[3 * e + 2] = 0.0;
+      for (int o = 0; o < n; o++) {
+        int orb = occ[o];
+        for (int e = 0; e < n; e++) {
+          double inv_v = inv[o * n + e];
+          lap_PR += w->Dxx[sp][e * a + orb] * inv_v;
+          g[3 * e + 0] += w->Dx[sp][0][e * a + orb] * inv_v;
+          g[3 * e + 1] += w->Dx[sp][1][e * a + orb] * inv_v;
+          g[3 * e + 2] += w->Dx[sp][2][e * a + orb] * inv_v;
+        }
+      }
+      w->rDxx[sp][ci] = lap_PR;
+    }
   }
   free(chi);
   free(D);
+  free(ciDet);
 }
 
 /* ------------------------------------------------------------ Jastrow (a6) */
@@ -708,18 +821,87 @@ static void potential(const orc_system *s, orc_walker *w)
 static void psi_quantities(const orc_system *s, orc_walker *w, const double *R)
 {
   int N = s->N, na = s->na, nb = s->nb, M = s->M;
-  if (w->sing[0] || w->sing[1]) {
+  int nd = s->ndet, any_sing = 0;
+  for (int ci = 0; ci < nd; ci++) any_sing |= w->sing[0][ci] | w->sing[1][ci];
+  /* update_SCF: D = sum_ci c_ci detA(ci) detB(ci), termPR(ci) = term / D.
+   * The reference keeps D in its extended-exponent QMCDouble, which is plain
+   * double arithmetic while the magnitudes stay within 1e+-100 (each factor)
+   * and 1e+-200 (products); outside that range the terms here are scaled by
+   * the largest |detA detB| instead (log_D = lmax + log|Dtot|). */
+  double Dtot = 1.0, lmax = 0.0;
+  if (any_sing) {
     w->singular = 1;
   } else {
+    double *termPR = (double *)malloc(sizeof(double) * nd);
+    int plain = 1; /* magnitudes where QMCDouble keeps everything in its plain mantissa */
+    for (int ci = 0; ci < nd; ci++) {
+      double a = fabs(w->det[0][ci]), b = fabs(w->det[1][ci]), t = a * b;
+      if (a > 1e100 || a < 1e-100 || b > 1e100 || b < 1e-100 || t > 1e200 || t < 1e-200) plain = 0;
+    }
+    if (nd == 1) {
+      termPR[0] = 1.0;
+    } else if (plain) {
+      Dtot = 0.0;
+      for (int ci = 0; ci < nd; ci++) {
+        termPR[ci] = s->ci[ci] * w->det[0][ci] * w->det[1][ci];
+        Dtot += termPR[ci];
+      }
+      if (Dtot != 0.0)
+        for (int ci = 0; ci < nd; ci++) termPR[ci] /= Dtot;
+      lmax = 0.0;
+    } else {
+      lmax = -INFINITY;
+      for (int ci = 0; ci < nd; ci++) {
+        double l = log(fabs(w->det[0][ci])) + log(fabs(w->det[1][ci]));
+        if (s->ci[ci] != 0.0 && l > lmax) lmax = l;
+      }
+      Dtot = 0.0;
+      for (int ci = 0; ci < nd; ci++) {
+        double sg = (w->det[0][ci] < 0) != (w->det[1][ci] < 0) ? -1.0 : 1.0;
+        termPR[ci] = s->ci[ci] * sg * exp(log(fabs(w->det[0][ci])) + log(fabs(w->det[1][ci])) - lmax);
+        Dtot += termPR[ci];
+      }
+      if (Dtot != 0.0)
+        for (int ci = 0; ci < nd; ci++) termPR[ci] /= Dtot;
+    }
     w->D_xx = 0.0;
     for (int i = 0; i < 3 * N; i++) w->D_x[i] = 0.0;
-    double termPR = 1.0;
-    if (na > 0) w->D_xx += termPR * w->rDxx[0];
-    if (nb > 0) w->D_xx += termPR * w->rDxx[1];
-    for (int e = 0; e < na; e++)
-      for (int k = 0; k < 3; k++) w->D_x[e * 3 + k] += termPR * w->rDx[0][e * 3 + k];
-    for (int e = 0; e < nb; e++)
-      for (int k = 0; k < 3; k++) w->D_x[(e + na) * 3 + k] += termPR * w->rDx[1][e * 3 + k];
+    /* determinant-mixing amplification of rounding in the laplacian:
+     * [sum_c |t_c lap_c| + 2 sum_i |U_x,i| . sum_c |t_c g_c,i|] over the same
+     * sums without the absolute values inside (1 for one determinant) */
+    double abs_l = 0.0, sum_l = 0.0, abs_g = 0.0, sum_g = 0.0;
+    for (int ci = 0; ci < nd; ci++) {
+      double l = (na > 0 ? w->rDxx[0][ci] : 0.0) + (nb > 0 ? w->rDxx[1][ci] : 0.0);
+      abs_l += fabs(termPR[ci] * l);
+      sum_l += termPR[ci] * l;
+    }
+    for (int i = 0; i < N; i++) {
+      int sp_i = i < na ? 0 : 1, e = i < na ? i : i - na;
+      for (int k = 0; k < 3; k++) {
+        double a = 0.0, b = 0.0;
+        for (int ci = 0; ci < nd; ci++) {
+          double g = w->rDx[sp_i][((size_t)ci * N + e) * 3 + k];
+          a += fabs(termPR[ci] * g);
+          b += termPR[ci] * g;
+        }
+        abs_g += fabs(w->U_x[3 * i + k]) * a;
+        sum_g += fabs(w->U_x[3 * i + k] * b);
+      }
+    }
+    for (int ci = 0; ci < nd; ci++) {
+      if (na > 0) w->D_xx += termPR[ci] * w->rDxx[0][ci];
+      if (nb > 0) w->D_xx += termPR[ci] * w->rDxx[1][ci];
+      const double *ga = w->rDx[0] + (size_t)ci * N * 3, *gb = w->rDx[1] + (size_t)ci * N * 3;
+      for (int e = 0; e < na; e++)
+        for (int k = 0; k < 3; k++) w->D_x[e * 3 + k] += termPR[ci] * ga[e * 3 + k];
+      for (int e = 0; e < nb; e++)
+        for (int k = 0; k < 3; k++) w->D_x[(e + na) * 3 + k] += termPR[ci] * gb[e * 3 + k];
+    }
+    free(termPR);
+    {
+      double den = fabs(sum_l) + 2.0 * sum_g;
+      w->kappa = (abs_l + 2.0 * abs_g) / (den > 1.0 ? den : 1.0);
+    }
     double L = w->D_xx + w->U_xx;
     for (int i = 0; i < N; i++)
       for (int j = 0; j < 3; j++) {
@@ -783,8 +965,13 @@ static void psi_quantities(const orc_system *s, orc_walker *w, const double *R)
   if (isnan(lm) || isnan(lu) || isnan(lm / lu) || lu == 0) w->singular = 1;
   w->KE = -0.5 * w->lap;
   w->E_L = -0.5 * w->lap + w->PE;
-  w->logpsi = log(fabs(w->det[0])) + log(fabs(w->det[1])) + w->U;
-  w->sign = (w->det[0] * w->det[1] < 0) ? -1.0 : 1.0;
+  if (nd == 1) {
+    w->logpsi = log(fabs(w->det[0][0])) + log(fabs(w->det[1][0])) + w->U;
+    w->sign = (w->det[0][0] * w->det[1][0] < 0) ? -1.0 : 1.0;
+  } else {
+    w->logpsi = lmax + log(fabs(Dtot)) + w->U;
+    w->sign = Dtot < 0 ? -1.0 : 1.0;
+  }
 }
 
 /* --------------------------------------------------------- evaluate (a1) */
@@ -818,8 +1005,8 @@ void orc_walker_get(const orc_walker *w, double *sc, double *grad, double *mgrad
   sc[5] = w->U;
   sc[6] = w->U_xx;
   sc[7] = w->D_xx;
-  sc[8] = w->s->na > 0 ? w->det[0] : 1.0;
-  sc[9] = w->s->nb > 0 ? w->det[1] : 1.0;
+  sc[8] = w->s->na > 0 ? w->det[0][0] : 1.0;
+  sc[9] = w->s->nb > 0 ? w->det[1][0] : 1.0;
   sc[10] = w->singular ? 1.0 : 0.0;
   sc[11] = w->logpsi;
   sc[12] = w->sign;
@@ -830,8 +1017,20 @@ void orc_walker_get(const orc_walker *w, double *sc, double *grad, double *mgrad
   }
 }
 
+/* the inverse of determinant 0 (Dc_invA(0) / Dc_invB(0)) */
 void orc_walker_inverse(const orc_walker *w, int beta, double *out)
 {
   int n = beta ? w->s->nb : w->s->na;
   memcpy(out, w->inv[beta ? 1 : 0], sizeof(double) * n * n);
+}
+
+/* how much more the determinant-weighted sums of the laplacian amplify
+ * rounding than a single determinant would (1 for one determinant) */
+double orc_walker_kappa(const orc_walker *w) { return w->kappa; }
+
+/* the inverse of determinant ci */
+void orc_walker_inverse_det(const orc_walker *w, int beta, int ci, double *out)
+{
+  int n = beta ? w->s->nb : w->s->na;
+  memcpy(out, w->inv[beta ? 1 : 0] + (size_t)ci * n * n, sizeof(double) * n * n);
 }

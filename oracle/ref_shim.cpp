@@ -109,6 +109,18 @@ void ref_walker_get(void *w, double *scalars, double *grad, double *mgrad)
   scalars[10] = wd->singular ? 1.0 : 0.0;
   scalars[11] = std::log(std::fabs(da)) + std::log(std::fabs(db)) + wd->U;
   scalars[12] = (da * db < 0) ? -1.0 : 1.0;
+  const int ndet = globalInput.WF.getNumberDeterminants();
+  if (ndet > 1) {
+    // psi_D = sum_ci c_ci DcA(ci) DcB(ci) (QMCSCFJastrow::update_SCF)
+    double D = 0.0;
+    for (int ci = 0; ci < ndet; ci++) {
+      double a = wd->DcA.dim1() > ci ? wd->DcA(ci) : 1.0;
+      double b = wd->DcB.dim1() > ci ? wd->DcB(ci) : 1.0;
+      D += globalInput.WF.CI_coeffs(ci) * a * b;
+    }
+    scalars[11] = std::log(std::fabs(D)) + wd->U;
+    scalars[12] = D < 0 ? -1.0 : 1.0;
+  }
   scalars[13] = (double)wd->psi;
   for (int e = 0; e < g_nel; e++)
     for (int d = 0; d < 3; d++) {

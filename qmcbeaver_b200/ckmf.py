@@ -172,7 +172,7 @@ class CkmfInput:
     # ------------------------------------------------------------ system
     def to_system(self, allow_cusp_replacement: bool = False, allow_three_body: bool = False,
                   name: Optional[str] = None) -> MolecularSystem:
-        """The single-determinant Slater-Jastrow system of this input.
+        """The Slater-Jastrow system of this input (one or several determinants).
 
         Refuses inputs that switch on features the walker path does not
         evaluate, unless told to drop them: cusp replacement
@@ -180,8 +180,6 @@ class CkmfInput:
         three-body Jastrow blocks."""
         if self.flag("trial_function_type", "restricted") not in ("restricted", "unrestricted"):
             raise CkmfError("only restricted / unrestricted trial functions are read")
-        if self.n_determinants != 1:
-            raise CkmfError(f"{self.n_determinants} determinants: the walker path evaluates one")
         if self.flag("replace_electron_nucleus_cusps", 1, int) and not allow_cusp_replacement:
             raise CkmfError("replace_electron_nucleus_cusps is on; pass allow_cusp_replacement=True to drop it")
         # the reference evaluates every used three-body block in the file,
@@ -193,6 +191,13 @@ class CkmfInput:
             raise CkmfError("more beta than alpha electrons")
         a_occ = np.nonzero(self.alpha_occupation[0])[0]
         b_occ = np.nonzero(self.beta_occupation[0])[0]
+        det_a = det_b = ci = None
+        if self.n_determinants > 1:
+            det_a = np.array([np.nonzero(r)[0] for r in self.alpha_occupation])
+            det_b = np.array([np.nonzero(r)[0] for r in self.beta_occupation]).reshape(self.n_determinants, nb)
+            if det_a.ndim != 2 or det_a.shape[1] != na:
+                raise CkmfError("every determinant must occupy the same number of orbitals per spin")
+            ci = np.asarray(self.ci_coeffs, np.float64)
         a_diag = self.flag("a_diag", -1e-5, float)
         link = self.flag("link_Jastrow_parameters", 1, int) == 1
         ee_anti = ee_up = ee_dn = None
@@ -232,7 +237,7 @@ class CkmfInput:
             labels=list(self.labels), Z=np.asarray(self.Z, float), coords=np.asarray(self.coords, float),
             basis=self.basis, mo=np.asarray(self.orbitals, float), n_alpha=na, n_beta=nb,
             alpha_occ=a_occ, beta_occ=b_occ, ee_anti=ee_anti, ee_para_up=ee_up, ee_para_dn=ee_dn,
-            en_up=en_up, en_dn=en_dn, name=name or self.path)
+            en_up=en_up, en_dn=en_dn, name=name or self.path, det_alpha=det_a, det_beta=det_b, ci_coeffs=ci)
 
     def run_params(self, **overrides) -> D.RunParams:
         """The library's run parameters for this input's flags

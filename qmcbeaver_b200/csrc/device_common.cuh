@@ -41,6 +41,8 @@ enum Sc {
   SC_MODRATIO,     // |modified grad| / |grad|
   SC_AGE_MOVED,    // age when the walker last moved
   SC_DW,           // weight factor of the last reweight
+  SC_MDCUR_A,      // several determinants: current copy (0/1) of the spin's determinant block
+  SC_MDCUR_B,
   SC_COUNT
 };
 constexpr int kScalars = 24;  // padded
@@ -49,6 +51,11 @@ constexpr int kShellPrim = 6;  // primitives kept in registers per shell
 
 struct DevSys {
   int M, na, nb, N, K, npade, nshell;
+  int ndet;              // determinants (1: the one-determinant kernels)
+  int nact[2];           // active orbital rows per spin (= na, nb for one determinant)
+  const int *docc[2];    // [ndet][n] active row of each determinant column
+  const int *dswap[2];   // [ndet][n] columns swapped in from determinant c-1 (-1 ends)
+  const double *ci;      // [ndet] CI coefficients
   int ee[3];
   double Pnn;
   const double4 *nuc;    // [M] x, y, z, Z
@@ -73,15 +80,19 @@ struct DevSys {
 struct Layout {
   int stride;
   int R;         // [N][3]
-  int Dv[2];     // [n][n]  electron-major Slater values
-  int DgT[2];    // [3][n][n] orbital-major gradients
-  int DlT[2];    // [n][n]    orbital-major laplacians
-  int Inv[2];    // [n][n]    Inv[o][e]
+  int Dv[2];     // [n][a]  electron-major Slater values (a = active orbitals, = n
+                 //         for one determinant)
+  int DgT[2];    // [3][a][n] orbital-major gradients
+  int DlT[2];    // [a][n]    orbital-major laplacians
+  int Inv[2];    // [n][n]    Inv[o][e]; several determinants: two copies of
+                 // [ndet][n][n] inverses | [ndet][n][3] grad ratios | [ndet][4]
+                 // (ln|det|, sign, lap ratio, singular), mdsz doubles each
   int gradD;     // [N][3] grad(D)/D per electron (rDc_x of its spin)
   int Ux;        // [N][3] grad ln J
   int grad;      // [N][3] gradPsiRatio
   int mgrad;     // [N][3] modifiedGradPsiRatio
   int sc;        // [kScalars]
+  int mdsz[2];   // several determinants: doubles in one copy of the determinant block
   // move-kernel scratch (doubles, even counts): region A, rows, factors,
   // staged positions, staged per-electron tail, staged spin block, stride
   int mv_region_a, mv_dn, mv_valc, mv_r, mv_tail, mv_spin[2], mv_stride;

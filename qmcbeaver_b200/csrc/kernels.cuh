@@ -320,7 +320,6 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
   double *vv = X + nmax * nmax;
   double *piv = vv + nmax;
   double *Rs = piv + nmax;
-  double *part = Rs + 3 * N;
   double *R = blk + L.R;
   double *sc = blk + L.sc;
 
@@ -439,14 +438,6 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
     for (int t = lane; t < 3 * N; t += 32) out.mgrad[(size_t)wi * 3 * N + t] = mg[t];
 }
 
-// ------------------------------------------------------------------------
-// One single-electron move of electron e for every walker in the list.
-// kMetropolis = false: the caller's positions R_in[wi] are taken and the
-// new state is committed unconditionally (QMCFunctions::evaluate with
-// whichE = e).  kMetropolis = true: proposal from the walker's own random
-// stream, acceptance test, DMC reweight when do_reweight, commit on accept
-// (QMCWalker::initializePropagation / processPropagation,
-// QMcBeaver/src/QMCWalker.cpp:179-282).
 struct MoveArgs {
   int e;             // moved electron
   int step;          // global step number (random stream position)
@@ -454,66 +445,28 @@ struct MoveArgs {
   int reweight_on;   // step >= reweight_start_step
 };
 
-template <bool kMetropolis, typename TS, typename TI>
-__global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
-                                              int num, const int *d_num, const double *R_in, MoveArgs mv,
-                                              const EnergyCtl *ectl, double *stats, EvalOut out)
+// ------------------------------------------------------------------------
+// Pieces of the single-electron move shared by the one- and the
+// several-determinant move kernels.
+
+// New position of electron e: the walker's own Philox stream and the drift
+// (QMCWalker::moveElectronsNoImportanceSampling / moveElectronsImportanceSampling,
+// QMcBeaver/src/QMCWalker.cpp:313-398), or the caller's position.  g_fwd is
+// the exponent sum of G(R -> R'), u_acc the acceptance uniform.
+template <bool kMetropolis>
+__device__ __forceinline__ void propose_move(const RunCfg &cfg, int slot, int step, int e, int N, const double ro[3],
+                                             const double *mgo, const double *R_in, int wi, double rn[3],
+                                             double &g_fwd, double &u_acc)
 {
-  extern __shared__ double smem[];
-  const int lane = lane_id(), warp = threadIdx.x >> 5;
-  const int nw = d_num ? *d_num : num;
-  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (wi >= nw) return;
-  const int N = S.N, K = S.K;
-  const int e = mv.e;
-  const int sp = e < S.na ? 0 : 1;
-  const int n = sp ? S.nb : S.na, base = sp ? S.na : 0, el = e - base;
-  const int slot = slots ? slots[wi] : wi;
-  double *blk = state + (size_t)slot * L.stride;
-
-  // ---- scratch of this warp (offsets in doubles, all even: 16-byte aligned)
-  double *sm = smem + (size_t)warp * L.mv_stride;
-  const int ldc = K;
-  TS *chi = (TS *)sm;                  // region A: basis values ...
-  TS *cpart = (TS *)sm;                // ... then contraction slice sums
-  double *part = sm;                   // ... then ratio-sum slice sums
-  double *gr = sm + kPart;             // ... and the new drift / modified drift
-  double *mg = gr + 3 * N;
-  TS *Dn = (TS *)(sm + L.mv_region_a); // new Slater / derivative rows [5][n]
-  TI *valc = (TI *)(sm + L.mv_region_a + L.mv_dn);  // Sherman-Morrison factors [n]
-  double *sR = sm + L.mv_region_a + L.mv_dn + L.mv_valc;  // positions (electron e updated in place)
-  double *sT = sR + L.mv_r;            // gradD, Ux, grad, mgrad, scalars (prefetched copy)
-  double *sS = sT + L.mv_tail;         // inverse of the moved spin (prefetched copy)
-  double *gD = sT;                     // grad(D)/D, updated in place for the moved spin
-  double *Ux = sT + (L.Ux - L.gradD);  // grad ln J, updated in place
-  const double *mgo = sT + (L.mgrad - L.gradD);
-  const double *sc0 = sT + (L.sc - L.gradD);
-  const TS *DgT = (const TS *)(blk + L.DgT[sp]);  // read once per move by the ratio sums
-  const TS *DlT = (const TS *)(blk + L.DlT[sp]);
-  TI *Inv = (TI *)sS;
-  double *sc = blk + L.sc;
-  const int inv_d = even((n * n * (int)sizeof(TI) + 7) / 8);
-
-  // ---- stage the walker's state: positions and the per-electron arrays
-  //      first, the moved spin's inverse as a second group that lands while
-  //      the basis and orbital rows are computed
-  warp_copy_async(sR, blk + L.R, L.mv_r);
-  warp_copy_async(sT, blk + L.gradD, L.mv_tail);
-  cp_async_commit();
-  warp_copy_async(sS, blk + L.Inv[sp], inv_d);
-  cp_async_commit();
-  cp_async_wait<1>();
-  __syncwarp();
-
-  const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
-  double rn[3];
-  double g_fwd = 0.0, g_unmoved = 0.0, u_acc = 0.5;
+  const int lane = lane_id();
+  g_fwd = 0.0;
+  u_acc = 0.5;
   if (kMetropolis) {
     // lanes 0-2 draw the three Gaussian displacements, lane 3 the acceptance
     // uniform, each from its own Philox counter; one round trip for the warp
     double zr, z[3];
     {
-      const U4 c = philox4x32(U4{(uint32_t)slot, (uint32_t)mv.step, (uint32_t)(lane & 3), 0x51ED2701u}, cfg.seed);
+      const U4 c = philox4x32(U4{(uint32_t)slot, (uint32_t)step, (uint32_t)(lane & 3), 0x51ED2701u}, cfg.seed);
       // Box-Muller in single precision: the proposal only needs a Gaussian
       // sample, not a particular one (the random streams differ from the
       // reference's ran1 in any case)
@@ -545,17 +498,24 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
         const double dd = cfg.dt * mgo[t];
         prt += dd * dd;
       }
-      g_unmoved = warp_sum(prt);
-      g_fwd += g_unmoved;
+      g_fwd += warp_sum(prt);
     }
   } else {
     for (int d = 0; d < 3; d++) rn[d] = R_in[(size_t)wi * 3 * N + 3 * e + d];
   }
+}
 
-  // ---- incremental Jastrow + potential (QMCJastrowElectronElectron::updateOne,
-  //      QMCJastrowElectronNuclear::evaluate, QMCPotential_Energy::evaluate);
-  //      lane j updates its own U_x[j] in place, U_x[e] is reduced afterwards
-  double dU = 0, dUxx = 0, ge[3] = {0, 0, 0}, dVee = 0, dVen = 0;
+// Incremental Jastrow + potential of moving electron e from ro to rn
+// (QMCJastrowElectronElectron::updateOne, QMCJastrowElectronNuclear::evaluate,
+// QMCPotential_Energy::evaluate); lane j updates its own U_x[j] in place,
+// U_x[e] and the staged position of e are written last.
+__device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR, double *Ux, int e, int sp,
+                                                     const double ro[3], const double rn[3], double &dU,
+                                                     double &dUxx, double &dVee, double &dVen)
+{
+  const int lane = lane_id(), N = S.N;
+  double ge[3] = {0, 0, 0};
+  dU = dUxx = dVee = dVen = 0.0;
   const double uxe[3] = {Ux[3 * e], Ux[3 * e + 1], Ux[3 * e + 2]};
   __syncwarp();
   for (int j = lane; j < N; j += 32) {
@@ -616,6 +576,207 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
       Ux[3 * e + d] = uxe[d] + ge[d];
       sR[3 * e + d] = rn[d];
     }
+}
+
+// Acceptance (QMCWalker::calculateMoveAcceptanceProbability,
+// QMcBeaver/src/QMCWalker.cpp:1578-1654), DMC reweight (reweight_walker,
+// :1060-1185) and observables (:2096-2123, 2306-2387) of one proposed move.
+// log_ratio = ln|psi'/psi|, negative = the ratio changed sign.  Writes the
+// walker's weight, age and the per-call sums; returns the acceptance.
+__device__ __forceinline__ bool metropolis_reweight(const RunCfg &cfg, const MoveArgs &mv, const EnergyCtl *ectl,
+                                                    double *stats, double *sc, const double *sc0, int N, int e,
+                                                    const double ro[3], const double rn[3], const double *mg,
+                                                    double g_fwd, double u_acc, double log_ratio, bool negative,
+                                                    bool bad, double EL, double modratio)
+{
+  const int lane = lane_id();
+  // G(R' -> R): only electron e moved, the others contribute (dt v'_i)^2
+  double log_g = 0.0;
+  if (cfg.sampling == 1) {
+    double pr = 0.0;
+    for (int t = lane; t < 3 * N; t += 32) {
+      const double tt = (t / 3 == e) ? (ro[t - 3 * e] - rn[t - 3 * e] - cfg.dt * mg[t]) : (cfg.dt * mg[t]);
+      pr += tt * tt;
+    }
+    const double g_rev = warp_sum(pr);
+    log_g = -(g_rev - g_fwd) / (2.0 * cfg.dt);
+  }
+  double p = exp(2.0 * log_ratio + log_g);
+  const double age = sc0[SC_AGE];
+  const double over = age - cfg.old_walker_acceptance;
+  if (!isnan(p)) {
+    if (over > 500)
+      p = 1.0;
+    else if (over > 0)
+      p *= pow(1.1, over);
+  } else {
+    p = 0.0;
+  }
+  if (bad) p = 0.0;
+  if (cfg.run_type == 1 && negative) p = 0.0;
+  if (p > 1.0) p = 1.0;
+  const bool accept = p > u_acc;
+  const double new_age = accept ? 0.0 : age + 1.0;
+  double w = sc0[SC_WEIGHT];
+  if (mv.do_reweight) {
+    if (cfg.run_type == 1 && mv.reweight_on) {
+      const double ET = ectl->e_trial, Eest = ectl->e_est;
+      const double mo = sc0[SC_MODRATIO];
+      double Eo = sc0[SC_EL];
+      double Et = bad ? Eo : EL;
+      if (cfg.ecut == 1) {
+        Et *= bad ? mo : modratio;
+        Eo *= mo;
+      } else if (cfg.ecut == 2) {
+        // DePasquale, Rothstein, Vrbik (1988) cutoff |E_L - E_orig| <= 2 / sqrt(dt)
+        const double cut = 2.0 / sqrt(cfg.dt);
+        Et = fmin(fmax(Et, cfg.e_orig - cut), cfg.e_orig + cut);
+        Eo = fmin(fmax(Eo, cfg.e_orig - cut), cfg.e_orig + cut);
+      }
+      double St, So;
+      if (cfg.emod == 0) {
+        St = ET - Et;
+        So = ET - Eo;
+      } else if (cfg.emod == 2) {
+        St = (ET - Et) * (bad ? mo : modratio);
+        So = (ET - Eo) * mo;
+      } else {
+        St = (ET - Eest) + (Eest - Et) * (bad ? mo : modratio);
+        So = (ET - Eest) + (Eest - Eo) * mo;
+      }
+      double rw;
+      if (cfg.reweighting == 0)
+        rw = 0.5 * (St + So);
+      else if (cfg.reweighting == 1)
+        rw = accept ? 0.5 * (St + So) : So;
+      else
+        rw = p * 0.5 * (So + St) + (1.0 - p) * So;
+      const double dW = exp(rw * cfg.dt_eff);
+      if (new_age - cfg.old_walker_acceptance > 0)
+        w *= 0.9;
+      else
+        w *= dW;
+      if (lane == 0) sc[SC_DW] = dW;
+      // a non-finite weight (NaN energy or exp overflow) removes the walker
+      // at the next branching instead of poisoning the ensemble sums
+      if (!isfinite(w)) w = 0.0;
+    }
+    const double Eobs = p * (bad ? 0.0 : EL) + (1.0 - p) * sc0[SC_EL];
+    // rel_cutoff filter of QMCWalker::calculateObservables (QMcBeaver/src/QMCWalker.cpp:2336-2351)
+    const bool in_avg = fabs((Eobs - cfg.e_orig) / cfg.e_orig) < cfg.rel_cutoff;
+    if (lane == 0 && w > 0.0 && in_avg) {
+      atomicAdd(&stats[ST_SUM_W], w);
+      atomicAdd(&stats[ST_SUM_WE], w * Eobs);
+      atomicAdd(&stats[ST_SUM_WE2], w * Eobs * Eobs);
+      atomicAdd(&stats[ST_RUN_SUM_W], w);
+      atomicAdd(&stats[ST_RUN_SUM_WE], w * Eobs);
+      atomicAdd(&stats[ST_RUN_COUNT], 1.0);
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(&stats[ST_SUM_ACC], p);
+    atomicAdd(&stats[ST_MOVES], 1.0);
+    if (bad) atomicAdd(&stats[ST_SINGULAR], 1.0);
+    sc[SC_WEIGHT] = w;
+    sc[SC_AGE] = new_age;
+    if (accept) sc[SC_AGE_MOVED] = age;
+  }
+  return accept;
+}
+
+// Outputs of one evaluate call for walker wi.
+__device__ __forceinline__ void write_eval_out(const EvalOut &out, int wi, int N, double log_abs_psi, double sign,
+                                               double lap, double EL, double PE, double Ven, double Vee, bool bad,
+                                               const double *gr, const double *mg)
+{
+  const int lane = lane_id();
+  if (lane == 0) {
+    unsigned st = bad ? 1u : 0u;
+    if (isnan(EL) || isnan(lap)) st |= 2u;
+    if (out.log_abs_psi) out.log_abs_psi[wi] = log_abs_psi;
+    if (out.sign) out.sign[wi] = sign;
+    if (out.lap) out.lap[wi] = lap;
+    if (out.e_local) out.e_local[wi] = EL;
+    if (out.pe) {
+      out.pe[3 * wi] = PE;
+      out.pe[3 * wi + 1] = Ven;
+      out.pe[3 * wi + 2] = Vee;
+    }
+    if (out.status) out.status[wi] = (unsigned char)st;
+  }
+  if (out.grad)
+    for (int t = lane; t < 3 * N; t += 32) out.grad[(size_t)wi * 3 * N + t] = gr[t];
+  if (out.mgrad)
+    for (int t = lane; t < 3 * N; t += 32) out.mgrad[(size_t)wi * 3 * N + t] = mg[t];
+}
+
+// ------------------------------------------------------------------------
+// One single-electron move of electron e for every walker in the list.
+// kMetropolis = false: the caller's positions R_in[wi] are taken and the
+// new state is committed unconditionally (QMCFunctions::evaluate with
+// whichE = e).  kMetropolis = true: proposal from the walker's own random
+// stream, acceptance test, DMC reweight when do_reweight, commit on accept
+// (QMCWalker::initializePropagation / processPropagation,
+// QMcBeaver/src/QMCWalker.cpp:179-282).
+
+template <bool kMetropolis, typename TS, typename TI>
+__global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+                                              int num, const int *d_num, const double *R_in, MoveArgs mv,
+                                              const EnergyCtl *ectl, double *stats, EvalOut out)
+{
+  extern __shared__ double smem[];
+  const int lane = lane_id(), warp = threadIdx.x >> 5;
+  const int nw = d_num ? *d_num : num;
+  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (wi >= nw) return;
+  const int N = S.N, K = S.K;
+  const int e = mv.e;
+  const int sp = e < S.na ? 0 : 1;
+  const int n = sp ? S.nb : S.na, base = sp ? S.na : 0, el = e - base;
+  const int slot = slots ? slots[wi] : wi;
+  double *blk = state + (size_t)slot * L.stride;
+
+  // ---- scratch of this warp (offsets in doubles, all even: 16-byte aligned)
+  double *sm = smem + (size_t)warp * L.mv_stride;
+  const int ldc = K;
+  TS *chi = (TS *)sm;                  // region A: basis values ...
+  TS *cpart = (TS *)sm;                // ... then contraction slice sums
+  double *part = sm;                   // ... then ratio-sum slice sums
+  double *gr = sm + kPart;             // ... and the new drift / modified drift
+  double *mg = gr + 3 * N;
+  TS *Dn = (TS *)(sm + L.mv_region_a); // new Slater / derivative rows [5][n]
+  TI *valc = (TI *)(sm + L.mv_region_a + L.mv_dn);  // Sherman-Morrison factors [n]
+  double *sR = sm + L.mv_region_a + L.mv_dn + L.mv_valc;  // positions (electron e updated in place)
+  double *sT = sR + L.mv_r;            // gradD, Ux, grad, mgrad, scalars (prefetched copy)
+  double *sS = sT + L.mv_tail;         // inverse of the moved spin (prefetched copy)
+  double *gD = sT;                     // grad(D)/D, updated in place for the moved spin
+  double *Ux = sT + (L.Ux - L.gradD);  // grad ln J, updated in place
+  const double *mgo = sT + (L.mgrad - L.gradD);
+  const double *sc0 = sT + (L.sc - L.gradD);
+  const TS *DgT = (const TS *)(blk + L.DgT[sp]);  // read once per move by the ratio sums
+  const TS *DlT = (const TS *)(blk + L.DlT[sp]);
+  TI *Inv = (TI *)sS;
+  double *sc = blk + L.sc;
+  const int inv_d = even((n * n * (int)sizeof(TI) + 7) / 8);
+
+  // ---- stage the walker's state: positions and the per-electron arrays
+  //      first, the moved spin's inverse as a second group that lands while
+  //      the basis and orbital rows are computed
+  warp_copy_async(sR, blk + L.R, L.mv_r);
+  warp_copy_async(sT, blk + L.gradD, L.mv_tail);
+  cp_async_commit();
+  warp_copy_async(sS, blk + L.Inv[sp], inv_d);
+  cp_async_commit();
+  cp_async_wait<1>();
+  __syncwarp();
+
+  const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
+  double rn[3], g_fwd, u_acc;
+  propose_move<kMetropolis>(cfg, slot, mv.step, e, N, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
+
+  // ---- incremental Jastrow + potential
+  double dU, dUxx, dVee, dVen;
+  jastrow_pe_move_warp(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
 
   // ---- basis at the new position and the new Slater / derivative rows
   if constexpr (sizeof(TS) == 8) {
@@ -758,103 +919,9 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
   const double sign_new = sc0[SC_SIGN_A + sp] * (ratio < 0 ? -1.0 : 1.0);
 
   bool accept = true;
-  double p = 1.0;
-  if (kMetropolis) {
-    // acceptance (QMCWalker::calculateMoveAcceptanceProbability, :1578-1654);
-    // G(R' -> R): only electron e moved, the others contribute (dt v'_i)^2
-    double log_g = 0.0;
-    if (cfg.sampling == 1) {
-      double pr = 0.0;
-      for (int t = lane; t < 3 * N; t += 32) {
-        const double tt = (t / 3 == e) ? (ro[t - 3 * e] - rn[t - 3 * e] - cfg.dt * mg[t]) : (cfg.dt * mg[t]);
-        pr += tt * tt;
-      }
-      const double g_rev = warp_sum(pr);
-      log_g = -(g_rev - g_fwd) / (2.0 * cfg.dt);
-    }
-    const double lpr = log(fabs(ratio)) + dU;
-    p = exp(2.0 * lpr + log_g);
-    const double age = sc0[SC_AGE];
-    const double over = age - cfg.old_walker_acceptance;
-    if (!isnan(p)) {
-      if (over > 500)
-        p = 1.0;
-      else if (over > 0)
-        p *= pow(1.1, over);
-    } else {
-      p = 0.0;
-    }
-    if (bad) p = 0.0;
-    if (cfg.run_type == 1 && ratio < 0) p = 0.0;
-    if (p > 1.0) p = 1.0;
-    accept = p > u_acc;
-    const double new_age = accept ? 0.0 : age + 1.0;
-    double w = sc0[SC_WEIGHT];
-    // reweight (QMCWalker::reweight_walker, :1060-1185), observables (:2096-2123, 2306-2387)
-    if (mv.do_reweight) {
-      if (cfg.run_type == 1 && mv.reweight_on) {
-        const double ET = ectl->e_trial, Eest = ectl->e_est;
-        const double mo = sc0[SC_MODRATIO];
-        double Eo = sc0[SC_EL];
-        double Et = bad ? Eo : EL;
-        if (cfg.ecut == 1) {
-          Et *= bad ? mo : modratio;
-          Eo *= mo;
-        } else if (cfg.ecut == 2) {
-          // DePasquale, Rothstein, Vrbik (1988) cutoff |E_L - E_orig| <= 2 / sqrt(dt)
-          const double cut = 2.0 / sqrt(cfg.dt);
-          Et = fmin(fmax(Et, cfg.e_orig - cut), cfg.e_orig + cut);
-          Eo = fmin(fmax(Eo, cfg.e_orig - cut), cfg.e_orig + cut);
-        }
-        double St, So;
-        if (cfg.emod == 0) {
-          St = ET - Et;
-          So = ET - Eo;
-        } else if (cfg.emod == 2) {
-          St = (ET - Et) * (bad ? mo : modratio);
-          So = (ET - Eo) * mo;
-        } else {
-          St = (ET - Eest) + (Eest - Et) * (bad ? mo : modratio);
-          So = (ET - Eest) + (Eest - Eo) * mo;
-        }
-        double rw;
-        if (cfg.reweighting == 0)
-          rw = 0.5 * (St + So);
-        else if (cfg.reweighting == 1)
-          rw = accept ? 0.5 * (St + So) : So;
-        else
-          rw = p * 0.5 * (So + St) + (1.0 - p) * So;
-        const double dW = exp(rw * cfg.dt_eff);
-        if (new_age - cfg.old_walker_acceptance > 0)
-          w *= 0.9;
-        else
-          w *= dW;
-        if (lane == 0) sc[SC_DW] = dW;
-        // a non-finite weight (NaN energy or exp overflow) removes the walker
-        // at the next branching instead of poisoning the ensemble sums
-        if (!isfinite(w)) w = 0.0;
-      }
-      const double Eobs = p * (bad ? 0.0 : EL) + (1.0 - p) * sc0[SC_EL];
-      // rel_cutoff filter of QMCWalker::calculateObservables (QMcBeaver/src/QMCWalker.cpp:2336-2351)
-      const bool in_avg = fabs((Eobs - cfg.e_orig) / cfg.e_orig) < cfg.rel_cutoff;
-      if (lane == 0 && w > 0.0 && in_avg) {
-        atomicAdd(&stats[ST_SUM_W], w);
-        atomicAdd(&stats[ST_SUM_WE], w * Eobs);
-        atomicAdd(&stats[ST_SUM_WE2], w * Eobs * Eobs);
-        atomicAdd(&stats[ST_RUN_SUM_W], w);
-        atomicAdd(&stats[ST_RUN_SUM_WE], w * Eobs);
-        atomicAdd(&stats[ST_RUN_COUNT], 1.0);
-      }
-    }
-    if (lane == 0) {
-      atomicAdd(&stats[ST_SUM_ACC], p);
-      atomicAdd(&stats[ST_MOVES], 1.0);
-      if (bad) atomicAdd(&stats[ST_SINGULAR], 1.0);
-      sc[SC_WEIGHT] = w;
-      sc[SC_AGE] = new_age;
-      if (accept) sc[SC_AGE_MOVED] = age;
-    }
-  }
+  if (kMetropolis)
+    accept = metropolis_reweight(cfg, mv, ectl, stats, sc, sc0, N, e, ro, rn, mg, g_fwd, u_acc,
+                                 log(fabs(ratio)) + dU, ratio < 0, bad, EL, modratio);
   __syncwarp();
 
   if (accept) {
@@ -894,28 +961,11 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
     }
   }
   if (!kMetropolis) {
-    if (lane == 0) {
-      const double la = sp == 0 ? logdet_new : sc0[SC_LOGDET_A];
-      const double lb = sp == 1 ? logdet_new : sc0[SC_LOGDET_B];
-      const double sa = sp == 0 ? sign_new : sc0[SC_SIGN_A];
-      const double sb = sp == 1 ? sign_new : sc0[SC_SIGN_B];
-      unsigned st = bad ? 1u : 0u;
-      if (isnan(EL) || isnan(lap)) st |= 2u;
-      if (out.log_abs_psi) out.log_abs_psi[wi] = la + lb + U_new;
-      if (out.sign) out.sign[wi] = sa * sb;
-      if (out.lap) out.lap[wi] = lap;
-      if (out.e_local) out.e_local[wi] = EL;
-      if (out.pe) {
-        out.pe[3 * wi] = PE;
-        out.pe[3 * wi + 1] = Ven;
-        out.pe[3 * wi + 2] = Vee;
-      }
-      if (out.status) out.status[wi] = (unsigned char)st;
-    }
-    if (out.grad)
-      for (int t = lane; t < 3 * N; t += 32) out.grad[(size_t)wi * 3 * N + t] = gr[t];
-    if (out.mgrad)
-      for (int t = lane; t < 3 * N; t += 32) out.mgrad[(size_t)wi * 3 * N + t] = mg[t];
+    const double la = sp == 0 ? logdet_new : sc0[SC_LOGDET_A];
+    const double lb = sp == 1 ? logdet_new : sc0[SC_LOGDET_B];
+    const double sa = sp == 0 ? sign_new : sc0[SC_SIGN_A];
+    const double sb = sp == 1 ? sign_new : sc0[SC_SIGN_B];
+    write_eval_out(out, wi, N, la + lb + U_new, sa * sb, lap, EL, PE, Ven, Vee, bad, gr, mg);
   }
 }
 

@@ -18,6 +18,7 @@
 
 #include "../../include/qmcb200.h"
 #include "kernels.cuh"
+#include "kernels_md.cuh"
 
 using namespace qmcb;
 
@@ -57,6 +58,10 @@ struct qmcb_handle {
   int2 *d_fn = nullptr;
   double *d_pexp = nullptr, *d_pcoef = nullptr;
   int *d_en[2] = {nullptr, nullptr};
+  int *d_docc[2] = {nullptr, nullptr};
+  int *d_dswap[2] = {nullptr, nullptr};
+  double *d_ci = nullptr;
+  bool md = false;  // several determinants: the k_*_md kernels
   double *d_state = nullptr;
   int *d_live = nullptr, *d_live_tmp = nullptr, *d_free = nullptr, *d_ctl = nullptr;
   int2 *d_copies = nullptr;
@@ -305,6 +310,39 @@ __global__ void __launch_bounds__(1024) k_branch_list(const double *w_in, int n,
 }
 
 namespace {
+// The order in which determinant c's columns are swapped in from determinant
+// c-1 so that no intermediate matrix holds one orbital twice
+// (QMCWavefunction::makeCoefficients, QMcBeaver/src/QMCWavefunction.cpp:924-976).
+// occ: [ndet][n] increasing active rows.  Returns [ndet][n] columns, -1 ends.
+// (Increasing column lists never block for good; the scan stops after n
+// passes regardless.)
+std::vector<int> determinant_swaps(const int *occ, int ndet, int n)
+{
+  std::vector<int> iu(occ, occ + (size_t)ndet * n), sw((size_t)ndet * std::max(n, 1), -1);
+  for (int c = 1; c < ndet; c++) {
+    int k = 0, pass = 0;
+    bool blocked;
+    do {
+      blocked = false;
+      for (int o = 0; o < n; o++) {
+        if (iu[(size_t)c * n + o] == iu[(size_t)(c - 1) * n + o]) continue;
+        bool good = true;
+        for (int o2 = 0; o2 < n; o2++)
+          if (o != o2 && iu[(size_t)c * n + o] == iu[(size_t)(c - 1) * n + o2]) {
+            blocked = true;
+            good = false;
+            break;
+          }
+        if (good) {
+          iu[(size_t)(c - 1) * n + o] = iu[(size_t)c * n + o];
+          sw[(size_t)c * n + k++] = o;
+        }
+      }
+    } while (blocked && ++pass <= n);
+  }
+  return sw;
+}
+
 std::mutex g_noalloc_mu;
 void *g_noalloc_w_addr[64];
 void *g_noalloc_i_addr[64];
@@ -326,6 +364,26 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
     return fail(nullptr, QMCB_E_ARG, "qmcb_create: bad sizes");
   if (na > 256 || nb > 256 || K > 4096 || M > 1024)
     return fail(nullptr, QMCB_E_LIMIT, "qmcb_create: n_alpha/n_beta <= 256, n_basis <= 4096, n_nuclei <= 1024");
+  // several determinants: active rows and increasing column lists
+  const bool md = d->n_det > 1;
+  const int nact[2] = {md ? d->n_act_alpha : na, md ? d->n_act_beta : nb};
+  if (md) {
+    if (!d->ci_coeff || (na > 0 && !d->det_occ_alpha) || (nb > 0 && !d->det_occ_beta) || nact[0] < na ||
+        nact[1] < nb || nact[0] > 1024 || nact[1] > 1024 || d->n_det > 4096)
+      return fail(nullptr, QMCB_E_ARG, "qmcb_create: bad determinant tables");
+    for (int sp = 0; sp < 2; sp++) {
+      const int n = sp ? nb : na;
+      const int *occ = sp ? d->det_occ_beta : d->det_occ_alpha;
+      for (int c = 0; c < d->n_det; c++)
+        for (int o = 0; o < n; o++) {
+          const int v = occ[c * n + o];
+          if (v < 0 || v >= nact[sp] || (o > 0 && v <= occ[c * n + o - 1]))
+            return fail(nullptr, QMCB_E_ARG, "qmcb_create: determinant columns must be increasing active rows");
+        }
+    }
+    for (int c = 0; c < d->n_det; c++)
+      if (!std::isfinite(d->ci_coeff[c])) return fail(nullptr, QMCB_E_ARG, "qmcb_create: CI coefficient not finite");
+  }
   int ndev = 0;
   cudaError_t ce = cudaGetDeviceCount(&ndev);
   if (ce != cudaSuccess || ndev == 0)
@@ -392,12 +450,24 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   });
   std::vector<double> ct[2];
   for (int sp = 0; sp < 2; sp++) {
-    int n = sp ? nb : na;
+    int n = nact[sp];
     const double *mo = sp ? d->mo_beta : d->mo_alpha;
     ct[sp].assign((size_t)K * std::max(n, 1), 0.0);
     for (int o = 0; o < n; o++)
       for (int k = 0; k < K; k++) ct[sp][(size_t)k * n + o] = mo[(size_t)o * K + k];
   }
+  std::vector<int> docc[2], dswap[2];
+  std::vector<double> ci(md ? d->n_det : 1, 1.0);
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? nb : na;
+    const int *occ = sp ? d->det_occ_beta : d->det_occ_alpha;
+    docc[sp].assign((size_t)std::max(md ? d->n_det * n : 0, 1), 0);
+    if (md)
+      for (int t = 0; t < d->n_det * n; t++) docc[sp][t] = occ[t];
+    dswap[sp] = md ? determinant_swaps(docc[sp].data(), d->n_det, n) : std::vector<int>(1, -1);
+  }
+  if (md)
+    for (int c = 0; c < d->n_det; c++) ci[c] = d->ci_coeff[c];
   std::vector<double> pade((size_t)std::max(d->n_pade, 1) * 2 * kPadeMax, 0.0);
   std::vector<int2> plen(std::max(d->n_pade, 1), make_int2(1, 1));
   for (int f = 0; f < d->n_pade; f++) {
@@ -497,6 +567,12 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(upload(&h->d_cparam, cparam));
   CKC(upload(&h->d_en[0], en[0]));
   CKC(upload(&h->d_en[1], en[1]));
+  CKC(upload(&h->d_docc[0], docc[0]));
+  CKC(upload(&h->d_docc[1], docc[1]));
+  CKC(upload(&h->d_dswap[0], dswap[0]));
+  CKC(upload(&h->d_dswap[1], dswap[1]));
+  CKC(upload(&h->d_ci, ci));
+  h->md = md;
 
   DevSys &S = h->sys;
   S.M = M;
@@ -527,6 +603,14 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   S.cparam = h->d_cparam;
   S.en[0] = h->d_en[0];
   S.en[1] = h->d_en[1];
+  S.ndet = md ? d->n_det : 1;
+  S.nact[0] = nact[0];
+  S.nact[1] = nact[1];
+  S.docc[0] = h->d_docc[0];
+  S.docc[1] = h->d_docc[1];
+  S.dswap[0] = h->d_dswap[0];
+  S.dswap[1] = h->d_dswap[1];
+  S.ci = h->d_ci;
 
   // ---- per-walker block layout (offsets in doubles, arrays 32-byte aligned)
   Layout &L = h->lay;
@@ -538,11 +622,18 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   };
   L.R = take(3 * h->N);
   for (int sp = 0; sp < 2; sp++) {
-    int n = sp ? nb : na;
-    L.Dv[sp] = take(n * n);
-    L.DgT[sp] = take(3 * n * n);
-    L.DlT[sp] = take(n * n);
-    L.Inv[sp] = take(n * n);
+    int n = sp ? nb : na, a = nact[sp];
+    L.Dv[sp] = take(n * a);
+    L.DgT[sp] = take(3 * a * n);
+    L.DlT[sp] = take(a * n);
+    if (md) {
+      // two copies of [inverses | grad ratios | (ln|det|, sign, lap, singular)]
+      L.mdsz[sp] = (S.ndet * n * n + S.ndet * 3 * n + S.ndet * 4 + 3) & ~3;
+      L.Inv[sp] = take(2 * L.mdsz[sp]);
+    } else {
+      L.mdsz[sp] = 0;
+      L.Inv[sp] = take(n * n);
+    }
   }
   L.gradD = take(3 * h->N);
   L.Ux = take(3 * h->N);
@@ -563,8 +654,8 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
     L.mv_spin[sp] = even(n * n);
   }
   L.mv_stride = L.mv_region_a + L.mv_dn + L.mv_valc + L.mv_r + L.mv_tail + std::max(L.mv_spin[0], L.mv_spin[1]) + 2;
-  if (L.R + L.mv_r > L.stride || L.gradD + L.mv_tail > L.stride || L.Inv[0] + L.mv_spin[0] > L.stride ||
-      L.Inv[1] + L.mv_spin[1] > L.stride) {
+  if (!md && (L.R + L.mv_r > L.stride || L.gradD + L.mv_tail > L.stride || L.Inv[0] + L.mv_spin[0] > L.stride ||
+              L.Inv[1] + L.mv_spin[1] > L.stride)) {
     qmcb_destroy(h);
     return fail(nullptr, QMCB_E_ARG, "qmcb_create: internal layout error (staged ranges exceed the walker block)");
   }
@@ -590,8 +681,13 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
 
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-  const size_t per_move = sizeof(double) * (size_t)L.mv_stride;
-  const size_t per_full = sizeof(double) * (size_t)full_scratch_doubles(h->N, K, h->nmax);
+  const int amax = std::max(nact[0], nact[1]);
+  const size_t per_move =
+      sizeof(double) * (size_t)(md ? move_md_scratch_doubles(h->N, K, h->nmax, amax, S.ndet, L.sc + kScalars - L.gradD)
+                                   : L.mv_stride);
+  const size_t per_full =
+      sizeof(double) * (size_t)(md ? full_md_scratch_doubles(h->N, K, h->nmax, amax, S.ndet)
+                                   : full_scratch_doubles(h->N, K, h->nmax));
   if (per_move > (size_t)max_optin || per_full > (size_t)max_optin) {
     qmcb_destroy(h);
     return fail(nullptr, QMCB_E_LIMIT, "qmcb_create: system too large for the per-walker shared-memory scratch");
@@ -609,6 +705,9 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_full<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_full<float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_full_md, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move_md<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move_md<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
 #undef CKC
   *out = h;
   return QMCB_OK;
@@ -618,7 +717,7 @@ int qmcb_destroy(qmcb_handle *h)
 {
   if (!h) return QMCB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *ptrs[] = {h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
+  void *ptrs[] = {h->d_docc[0], h->d_docc[1], h->d_dswap[0], h->d_dswap[1], h->d_ci, h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
                   h->d_copies, h->d_stats, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
   for (void *p : ptrs)
@@ -644,6 +743,8 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");
   if (p->precision != QMCB_PREC_FP64 && p->precision != QMCB_PREC_MIXED)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown precision");
+  if (h->md && p->precision != QMCB_PREC_FP64)
+    return fail(h, QMCB_E_ARG, "qmcb_set_params: several determinants run in FP64 only");
   h->params = *p;
   if (h->n_live_host > 0) {
     // the host's E_T / E_est feed the next steps (QMCManager::updateTrialEnergy)
@@ -680,6 +781,23 @@ static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num,
 {
   RunCfg cfg = make_cfg(h->params);
   const bool mixed = h->params.precision == QMCB_PREC_MIXED;
+  if (h->md) {
+    if (mixed) return fail(h, QMCB_E_ARG, "evaluate: several determinants run in FP64 (precision QMCB_PREC_FP64)");
+    if (which_e < 0) {
+      int blocks = (num + h->wpb_full - 1) / h->wpb_full;
+      k_full_md<<<blocks, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
+                                                                 nullptr, d_R, 1, o);
+    } else {
+      MoveArgs mv{which_e, 0, 0, 0};
+      int blocks = (num + h->wpb_move - 1) / h->wpb_move;
+      k_move_md<false><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
+                                                                        num, nullptr, d_R, mv, h->d_ectl,
+                                                                        h->d_stats, o);
+    }
+    CK(cudaGetLastError());
+    if (which_e < 0) h->state_prec = h->params.precision;
+    return QMCB_OK;
+  }
   if (which_e < 0) {
     int blocks = (num + h->wpb_full - 1) / h->wpb_full;
     if (mixed)
@@ -819,7 +937,11 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps)
     EvalOut o{};
     {
       ProfScope ps(h, QMCB_KERNEL_MOVE, st);
-      if (mixed)
+      if (h->md)
+        k_move_md<true><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state,
+                                                                         h->d_live, 0, h->d_ctl, nullptr, mv,
+                                                                         h->d_ectl, h->d_stats, o);
+      else if (mixed)
         k_move<true, float, MIXED_TI><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state,
                                                                             h->d_live, 0, h->d_ctl, nullptr, mv,
                                                                             h->d_ectl, h->d_stats, o);
@@ -851,7 +973,10 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps)
     if (h->params.refresh_interval > 0 && (step + 1) % h->params.refresh_interval == 0) {
       EvalOut o2{};
       ProfScope ps(h, QMCB_KERNEL_REFRESH, st);
-      if (mixed)
+      if (h->md)
+        k_full_md<<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live, 0,
+                                                                        h->d_ctl, nullptr, 0, o2);
+      else if (mixed)
         k_full<float, MIXED_TI><<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state,
                                                                            h->d_live, 0, h->d_ctl, nullptr, 0, o2);
       else

@@ -32,6 +32,8 @@ class SystemDesc(C.Structure):
         ("n_pade", C.c_int), ("pade_num", _dp), ("pade_den", _dp), ("pade_nnum", _ip), ("pade_nden", _ip),
         ("corr_type", _ip), ("corr_param", _dp),
         ("ee_pade", C.c_int * 3), ("en_pade_up", _ip), ("en_pade_dn", _ip),
+        ("n_det", C.c_int), ("n_act_alpha", C.c_int), ("n_act_beta", C.c_int),
+        ("det_occ_alpha", _ip), ("det_occ_beta", _ip), ("ci_coeff", _dp),
     ]
 
 
@@ -114,6 +116,9 @@ class PackedSystem:
             num=np.ascontiguousarray(num), den=np.ascontiguousarray(den), nn=nn, nd=nd,
             en_up=en_up, en_dn=en_dn, ctype=np.ascontiguousarray(ctype, np.int32),
             cparam=np.ascontiguousarray(cparam, np.float64),
+            occ_a=np.ascontiguousarray(s.det_columns(False) if s.n_det > 1 else np.zeros(1), np.int32),
+            occ_b=np.ascontiguousarray(s.det_columns(True) if s.n_det > 1 and s.n_beta else np.zeros(1), np.int32),
+            ci=np.ascontiguousarray(s.ci_coeffs if s.n_det > 1 else np.ones(1), np.float64),
         )
         k = self._keep
         d = SystemDesc()
@@ -143,5 +148,11 @@ class PackedSystem:
             d.ee_pade[i] = int(ee[i])
         d.en_pade_up = _i(k["en_up"])
         d.en_pade_dn = _i(k["en_dn"])
+        d.n_det = s.n_det
+        d.n_act_alpha = len(s.active_orbitals(False))
+        d.n_act_beta = len(s.active_orbitals(True))
+        d.det_occ_alpha = _i(k["occ_a"])
+        d.det_occ_beta = _i(k["occ_b"])
+        d.ci_coeff = _d(k["ci"])
         self.desc = d
         assert PADE_MAX == 16

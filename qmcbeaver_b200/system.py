@@ -175,6 +175,12 @@ class MolecularSystem:
     en_up: Dict[str, Pade]  # by nucleus label
     en_dn: Dict[str, Pade]
     name: str = "synthetic"
+    # several determinants: rows of `mo` occupied by each determinant (each
+    # row increasing) and the CI coefficients; None = the one determinant
+    # alpha_occ / beta_occ
+    det_alpha: Optional[np.ndarray] = None  # (n_det, n_alpha)
+    det_beta: Optional[np.ndarray] = None   # (n_det, n_beta)
+    ci_coeffs: Optional[np.ndarray] = None  # (n_det,)
 
     # ------------------------------------------------------------------ sizes
     @property
@@ -210,11 +216,28 @@ class MolecularSystem:
                 np.asarray(nprim, np.int32), np.asarray(off, np.int32),
                 np.asarray(ex, np.float64), np.asarray(co, np.float64))
 
+    @property
+    def n_det(self) -> int:
+        return 1 if self.det_alpha is None else int(np.asarray(self.det_alpha).shape[0])
+
+    def active_orbitals(self, beta: bool) -> np.ndarray:
+        """Rows of `mo` used by some determinant of the spin, increasing
+        (QMCWavefunction::makeCoefficients, QMcBeaver/src/QMCWavefunction.cpp:873-905)."""
+        if self.det_alpha is None:
+            return np.asarray(self.beta_occ if beta else self.alpha_occ)
+        return np.unique(np.asarray(self.det_beta if beta else self.det_alpha))
+
+    def det_columns(self, beta: bool) -> np.ndarray:
+        """(n_det, n) active-row index of every determinant column."""
+        act = self.active_orbitals(beta)
+        occ = np.asarray(self.det_beta if beta else self.det_alpha).reshape(self.n_det, -1)
+        return np.searchsorted(act, occ).astype(np.int32)
+
     def mo_alpha(self) -> np.ndarray:
-        return np.ascontiguousarray(self.mo[self.alpha_occ])
+        return np.ascontiguousarray(self.mo[self.active_orbitals(False)])
 
     def mo_beta(self) -> np.ndarray:
-        return np.ascontiguousarray(self.mo[self.beta_occ])
+        return np.ascontiguousarray(self.mo[self.active_orbitals(True)])
 
     def pade_tables(self):
         """Correlation-function table + indices: ee[3] = (anti, up-up, dn-dn),
@@ -328,7 +351,7 @@ class MolecularSystem:
             "charge": self.charge,
             "norbitals": self.mo.shape[0],
             "nbasisfunc": self.n_basis,
-            "ndeterminants": 1,
+            "ndeterminants": self.n_det,
             "trial_function_type": "restricted",
         })
         if flags:
@@ -356,18 +379,18 @@ class MolecularSystem:
         for row in self.mo:
             out.append(" ".join(g % v for v in row))
         out.append("")
-        occ_a = np.zeros(self.mo.shape[0], int)
-        occ_a[self.alpha_occ] = 1
-        occ_b = np.zeros(self.mo.shape[0], int)
-        occ_b[self.beta_occ] = 1
-        out.append("Alpha Occupation")
-        out.append(" ".join(str(v) for v in occ_a))
-        out.append("")
-        out.append("Beta Occupation")
-        out.append(" ".join(str(v) for v in occ_b))
-        out.append("")
+        dets_a = [self.alpha_occ] if self.det_alpha is None else list(self.det_alpha)
+        dets_b = [self.beta_occ] if self.det_beta is None else list(self.det_beta)
+        for title, dets in (("Alpha Occupation", dets_a), ("Beta Occupation", dets_b)):
+            out.append(title)
+            for occ in dets:
+                row = np.zeros(self.mo.shape[0], int)
+                row[np.asarray(occ, int)] = 1
+                out.append(" ".join(str(v) for v in row))
+            out.append("")
         out.append("CI Coeffs")
-        out.append("1")
+        ci = [1.0] if self.ci_coeffs is None else list(self.ci_coeffs)
+        out.append(" ".join(g % v for v in ci))
         out.append("")
         out.append("&")
         out.append("")
@@ -671,6 +694,50 @@ def with_cambridge2(s: MolecularSystem, seed: int = 1) -> MolecularSystem:
                                en_up=en_up, en_dn=en_dn, name=s.name + " cambridge2")
 
 
+def with_determinants(s: MolecularSystem, n_det: int = 9, n_virtual: int = 4, seed: int = 1,
+                      ci_scale: float = 0.3) -> MolecularSystem:
+    """The same molecule with a CI expansion over the lowest
+    max(n_alpha, n_beta) + n_virtual orbitals of the approximate core
+    Hamiltonian: the ground determinant, one single excitation of each spin
+    into every virtual orbital (so every listed orbital is active in both
+    spins), then distinct random doubles (one electron of each spin) up to
+    n_det; CI coefficients 1 and N(0, ci_scale).  The shape of the
+    reference's multi-determinant inputs (QMcBeaver/examples/BeMCSCF.ckmf)."""
+    rng = np.random.default_rng(seed)
+    na, nb = s.n_alpha, s.n_beta
+    n_orb = max(na, nb) + n_virtual
+    mo = core_hamiltonian_orbitals(s, n_orb)
+    ground = (tuple(range(na)), tuple(range(nb)))
+    dets = [ground]
+
+    def excite(occ, n, v):
+        o = list(occ)
+        o[int(rng.integers(n))] = v
+        return tuple(sorted(o))
+
+    for v in range(max(na, nb), n_orb):
+        if na > 0:
+            dets.append((excite(ground[0], na, v), ground[1]))
+        if nb > 0:
+            dets.append((ground[0], excite(ground[1], nb, v)))
+    tries = 0
+    while len(dets) < n_det and tries < 10000 and na > 0 and nb > 0:
+        tries += 1
+        key = (excite(ground[0], na, int(rng.integers(na, n_orb))), excite(ground[1], nb, int(rng.integers(nb, n_orb))))
+        if key not in dets:
+            dets.append(key)
+    if len(dets) < n_det:
+        raise ValueError("not enough distinct excitations")
+    dets = dets[:max(n_det, 1 + (na > 0) * n_virtual + (nb > 0) * n_virtual)]
+    nd = len(dets)
+    ci = np.concatenate([[1.0], rng.normal(0.0, ci_scale, nd - 1)])
+    return dataclasses.replace(
+        s, mo=mo, alpha_occ=np.arange(na), beta_occ=np.arange(nb),
+        det_alpha=np.array([d[0] for d in dets], np.int64).reshape(nd, na),
+        det_beta=np.array([d[1] for d in dets], np.int64).reshape(nd, nb),
+        ci_coeffs=ci, name=s.name + f" {nd} determinants")
+
+
 def make_water_like(seed: int = 1, jastrow: bool = True) -> MolecularSystem:
     """The small VMC system: O at the origin, H at (+-1.43, 1.11, 0) bohr,
     5 up + 5 down electrons, 24 contracted Cartesian Gaussians with 3
@@ -727,6 +794,10 @@ WORKLOADS = {
     "vmc_cambridge2_16e": dict(kind="random", n_elec=16, n_nuclei=4, n_basis=64, box=5.0, z=(1, 6, 7, 8),
                                walkers=4096, run="vmc", dt=0.01, importance=True, refresh=50,
                                correlation="cambridge2"),
+    # twelve determinants (singles and doubles into four virtual orbitals)
+    "vmc_multidet_12e": dict(kind="random", n_elec=12, n_nuclei=3, n_basis=48, box=4.5, z=(1, 6, 7, 8),
+                             walkers=4096, run="vmc", dt=0.01, importance=True, refresh=50,
+                             determinants=(12, 4)),
 }
 
 
@@ -738,6 +809,10 @@ def make_system(workload: str, seed: int = 1, jastrow: bool = True) -> Molecular
                              jastrow=jastrow, name=workload)
     if jastrow and w.get("correlation") == "cambridge2":
         s = with_cambridge2(s, seed=seed + 1)
+        s.name = workload
+    if "determinants" in w:
+        nd, nv = w["determinants"]
+        s = with_determinants(s, nd, nv, seed=seed + 2)
         s.name = workload
     return s
 
@@ -777,7 +852,9 @@ def system_to_arrays(s: MolecularSystem) -> Dict[str, np.ndarray]:
         ee_anti=pade_arr(s.ee_anti), ee_para_up=pade_arr(s.ee_para_up), ee_para_dn=pade_arr(s.ee_para_dn),
         en_up=np.stack([pade_arr(s.en_up.get(l)) for l in s.labels]),
         en_dn=np.stack([pade_arr(s.en_dn.get(l)) for l in s.labels]),
-        name=np.array(s.name))
+        name=np.array(s.name),
+        **({} if s.det_alpha is None else dict(det_alpha=np.asarray(s.det_alpha), det_beta=np.asarray(s.det_beta),
+                                              ci_coeffs=np.asarray(s.ci_coeffs, np.float64))))
 
 
 def system_from_arrays(d) -> MolecularSystem:
@@ -810,4 +887,7 @@ def system_from_arrays(d) -> MolecularSystem:
         mo=np.array(d["mo"], np.float64), n_alpha=int(d["n_alpha"]), n_beta=int(d["n_beta"]),
         alpha_occ=np.array(d["alpha_occ"]), beta_occ=np.array(d["beta_occ"]),
         ee_anti=pade_of(d["ee_anti"]), ee_para_up=pade_of(d["ee_para_up"]), ee_para_dn=pade_of(d["ee_para_dn"]),
-        en_up=en_up, en_dn=en_dn, name=str(d["name"]))
+        en_up=en_up, en_dn=en_dn, name=str(d["name"]),
+        det_alpha=np.array(d["det_alpha"]) if "det_alpha" in d else None,
+        det_beta=np.array(d["det_beta"]) if "det_beta" in d else None,
+        ci_coeffs=np.array(d["ci_coeffs"], np.float64) if "ci_coeffs" in d else None)

@@ -29,6 +29,9 @@ CASES = {
     "dmc30_equal": ("dmc_6nuc_30e", 1, 0.01, 2, 8, 0.15, 0),
     # Cambridge2 two-body Jastrow with C = 2 and C = 3 and an inactive function
     "cambridge2_vmc": ("vmc_cambridge2_16e", 2, 0.01, 6, 40, 0.2, 6),
+    # twelve determinants (single excitations into every virtual orbital of
+    # both spins, doubles)
+    "multidet_vmc": ("vmc_multidet_12e", 2, 0.01, 6, 40, 0.2, 6),
 }
 
 

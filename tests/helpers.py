@@ -26,15 +26,20 @@ def rel_err(a, b, floor=1.0):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))) if a.size else 0.0
 
 
-def compare(out, ref, rtol, label="", mask=None):
+def compare(out, ref, rtol, label="", mask=None, kappa=None):
     """Checks one evaluate call's outputs against reference outputs (walkers
-    in `mask`, default all non-singular ones)."""
+    in `mask`, default all non-singular ones).  kappa: per-walker condition
+    number of the determinant-weighted laplacian sum (several determinants);
+    lap and E_L are checked at rtol * max(kappa, 1)."""
     ok = ref["singular"] == 0 if "singular" in ref else np.ones(len(ref["e_local"]), bool)
     if mask is not None:
         ok = ok & mask
     msgs = []
+    amp = np.ones(len(ok)) if kappa is None else np.maximum(np.asarray(kappa, np.float64), 1.0)
     for k, floor in (("e_local", 1.0), ("lap", 1.0), ("potential", 1.0)):
-        e = rel_err(out[k][ok], ref[k][ok], floor)
+        a, b = np.asarray(out[k], np.float64)[ok], np.asarray(ref[k], np.float64)[ok]
+        s = amp[ok] if k != "potential" else np.ones(ok.sum())
+        e = float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor) / s)) if a.size else 0.0
         if e > rtol:
             msgs.append(f"{k} {e:.3e}")
     # psi ratio: |d log psi| is the relative error of psi
@@ -52,13 +57,16 @@ def compare(out, ref, rtol, label="", mask=None):
     assert not msgs, f"{label}: " + ", ".join(msgs)
 
 
-def replay(ev_eval, d, rtol, label):
-    """Feeds the golden call sequence through ev_eval(which_e, R) -> outputs."""
+def replay(ev_eval, d, rtol, label, kappa=None):
+    """Feeds the golden call sequence through ev_eval(which_e, R) -> outputs.
+    kappa(which_e, R) -> per-walker laplacian-sum condition numbers (several
+    determinants), or None."""
     for i, e in enumerate(d["whichE"]):
         out = ev_eval(int(e), d["R"][i])
         ref = {k: d[k][i] for k in ("log_abs_psi", "sign", "grad", "mod_grad", "lap", "e_local", "potential",
                                      "singular")}
-        compare(out, ref, rtol, f"{label} call {i} whichE={e}")
+        kap = kappa(int(e), d["R"][i]) if kappa is not None else None
+        compare(out, ref, rtol, f"{label} call {i} whichE={e}", kappa=kap)
 
 
 # Rounding differences between two FP64 implementations grow with the
@@ -68,12 +76,27 @@ def replay(ev_eval, d, rtol, label):
 # COND_SLOPE * cond (a walker that once exceeded the limit stays there).
 COND_SLOPE = 2e-15
 COND_LIMIT = 5e4
+# Several determinants: every determinant's inverse is carried through its
+# own Sherman-Morrison chain and the combined ratios take the worst of them
+# (measured up to 2.2e-15 * cond once the determinant-mixing amplification
+# kappa is divided out), so the bound doubles: 1e-10 up to cond 2.5e4, then
+# 4e-15 * cond, each times kappa.
+COND_SLOPE_MULTIDET = 4e-15
+COND_LIMIT_MULTIDET = 2.5e4
+
+
+def cond_bounds(system):
+    """(slope, limit) of the condition-scaled parity bound for the system."""
+    return (COND_SLOPE_MULTIDET, COND_LIMIT_MULTIDET) if system.n_det > 1 else (COND_SLOPE, COND_LIMIT)
 
 
 def slater_conditions(orc, walkers, system):
+    """Largest condition number over the Slater matrices (every determinant,
+    both spins) of each walker."""
     c = np.zeros(len(walkers))
     for i, w in enumerate(walkers):
         for beta, n in ((0, system.n_alpha), (1, system.n_beta)):
             if n > 0:
-                c[i] = max(c[i], np.linalg.cond(orc.inverse(w, beta)))
+                for det in range(system.n_det):
+                    c[i] = max(c[i], np.linalg.cond(orc.inverse(w, beta, det)))
     return c

@@ -53,3 +53,31 @@ def test_bad_arguments_rejected_before_device_use():
     h = C.c_void_p()
     assert lib.qmcb_create(None, 4, C.byref(h)) == 1  # QMCB_E_ARG
     assert b"null argument" in lib.qmcb_last_error(None)
+
+
+@pytest.mark.parametrize("cname,pyname", [("qmcb_system_desc", "SystemDesc"), ("qmcb_run_params", "RunParams"),
+                                          ("qmcb_step_stats", "StepStats")])
+def test_ctypes_mirror_matches_header_layout(tmp_path, cname, pyname):
+    """Every field of the ctypes mirrors in qmcbeaver_b200/desc.py sits at the
+    offset the C compiler gives it in include/qmcb200.h (and the sizes agree)."""
+    import shutil
+    import subprocess
+    from qmcbeaver_b200 import desc as D
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    st = getattr(D, pyname)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "qmcb200.h"', "int main(void) {",
+             f'  printf("%zu\\n", sizeof({cname}));']
+    for name, _ in st._fields_:
+        lines.append(f'  printf("%zu\\n", offsetof({cname}, {name}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.check_call([gcc, "-I", os.path.join(root, "include"), str(src), "-o", str(exe)])
+    got = [int(x) for x in subprocess.check_output([str(exe)]).split()]
+    assert got[0] == C.sizeof(st), (pyname, got[0], C.sizeof(st))
+    for (name, _), off in zip(st._fields_, got[1:]):
+        assert getattr(st, name).offset == off, (pyname, name, off)

@@ -24,7 +24,7 @@ def _same_tables(a, b):
 
 
 @pytest.mark.parametrize("workload,cambridge", [("vmc_water_10e", False), ("dmc_6nuc_30e", True),
-                                                ("vmc_cambridge2_16e", False)])
+                                                ("vmc_cambridge2_16e", False), ("vmc_multidet_12e", False)])
 def test_writer_reader_round_trip(tmp_path, workload, cambridge):
     s = make_system(workload, seed=1)
     if cambridge:
@@ -32,7 +32,7 @@ def test_writer_reader_round_trip(tmp_path, workload, cambridge):
     p = tmp_path / "sys.ckmf"
     s.to_ckmf(str(p))
     c = read_ckmf(str(p))
-    assert c.n_alpha == s.n_alpha and c.n_beta == s.n_beta and c.n_determinants == 1
+    assert c.n_alpha == s.n_alpha and c.n_beta == s.n_beta and c.n_determinants == s.n_det
     t = c.to_system()
     np.testing.assert_array_equal(t.coords, s.coords)
     np.testing.assert_array_equal(t.Z, s.Z)
@@ -41,6 +41,11 @@ def test_writer_reader_round_trip(tmp_path, workload, cambridge):
     for x, y in zip(t.flat_basis(), s.flat_basis()):
         np.testing.assert_array_equal(x, y)
     _same_tables(t, s)
+    assert t.n_det == s.n_det
+    if s.n_det > 1:
+        np.testing.assert_array_equal(t.det_alpha, s.det_alpha)
+        np.testing.assert_array_equal(t.det_beta, s.det_beta)
+        np.testing.assert_array_equal(t.ci_coeffs, s.ci_coeffs)
 
 
 def test_cambridge2_parameters_and_evaluation():
@@ -173,8 +178,10 @@ def test_reader_refusals_and_constraints():
     c = read_ckmf("t", _text(ndet=2, aocc="1 0\n0 1", bocc="1 0\n1 0", ci="0.9 c 0 -0.5"))
     assert c.n_determinants == 2
     np.testing.assert_allclose(c.ci_coeffs, [0.9, -0.45])
-    with pytest.raises(CkmfError, match="determinants"):
-        c.to_system(allow_cusp_replacement=True, allow_three_body=True)
+    s = c.to_system(allow_cusp_replacement=True, allow_three_body=True)
+    assert s.n_det == 2 and s.det_alpha.tolist() == [[0], [1]] and s.det_beta.tolist() == [[0], [0]]
+    np.testing.assert_array_equal(s.mo_alpha(), s.mo)          # both orbitals active for alpha
+    assert s.det_columns(True).tolist() == [[0], [0]]
     with pytest.raises(CkmfError, match="electrons"):
         read_ckmf("t", _text(aocc="1 1"))
     with pytest.raises(CkmfError, match="walker path"):
@@ -274,7 +281,9 @@ print("WORST", worst)
 @pytest.mark.parametrize("rel,one_e", [
     ("test/oepi.ckmf", 1), ("test/he.ckmf", 1), ("test/bare.ckmf", 1), ("examples/h2o.ckmf", 1),
     ("examples/ne0.ckmf", 1), ("examples/ne0P.ckmf", 1), ("examples/H2_hf_631Gss-vmc.ckmf", 1),
-    ("examples/10_Annulene-heart-DZd_CCSDT.HF_CC-PVDZ.DMC.ckmf", 1), ("test/hmx.ckmf", 0)])
+    ("examples/10_Annulene-heart-DZd_CCSDT.HF_CC-PVDZ.DMC.ckmf", 1), ("test/hmx.ckmf", 0),
+    # several determinants (2 to 10; det.ckmf: 42 electrons, 480 basis functions)
+    ("examples/BeMCSCF.ckmf", 1), ("examples/CH2MCSCF.ckmf", 1), ("test/chkpnt.ckmf", 1), ("test/det.ckmf", 1)])
 def test_oracle_matches_reference_on_reference_inputs(rel, one_e):
     code = _CHILD.format(root=ROOT, path=os.path.join(REF_INPUTS, rel), one_e=one_e)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)

@@ -29,7 +29,7 @@ def test_oracle_reproduces_reference_golden(case):
 
 
 def test_golden_cases_present():
-    assert {"water_vmc", "dmc30_unequal", "dmc30_equal"} <= set(GOLDEN_CASES)
+    assert {"water_vmc", "dmc30_unequal", "dmc30_equal", "cambridge2_vmc", "multidet_vmc"} <= set(GOLDEN_CASES)
 
 
 def test_golden_sequences_cover_rollback_and_both_spins():
@@ -44,9 +44,10 @@ def test_golden_sequences_cover_rollback_and_both_spins():
 _CHILD = r"""
 import sys, numpy as np
 sys.path.insert(0, {root!r})
-from qmcbeaver_b200.system import make_random_molecule
+from qmcbeaver_b200.system import make_random_molecule, with_cambridge2, with_determinants
 from oracle.evaluators import OracleEvaluator, ReferenceEvaluator
 s = make_random_molecule({ne}, {nn}, {nb}, 5.0, (1, 6, 7, 8), seed={seed})
+s = {wrap}
 qf, dt = {qf}, 0.02
 ref = ReferenceEvaluator(s, qf_mod=qf, dt=dt); orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
 W = 5
@@ -74,10 +75,14 @@ print("WORST", worst)
 # path copies derivative rows with the full orbital-row width
 # (QMcBeaver/src/QMCWalkerData.cpp:80-93, QMcBeaver/include/Array2D.h:986), so it
 # reads past its rows whenever the beta spin occupies fewer orbitals.
-@pytest.mark.parametrize("ne,nn,nb,seed,qf", [(6, 2, 16, 3, 0), (10, 3, 30, 4, 2), (14, 4, 40, 5, 1)])
-def test_oracle_matches_reference_call_for_call(ne, nn, nb, seed, qf):
+@pytest.mark.parametrize("ne,nn,nb,seed,qf,wrap", [
+    (6, 2, 16, 3, 0, "s"), (10, 3, 30, 4, 2, "s"), (14, 4, 40, 5, 1, "s"),
+    (10, 3, 30, 6, 2, "with_cambridge2(s, seed=2)"),
+    (8, 2, 24, 7, 2, "with_determinants(s, 7, 3, seed=3)"),
+    (10, 3, 30, 8, 1, "with_determinants(with_cambridge2(s, seed=4), 10, 3, seed=5)")])
+def test_oracle_matches_reference_call_for_call(ne, nn, nb, seed, qf, wrap):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    code = _CHILD.format(root=root, ne=ne, nn=nn, nb=nb, seed=seed, qf=qf)
+    code = _CHILD.format(root=root, ne=ne, nn=nn, nb=nb, seed=seed, qf=qf, wrap=wrap)
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     worst = float([l for l in r.stdout.splitlines() if l.startswith("WORST")][0].split()[1])

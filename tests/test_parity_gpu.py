@@ -4,7 +4,7 @@ seeded configurations.  Plain FP64 path: 1e-10 relative."""
 import numpy as np
 import pytest
 
-from helpers import COND_LIMIT, COND_SLOPE, GOLDEN_CASES, PARITY_RTOL, compare, load_golden, replay, slater_conditions
+from helpers import GOLDEN_CASES, PARITY_RTOL, compare, cond_bounds, load_golden, replay, slater_conditions
 from qmcbeaver_b200.api import QMCB200Functions
 from qmcbeaver_b200.system import make_random_molecule, make_system
 
@@ -17,7 +17,18 @@ def test_gpu_reproduces_reference_golden(case):
     W = d["R"].shape[1]
     f = QMCB200Functions(s, W, qf_modification=int(d["qf_mod"]), dt=float(d["dt"]))
     slots = np.arange(W)
-    replay(lambda e, R: f.evaluate(slots, R, e), d, PARITY_RTOL, f"gpu/{case}")
+    kappa = None
+    if s.n_det > 1:
+        # several determinants: the oracle follows the same calls and gives
+        # each walker's laplacian-sum condition number
+        from oracle.evaluators import OracleEvaluator
+        orc = OracleEvaluator(s, qf_mod=int(d["qf_mod"]), dt=float(d["dt"]))
+        ws = orc.new_walkers(W)
+
+        def kappa(e, R):
+            orc.evaluate(ws, R, e)
+            return orc.kappa(ws)
+    replay(lambda e, R: f.evaluate(slots, R, e), d, PARITY_RTOL, f"gpu/{case}", kappa=kappa)
     f.close()
 
 
@@ -33,6 +44,7 @@ def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good
     calls = [(-1, None)] + [(m % N, None) for m in range(sweeps * N)]
     good = np.ones(W, bool)
     worst_cond = np.zeros(W)
+    slope, limit = cond_bounds(s)
     for i, (e, _) in enumerate(calls):
         if e >= 0:
             R[:, e] += sigma * rng.standard_normal((W, 3))
@@ -40,14 +52,16 @@ def _oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good
         ref = orc.results(ws)
         cond = slater_conditions(orc, ws, s)
         worst_cond = np.maximum(worst_cond, cond)
-        good &= cond < COND_LIMIT
+        good &= cond < limit
         out = f.evaluate(slots, R, e)
-        compare(out, ref, PARITY_RTOL, f"{s.name} call {i} whichE={e}", mask=good)
+        kap = orc.kappa(ws)
+        compare(out, ref, PARITY_RTOL, f"{s.name} call {i} whichE={e}", mask=good, kappa=kap)
         if (~good).any():
             # ill-conditioned Slater matrices: rounding differences of two
             # FP64 implementations grow as ~cond * 1e-15
-            tol = max(PARITY_RTOL, COND_SLOPE * float(worst_cond[~good].max()))
-            compare(out, ref, tol, f"{s.name} call {i} whichE={e} (cond {worst_cond[~good].max():.1e})", mask=~good)
+            tol = max(PARITY_RTOL, slope * float(worst_cond[~good].max()))
+            compare(out, ref, tol, f"{s.name} call {i} whichE={e} (cond {worst_cond[~good].max():.1e})", mask=~good,
+                    kappa=kap)
     f.close()
     assert good.mean() >= min_good, f"only {good.sum()} of {W} walkers stayed well conditioned"
     return good.mean()
