@@ -198,6 +198,50 @@ def mixed_section(system, W, e0, rank, args):
                     "LU refresh and energies"}
 
 
+def rows_section(args, rank: int):
+    """The widened rows on their own workloads: Cambridge2 two-body Jastrow
+    and a 12-determinant CI expansion, VMC with drift on the device (timed
+    with CUDA events on the library's stream), next to the reference CPU
+    program on the same systems (all host cores, a bounded sample)."""
+    import torch
+    from qmcbeaver_b200.api import QMCB200Functions
+    from qmcbeaver_b200.desc import QMCB_IMPORTANCE_SAMPLING, QMCB_QF_UMRIGAR93_UNEQUAL, run_params
+    from qmcbeaver_b200.replicas import aggregate_timing, replica_seed
+    from qmcbeaver_b200.system import make_system
+    out = {}
+    for wl, W in (("vmc_cambridge2_16e", 8192), ("vmc_multidet_12e", 8192)):
+        s = make_system(wl, seed=1)
+        N = s.n_electrons
+        p = run_params(sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01,
+                       refresh_interval=50, seed=replica_seed(17, rank), rel_cutoff=0.0)
+        f = QMCB200Functions(s, W, p)
+        f.init_walkers(s.initial_positions(W, seed=300 + rank))
+        f.run_steps(0, 5 * N)
+        steps = max(40 * N, args.warmup)
+        torch.cuda.synchronize()
+        s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream = torch.cuda.ExternalStream(f.stream)
+        s_ev.record(stream)
+        st = f.run_steps(5 * N, steps)
+        e_ev.record(stream)
+        torch.cuda.synchronize()
+        ms, moves = aggregate_timing(s_ev.elapsed_time(e_ev), st.n_moves)
+        f.close()
+        row = {"value": moves / (ms / 1e3), "unit": "walker-moves/s", "walkers": W, "steps": steps,
+               "electrons": N, "basis_functions": s.n_basis, "determinants": s.n_det,
+               "energy": st.sum_weight_energy / max(st.sum_weight, 1e-300)}
+        if rank == 0 and not args.no_cpu_baseline:
+            from oracle import refrun
+            if refrun.available():
+                r = refrun.run_reference(s, "vmc_drift", 0.01, 32, 400, os.cpu_count() or 1)
+                if r["ok"]:
+                    row["cpu_reference"] = {"value": r["moves_per_s"], "unit": "walker-moves/s", "cores": r["procs"],
+                                            "sample": f"{r['procs']} processes x 32 walkers x 400 steps of the "
+                                                      "reference's drift-diffusion VMC"}
+        out[wl] = row
+    return out
+
+
 def serving_section(args):
     """Poisson arrivals of VMC energy jobs (molecules drawn like the
     uneven-batching workload, 4-40 electrons), run concurrently with
@@ -407,6 +451,7 @@ def main():
     f.close()
     if not args.no_extras:
         out["mixed"] = mixed_section(system, W, e0, rank, args)
+        out["rows"] = rows_section(args, rank)
         if world == 1:
             out["serving"] = serving_section(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
