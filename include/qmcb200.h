@@ -111,7 +111,21 @@ typedef struct qmcb_system_desc {
   const int *det_occ_alpha;     /* [n_det][n_alpha] */
   const int *det_occ_beta;      /* [n_det][n_beta] */
   const double *ci_coeff;       /* [n_det] */
+  /* Electron-nucleus cusp replacement (replace_electron_nucleus_cusps,
+     QMCElectronNucleusCusp, QMcBeaver/src/QMCSlater.cpp:85-93,856-872): near
+     each nucleus the s-type part of every orbital row is replaced by
+     C + sgn0 exp(alpha(r)).  replace_cusps = 1 turns it on; cusp_alpha /
+     cusp_beta may hold the fitted records of qmcb_fit_cusps
+     ([M][rows of mo_alpha / mo_beta][QMCB_CUSP_REC]); NULL = fit in
+     qmcb_create. */
+  int replace_cusps;
+  const double *cusp_alpha;
+  const double *cusp_beta;
 } qmcb_system_desc;
+
+/* One fitted cusp-replacement record: rc, sgn0, C, alpha_0 .. alpha_4
+   (rc = 0: the orbital keeps its own s part at this nucleus). */
+#define QMCB_CUSP_REC 8
 
 /* Sampling / DMC parameters (the QMCFlags fields the path reads). */
 typedef struct qmcb_run_params {
@@ -161,6 +175,13 @@ typedef struct qmcb_handle qmcb_handle;
 
 /* Library version string. */
 const char *qmcb_version(void);
+
+/* Fits the electron-nucleus cusp replacement of every (nucleus, orbital
+   row) of one spin (beta = 0: mo_alpha rows, 1: mo_beta rows) into
+   out[n_nuclei][rows][QMCB_CUSP_REC], as QMCElectronNucleusCusp::
+   fitReplacementOrbitals does (QMcBeaver/src/QMCElectronNucleusCusp.cpp:
+   46-172).  Host only, needs no device.  Errors: qmcb_last_error(NULL). */
+int qmcb_fit_cusps(const qmcb_system_desc *desc, int beta, double *out);
 
 /* Message of the last failure on this handle (or of the last failed create
  * or handle-free call when h is NULL). */

@@ -97,6 +97,11 @@ class OracleEvaluator(_Base):
         L.orc_walker_kappa.restype = C.c_double
         L.orc_basis_at.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         self.packed = PackedSystem(system)
+        if system.replace_cusps:
+            # the fitted replacement records come from the library's fit
+            # (pinned against the reference's own fit by tests/test_cusp.py)
+            from qmcbeaver_b200.api import fit_cusps
+            self.packed.set_cusp_tables(*fit_cusps(system))
         self.system = system
         self.N = system.n_electrons
         self.sys = L.orc_system_new(C.byref(self.packed.desc), qf_mod, qf_a, dt)
@@ -168,6 +173,7 @@ class ReferenceEvaluator(_Base):
         L.ref_evaluate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.ref_walker_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_walker_inverse.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.ref_cusp_params.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p]
         self.system = system
         self.N = system.n_electrons
         self.max_batch = max_batch
@@ -182,7 +188,8 @@ class ReferenceEvaluator(_Base):
             system.to_ckmf(path, flags)
         else:
             from qmcbeaver_b200.ckmf import patch_flags, strip_three_body
-            flags.update({"replace_electron_nucleus_cusps": 0, "use_three_body_jastrow": 0,
+            flags.update({"replace_electron_nucleus_cusps": 1 if system.replace_cusps else 0,
+                          "use_three_body_jastrow": 0,
                           "one_e_per_iter": int(one_e_per_iter),
                           "print_configs": 0, "optimize_Psi": 0})
             with open(path, "w") as fh:
@@ -210,6 +217,18 @@ class ReferenceEvaluator(_Base):
 
     def _get(self, w, a, b, c):
         self.lib.ref_walker_get(w, a, b, c)
+
+    def cusp_params(self, beta: int) -> np.ndarray:
+        """The reference's own fitted cusp records [nucleus][orbital row][8]
+        (rc, sgn0, C, alpha_0..alpha_4) of one spin."""
+        rows = len(self.system.active_orbitals(bool(beta)))
+        out = np.zeros((self.system.n_nuclei, rows, 8))
+        buf = np.zeros(8)
+        for i in range(self.system.n_nuclei):
+            for k in range(rows):
+                self.lib.ref_cusp_params(beta, i, k, buf.ctypes.data_as(C.c_void_p))
+                out[i, k] = buf
+        return out
 
     def inverse(self, w, beta: int) -> np.ndarray:
         n = self.system.n_beta if beta else self.system.n_alpha

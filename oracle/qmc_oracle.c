@@ -26,6 +26,11 @@ struct orc_system {
   int *occ[2];                            /* [ndet][n] active row of each column */
   int *swaps[2];                          /* [ndet][n] columns replaced from det ci-1, -1 ends */
   double *ci;                             /* [ndet] */
+  int cusp, nsmax;                        /* electron-nucleus cusp replacement */
+  int *cns;                               /* [M] s primitives per nucleus */
+  double *csexp;                          /* [M][nsmax] */
+  double *cscoef[2];                      /* [M][nact][nsmax] */
+  double *cpar[2];                        /* [M][nact][8] rc, sgn0, C, alpha_0..4 */
   int npade;
   double *pnum, *pden;
   int *pnn, *pnd;
@@ -139,6 +144,43 @@ orc_system *orc_system_new(const qmcb_system_desc *d, int qf_mod, double qf_a, d
       for (int o = 0; o < n; o++) s->occ[sp][c * n + o] = d->n_det > 1 ? src[c * n + o] : o;
     make_swaps(s->occ[sp], s->ndet, n, s->swaps[sp]);
   }
+  /* cusp replacement: the fitted records come with the descriptor; the s
+   * parts (sTypeCoeffs, QMcBeaver/src/QMCElectronNucleusCusp.cpp:83-102) are
+   * built here from the basis and the orbital rows */
+  s->cusp = d->replace_cusps != 0;
+  s->cns = (int *)calloc(s->M, sizeof(int));
+  for (int k = 0; k < s->K; k++)
+    if (s->bf_pow[3 * k] + s->bf_pow[3 * k + 1] + s->bf_pow[3 * k + 2] == 0) s->cns[s->bf_atom[k]] += s->bf_nprim[k];
+  s->nsmax = 1;
+  for (int a = 0; a < s->M; a++)
+    if (s->cns[a] > s->nsmax) s->nsmax = s->cns[a];
+  s->csexp = (double *)calloc((size_t)s->M * s->nsmax, sizeof(double));
+  for (int a = 0; a < s->M; a++) {
+    int cnt = 0;
+    for (int k = 0; k < s->K; k++) {
+      if (s->bf_atom[k] != a) continue;
+      if (s->bf_pow[3 * k] + s->bf_pow[3 * k + 1] + s->bf_pow[3 * k + 2] != 0) continue;
+      for (int l = 0; l < s->bf_nprim[k]; l++) s->csexp[(size_t)a * s->nsmax + cnt++] = s->pexp[s->bf_off[k] + l];
+    }
+  }
+  for (int sp = 0; sp < 2; sp++) {
+    int a_ = s->nact[sp] ? s->nact[sp] : 1;
+    const double *mo = sp ? s->mo_b : s->mo_a;
+    const double *given = sp ? d->cusp_beta : d->cusp_alpha;
+    s->cpar[sp] = (double *)calloc((size_t)s->M * a_ * 8, sizeof(double));
+    s->cscoef[sp] = (double *)calloc((size_t)s->M * a_ * s->nsmax, sizeof(double));
+    if (!s->cusp || s->nact[sp] == 0) continue;
+    if (given) memcpy(s->cpar[sp], given, sizeof(double) * (size_t)s->M * s->nact[sp] * 8);
+    for (int a = 0; a < s->M; a++)
+      for (int o = 0; o < s->nact[sp]; o++) {
+        int cnt = 0;
+        for (int k = 0; k < s->K; k++) {
+          if (s->bf_atom[k] != a || s->bf_pow[3 * k] + s->bf_pow[3 * k + 1] + s->bf_pow[3 * k + 2] != 0) continue;
+          for (int l = 0; l < s->bf_nprim[k]; l++)
+            s->cscoef[sp][((size_t)a * s->nact[sp] + o) * s->nsmax + cnt++] = s->pcoef[s->bf_off[k] + l] * mo[(size_t)o * s->K + k];
+        }
+      }
+  }
   s->npade = d->n_pade;
   s->pnum = dup_d(d->pade_num, (size_t)s->npade * QMCB_PADE_MAX);
   s->pden = dup_d(d->pade_den, (size_t)s->npade * QMCB_PADE_MAX);
@@ -188,7 +230,9 @@ void orc_system_free(orc_system *s)
   free(s->pden); free(s->pnn); free(s->pnd); free(s->ctype); free(s->cparam); free(s->en_up); free(s->en_dn);
   free(s->atom_first); free(s->atom_nbf); free(s->atom_lmax);
   free(s->ci);
-  for (int sp = 0; sp < 2; sp++) { free(s->occ[sp]); free(s->swaps[sp]); }
+  free(s->cns);
+  free(s->csexp);
+  for (int sp = 0; sp < 2; sp++) { free(s->occ[sp]); free(s->swaps[sp]); free(s->cpar[sp]); free(s->cscoef[sp]); }
   free(s);
 }
 
@@ -569,6 +613,65 @@ static double inverse_update_col(double *inv, int n, int col, const double *newD
   return detRatio;
 }
 
+static void poly_all(const double *c, int len, double x, double *f, double *df, double *d2f);
+
+/* QMCElectronNucleusCusp::replaceCusps (QMcBeaver/src/QMCElectronNucleusCusp.cpp:574-638)
+ * with QMCElectronNucleusCuspParameters::replaceOrbitalValues,
+ * evaluateOriginalOrbital and evaluateReplacementOrbital
+ * (QMcBeaver/src/QMCElectronNucleusCuspParameters.cpp:107-285).
+ * D: [5][nUP][a] rows of electrons start..stop. */
+static void replace_cusps(const orc_system *s, int sp, const double *R, int start, int stop, double *D, int nUP, int a)
+{
+  for (int i = 0; i < s->M; i++) {
+    const double *nuc = s->nuc_xyz + 3 * i;
+    int counter = 0;
+    for (int j = start; j <= stop; j++) {
+      double xrel = R[3 * j] - nuc[0], yrel = R[3 * j + 1] - nuc[1], zrel = R[3 * j + 2] - nuc[2];
+      double rrel = sqrt(xrel * xrel + yrel * yrel + zrel * zrel);
+      for (int k = 0; k < a; k++) {
+        const double *par = s->cpar[sp] + ((size_t)i * a + k) * 8;
+        if (!(rrel < par[0])) continue;
+        double v = 0.0, gx = 0.0, gy = 0.0, gz = 0.0, l = 0.0;
+        /* evaluateOriginalOrbital */
+        const double *co = s->cscoef[sp] + ((size_t)i * a + k) * s->nsmax;
+        const double *ex = s->csexp + (size_t)i * s->nsmax;
+        double r_sq = rrel * rrel, ov = 0.0, ogx = 0.0, ogy = 0.0, ogz = 0.0, ol = 0.0;
+        for (int q = 0; q < s->cns[i]; q++) {
+          double p0 = ex[q], p1 = co[q];
+          double term = p1 * exp(-p0 * r_sq);
+          ov += term;
+          double temp = -2 * p0 * term;
+          ogx += xrel * temp;
+          ogy += yrel * temp;
+          ogz += zrel * temp;
+          ol += 2 * p0 * (2 * p0 * r_sq - 3) * term;
+        }
+        v -= ov;
+        gx -= ogx;
+        gy -= ogy;
+        gz -= ogz;
+        l -= ol;
+        /* evaluateReplacementOrbital */
+        double f, df, d2f;
+        poly_all(par + 3, 5, rrel, &f, &df, &d2f);
+        double e = par[1] * exp(f);
+        double tg = (e * df) / rrel;
+        v += par[2] + e;
+        gx += tg * xrel;
+        gy += tg * yrel;
+        gz += tg * zrel;
+        l += e * (d2f + df * (2.0 / rrel + df));
+        D[((size_t)0 * nUP + counter) * a + k] += v;
+        D[((size_t)1 * nUP + counter) * a + k] += gx;
+        D[((size_t)2 * nUP + counter) * a + k] += gy;
+        D[((size_t)3 * nUP + counter) * a + k] += gz;
+        D[((size_t)4 * nUP + counter) * a + k] += l;
+      }
+      counter++;
+    }
+  }
+}
+
 /* ---------------------------------------------------- Slater spin (a2-a4) */
 /* QMCSlater::evaluate (QMcBeaver/src/QMCSlater.cpp:828-884) followed by
  * update_Ds (:390-541) and calculate_DerivativeRatios (:648-764) for one spin,
@@ -592,6 +695,7 @@ static void slater_spin(const orc_system *s, orc_walker *w, int sp, const double
   double *ciDet = (double *)malloc(sizeof(double) * (size_t)nUP * n);
   basis_eval(s, R, start, stop, chi);
   contract(s, chi, nUP, C, a, D);
+  if (s->cusp) replace_cusps(s, sp, R, start, stop, D, nUP, a);
   /* splice new rows into D_x / D_xx (QMcBeaver/src/QMCSlater.cpp:465-491) */
   int iEl = whichE == -1 ? 0 : whichE - Start;
   for (int e = 0; e < nUP; e++)

@@ -14,6 +14,18 @@
 // electron update (Sherman-Morrison path, requires one_e_per_iter 1 in the
 // input file, QMcBeaver/src/QMCSlater.cpp:700-711).
 
+// Standard headers first; then the reference's own headers with their
+// private members opened, so that the cusp-replacement records the
+// reference fitted can be read back for comparison (ref_cusp_params).
+#include <cmath>
+#include <iostream>
+#include <list>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+#define private public
+#define protected public
 #include "QMCInput.h"
 #include "QMCSCFJastrow.h"
 #include "QMCWalkerData.h"
@@ -137,6 +149,22 @@ void ref_walker_inverse(void *w, int beta, double *out)
   Array2D<double> &inv = beta ? wd->Dc_invB(0) : wd->Dc_invA(0);
   for (int i = 0; i < inv.dim1(); i++)
     for (int j = 0; j < inv.dim2(); j++) out[i * inv.dim2() + j] = inv(i, j);
+}
+
+// The reference's fitted cusp replacement of (nucleus, orbital) for one
+// spin: rc, sgn0, C, alpha_0..alpha_4 (QMCElectronNucleusCuspParameters);
+// zeros where no replacement was fitted.
+void ref_cusp_params(int beta, int atom, int orbital, double *out)
+{
+  for (int i = 0; i < 8; i++) out[i] = 0.0;
+  QMCSlater &S = beta ? g_qmf->Beta : g_qmf->Alpha;
+  QMCElectronNucleusCuspParameters &P = S.ElectronNucleusCusp.ORParams(atom, orbital);
+  out[0] = P.rc;
+  if (P.rc <= 0.0) return;
+  out[1] = P.sgn0;
+  out[2] = P.C;
+  Array1D<double> c = P.alpha.getCoefficients();
+  for (int i = 0; i < 5 && i < c.dim1(); i++) out[3 + i] = c(i);
 }
 
 } // extern "C"

@@ -29,7 +29,7 @@ EXPORTS = [
     "qmcb_run_steps", "qmcb_num_walkers", "qmcb_get_walkers", "qmcb_copy_slot", "qmcb_synchronize",
     "qmcb_stream", "qmcb_set_walker_weights", "qmcb_branch", "qmcb_set_profiling", "qmcb_get_kernel_stats",
     "qmcb_branch_weights_noalloc", "qmcb_run_steps_async", "qmcb_steps_done", "qmcb_steps_collect",
-    "qmcb_state_bytes",
+    "qmcb_state_bytes", "qmcb_fit_cusps",
 ]
 
 KERNELS = ["move", "branch", "copy", "energy", "refresh"]
@@ -54,6 +54,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.qmcb_last_error.restype = C.c_char_p
     L.qmcb_last_error.argtypes = [vp]
     L.qmcb_create.argtypes = [vp, C.c_int, C.POINTER(vp)]
+    L.qmcb_fit_cusps.argtypes = [vp, C.c_int, vp]
     L.qmcb_destroy.argtypes = [vp]
     L.qmcb_set_params.argtypes = [vp, vp]
     L.qmcb_get_params.argtypes = [vp, vp]
@@ -215,4 +216,22 @@ class QMCB200Functions:
         return int(self.lib.qmcb_stream(self.h) or 0)
 
 
-__all__ = ["QMCB200Functions", "QMCBError", "load_library", "run_params", "QMCB_VMC", "QMCB_DMC", "EXPORTS"]
+def fit_cusps(system: MolecularSystem) -> "tuple[np.ndarray, np.ndarray]":
+    """The electron-nucleus cusp replacement records of both spins
+    (qmcb_fit_cusps; host only): arrays [n_nuclei][orbital rows][8] of rc,
+    sgn0, C, alpha_0..alpha_4 for the mo_alpha / mo_beta rows."""
+    from .desc import PackedSystem
+    lib = load_library()
+    p = PackedSystem(system)
+    out = []
+    for beta in (0, 1):
+        rows = len(system.active_orbitals(bool(beta)))
+        a = np.zeros((system.n_nuclei, max(rows, 1), 8))
+        rc = lib.qmcb_fit_cusps(C.byref(p.desc), beta, a.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise QMCBError(lib.qmcb_last_error(None).decode())
+        out.append(a[:, :rows])
+    return out[0], out[1]
+
+
+__all__ = ["QMCB200Functions", "fit_cusps", "QMCBError", "load_library", "run_params", "QMCB_VMC", "QMCB_DMC", "EXPORTS"]

@@ -170,18 +170,17 @@ class CkmfInput:
         return int(self.beta_occupation[0].sum())
 
     # ------------------------------------------------------------ system
-    def to_system(self, allow_cusp_replacement: bool = False, allow_three_body: bool = False,
+    def to_system(self, replace_cusps: Optional[bool] = None, allow_three_body: bool = False,
                   name: Optional[str] = None) -> MolecularSystem:
         """The Slater-Jastrow system of this input (one or several determinants).
 
-        Refuses inputs that switch on features the walker path does not
-        evaluate, unless told to drop them: cusp replacement
-        (``replace_electron_nucleus_cusps``, default 1 in the reference) and
-        three-body Jastrow blocks."""
+        replace_cusps: None follows ``replace_electron_nucleus_cusps`` (on by
+        default in the reference); True / False overrides it.  Three-body
+        Jastrow blocks are refused unless allow_three_body drops them."""
         if self.flag("trial_function_type", "restricted") not in ("restricted", "unrestricted"):
             raise CkmfError("only restricted / unrestricted trial functions are read")
-        if self.flag("replace_electron_nucleus_cusps", 1, int) and not allow_cusp_replacement:
-            raise CkmfError("replace_electron_nucleus_cusps is on; pass allow_cusp_replacement=True to drop it")
+        if replace_cusps is None:
+            replace_cusps = self.flag("replace_electron_nucleus_cusps", 1, int) == 1
         # the reference evaluates every used three-body block in the file,
         # whatever use_three_body_jastrow says
         if self.three_body_blocks and not allow_three_body:
@@ -237,7 +236,8 @@ class CkmfInput:
             labels=list(self.labels), Z=np.asarray(self.Z, float), coords=np.asarray(self.coords, float),
             basis=self.basis, mo=np.asarray(self.orbitals, float), n_alpha=na, n_beta=nb,
             alpha_occ=a_occ, beta_occ=b_occ, ee_anti=ee_anti, ee_para_up=ee_up, ee_para_dn=ee_dn,
-            en_up=en_up, en_dn=en_dn, name=name or self.path, det_alpha=det_a, det_beta=det_b, ci_coeffs=ci)
+            en_up=en_up, en_dn=en_dn, name=name or self.path, det_alpha=det_a, det_beta=det_b, ci_coeffs=ci,
+            replace_cusps=bool(replace_cusps))
 
     def run_params(self, **overrides) -> D.RunParams:
         """The library's run parameters for this input's flags

@@ -56,6 +56,13 @@ struct DevSys {
   const int *docc[2];    // [ndet][n] active row of each determinant column
   const int *dswap[2];   // [ndet][n] columns swapped in from determinant c-1 (-1 ends)
   const double *ci;      // [ndet] CI coefficients
+  // electron-nucleus cusp replacement (cusp = 0: off)
+  int cusp, nsmax;
+  const int *cns;        // [M] s-type primitives on each nucleus
+  const double *csexp;   // [M][nsmax] their exponents
+  const double *cscoef[2];  // [M][nact][nsmax] primitive coefficient x orbital coefficient
+  const double *cpar[2];    // [M][nact][8] rc, sgn0, C, alpha_0..alpha_4
+  const double *crmax[2];   // [M] largest rc of the spin's orbitals at the nucleus
   int ee[3];
   double Pnn;
   const double4 *nuc;    // [M] x, y, z, Z
@@ -212,6 +219,55 @@ __device__ __forceinline__ void poly_all(const double *c, int len, double x, dou
     f = f * x + c[i];
   }
   d2f *= 2.0;
+}
+
+// Electron-nucleus cusp replacement of one electron's orbital rows
+// D[q * ld + k] (q = value, d/dx, d/dy, d/dz, laplacian; k < a orbitals):
+// within rc of nucleus i the s-type part of orbital k from that nucleus is
+// replaced by C + sgn0 exp(alpha(r)) (QMCElectronNucleusCusp::replaceCusps,
+// QMcBeaver/src/QMCElectronNucleusCusp.cpp:574-638, and
+// QMCElectronNucleusCuspParameters::replaceOrbitalValues /
+// evaluateOriginalOrbital / evaluateReplacementOrbital,
+// QMcBeaver/src/QMCElectronNucleusCuspParameters.cpp:107-285).
+template <typename T>
+__device__ inline void cusp_replace_warp(const DevSys &S, int sp, const double r[3], T *D, int ld, int a)
+{
+  const int lane = threadIdx.x & 31;
+  for (int i = 0; i < S.M; i++) {
+    const double4 P = S.nuc[i];
+    const double x = r[0] - P.x, y = r[1] - P.y, z = r[2] - P.z;
+    const double rr = sqrt(x * x + y * y + z * z);
+    if (!(rr < S.crmax[sp][i])) continue;
+    const int ns = S.cns[i];
+    const double r_sq = rr * rr;
+    for (int k = lane; k < a; k += 32) {
+      const double *par = S.cpar[sp] + ((size_t)i * a + k) * 8;
+      if (!(rr < par[0])) continue;
+      const double *co = S.cscoef[sp] + ((size_t)i * a + k) * S.nsmax;
+      const double *ex = S.csexp + (size_t)i * S.nsmax;
+      double ov = 0.0, ogx = 0.0, ogy = 0.0, ogz = 0.0, ol = 0.0;
+      for (int l = 0; l < ns; l++) {
+        const double p0 = ex[l], p1 = co[l];
+        const double t = p1 * exp(-p0 * r_sq);
+        ov += t;
+        const double tmp = -2 * p0 * t;
+        ogx += x * tmp;
+        ogy += y * tmp;
+        ogz += z * tmp;
+        ol += 2 * p0 * (2 * p0 * r_sq - 3) * t;
+      }
+      double f, df, d2f;
+      poly_all(par + 3, 5, rr, f, df, d2f);
+      const double e = par[1] * exp(f);
+      const double tg = (e * df) / rr;
+      const double rl = e * (d2f + df * (2.0 / rr + df));
+      D[k] = (T)((double)D[k] + ((0.0 - ov) + (par[2] + e)));
+      D[ld + k] = (T)((double)D[ld + k] + ((0.0 - ogx) + tg * x));
+      D[2 * ld + k] = (T)((double)D[2 * ld + k] + ((0.0 - ogy) + tg * y));
+      D[3 * ld + k] = (T)((double)D[3 * ld + k] + ((0.0 - ogz) + tg * z));
+      D[4 * ld + k] = (T)((double)D[4 * ld + k] + ((0.0 - ol) + rl));
+    }
+  }
 }
 
 __device__ __forceinline__ void pade_eval(const DevSys &S, int f, double r, double &u, double &du, double &d2u)

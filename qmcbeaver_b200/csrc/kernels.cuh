@@ -348,6 +348,10 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
         __syncwarp();
         contract_dmma_warp(chi, ldc, S.ct[sp], n, K, Dn);
         __syncwarp();
+        if (S.cusp) {
+          cusp_replace_warp(S, sp, r, Dn, n, n);
+          __syncwarp();
+        }
         for (int o = lane; o < n; o += 32) {
           Dv[e * n + o] = (TS)Dn[o];
           DgT[(0 * n + o) * n + e] = (TS)Dn[n + o];
@@ -787,6 +791,10 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
     basis_shells_warp_f(S, rn, (float *)chi, ldc);
     __syncwarp();
     contract_slices_warp_f((const float *)chi, ldc, S.ctf[sp], n, K, (float *)Dn, (float *)cpart);
+  }
+  if (S.cusp) {
+    __syncwarp();
+    cusp_replace_warp(S, sp, rn, Dn, n, n);
   }
   cp_async_wait<0>();
   __syncwarp();

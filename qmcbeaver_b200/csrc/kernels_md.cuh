@@ -196,6 +196,10 @@ __global__ void __launch_bounds__(128) k_full_md(DevSys S, Layout L, RunCfg cfg,
         __syncwarp();
         contract_dmma_warp(chi, ldc, S.ct[sp], a, K, Dn);
         __syncwarp();
+        if (S.cusp) {
+          cusp_replace_warp(S, sp, r, Dn, a, a);
+          __syncwarp();
+        }
         for (int o = lane; o < a; o += 32) {
           Dv[e * a + o] = Dn[o];
           DgT[(0 * a + o) * n + e] = Dn[a + o];
@@ -359,6 +363,10 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
   __syncwarp();
   contract_dmma_warp(chi, K, S.ct[sp], a, K, Dn);
   __syncwarp();
+  if (S.cusp) {
+    cusp_replace_warp(S, sp, rn, Dn, a, a);
+    __syncwarp();
+  }
 
   const int cur = sc0[SC_MDCUR_A + sp] != 0.0 ? 1 : 0;
   const MdBlock src = md_block(S, L, blk, sp, cur), dst = md_block(S, L, blk, sp, 1 - cur);

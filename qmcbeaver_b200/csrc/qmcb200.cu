@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/qmcb200.h"
+#include "cusp_fit.h"
 #include "kernels.cuh"
 #include "kernels_md.cuh"
 
@@ -60,6 +61,9 @@ struct qmcb_handle {
   int *d_en[2] = {nullptr, nullptr};
   int *d_docc[2] = {nullptr, nullptr};
   int *d_dswap[2] = {nullptr, nullptr};
+  int *d_cns = nullptr;
+  double *d_csexp = nullptr, *d_cscoef[2] = {nullptr, nullptr}, *d_cpar[2] = {nullptr, nullptr};
+  double *d_crmax[2] = {nullptr, nullptr};
   double *d_ci = nullptr;
   bool md = false;  // several determinants: the k_*_md kernels
   double *d_state = nullptr;
@@ -354,6 +358,19 @@ const char *qmcb_version(void) { return "qmcb200 0.1 (sm_100a, FP64 parity path)
 
 const char *qmcb_last_error(const qmcb_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
 
+int qmcb_fit_cusps(const qmcb_system_desc *d, int beta, double *out)
+{
+  if (!d || !out || d->n_nuclei <= 0 || d->n_basis <= 0) return fail(nullptr, QMCB_E_ARG, "qmcb_fit_cusps: bad argument");
+  const int rows = d->n_det > 1 ? (beta ? d->n_act_beta : d->n_act_alpha) : (beta ? d->n_beta : d->n_alpha);
+  const double *mo = beta ? d->mo_beta : d->mo_alpha;
+  if (rows <= 0) return QMCB_OK;
+  char err[256];
+  if (qmcb_cusp_fit(d->n_nuclei, d->nuc_xyz, d->nuc_charge, d->n_basis, d->bf_atom, d->bf_powers, d->bf_nprim,
+                    d->bf_prim_offset, d->prim_exponent, d->prim_coeff, rows, mo, out, err))
+    return fail(nullptr, QMCB_E_ARG, std::string("qmcb_fit_cusps: ") + err);
+  return QMCB_OK;
+}
+
 int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
 {
   qmcb_handle *h = nullptr;
@@ -468,6 +485,62 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   }
   if (md)
     for (int c = 0; c < d->n_det; c++) ci[c] = d->ci_coeff[c];
+  // electron-nucleus cusp replacement tables
+  std::vector<int> cns(M, 0);
+  int nsmax = 1;
+  for (int k = 0; k < K; k++)
+    if (d->bf_powers[3 * k] + d->bf_powers[3 * k + 1] + d->bf_powers[3 * k + 2] == 0) cns[d->bf_atom[k]] += d->bf_nprim[k];
+  for (int a = 0; a < M; a++) nsmax = std::max(nsmax, cns[a]);
+  std::vector<double> csexp((size_t)M * nsmax, 0.0), cscoef[2], cpar[2], crmax[2];
+  for (int sp = 0; sp < 2; sp++) {
+    const int a_ = std::max(nact[sp], 1);
+    cscoef[sp].assign((size_t)M * a_ * nsmax, 0.0);
+    cpar[sp].assign((size_t)M * a_ * QMCB_CUSP_REC, 0.0);
+    crmax[sp].assign(M, 0.0);
+  }
+  if (d->replace_cusps) {
+    std::vector<int> fill(M, 0);
+    for (int k = 0; k < K; k++) {
+      const int at = d->bf_atom[k];
+      if (d->bf_powers[3 * k] + d->bf_powers[3 * k + 1] + d->bf_powers[3 * k + 2] != 0) continue;
+      for (int l = 0; l < d->bf_nprim[k]; l++) csexp[(size_t)at * nsmax + fill[at]++] = d->prim_exponent[d->bf_prim_offset[k] + l];
+    }
+    for (int sp = 0; sp < 2; sp++) {
+      const int a_ = nact[sp];
+      if (a_ == 0) continue;
+      const double *mo = sp ? d->mo_beta : d->mo_alpha;
+      const double *given = sp ? d->cusp_beta : d->cusp_alpha;
+      if (given) {
+        std::copy(given, given + (size_t)M * a_ * QMCB_CUSP_REC, cpar[sp].begin());
+      } else {
+        std::vector<double> xyz(3 * M), Zd(M);
+        for (int at = 0; at < M; at++) {
+          for (int x = 0; x < 3; x++) xyz[3 * at + x] = d->nuc_xyz[3 * at + x];
+          Zd[at] = d->nuc_charge[at];
+        }
+        char err[256];
+        if (qmcb_cusp_fit(M, xyz.data(), Zd.data(), K, d->bf_atom, d->bf_powers, d->bf_nprim, d->bf_prim_offset,
+                          d->prim_exponent, d->prim_coeff, a_, mo, cpar[sp].data(), err)) {
+          delete h;
+          return fail(nullptr, QMCB_E_ARG, std::string("qmcb_create: ") + err);
+        }
+      }
+      // s-part coefficients of every (nucleus, orbital): primitive coefficient x orbital coefficient
+      for (int at = 0; at < M; at++) {
+        for (int o = 0; o < a_; o++) {
+          int cnt = 0;
+          for (int k = 0; k < K; k++) {
+            if (d->bf_atom[k] != at || d->bf_powers[3 * k] + d->bf_powers[3 * k + 1] + d->bf_powers[3 * k + 2] != 0)
+              continue;
+            for (int l = 0; l < d->bf_nprim[k]; l++)
+              cscoef[sp][((size_t)at * a_ + o) * nsmax + cnt++] =
+                  d->prim_coeff[d->bf_prim_offset[k] + l] * mo[(size_t)o * K + k];
+          }
+          crmax[sp][at] = std::max(crmax[sp][at], cpar[sp][((size_t)at * a_ + o) * QMCB_CUSP_REC]);
+        }
+      }
+    }
+  }
   std::vector<double> pade((size_t)std::max(d->n_pade, 1) * 2 * kPadeMax, 0.0);
   std::vector<int2> plen(std::max(d->n_pade, 1), make_int2(1, 1));
   for (int f = 0; f < d->n_pade; f++) {
@@ -572,6 +645,13 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(upload(&h->d_dswap[0], dswap[0]));
   CKC(upload(&h->d_dswap[1], dswap[1]));
   CKC(upload(&h->d_ci, ci));
+  CKC(upload(&h->d_cns, cns));
+  CKC(upload(&h->d_csexp, csexp));
+  for (int sp = 0; sp < 2; sp++) {
+    CKC(upload(&h->d_cscoef[sp], cscoef[sp]));
+    CKC(upload(&h->d_cpar[sp], cpar[sp]));
+    CKC(upload(&h->d_crmax[sp], crmax[sp]));
+  }
   h->md = md;
 
   DevSys &S = h->sys;
@@ -610,6 +690,15 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   S.docc[1] = h->d_docc[1];
   S.dswap[0] = h->d_dswap[0];
   S.dswap[1] = h->d_dswap[1];
+  S.cusp = d->replace_cusps ? 1 : 0;
+  S.nsmax = nsmax;
+  S.cns = h->d_cns;
+  S.csexp = h->d_csexp;
+  for (int sp = 0; sp < 2; sp++) {
+    S.cscoef[sp] = h->d_cscoef[sp];
+    S.cpar[sp] = h->d_cpar[sp];
+    S.crmax[sp] = h->d_crmax[sp];
+  }
   S.ci = h->d_ci;
 
   // ---- per-walker block layout (offsets in doubles, arrays 32-byte aligned)
@@ -717,7 +806,8 @@ int qmcb_destroy(qmcb_handle *h)
 {
   if (!h) return QMCB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *ptrs[] = {h->d_docc[0], h->d_docc[1], h->d_dswap[0], h->d_dswap[1], h->d_ci, h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
+  void *ptrs[] = {h->d_cns, h->d_csexp, h->d_cscoef[0], h->d_cscoef[1], h->d_cpar[0], h->d_cpar[1], h->d_crmax[0],
+                  h->d_crmax[1], h->d_docc[0], h->d_docc[1], h->d_dswap[0], h->d_dswap[1], h->d_ci, h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
                   h->d_copies, h->d_stats, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
   for (void *p : ptrs)

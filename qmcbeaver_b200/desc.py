@@ -34,6 +34,7 @@ class SystemDesc(C.Structure):
         ("ee_pade", C.c_int * 3), ("en_pade_up", _ip), ("en_pade_dn", _ip),
         ("n_det", C.c_int), ("n_act_alpha", C.c_int), ("n_act_beta", C.c_int),
         ("det_occ_alpha", _ip), ("det_occ_beta", _ip), ("ci_coeff", _dp),
+        ("replace_cusps", C.c_int), ("cusp_alpha", _dp), ("cusp_beta", _dp),
     ]
 
 
@@ -154,5 +155,13 @@ class PackedSystem:
         d.det_occ_alpha = _i(k["occ_a"])
         d.det_occ_beta = _i(k["occ_b"])
         d.ci_coeff = _d(k["ci"])
+        d.replace_cusps = 1 if s.replace_cusps else 0
         self.desc = d
+
+    def set_cusp_tables(self, alpha: np.ndarray, beta: np.ndarray) -> None:
+        """Passes fitted cusp records (qmcb_fit_cusps) instead of fitting again."""
+        self._keep["cusp_a"] = np.ascontiguousarray(alpha, np.float64)
+        self._keep["cusp_b"] = np.ascontiguousarray(beta, np.float64)
+        self.desc.cusp_alpha = _d(self._keep["cusp_a"])
+        self.desc.cusp_beta = _d(self._keep["cusp_b"])
         assert PADE_MAX == 16

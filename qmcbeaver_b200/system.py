@@ -181,6 +181,8 @@ class MolecularSystem:
     det_alpha: Optional[np.ndarray] = None  # (n_det, n_alpha)
     det_beta: Optional[np.ndarray] = None   # (n_det, n_beta)
     ci_coeffs: Optional[np.ndarray] = None  # (n_det,)
+    # electron-nucleus cusp replacement of the orbitals (replace_electron_nucleus_cusps)
+    replace_cusps: bool = False
 
     # ------------------------------------------------------------------ sizes
     @property
@@ -347,6 +349,7 @@ class MolecularSystem:
             (self.n_beta == 0 or self.en_dn == self.en_up)
         f.update({
             "link_Jastrow_parameters": 1 if linked else 0,
+            "replace_electron_nucleus_cusps": 1 if self.replace_cusps else 0,
             "atoms": self.n_nuclei,
             "charge": self.charge,
             "norbitals": self.mo.shape[0],
@@ -852,7 +855,7 @@ def system_to_arrays(s: MolecularSystem) -> Dict[str, np.ndarray]:
         ee_anti=pade_arr(s.ee_anti), ee_para_up=pade_arr(s.ee_para_up), ee_para_dn=pade_arr(s.ee_para_dn),
         en_up=np.stack([pade_arr(s.en_up.get(l)) for l in s.labels]),
         en_dn=np.stack([pade_arr(s.en_dn.get(l)) for l in s.labels]),
-        name=np.array(s.name),
+        name=np.array(s.name), replace_cusps=np.array(1 if s.replace_cusps else 0),
         **({} if s.det_alpha is None else dict(det_alpha=np.asarray(s.det_alpha), det_beta=np.asarray(s.det_beta),
                                               ci_coeffs=np.asarray(s.ci_coeffs, np.float64))))
 
@@ -890,4 +893,5 @@ def system_from_arrays(d) -> MolecularSystem:
         en_up=en_up, en_dn=en_dn, name=str(d["name"]),
         det_alpha=np.array(d["det_alpha"]) if "det_alpha" in d else None,
         det_beta=np.array(d["det_beta"]) if "det_beta" in d else None,
-        ci_coeffs=np.array(d["ci_coeffs"], np.float64) if "ci_coeffs" in d else None)
+        ci_coeffs=np.array(d["ci_coeffs"], np.float64) if "ci_coeffs" in d else None,
+        replace_cusps=bool(int(d["replace_cusps"])) if "replace_cusps" in d else False)

@@ -32,17 +32,30 @@ CASES = {
     # twelve determinants (single excitations into every virtual orbital of
     # both spins, doubles)
     "multidet_vmc": ("vmc_multidet_12e", 2, 0.01, 6, 40, 0.2, 6),
+    # electron-nucleus cusp replacement, electrons placed inside the
+    # replacement radii every third move
+    "cusp_dmc30": ("dmc_6nuc_30e", 2, 0.01, 4, 40, 0.15, 7),
 }
+CUSP_CASES = {"cusp_dmc30"}
 
 
 def run_case(name: str) -> None:
+    import dataclasses
     from qmcbeaver_b200.system import make_system, system_to_arrays
     from oracle.evaluators import ReferenceEvaluator
     workload, qf, dt, W, moves, sigma, revert = CASES[name]
     s = make_system(workload, seed=1)
+    cusp = name in CUSP_CASES
+    if cusp:
+        s = dataclasses.replace(s, replace_cusps=True)
     ref = ReferenceEvaluator(s, qf_mod=qf, dt=dt)
     rng = np.random.default_rng(2024)
     R = s.initial_positions(W, seed=11)
+    if cusp:
+        # one electron of each walker within 0.03 bohr of a nucleus
+        for w in range(W):
+            R[w, int(rng.integers(s.n_electrons))] = s.coords[int(rng.integers(s.n_nuclei))] + 0.03 * rng.random() * \
+                rng.standard_normal(3) / np.sqrt(3.0)
     N = s.n_electrons
     ws = ref.new_walkers(W)
     whichE, Rseq, outs = [], [], []
@@ -66,7 +79,10 @@ def run_case(name: str) -> None:
             prev = None
             continue
         old = R[:, e].copy()
-        R[:, e] = R[:, e] + sigma * rng.standard_normal((W, 3))
+        if cusp and m % 3 == 0:
+            R[:, e] = s.coords[int(rng.integers(s.n_nuclei))] + 0.02 * rng.standard_normal((W, 3))
+        else:
+            R[:, e] = R[:, e] + sigma * rng.standard_normal((W, 3))
         call(e, R)
         prev = (e, old)
     keys = ["log_abs_psi", "sign", "grad", "mod_grad", "lap", "e_local", "potential", "ne", "ee", "singular"]

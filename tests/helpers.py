@@ -100,3 +100,18 @@ def slater_conditions(orc, walkers, system):
                 for det in range(system.n_det):
                     c[i] = max(c[i], np.linalg.cond(orc.inverse(w, beta, det)))
     return c
+
+
+def place_near_nuclei(R, system, rng, radius=0.03):
+    """Moves one electron of every walker to within `radius` bohr of a nucleus
+    (inside every cusp-replacement radius of the systems tested), so the
+    replacement branch is exercised; returns the electron index per walker."""
+    W, N = R.shape[0], R.shape[1]
+    es = np.zeros(W, int)
+    for w in range(W):
+        e = int(rng.integers(N))
+        a = int(rng.integers(system.n_nuclei))
+        v = rng.standard_normal(3)
+        R[w, e] = system.coords[a] + radius * rng.random() * v / np.linalg.norm(v)
+        es[w] = e
+    return es

@@ -1,7 +1,7 @@
 """The .ckmf reader and writer (config I/O), and -- where the reference tree
 is present -- the oracle against the reference run on the reference's own
-input files (two-body Jastrows; cusp replacement and three-body blocks
-left out, as the walker path evaluates neither)."""
+input files (two-body Jastrows, one or several determinants; three-body
+blocks left out; cusp replacement off here, on in test_cusp.py)."""
 import os
 import subprocess
 import sys
@@ -173,12 +173,13 @@ def test_reader_sections_and_function_layouts():
 
 
 def test_reader_refusals_and_constraints():
-    with pytest.raises(CkmfError, match="replace_electron_nucleus_cusps"):
-        read_ckmf("t", _text()).to_system(allow_three_body=True)
+    # cusp replacement follows the input's flag (on by default in the reference)
+    assert read_ckmf("t", _text()).to_system(allow_three_body=True).replace_cusps
+    assert not read_ckmf("t", _text()).to_system(replace_cusps=False, allow_three_body=True).replace_cusps
     c = read_ckmf("t", _text(ndet=2, aocc="1 0\n0 1", bocc="1 0\n1 0", ci="0.9 c 0 -0.5"))
     assert c.n_determinants == 2
     np.testing.assert_allclose(c.ci_coeffs, [0.9, -0.45])
-    s = c.to_system(allow_cusp_replacement=True, allow_three_body=True)
+    s = c.to_system(allow_three_body=True)
     assert s.n_det == 2 and s.det_alpha.tolist() == [[0], [1]] and s.det_beta.tolist() == [[0], [0]]
     np.testing.assert_array_equal(s.mo_alpha(), s.mo)          # both orbitals active for alpha
     assert s.det_columns(True).tolist() == [[0], [0]]
@@ -227,7 +228,7 @@ def test_reader_reads_every_reference_input():
             continue
         c = read_ckmf(p)
         if c.n_determinants == 1:
-            s = c.to_system(allow_cusp_replacement=True, allow_three_body=True)
+            s = c.to_system(allow_three_body=True)
             assert s.n_electrons == int(round(s.Z.sum())) - int(c.flags.get("charge", 0))
 
 
@@ -239,7 +240,7 @@ from oracle.evaluators import OracleEvaluator, ReferenceEvaluator
 from helpers import slater_conditions
 path, one_e = {path!r}, {one_e}
 text = open(path).read()
-s = read_ckmf(path).to_system(allow_cusp_replacement=True, allow_three_body=True)
+s = read_ckmf(path).to_system(replace_cusps=False, allow_three_body=True)
 W, qf, dt = 3, 2, 0.01
 ref = ReferenceEvaluator(s, qf_mod=qf, dt=dt, ckmf_text=text, one_e_per_iter=one_e)
 orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
