@@ -121,6 +121,19 @@ typedef struct qmcb_system_desc {
   int replace_cusps;
   const double *cusp_alpha;
   const double *cusp_beta;
+  /* Three-body electron-electron-nucleus Jastrow (QMCThreeBodyJastrow with
+     CambridgeThreeBodyCorrelationFunction, QMcBeaver/src/QMCThreeBodyJastrow.cpp,
+     QMcBeaver/src/CambridgeThreeBodyCorrelationFunction.cpp): n_tb functions,
+     each U = (L r1 - 1)^C (L r2 - 1)^C sum_lmn c_lmn (L r1)^l (L r2)^m (L r12)^n
+     for L r1, L r2 < 1; the coefficients after the input's dependency matrix. */
+  int n_tb;
+  const int *tb_nen;            /* [n_tb] NeN (powers of r1, r2: 0 .. NeN-1) */
+  const int *tb_nee;            /* [n_tb] Nee (powers of r12) */
+  const int *tb_C;              /* [n_tb] cutoff exponent C */
+  const double *tb_cutoff;      /* [n_tb] L */
+  const int *tb_offset;         /* [n_tb] first coefficient in tb_coeff */
+  const double *tb_coeff;       /* c_lmn at offset + l*NeN*Nee + m*Nee + n */
+  const int *tb_pair;           /* [M][3] function of up-down, up-up, down-down pairs (-1 none) */
 } qmcb_system_desc;
 
 /* One fitted cusp-replacement record: rc, sgn0, C, alpha_0 .. alpha_4

@@ -192,8 +192,10 @@ class ReferenceEvaluator(_Base):
                           "use_three_body_jastrow": 0,
                           "one_e_per_iter": int(one_e_per_iter),
                           "print_configs": 0, "optimize_Psi": 0})
+            if not system.three_body:
+                ckmf_text = strip_three_body(ckmf_text)
             with open(path, "w") as fh:
-                fh.write(patch_flags(strip_three_body(ckmf_text), flags))
+                fh.write(patch_flags(ckmf_text, flags))
         L.ref_init(path.encode())
         os.unlink(path)
         ReferenceEvaluator._loaded = path

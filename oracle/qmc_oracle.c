@@ -31,6 +31,9 @@ struct orc_system {
   double *csexp;                          /* [M][nsmax] */
   double *cscoef[2];                      /* [M][nact][nsmax] */
   double *cpar[2];                        /* [M][nact][8] rc, sgn0, C, alpha_0..4 */
+  int ntb;                                /* three-body functions */
+  int *tb_nen, *tb_nee, *tb_C, *tb_off, *tb_pair;
+  double *tb_cut, *tb_coef;
   int npade;
   double *pnum, *pden;
   int *pnn, *pnd;
@@ -63,6 +66,7 @@ struct orc_walker {
   int singular;
   double logpsi, sign;
   double kappa;       /* condition number of the determinant-weighted laplacian sum */
+  double *tU, *tUxx, *tUx1, *tUx2;  /* three-body pair caches UijA, UijA_xx, UijA_x1, UijA_x2 [N][N](x3) */
 };
 
 static double *dup_d(const double *p, size_t n)
@@ -143,6 +147,28 @@ orc_system *orc_system_new(const qmcb_system_desc *d, int qf_mod, double qf_a, d
     for (int c = 0; c < s->ndet; c++)
       for (int o = 0; o < n; o++) s->occ[sp][c * n + o] = d->n_det > 1 ? src[c * n + o] : o;
     make_swaps(s->occ[sp], s->ndet, n, s->swaps[sp]);
+  }
+  /* three-body Jastrow tables */
+  s->ntb = d->n_tb;
+  {
+    int nt = s->ntb > 0 ? s->ntb : 1, ncoef = 0;
+    s->tb_nen = (int *)calloc(nt, sizeof(int));
+    s->tb_nee = (int *)calloc(nt, sizeof(int));
+    s->tb_C = (int *)calloc(nt, sizeof(int));
+    s->tb_off = (int *)calloc(nt, sizeof(int));
+    s->tb_cut = (double *)calloc(nt, sizeof(double));
+    s->tb_pair = (int *)malloc(sizeof(int) * 3 * s->M);
+    for (int t = 0; t < 3 * s->M; t++) s->tb_pair[t] = s->ntb > 0 ? d->tb_pair[t] : -1;
+    for (int f = 0; f < s->ntb; f++) {
+      s->tb_nen[f] = d->tb_nen[f];
+      s->tb_nee[f] = d->tb_nee[f];
+      s->tb_C[f] = d->tb_C[f];
+      s->tb_off[f] = d->tb_offset[f];
+      s->tb_cut[f] = d->tb_cutoff[f];
+      int e = d->tb_offset[f] + d->tb_nen[f] * d->tb_nen[f] * d->tb_nee[f];
+      if (e > ncoef) ncoef = e;
+    }
+    s->tb_coef = dup_d(s->ntb > 0 ? d->tb_coeff : NULL, ncoef);
   }
   /* cusp replacement: the fitted records come with the descriptor; the s
    * parts (sTypeCoeffs, QMcBeaver/src/QMCElectronNucleusCusp.cpp:83-102) are
@@ -232,6 +258,7 @@ void orc_system_free(orc_system *s)
   free(s->ci);
   free(s->cns);
   free(s->csexp);
+  free(s->tb_nen); free(s->tb_nee); free(s->tb_C); free(s->tb_off); free(s->tb_cut); free(s->tb_pair); free(s->tb_coef);
   for (int sp = 0; sp < 2; sp++) { free(s->occ[sp]); free(s->swaps[sp]); free(s->cpar[sp]); free(s->cscoef[sp]); }
   free(s);
 }
@@ -270,6 +297,10 @@ static void walker_alloc(orc_walker *w, const orc_system *s)
   w->D_x = (double *)calloc((size_t)N * 3, sizeof(double));
   w->grad = (double *)calloc((size_t)N * 3, sizeof(double));
   w->mgrad = (double *)calloc((size_t)N * 3, sizeof(double));
+  w->tU = (double *)calloc((size_t)N * N, sizeof(double));
+  w->tUxx = (double *)calloc((size_t)N * N, sizeof(double));
+  w->tUx1 = (double *)calloc((size_t)N * N * 3, sizeof(double));
+  w->tUx2 = (double *)calloc((size_t)N * N * 3, sizeof(double));
 }
 
 orc_walker *orc_walker_new(const orc_system *s)
@@ -295,6 +326,7 @@ void orc_walker_free(orc_walker *w)
   free(w->rij); free(w->rij_uvec); free(w->riA); free(w->riA_uvec); free(w->Uij); free(w->Uij_x);
   free(w->Uij_xx); free(w->UiA); free(w->UiA_x); free(w->UiA_xx); free(w->U_x); free(w->D_x);
   free(w->grad); free(w->mgrad);
+  free(w->tU); free(w->tUxx); free(w->tUx1); free(w->tUx2);
   free(w);
 }
 
@@ -328,6 +360,10 @@ void orc_walker_copy(orc_walker *dst, const orc_walker *src)
   memcpy(dst->D_x, src->D_x, (size_t)N * 3 * sizeof(double));
   memcpy(dst->grad, src->grad, (size_t)N * 3 * sizeof(double));
   memcpy(dst->mgrad, src->mgrad, (size_t)N * 3 * sizeof(double));
+  memcpy(dst->tU, src->tU, (size_t)N * N * sizeof(double));
+  memcpy(dst->tUxx, src->tUxx, (size_t)N * N * sizeof(double));
+  memcpy(dst->tUx1, src->tUx1, (size_t)N * N * 3 * sizeof(double));
+  memcpy(dst->tUx2, src->tUx2, (size_t)N * N * 3 * sizeof(double));
   dst->U = src->U; dst->U_xx = src->U_xx; dst->D_xx = src->D_xx;
   dst->E_L = src->E_L; dst->KE = src->KE; dst->PE = src->PE; dst->neE = src->neE; dst->eeE = src->eeE;
   dst->lap = src->lap; dst->singular = src->singular; dst->logpsi = src->logpsi; dst->sign = src->sign;
@@ -901,6 +937,201 @@ static void jastrow_en(const orc_system *s, orc_walker *w, int whichE)
   }
 }
 
+/* ------------------------------------------------------- three-body (a6) */
+/* CambridgeThreeBodyCorrelationFunction::setElectron / evaluate / getLapPoly
+ * (QMcBeaver/src/CambridgeThreeBodyCorrelationFunction.cpp:150-470) for the
+ * pair (E1 first, E2 second) around nucleus `nuc` with function f.  Returns 0
+ * when either electron is outside the cutoff. */
+static int tb_pair_eval(const orc_system *s, const orc_walker *w, int f, int E1, int E2, int nuc, double *U,
+                        double *lapv, double g1[3], double g2[3])
+{
+  int N = s->N, M = s->M;
+  int Nen = s->tb_nen[f], Nee = s->tb_nee[f], C = s->tb_C[f];
+  double L = s->tb_cut[f];
+  if (fabs(L) < 1e-10) L = 1.0e10;
+  const double *coeffs = s->tb_coef + s->tb_off[f];
+  double d1pow[16], d1pow1[16], d1pow2[16], d2pow[16], d2pow1[16], d2pow2[16], r12pow[16], r12pow1[16], r12pow2[16];
+  /* setElectron(true, E1) */
+  double r1 = w->riA[E1 * M + nuc] * L, d1 = r1 - 1.0;
+  if (d1 > 0.0) return 0;
+  const double *r1v = w->riA_uvec + ((size_t)E1 * M + nuc) * 3;
+  double pre1 = pow(d1, C), d1pre1 = pre1 * C / d1, d2pre1 = (C - 1.0) * d1pre1 / d1;
+  d1pow[0] = 1.0; d1pow1[0] = 0.0; d1pow2[0] = 0.0; d1pow2[1] = 0.0;
+  for (int i = 1; i < Nen; i++) {
+    d1pow[i] = d1pow[i - 1] * r1;
+    d1pow1[i] = d1pow[i - 1] * i;
+    if (i < 2) continue;
+    d1pow2[i] = d1pow[i - 2] * i * (i - 1);
+  }
+  /* setElectron(false, E2) */
+  double r2 = w->riA[E2 * M + nuc] * L, d2 = r2 - 1.0;
+  if (d2 > 0.0) return 0;
+  const double *r2v = w->riA_uvec + ((size_t)E2 * M + nuc) * 3;
+  double pre2 = pow(d2, C), d1pre2 = pre2 * C / d2, d2pre2 = (C - 1.0) * d1pre2 / d2;
+  d2pow[0] = 1.0; d2pow1[0] = 0.0; d2pow2[0] = 0.0; d2pow2[1] = 0.0;
+  for (int i = 1; i < Nen; i++) {
+    d2pow[i] = d2pow[i - 1] * r2;
+    d2pow1[i] = d2pow[i - 1] * i;
+    if (i < 2) continue;
+    d2pow2[i] = d2pow[i - 2] * i * (i - 1);
+  }
+  /* evaluate(rij_uvec(E1, E2), rij(E1, E2)) */
+  double r12 = w->rij[E1 * N + E2] * L;
+  const double *r12v = w->rij_uvec + ((size_t)E1 * N + E2) * 3;
+  r12pow[0] = 1.0; r12pow1[0] = 0.0; r12pow2[0] = 0.0; r12pow2[1] = 0.0;
+  for (int i = 1; i < Nee; i++) {
+    r12pow[i] = r12pow[i - 1] * r12;
+    r12pow1[i] = r12pow[i - 1] * i;
+    if (i < 2) continue;
+    r12pow2[i] = r12pow[i - 2] * i * (i - 1);
+  }
+  double P = 0, Pl = 0, Pl2 = 0, Pln = 0, Pm = 0, Pm2 = 0, Pmn = 0, Pn = 0, Pn2 = 0;
+  int ai = 0;
+  for (int l = 0; l < Nen; l++)
+    for (int m = 0; m < Nen; m++) {
+      double lm = d1pow[l] * d2pow[m], dlm = d1pow1[l] * d2pow[m], ldm = d1pow[l] * d2pow1[m];
+      double d2lm = d1pow2[l] * d2pow[m], ld2m = d1pow[l] * d2pow2[m];
+      for (int n = 0; n < Nee; n++) {
+        double coeff = coeffs[ai];
+        ai++;
+        if (fabs(coeff) < 1e-30) continue;
+        double term = lm * r12pow[n];
+        double _l = dlm * r12pow[n], _m = ldm * r12pow[n], _n = lm * r12pow1[n];
+        double ln = dlm * r12pow1[n], mn = ldm * r12pow1[n];
+        double l2 = d2lm * r12pow[n], m2 = ld2m * r12pow[n], n2 = lm * r12pow2[n];
+        P += coeff * term;
+        Pl += coeff * _l;
+        Pm += coeff * _m;
+        Pn += coeff * _n;
+        Pln += coeff * ln;
+        Pmn += coeff * mn;
+        Pl2 += coeff * l2;
+        Pm2 += coeff * m2;
+        Pn2 += coeff * n2;
+      }
+    }
+  *U = pre1 * pre2 * P;
+  double dU_dr12 = pre1 * pre2 * Pn;
+  double dU_dr1 = (d1pre1 * P + pre1 * Pl) * pre2;
+  double dU_dr2 = (d1pre2 * P + pre2 * Pm) * pre1;
+  for (int i = 0; i < 3; i++) {
+    g1[i] = L * (dU_dr1 * r1v[i] + dU_dr12 * r12v[i]);
+    g2[i] = L * (dU_dr2 * r2v[i] - dU_dr12 * r12v[i]);
+  }
+  /* getLapPoly */
+  double lap = 2.0 * (2.0 * dU_dr12 / r12 + dU_dr1 / r1 + dU_dr2 / r2);
+  double d2U_d2r1 = pre2 * (d2pre1 * P + 2.0 * d1pre1 * Pl + pre1 * Pl2);
+  double d2U_d2r2 = pre1 * (d2pre2 * P + 2.0 * d1pre2 * Pm + pre2 * Pm2);
+  double d2U_d2r12 = pre1 * pre2 * Pn2;
+  lap += 2.0 * d2U_d2r12 + d2U_d2r1 + d2U_d2r2;
+  double d2U_dr1r12 = 2.0 * pre2 * (d1pre1 * Pn + pre1 * Pln);
+  double d2U_dr2r12 = 2.0 * pre1 * (d1pre2 * Pn + pre2 * Pmn);
+  for (int i = 0; i < 3; i++) lap += r12v[i] * (r1v[i] * d2U_dr1r12 - r2v[i] * d2U_dr2r12);
+  *lapv = lap * L * L;
+  return 1;
+}
+
+/* QMCThreeBodyJastrow::collectForPair (QMcBeaver/src/QMCThreeBodyJastrow.cpp:403-441) */
+static void tb_collect(const orc_system *s, orc_walker *w, int f, int E1, int E2, int nuc)
+{
+  if (f < 0) return;
+  int N = s->N;
+  double U, lap, g1[3], g2[3];
+  if (!tb_pair_eval(s, w, f, E1, E2, nuc, &U, &lap, g1, g2)) return;
+  w->tU[E1 * N + E2] += U;
+  w->tUxx[E1 * N + E2] += lap;
+  for (int i = 0; i < 3; i++) {
+    w->tUx1[(E1 * N + E2) * 3 + i] += g1[i];
+    w->tUx2[(E1 * N + E2) * 3 + i] += g2[i];
+  }
+}
+
+/* QMCThreeBodyJastrow::updateAll / updateOne (QMcBeaver/src/QMCThreeBodyJastrow.cpp:43-178,320-401) */
+static void jastrow_3b(const orc_system *s, orc_walker *w, int whichE)
+{
+  if (s->ntb <= 0) return;
+  int N = s->N, na = s->na, nb = s->nb, M = s->M;
+  if (whichE == -1) {
+    for (int E1 = 0; E1 < N; E1++)
+      for (int E2 = 0; E2 < E1; E2++) {
+        w->U -= w->tU[E1 * N + E2];
+        w->U_xx -= w->tUxx[E1 * N + E2];
+        for (int x = 0; x < 3; x++) {
+          w->U_x[E1 * 3 + x] -= w->tUx1[(E1 * N + E2) * 3 + x];
+          w->U_x[E2 * 3 + x] -= w->tUx2[(E1 * N + E2) * 3 + x];
+        }
+      }
+    memset(w->tU, 0, sizeof(double) * N * N);
+    memset(w->tUxx, 0, sizeof(double) * N * N);
+    memset(w->tUx1, 0, sizeof(double) * N * N * 3);
+    memset(w->tUx2, 0, sizeof(double) * N * N * 3);
+    for (int nuc = 0; nuc < M; nuc++) {
+      int fud = s->tb_pair[3 * nuc], fuu = s->tb_pair[3 * nuc + 1], fdd = s->tb_pair[3 * nuc + 2];
+      if (na > 0 && nb > 0)
+        for (int E2 = na; E2 < na + nb; E2++)
+          for (int E1 = 0; E1 < na; E1++) tb_collect(s, w, fud, E2, E1, nuc);
+      if (na > 1)
+        for (int E1 = 1; E1 < na; E1++)
+          for (int E2 = 0; E2 < E1; E2++) tb_collect(s, w, fuu, E1, E2, nuc);
+      if (nb > 1)
+        for (int E1 = na + 1; E1 < N; E1++)
+          for (int E2 = na; E2 < E1; E2++) tb_collect(s, w, fdd, E1, E2, nuc);
+    }
+    for (int E1 = 0; E1 < N; E1++)
+      for (int E2 = 0; E2 < E1; E2++) {
+        w->U += w->tU[E1 * N + E2];
+        w->U_xx += w->tUxx[E1 * N + E2];
+        for (int x = 0; x < 3; x++) {
+          w->U_x[E1 * 3 + x] += w->tUx1[(E1 * N + E2) * 3 + x];
+          w->U_x[E2 * 3 + x] += w->tUx2[(E1 * N + E2) * 3 + x];
+        }
+      }
+    return;
+  }
+  int E = whichE, isAlpha = E < na;
+  for (int E2 = 0; E2 < N; E2++) {
+    if (E == E2) continue;
+    int EH = E > E2 ? E : E2, EL = E < E2 ? E : E2;
+    w->U -= w->tU[EH * N + EL];
+    w->tU[EH * N + EL] = 0.0;
+    w->U_xx -= w->tUxx[EH * N + EL];
+    w->tUxx[EH * N + EL] = 0.0;
+    for (int x = 0; x < 3; x++) {
+      w->U_x[EH * 3 + x] -= w->tUx1[(EH * N + EL) * 3 + x];
+      w->tUx1[(EH * N + EL) * 3 + x] = 0.0;
+      w->U_x[EL * 3 + x] -= w->tUx2[(EH * N + EL) * 3 + x];
+      w->tUx2[(EH * N + EL) * 3 + x] = 0.0;
+    }
+  }
+  for (int nuc = 0; nuc < M; nuc++) {
+    int fud = s->tb_pair[3 * nuc], fuu = s->tb_pair[3 * nuc + 1], fdd = s->tb_pair[3 * nuc + 2];
+    if (na > 0 && nb > 0) {
+      if (isAlpha)
+        for (int EB = na; EB < N; EB++) tb_collect(s, w, fud, EB, E, nuc);
+      else
+        for (int EA = 0; EA < na; EA++) tb_collect(s, w, fud, E, EA, nuc);
+    }
+    if (na > 1 && isAlpha) {
+      for (int EA = 0; EA < E; EA++) tb_collect(s, w, fuu, E, EA, nuc);
+      for (int EA = E + 1; EA < na; EA++) tb_collect(s, w, fuu, EA, E, nuc);
+    }
+    if (nb > 1 && !isAlpha) {
+      for (int EB = na; EB < E; EB++) tb_collect(s, w, fdd, E, EB, nuc);
+      for (int EB = E + 1; EB < N; EB++) tb_collect(s, w, fdd, EB, E, nuc);
+    }
+  }
+  for (int E2 = 0; E2 < N; E2++) {
+    if (E == E2) continue;
+    int EH = E > E2 ? E : E2, EL = E < E2 ? E : E2;
+    w->U += w->tU[EH * N + EL];
+    w->U_xx += w->tUxx[EH * N + EL];
+    for (int x = 0; x < 3; x++) {
+      w->U_x[EH * 3 + x] += w->tUx1[(EH * N + EL) * 3 + x];
+      w->U_x[EL * 3 + x] += w->tUx2[(EH * N + EL) * 3 + x];
+    }
+  }
+}
+
 /* -------------------------------------------------------- potential (a7) */
 /* QMCPotential_Energy::evaluate / calc_P_en / calc_P_ee (QMcBeaver/src/QMCPotential_Energy.cpp:242-333) */
 static void potential(const orc_system *s, orc_walker *w)
@@ -1090,6 +1321,7 @@ int orc_evaluate(const orc_system *s, orc_walker **walkers, const double *R, int
     /* QMCJastrow::evaluate: e-n then e-e (QMcBeaver/src/QMCJastrow.cpp:134-151) */
     jastrow_en(s, w, whichE);
     jastrow_ee(s, w, whichE);
+    jastrow_3b(s, w, whichE);
     slater_spin(s, w, 0, Rw, whichE);
     slater_spin(s, w, 1, Rw, whichE);
     potential(s, w);

@@ -167,4 +167,27 @@ void ref_cusp_params(int beta, int atom, int orbital, double *out)
   for (int i = 0; i < 5 && i < c.dim1(); i++) out[3 + i] = c(i);
 }
 
+// The reference's three-body coefficients for nucleus type j (in its
+// NucleiTypes order) and pair kind (0 up-down, 1 up-up, 2 down-down):
+// out = [NeN, Nee, C, cutoff, used, coefficients...]; returns the count
+// written (0 when the kind has no function).
+int ref_three_body(int kind, int j, double *out, int cap)
+{
+  QMCJastrowParameters &JP = globalInput.JP;
+  Array1D<QMCThreeBodyCorrelationFunctionParameters> &A =
+      kind == 0 ? JP.EupEdnNuclear : (kind == 1 ? JP.EupEupNuclear : JP.EdnEdnNuclear);
+  if (j >= A.dim1()) return 0;
+  QMCThreeBodyCorrelationFunctionParameters &P = A(j);
+  if (!P.isUsed()) return 0;
+  int T = P.Parameters.dim1();
+  if (5 + T > cap) return -1;
+  out[0] = P.NeN;
+  out[1] = P.Nee;
+  out[2] = P.C;
+  out[3] = P.cutoff;
+  out[4] = 1.0;
+  for (int i = 0; i < T; i++) out[5 + i] = P.Parameters(i);
+  return 5 + T;
+}
+
 } // extern "C"

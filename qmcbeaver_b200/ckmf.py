@@ -33,6 +33,7 @@ import numpy as np
 
 from . import desc as D
 from .system import BasisFunction, Cambridge2, MolecularSystem, Pade
+from .threebody import ThreeBody
 
 
 class CkmfError(ValueError):
@@ -136,6 +137,30 @@ class CorrelationBlock:
 
 
 @dataclasses.dataclass
+class ThreeBodyBlock:
+    """One three-body block (QMCThreeBodyCorrelationFunctionParameters::read,
+    QMcBeaver/src/QMCThreeBodyCorrelationFunctionParameters.cpp:48-277)."""
+    nucleus: str
+    p2: str
+    p3: str
+    kind: str
+    nen: int
+    nee: int
+    params: List[float]
+    C: int
+    cutoff: float
+
+    def function(self, rep_ne: bool, rep_ee: bool) -> Optional[ThreeBody]:
+        if self.kind == "None":
+            return None
+        if self.kind != "Cambridge":
+            raise CkmfError(f"three-body function type {self.kind!r} is not supported")
+        if self.nen < 3 or self.nee < 3:
+            raise CkmfError("three-body functions need NeN, Nee >= 3")
+        return ThreeBody.from_input(self.params, self.nen, self.nee, self.C, self.cutoff, rep_ne, rep_ee)
+
+
+@dataclasses.dataclass
 class CkmfInput:
     flags: Dict[str, str]
     labels: List[str]
@@ -147,8 +172,13 @@ class CkmfInput:
     beta_occupation: np.ndarray
     ci_coeffs: np.ndarray
     jastrow: List[CorrelationBlock]
-    three_body_blocks: int
+    three_body: List[ThreeBodyBlock]
     path: str = ""
+
+    @property
+    def three_body_blocks(self) -> int:
+        """Three-body blocks in use (type other than None)."""
+        return sum(1 for b in self.three_body if b.kind != "None")
 
     # ------------------------------------------------------------- flags
     def flag(self, key: str, default=None, kind=str):
@@ -170,21 +200,19 @@ class CkmfInput:
         return int(self.beta_occupation[0].sum())
 
     # ------------------------------------------------------------ system
-    def to_system(self, replace_cusps: Optional[bool] = None, allow_three_body: bool = False,
+    def to_system(self, replace_cusps: Optional[bool] = None, three_body: Optional[bool] = None,
                   name: Optional[str] = None) -> MolecularSystem:
         """The Slater-Jastrow system of this input (one or several determinants).
 
         replace_cusps: None follows ``replace_electron_nucleus_cusps`` (on by
-        default in the reference); True / False overrides it.  Three-body
-        Jastrow blocks are refused unless allow_three_body drops them."""
+        default in the reference); True / False overrides it.  three_body:
+        None / True evaluates the input's three-body blocks (the reference
+        evaluates every block present, whatever use_three_body_jastrow says),
+        False leaves them out."""
         if self.flag("trial_function_type", "restricted") not in ("restricted", "unrestricted"):
             raise CkmfError("only restricted / unrestricted trial functions are read")
         if replace_cusps is None:
             replace_cusps = self.flag("replace_electron_nucleus_cusps", 1, int) == 1
-        # the reference evaluates every used three-body block in the file,
-        # whatever use_three_body_jastrow says
-        if self.three_body_blocks and not allow_three_body:
-            raise CkmfError("three-body Jastrow blocks present; pass allow_three_body=True to drop them")
         na, nb = self.n_alpha, self.n_beta
         if nb > na:
             raise CkmfError("more beta than alpha electrons")
@@ -232,12 +260,44 @@ class CkmfInput:
                 en_dn = dict(en_up)
         en_up = {k: v for k, v in en_up.items() if v is not None}
         en_dn = {k: v for k, v in en_dn.items() if v is not None}
+        tb = self._three_body(types, na, nb) if three_body is not False else {}
         return MolecularSystem(
             labels=list(self.labels), Z=np.asarray(self.Z, float), coords=np.asarray(self.coords, float),
             basis=self.basis, mo=np.asarray(self.orbitals, float), n_alpha=na, n_beta=nb,
             alpha_occ=a_occ, beta_occ=b_occ, ee_anti=ee_anti, ee_para_up=ee_up, ee_para_dn=ee_dn,
             en_up=en_up, en_dn=en_dn, name=name or self.path, det_alpha=det_a, det_beta=det_b, ci_coeffs=ci,
-            replace_cusps=bool(replace_cusps))
+            replace_cusps=bool(replace_cusps), three_body=tb)
+
+    def _three_body(self, types: List[str], na: int, nb: int) -> Dict[str, tuple]:
+        """Per nucleus type (up-down, up-up, down-down) three-body functions,
+        linked as link_NEE_Jastrows says (default 2: every pair kind takes the
+        up-down function) (QMcBeaver/src/QMCJastrowParameters.cpp:911-1066)."""
+        rep_ne = self.flag("reproduce_NE_with_NEE_jastrow", 0, int) == 1
+        rep_ee = self.flag("reproduce_EE_with_NEE_jastrow", 0, int) == 1
+        link = self.flag("link_NEE_Jastrows", 2, int)
+        tb = {l: [None, None, None] for l in types}
+        for b in self.three_body:
+            if b.nucleus not in tb:
+                continue
+            f = b.function(rep_ne, rep_ee)
+            if b.p2 == "Electron_up" and b.p3 == "Electron_down":
+                tb[b.nucleus][0] = f
+            elif b.p2 == "Electron_up" and b.p3 == "Electron_up":
+                if na < 2:
+                    raise CkmfError("Electron_up-Electron_up three-body block with fewer than two up electrons")
+                tb[b.nucleus][1] = f
+            elif b.p2 == "Electron_down" and b.p3 == "Electron_down":
+                if nb < 2:
+                    raise CkmfError("Electron_down-Electron_down three-body block with fewer than two down electrons")
+                tb[b.nucleus][2] = f
+        if na > 1 and nb > 1:
+            for l in types:
+                if link == 1:
+                    tb[l][2] = tb[l][1]
+                elif link == 2:
+                    tb[l][1] = tb[l][0]
+                    tb[l][2] = tb[l][0]
+        return {l: tuple(v) for l, v in tb.items() if any(x is not None for x in v)}
 
     def run_params(self, **overrides) -> D.RunParams:
         """The library's run parameters for this input's flags
@@ -392,7 +452,6 @@ def _read_jastrow(t: _Tokens):
     blocks: List[CorrelationBlock] = []
     if not t.seek("&Jastrow"):
         raise CkmfError("no &Jastrow section")
-    three = 0
     while t.peek() == "ParticleTypes:":
         start = t.i
         t.next()
@@ -427,12 +486,26 @@ def _read_jastrow(t: _Tokens):
         else:
             raise CkmfError(f"two non-electron particles ({p1}, {p2}) in one correlation function")
         blocks.append(CorrelationBlock(a, b, kind, nparams, params, nconsts, consts))
-    # count the used three-body blocks up to the closing marker
-    j = t.i
-    while j + 1 < len(t.tok) and t.tok[j][0] != "&Jastrow":
-        if t.tok[j][0] == "threeBodyCorrelationFunctionType:" and t.tok[j + 1][0] != "None":
-            three += 1
-        j += 1
+    three: List[ThreeBodyBlock] = []
+    while t.peek() == "ParticleTypes:":
+        t.next()
+        p1, p2, p3 = first_upper(t.next()), first_upper(t.next()), first_upper(t.next())
+        if t.next() != "threeBodyCorrelationFunctionType:":
+            raise CkmfError(f"({p1},{p2},{p3}): expected a three-body block")
+        kind = t.next()
+        t.next()
+        npt = int(t.next())
+        if npt != 2:
+            raise CkmfError("three-body blocks have two parameter types (NeN, Nee)")
+        t.next()
+        nen, nee = int(t.next()), int(t.next())
+        t.next()
+        params = t.numbers()
+        t.next()
+        C = int(float(t.next()))
+        t.next()
+        cutoff = float(t.next())
+        three.append(ThreeBodyBlock(p1, p2, p3, kind, nen, nee, params, C, cutoff))
     return blocks, three
 
 
@@ -461,7 +534,7 @@ def read_ckmf(path: str, text: Optional[str] = None) -> CkmfInput:
     jas, three = _read_jastrow(_Tokens(text))
     return CkmfInput(flags=flags, labels=labels, Z=Z, coords=xyz, basis=basis, orbitals=orb,
                      alpha_occupation=aocc, beta_occupation=bocc, ci_coeffs=ci, jastrow=jas,
-                     three_body_blocks=three, path=path)
+                     three_body=three, path=path)
 
 
 def patch_flags(text: str, updates: Dict[str, object]) -> str:

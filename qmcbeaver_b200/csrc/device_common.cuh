@@ -48,6 +48,7 @@ enum Sc {
 constexpr int kScalars = 24;  // padded
 
 constexpr int kShellPrim = 6;  // primitives kept in registers per shell
+constexpr int kTbMax = 8;      // largest NeN / Nee of a three-body function
 
 struct DevSys {
   int M, na, nb, N, K, npade, nshell;
@@ -63,6 +64,12 @@ struct DevSys {
   const double *cscoef[2];  // [M][nact][nsmax] primitive coefficient x orbital coefficient
   const double *cpar[2];    // [M][nact][8] rc, sgn0, C, alpha_0..alpha_4
   const double *crmax[2];   // [M] largest rc of the spin's orbitals at the nucleus
+  // three-body (e-e-n) Jastrow (ntb = 0: none)
+  int ntb;
+  const int4 *tbi;       // [ntb] NeN, Nee, C, coefficient offset
+  const double *tbL;     // [ntb] L (inverse cutoff)
+  const double *tbc;     // coefficients
+  const int *tbp;        // [M][3] function of up-down, up-up, down-down pairs
   int ee[3];
   double Pnn;
   const double4 *nuc;    // [M] x, y, z, Z
@@ -316,6 +323,170 @@ __device__ __forceinline__ void pade_eval(const DevSys &S, int f, double r, doub
   u = aDIVb;
   du = apDIVb - bpDIVb * aDIVb;
   d2u = (app - bpp * aDIVb) * ib - 2.0 * bpDIVb * du;
+}
+
+// ------------------------------------------------------------ three-body
+// One Cambridge three-body term (CambridgeThreeBodyCorrelationFunction::
+// setElectron / evaluate / getLapPoly, QMcBeaver/src/CambridgeThreeBodyCorrelationFunction.cpp:
+// 150-470) of the electron pair (first, second) around one nucleus: d1, d2 the
+// electrons' offsets from the nucleus, d12 = first - second.  Returns false
+// (and zeros) outside the cutoff.  g1 / g2: gradients on the two electrons,
+// lap: the sum of both laplacians.
+__device__ inline bool tb_term(const DevSys &S, int f, const double d1[3], const double d2[3], const double d12[3],
+                               double &U, double &lap, double g1[3], double g2[3])
+{
+  const int4 info = S.tbi[f];
+  const int Nen = info.x, Nee = info.y, C = info.z;
+  double L = S.tbL[f];
+  if (fabs(L) < 1e-10) L = 1.0e10;
+  const double a1 = sqrt(d1[0] * d1[0] + d1[1] * d1[1] + d1[2] * d1[2]);
+  const double a2 = sqrt(d2[0] * d2[0] + d2[1] * d2[1] + d2[2] * d2[2]);
+  const double r1 = a1 * L, r2 = a2 * L, e1 = r1 - 1.0, e2 = r2 - 1.0;
+  U = lap = 0.0;
+  g1[0] = g1[1] = g1[2] = g2[0] = g2[1] = g2[2] = 0.0;
+  if (e1 > 0.0 || e2 > 0.0) return false;
+  const double a12 = sqrt(d12[0] * d12[0] + d12[1] * d12[1] + d12[2] * d12[2]);
+  const double r12 = a12 * L;
+  double p1 = 1.0, p2 = 1.0;
+  for (int i = 0; i < C; i++) {
+    p1 *= e1;
+    p2 *= e2;
+  }
+  const double dp1 = p1 * C / e1, ddp1 = (C - 1.0) * dp1 / e1;
+  const double dp2 = p2 * C / e2, ddp2 = (C - 1.0) * dp2 / e2;
+  double x1[kTbMax], x2[kTbMax], x12[kTbMax];
+  x1[0] = x2[0] = x12[0] = 1.0;
+  for (int i = 1; i < Nen; i++) {
+    x1[i] = x1[i - 1] * r1;
+    x2[i] = x2[i - 1] * r2;
+  }
+  for (int i = 1; i < Nee; i++) x12[i] = x12[i - 1] * r12;
+  // polynomial sums: value, d/dr1, d/dr2, d/dr12 and the second derivatives
+  double P = 0, Pl = 0, Pm = 0, Pn = 0, Pll = 0, Pmm = 0, Pnn = 0, Pln = 0, Pmn = 0;
+  const double *c = S.tbc + info.w;
+  for (int l = 0; l < Nen; l++) {
+    const double xl = x1[l], xl1 = l > 0 ? l * x1[l - 1] : 0.0, xl2 = l > 1 ? l * (l - 1.0) * x1[l - 2] : 0.0;
+    for (int m = 0; m < Nen; m++) {
+      const double xm = x2[m], xm1 = m > 0 ? m * x2[m - 1] : 0.0, xm2 = m > 1 ? m * (m - 1.0) * x2[m - 2] : 0.0;
+      const double lm = xl * xm, dlm = xl1 * xm, ldm = xl * xm1;
+      double s0 = 0, s1 = 0, s2 = 0;  // sum c x12^n, sum c n x12^(n-1), sum c n(n-1) x12^(n-2)
+      for (int n = 0; n < Nee; n++) {
+        const double cc = __ldg(&c[(l * Nen + m) * Nee + n]);
+        s0 = fma(cc, x12[n], s0);
+        if (n > 0) s1 = fma(cc * n, x12[n - 1], s1);
+        if (n > 1) s2 = fma(cc * (n * (n - 1.0)), x12[n - 2], s2);
+      }
+      P = fma(lm, s0, P);
+      Pl = fma(dlm, s0, Pl);
+      Pm = fma(ldm, s0, Pm);
+      Pn = fma(lm, s1, Pn);
+      Pln = fma(dlm, s1, Pln);
+      Pmn = fma(ldm, s1, Pmn);
+      Pll = fma(xl2 * xm, s0, Pll);
+      Pmm = fma(xl * xm2, s0, Pmm);
+      Pnn = fma(lm, s2, Pnn);
+    }
+  }
+  U = p1 * p2 * P;
+  const double dU12 = p1 * p2 * Pn;
+  const double dU1 = (dp1 * P + p1 * Pl) * p2;
+  const double dU2 = (dp2 * P + p2 * Pm) * p1;
+  const double i1 = 1.0 / a1, i2 = 1.0 / a2, i12 = 1.0 / a12;
+  double dot = 0.0;
+  for (int k = 0; k < 3; k++) {
+    const double u1 = d1[k] * i1, u2 = d2[k] * i2, u12 = d12[k] * i12;
+    g1[k] = L * (dU1 * u1 + dU12 * u12);
+    g2[k] = L * (dU2 * u2 - dU12 * u12);
+    dot += u12 * (u1 * (2.0 * p2 * (dp1 * Pn + p1 * Pln)) - u2 * (2.0 * p1 * (dp2 * Pn + p2 * Pmn)));
+  }
+  double lp = 2.0 * (2.0 * dU12 / r12 + dU1 / r1 + dU2 / r2);
+  lp += 2.0 * (p1 * p2 * Pnn) + p2 * (ddp1 * P + 2.0 * dp1 * Pl + p1 * Pll) + p1 * (ddp2 * P + 2.0 * dp2 * Pm + p2 * Pmm);
+  lap = (lp + dot) * L * L;
+  return true;
+}
+
+// Three-body function of the pair (i, j) around nucleus A (-1: none).
+__device__ __forceinline__ int tb_func(const DevSys &S, int A, int i, int j)
+{
+  const bool ai = i < S.na, aj = j < S.na;
+  return S.tbp[3 * A + (ai != aj ? 0 : (ai ? 1 : 2))];
+}
+
+// Three-body changes when electron e moves from ro to rn, for the partners j
+// of this lane (j = lane + 32 k): U, laplacian and the gradient on e are
+// added to the lane's partial sums, U_x[j] is updated in place
+// (QMCThreeBodyJastrow::updateOne, QMcBeaver/src/QMCThreeBodyJastrow.cpp:43-178).
+__device__ __noinline__ void tb_move_lane(const DevSys &S, const double *R, double *Ux, int e, const double *ro,
+                                          const double *rn, double *acc)
+{
+  const int N = S.N;
+  for (int j = threadIdx.x & 31; j < N; j += 32) {
+    if (j == e) continue;
+    const double *rj = R + 3 * j;
+    const bool e_first = e > j;
+    for (int A = 0; A < S.M; A++) {
+      const int f = tb_func(S, A, e, j);
+      if (f < 0) continue;
+      const double4 P = S.nuc[A];
+      const double dj[3] = {rj[0] - P.x, rj[1] - P.y, rj[2] - P.z};
+      double Uo, Lo, go1[3], go2[3], Un, Ln, gn1[3], gn2[3];
+      {
+        const double de[3] = {ro[0] - P.x, ro[1] - P.y, ro[2] - P.z};
+        const double d12[3] = {e_first ? ro[0] - rj[0] : rj[0] - ro[0], e_first ? ro[1] - rj[1] : rj[1] - ro[1],
+                               e_first ? ro[2] - rj[2] : rj[2] - ro[2]};
+        tb_term(S, f, e_first ? de : dj, e_first ? dj : de, d12, Uo, Lo, go1, go2);
+      }
+      {
+        const double de[3] = {rn[0] - P.x, rn[1] - P.y, rn[2] - P.z};
+        const double d12[3] = {e_first ? rn[0] - rj[0] : rj[0] - rn[0], e_first ? rn[1] - rj[1] : rj[1] - rn[1],
+                               e_first ? rn[2] - rj[2] : rj[2] - rn[2]};
+        tb_term(S, f, e_first ? de : dj, e_first ? dj : de, d12, Un, Ln, gn1, gn2);
+      }
+      acc[0] += Un - Uo;
+      acc[1] += Ln - Lo;
+      for (int k = 0; k < 3; k++) {
+        const double ge = e_first ? gn1[k] - go1[k] : gn2[k] - go2[k];
+        const double gj = e_first ? gn2[k] - go2[k] : gn1[k] - go1[k];
+        acc[2 + k] += ge;
+        Ux[3 * j + k] += gj;
+      }
+    }
+  }
+}
+
+// Three-body U, laplacian and gradients of all electrons from scratch
+// (QMCThreeBodyJastrow::updateAll, QMcBeaver/src/QMCThreeBodyJastrow.cpp:320-401):
+// lane i sums the gradient on its electron over every partner; U and the
+// laplacian count each pair once (on its higher electron).
+__device__ __noinline__ void tb_full_lane(const DevSys &S, const double *R, double *ux, double *acc)
+{
+  const int N = S.N;
+  for (int i = threadIdx.x & 31; i < N; i += 32) {
+    const double *ri = R + 3 * i;
+    double g[3] = {0, 0, 0};
+    for (int j = 0; j < N; j++) {
+      if (j == i) continue;
+      const double *rj = R + 3 * j;
+      const bool i_first = i > j;
+      for (int A = 0; A < S.M; A++) {
+        const int f = tb_func(S, A, i, j);
+        if (f < 0) continue;
+        const double4 P = S.nuc[A];
+        const double di[3] = {ri[0] - P.x, ri[1] - P.y, ri[2] - P.z};
+        const double dj[3] = {rj[0] - P.x, rj[1] - P.y, rj[2] - P.z};
+        const double d12[3] = {i_first ? ri[0] - rj[0] : rj[0] - ri[0], i_first ? ri[1] - rj[1] : rj[1] - ri[1],
+                               i_first ? ri[2] - rj[2] : rj[2] - ri[2]};
+        double U, Lp, g1[3], g2[3];
+        if (!tb_term(S, f, i_first ? di : dj, i_first ? dj : di, d12, U, Lp, g1, g2)) continue;
+        for (int k = 0; k < 3; k++) g[k] += i_first ? g1[k] : g2[k];
+        if (i_first) {
+          acc[0] += U;
+          acc[1] += Lp;
+        }
+      }
+    }
+    for (int k = 0; k < 3; k++) ux[3 * i + k] += g[k];
+  }
 }
 
 // e-e correlation function index for electrons i, j

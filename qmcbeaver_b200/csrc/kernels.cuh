@@ -270,6 +270,12 @@ __device__ inline void jastrow_pe_full_warp(const DevSys &S, const double *R, do
     ux[3 * i + 1] = gy;
     ux[3 * i + 2] = gz;
   }
+  if (S.ntb > 0) {
+    double acc[2] = {0.0, 0.0};
+    tb_full_lane(S, R, ux, acc);
+    pu += acc[0];
+    pxx += acc[1];
+  }
   U = warp_sum(pu);
   Uxx = warp_sum(pxx);
   Vee = warp_sum(pee);
@@ -568,6 +574,15 @@ __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR
       ge[1] += sn * dyn - so * dyo;
       ge[2] += sn * dzn - so * dzo;
     }
+  }
+  if (S.ntb > 0) {
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    tb_move_lane(S, sR, Ux, e, ro, rn, acc);
+    dU += acc[0];
+    dUxx += acc[1];
+    ge[0] += acc[2];
+    ge[1] += acc[3];
+    ge[2] += acc[4];
   }
   dU = warp_sum(dU);
   dUxx = warp_sum(dUxx);

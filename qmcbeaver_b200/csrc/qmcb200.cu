@@ -64,6 +64,9 @@ struct qmcb_handle {
   int *d_cns = nullptr;
   double *d_csexp = nullptr, *d_cscoef[2] = {nullptr, nullptr}, *d_cpar[2] = {nullptr, nullptr};
   double *d_crmax[2] = {nullptr, nullptr};
+  int4 *d_tbi = nullptr;
+  double *d_tbL = nullptr, *d_tbc = nullptr;
+  int *d_tbp = nullptr;
   double *d_ci = nullptr;
   bool md = false;  // several determinants: the k_*_md kernels
   double *d_state = nullptr;
@@ -485,6 +488,36 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   }
   if (md)
     for (int c = 0; c < d->n_det; c++) ci[c] = d->ci_coeff[c];
+  // three-body Jastrow tables
+  const int ntb = d->n_tb > 0 ? d->n_tb : 0;
+  std::vector<int4> tbi(std::max(ntb, 1), make_int4(0, 0, 0, 0));
+  std::vector<double> tbL(std::max(ntb, 1), 0.0), tbc(1, 0.0);
+  std::vector<int> tbp((size_t)3 * M, -1);
+  if (ntb > 0) {
+    if (!d->tb_nen || !d->tb_nee || !d->tb_C || !d->tb_cutoff || !d->tb_offset || !d->tb_coeff || !d->tb_pair) {
+      delete h;
+      return fail(nullptr, QMCB_E_ARG, "qmcb_create: incomplete three-body tables");
+    }
+    size_t ncoef = 0;
+    for (int f = 0; f < ntb; f++) {
+      const int nen = d->tb_nen[f], nee = d->tb_nee[f];
+      if (nen < 1 || nee < 1 || nen > kTbMax || nee > kTbMax || d->tb_C[f] < 0 || d->tb_C[f] > 16 || d->tb_offset[f] < 0) {
+        delete h;
+        return fail(nullptr, QMCB_E_ARG, "qmcb_create: three-body sizes out of range (NeN, Nee <= 8, C <= 16)");
+      }
+      tbi[f] = make_int4(nen, nee, d->tb_C[f], d->tb_offset[f]);
+      tbL[f] = d->tb_cutoff[f];
+      ncoef = std::max(ncoef, (size_t)d->tb_offset[f] + (size_t)nen * nen * nee);
+    }
+    tbc.assign(d->tb_coeff, d->tb_coeff + ncoef);
+    for (int t = 0; t < 3 * M; t++) {
+      tbp[t] = d->tb_pair[t];
+      if (tbp[t] >= ntb) {
+        delete h;
+        return fail(nullptr, QMCB_E_ARG, "qmcb_create: three-body function index out of range");
+      }
+    }
+  }
   // electron-nucleus cusp replacement tables
   std::vector<int> cns(M, 0);
   int nsmax = 1;
@@ -645,6 +678,10 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(upload(&h->d_dswap[0], dswap[0]));
   CKC(upload(&h->d_dswap[1], dswap[1]));
   CKC(upload(&h->d_ci, ci));
+  CKC(upload(&h->d_tbi, tbi));
+  CKC(upload(&h->d_tbL, tbL));
+  CKC(upload(&h->d_tbc, tbc));
+  CKC(upload(&h->d_tbp, tbp));
   CKC(upload(&h->d_cns, cns));
   CKC(upload(&h->d_csexp, csexp));
   for (int sp = 0; sp < 2; sp++) {
@@ -690,6 +727,11 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   S.docc[1] = h->d_docc[1];
   S.dswap[0] = h->d_dswap[0];
   S.dswap[1] = h->d_dswap[1];
+  S.ntb = ntb;
+  S.tbi = h->d_tbi;
+  S.tbL = h->d_tbL;
+  S.tbc = h->d_tbc;
+  S.tbp = h->d_tbp;
   S.cusp = d->replace_cusps ? 1 : 0;
   S.nsmax = nsmax;
   S.cns = h->d_cns;
@@ -806,7 +848,7 @@ int qmcb_destroy(qmcb_handle *h)
 {
   if (!h) return QMCB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void *ptrs[] = {h->d_cns, h->d_csexp, h->d_cscoef[0], h->d_cscoef[1], h->d_cpar[0], h->d_cpar[1], h->d_crmax[0],
+  void *ptrs[] = {h->d_tbi, h->d_tbL, h->d_tbc, h->d_tbp, h->d_cns, h->d_csexp, h->d_cscoef[0], h->d_cscoef[1], h->d_cpar[0], h->d_cpar[1], h->d_crmax[0],
                   h->d_crmax[1], h->d_docc[0], h->d_docc[1], h->d_dswap[0], h->d_dswap[1], h->d_ci, h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
                   h->d_copies, h->d_stats, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};

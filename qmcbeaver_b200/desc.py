@@ -35,6 +35,8 @@ class SystemDesc(C.Structure):
         ("n_det", C.c_int), ("n_act_alpha", C.c_int), ("n_act_beta", C.c_int),
         ("det_occ_alpha", _ip), ("det_occ_beta", _ip), ("ci_coeff", _dp),
         ("replace_cusps", C.c_int), ("cusp_alpha", _dp), ("cusp_beta", _dp),
+        ("n_tb", C.c_int), ("tb_nen", _ip), ("tb_nee", _ip), ("tb_C", _ip), ("tb_cutoff", _dp),
+        ("tb_offset", _ip), ("tb_coeff", _dp), ("tb_pair", _ip),
     ]
 
 
@@ -156,6 +158,16 @@ class PackedSystem:
         d.det_occ_beta = _i(k["occ_b"])
         d.ci_coeff = _d(k["ci"])
         d.replace_cusps = 1 if s.replace_cusps else 0
+        tb = s.three_body_tables()
+        self._keep.update({"tb_" + k: v for k, v in tb.items()})
+        d.n_tb = int(len(tb["nen"])) if tb["used"] else 0
+        d.tb_nen = _i(self._keep["tb_nen"])
+        d.tb_nee = _i(self._keep["tb_nee"])
+        d.tb_C = _i(self._keep["tb_C"])
+        d.tb_cutoff = _d(self._keep["tb_cutoff"])
+        d.tb_offset = _i(self._keep["tb_offset"])
+        d.tb_coeff = _d(self._keep["tb_coeff"])
+        d.tb_pair = _i(self._keep["tb_pair"])
         self.desc = d
 
     def set_cusp_tables(self, alpha: np.ndarray, beta: np.ndarray) -> None:

@@ -183,6 +183,8 @@ class MolecularSystem:
     ci_coeffs: Optional[np.ndarray] = None  # (n_det,)
     # electron-nucleus cusp replacement of the orbitals (replace_electron_nucleus_cusps)
     replace_cusps: bool = False
+    # three-body (e-e-n) Jastrow per nucleus label: (up-down, up-up, down-down)
+    three_body: Dict[str, tuple] = dataclasses.field(default_factory=dict)
 
     # ------------------------------------------------------------------ sizes
     @property
@@ -240,6 +242,32 @@ class MolecularSystem:
 
     def mo_beta(self) -> np.ndarray:
         return np.ascontiguousarray(self.mo[self.active_orbitals(True)])
+
+    def three_body_tables(self) -> Dict[str, np.ndarray]:
+        """Three-body function tables for the descriptor: distinct functions
+        with their NeN, Nee, C, cutoff and coefficient offsets, and per nucleus
+        (geometry order) the function of each pair kind (-1: none)."""
+        funcs: List[object] = []
+        pair = np.full((max(self.n_nuclei, 1), 3), -1, np.int32)
+        for a, l in enumerate(self.labels):
+            for kind, f in enumerate(self.three_body.get(l, (None, None, None))):
+                if f is None:
+                    continue
+                for i, g in enumerate(funcs):
+                    if g is f:
+                        pair[a, kind] = i
+                        break
+                else:
+                    funcs.append(f)
+                    pair[a, kind] = len(funcs) - 1
+        nen = np.array([f.nen for f in funcs] or [0], np.int32)
+        nee = np.array([f.nee for f in funcs] or [0], np.int32)
+        Cs = np.array([f.C for f in funcs] or [0], np.int32)
+        cut = np.array([f.cutoff for f in funcs] or [0.0], np.float64)
+        off = np.cumsum([0] + [len(f.coeffs) for f in funcs])[:-1].astype(np.int32) if funcs else np.zeros(1, np.int32)
+        coef = np.concatenate([np.asarray(f.coeffs, np.float64) for f in funcs]) if funcs else np.zeros(1)
+        return dict(used=bool(funcs), nen=nen, nee=nee, C=Cs, cutoff=cut, offset=off,
+                    coeff=np.ascontiguousarray(coef), pair=np.ascontiguousarray(pair.reshape(-1)))
 
     def pade_tables(self):
         """Correlation-function table + indices: ee[3] = (anti, up-up, dn-dn),
@@ -350,6 +378,12 @@ class MolecularSystem:
         f.update({
             "link_Jastrow_parameters": 1 if linked else 0,
             "replace_electron_nucleus_cusps": 1 if self.replace_cusps else 0,
+            # three-body blocks are written per pair kind with coefficients
+            # that already satisfy the Gaussian-elimination constraints
+            "use_three_body_jastrow": 1 if self.three_body else 0,
+            "link_NEE_Jastrows": 0,
+            "reproduce_NE_with_NEE_jastrow": 1,
+            "reproduce_EE_with_NEE_jastrow": 1,
             "atoms": self.n_nuclei,
             "charge": self.charge,
             "norbitals": self.mo.shape[0],
@@ -437,6 +471,22 @@ class MolecularSystem:
                 block("Electron_up", l, self.en_up[l])
             if l in self.en_dn and self.n_beta > 0:
                 block("Electron_down", l, self.en_dn[l])
+        kinds = (("Electron_up", "Electron_down"), ("Electron_up", "Electron_up"), ("Electron_down", "Electron_down"))
+        for l in dict.fromkeys(self.labels):
+            for (p2, p3), tb in zip(kinds, self.three_body.get(l, (None, None, None))):
+                if tb is None or (p2 == p3 == "Electron_up" and self.n_alpha < 2) or \
+                        (p2 == p3 == "Electron_down" and self.n_beta < 2) or \
+                        (p2 != p3 and (self.n_alpha < 1 or self.n_beta < 1)):
+                    continue
+                out.append(f"ParticleTypes: {l} {p2} {p3}")
+                out.append("threeBodyCorrelationFunctionType: Cambridge")
+                out.append("NumberOfParameterTypes: 2")
+                out.append(f"NumberOfParametersOfEachType: {tb.nen} {tb.nee}")
+                out.append("Parameters:")
+                out.append(" ".join(g % v for v in tb.input_parameters()))
+                out.append(f"C: {tb.C}")
+                out.append(f"Cutoff: {g % tb.cutoff}")
+                out.append("")
         out.append("&Jastrow")
         out.append("")
         with open(path, "w") as fh:
@@ -697,6 +747,26 @@ def with_cambridge2(s: MolecularSystem, seed: int = 1) -> MolecularSystem:
                                en_up=en_up, en_dn=en_dn, name=s.name + " cambridge2")
 
 
+def with_three_body(s: MolecularSystem, seed: int = 1, nen: int = 4, nee: int = 4, scale: float = 0.5,
+                    separate_kinds: bool = True) -> MolecularSystem:
+    """The same molecule with Cambridge three-body functions on every nucleus
+    type, of the reference inputs' shape (QMcBeaver/test/oepi.ckmf: NeN =
+    Nee = 4, C = 3, cutoff L so that each reaches 2.5 to 4 bohr); with
+    separate_kinds the up-up and down-down pairs get their own functions."""
+    from .threebody import random_three_body
+    rng = np.random.default_rng(seed)
+    tb = {}
+    for l in dict.fromkeys(s.labels):
+        ud = random_three_body(rng, nen, nee, 3, float(rng.uniform(0.25, 0.4)), scale)
+        if separate_kinds:
+            uu = random_three_body(rng, nen, nee, 3, float(rng.uniform(0.25, 0.4)), scale)
+            dd = random_three_body(rng, nen, nee, 2, float(rng.uniform(0.25, 0.4)), scale)
+            tb[l] = (ud, uu, dd)
+        else:
+            tb[l] = (ud, ud, ud)
+    return dataclasses.replace(s, three_body=tb, name=s.name + " three-body")
+
+
 def with_determinants(s: MolecularSystem, n_det: int = 9, n_virtual: int = 4, seed: int = 1,
                       ci_scale: float = 0.3) -> MolecularSystem:
     """The same molecule with a CI expansion over the lowest
@@ -797,6 +867,10 @@ WORKLOADS = {
     "vmc_cambridge2_16e": dict(kind="random", n_elec=16, n_nuclei=4, n_basis=64, box=5.0, z=(1, 6, 7, 8),
                                walkers=4096, run="vmc", dt=0.01, importance=True, refresh=50,
                                correlation="cambridge2"),
+    # Cambridge2 two-body and Cambridge three-body Jastrow (the reference's test inputs' form)
+    "vmc_threebody_16e": dict(kind="random", n_elec=16, n_nuclei=4, n_basis=64, box=5.0, z=(1, 6, 7, 8),
+                              walkers=4096, run="vmc", dt=0.01, importance=True, refresh=50,
+                              correlation="cambridge2", three_body=True),
     # twelve determinants (singles and doubles into four virtual orbitals)
     "vmc_multidet_12e": dict(kind="random", n_elec=12, n_nuclei=3, n_basis=48, box=4.5, z=(1, 6, 7, 8),
                              walkers=4096, run="vmc", dt=0.01, importance=True, refresh=50,
@@ -812,6 +886,9 @@ def make_system(workload: str, seed: int = 1, jastrow: bool = True) -> Molecular
                              jastrow=jastrow, name=workload)
     if jastrow and w.get("correlation") == "cambridge2":
         s = with_cambridge2(s, seed=seed + 1)
+        s.name = workload
+    if jastrow and w.get("three_body"):
+        s = with_three_body(s, seed=seed + 3)
         s.name = workload
     if "determinants" in w:
         nd, nv = w["determinants"]
@@ -856,8 +933,41 @@ def system_to_arrays(s: MolecularSystem) -> Dict[str, np.ndarray]:
         en_up=np.stack([pade_arr(s.en_up.get(l)) for l in s.labels]),
         en_dn=np.stack([pade_arr(s.en_dn.get(l)) for l in s.labels]),
         name=np.array(s.name), replace_cusps=np.array(1 if s.replace_cusps else 0),
+        three_body=_three_body_arr(s),
         **({} if s.det_alpha is None else dict(det_alpha=np.asarray(s.det_alpha), det_beta=np.asarray(s.det_beta),
                                               ci_coeffs=np.asarray(s.ci_coeffs, np.float64))))
+
+
+TB_MAX = 512  # coefficients per serialised three-body function
+
+
+def _three_body_arr(s: MolecularSystem) -> np.ndarray:
+    """[M][3][4 + TB_MAX]: NeN, Nee, C, cutoff, coefficients (NeN = 0: none)."""
+    out = np.zeros((max(s.n_nuclei, 1), 3, 4 + TB_MAX))
+    for a, l in enumerate(s.labels):
+        for k, f in enumerate(s.three_body.get(l, (None, None, None))):
+            if f is not None:
+                out[a, k, :4] = (f.nen, f.nee, f.C, f.cutoff)
+                out[a, k, 4:4 + len(f.coeffs)] = f.coeffs
+    return out
+
+
+def _three_body_of(arr, labels) -> Dict[str, tuple]:
+    from .threebody import ThreeBody
+    out: Dict[str, tuple] = {}
+    for a, l in enumerate(labels):
+        fs = []
+        for k in range(3):
+            nen, nee, C, cut = arr[a, k, :4]
+            if nen == 0:
+                fs.append(None)
+                continue
+            n = int(nen) * int(nen) * int(nee)
+            fs.append(ThreeBody(nen=int(nen), nee=int(nee), C=int(C), cutoff=float(cut),
+                                coeffs=np.array(arr[a, k, 4:4 + n])))
+        if any(f is not None for f in fs):
+            out[l] = tuple(fs)
+    return out
 
 
 def system_from_arrays(d) -> MolecularSystem:
@@ -894,4 +1004,5 @@ def system_from_arrays(d) -> MolecularSystem:
         det_alpha=np.array(d["det_alpha"]) if "det_alpha" in d else None,
         det_beta=np.array(d["det_beta"]) if "det_beta" in d else None,
         ci_coeffs=np.array(d["ci_coeffs"], np.float64) if "ci_coeffs" in d else None,
-        replace_cusps=bool(int(d["replace_cusps"])) if "replace_cusps" in d else False)
+        replace_cusps=bool(int(d["replace_cusps"])) if "replace_cusps" in d else False,
+        three_body=_three_body_of(np.asarray(d["three_body"]), labels) if "three_body" in d else {})

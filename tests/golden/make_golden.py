@@ -35,8 +35,11 @@ CASES = {
     # electron-nucleus cusp replacement, electrons placed inside the
     # replacement radii every third move
     "cusp_dmc30": ("dmc_6nuc_30e", 2, 0.01, 4, 40, 0.15, 7),
+    # Cambridge2 two-body + three-body Jastrow with cusp replacement (the
+    # combination the reference's own test inputs use)
+    "threebody_cusp_vmc": ("vmc_threebody_16e", 2, 0.01, 6, 40, 0.2, 6),
 }
-CUSP_CASES = {"cusp_dmc30"}
+CUSP_CASES = {"cusp_dmc30", "threebody_cusp_vmc"}
 
 
 def run_case(name: str) -> None:

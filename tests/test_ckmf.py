@@ -142,6 +142,10 @@ Constants: 0 2
 ParticleTypes: He Electron_up Electron_down
 threeBodyCorrelationFunctionType: Cambridge
 NumberOfParameterTypes: 2
+NumberOfParametersOfEachType: 3 3
+Parameters: 0 0 0
+C: 3
+Cutoff: 0.4
 &Jastrow
 """
 
@@ -155,9 +159,10 @@ def test_reader_sections_and_function_layouts():
     assert c.labels == ["He"] and c.flag("dt", kind=float) == 0.02
     assert [f.type for f in c.basis[0]] == ["s", "px"]
     assert c.three_body_blocks == 1
-    with pytest.raises(CkmfError, match="three-body"):
-        c.to_system()
-    s = c.to_system(allow_three_body=True)
+    tb = c.to_system().three_body["He"][0]
+    assert (tb.nen, tb.nee, tb.C, tb.cutoff) == (3, 3, 3, 0.4) and not np.any(tb.coeffs)
+    assert not c.to_system(three_body=False).three_body
+    s = c.to_system(three_body=False)
     # Pade: numerator [0, type-0 parameters], denominator [1, the rest]
     assert isinstance(s.ee_anti, Pade)
     assert list(s.ee_anti.num) == [0.0, 0.5, 0.1] and list(s.ee_anti.den) == [1.0, 2.0]
@@ -168,18 +173,18 @@ def test_reader_sections_and_function_layouts():
     dn = s.en_dn["He"]
     assert isinstance(dn, Cambridge2) and dn.C == 2 and dn.fL == 0.25
     # linked (the reference's default): down electrons take the up functions
-    s2 = read_ckmf("t", _text(extra="replace_electron_nucleus_cusps\n 0")).to_system(allow_three_body=True)
+    s2 = read_ckmf("t", _text(extra="replace_electron_nucleus_cusps\n 0")).to_system(three_body=False)
     assert s2.en_dn["He"] is s2.en_up["He"]
 
 
 def test_reader_refusals_and_constraints():
     # cusp replacement follows the input's flag (on by default in the reference)
-    assert read_ckmf("t", _text()).to_system(allow_three_body=True).replace_cusps
-    assert not read_ckmf("t", _text()).to_system(replace_cusps=False, allow_three_body=True).replace_cusps
+    assert read_ckmf("t", _text()).to_system(three_body=False).replace_cusps
+    assert not read_ckmf("t", _text()).to_system(replace_cusps=False, three_body=False).replace_cusps
     c = read_ckmf("t", _text(ndet=2, aocc="1 0\n0 1", bocc="1 0\n1 0", ci="0.9 c 0 -0.5"))
     assert c.n_determinants == 2
     np.testing.assert_allclose(c.ci_coeffs, [0.9, -0.45])
-    s = c.to_system(allow_three_body=True)
+    s = c.to_system(three_body=False)
     assert s.n_det == 2 and s.det_alpha.tolist() == [[0], [1]] and s.det_beta.tolist() == [[0], [0]]
     np.testing.assert_array_equal(s.mo_alpha(), s.mo)          # both orbitals active for alpha
     assert s.det_columns(True).tolist() == [[0], [0]]
@@ -228,7 +233,7 @@ def test_reader_reads_every_reference_input():
             continue
         c = read_ckmf(p)
         if c.n_determinants == 1:
-            s = c.to_system(allow_three_body=True)
+            s = c.to_system(three_body=False)
             assert s.n_electrons == int(round(s.Z.sum())) - int(c.flags.get("charge", 0))
 
 
@@ -240,7 +245,7 @@ from oracle.evaluators import OracleEvaluator, ReferenceEvaluator
 from helpers import slater_conditions
 path, one_e = {path!r}, {one_e}
 text = open(path).read()
-s = read_ckmf(path).to_system(replace_cusps=False, allow_three_body=True)
+s = read_ckmf(path).to_system(replace_cusps=False, three_body=False)
 W, qf, dt = 3, 2, 0.01
 ref = ReferenceEvaluator(s, qf_mod=qf, dt=dt, ckmf_text=text, one_e_per_iter=one_e)
 orc = OracleEvaluator(s, qf_mod=qf, dt=dt)

@@ -30,7 +30,7 @@ if src.startswith("workload:"):
     s = dataclasses.replace(make_system(src[9:], seed=2), replace_cusps=True)
     text = None
 else:
-    s = read_ckmf(src).to_system(replace_cusps=True, allow_three_body=True)
+    s = read_ckmf(src).to_system(replace_cusps=True, three_body=False)
     text = open(src).read()
 ref = ReferenceEvaluator(s, qf_mod=2, dt=0.01, ckmf_text=text)
 """
