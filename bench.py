@@ -199,8 +199,9 @@ def mixed_section(system, W, e0, rank, args):
 
 
 def rows_section(args, rank: int):
-    """The widened rows on their own workloads: Cambridge2 two-body Jastrow
-    and a 12-determinant CI expansion, VMC with drift on the device (timed
+    """The widened rows on their own workloads: Cambridge2 two-body Jastrow,
+    a 12-determinant CI expansion and the three-body Jastrow (with Cambridge2),
+    VMC with drift on the device (timed
     with CUDA events on the library's stream), next to the reference CPU
     program on the same systems (all host cores, a bounded sample)."""
     import torch
@@ -209,7 +210,7 @@ def rows_section(args, rank: int):
     from qmcbeaver_b200.replicas import aggregate_timing, replica_seed
     from qmcbeaver_b200.system import make_system
     out = {}
-    for wl, W in (("vmc_cambridge2_16e", 8192), ("vmc_multidet_12e", 8192)):
+    for wl, W in (("vmc_cambridge2_16e", 8192), ("vmc_multidet_12e", 8192), ("vmc_threebody_16e", 8192)):
         s = make_system(wl, seed=1)
         N = s.n_electrons
         p = run_params(sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01,

@@ -225,6 +225,7 @@ __device__ inline bool lu_inverse_warp(double *A, double *X, double *vv, double 
 // Jastrow and potential from scratch for all electrons (updateAll order of
 // pairs is irrelevant here: totals are summed fresh, not incrementally).
 // Writes Ux[N][3] to `ux`, returns U, U_xx, V_ee, V_en through refs.
+template <bool kTB>
 __device__ inline void jastrow_pe_full_warp(const DevSys &S, const double *R, double *ux, double &U, double &Uxx,
                                             double &Vee, double &Ven)
 {
@@ -270,7 +271,7 @@ __device__ inline void jastrow_pe_full_warp(const DevSys &S, const double *R, do
     ux[3 * i + 1] = gy;
     ux[3 * i + 2] = gz;
   }
-  if (S.ntb > 0) {
+  if (kTB && S.ntb > 0) {
     double acc[2] = {0.0, 0.0};
     tb_full_lane(S, R, ux, acc);
     pu += acc[0];
@@ -304,7 +305,7 @@ __device__ inline double psi_lap_warp(int N, const double *gD, const double *Ux,
 // Full evaluation (do_basis = true: QMCSCFJastrow::evaluate with whichE = -1)
 // or refresh from the stored Slater values (do_basis = false).
 // R_in: [num][N][3] positions to store first (null: use the stored ones).
-template <typename TS, typename TI>
+template <typename TS, typename TI, bool kExtras>
 __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, int do_basis,
                                               EvalOut out)
@@ -354,7 +355,7 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
         __syncwarp();
         contract_dmma_warp(chi, ldc, S.ct[sp], n, K, Dn);
         __syncwarp();
-        if (S.cusp) {
+        if (kExtras && S.cusp) {
           cusp_replace_warp(S, sp, r, Dn, n, n);
           __syncwarp();
         }
@@ -401,7 +402,7 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
 
   double U, Uxx, Vee, Ven;
   double *ux = blk + L.Ux;
-  jastrow_pe_full_warp(S, Rs, ux, U, Uxx, Vee, Ven);
+  jastrow_pe_full_warp<kExtras>(S, Rs, ux, U, Uxx, Vee, Ven);
   __syncwarp();
   double *gD = blk + L.gradD, *gr = blk + L.grad, *mg = blk + L.mgrad;
   double Dxx = 0.0;
@@ -518,7 +519,10 @@ __device__ __forceinline__ void propose_move(const RunCfg &cfg, int slot, int st
 // Incremental Jastrow + potential of moving electron e from ro to rn
 // (QMCJastrowElectronElectron::updateOne, QMCJastrowElectronNuclear::evaluate,
 // QMCPotential_Energy::evaluate); lane j updates its own U_x[j] in place,
-// U_x[e] and the staged position of e are written last.
+// U_x[e] and the staged position of e are written last.  kTB: the system
+// may have three-body terms (a separate instantiation keeps them out of the
+// register allocation of the plain move).
+template <bool kTB>
 __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR, double *Ux, int e, int sp,
                                                      const double ro[3], const double rn[3], double &dU,
                                                      double &dUxx, double &dVee, double &dVen)
@@ -575,7 +579,7 @@ __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR
       ge[2] += sn * dzn - so * dzo;
     }
   }
-  if (S.ntb > 0) {
+  if (kTB && S.ntb > 0) {
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     tb_move_lane(S, sR, Ux, e, ro, rn, acc);
     dU += acc[0];
@@ -738,7 +742,9 @@ __device__ __forceinline__ void write_eval_out(const EvalOut &out, int wi, int N
 // (QMCWalker::initializePropagation / processPropagation,
 // QMcBeaver/src/QMCWalker.cpp:179-282).
 
-template <bool kMetropolis, typename TS, typename TI>
+// kExtras: cusp replacement and three-body terms compiled in (the plain
+// instantiation, used when the system has neither, carries none of their code).
+template <bool kMetropolis, typename TS, typename TI, bool kExtras>
 __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, MoveArgs mv,
                                               const EnergyCtl *ectl, double *stats, EvalOut out)
@@ -795,7 +801,7 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
 
   // ---- incremental Jastrow + potential
   double dU, dUxx, dVee, dVen;
-  jastrow_pe_move_warp(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
+  jastrow_pe_move_warp<kExtras>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
 
   // ---- basis at the new position and the new Slater / derivative rows
   if constexpr (sizeof(TS) == 8) {
@@ -807,9 +813,11 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
     __syncwarp();
     contract_slices_warp_f((const float *)chi, ldc, S.ctf[sp], n, K, (float *)Dn, (float *)cpart);
   }
-  if (S.cusp) {
-    __syncwarp();
-    cusp_replace_warp(S, sp, rn, Dn, n, n);
+  if constexpr (kExtras) {
+    if (S.cusp) {
+      __syncwarp();
+      cusp_replace_warp(S, sp, rn, Dn, n, n);
+    }
   }
   cp_async_wait<0>();
   __syncwarp();

@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(128) k_full_md(DevSys S, Layout L, RunCfg cfg,
   double *gD = blk + L.gradD, *gr = blk + L.grad, *mg = blk + L.mgrad, *ux = blk + L.Ux;
   const double Dxx = md_combine(S, &mb[0], &mb[1], tpr, gD);
   double U, Uxx, Vee, Ven;
-  jastrow_pe_full_warp(S, Rs, ux, U, Uxx, Vee, Ven);
+  jastrow_pe_full_warp<true>(S, Rs, ux, U, Uxx, Vee, Ven);
   __syncwarp();
   const double lap = psi_lap_warp(N, gD, ux, gr, Dxx, Uxx);
   __syncwarp();
@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
   double rn[3], g_fwd, u_acc;
   propose_move<kMetropolis>(cfg, slot, mv.step, e, N, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
   double dU, dUxx, dVee, dVen;
-  jastrow_pe_move_warp(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
+  jastrow_pe_move_warp<true>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
 
   basis_shells_warp(S, rn, chi, K);
   __syncwarp();

@@ -69,6 +69,7 @@ struct qmcb_handle {
   int *d_tbp = nullptr;
   double *d_ci = nullptr;
   bool md = false;  // several determinants: the k_*_md kernels
+  bool extras = false;  // cusp replacement or three-body terms: the k_move<..., true> instantiation
   double *d_state = nullptr;
   int *d_live = nullptr, *d_live_tmp = nullptr, *d_free = nullptr, *d_ctl = nullptr;
   int2 *d_copies = nullptr;
@@ -354,6 +355,31 @@ std::mutex g_noalloc_mu;
 void *g_noalloc_w_addr[64];
 void *g_noalloc_i_addr[64];
 }  // namespace
+
+// One launch of the single-determinant move kernel in the walker state's
+// precision, with the cusp / three-body code only when the system has them.
+template <bool kMetropolis>
+static void launch_move(qmcb_handle *h, int blocks, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
+                        const int *d_num, const double *R_in, MoveArgs mv, EvalOut o)
+{
+  const dim3 g(blocks), b(32 * h->wpb_move);
+  const size_t sm = h->smem_move;
+  if (h->params.precision == QMCB_PREC_MIXED) {
+    if (h->extras)
+      k_move<kMetropolis, float, MIXED_TI, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+                                                                   R_in, mv, h->d_ectl, h->d_stats, o);
+    else
+      k_move<kMetropolis, float, MIXED_TI, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+                                                                    R_in, mv, h->d_ectl, h->d_stats, o);
+  } else {
+    if (h->extras)
+      k_move<kMetropolis, double, double, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+                                                                  R_in, mv, h->d_ectl, h->d_stats, o);
+    else
+      k_move<kMetropolis, double, double, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+                                                                   R_in, mv, h->d_ectl, h->d_stats, o);
+  }
+}
 
 extern "C" {
 
@@ -733,6 +759,7 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   S.tbc = h->d_tbc;
   S.tbp = h->d_tbp;
   S.cusp = d->replace_cusps ? 1 : 0;
+  h->extras = S.cusp || S.ntb > 0;
   S.nsmax = nsmax;
   S.cns = h->d_cns;
   S.csexp = h->d_csexp;
@@ -830,12 +857,18 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   // the dynamic shared-memory limit is a per-kernel, process-wide attribute:
   // raise it to the device maximum once, so handles of different systems
   // (each launching with its own size) never undercut one another
-  CKC(cudaFuncSetAttribute(k_move<true, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<false, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<true, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_full<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_full<float, MIXED_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<true, double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<false, double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<true, float, MIXED_TI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<true, double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<false, double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<true, float, MIXED_TI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_full<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_full<float, MIXED_TI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_full<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC(cudaFuncSetAttribute(k_full<float, MIXED_TI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_full_md, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_move_md<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_move_md<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
@@ -908,6 +941,27 @@ int qmcb_synchronize(qmcb_handle *h)
   return QMCB_OK;
 }
 
+// One launch of the single-determinant full-evaluation / refresh kernel.
+static void launch_full(qmcb_handle *h, int blocks, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
+                        const int *d_num, const double *R_in, int do_basis, EvalOut o)
+{
+  const dim3 g(blocks), b(32 * h->wpb_full);
+  const size_t sm = h->smem_full;
+  if (h->params.precision == QMCB_PREC_MIXED) {
+    if (h->extras)
+      k_full<float, MIXED_TI, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, do_basis, o);
+    else
+      k_full<float, MIXED_TI, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, do_basis,
+                                                       o);
+  } else {
+    if (h->extras)
+      k_full<double, double, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, do_basis, o);
+    else
+      k_full<double, double, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, do_basis,
+                                                      o);
+  }
+}
+
 static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num, const double *d_R, EvalOut o,
                        cudaStream_t st)
 {
@@ -932,25 +986,13 @@ static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num,
   }
   if (which_e < 0) {
     int blocks = (num + h->wpb_full - 1) / h->wpb_full;
-    if (mixed)
-      k_full<float, MIXED_TI><<<blocks, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
-                                                                    nullptr, d_R, 1, o);
-    else
-      k_full<double, double><<<blocks, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots, num,
-                                                                     nullptr, d_R, 1, o);
+    launch_full(h, blocks, st, cfg, d_slots, num, nullptr, d_R, 1, o);
   } else {
     if (h->state_prec != h->params.precision)
       return fail(h, QMCB_E_STATE, "evaluate: walker state was written in another precision; evaluate all electrons first");
     MoveArgs mv{which_e, 0, 0, 0};
     int blocks = (num + h->wpb_move - 1) / h->wpb_move;
-    if (mixed)
-      k_move<false, float, MIXED_TI><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
-                                                                          num, nullptr, d_R, mv, h->d_ectl,
-                                                                          h->d_stats, o);
-    else
-      k_move<false, double, double><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
-                                                                           num, nullptr, d_R, mv, h->d_ectl,
-                                                                           h->d_stats, o);
+    launch_move<false>(h, blocks, st, cfg, d_slots, num, nullptr, d_R, mv, o);
   }
   CK(cudaGetLastError());
   if (which_e < 0) h->state_prec = h->params.precision;
@@ -1050,7 +1092,6 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps)
   if (h->state_prec != h->params.precision)
     return fail(h, QMCB_E_STATE, "qmcb_run_steps: walker state was written in another precision; call qmcb_init_walkers");
   if (h->in_flight) return fail(h, QMCB_E_STATE, "qmcb_run_steps: a batch of steps is still in flight on this handle");
-  const bool mixed = h->params.precision == QMCB_PREC_MIXED;
   if (h->n_live_host <= 0) return fail(h, QMCB_E_STATE, "qmcb_run_steps: no live walkers (population died out)");
   cudaStream_t st = h->stream;
   RunCfg cfg = make_cfg(h->params);
@@ -1073,14 +1114,8 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps)
         k_move_md<true><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state,
                                                                          h->d_live, 0, h->d_ctl, nullptr, mv,
                                                                          h->d_ectl, h->d_stats, o);
-      else if (mixed)
-        k_move<true, float, MIXED_TI><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state,
-                                                                            h->d_live, 0, h->d_ctl, nullptr, mv,
-                                                                            h->d_ectl, h->d_stats, o);
       else
-        k_move<true, double, double><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state,
-                                                                             h->d_live, 0, h->d_ctl, nullptr, mv,
-                                                                             h->d_ectl, h->d_stats, o);
+        launch_move<true>(h, blocks, st, cfg, h->d_live, 0, h->d_ctl, nullptr, mv, o);
       ps.end(st);
     }
     if (dmc && mv.e == 0) {
@@ -1108,12 +1143,8 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps)
       if (h->md)
         k_full_md<<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live, 0,
                                                                         h->d_ctl, nullptr, 0, o2);
-      else if (mixed)
-        k_full<float, MIXED_TI><<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state,
-                                                                           h->d_live, 0, h->d_ctl, nullptr, 0, o2);
       else
-        k_full<double, double><<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state,
-                                                                            h->d_live, 0, h->d_ctl, nullptr, 0, o2);
+        launch_full(h, blocks_full, st, cfg, h->d_live, 0, h->d_ctl, nullptr, 0, o2);
       ps.end(st);
     }
   }
