@@ -54,6 +54,10 @@ extern "C" {
 #define QMCB_DMC 1
 #define QMCB_NO_IMPORTANCE_SAMPLING 0
 #define QMCB_IMPORTANCE_SAMPLING 1
+/* umrigar93_importance_sampling: the drift-diffusion move near a nucleus mixed
+   with a hydrogen-like move (QMCWalker::moveElectronsUmrigar93ImportanceSampling,
+   QMcBeaver/src/QMCWalker.cpp:400-586) */
+#define QMCB_UMRIGAR93_IMPORTANCE_SAMPLING 2
 #define QMCB_QF_NONE 0
 #define QMCB_QF_UMRIGAR93_EQUAL 1
 #define QMCB_QF_UMRIGAR93_UNEQUAL 2

@@ -155,12 +155,14 @@ class ReferenceEvaluator(_Base):
     _loaded: Optional[str] = None
 
     def __init__(self, system: MolecularSystem, qf_mod: int = QMCB_QF_NONE, qf_a: float = 0.5, dt: float = 0.09,
-                 max_batch: int = 256, ckmf_text: Optional[str] = None, one_e_per_iter: int = 1):
+                 max_batch: int = 256, ckmf_text: Optional[str] = None, one_e_per_iter: int = 1,
+                 extra_flags: Optional[dict] = None):
         """`ckmf_text`: run this input (a reference .ckmf, flags patched for
         the batch size, the QF options and dt) instead of one written from
         `system`; `system` must then be the same input read by
         qmcbeaver_b200.ckmf.  `one_e_per_iter` = 0 selects the reference's
-        all-electron evaluation path (full evaluations only)."""
+        all-electron evaluation path (full evaluations only).  `extra_flags`
+        are further input flags (e.g. sampling_method for walker_move)."""
         if ReferenceEvaluator._loaded is not None:
             raise RuntimeError("the reference library holds one system per process")
         self.lib = C.CDLL(build_reference())
@@ -174,6 +176,7 @@ class ReferenceEvaluator(_Base):
         L.ref_walker_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_walker_inverse.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.ref_cusp_params.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.ref_walker_move.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]
         self.system = system
         self.N = system.n_electrons
         self.max_batch = max_batch
@@ -184,6 +187,7 @@ class ReferenceEvaluator(_Base):
                  "umrigar93_equalelectrons_parameter": float(qf_a), "dt": float(dt),
                  # read_flags starts the run at dt_equilibration (QMcBeaver/src/QMCFlags.cpp:915-916)
                  "dt_equilibration": float(dt)}
+        flags.update(extra_flags or {})
         if ckmf_text is None:
             system.to_ckmf(path, flags)
         else:
@@ -230,6 +234,21 @@ class ReferenceEvaluator(_Base):
             for k in range(rows):
                 self.lib.ref_cusp_params(beta, i, k, buf.ctypes.data_as(C.c_void_p))
                 out[i, k] = buf
+        return out
+
+    def walker_move(self, R0: np.ndarray, iteration: int, seed: int) -> Dict[str, np.ndarray]:
+        """One move of the reference's own QMCWalker from R0[N][3] with the
+        input's sampling_method (ref_walker_move): the proposed positions R,
+        gf = [ln G(R -> R'), ln G(R' -> R), G(R' -> R) / G(R -> R')], the
+        modified drift of the original (mg0) and trial (mg1) walkers, and
+        the electron moved (whichE, -1 = all)."""
+        R0 = np.ascontiguousarray(R0, np.float64)
+        out = dict(R=np.zeros((self.N, 3)), gf=np.zeros(3), mg=np.zeros((2, self.N, 3)))
+        e = self.lib.ref_walker_move(R0.ctypes.data_as(C.c_void_p), int(iteration), int(seed),
+                                     out["R"].ctypes.data_as(C.c_void_p), out["gf"].ctypes.data_as(C.c_void_p),
+                                     out["mg"].ctypes.data_as(C.c_void_p))
+        out["whichE"] = e
+        out["mg0"], out["mg1"] = out.pop("mg")
         return out
 
     def inverse(self, w, beta: int) -> np.ndarray:

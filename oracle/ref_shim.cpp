@@ -43,6 +43,9 @@ char **argv = 0;
 static QMCSCFJastrow *g_qmf = 0;
 static int g_nel = 0;
 
+// The evaluator ref_walker.cpp drives walkers with.
+QMCSCFJastrow *ref_shim_functions(void) { return g_qmf; }
+
 extern "C" {
 
 int ref_init(const char *ckmf)

@@ -305,7 +305,8 @@ class CkmfInput:
         f = self.flag
         run_type = {"variational": D.QMCB_VMC, "diffusion": D.QMCB_DMC}
         sampling = {"no_importance_sampling": D.QMCB_NO_IMPORTANCE_SAMPLING,
-                    "importance_sampling": D.QMCB_IMPORTANCE_SAMPLING}
+                    "importance_sampling": D.QMCB_IMPORTANCE_SAMPLING,
+                    "umrigar93_importance_sampling": D.QMCB_UMRIGAR93_IMPORTANCE_SAMPLING}
         qf = {"none": D.QMCB_QF_NONE, "umrigar93_equalelectrons": D.QMCB_QF_UMRIGAR93_EQUAL,
               "umrigar93_unequalelectrons": D.QMCB_QF_UMRIGAR93_UNEQUAL}
         emod = {"none": D.QMCB_EMOD_NONE, "umrigar93": D.QMCB_EMOD_UMRIGAR93,

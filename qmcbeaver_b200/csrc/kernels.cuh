@@ -460,19 +460,155 @@ struct MoveArgs {
 // Pieces of the single-electron move shared by the one- and the
 // several-determinant move kernels.
 
+// ---- umrigar93_importance_sampling (QMCWalker::moveElectronsUmrigar93ImportanceSampling
+//      and calculateReverseGreensFunctionUmrigar93ImportanceSampling,
+//      QMcBeaver/src/QMCWalker.cpp:400-586, 783-926; C. J. Umrigar, M. P.
+//      Nightingale, K. J. Runge, J. Chem. Phys. 99, 2865 (1993)).  Each
+//      electron moves either by the drift-diffusion Gaussian, its drift split
+//      into components along and across the direction from the nearest
+//      nucleus, or by a hydrogen-like exponential centred on that nucleus.
+struct UmrigarFrame {
+  double A[3], c[3];   // nearest nucleus, centre of the drifted Gaussian
+  double zeta, pg, ps; // exponential's exponent, Gaussian / exponential move probabilities
+};
+
+__device__ inline void umrigar_frame(const DevSys &S, const RunCfg &cfg, const double x[3], const double v[3],
+                                     UmrigarFrame &F)
+{
+  int nn = 0;
+  double best = 1e300;
+  for (int A = 0; A < S.M; A++) {
+    const double4 P = S.nuc[A];
+    const double dx = x[0] - P.x, dy = x[1] - P.y, dz = x[2] - P.z;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 < best) {
+      best = d2;
+      nn = A;
+    }
+  }
+  const double4 P = S.nuc[nn];
+  F.A[0] = P.x;
+  F.A[1] = P.y;
+  F.A[2] = P.z;
+  const double tau = cfg.dt;
+  const double d = sqrt(best);
+  double zu[3], rad[3], zc = 0.0, rc = 0.0;
+  for (int k = 0; k < 3; k++) {
+    zu[k] = (x[k] - F.A[k]) / d;
+    zc += zu[k] * v[k];
+  }
+  for (int k = 0; k < 3; k++) {
+    rad[k] = v[k] - zc * zu[k];
+    rc += rad[k] * rad[k];
+  }
+  rc = sqrt(rc);
+  if (rc > 1e-15)
+    for (int k = 0; k < 3; k++) rad[k] /= rc;
+  const double zC = fmax(d + zc * tau, 0.0);
+  const double rC = 2.0 * rc * tau * zC / (d + zC);
+  F.zeta = sqrt(P.w * P.w + 1.0 / tau);
+  F.ps = fmin(fmax(0.5 * erfc((d + zc * tau) / sqrt(2.0 * tau)), 0.0), 1.0);
+  F.pg = 1.0 - F.ps;
+  for (int k = 0; k < 3; k++) F.c[k] = F.A[k] + rC * rad[k] + zC * zu[k];
+}
+
+// ln of the one-electron transition density of the frame at y:
+// pg (2 pi tau)^-3/2 exp(-|y - c|^2 / 2 tau) + ps / pi zeta^3 exp(-2 zeta |y - A|)
+__device__ inline double umrigar_log_gf(const UmrigarFrame &F, const RunCfg &cfg, const double y[3])
+{
+  double d1 = 0.0, d2 = 0.0;
+  for (int k = 0; k < 3; k++) {
+    d1 += (y[k] - F.c[k]) * (y[k] - F.c[k]);
+    d2 += (y[k] - F.A[k]) * (y[k] - F.A[k]);
+  }
+  const double tau = cfg.dt;
+  const double lg = F.pg > 0.0 ? log(F.pg) - 1.5 * log(6.283185307179586 * tau) - d1 / (2.0 * tau) : -INFINITY;
+  const double ls = F.ps > 0.0 ? log(F.ps / 3.141592653589793) + 3.0 * log(F.zeta) - 2.0 * F.zeta * sqrt(d2)
+                               : -INFINITY;
+  const double m = fmax(lg, ls);
+  if (m == -INFINITY) return -INFINITY;
+  return m + log(exp(lg - m) + exp(ls - m));
+}
+
+// Proposal of electron e and ln G(R -> R') over all electrons (the
+// unmoved ones contribute their stay-in-place density).
+__device__ __noinline__ void umrigar_propose(const DevSys &S, const RunCfg &cfg, int slot, int step, int e, int N,
+                                             const double *R, const double *mgo, double *rn, double *log_fwd,
+                                             double *u_acc)
+{
+  const int lane = threadIdx.x & 31;
+  // lanes 0-3 draw two uniforms each from their own Philox counters
+  double u[8];
+  {
+    const U4 c = philox4x32(U4{(uint32_t)slot, (uint32_t)step, (uint32_t)(8 + (lane & 3)), 0x0A7E5A21u}, cfg.seed);
+    const double ua = u01(c.x, c.y), ub = u01(c.z, c.w);
+    for (int k = 0; k < 4; k++) {
+      u[2 * k] = __shfl_sync(QMCB_FULL_MASK, ua, k);
+      u[2 * k + 1] = __shfl_sync(QMCB_FULL_MASK, ub, k);
+    }
+  }
+  UmrigarFrame F;
+  umrigar_frame(S, cfg, R + 3 * e, mgo + 3 * e, F);
+  if (u[0] < F.pg) {
+    // Gaussian around the drifted centre (Box-Muller from u[1..4])
+    const double r1 = sqrt(-2.0 * log(u[1])), r2 = sqrt(-2.0 * log(u[3]));
+    const double g[3] = {r1 * cos(6.283185307179586 * u[2]), r1 * sin(6.283185307179586 * u[2]),
+                         r2 * cos(6.283185307179586 * u[4])};
+    const double sg = sqrt(cfg.dt);
+    for (int k = 0; k < 3; k++) rn[k] = F.c[k] + sg * g[k];
+  } else {
+    // hydrogen-like: r from r^2 exp(-2 zeta r) (a Gamma(3) variate over 2 zeta;
+    // Random::randomDistribution1 draws the same law by rejection), uniform direction
+    const double r = -log(u[1] * u[2] * u[3]) / (2.0 * F.zeta);
+    const double phi = 6.283185307179586 * u[4], theta = acos(1.0 - 2.0 * u[5]);
+    rn[0] = F.A[0] + r * sin(theta) * cos(phi);
+    rn[1] = F.A[1] + r * sin(theta) * sin(phi);
+    rn[2] = F.A[2] + r * cos(theta);
+  }
+  *u_acc = u[6];
+  double part = 0.0;
+  for (int i = lane; i < N; i += 32) {
+    UmrigarFrame Fi;
+    if (i == e) {
+      part += umrigar_log_gf(F, cfg, rn);
+    } else {
+      umrigar_frame(S, cfg, R + 3 * i, mgo + 3 * i, Fi);
+      part += umrigar_log_gf(Fi, cfg, R + 3 * i);
+    }
+  }
+  *log_fwd = warp_sum(part);
+}
+
+// ln G(R' -> R): frames of the new positions R' with the new drift, density
+// at the old positions (the moved electron's old position is ro).
+__device__ __noinline__ double umrigar_log_reverse(const DevSys &S, const RunCfg &cfg, int e, int N, const double *Rn,
+                                                   const double *mg, const double *ro)
+{
+  double part = 0.0;
+  for (int i = threadIdx.x & 31; i < N; i += 32) {
+    UmrigarFrame F;
+    umrigar_frame(S, cfg, Rn + 3 * i, mg + 3 * i, F);
+    part += umrigar_log_gf(F, cfg, i == e ? ro : Rn + 3 * i);
+  }
+  return warp_sum(part);
+}
+
 // New position of electron e: the walker's own Philox stream and the drift
-// (QMCWalker::moveElectronsNoImportanceSampling / moveElectronsImportanceSampling,
-// QMcBeaver/src/QMCWalker.cpp:313-398), or the caller's position.  g_fwd is
-// the exponent sum of G(R -> R'), u_acc the acceptance uniform.
+// (QMCWalker::moveElectronsNoImportanceSampling / moveElectronsImportanceSampling /
+// moveElectronsUmrigar93ImportanceSampling, QMcBeaver/src/QMCWalker.cpp:313-586),
+// or the caller's position.  g_fwd: the exponent sum of G(R -> R') (drift
+// diffusion) or ln G(R -> R') (Umrigar93); u_acc the acceptance uniform.
 template <bool kMetropolis>
-__device__ __forceinline__ void propose_move(const RunCfg &cfg, int slot, int step, int e, int N, const double ro[3],
-                                             const double *mgo, const double *R_in, int wi, double rn[3],
-                                             double &g_fwd, double &u_acc)
+__device__ __forceinline__ void propose_move(const DevSys &S, const RunCfg &cfg, int slot, int step, int e, int N,
+                                             const double *R, const double ro[3], const double *mgo,
+                                             const double *R_in, int wi, double rn[3], double &g_fwd, double &u_acc)
 {
   const int lane = lane_id();
   g_fwd = 0.0;
   u_acc = 0.5;
-  if (kMetropolis) {
+  if (kMetropolis && cfg.sampling == 2) {
+    umrigar_propose(S, cfg, slot, step, e, N, R, mgo, rn, &g_fwd, &u_acc);
+  } else if (kMetropolis) {
     // lanes 0-2 draw the three Gaussian displacements, lane 3 the acceptance
     // uniform, each from its own Philox counter; one round trip for the warp
     double zr, z[3];
@@ -606,8 +742,9 @@ __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR
 // :1060-1185) and observables (:2096-2123, 2306-2387) of one proposed move.
 // log_ratio = ln|psi'/psi|, negative = the ratio changed sign.  Writes the
 // walker's weight, age and the per-call sums; returns the acceptance.
-__device__ __forceinline__ bool metropolis_reweight(const RunCfg &cfg, const MoveArgs &mv, const EnergyCtl *ectl,
-                                                    double *stats, double *sc, const double *sc0, int N, int e,
+__device__ __forceinline__ bool metropolis_reweight(const DevSys &S, const RunCfg &cfg, const MoveArgs &mv,
+                                                    const EnergyCtl *ectl, double *stats, double *sc,
+                                                    const double *sc0, int N, int e, const double *Rn,
                                                     const double ro[3], const double rn[3], const double *mg,
                                                     double g_fwd, double u_acc, double log_ratio, bool negative,
                                                     bool bad, double EL, double modratio)
@@ -615,7 +752,9 @@ __device__ __forceinline__ bool metropolis_reweight(const RunCfg &cfg, const Mov
   const int lane = lane_id();
   // G(R' -> R): only electron e moved, the others contribute (dt v'_i)^2
   double log_g = 0.0;
-  if (cfg.sampling == 1) {
+  if (cfg.sampling == 2) {
+    log_g = umrigar_log_reverse(S, cfg, e, N, Rn, mg, ro) - g_fwd;
+  } else if (cfg.sampling == 1) {
     double pr = 0.0;
     for (int t = lane; t < 3 * N; t += 32) {
       const double tt = (t / 3 == e) ? (ro[t - 3 * e] - rn[t - 3 * e] - cfg.dt * mg[t]) : (cfg.dt * mg[t]);
@@ -797,7 +936,7 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
 
   const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3], g_fwd, u_acc;
-  propose_move<kMetropolis>(cfg, slot, mv.step, e, N, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
+  propose_move<kMetropolis>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
 
   // ---- incremental Jastrow + potential
   double dU, dUxx, dVee, dVen;
@@ -951,7 +1090,7 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
 
   bool accept = true;
   if (kMetropolis)
-    accept = metropolis_reweight(cfg, mv, ectl, stats, sc, sc0, N, e, ro, rn, mg, g_fwd, u_acc,
+    accept = metropolis_reweight(S, cfg, mv, ectl, stats, sc, sc0, N, e, sR, ro, rn, mg, g_fwd, u_acc,
                                  log(fabs(ratio)) + dU, ratio < 0, bad, EL, modratio);
   __syncwarp();
 

@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
 
   const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3], g_fwd, u_acc;
-  propose_move<kMetropolis>(cfg, slot, mv.step, e, N, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
+  propose_move<kMetropolis>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
   double dU, dUxx, dVee, dVen;
   jastrow_pe_move_warp<true>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
 
@@ -469,8 +469,8 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
 
   bool accept = true;
   if (kMetropolis)
-    accept = metropolis_reweight(cfg, mv, ectl, stats, sc, sc0, N, e, ro, rn, mg, g_fwd, u_acc, log(fabs(RD)) + dU,
-                                 RD < 0, bad, EL, modratio);
+    accept = metropolis_reweight(S, cfg, mv, ectl, stats, sc, sc0, N, e, sR, ro, rn, mg, g_fwd, u_acc,
+                                 log(fabs(RD)) + dU, RD < 0, bad, EL, modratio);
   __syncwarp();
 
   if (accept) {

@@ -902,7 +902,7 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
   if (!(p->dt > 0)) return fail(h, QMCB_E_ARG, "qmcb_set_params: dt must be positive");
   if (p->qf_modification == QMCB_QF_UMRIGAR93_EQUAL && (p->qf_equal_a > 1 || p->qf_equal_a <= 0))
     return fail(h, QMCB_E_ARG, "qmcb_set_params: umrigar93_equalelectrons_parameter must be in (0, 1]");
-  if (p->run_type < 0 || p->run_type > 1 || p->sampling < 0 || p->sampling > 1 || p->qf_modification < 0 ||
+  if (p->run_type < 0 || p->run_type > 1 || p->sampling < 0 || p->sampling > 2 || p->qf_modification < 0 ||
       p->qf_modification > 2 || p->energy_modification < 0 || p->energy_modification > 2 || p->reweighting < 0 ||
       p->reweighting > 2 || p->energy_cutoff < 0 || p->energy_cutoff > 2)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");

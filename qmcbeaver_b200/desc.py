@@ -13,7 +13,7 @@ _ip = C.POINTER(C.c_int)
 
 # constants of include/qmcb200.h
 QMCB_VMC, QMCB_DMC = 0, 1
-QMCB_NO_IMPORTANCE_SAMPLING, QMCB_IMPORTANCE_SAMPLING = 0, 1
+QMCB_NO_IMPORTANCE_SAMPLING, QMCB_IMPORTANCE_SAMPLING, QMCB_UMRIGAR93_IMPORTANCE_SAMPLING = 0, 1, 2
 QMCB_QF_NONE, QMCB_QF_UMRIGAR93_EQUAL, QMCB_QF_UMRIGAR93_UNEQUAL = 0, 1, 2
 QMCB_EMOD_NONE, QMCB_EMOD_UMRIGAR93, QMCB_EMOD_MODIFIED_UMRIGAR93 = 0, 1, 2
 QMCB_RW_SIMPLE_SYMMETRIC, QMCB_RW_SIMPLE_ASYMMETRIC, QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED = 0, 1, 2

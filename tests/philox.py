@@ -28,3 +28,14 @@ def uniform4(seed, walker, step, purpose):
     r1 = philox4x32((walker & MASK, step & MASK, purpose & MASK, 0x51ED2701), seed)
     r2 = philox4x32((walker & MASK, step & MASK, purpose & MASK, 0x51ED2702), seed)
     return [u01(r1[0], r1[1]), u01(r1[2], r1[3]), u01(r2[0], r2[1]), u01(r2[2], r2[3])]
+
+
+def umrigar_uniforms(seed, slot, step):
+    """The eight uniforms of one Umrigar93 move (lanes 0-3 of the walker's
+    warp, two each from their own counter): u[0] picks the branch, u[1..5]
+    place the electron, u[6] is the acceptance uniform."""
+    u = []
+    for k in range(4):
+        c = philox4x32((slot & MASK, step & MASK, 8 + k, 0x0A7E5A21), seed)
+        u += [u01(c[0], c[1]), u01(c[2], c[3])]
+    return u
