@@ -259,6 +259,23 @@ int qmcb_init_walkers(qmcb_handle *h, int n, const double *R);
  */
 int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats *stats);
 
+/*
+ * One step, as qmcb_run_steps(h, step, 1, stats), that also returns the
+ * configuration records the reference writes with print_configs 1
+ * (QMCWalker::processPropagation -> QMCWalkerData::writeConfigs,
+ * QMcBeaver/src/QMCWalker.cpp:238-250, QMcBeaver/src/QMCWalkerData.cpp:216-224;
+ * the binary record of QMCConfigIO::writeCorrelatedSamplingConfiguration,
+ * QMcBeaver/src/QMCConfigIO.cpp:271-384, less its leading int electron count):
+ * for every walker live before the step, in list order, the trial walker
+ * with weight p (the acceptance probability) and then the original walker
+ * with weight 1 - p.  Each record is QMCB_CONFIG_RECORD(N) doubles:
+ * R[N][3], lap(D)/D, grad(D)/D [N][3], ln J, potential energy, weight.
+ * records holds capacity walkers (2 * capacity records); *n_records is set.
+ */
+#define QMCB_CONFIG_RECORD(N) (6 * (N) + 4)
+int qmcb_run_step_configs(qmcb_handle *h, int step, double *records, int capacity, int *n_records,
+                          qmcb_step_stats *stats);
+
 /* Asynchronous form for drivers that keep several handles busy at once
  * (one stream per handle; kernels of different handles overlap on the GPU):
  * qmcb_run_steps_async enqueues the steps and returns; qmcb_steps_done

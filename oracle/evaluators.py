@@ -92,6 +92,7 @@ class OracleEvaluator(_Base):
         L.orc_evaluate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.orc_walker_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_walker_inverse.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_walker_slater_grad.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_walker_inverse_det.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.orc_walker_kappa.argtypes = [C.c_void_p]
         L.orc_walker_kappa.restype = C.c_double
@@ -126,6 +127,13 @@ class OracleEvaluator(_Base):
 
     def _get(self, w, a, b, c):
         self.lib.orc_walker_get(w, a, b, c)
+
+    def slater_grad(self, walkers) -> np.ndarray:
+        """grad(D)/D [n][N][3], the Slater part of the drift (QMCWalkerData::D_x)."""
+        out = np.zeros((len(walkers), self.N, 3))
+        for i, w in enumerate(walkers):
+            self.lib.orc_walker_slater_grad(w, out[i].ctypes.data_as(C.c_void_p))
+        return out
 
     def inverse(self, w, beta: int, det: int = 0) -> np.ndarray:
         """Inverse Slater matrix of determinant `det` of one spin."""

@@ -1353,6 +1353,13 @@ void orc_walker_get(const orc_walker *w, double *sc, double *grad, double *mgrad
   }
 }
 
+/* grad(D)/D of every electron, the Slater part without the Jastrow
+   (QMCWalkerData::D_x, written to configuration files) */
+void orc_walker_slater_grad(const orc_walker *w, double *out)
+{
+  for (int i = 0; i < 3 * w->s->N; i++) out[i] = w->D_x[i];
+}
+
 /* the inverse of determinant 0 (Dc_invA(0) / Dc_invB(0)) */
 void orc_walker_inverse(const orc_walker *w, int beta, double *out)
 {

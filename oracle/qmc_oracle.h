@@ -38,6 +38,7 @@ int orc_evaluate(const orc_system *s, orc_walker **walkers, const double *R, int
 
 /* Same layout as ref_walker_get (oracle/ref_shim.cpp). */
 void orc_walker_get(const orc_walker *w, double *scalars, double *grad, double *mgrad);
+void orc_walker_slater_grad(const orc_walker *w, double *out);
 void orc_walker_inverse(const orc_walker *w, int beta, double *out);
 void orc_walker_inverse_det(const orc_walker *w, int beta, int ci, double *out);
 double orc_walker_kappa(const orc_walker *w);

@@ -29,7 +29,7 @@ EXPORTS = [
     "qmcb_run_steps", "qmcb_num_walkers", "qmcb_get_walkers", "qmcb_copy_slot", "qmcb_synchronize",
     "qmcb_stream", "qmcb_set_walker_weights", "qmcb_branch", "qmcb_set_profiling", "qmcb_get_kernel_stats",
     "qmcb_branch_weights_noalloc", "qmcb_run_steps_async", "qmcb_steps_done", "qmcb_steps_collect",
-    "qmcb_state_bytes", "qmcb_fit_cusps",
+    "qmcb_state_bytes", "qmcb_fit_cusps", "qmcb_run_step_configs",
 ]
 
 KERNELS = ["move", "branch", "copy", "energy", "refresh"]
@@ -75,6 +75,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.qmcb_set_profiling.argtypes = [vp, C.c_int]
     L.qmcb_get_kernel_stats.argtypes = [vp, vp, C.c_int]
     L.qmcb_run_steps_async.argtypes = [vp, C.c_int, C.c_int]
+    L.qmcb_run_step_configs.argtypes = [vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int), vp]
     L.qmcb_steps_done.argtypes = [vp]
     L.qmcb_steps_collect.argtypes = [vp, vp]
     L.qmcb_state_bytes.argtypes = [vp]
@@ -158,6 +159,19 @@ class QMCB200Functions:
         st = StepStats()
         self._check(self.lib.qmcb_run_steps(self.h, int(first_step), int(n_steps), C.byref(st)), "qmcb_run_steps")
         return st
+
+    def run_step_configs(self, step: int) -> "tuple[np.ndarray, StepStats]":
+        """One step that also returns its configuration records (the
+        reference's print_configs output; qmcb_run_step_configs): array
+        [2 * live walkers][6N + 4] of R, lap(D)/D, grad(D)/D, ln J, PE,
+        weight -- the trial walker (weight p) then the original (1 - p)."""
+        n = self.num_walkers()
+        rec = np.zeros((2 * max(n, 1), 6 * self.N + 4))
+        cnt = C.c_int()
+        st = StepStats()
+        self._check(self.lib.qmcb_run_step_configs(self.h, int(step), _ptr(rec), n, C.byref(cnt), C.byref(st)),
+                    "qmcb_run_step_configs")
+        return rec[:cnt.value], st
 
     def run_steps_async(self, first_step: int, n_steps: int) -> None:
         self._check(self.lib.qmcb_run_steps_async(self.h, int(first_step), int(n_steps)), "qmcb_run_steps_async")

@@ -454,7 +454,43 @@ struct MoveArgs {
   int step;          // global step number (random stream position)
   int do_reweight;   // this step reweights / collects observables (whichE == 0)
   int reweight_on;   // step >= reweight_start_step
+  double *dump;      // configuration records of this step (null: none), see dump_configs
 };
+
+// Configuration records of one Metropolis step (print_configs:
+// QMCWalker::processPropagation -> QMCWalkerData::writeConfigs ->
+// QMCConfigIO::writeCorrelatedSamplingConfiguration, QMcBeaver/src/QMCWalker.cpp:
+// 238-250, QMcBeaver/src/QMCWalkerData.cpp:216-224): the trial walker with
+// weight p, then the original walker with weight 1 - p.  A record is
+// R[3N], lap(D)/D, grad(D)/D [3N], ln J, potential energy, weight (6N + 4
+// doubles); walker wi writes records 2 wi and 2 wi + 1.  sR holds the trial
+// positions, gD_new / gD_old the Slater gradient ratios of all electrons.
+__device__ __forceinline__ void dump_configs(double *dump, int wi, int N, int e, const double *sR,
+                                             const double ro[3], double Dxx_new, const double *gD_new,
+                                             double U_new, double PE_new, double Dxx_old, const double *gD_old,
+                                             double U_old, double PE_old, double p)
+{
+  const int lane = lane_id();
+  const int rec = 6 * N + 4;
+  double *t = dump + (size_t)wi * 2 * rec, *o = t + rec;
+  for (int k = lane; k < 3 * N; k += 32) {
+    const double x = sR[k];
+    t[k] = x;
+    o[k] = (k / 3 == e) ? ro[k - 3 * e] : x;
+    t[3 * N + 1 + k] = gD_new[k];
+    o[3 * N + 1 + k] = gD_old[k];
+  }
+  if (lane == 0) {
+    t[3 * N] = Dxx_new;
+    o[3 * N] = Dxx_old;
+    t[6 * N + 1] = U_new;
+    o[6 * N + 1] = U_old;
+    t[6 * N + 2] = PE_new;
+    o[6 * N + 2] = PE_old;
+    t[6 * N + 3] = p;
+    o[6 * N + 3] = 1.0 - p;
+  }
+}
 
 // ------------------------------------------------------------------------
 // Pieces of the single-electron move shared by the one- and the
@@ -598,7 +634,9 @@ __device__ __noinline__ double umrigar_log_reverse(const DevSys &S, const RunCfg
 // moveElectronsUmrigar93ImportanceSampling, QMcBeaver/src/QMCWalker.cpp:313-586),
 // or the caller's position.  g_fwd: the exponent sum of G(R -> R') (drift
 // diffusion) or ln G(R -> R') (Umrigar93); u_acc the acceptance uniform.
-template <bool kMetropolis>
+// kUmr: the Umrigar93 move is compiled in (the launcher picks such an
+// instantiation whenever the run uses it).
+template <bool kMetropolis, bool kUmr>
 __device__ __forceinline__ void propose_move(const DevSys &S, const RunCfg &cfg, int slot, int step, int e, int N,
                                              const double *R, const double ro[3], const double *mgo,
                                              const double *R_in, int wi, double rn[3], double &g_fwd, double &u_acc)
@@ -606,7 +644,7 @@ __device__ __forceinline__ void propose_move(const DevSys &S, const RunCfg &cfg,
   const int lane = lane_id();
   g_fwd = 0.0;
   u_acc = 0.5;
-  if (kMetropolis && cfg.sampling == 2) {
+  if (kMetropolis && kUmr && cfg.sampling == 2) {
     umrigar_propose(S, cfg, slot, step, e, N, R, mgo, rn, &g_fwd, &u_acc);
   } else if (kMetropolis) {
     // lanes 0-2 draw the three Gaussian displacements, lane 3 the acceptance
@@ -742,17 +780,18 @@ __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR
 // :1060-1185) and observables (:2096-2123, 2306-2387) of one proposed move.
 // log_ratio = ln|psi'/psi|, negative = the ratio changed sign.  Writes the
 // walker's weight, age and the per-call sums; returns the acceptance.
+template <bool kUmr>
 __device__ __forceinline__ bool metropolis_reweight(const DevSys &S, const RunCfg &cfg, const MoveArgs &mv,
                                                     const EnergyCtl *ectl, double *stats, double *sc,
                                                     const double *sc0, int N, int e, const double *Rn,
                                                     const double ro[3], const double rn[3], const double *mg,
                                                     double g_fwd, double u_acc, double log_ratio, bool negative,
-                                                    bool bad, double EL, double modratio)
+                                                    bool bad, double EL, double modratio, double &p_acc)
 {
   const int lane = lane_id();
   // G(R' -> R): only electron e moved, the others contribute (dt v'_i)^2
   double log_g = 0.0;
-  if (cfg.sampling == 2) {
+  if (kUmr && cfg.sampling == 2) {
     log_g = umrigar_log_reverse(S, cfg, e, N, Rn, mg, ro) - g_fwd;
   } else if (cfg.sampling == 1) {
     double pr = 0.0;
@@ -777,6 +816,7 @@ __device__ __forceinline__ bool metropolis_reweight(const DevSys &S, const RunCf
   if (bad) p = 0.0;
   if (cfg.run_type == 1 && negative) p = 0.0;
   if (p > 1.0) p = 1.0;
+  p_acc = p;
   const bool accept = p > u_acc;
   const double new_age = accept ? 0.0 : age + 1.0;
   double w = sc0[SC_WEIGHT];
@@ -881,8 +921,9 @@ __device__ __forceinline__ void write_eval_out(const EvalOut &out, int wi, int N
 // (QMCWalker::initializePropagation / processPropagation,
 // QMcBeaver/src/QMCWalker.cpp:179-282).
 
-// kExtras: cusp replacement and three-body terms compiled in (the plain
-// instantiation, used when the system has neither, carries none of their code).
+// kExtras: cusp replacement, three-body terms and the Umrigar93 move compiled
+// in (the plain instantiation, used when the run needs none of them, carries
+// none of their code).
 template <bool kMetropolis, typename TS, typename TI, bool kExtras>
 __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, MoveArgs mv,
@@ -936,7 +977,7 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
 
   const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3], g_fwd, u_acc;
-  propose_move<kMetropolis>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
+  propose_move<kMetropolis, kExtras>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
 
   // ---- incremental Jastrow + potential
   double dU, dUxx, dVee, dVen;
@@ -1089,9 +1130,16 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
   const double sign_new = sc0[SC_SIGN_A + sp] * (ratio < 0 ? -1.0 : 1.0);
 
   bool accept = true;
-  if (kMetropolis)
-    accept = metropolis_reweight(S, cfg, mv, ectl, stats, sc, sc0, N, e, sR, ro, rn, mg, g_fwd, u_acc,
-                                 log(fabs(ratio)) + dU, ratio < 0, bad, EL, modratio);
+  if (kMetropolis) {
+    double p_acc;
+    accept = metropolis_reweight<kExtras>(S, cfg, mv, ectl, stats, sc, sc0, N, e, sR, ro, rn, mg, g_fwd, u_acc,
+                                          log(fabs(ratio)) + dU, ratio < 0, bad, EL, modratio, p_acc);
+    if (mv.dump) {
+      const double Dxx_old = (S.na > 0 ? sc0[SC_LAPR_A] : 0.0) + (S.nb > 0 ? sc0[SC_LAPR_B] : 0.0);
+      dump_configs(mv.dump, wi, N, e, sR, ro, Dxx, gD, U_new, PE, Dxx_old, blk + L.gradD, sc0[SC_U],
+                   sc0[SC_PE], p_acc);
+    }
+  }
   __syncwarp();
 
   if (accept) {

@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
 
   const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3], g_fwd, u_acc;
-  propose_move<kMetropolis>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
+  propose_move<kMetropolis, true>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
   double dU, dUxx, dVee, dVen;
   jastrow_pe_move_warp<true>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
 
@@ -468,9 +468,14 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
   const double sgnD_new = sgnD0 * (RD < 0 ? -1.0 : 1.0);
 
   bool accept = true;
-  if (kMetropolis)
-    accept = metropolis_reweight(S, cfg, mv, ectl, stats, sc, sc0, N, e, sR, ro, rn, mg, g_fwd, u_acc,
-                                 log(fabs(RD)) + dU, RD < 0, bad, EL, modratio);
+  if (kMetropolis) {
+    double p_acc;
+    accept = metropolis_reweight<true>(S, cfg, mv, ectl, stats, sc, sc0, N, e, sR, ro, rn, mg, g_fwd, u_acc,
+                                 log(fabs(RD)) + dU, RD < 0, bad, EL, modratio, p_acc);
+    if (mv.dump)
+      dump_configs(mv.dump, wi, N, e, sR, ro, Dxx, gD, U_new, PE, sc0[SC_LAPR_A], blk + L.gradD, sc0[SC_U],
+                   sc0[SC_PE], p_acc);
+  }
   __syncwarp();
 
   if (accept) {

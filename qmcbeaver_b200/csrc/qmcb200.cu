@@ -74,6 +74,7 @@ struct qmcb_handle {
   int *d_live = nullptr, *d_live_tmp = nullptr, *d_free = nullptr, *d_ctl = nullptr;
   int2 *d_copies = nullptr;
   double *d_stats = nullptr;
+  double *d_dump = nullptr;  // configuration records of one step (qmcb_run_step_configs), on first use
   EnergyCtl *d_ectl = nullptr;
   // staging for the host-pointer evaluate
   int *d_slots = nullptr;
@@ -364,15 +365,17 @@ static void launch_move(qmcb_handle *h, int blocks, cudaStream_t st, const RunCf
 {
   const dim3 g(blocks), b(32 * h->wpb_move);
   const size_t sm = h->smem_move;
+  // the Umrigar93 move is compiled only into the extras instantiation
+  const bool extras = h->extras || (kMetropolis && cfg.sampling == QMCB_UMRIGAR93_IMPORTANCE_SAMPLING);
   if (h->params.precision == QMCB_PREC_MIXED) {
-    if (h->extras)
+    if (extras)
       k_move<kMetropolis, float, MIXED_TI, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
                                                                    R_in, mv, h->d_ectl, h->d_stats, o);
     else
       k_move<kMetropolis, float, MIXED_TI, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
                                                                     R_in, mv, h->d_ectl, h->d_stats, o);
   } else {
-    if (h->extras)
+    if (extras)
       k_move<kMetropolis, double, double, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
                                                                   R_in, mv, h->d_ectl, h->d_stats, o);
     else
@@ -884,7 +887,7 @@ int qmcb_destroy(qmcb_handle *h)
   void *ptrs[] = {h->d_tbi, h->d_tbL, h->d_tbc, h->d_tbp, h->d_cns, h->d_csexp, h->d_cscoef[0], h->d_cscoef[1], h->d_cpar[0], h->d_cpar[1], h->d_crmax[0],
                   h->d_crmax[1], h->d_docc[0], h->d_docc[1], h->d_dswap[0], h->d_dswap[1], h->d_ci, h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
-                  h->d_copies, h->d_stats, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
+                  h->d_copies, h->d_stats, h->d_dump, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
@@ -1085,7 +1088,9 @@ int qmcb_init_walkers(qmcb_handle *h, int n, const double *R)
 
 // Enqueues n_steps Monte Carlo steps and the copy of the step statistics
 // into the handle's pinned buffer, then records the completion event.
-static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps)
+// dump: device buffer for the configuration records of every step's move
+// (each step overwrites it; null: none).
+static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps, double *dump = nullptr)
 {
   if (n_steps < 0 || first_step < 0) return fail(h, QMCB_E_ARG, "qmcb_run_steps: bad step range");
   if (!h->evaluated_once) return fail(h, QMCB_E_STATE, "qmcb_run_steps: call qmcb_init_walkers first");
@@ -1107,6 +1112,7 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps)
     mv.step = step;
     mv.do_reweight = mv.e == 0;
     mv.reweight_on = step >= h->params.reweight_start_step;
+    mv.dump = dump;
     EvalOut o{};
     {
       ProfScope ps(h, QMCB_KERNEL_MOVE, st);
@@ -1184,6 +1190,24 @@ int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats 
   int rc = enqueue_steps(h, first_step, n_steps);
   if (rc) return rc;
   return finish_steps(h, stats);
+}
+
+int qmcb_run_step_configs(qmcb_handle *h, int step, double *records, int capacity, int *n_records,
+                          qmcb_step_stats *stats)
+{
+  if (!h || !records || !n_records) return QMCB_E_ARG;
+  const int n = h->n_live_host;
+  if (capacity < n) return fail(h, QMCB_E_ARG, "qmcb_run_step_configs: capacity below the live walker count");
+  const size_t rec = (size_t)QMCB_CONFIG_RECORD(h->N);
+  if (!h->d_dump) CK(cudaMalloc(&h->d_dump, sizeof(double) * 2 * rec * (size_t)h->max_walkers));
+  int rc = enqueue_steps(h, step, 1, h->d_dump);
+  if (rc) return rc;
+  // the walkers that moved are the n live before the step, in list order
+  CK(cudaMemcpyAsync(records, h->d_dump, sizeof(double) * 2 * rec * (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+  rc = finish_steps(h, stats);
+  if (rc) return rc;
+  *n_records = 2 * n;
+  return QMCB_OK;
 }
 
 int qmcb_run_steps_async(qmcb_handle *h, int first_step, int n_steps)
