@@ -985,7 +985,9 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
 
   // ---- basis at the new position and the new Slater / derivative rows
   if constexpr (sizeof(TS) == 8) {
-    basis_shells_warp(S, rn, (double *)chi, ldc);
+    // the exponential slots follow the five chi rows (into the Dn / valc
+    // space, unused until the contraction)
+    basis_slots_warp(S, rn, (double *)chi, ldc, sm + 5 * ldc);
     __syncwarp();
     contract_dmma_warp((const double *)chi, ldc, S.ct[sp], n, K, (double *)Dn);
   } else {

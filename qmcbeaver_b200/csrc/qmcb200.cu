@@ -57,6 +57,8 @@ struct qmcb_handle {
   double4 *d_cparam = nullptr;
   int4 *d_shell = nullptr;
   int2 *d_fn = nullptr;
+  int2 *d_xsl = nullptr;
+  int4 *d_fq = nullptr;
   double *d_pexp = nullptr, *d_pcoef = nullptr;
   int *d_en[2] = {nullptr, nullptr};
   int *d_docc[2] = {nullptr, nullptr};
@@ -497,6 +499,16 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   std::stable_sort(shells.begin(), shells.end(), [](const int4 &x, const int4 &y) {
     return (x.z & 0xffff) < (y.z & 0xffff);
   });
+  // exponential slots of the move kernel's basis pass: one per (shell,
+  // primitive) in shell order; every function points at its shell's slots
+  std::vector<int2> xsl;
+  std::vector<int4> fq(K);
+  for (const int4 &sh : shells) {
+    const int nmem = sh.z & 0xff, L = (sh.z >> 8) & 0xff, np = sh.z >> 16;
+    const int q0 = (int)xsl.size();
+    for (int i = 0; i < np; i++) xsl.push_back(make_int2(sh.x, sh.w + i));
+    for (int m = 0; m < nmem; m++) fq[sh.y + m] = make_int4(sh.x, q0, np, L);
+  }
   std::vector<double> ct[2];
   for (int sp = 0; sp < 2; sp++) {
     int n = nact[sp];
@@ -687,6 +699,8 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(upload(&h->d_prim, prim));
   CKC(upload(&h->d_shell, shells));
   CKC(upload(&h->d_fn, fn));
+  CKC(upload(&h->d_xsl, xsl));
+  CKC(upload(&h->d_fq, fq));
   CKC(upload(&h->d_pexp, pexp));
   CKC(upload(&h->d_pcoef, pcoef));
   CKC(upload(&h->d_ct[0], ct[0]));
@@ -735,6 +749,9 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   S.nshell = (int)shells.size();
   S.shell = h->d_shell;
   S.fn = h->d_fn;
+  S.nslot = (int)xsl.size();
+  S.xsl = h->d_xsl;
+  S.fq = h->d_fq;
   S.pexp = h->d_pexp;
   S.pcoef = h->d_pcoef;
   S.ct[0] = h->d_ct[0];
@@ -796,18 +813,22 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
       L.Inv[sp] = take(n * n);
     }
   }
+  // the move kernel stages gradD .. sc in one copy; grad (an evaluate
+  // output only) sits after them
   L.gradD = take(3 * h->N);
   L.Ux = take(3 * h->N);
-  L.grad = take(3 * h->N);
   L.mgrad = take(3 * h->N);
   L.sc = take(kScalars);
+  L.grad = take(3 * h->N);
   L.stride = (off + 31) & ~31;  // 256-byte aligned blocks
   // move-kernel scratch: staged copies read whole padded ranges of the block
   // (all inside the block: arrays start on 32-byte boundaries, the block is
   // padded to 256 bytes)
-  L.mv_region_a = move_region_a(h->N, K);
   L.mv_dn = even(5 * h->nmax);
   L.mv_valc = even(h->nmax);
+  // the basis pass keeps its exponential slots after the five chi rows,
+  // reaching into the Dn / valc space
+  L.mv_region_a = std::max(move_region_a(h->N, K), even(5 * K + (int)xsl.size() - L.mv_dn - L.mv_valc));
   L.mv_r = even(3 * h->N);
   L.mv_tail = even(L.sc + kScalars - L.gradD);
   for (int sp = 0; sp < 2; sp++) {
@@ -885,7 +906,7 @@ int qmcb_destroy(qmcb_handle *h)
   if (!h) return QMCB_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
   void *ptrs[] = {h->d_tbi, h->d_tbL, h->d_tbc, h->d_tbp, h->d_cns, h->d_csexp, h->d_cscoef[0], h->d_cscoef[1], h->d_cpar[0], h->d_cpar[1], h->d_crmax[0],
-                  h->d_crmax[1], h->d_docc[0], h->d_docc[1], h->d_dswap[0], h->d_dswap[1], h->d_ci, h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
+                  h->d_crmax[1], h->d_docc[0], h->d_docc[1], h->d_dswap[0], h->d_dswap[1], h->d_ci, h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_xsl, h->d_fq, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
                   h->d_copies, h->d_stats, h->d_dump, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
   for (void *p : ptrs)
