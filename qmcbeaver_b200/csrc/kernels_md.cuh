@@ -29,10 +29,17 @@ __host__ __device__ inline int full_md_scratch_doubles(int N, int K, int nmax, i
 {
   return even(5 * (K + 1)) + even(5 * amax) + 2 * nmax * nmax + 2 * even(nmax) + even(3 * N) + even(ndet) + 8;
 }
-__host__ __device__ inline int move_md_scratch_doubles(int N, int K, int nmax, int amax, int ndet, int tail)
+// chi rows of the move kernel; the basis pass's exponential slots follow
+// them into the gr .. valc space (written only after the contraction)
+__host__ __device__ inline int move_md_chi_doubles(int N, int K, int nmax, int amax, int ndet, int nslot)
 {
-  return even(5 * K) + 2 * even(3 * N) + even(5 * amax) + 2 * even(ndet) + even(nmax) + even(3 * N) + even(tail) +
-         2;
+  const int rest = 2 * even(3 * N) + even(5 * amax) + 2 * even(ndet) + even(nmax);
+  return even(max(5 * K, 5 * K + nslot - rest));
+}
+__host__ __device__ inline int move_md_scratch_doubles(int N, int K, int nmax, int amax, int ndet, int tail, int nslot)
+{
+  return move_md_chi_doubles(N, K, nmax, amax, ndet, nslot) + 2 * even(3 * N) + even(5 * amax) + 2 * even(ndet) +
+         even(nmax) + even(3 * N) + even(tail) + 2;
 }
 
 // One copy of spin sp's determinant block.
@@ -332,9 +339,9 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
   double *blk = state + (size_t)slot * L.stride;
   const int tail = L.sc + kScalars - L.gradD;
 
-  double *sm = smem + (size_t)warp * move_md_scratch_doubles(N, K, nmax, amax, nd, tail);
+  double *sm = smem + (size_t)warp * move_md_scratch_doubles(N, K, nmax, amax, nd, tail, S.nslot);
   double *chi = sm;
-  double *gr = chi + even(5 * K);
+  double *gr = chi + move_md_chi_doubles(N, K, nmax, amax, nd, S.nslot);
   double *mg = gr + even(3 * N);
   double *Dn = mg + even(3 * N);       // new rows of the active orbitals [5][a]
   double *rat = Dn + even(5 * amax);   // per-determinant ratios
@@ -359,7 +366,7 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
   double dU, dUxx, dVee, dVen;
   jastrow_pe_move_warp<true>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
 
-  basis_shells_warp(S, rn, chi, K);
+  basis_slots_warp(S, rn, chi, K, chi + 5 * K);
   __syncwarp();
   contract_dmma_warp(chi, K, S.ct[sp], a, K, Dn);
   __syncwarp();

@@ -865,7 +865,7 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   const int amax = std::max(nact[0], nact[1]);
   const size_t per_move =
-      sizeof(double) * (size_t)(md ? move_md_scratch_doubles(h->N, K, h->nmax, amax, S.ndet, L.sc + kScalars - L.gradD)
+      sizeof(double) * (size_t)(md ? move_md_scratch_doubles(h->N, K, h->nmax, amax, S.ndet, L.sc + kScalars - L.gradD, S.nslot)
                                    : L.mv_stride);
   const size_t per_full =
       sizeof(double) * (size_t)(md ? full_md_scratch_doubles(h->N, K, h->nmax, amax, S.ndet)
