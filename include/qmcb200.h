@@ -286,6 +286,36 @@ int qmcb_run_steps_async(qmcb_handle *h, int first_step, int n_steps);
 int qmcb_steps_done(qmcb_handle *h);
 int qmcb_steps_collect(qmcb_handle *h, qmcb_step_stats *stats);
 
+/*
+ * Groups: many handles (systems of different sizes, each with its own
+ * walkers) stepped together.  No counterpart in the reference, which runs
+ * one molecule per process; it serves many small jobs on one GPU.  Each step
+ * is one persistent kernel per bucket of members with similar per-walker
+ * shared-memory needs, in which every warp takes the next walker of any
+ * member, then (DMC members) one branching launch for all members.  The
+ * first calls of qmcb_group_run_steps time the candidate launch
+ * configurations (bucketing, warps per block) on the real steps and keep the
+ * fastest; results do not depend on the configuration.  Batches without
+ * refresh are captured as one CUDA graph and replayed while the batch length
+ * and configuration stay the same.
+ * Members: single-determinant FP64 handles on one device, each initialised
+ * (qmcb_init_walkers), none in flight; the caller does not use a member's
+ * handle for steps while the group steps it.  At most 512 members.
+ * qmcb_group_run_steps advances member i by n_steps steps from
+ * first_steps[i] (the same steps as qmcb_run_steps(member, first_steps[i],
+ * n_steps)); stats[i] receives member i's statistics (stats may be NULL).
+ */
+typedef struct qmcb_group qmcb_group;
+int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out);
+int qmcb_group_destroy(qmcb_group *g);
+const char *qmcb_group_last_error(const qmcb_group *g);
+int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmcb_step_stats *stats);
+/* Candidate configurations, the tuned one (-1 while tuning), the one the
+ * last batch ran, and that one's bucket count and warps per block. */
+int qmcb_group_config(const qmcb_group *g, int *n_configs, int *chosen, int *last, int *n_buckets, int *wpb);
+/* Fix the configuration (0 .. n_configs - 1), or -1 to time them again. */
+int qmcb_group_set_config(qmcb_group *g, int config);
+
 /* Device bytes of the walker state of a handle (admission control). */
 size_t qmcb_state_bytes(const qmcb_handle *h);
 

@@ -30,6 +30,8 @@ EXPORTS = [
     "qmcb_stream", "qmcb_set_walker_weights", "qmcb_branch", "qmcb_set_profiling", "qmcb_get_kernel_stats",
     "qmcb_branch_weights_noalloc", "qmcb_run_steps_async", "qmcb_steps_done", "qmcb_steps_collect",
     "qmcb_state_bytes", "qmcb_fit_cusps", "qmcb_run_step_configs",
+    "qmcb_group_create", "qmcb_group_destroy", "qmcb_group_last_error", "qmcb_group_run_steps", "qmcb_group_config",
+    "qmcb_group_set_config",
 ]
 
 KERNELS = ["move", "branch", "copy", "energy", "refresh"]
@@ -75,6 +77,13 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.qmcb_set_profiling.argtypes = [vp, C.c_int]
     L.qmcb_get_kernel_stats.argtypes = [vp, vp, C.c_int]
     L.qmcb_run_steps_async.argtypes = [vp, C.c_int, C.c_int]
+    L.qmcb_group_create.argtypes = [vp, C.c_int, C.POINTER(vp)]
+    L.qmcb_group_destroy.argtypes = [vp]
+    L.qmcb_group_last_error.argtypes = [vp]
+    L.qmcb_group_last_error.restype = C.c_char_p
+    L.qmcb_group_run_steps.argtypes = [vp, vp, C.c_int, vp]
+    L.qmcb_group_config.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.qmcb_group_set_config.argtypes = [vp, C.c_int]
     L.qmcb_run_step_configs.argtypes = [vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int), vp]
     L.qmcb_steps_done.argtypes = [vp]
     L.qmcb_steps_collect.argtypes = [vp, vp]
@@ -230,6 +239,59 @@ class QMCB200Functions:
         return int(self.lib.qmcb_stream(self.h) or 0)
 
 
+class QMCB200Group:
+    """Several handles (systems of different sizes, each with its own
+    walkers) stepped together: one persistent launch per bucket of similar
+    shared-memory need per step, the launch configuration tuned by timing
+    the first batches, batches replayed as CUDA graphs (qmcb_group_*).
+    The members keep their own state: get_walkers etc. on a member read what
+    the group's steps left there."""
+
+    def __init__(self, members: "list[QMCB200Functions]"):
+        self.lib = load_library()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.h for m in self.members])
+        g = C.c_void_p()
+        rc = self.lib.qmcb_group_create(arr, len(self.members), C.byref(g))
+        if rc != 0:
+            raise QMCBError(f"qmcb_group_create failed ({rc}): {self.lib.qmcb_group_last_error(None).decode()}")
+        self.g = g
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            raise QMCBError(f"{what} failed ({rc}): {self.lib.qmcb_group_last_error(self.g).decode()}")
+
+    def close(self) -> None:
+        if getattr(self, "g", None):
+            self.lib.qmcb_group_destroy(self.g)
+            self.g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run_steps(self, first_steps, n_steps: int) -> "list[StepStats]":
+        """Member i runs steps first_steps[i] .. + n_steps - 1 (an int:
+        the same first step for every member)."""
+        n = len(self.members)
+        if isinstance(first_steps, int):
+            first_steps = [first_steps] * n
+        fs = (C.c_int * n)(*[int(x) for x in first_steps])
+        st = (StepStats * n)()
+        self._check(self.lib.qmcb_group_run_steps(self.g, fs, int(n_steps), st), "qmcb_group_run_steps")
+        return list(st)
+
+    def config(self) -> Dict[str, int]:
+        v = [C.c_int() for _ in range(5)]
+        self._check(self.lib.qmcb_group_config(self.g, *[C.byref(x) for x in v]), "qmcb_group_config")
+        return dict(zip(("n_configs", "chosen", "last", "n_buckets", "warps_per_block"), [x.value for x in v]))
+
+    def set_config(self, config: int) -> None:
+        self._check(self.lib.qmcb_group_set_config(self.g, int(config)), "qmcb_group_set_config")
+
+
 def fit_cusps(system: MolecularSystem) -> "tuple[np.ndarray, np.ndarray]":
     """The electron-nucleus cusp replacement records of both spins
     (qmcb_fit_cusps; host only): arrays [n_nuclei][orbital rows][8] of rc,
@@ -248,4 +310,4 @@ def fit_cusps(system: MolecularSystem) -> "tuple[np.ndarray, np.ndarray]":
     return out[0], out[1]
 
 
-__all__ = ["QMCB200Functions", "fit_cusps", "QMCBError", "load_library", "run_params", "QMCB_VMC", "QMCB_DMC", "EXPORTS"]
+__all__ = ["QMCB200Functions", "QMCB200Group", "fit_cusps", "QMCBError", "load_library", "run_params", "QMCB_VMC", "QMCB_DMC", "EXPORTS"]

@@ -924,16 +924,17 @@ __device__ __forceinline__ void write_eval_out(const EvalOut &out, int wi, int N
 // kExtras: cusp replacement, three-body terms and the Umrigar93 move compiled
 // in (the plain instantiation, used when the run needs none of them, carries
 // none of their code).
+//
+// move_walker is the work of one warp on walker wi of the list (sm: the
+// warp's L.mv_stride doubles of shared memory); k_move runs it for one
+// system, k_move_group for the walkers of many systems in one launch.
 template <bool kMetropolis, typename TS, typename TI, bool kExtras>
-__global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
-                                              int num, const int *d_num, const double *R_in, MoveArgs mv,
-                                              const EnergyCtl *ectl, double *stats, EvalOut out)
+__device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, const RunCfg &cfg, double *state,
+                                            const int *slots, int wi, double *sm, const double *R_in,
+                                            const MoveArgs &mv, const EnergyCtl *ectl, double *stats,
+                                            const EvalOut &out)
 {
-  extern __shared__ double smem[];
-  const int lane = lane_id(), warp = threadIdx.x >> 5;
-  const int nw = d_num ? *d_num : num;
-  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (wi >= nw) return;
+  const int lane = lane_id();
   const int N = S.N, K = S.K;
   const int e = mv.e;
   const int sp = e < S.na ? 0 : 1;
@@ -942,7 +943,6 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
   double *blk = state + (size_t)slot * L.stride;
 
   // ---- scratch of this warp (offsets in doubles, all even: 16-byte aligned)
-  double *sm = smem + (size_t)warp * L.mv_stride;
   const int ldc = K;
   TS *chi = (TS *)sm;                  // region A: basis values ...
   TS *cpart = (TS *)sm;                // ... then contraction slice sums
@@ -1189,6 +1189,20 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
   }
 }
 
+template <bool kMetropolis, typename TS, typename TI, bool kExtras>
+__global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+                                              int num, const int *d_num, const double *R_in, MoveArgs mv,
+                                              const EnergyCtl *ectl, double *stats, EvalOut out)
+{
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5;
+  const int nw = d_num ? *d_num : num;
+  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (wi >= nw) return;
+  move_walker<kMetropolis, TS, TI, kExtras>(S, L, cfg, state, slots, wi, smem + (size_t)warp * L.mv_stride, R_in,
+                                            mv, ectl, stats, out);
+}
+
 // ------------------------------------------------------------------------
 // Nonunit-weight branching (QMCRun::nonunitWeightBranching,
 // QMcBeaver/src/QMCRun.cpp:740-814) on the live slot list, one CTA of
@@ -1218,10 +1232,10 @@ __device__ __forceinline__ bool branch_recommended(const double *sc, double e_or
   return ok;
 }
 
-__global__ void __launch_bounds__(1024) k_branch(double *state, Layout L, int *live, int *live_tmp, int *free_stack,
-                                                 int *ctl, int2 *copies, double thr_split, double thr_fuse,
-                                                 uint64_t seed, int step, double *stats, double e_orig,
-                                                 int limit_branching)
+__device__ __forceinline__ void branch_block(double *state, const Layout &L, int *live, int *live_tmp,
+                                             int *free_stack, int *ctl, int2 *copies, double thr_split,
+                                             double thr_fuse, uint64_t seed, int step, double *stats, double e_orig,
+                                             int limit_branching)
 {
   __shared__ int s_warp[32];
   __shared__ int s_base[4];
@@ -1375,12 +1389,22 @@ __global__ void __launch_bounds__(1024) k_branch(double *state, Layout L, int *l
   }
 }
 
+__global__ void __launch_bounds__(1024) k_branch(double *state, Layout L, int *live, int *live_tmp, int *free_stack,
+                                                 int *ctl, int2 *copies, double thr_split, double thr_fuse,
+                                                 uint64_t seed, int step, double *stats, double e_orig,
+                                                 int limit_branching)
+{
+  branch_block(state, L, live, live_tmp, free_stack, ctl, copies, thr_split, thr_fuse, seed, step, stats, e_orig,
+               limit_branching);
+}
+
 // Copies whole walker blocks for the splits recorded by k_branch; the copy
 // keeps the halved weight already written to the source.
-__global__ void k_copy(double *state, Layout L, const int2 *copies, const int *ctl)
+__device__ __forceinline__ void copy_blocks(double *state, const Layout &L, const int2 *copies, const int *ctl,
+                                            int first, int stride)
 {
   const int nc = ctl[2];
-  for (int c = blockIdx.x; c < nc; c += gridDim.x) {
+  for (int c = first; c < nc; c += stride) {
     int2 p = copies[c];
     const double *src = state + (size_t)p.x * L.stride;
     double *dst = state + (size_t)p.y * L.stride;
@@ -1388,12 +1412,16 @@ __global__ void k_copy(double *state, Layout L, const int2 *copies, const int *c
   }
 }
 
+__global__ void k_copy(double *state, Layout L, const int2 *copies, const int *ctl)
+{
+  copy_blocks(state, L, copies, ctl, blockIdx.x, gridDim.x);
+}
+
 // E_est from the running weighted energy average and
 // E_T = E_est - c ln(W / W0) (QMCManager::updateEstimatedEnergy /
 // updateTrialEnergy, QMcBeaver/src/QMCManager.cpp:2247-2310).
-__global__ void k_energy(EnergyCtl *ectl, const double *stats, int min_samples_ok)
+__device__ __forceinline__ void update_energy(EnergyCtl *ectl, const double *stats, int min_samples_ok)
 {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double sw = stats[ST_RUN_SUM_W];
   // E_est follows the running average once it holds 100 samples
   // (QMCManager::updateEstimatedEnergy, QMcBeaver/src/QMCManager.cpp:2247-2261)
@@ -1401,6 +1429,12 @@ __global__ void k_energy(EnergyCtl *ectl, const double *stats, int min_samples_o
   double ratio = stats[ST_FINAL_W] / ectl->target_weight;
   double lr = ratio > 1e-250 ? log(ratio) : 0.0;
   ectl->e_trial = ectl->e_est - ectl->pop_control * lr;
+}
+
+__global__ void k_energy(EnergyCtl *ectl, const double *stats, int min_samples_ok)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  update_energy(ectl, stats, min_samples_ok);
 }
 
 // Packs R, weight, E_L, log|psi|, sign of the first n live walkers into

@@ -20,6 +20,7 @@
 #include "cusp_fit.h"
 #include "kernels.cuh"
 #include "kernels_md.cuh"
+#include "kernels_group.cuh"
 
 using namespace qmcb;
 
@@ -1387,6 +1388,387 @@ int qmcb_branch_weights_noalloc(const double *d_weight_in, int n, double branchi
   e = cudaGetLastError();
   if (e != cudaSuccess)
     return fail(nullptr, QMCB_E_CUDA, std::string("qmcb_branch_weights_noalloc: launch: ") + cudaGetErrorString(e));
+  return QMCB_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------
+// Groups: the walkers of many handles (systems of different sizes) stepped
+// by one persistent launch per bucket of similar shared-memory need
+// (kernels_group.cuh).  No counterpart in the reference, which runs one
+// molecule per process.
+
+struct qmcb_group {
+  int device = 0;
+  int n_sm = 0, max_optin = 0;  // max_optin: dynamic shared memory a group block may use
+  cudaStream_t stream = nullptr;
+  std::vector<qmcb_handle *> mem;  // in launch order (extras flag, then per-warp scratch)
+  std::vector<int> user;           // mem[i] is the caller's member user[i]
+  GroupMember *d_gm = nullptr;
+  std::vector<GroupMember> h_gm;
+  int *d_counter = nullptr;  // one per bucket
+  struct Bucket {
+    int first, count, stride, wpb, grid;
+    bool extras;
+  };
+  std::vector<std::vector<Bucket>> cands;  // launch configurations the tuner tries
+  std::vector<double> cost;                // ms per walker-move of each (< 0: not yet timed)
+  int chosen = -1;                         // the tuned configuration
+  int last = -1;                           // configuration of the last batch
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t gexec = nullptr;  // the last batch's launch sequence
+  int g_steps = -1, g_config = -1;
+  std::string err;
+};
+
+static int gfail(qmcb_group *g, int code, const std::string &msg)
+{
+  if (g)
+    g->err = msg;
+  else
+    g_create_error = msg;
+  return code;
+}
+
+#define GK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return gfail(g, QMCB_E_CUDA, std::string(#call ": ") + cudaGetErrorString(e_));  \
+  } while (0)
+
+static bool member_extras(const qmcb_handle *h)
+{
+  return h->extras || h->params.sampling == QMCB_UMRIGAR93_IMPORTANCE_SAMPLING;
+}
+
+// Persistent grid of one bucket: as many blocks as fit on every SM at once.
+static int bucket_grid(qmcb_group *g, bool extras, int stride, int wpb, int *grid)
+{
+  int per_sm = 0;
+  const size_t smem = sizeof(double) * (size_t)stride * wpb;
+  cudaError_t e = extras ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_move_group<true>, 32 * wpb, smem)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_move_group<false>, 32 * wpb, smem);
+  if (e != cudaSuccess) return gfail(g, QMCB_E_CUDA, std::string("qmcb_group: occupancy: ") + cudaGetErrorString(e));
+  if (per_sm < 1) return gfail(g, QMCB_E_LIMIT, "qmcb_group: a member's scratch does not fit one block");
+  *grid = per_sm * g->n_sm;
+  return QMCB_OK;
+}
+
+// The configurations the tuner tries: members in runs of equal extras flag,
+// each run as one bucket or split at its one or two largest jumps in
+// scratch size; 4 or 2 warps per block.
+static int build_candidates(qmcb_group *g)
+{
+  const int n = (int)g->mem.size();
+  std::vector<int> cuts;  // run boundaries (extras flag changes)
+  for (int i = 1; i < n; i++)
+    if (member_extras(g->mem[i]) != member_extras(g->mem[i - 1])) cuts.push_back(i);
+  // largest relative jumps of the scratch size inside runs
+  std::vector<std::pair<double, int>> jumps;
+  for (int i = 1; i < n; i++) {
+    if (std::find(cuts.begin(), cuts.end(), i) != cuts.end()) continue;
+    const double r = (double)g->mem[i]->lay.mv_stride / g->mem[i - 1]->lay.mv_stride;
+    if (r > 1.0) jumps.push_back({r, i});
+  }
+  std::sort(jumps.begin(), jumps.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
+    return a.first > b.first;
+  });
+  std::vector<std::vector<int>> splits;
+  splits.push_back(cuts);
+  for (int k = 1; k <= 2 && k <= (int)jumps.size(); k++) {
+    std::vector<int> c = cuts;
+    for (int j = 0; j < k; j++) c.push_back(jumps[j].second);
+    std::sort(c.begin(), c.end());
+    splits.push_back(c);
+  }
+  g->cands.clear();
+  for (const auto &c : splits)
+    for (int wpb : {4, 2}) {
+      std::vector<qmcb_group::Bucket> bs;
+      int lo = 0;
+      for (size_t j = 0; j <= c.size(); j++) {
+        const int hi = j < c.size() ? c[j] : n;
+        if (hi <= lo) continue;
+        qmcb_group::Bucket b{};
+        b.first = lo;
+        b.count = hi - lo;
+        b.extras = member_extras(g->mem[lo]);
+        b.stride = 0;
+        for (int i = lo; i < hi; i++) b.stride = std::max(b.stride, g->mem[i]->lay.mv_stride);
+        b.wpb = std::max(1, std::min<int>(wpb, g->max_optin / (int)(sizeof(double) * b.stride)));
+        int rc = bucket_grid(g, b.extras, b.stride, b.wpb, &b.grid);
+        if (rc) return rc;
+        bs.push_back(b);
+        lo = hi;
+      }
+      g->cands.push_back(bs);
+    }
+  g->cost.assign(g->cands.size(), -1.0);
+  g->chosen = g->cands.size() == 1 ? 0 : -1;
+  return QMCB_OK;
+}
+
+// The launches of n_steps steps in configuration c (graph capturable when
+// no member refreshes).
+static int group_enqueue(qmcb_group *g, int c, int n_steps, const int *first_steps, bool refresh)
+{
+  cudaStream_t st = g->stream;
+  const int nm = (int)g->mem.size();
+  bool any_dmc = false;
+  for (auto *h : g->mem) any_dmc |= h->params.run_type == QMCB_DMC;
+  for (int t = 0; t < n_steps; t++) {
+    const auto &bs = g->cands[c];
+    for (size_t b = 0; b < bs.size(); b++) {
+      const auto &B = bs[b];
+      GK(cudaMemsetAsync(g->d_counter + b, 0, sizeof(int), st));
+      const size_t smem = sizeof(double) * (size_t)B.stride * B.wpb;
+      if (B.extras)
+        k_move_group<true><<<B.grid, 32 * B.wpb, smem, st>>>(g->d_gm + B.first, B.count, t, B.stride,
+                                                             g->d_counter + b);
+      else
+        k_move_group<false><<<B.grid, 32 * B.wpb, smem, st>>>(g->d_gm + B.first, B.count, t, B.stride,
+                                                              g->d_counter + b);
+    }
+    if (any_dmc) {
+      k_branch_group<<<nm, 1024, 0, st>>>(g->d_gm, t);
+      k_copy_group<<<dim3(64, nm), 256, 0, st>>>(g->d_gm, t);
+      k_energy_group<<<(nm + 127) / 128, 128, 0, st>>>(g->d_gm, nm, t);
+    }
+    if (refresh) {
+      for (int i = 0; i < nm; i++) {
+        qmcb_handle *h = g->mem[i];
+        const int step = first_steps[g->user[i]] + t;
+        if (h->params.refresh_interval > 0 && (step + 1) % h->params.refresh_interval == 0) {
+          EvalOut o2{};
+          const int blocks_full = (h->max_walkers + h->wpb_full - 1) / h->wpb_full;
+          launch_full(h, blocks_full, st, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, 0, o2);
+        }
+      }
+    }
+  }
+  GK(cudaGetLastError());
+  return QMCB_OK;
+}
+
+extern "C" {
+
+int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out)
+{
+  if (!members || !out || n <= 0) return gfail(nullptr, QMCB_E_ARG, "qmcb_group_create: bad argument");
+  if (n > kGroupMax) return gfail(nullptr, QMCB_E_LIMIT, "qmcb_group_create: more than 512 members");
+  *out = nullptr;
+  for (int i = 0; i < n; i++) {
+    const qmcb_handle *h = members[i];
+    if (!h) return gfail(nullptr, QMCB_E_ARG, "qmcb_group_create: null member");
+    if (h->md)
+      return gfail(nullptr, QMCB_E_ARG,
+                   "qmcb_group_create: member " + std::to_string(i) + " has several determinants; step it on its own");
+    if (h->device != members[0]->device)
+      return gfail(nullptr, QMCB_E_ARG, "qmcb_group_create: members on different devices");
+    for (int j = 0; j < i; j++)
+      if (members[j] == h) return gfail(nullptr, QMCB_E_ARG, "qmcb_group_create: a handle appears twice");
+  }
+  qmcb_group *g = new qmcb_group();
+  g->device = members[0]->device;
+  cudaSetDevice(g->device);
+  cudaDeviceGetAttribute(&g->n_sm, cudaDevAttrMultiProcessorCount, g->device);
+  cudaDeviceGetAttribute(&g->max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, g->device);
+  std::vector<int> idx(n);
+  for (int i = 0; i < n; i++) idx[i] = i;
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+    const bool ea = member_extras(members[a]), eb = member_extras(members[b]);
+    if (ea != eb) return !ea;
+    return members[a]->lay.mv_stride < members[b]->lay.mv_stride;
+  });
+  for (int i : idx) {
+    g->mem.push_back(members[i]);
+    g->user.push_back(i);
+  }
+  int rc = QMCB_OK;
+  cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&g->d_gm, sizeof(GroupMember) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&g->d_counter, sizeof(int) * (n + 1));
+  if (e == cudaSuccess) e = cudaEventCreate(&g->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&g->ev1);
+  // the group kernels hold the member prefix sums in static shared memory:
+  // the dynamic part may use the rest of the opt-in maximum
+  cudaFuncAttributes fa0{}, fa1{};
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa0, k_move_group<false>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa1, k_move_group<true>);
+  if (e == cudaSuccess) g->max_optin -= (int)std::max(fa0.sharedSizeBytes, fa1.sharedSizeBytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, g->max_optin);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, g->max_optin);
+  if (e != cudaSuccess) rc = gfail(nullptr, QMCB_E_CUDA, std::string("qmcb_group_create: ") + cudaGetErrorString(e));
+  if (!rc) {
+    rc = build_candidates(g);
+    if (rc) g_create_error = g->err;
+  }
+  if (rc) {
+    qmcb_group_destroy(g);
+    return rc;
+  }
+  *out = g;
+  return QMCB_OK;
+}
+
+int qmcb_group_destroy(qmcb_group *g)
+{
+  if (!g) return QMCB_OK;
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->gexec) cudaGraphExecDestroy(g->gexec);
+  if (g->d_gm) cudaFree(g->d_gm);
+  if (g->d_counter) cudaFree(g->d_counter);
+  if (g->ev0) cudaEventDestroy(g->ev0);
+  if (g->ev1) cudaEventDestroy(g->ev1);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+  return QMCB_OK;
+}
+
+const char *qmcb_group_last_error(const qmcb_group *g) { return g ? g->err.c_str() : g_create_error.c_str(); }
+
+int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmcb_step_stats *stats)
+{
+  if (!g || !first_steps || n_steps < 0) return gfail(g, QMCB_E_ARG, "qmcb_group_run_steps: bad argument");
+  const int nm = (int)g->mem.size();
+  bool refresh = false;
+  for (int i = 0; i < nm; i++) {
+    qmcb_handle *h = g->mem[i];
+    const std::string who = "qmcb_group_run_steps: member " + std::to_string(g->user[i]);
+    if (first_steps[g->user[i]] < 0) return gfail(g, QMCB_E_ARG, who + ": negative first step");
+    if (!h->evaluated_once) return gfail(g, QMCB_E_STATE, who + ": call qmcb_init_walkers first");
+    if (h->in_flight) return gfail(g, QMCB_E_STATE, who + ": a batch of steps is in flight on its handle");
+    if (h->params.precision != QMCB_PREC_FP64 || h->state_prec != QMCB_PREC_FP64)
+      return gfail(g, QMCB_E_ARG, who + ": groups step FP64 walkers only");
+    refresh |= h->params.refresh_interval > 0;
+  }
+  cudaSetDevice(g->device);
+  // members' tables, parameters and step numbers
+  g->h_gm.assign(nm, GroupMember{});
+  for (int i = 0; i < nm; i++) {
+    qmcb_handle *h = g->mem[i];
+    GroupMember &G = g->h_gm[i];
+    G.S = h->sys;
+    G.L = h->lay;
+    G.cfg = make_cfg(h->params);
+    G.state = h->d_state;
+    G.live = h->d_live;
+    G.live_tmp = h->d_live_tmp;
+    G.free_stack = h->d_free;
+    G.ctl = h->d_ctl;
+    G.copies = h->d_copies;
+    G.ectl = h->d_ectl;
+    G.stats = h->d_stats;
+    G.step0 = first_steps[g->user[i]];
+    G.reweight_start = h->params.reweight_start_step;
+    G.dmc = h->params.run_type == QMCB_DMC;
+    G.limit_branching = h->params.limit_branching;
+    G.thr_split = h->params.branching_threshold;
+    G.thr_fuse = h->params.fusion_threshold;
+  }
+  cudaStream_t st = g->stream;
+  // the members' own streams finish first (their last evaluate or copy)
+  for (auto *h : g->mem) GK(cudaStreamSynchronize(h->stream));
+  GK(cudaMemcpyAsync(g->d_gm, g->h_gm.data(), sizeof(GroupMember) * nm, cudaMemcpyHostToDevice, st));
+  for (auto *h : g->mem) GK(cudaMemsetAsync(h->d_stats, 0, sizeof(double) * ST_RUN_SUM_W, st));
+  // configuration: the tuned one, else the next one not yet timed
+  int c = g->chosen;
+  if (c < 0)
+    for (size_t k = 0; k < g->cost.size(); k++)
+      if (g->cost[k] < 0) {
+        c = (int)k;
+        break;
+      }
+  GK(cudaEventRecord(g->ev0, st));
+  if (!refresh && n_steps > 0) {
+    if (!(g->gexec && g->g_steps == n_steps && g->g_config == c)) {
+      if (g->gexec) {
+        cudaGraphExecDestroy(g->gexec);
+        g->gexec = nullptr;
+      }
+      cudaGraph_t graph = nullptr;
+      GK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      int rc = group_enqueue(g, c, n_steps, first_steps, false);
+      cudaError_t ec = cudaStreamEndCapture(st, &graph);
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      if (ec != cudaSuccess) return gfail(g, QMCB_E_CUDA, std::string("qmcb_group_run_steps: capture: ") + cudaGetErrorString(ec));
+      ec = cudaGraphInstantiate(&g->gexec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ec != cudaSuccess) {
+        g->gexec = nullptr;
+        return gfail(g, QMCB_E_CUDA, std::string("qmcb_group_run_steps: instantiate: ") + cudaGetErrorString(ec));
+      }
+      g->g_steps = n_steps;
+      g->g_config = c;
+    }
+    GK(cudaGraphLaunch(g->gexec, st));
+  } else {
+    int rc = group_enqueue(g, c, n_steps, first_steps, refresh);
+    if (rc) return rc;
+  }
+  GK(cudaEventRecord(g->ev1, st));
+  for (auto *h : g->mem) {
+    GK(cudaMemcpyAsync(h->h_stats, h->d_stats, sizeof(double) * ST_COUNT, cudaMemcpyDeviceToHost, st));
+    GK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  }
+  GK(cudaStreamSynchronize(st));
+  g->last = c;
+  double moves = 0.0;
+  for (int i = 0; i < nm; i++) {
+    qmcb_handle *h = g->mem[i];
+    const double *sv = h->h_stats;
+    h->n_live_host = h->h_ctl[0];
+    moves += sv[ST_MOVES];
+    if (stats) {
+      qmcb_step_stats &s = stats[g->user[i]];
+      s.sum_weight = sv[ST_SUM_W];
+      s.sum_weight_energy = sv[ST_SUM_WE];
+      s.sum_weight_energy2 = sv[ST_SUM_WE2];
+      s.sum_accept = sv[ST_SUM_ACC];
+      s.n_moves = sv[ST_MOVES];
+      s.final_weight = sv[ST_FINAL_W];
+      s.n_walkers = h->h_ctl[0];
+      s.n_singular = (int)sv[ST_SINGULAR];
+    }
+  }
+  if (g->chosen < 0 && moves > 0) {
+    float ms = 0.0f;
+    GK(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+    g->cost[c] = ms / moves;
+    bool done = true;
+    for (double v : g->cost) done &= v >= 0;
+    if (done) g->chosen = (int)(std::min_element(g->cost.begin(), g->cost.end()) - g->cost.begin());
+  }
+  return QMCB_OK;
+}
+
+int qmcb_group_config(const qmcb_group *g, int *n_configs, int *chosen, int *last, int *n_buckets, int *wpb)
+{
+  if (!g) return QMCB_E_ARG;
+  if (n_configs) *n_configs = (int)g->cands.size();
+  if (chosen) *chosen = g->chosen;
+  if (last) *last = g->last;
+  const int c = g->last >= 0 ? g->last : (g->chosen >= 0 ? g->chosen : 0);
+  if (n_buckets) *n_buckets = (int)g->cands[c].size();
+  if (wpb) *wpb = g->cands[c].empty() ? 0 : g->cands[c][0].wpb;
+  return QMCB_OK;
+}
+
+int qmcb_group_set_config(qmcb_group *g, int config)
+{
+  if (!g) return QMCB_E_ARG;
+  if (config < -1 || config >= (int)g->cands.size()) return gfail(g, QMCB_E_ARG, "qmcb_group_set_config: no such configuration");
+  if (config == -1) {
+    g->cost.assign(g->cands.size(), -1.0);
+    g->chosen = -1;
+  } else {
+    g->chosen = config;
+  }
   return QMCB_OK;
 }
 

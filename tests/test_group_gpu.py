@@ -1,0 +1,149 @@
+"""Groups (qmcb_group_*): the walkers of several systems of different sizes
+stepped by one persistent launch per bucket.  Each member must follow
+exactly the chain it follows when its own handle steps it (same random
+streams, same arithmetic), whatever launch configuration the tuner tries."""
+import numpy as np
+import pytest
+
+from qmcbeaver_b200.api import QMCB200Functions, QMCB200Group, QMCBError
+from qmcbeaver_b200.desc import (QMCB_DMC, QMCB_ECUT_BDJM_PUSH88, QMCB_EMOD_UMRIGAR93, QMCB_IMPORTANCE_SAMPLING,
+                                 QMCB_PREC_MIXED, QMCB_QF_UMRIGAR93_UNEQUAL, QMCB_UMRIGAR93_IMPORTANCE_SAMPLING,
+                                 run_params)
+from qmcbeaver_b200.system import make_random_molecule, with_determinants, with_three_body
+
+pytestmark = pytest.mark.gpu
+
+# (electrons, nuclei, basis functions, walkers): uneven sizes, as in a
+# batch of serving jobs
+SIZES = [(4, 1, 16, 300), (30, 6, 120, 700), (10, 2, 40, 513), (56, 10, 224, 260), (18, 3, 72, 900)]
+
+
+def _systems(extra_threebody=False):
+    out = []
+    for k, (ne, nn, nb, w) in enumerate(SIZES):
+        s = make_random_molecule(ne, nn, nb, 5.0 + ne / 10, (1, 6, 7, 8), seed=10 + k)
+        if extra_threebody and k == 2:
+            s = with_three_body(s, seed=3)
+        out.append((s, w))
+    return out
+
+
+def _params(k, sampling=QMCB_IMPORTANCE_SAMPLING):
+    return run_params(sampling=sampling, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01, seed=100 + k,
+                      rel_cutoff=0.0)
+
+
+def _dmc_params(k, e0):
+    # DMC with the Umrigar93 energy modification and the BDJM cutoff around
+    # the initial mean local energy, a full refresh every 25 steps (so the
+    # group takes its launch-by-launch path, not the graph)
+    return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
+                      energy_modification=QMCB_EMOD_UMRIGAR93, energy_cutoff=QMCB_ECUT_BDJM_PUSH88, dt=0.01,
+                      refresh_interval=25, energy_trial=e0, energy_estimated=e0, energy_original=e0,
+                      population_control=100.0, seed=200 + k, rel_cutoff=0.0)
+
+
+def _handles(systems, params):
+    hs = []
+    for k, (s, w) in enumerate(systems):
+        f = QMCB200Functions(s, 2 * w, params(k))
+        f.init_walkers(s.initial_positions(w, seed=k + 1))
+        hs.append(f)
+    return hs
+
+
+def _first_steps(systems):
+    # members start at different points of their own step sequences
+    return [3 * k + 1 for k in range(len(systems))]
+
+
+@pytest.mark.parametrize("extras", [False, True])
+def test_vmc_group_matches_members_alone(extras):
+    systems = _systems(extra_threebody=extras)
+    sampling = QMCB_UMRIGAR93_IMPORTANCE_SAMPLING if extras else QMCB_IMPORTANCE_SAMPLING
+
+    def params(k):
+        return _params(k, sampling=sampling if k in (0, 2) else QMCB_IMPORTANCE_SAMPLING)
+
+    solo, grouped = _handles(systems, params), _handles(systems, params)
+    g = QMCB200Group(grouped)
+    fs = _first_steps(systems)
+    n_batches, n_steps = 7, 13
+    cfg = g.config()
+    assert cfg["n_configs"] >= 2
+    for b in range(n_batches):
+        st_g = g.run_steps([f + b * n_steps for f in fs], n_steps)
+        for k, f in enumerate(solo):
+            st = f.run_steps(fs[k] + b * n_steps, n_steps)
+            assert st.n_moves == st_g[k].n_moves
+            assert st_g[k].sum_weight_energy == pytest.approx(st.sum_weight_energy, rel=1e-12, abs=1e-9)
+            assert st_g[k].sum_accept == pytest.approx(st.sum_accept, rel=1e-12)
+    # every candidate configuration was timed, the fastest kept
+    cfg = g.config()
+    assert cfg["chosen"] >= 0 and cfg["last"] == cfg["chosen"]
+    for a, b in zip(solo, grouped):
+        wa, wb = a.get_walkers(), b.get_walkers()
+        assert np.array_equal(wa["R"], wb["R"])
+        assert np.allclose(wa["e_local"], wb["e_local"], rtol=1e-12, atol=1e-12)
+
+
+def test_every_configuration_gives_the_same_chain():
+    systems = _systems()
+    ref = _handles(systems, _params)
+    fs = _first_steps(systems)
+    for k, f in enumerate(ref):
+        f.run_steps(fs[k], 20)
+    want = [f.get_walkers()["R"] for f in ref]
+    probe = _handles(systems, _params)
+    n = QMCB200Group(probe).config()["n_configs"]
+    for c in range(n):
+        hs = _handles(systems, _params)
+        g = QMCB200Group(hs)
+        g.set_config(c)
+        g.run_steps(fs, 20)
+        assert g.config()["last"] == c
+        for w, h in zip(want, hs):
+            assert np.array_equal(w, h.get_walkers()["R"])
+
+
+def test_dmc_group_branches_like_members_alone():
+    systems = _systems()
+    e0 = []
+    for k, f in enumerate(_handles(systems, _params)):
+        e0.append(float(np.median(f.get_walkers()["e_local"])))
+
+    def params(k):
+        return _dmc_params(k, e0[k])
+
+    solo, grouped = _handles(systems, params), _handles(systems, params)
+    g = QMCB200Group(grouped)
+    fs = [0] * len(systems)
+    # two batches: every member branches at least once (steps that move
+    # electron 0); the trial energies feed back through device sums
+    for b in range(2):
+        n_steps = 60
+        st_g = g.run_steps([f + b * n_steps for f in fs], n_steps)
+        for k, f in enumerate(solo):
+            st = f.run_steps(fs[k] + b * n_steps, n_steps)
+            assert st_g[k].n_walkers == st.n_walkers
+            assert st_g[k].final_weight == pytest.approx(st.final_weight, rel=1e-9)
+            assert st_g[k].sum_weight_energy == pytest.approx(st.sum_weight_energy, rel=1e-9)
+    for a, b in zip(solo, grouped):
+        wa, wb = a.get_walkers(), b.get_walkers()
+        assert np.array_equal(wa["R"], wb["R"])
+        assert np.allclose(wa["weight"], wb["weight"], rtol=1e-9)
+
+
+def test_group_refuses_unsupported_members():
+    s = make_random_molecule(8, 2, 32, 5.0, (1, 6, 7, 8), seed=4)
+    md = with_determinants(s, 3, 2, seed=1)
+    a = QMCB200Functions(s, 64, _params(0))
+    b = QMCB200Functions(md, 64, _params(1))
+    with pytest.raises(QMCBError, match="several determinants"):
+        QMCB200Group([a, b])
+    c = QMCB200Functions(s, 64, run_params(precision=QMCB_PREC_MIXED, dt=0.01))
+    c.init_walkers(s.initial_positions(32, seed=1))
+    a.init_walkers(s.initial_positions(32, seed=2))
+    g = QMCB200Group([a, c])
+    with pytest.raises(QMCBError, match="FP64"):
+        g.run_steps(0, 4)
