@@ -263,6 +263,75 @@ def serving_section(args):
             "same_results_alone_and_mixed": bool(same)}
 
 
+def batching_section(args):
+    """The uneven-batching workload: 64 synthetic molecules, even electron
+    counts uniform in 4-200, basis 4N, N/5 nuclei with Z in {1, 6, 7, 8},
+    orthonormalised random orbital coefficients;
+    walkers per molecule uniform in 256-2048 (the workload's 256-8192
+    capped at 2048 so that all 64 walker populations fit in HBM together:
+    this layout keeps every walker's orbital rows, derivative rows and
+    inverses resident, 24 n^2 doubles for n electrons per spin).  VMC
+    importance-sampled steps, 100 per batch.  One group (persistent launches
+    per bucket, configuration tuned on the first batches, batches replayed
+    as CUDA graphs) against the same steps run handle after handle and on
+    all handles' streams at once.  Wall-clock walker-moves/s around
+    synchronous batches."""
+    from qmcbeaver_b200.api import QMCB200Functions, QMCB200Group
+    from qmcbeaver_b200.desc import QMCB_IMPORTANCE_SAMPLING, QMCB_QF_UMRIGAR93_UNEQUAL, run_params
+    from qmcbeaver_b200.serving import make_jobs
+    jobs = make_jobs(64, rate=1.0, seed=23, electrons=(4, 200), walkers=(256, 2048), orbitals="random")
+    hs = []
+    for j in jobs:
+        p = run_params(sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01,
+                       seed=j.seed, rel_cutoff=0.0)
+        f = QMCB200Functions(j.system, j.walkers, p)
+        f.init_walkers(j.system.initial_positions(j.walkers, seed=j.seed))
+        hs.append(f)
+    B, timed = 100, 2
+    g = QMCB200Group(hs)
+    step = 0
+    tune_t0 = time.perf_counter()
+    while g.config()["chosen"] < 0:
+        g.run_steps(step, B)
+        step += B
+    tune_s = time.perf_counter() - tune_t0
+
+    def timed_run(run_batch):
+        nonlocal step
+        moves = 0.0
+        t0 = time.perf_counter()
+        for _ in range(timed):
+            moves += run_batch(step)
+            step += B
+        return moves / (time.perf_counter() - t0)
+
+    def grouped(s0):
+        return sum(st.n_moves for st in g.run_steps(s0, B))
+
+    def one_by_one(s0):
+        return sum(f.run_steps(s0, B).n_moves for f in hs)
+
+    def streams(s0):
+        for f in hs:
+            f.run_steps_async(s0, B)
+        return sum(f.steps_collect().n_moves for f in hs)
+
+    r_group = timed_run(grouped)
+    r_seq = timed_run(one_by_one)
+    r_streams = timed_run(streams)
+    cfg = g.config()
+    g.close()
+    for f in hs:
+        f.close()
+    ne = [j.system.n_electrons for j in jobs]
+    return {"molecules": len(jobs), "electrons": [min(ne), max(ne)], "walkers": sum(j.walkers for j in jobs),
+            "steps_per_batch": B, "timed_batches": timed, "unit": "walker-moves/s",
+            "group": r_group, "one_handle_after_another": r_seq, "concurrent_streams": r_streams,
+            "group_speedup_vs_sequential": r_group / r_seq, "group_speedup_vs_streams": r_group / r_streams,
+            "tuning": {"configurations": cfg["n_configs"], "chosen": cfg["chosen"], "buckets": cfg["n_buckets"],
+                       "warps_per_block": cfg["warps_per_block"], "tuning_batches_s": tune_s}}
+
+
 def run_reference_arm(args, rank: int):
     if rank != 0:
         return
@@ -455,6 +524,7 @@ def main():
         out["rows"] = rows_section(args, rank)
         if world == 1:
             out["serving"] = serving_section(args)
+            out["batching"] = batching_section(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_sample(system, walkers=64, steps=1500, procs=os.cpu_count() or 1, e0=E_GUESS)
         if r is not None:

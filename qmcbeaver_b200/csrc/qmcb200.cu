@@ -1417,6 +1417,9 @@ struct qmcb_group {
   int chosen = -1;                         // the tuned configuration
   int last = -1;                           // configuration of the last batch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t fork_ev = nullptr;
+  std::vector<cudaStream_t> side;  // one stream per bucket
+  std::vector<cudaEvent_t> side_ev;
   cudaGraphExec_t gexec = nullptr;  // the last batch's launch sequence
   int g_steps = -1, g_config = -1;
   std::string err;
@@ -1457,31 +1460,25 @@ static int bucket_grid(qmcb_group *g, bool extras, int stride, int wpb, int *gri
 }
 
 // The configurations the tuner tries: members in runs of equal extras flag,
-// each run as one bucket or split at its one or two largest jumps in
-// scratch size; 4 or 2 warps per block.
+// each run one bucket or cut into size classes whose per-warp scratch stays
+// within a factor 2 or 1.4 of the class's smallest; 4 or 2 warps per block
+// (fewer where one block could not hold them).
 static int build_candidates(qmcb_group *g)
 {
   const int n = (int)g->mem.size();
-  std::vector<int> cuts;  // run boundaries (extras flag changes)
-  for (int i = 1; i < n; i++)
-    if (member_extras(g->mem[i]) != member_extras(g->mem[i - 1])) cuts.push_back(i);
-  // largest relative jumps of the scratch size inside runs
-  std::vector<std::pair<double, int>> jumps;
-  for (int i = 1; i < n; i++) {
-    if (std::find(cuts.begin(), cuts.end(), i) != cuts.end()) continue;
-    const double r = (double)g->mem[i]->lay.mv_stride / g->mem[i - 1]->lay.mv_stride;
-    if (r > 1.0) jumps.push_back({r, i});
-  }
-  std::sort(jumps.begin(), jumps.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
-    return a.first > b.first;
-  });
   std::vector<std::vector<int>> splits;
-  splits.push_back(cuts);
-  for (int k = 1; k <= 2 && k <= (int)jumps.size(); k++) {
-    std::vector<int> c = cuts;
-    for (int j = 0; j < k; j++) c.push_back(jumps[j].second);
-    std::sort(c.begin(), c.end());
-    splits.push_back(c);
+  for (double ratio : {0.0, 2.0, 1.4}) {
+    std::vector<int> c;
+    int lo = 0;
+    for (int i = 1; i < n; i++) {
+      const bool run_end = member_extras(g->mem[i]) != member_extras(g->mem[i - 1]);
+      const bool class_end = ratio > 0 && g->mem[i]->lay.mv_stride > ratio * g->mem[lo]->lay.mv_stride;
+      if (run_end || class_end) {
+        c.push_back(i);
+        lo = i;
+      }
+    }
+    if (std::find(splits.begin(), splits.end(), c) == splits.end()) splits.push_back(c);
   }
   g->cands.clear();
   for (const auto &c : splits)
@@ -1496,10 +1493,17 @@ static int build_candidates(qmcb_group *g)
         b.count = hi - lo;
         b.extras = member_extras(g->mem[lo]);
         b.stride = 0;
-        for (int i = lo; i < hi; i++) b.stride = std::max(b.stride, g->mem[i]->lay.mv_stride);
+        long long walkers = 0;
+        for (int i = lo; i < hi; i++) {
+          b.stride = std::max(b.stride, g->mem[i]->lay.mv_stride);
+          walkers += g->mem[i]->max_walkers;
+        }
         b.wpb = std::max(1, std::min<int>(wpb, g->max_optin / (int)(sizeof(double) * b.stride)));
         int rc = bucket_grid(g, b.extras, b.stride, b.wpb, &b.grid);
         if (rc) return rc;
+        // no more warps than the bucket has walkers, so that concurrent
+        // buckets leave each other room on the SMs
+        b.grid = (int)std::min<long long>(b.grid, (walkers + b.wpb - 1) / b.wpb);
         bs.push_back(b);
         lo = hi;
       }
@@ -1507,46 +1511,61 @@ static int build_candidates(qmcb_group *g)
     }
   g->cost.assign(g->cands.size(), -1.0);
   g->chosen = g->cands.size() == 1 ? 0 : -1;
+  size_t nb = 0;
+  for (const auto &bs : g->cands) nb = std::max(nb, bs.size());
+  while (g->side.size() < nb) {
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t e2 = nullptr;
+    GK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    g->side.push_back(s2);
+    GK(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+    g->side_ev.push_back(e2);
+  }
   return QMCB_OK;
 }
 
 // The launches of n_steps steps in configuration c (graph capturable when
-// no member refreshes).
+// no member refreshes).  Buckets are independent (a member's step depends
+// only on its own previous step), so each runs all its steps on a stream of
+// its own, forked from and joined back into the group stream.
 static int group_enqueue(qmcb_group *g, int c, int n_steps, const int *first_steps, bool refresh)
 {
   cudaStream_t st = g->stream;
-  const int nm = (int)g->mem.size();
-  bool any_dmc = false;
-  for (auto *h : g->mem) any_dmc |= h->params.run_type == QMCB_DMC;
-  for (int t = 0; t < n_steps; t++) {
-    const auto &bs = g->cands[c];
-    for (size_t b = 0; b < bs.size(); b++) {
-      const auto &B = bs[b];
-      GK(cudaMemsetAsync(g->d_counter + b, 0, sizeof(int), st));
-      const size_t smem = sizeof(double) * (size_t)B.stride * B.wpb;
+  const auto &bs = g->cands[c];
+  GK(cudaEventRecord(g->fork_ev, st));
+  for (size_t b = 0; b < bs.size(); b++) {
+    const auto &B = bs[b];
+    cudaStream_t sb = g->side[b];
+    GK(cudaStreamWaitEvent(sb, g->fork_ev, 0));
+    bool dmc = false;
+    for (int i = B.first; i < B.first + B.count; i++) dmc |= g->mem[i]->params.run_type == QMCB_DMC;
+    const GroupMember *gm = g->d_gm + B.first;
+    const size_t smem = sizeof(double) * (size_t)B.stride * B.wpb;
+    for (int t = 0; t < n_steps; t++) {
+      GK(cudaMemsetAsync(g->d_counter + b, 0, sizeof(int), sb));
       if (B.extras)
-        k_move_group<true><<<B.grid, 32 * B.wpb, smem, st>>>(g->d_gm + B.first, B.count, t, B.stride,
-                                                             g->d_counter + b);
+        k_move_group<true><<<B.grid, 32 * B.wpb, smem, sb>>>(gm, B.count, t, B.stride, g->d_counter + b);
       else
-        k_move_group<false><<<B.grid, 32 * B.wpb, smem, st>>>(g->d_gm + B.first, B.count, t, B.stride,
-                                                              g->d_counter + b);
-    }
-    if (any_dmc) {
-      k_branch_group<<<nm, 1024, 0, st>>>(g->d_gm, t);
-      k_copy_group<<<dim3(64, nm), 256, 0, st>>>(g->d_gm, t);
-      k_energy_group<<<(nm + 127) / 128, 128, 0, st>>>(g->d_gm, nm, t);
-    }
-    if (refresh) {
-      for (int i = 0; i < nm; i++) {
-        qmcb_handle *h = g->mem[i];
-        const int step = first_steps[g->user[i]] + t;
-        if (h->params.refresh_interval > 0 && (step + 1) % h->params.refresh_interval == 0) {
-          EvalOut o2{};
-          const int blocks_full = (h->max_walkers + h->wpb_full - 1) / h->wpb_full;
-          launch_full(h, blocks_full, st, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, 0, o2);
+        k_move_group<false><<<B.grid, 32 * B.wpb, smem, sb>>>(gm, B.count, t, B.stride, g->d_counter + b);
+      if (dmc) {
+        k_branch_group<<<B.count, 1024, 0, sb>>>(gm, t);
+        k_copy_group<<<dim3(64, B.count), 256, 0, sb>>>(gm, t);
+        k_energy_group<<<(B.count + 127) / 128, 128, 0, sb>>>(gm, B.count, t);
+      }
+      if (refresh) {
+        for (int i = B.first; i < B.first + B.count; i++) {
+          qmcb_handle *h = g->mem[i];
+          const int step = first_steps[g->user[i]] + t;
+          if (h->params.refresh_interval > 0 && (step + 1) % h->params.refresh_interval == 0) {
+            EvalOut o2{};
+            const int blocks_full = (h->max_walkers + h->wpb_full - 1) / h->wpb_full;
+            launch_full(h, blocks_full, sb, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, 0, o2);
+          }
         }
       }
     }
+    GK(cudaEventRecord(g->side_ev[b], sb));
+    GK(cudaStreamWaitEvent(st, g->side_ev[b], 0));
   }
   GK(cudaGetLastError());
   return QMCB_OK;
@@ -1592,6 +1611,7 @@ int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out)
   if (e == cudaSuccess) e = cudaMalloc(&g->d_counter, sizeof(int) * (n + 1));
   if (e == cudaSuccess) e = cudaEventCreate(&g->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&g->ev1);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork_ev, cudaEventDisableTiming);
   // the group kernels hold the member prefix sums in static shared memory:
   // the dynamic part may use the rest of the opt-in maximum
   cudaFuncAttributes fa0{}, fa1{};
@@ -1622,6 +1642,12 @@ int qmcb_group_destroy(qmcb_group *g)
   if (g->d_counter) cudaFree(g->d_counter);
   if (g->ev0) cudaEventDestroy(g->ev0);
   if (g->ev1) cudaEventDestroy(g->ev1);
+  if (g->fork_ev) cudaEventDestroy(g->fork_ev);
+  for (cudaEvent_t e : g->side_ev) cudaEventDestroy(e);
+  for (cudaStream_t s2 : g->side) {
+    cudaStreamSynchronize(s2);
+    cudaStreamDestroy(s2);
+  }
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
   return QMCB_OK;

@@ -13,6 +13,12 @@ until the blocked standard error of the energy reaches the job's target.
 A job's random streams depend only on its own seed and walker slots, so its
 energies are the same whether it runs alone or in a mix (up to the
 summation order of the per-step ensemble sums).
+
+With ``mode="group"`` the admitted jobs are instead stepped together: one
+group (``qmcb_group_*``) over all active jobs runs a batch of
+``batch_steps`` steps of every job in one persistent launch per bucket per
+step, rebuilt whenever a job joins or leaves.  Each job's energy blocks
+are then its batches (the same whether it runs alone or in a mix).
 """
 from __future__ import annotations
 
@@ -23,7 +29,7 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-from .api import QMCB200Functions
+from .api import QMCB200Functions, QMCB200Group
 from .desc import QMCB_IMPORTANCE_SAMPLING, QMCB_PREC_FP64, QMCB_QF_UMRIGAR93_UNEQUAL, QMCB_VMC, run_params
 from .system import MolecularSystem, make_random_molecule
 
@@ -84,21 +90,44 @@ class Server:
     """Admits jobs in arrival order while the sum of their device footprints
     stays under `hbm_budget` bytes and at most `max_active` run at once."""
 
-    def __init__(self, hbm_budget: int = 40 << 30, max_active: int = 16):
+    def __init__(self, hbm_budget: int = 40 << 30, max_active: int = 16, mode: str = "streams",
+                 batch_steps: int = 64):
+        if mode not in ("streams", "group"):
+            raise ValueError(f"unknown serving mode {mode!r}")
         self.hbm_budget = int(hbm_budget)
         self.max_active = int(max_active)
+        self.mode = mode
+        self.batch_steps = int(batch_steps)
+
+    def _handle(self, job: Job) -> QMCB200Functions:
+        # the group path steps FP64 walkers and needs no refresh (a refresh
+        # is a per-member launch outside the captured batch)
+        p = run_params(run_type=QMCB_VMC, sampling=QMCB_IMPORTANCE_SAMPLING,
+                       qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=job.dt,
+                       refresh_interval=50 if self.mode == "streams" else 0,
+                       seed=job.seed, precision=job.precision, rel_cutoff=0.0)
+        f = QMCB200Functions(job.system, (2 if self.mode == "streams" else 1) * job.walkers, p)
+        f.init_walkers(job.system.initial_positions(job.walkers, seed=job.seed))
+        return f
 
     def _start(self, job: Job) -> Dict:
         N = job.system.n_electrons
-        p = run_params(run_type=QMCB_VMC, sampling=QMCB_IMPORTANCE_SAMPLING,
-                       qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=job.dt, refresh_interval=50,
-                       seed=job.seed, precision=job.precision, rel_cutoff=0.0)
-        f = QMCB200Functions(job.system, 2 * job.walkers, p)
-        f.init_walkers(job.system.initial_positions(job.walkers, seed=job.seed))
+        f = self._handle(job)
         f.run_steps_async(0, job.equil_sweeps * N)
         return {"f": f, "step": job.equil_sweeps * N, "phase": "equil", "N": N}
 
+    def _finish(self, j: Job, t0: float) -> None:
+        j.finished = time.perf_counter() - t0
+        j.energy = float(np.mean(j.energies))
+        j.error = blocked_error(j.energies)
+
+    def _done(self, j: Job) -> bool:
+        err = blocked_error(j.energies)
+        return (len(j.energies) >= j.min_blocks and err <= j.target_error) or len(j.energies) >= j.max_sweeps
+
     def run(self, jobs: Sequence[Job], poll_sleep: float = 0.0) -> Dict[str, object]:
+        if self.mode == "group":
+            return self._run_group(jobs)
         pending = sorted(jobs, key=lambda j: j.arrival)
         queue: List[Job] = []
         active: Dict[int, Dict] = {}
@@ -135,11 +164,8 @@ class Server:
                     total_moves += st.n_moves
                     if st.sum_weight > 0:
                         j.energies.append(st.sum_weight_energy / st.sum_weight)
-                    err = blocked_error(j.energies)
-                    if (len(j.energies) >= j.min_blocks and err <= j.target_error) or len(j.energies) >= j.max_sweeps:
-                        j.finished = time.perf_counter() - t0
-                        j.energy = float(np.mean(j.energies))
-                        j.error = err
+                    if self._done(j):
+                        self._finish(j, t0)
                         f.close()
                         used -= a["need"]
                         del active[jid]
@@ -149,7 +175,74 @@ class Server:
                 a["step"] += a["N"]
             if not progressed and poll_sleep > 0:
                 time.sleep(poll_sleep)
-        wall = time.perf_counter() - t0
+        return self._summary(done, total_moves, time.perf_counter() - t0)
+
+    def _run_group(self, jobs: Sequence[Job]) -> Dict[str, object]:
+        """Active jobs stepped together, batch_steps steps per batch; a job's
+        first ceil(equil_sweeps N / batch_steps) batches equilibrate."""
+        pending = sorted(jobs, key=lambda j: j.arrival)
+        queue: List[Job] = []
+        active: Dict[int, Dict] = {}
+        used = 0
+        t0 = time.perf_counter()
+        done: List[Job] = []
+        total_moves = 0.0
+        group = None
+        B = self.batch_steps
+        while pending or queue or active:
+            now = time.perf_counter() - t0
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.pop(0))
+            changed = False
+            while queue and len(active) < self.max_active:
+                j = queue[0]
+                need = state_footprint(j.system, j.walkers) // 2
+                if active and used + need > self.hbm_budget:
+                    break
+                queue.pop(0)
+                j.admitted = now
+                eq = -(-j.equil_sweeps * j.system.n_electrons // B)
+                active[j.job_id] = {"f": self._handle(j), "job": j, "need": need, "step": 0, "equil": eq}
+                used += need
+                changed = True
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
+                continue
+            if changed or group is None:
+                if group is not None:
+                    group.close()
+                order = list(active.keys())
+                group = QMCB200Group([active[k]["f"] for k in order])
+            stats = group.run_steps([active[k]["step"] for k in order], B)
+            for k, st in zip(order, stats):
+                a = active[k]
+                a["step"] += B
+                if a["equil"] > 0:
+                    a["equil"] -= 1
+                    continue
+                j = a["job"]
+                j.moves += st.n_moves
+                total_moves += st.n_moves
+                if st.sum_weight > 0:
+                    j.energies.append(st.sum_weight_energy / st.sum_weight)
+                if self._done(j):
+                    self._finish(j, t0)
+                    done.append(j)
+            finished = [k for k in order if active[k]["job"].finished is not None]
+            if finished:
+                group.close()
+                group = None
+                for k in finished:
+                    active[k]["f"].close()
+                    used -= active[k]["need"]
+                    del active[k]
+        if group is not None:
+            group.close()
+        return self._summary(done, total_moves, time.perf_counter() - t0)
+
+    @staticmethod
+    def _summary(done: List[Job], total_moves: float, wall: float) -> Dict[str, object]:
         lat = np.array([j.latency for j in done])
         return {"jobs": len(done), "wall_s": wall, "walker_moves": total_moves,
                 "walker_moves_per_s": total_moves / wall if wall > 0 else 0.0,
@@ -159,11 +252,13 @@ class Server:
 
 
 def make_jobs(n_jobs: int, rate: float, seed: int = 1, electrons=(4, 40), walkers=(256, 2048),
-              target_error: float = 0.2, max_sweeps: int = 400, precision: int = QMCB_PREC_FP64) -> List[Job]:
+              target_error: float = 0.2, max_sweeps: int = 400, precision: int = QMCB_PREC_FP64,
+              orbitals: str = "core") -> List[Job]:
     """Poisson arrivals at `rate` jobs/s of synthetic molecules drawn like the
     uneven-batching workload: even electron count uniform in `electrons`,
     basis size 4 N, N/5 nuclei with Z in {1, 6, 7, 8}, walkers uniform in
-    `walkers`."""
+    `walkers`; orbitals "core" (approximate core-Hamiltonian orbitals) or
+    "random" (orthonormalised random coefficients, cheap for large bases)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     jobs = []
@@ -173,7 +268,7 @@ def make_jobs(n_jobs: int, rate: float, seed: int = 1, electrons=(4, 40), walker
         nn = max(1, ne // 5)
         box = 2.0 + 1.5 * nn ** (1.0 / 3.0) * 2.0
         sysm = make_random_molecule(ne, nn, 4 * ne, box, (1, 6, 7, 8), seed=seed * 1000 + i,
-                                    min_sep=1.4, name=f"job{i}-{ne}e")
+                                    min_sep=1.4, name=f"job{i}-{ne}e", orbitals=orbitals)
         W = int(rng.integers(walkers[0], walkers[1] + 1))
         jobs.append(Job(job_id=i, system=sysm, walkers=W, target_error=target_error, seed=seed * 7919 + i,
                         arrival=t, max_sweeps=max_sweeps, precision=precision))

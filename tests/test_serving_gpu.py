@@ -1,5 +1,6 @@
 """Serving loop: jobs admitted by device footprint, run concurrently (one
-stream per job), each job's energies the same alone and in the mix."""
+stream per job, or all active jobs stepped together as one group), each
+job's energies the same alone and in the mix."""
 import numpy as np
 import pytest
 
@@ -8,9 +9,10 @@ from qmcbeaver_b200.serving import Job, Server, blocked_error, make_jobs, state_
 pytestmark = pytest.mark.gpu
 
 
-def test_jobs_complete_and_report_latency():
+@pytest.mark.parametrize("mode", ["streams", "group"])
+def test_jobs_complete_and_report_latency(mode):
     jobs = make_jobs(6, rate=50.0, seed=3, electrons=(4, 20), walkers=(256, 512), target_error=0.5, max_sweeps=40)
-    out = Server(max_active=4).run(jobs)
+    out = Server(max_active=4, mode=mode, batch_steps=24).run(jobs)
     assert out["jobs"] == 6
     assert out["latency_p50_s"] is not None and out["latency_p99_s"] >= out["latency_p50_s"]
     for j in jobs:
@@ -18,16 +20,17 @@ def test_jobs_complete_and_report_latency():
         assert len(j.energies) >= j.min_blocks
 
 
-def test_result_same_alone_and_in_mix():
+@pytest.mark.parametrize("mode", ["streams", "group"])
+def test_result_same_alone_and_in_mix(mode):
     def fresh():
         js = make_jobs(5, rate=1e3, seed=5, electrons=(6, 16), walkers=(256, 512), target_error=0.0, max_sweeps=24)
         for j in js:
             j.arrival = 0.0
         return js
     mix = fresh()
-    Server(max_active=5).run(mix)
+    Server(max_active=5, mode=mode, batch_steps=16).run(mix)
     alone = fresh()[2]
-    Server(max_active=1).run([alone])
+    Server(max_active=1, mode=mode, batch_steps=16).run([alone])
     assert len(alone.energies) == len(mix[2].energies) == 24
     np.testing.assert_allclose(alone.energies, mix[2].energies, rtol=1e-10, atol=0)
 
