@@ -316,6 +316,12 @@ int qmcb_group_config(const qmcb_group *g, int *n_configs, int *chosen, int *las
 /* Fix the configuration (0 .. n_configs - 1), or -1 to time them again. */
 int qmcb_group_set_config(qmcb_group *g, int config);
 
+/* Layout choice at qmcb_create: spins of more than 16 electrons keep their
+ * inverse in device memory (two copies per walker and spin) instead of
+ * staging it in the move kernel's shared memory; the environment variable
+ * QMCB_STAGED_INVERSE_MAX, read by qmcb_create, moves that threshold.  Both
+ * layouts compute the same numbers. */
+
 /* Device bytes of the walker state of a handle (admission control). */
 size_t qmcb_state_bytes(const qmcb_handle *h);
 

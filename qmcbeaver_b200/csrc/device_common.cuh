@@ -43,6 +43,8 @@ enum Sc {
   SC_DW,           // weight factor of the last reweight
   SC_MDCUR_A,      // several determinants: current copy (0/1) of the spin's determinant block
   SC_MDCUR_B,
+  SC_INVCUR_A,     // inverse kept in HBM (large spins): current copy (0/1) of the spin's inverse
+  SC_INVCUR_B,
   SC_COUNT
 };
 constexpr int kScalars = 24;  // padded
@@ -110,6 +112,7 @@ struct Layout {
   int mgrad;     // [N][3] modifiedGradPsiRatio
   int sc;        // [kScalars]
   int mdsz[2];   // several determinants: doubles in one copy of the determinant block
+  int invsz[2];  // inverse kept in HBM: offset of its second copy (0: one copy, staged in shared memory)
   // move-kernel scratch (doubles, even counts): region A, rows, factors,
   // staged positions, staged per-electron tail, staged spin block, stride
   int mv_region_a, mv_dn, mv_valc, mv_r, mv_tail, mv_spin[2], mv_stride;

@@ -396,6 +396,7 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
       sc[SC_LAPR_A + sp] = lp;
       sc[SC_LOGDET_A + sp] = logdet;
       sc[SC_SIGN_A + sp] = sign;
+      sc[SC_INVCUR_A + sp] = 0.0;  // the inverse was written to its first copy
     }
     __syncwarp();
   }
@@ -928,7 +929,11 @@ __device__ __forceinline__ void write_eval_out(const EvalOut &out, int wi, int N
 // move_walker is the work of one warp on walker wi of the list (sm: the
 // warp's L.mv_stride doubles of shared memory); k_move runs it for one
 // system, k_move_group for the walkers of many systems in one launch.
-template <bool kMetropolis, typename TS, typename TI, bool kExtras>
+//
+// kGInv: the moved spin's inverse stays in HBM (large spins, whose inverse
+// would crowd shared memory): the update reads the current copy and writes
+// the other one, and acceptance flips which copy is current.
+template <bool kMetropolis, typename TS, typename TI, bool kExtras, bool kGInv>
 __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, const RunCfg &cfg, double *state,
                                             const int *slots, int wi, double *sm, const double *R_in,
                                             const MoveArgs &mv, const EnergyCtl *ectl, double *stats,
@@ -960,7 +965,6 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   const double *sc0 = sT + (L.sc - L.gradD);
   const TS *DgT = (const TS *)(blk + L.DgT[sp]);  // read once per move by the ratio sums
   const TS *DlT = (const TS *)(blk + L.DlT[sp]);
-  TI *Inv = (TI *)sS;
   double *sc = blk + L.sc;
   const int inv_d = even((n * n * (int)sizeof(TI) + 7) / 8);
 
@@ -970,10 +974,15 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   warp_copy_async(sR, blk + L.R, L.mv_r);
   warp_copy_async(sT, blk + L.gradD, L.mv_tail);
   cp_async_commit();
-  warp_copy_async(sS, blk + L.Inv[sp], inv_d);
+  if (!kGInv) warp_copy_async(sS, blk + L.Inv[sp], inv_d);
   cp_async_commit();
   cp_async_wait<1>();
   __syncwarp();
+  // the inverse the update reads (InvO) and the one it leaves (Inv): the
+  // staged copy updated in place, or the spin's two copies in HBM
+  const int icur = kGInv ? (int)sc0[SC_INVCUR_A + sp] : 0;
+  const TI *InvO = kGInv ? (const TI *)(blk + L.Inv[sp] + icur * L.invsz[sp]) : (const TI *)sS;
+  TI *Inv = kGInv ? (TI *)(blk + L.Inv[sp] + (1 - icur) * L.invsz[sp]) : (TI *)sS;
 
   const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3], g_fwd, u_acc;
@@ -1009,18 +1018,52 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   // determinant ratio accumulated in FP64; the inverse update itself runs
   // in the state precision TS
   double rpart = 0.0;
-  for (int o = lane; o < n; o += 32) rpart = fma((double)Dn[o], (double)Inv[o * n + el], rpart);
+  for (int o = lane; o < n; o += 32) rpart = fma((double)Dn[o], (double)InvO[o * n + el], rpart);
   const double ratio = warp_sum(rpart);
   bool bad = !(ratio != 0.0) || !isfinite(ratio);
   const double q = 1.0 / ratio;
   for (int c = lane; c < n; c += 32) {
     if (c == el) continue;
     TI val = (TI)0;
-    for (int l = 0; l < n; l++) val = fma((TI)Dn[l], Inv[l * n + c], val);
+    if (kGInv) {
+      // HBM / L2 operands: four loads in flight before their FMAs
+      int l = 0;
+      for (; l + 4 <= n; l += 4) {
+        TI v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) v[u] = InvO[(l + u) * n + c];
+#pragma unroll
+        for (int u = 0; u < 4; u++) val = fma((TI)Dn[l + u], v[u], val);
+      }
+      for (; l < n; l++) val = fma((TI)Dn[l], InvO[l * n + c], val);
+    } else {
+      for (int l = 0; l < n; l++) val = fma((TI)Dn[l], Inv[l * n + c], val);
+    }
     valc[c] = (TI)(val * q);
   }
   __syncwarp();
-  if (n <= 32) {
+  if (kGInv) {
+    // the same element formulas as the in-place update, old copy -> new
+    // copy, four rows' loads in flight at a time
+    for (int c = lane; c < n; c += 32) {
+      const TI vc = c == el ? (TI)0 : valc[c];
+      int r = 0;
+      for (; r + 4 <= n; r += 4) {
+        TI ie[4], x[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          ie[u] = InvO[(r + u) * n + el];
+          x[u] = InvO[(r + u) * n + c];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) Inv[(r + u) * n + c] = c == el ? (TI)(ie[u] * q) : x[u] - vc * ie[u];
+      }
+      for (; r < n; r++) {
+        const TI ie = InvO[r * n + el];
+        Inv[r * n + c] = c == el ? (TI)(ie * q) : InvO[r * n + c] - vc * ie;
+      }
+    }
+  } else if (n <= 32) {
     const int rpp = 32 / n, r0 = lane / n, c = lane - r0 * n;
     if (r0 < rpp && c != el) {
       const TI vc = valc[c];
@@ -1034,7 +1077,8 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
     }
   }
   __syncwarp();
-  for (int r = lane; r < n; r += 32) Inv[r * n + el] = (TI)(Inv[r * n + el] * q);
+  if (!kGInv)
+    for (int r = lane; r < n; r += 32) Inv[r * n + el] = (TI)(Inv[r * n + el] * q);
   __syncwarp();
 
   // ---- ratio sums of the moved spin (QMcBeaver/src/QMCSlater.cpp:741-762)
@@ -1147,8 +1191,12 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   if (accept) {
     double *Rw = blk + L.R;
     if (lane < 3) Rw[3 * e + lane] = rn[lane];
-    TI *InvW = (TI *)(blk + L.Inv[sp]);
-    for (int t = lane; t < n * n; t += 32) InvW[t] = Inv[t];
+    if (!kGInv) {
+      TI *InvW = (TI *)(blk + L.Inv[sp]);
+      for (int t = lane; t < n * n; t += 32) InvW[t] = Inv[t];
+    } else if (lane == 0) {
+      sc[SC_INVCUR_A + sp] = (double)(1 - icur);
+    }
     TS *Dv = (TS *)(blk + L.Dv[sp]), *DgW = (TS *)(blk + L.DgT[sp]), *DlW = (TS *)(blk + L.DlT[sp]);
     for (int o = lane; o < n; o += 32) {
       Dv[el * n + o] = Dn[o];
@@ -1189,7 +1237,7 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   }
 }
 
-template <bool kMetropolis, typename TS, typename TI, bool kExtras>
+template <bool kMetropolis, typename TS, typename TI, bool kExtras, bool kGInv>
 __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, MoveArgs mv,
                                               const EnergyCtl *ectl, double *stats, EvalOut out)
@@ -1199,8 +1247,8 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
   const int nw = d_num ? *d_num : num;
   const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
   if (wi >= nw) return;
-  move_walker<kMetropolis, TS, TI, kExtras>(S, L, cfg, state, slots, wi, smem + (size_t)warp * L.mv_stride, R_in,
-                                            mv, ectl, stats, out);
+  move_walker<kMetropolis, TS, TI, kExtras, kGInv>(S, L, cfg, state, slots, wi, smem + (size_t)warp * L.mv_stride,
+                                                   R_in, mv, ectl, stats, out);
 }
 
 // ------------------------------------------------------------------------

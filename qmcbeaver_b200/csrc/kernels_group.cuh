@@ -54,7 +54,7 @@ __device__ __forceinline__ int group_find(const int *prefix, int nm, int i)
 // One Metropolis / DMC step (step offset t) of every live walker of the
 // members gm[0..nm); stride: doubles of shared memory per warp (at least
 // every member's L.mv_stride); *counter is zero at launch.
-template <bool kExtras>
+template <bool kExtras, bool kGInv>
 __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__restrict__ gm, int nm, int t, int stride,
                                                     int *counter)
 {
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__rest
     mv.do_reweight = mv.e == 0;
     mv.reweight_on = mv.step >= G.reweight_start;
     mv.dump = nullptr;
-    move_walker<true, double, double, kExtras>(G.S, G.L, G.cfg, G.state, G.live, i - prefix[m], sm, nullptr, mv,
+    move_walker<true, double, double, kExtras, kGInv>(G.S, G.L, G.cfg, G.state, G.live, i - prefix[m], sm, nullptr, mv,
                                                G.ectl, G.stats, EvalOut{});
     __syncwarp();
   }

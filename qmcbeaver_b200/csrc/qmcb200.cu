@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -33,6 +34,7 @@ using namespace qmcb;
 namespace {
 
 const int kMaxWarpsPerBlock = 4;
+const int kStagedInverseMax = 16;  // largest spin whose inverse the move kernel stages in shared memory
 
 std::string g_create_error;
 
@@ -73,6 +75,7 @@ struct qmcb_handle {
   double *d_ci = nullptr;
   bool md = false;  // several determinants: the k_*_md kernels
   bool extras = false;  // cusp replacement or three-body terms: the k_move<..., true> instantiation
+  bool ginv = false;    // large spins: inverses in HBM, double-buffered (k_move<..., kGInv = true>)
   double *d_state = nullptr;
   int *d_live = nullptr, *d_live_tmp = nullptr, *d_free = nullptr, *d_ctl = nullptr;
   int2 *d_copies = nullptr;
@@ -362,6 +365,19 @@ void *g_noalloc_i_addr[64];
 
 // One launch of the single-determinant move kernel in the walker state's
 // precision, with the cusp / three-body code only when the system has them.
+template <bool kMetropolis, typename TS, typename TI, bool kExtras>
+static void launch_move_g(qmcb_handle *h, const dim3 &g, const dim3 &b, size_t sm, cudaStream_t st, const RunCfg &cfg,
+                          const int *slots, int num, const int *d_num, const double *R_in, const MoveArgs &mv,
+                          const EvalOut &o)
+{
+  if (h->ginv)
+    k_move<kMetropolis, TS, TI, kExtras, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+                                                                 R_in, mv, h->d_ectl, h->d_stats, o);
+  else
+    k_move<kMetropolis, TS, TI, kExtras, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+                                                                  R_in, mv, h->d_ectl, h->d_stats, o);
+}
+
 template <bool kMetropolis>
 static void launch_move(qmcb_handle *h, int blocks, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
                         const int *d_num, const double *R_in, MoveArgs mv, EvalOut o)
@@ -372,19 +388,27 @@ static void launch_move(qmcb_handle *h, int blocks, cudaStream_t st, const RunCf
   const bool extras = h->extras || (kMetropolis && cfg.sampling == QMCB_UMRIGAR93_IMPORTANCE_SAMPLING);
   if (h->params.precision == QMCB_PREC_MIXED) {
     if (extras)
-      k_move<kMetropolis, float, MIXED_TI, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
-                                                                   R_in, mv, h->d_ectl, h->d_stats, o);
+      launch_move_g<kMetropolis, float, MIXED_TI, true>(h, g, b, sm, st, cfg, slots, num, d_num, R_in, mv, o);
     else
-      k_move<kMetropolis, float, MIXED_TI, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
-                                                                    R_in, mv, h->d_ectl, h->d_stats, o);
+      launch_move_g<kMetropolis, float, MIXED_TI, false>(h, g, b, sm, st, cfg, slots, num, d_num, R_in, mv, o);
   } else {
     if (extras)
-      k_move<kMetropolis, double, double, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
-                                                                  R_in, mv, h->d_ectl, h->d_stats, o);
+      launch_move_g<kMetropolis, double, double, true>(h, g, b, sm, st, cfg, slots, num, d_num, R_in, mv, o);
     else
-      k_move<kMetropolis, double, double, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
-                                                                   R_in, mv, h->d_ectl, h->d_stats, o);
+      launch_move_g<kMetropolis, double, double, false>(h, g, b, sm, st, cfg, slots, num, d_num, R_in, mv, o);
   }
+}
+
+// The dynamic shared-memory limit of every move-kernel instantiation.
+template <bool kMetropolis, typename TS, typename TI>
+static cudaError_t move_smem_limits(int bytes)
+{
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move<kMetropolis, TS, TI, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move<kMetropolis, TS, TI, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move<kMetropolis, TS, TI, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move<kMetropolis, TS, TI, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
 }
 
 extern "C" {
@@ -793,6 +817,13 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
 
   // ---- per-walker block layout (offsets in doubles, arrays 32-byte aligned)
   Layout &L = h->lay;
+  // spins above kStagedInverseMax electrons keep their inverse in HBM: a
+  // staged n x n copy would cost the move kernel most of its occupancy
+  int staged_max = kStagedInverseMax;
+  if (const char *ev = getenv("QMCB_STAGED_INVERSE_MAX")) staged_max = atoi(ev);
+  const bool ginv = !md && h->nmax > staged_max;
+  h->ginv = ginv;
+  L.invsz[0] = L.invsz[1] = 0;
   int off = 0;
   auto take = [&](int count) {
     int o = off;
@@ -809,6 +840,11 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
       // two copies of [inverses | grad ratios | (ln|det|, sign, lap, singular)]
       L.mdsz[sp] = (S.ndet * n * n + S.ndet * 3 * n + S.ndet * 4 + 3) & ~3;
       L.Inv[sp] = take(2 * L.mdsz[sp]);
+    } else if (ginv) {
+      // two copies: the move reads one and writes the other
+      L.mdsz[sp] = 0;
+      L.invsz[sp] = (n * n + 3) & ~3;
+      L.Inv[sp] = take(2 * L.invsz[sp]);
     } else {
       L.mdsz[sp] = 0;
       L.Inv[sp] = take(n * n);
@@ -834,7 +870,7 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   L.mv_tail = even(L.sc + kScalars - L.gradD);
   for (int sp = 0; sp < 2; sp++) {
     int n = sp ? nb : na;
-    L.mv_spin[sp] = even(n * n);
+    L.mv_spin[sp] = ginv ? 0 : even(n * n);
   }
   L.mv_stride = L.mv_region_a + L.mv_dn + L.mv_valc + L.mv_r + L.mv_tail + std::max(L.mv_spin[0], L.mv_spin[1]) + 2;
   if (!md && (L.R + L.mv_r > L.stride || L.gradD + L.mv_tail > L.stride || L.Inv[0] + L.mv_spin[0] > L.stride ||
@@ -882,14 +918,10 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   // the dynamic shared-memory limit is a per-kernel, process-wide attribute:
   // raise it to the device maximum once, so handles of different systems
   // (each launching with its own size) never undercut one another
-  CKC(cudaFuncSetAttribute(k_move<true, double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<false, double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<true, float, MIXED_TI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<true, double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<false, double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<true, float, MIXED_TI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
-  CKC(cudaFuncSetAttribute(k_move<false, float, MIXED_TI, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  CKC((move_smem_limits<true, double, double>(max_optin)));
+  CKC((move_smem_limits<false, double, double>(max_optin)));
+  CKC((move_smem_limits<true, float, MIXED_TI>(max_optin)));
+  CKC((move_smem_limits<false, float, MIXED_TI>(max_optin)));
   CKC(cudaFuncSetAttribute(k_full<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_full<float, MIXED_TI, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_full<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
@@ -1410,7 +1442,7 @@ struct qmcb_group {
   int *d_counter = nullptr;  // one per bucket
   struct Bucket {
     int first, count, stride, wpb, grid;
-    bool extras;
+    bool extras, ginv;
   };
   std::vector<std::vector<Bucket>> cands;  // launch configurations the tuner tries
   std::vector<double> cost;                // ms per walker-move of each (< 0: not yet timed)
@@ -1447,12 +1479,31 @@ static bool member_extras(const qmcb_handle *h)
 }
 
 // Persistent grid of one bucket: as many blocks as fit on every SM at once.
-static int bucket_grid(qmcb_group *g, bool extras, int stride, int wpb, int *grid)
+template <bool kExtras, bool kGInv>
+static void launch_group_move(const qmcb_group::Bucket &B, cudaStream_t st, const GroupMember *gm, int t,
+                              int *counter)
+{
+  const size_t smem = sizeof(double) * (size_t)B.stride * B.wpb;
+  k_move_group<kExtras, kGInv><<<B.grid, 32 * B.wpb, smem, st>>>(gm, B.count, t, B.stride, counter);
+}
+
+static void launch_group_move_any(const qmcb_group::Bucket &B, cudaStream_t st, const GroupMember *gm, int t,
+                                  int *counter)
+{
+  if (B.extras)
+    B.ginv ? launch_group_move<true, true>(B, st, gm, t, counter) : launch_group_move<true, false>(B, st, gm, t, counter);
+  else
+    B.ginv ? launch_group_move<false, true>(B, st, gm, t, counter)
+           : launch_group_move<false, false>(B, st, gm, t, counter);
+}
+
+static int bucket_grid(qmcb_group *g, bool extras, bool ginv, int stride, int wpb, int *grid)
 {
   int per_sm = 0;
   const size_t smem = sizeof(double) * (size_t)stride * wpb;
-  cudaError_t e = extras ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_move_group<true>, 32 * wpb, smem)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_move_group<false>, 32 * wpb, smem);
+  const void *fn = extras ? (ginv ? (const void *)k_move_group<true, true> : (const void *)k_move_group<true, false>)
+                          : (ginv ? (const void *)k_move_group<false, true> : (const void *)k_move_group<false, false>);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem);
   if (e != cudaSuccess) return gfail(g, QMCB_E_CUDA, std::string("qmcb_group: occupancy: ") + cudaGetErrorString(e));
   if (per_sm < 1) return gfail(g, QMCB_E_LIMIT, "qmcb_group: a member's scratch does not fit one block");
   *grid = per_sm * g->n_sm;
@@ -1471,7 +1522,8 @@ static int build_candidates(qmcb_group *g)
     std::vector<int> c;
     int lo = 0;
     for (int i = 1; i < n; i++) {
-      const bool run_end = member_extras(g->mem[i]) != member_extras(g->mem[i - 1]);
+      const bool run_end = member_extras(g->mem[i]) != member_extras(g->mem[i - 1]) ||
+                           g->mem[i]->ginv != g->mem[i - 1]->ginv;
       const bool class_end = ratio > 0 && g->mem[i]->lay.mv_stride > ratio * g->mem[lo]->lay.mv_stride;
       if (run_end || class_end) {
         c.push_back(i);
@@ -1492,6 +1544,7 @@ static int build_candidates(qmcb_group *g)
         b.first = lo;
         b.count = hi - lo;
         b.extras = member_extras(g->mem[lo]);
+        b.ginv = g->mem[lo]->ginv;
         b.stride = 0;
         long long walkers = 0;
         for (int i = lo; i < hi; i++) {
@@ -1499,7 +1552,7 @@ static int build_candidates(qmcb_group *g)
           walkers += g->mem[i]->max_walkers;
         }
         b.wpb = std::max(1, std::min<int>(wpb, g->max_optin / (int)(sizeof(double) * b.stride)));
-        int rc = bucket_grid(g, b.extras, b.stride, b.wpb, &b.grid);
+        int rc = bucket_grid(g, b.extras, b.ginv, b.stride, b.wpb, &b.grid);
         if (rc) return rc;
         // no more warps than the bucket has walkers, so that concurrent
         // buckets leave each other room on the SMs
@@ -1540,13 +1593,9 @@ static int group_enqueue(qmcb_group *g, int c, int n_steps, const int *first_ste
     bool dmc = false;
     for (int i = B.first; i < B.first + B.count; i++) dmc |= g->mem[i]->params.run_type == QMCB_DMC;
     const GroupMember *gm = g->d_gm + B.first;
-    const size_t smem = sizeof(double) * (size_t)B.stride * B.wpb;
     for (int t = 0; t < n_steps; t++) {
       GK(cudaMemsetAsync(g->d_counter + b, 0, sizeof(int), sb));
-      if (B.extras)
-        k_move_group<true><<<B.grid, 32 * B.wpb, smem, sb>>>(gm, B.count, t, B.stride, g->d_counter + b);
-      else
-        k_move_group<false><<<B.grid, 32 * B.wpb, smem, sb>>>(gm, B.count, t, B.stride, g->d_counter + b);
+      launch_group_move_any(B, sb, gm, t, g->d_counter + b);
       if (dmc) {
         k_branch_group<<<B.count, 1024, 0, sb>>>(gm, t);
         k_copy_group<<<dim3(64, B.count), 256, 0, sb>>>(gm, t);
@@ -1599,6 +1648,7 @@ int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out)
   std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
     const bool ea = member_extras(members[a]), eb = member_extras(members[b]);
     if (ea != eb) return !ea;
+    if (members[a]->ginv != members[b]->ginv) return !members[a]->ginv;
     return members[a]->lay.mv_stride < members[b]->lay.mv_stride;
   });
   for (int i : idx) {
@@ -1614,12 +1664,17 @@ int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out)
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork_ev, cudaEventDisableTiming);
   // the group kernels hold the member prefix sums in static shared memory:
   // the dynamic part may use the rest of the opt-in maximum
-  cudaFuncAttributes fa0{}, fa1{};
-  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa0, k_move_group<false>);
-  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa1, k_move_group<true>);
-  if (e == cudaSuccess) g->max_optin -= (int)std::max(fa0.sharedSizeBytes, fa1.sharedSizeBytes);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, g->max_optin);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, g->max_optin);
+  const void *fns[4] = {(const void *)k_move_group<false, false>, (const void *)k_move_group<true, false>,
+                        (const void *)k_move_group<false, true>, (const void *)k_move_group<true, true>};
+  size_t stat = 0;
+  for (const void *fn : fns) {
+    cudaFuncAttributes fa{};
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+    stat = std::max(stat, fa.sharedSizeBytes);
+  }
+  if (e == cudaSuccess) g->max_optin -= (int)stat;
+  for (const void *fn : fns)
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, g->max_optin);
   if (e != cudaSuccess) rc = gfail(nullptr, QMCB_E_CUDA, std::string("qmcb_group_create: ") + cudaGetErrorString(e));
   if (!rc) {
     rc = build_candidates(g);

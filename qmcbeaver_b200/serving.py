@@ -73,14 +73,16 @@ def blocked_error(samples: Sequence[float], nblocks: int = 8) -> float:
 def state_footprint(system: MolecularSystem, walkers: int) -> int:
     """Device bytes a job's handle allocates for its walker state
     (the per-walker block of the library, 2x walker capacity, 256-byte
-    blocks): positions, Slater rows / derivatives / inverse per spin,
-    per-electron arrays, scalars."""
+    blocks): positions, Slater rows / derivatives / inverse per spin (two
+    inverse copies for spins above 16 electrons), per-electron arrays,
+    scalars."""
     def pad4(x):
         return (x + 3) & ~3
     N, na, nb = system.n_electrons, system.n_alpha, system.n_beta
+    ginv = max(na, nb) > 16  # inverses in HBM, two copies (kStagedInverseMax)
     words = pad4(3 * N)
     for n in (na, nb):
-        words += pad4(n * n) + pad4(3 * n * n) + pad4(n * n) + pad4(n * n)
+        words += pad4(n * n) + pad4(3 * n * n) + pad4(n * n) + (2 * pad4(n * n) if ginv else pad4(n * n))
     words += 4 * pad4(3 * N) + pad4(24)
     words = (words + 31) & ~31
     return 2 * walkers * words * 8

@@ -50,8 +50,9 @@ def test_admission_respects_footprint_budget():
 def test_footprint_matches_library():
     from qmcbeaver_b200.api import QMCB200Functions
     from qmcbeaver_b200.system import make_system
-    for wl in ("vmc_water_10e", "dmc_6nuc_30e"):
-        s = make_system(wl)
+    from qmcbeaver_b200.system import make_random_molecule
+    for s in (make_system("vmc_water_10e"), make_system("dmc_6nuc_30e"),
+              make_random_molecule(60, 8, 120, 8.0, (1, 6, 7, 8), seed=2)):
         f = QMCB200Functions(s, 2 * 300)
         assert f.state_bytes() == state_footprint(s, 300)
         f.close()
