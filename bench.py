@@ -263,23 +263,12 @@ def serving_section(args):
             "same_results_alone_and_mixed": bool(same)}
 
 
-def batching_section(args):
-    """The uneven-batching workload: 64 synthetic molecules, even electron
-    counts uniform in 4-200, basis 4N, N/5 nuclei with Z in {1, 6, 7, 8},
-    orthonormalised random orbital coefficients;
-    walkers per molecule uniform in 256-2048 (the workload's 256-8192
-    capped at 2048 so that all 64 walker populations fit in HBM together:
-    this layout keeps every walker's orbital rows, derivative rows and
-    inverses resident, 24 n^2 doubles for n electrons per spin).  VMC
-    importance-sampled steps, 100 per batch.  One group (persistent launches
-    per bucket, configuration tuned on the first batches, batches replayed
-    as CUDA graphs) against the same steps run handle after handle and on
-    all handles' streams at once.  Wall-clock walker-moves/s around
-    synchronous batches."""
+def _batch_compare(jobs, B, timed):
+    """One group over the jobs' handles (tuned first) against the same steps
+    run handle after handle and on all handles' streams at once; wall-clock
+    walker-moves/s around synchronous batches of B steps."""
     from qmcbeaver_b200.api import QMCB200Functions, QMCB200Group
     from qmcbeaver_b200.desc import QMCB_IMPORTANCE_SAMPLING, QMCB_QF_UMRIGAR93_UNEQUAL, run_params
-    from qmcbeaver_b200.serving import make_jobs
-    jobs = make_jobs(64, rate=1.0, seed=23, electrons=(4, 200), walkers=(256, 2048), orbitals="random")
     hs = []
     for j in jobs:
         p = run_params(sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01,
@@ -287,7 +276,6 @@ def batching_section(args):
         f = QMCB200Functions(j.system, j.walkers, p)
         f.init_walkers(j.system.initial_positions(j.walkers, seed=j.seed))
         hs.append(f)
-    B, timed = 100, 2
     g = QMCB200Group(hs)
     step = 0
     tune_t0 = time.perf_counter()
@@ -330,6 +318,24 @@ def batching_section(args):
             "group_speedup_vs_sequential": r_group / r_seq, "group_speedup_vs_streams": r_group / r_streams,
             "tuning": {"configurations": cfg["n_configs"], "chosen": cfg["chosen"], "buckets": cfg["n_buckets"],
                        "warps_per_block": cfg["warps_per_block"], "tuning_batches_s": tune_s}}
+
+
+def batching_section(args):
+    """The uneven-batching workload: 64 synthetic molecules, even electron
+    counts uniform in 4-200, basis 4N, N/5 nuclei with Z in {1, 6, 7, 8},
+    orthonormalised random orbital coefficients; walkers per molecule
+    uniform in 256-2048 (the workload's 256-8192 capped at 2048 so that all
+    64 walker populations fit in HBM together: this layout keeps every
+    walker's orbital rows, derivative rows and inverses resident).  VMC
+    importance-sampled steps, 100 per batch.  Next to it the same comparison
+    for 64 small molecules (4-40 electrons, the serving jobs' sizes), where
+    each molecule's step is a short kernel."""
+    from qmcbeaver_b200.serving import make_jobs
+    out = _batch_compare(make_jobs(64, rate=1.0, seed=23, electrons=(4, 200), walkers=(256, 2048),
+                                   orbitals="random"), B=100, timed=2)
+    out["small_molecules"] = _batch_compare(make_jobs(64, rate=1.0, seed=29, electrons=(4, 40), walkers=(256, 2048),
+                                                      orbitals="random"), B=40, timed=5)
+    return out
 
 
 def run_reference_arm(args, rank: int):

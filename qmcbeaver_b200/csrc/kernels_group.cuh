@@ -34,6 +34,12 @@ struct GroupMember {
   double thr_split, thr_fuse;
 };
 
+// Member tables of groups that fit (kConst launches): read through the
+// constant cache with warp-uniform indices; groups that do not fit read
+// their table from global memory.
+constexpr int kConstMembers = 84;
+__constant__ GroupMember c_gm[kConstMembers];
+
 __device__ __forceinline__ int group_step(const GroupMember &G, int t) { return G.step0 + t; }
 
 // Largest m with prefix[m] <= i (members without live walkers have equal
@@ -52,11 +58,12 @@ __device__ __forceinline__ int group_find(const int *prefix, int nm, int i)
 }
 
 // One Metropolis / DMC step (step offset t) of every live walker of the
-// members gm[0..nm); stride: doubles of shared memory per warp (at least
-// every member's L.mv_stride); *counter is zero at launch.
-template <bool kExtras, bool kGInv>
+// members gm[0..nm) (kConst: c_gm[cbase .. cbase + nm)); stride: doubles of
+// shared memory per warp (at least every member's L.mv_stride); *counter is
+// zero at launch.
+template <bool kExtras, bool kGInv, bool kConst>
 __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__restrict__ gm, int nm, int t, int stride,
-                                                    int *counter)
+                                                    int *counter, int cbase)
 {
   extern __shared__ double smem[];
   __shared__ int prefix[kGroupMax + 1];
@@ -64,7 +71,7 @@ __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__rest
     int acc = 0;
     for (int m = 0; m < nm; m++) {
       prefix[m] = acc;
-      acc += *gm[m].ctl;
+      acc += kConst ? *c_gm[cbase + m].ctl : *gm[m].ctl;
     }
     prefix[nm] = acc;
   }
@@ -78,7 +85,7 @@ __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__rest
     i = __shfl_sync(QMCB_FULL_MASK, i, 0);
     if (i >= total) break;
     const int m = group_find(prefix, nm, i);
-    const GroupMember &G = gm[m];
+    const GroupMember &G = kConst ? c_gm[cbase + m] : gm[m];
     MoveArgs mv;
     mv.step = group_step(G, t);
     mv.e = mv.step % G.S.N;

@@ -1440,6 +1440,7 @@ struct qmcb_group {
   GroupMember *d_gm = nullptr;
   std::vector<GroupMember> h_gm;
   int *d_counter = nullptr;  // one per bucket
+  int cbase = -1;            // first slot of the member table in c_gm (-1: table in global memory)
   struct Bucket {
     int first, count, stride, wpb, grid;
     bool extras, ginv;
@@ -1479,31 +1480,61 @@ static bool member_extras(const qmcb_handle *h)
 }
 
 // Persistent grid of one bucket: as many blocks as fit on every SM at once.
-template <bool kExtras, bool kGInv>
-static void launch_group_move(const qmcb_group::Bucket &B, cudaStream_t st, const GroupMember *gm, int t,
-                              int *counter)
+// The group move kernel for a bucket's flags; cbase >= 0: the group's
+// member table sits in c_gm from cbase on.
+static const void *group_move_fn(bool extras, bool ginv, bool cst)
 {
-  const size_t smem = sizeof(double) * (size_t)B.stride * B.wpb;
-  k_move_group<kExtras, kGInv><<<B.grid, 32 * B.wpb, smem, st>>>(gm, B.count, t, B.stride, counter);
+  const void *fns[8] = {(const void *)k_move_group<false, false, false>, (const void *)k_move_group<true, false, false>,
+                        (const void *)k_move_group<false, true, false>,  (const void *)k_move_group<true, true, false>,
+                        (const void *)k_move_group<false, false, true>,  (const void *)k_move_group<true, false, true>,
+                        (const void *)k_move_group<false, true, true>,   (const void *)k_move_group<true, true, true>};
+  return fns[(extras ? 1 : 0) + (ginv ? 2 : 0) + (cst ? 4 : 0)];
 }
 
-static void launch_group_move_any(const qmcb_group::Bucket &B, cudaStream_t st, const GroupMember *gm, int t,
-                                  int *counter)
+static cudaError_t launch_group_move_any(const qmcb_group::Bucket &B, cudaStream_t st, const GroupMember *gm, int t,
+                                         int *counter, int cbase)
 {
-  if (B.extras)
-    B.ginv ? launch_group_move<true, true>(B, st, gm, t, counter) : launch_group_move<true, false>(B, st, gm, t, counter);
-  else
-    B.ginv ? launch_group_move<false, true>(B, st, gm, t, counter)
-           : launch_group_move<false, false>(B, st, gm, t, counter);
+  const size_t smem = sizeof(double) * (size_t)B.stride * B.wpb;
+  int nm = B.count, stride = B.stride;
+  void *args[] = {(void *)&gm, (void *)&nm, (void *)&t, (void *)&stride, (void *)&counter, (void *)&cbase};
+  return cudaLaunchKernel(group_move_fn(B.extras, B.ginv, cbase >= 0), dim3(B.grid), dim3(32 * B.wpb), args, smem, st);
+}
+
+// Slots of c_gm per device, handed out to groups at create.
+static std::mutex g_const_mu;
+static std::vector<std::vector<char>> g_const_used;
+
+static int const_reserve(int device, int n)
+{
+  std::lock_guard<std::mutex> lock(g_const_mu);
+  if ((int)g_const_used.size() <= device) g_const_used.resize(device + 1);
+  auto &u = g_const_used[device];
+  if (u.empty()) u.assign(kConstMembers, 0);
+  for (int b = 0; b + n <= kConstMembers; b++) {
+    bool free = true;
+    for (int i = b; i < b + n && free; i++) free = !u[i];
+    if (free) {
+      for (int i = b; i < b + n; i++) u[i] = 1;
+      return b;
+    }
+  }
+  return -1;
+}
+
+static void const_release(int device, int base, int n)
+{
+  if (base < 0) return;
+  std::lock_guard<std::mutex> lock(g_const_mu);
+  auto &u = g_const_used[device];
+  for (int i = base; i < base + n; i++) u[i] = 0;
 }
 
 static int bucket_grid(qmcb_group *g, bool extras, bool ginv, int stride, int wpb, int *grid)
 {
   int per_sm = 0;
   const size_t smem = sizeof(double) * (size_t)stride * wpb;
-  const void *fn = extras ? (ginv ? (const void *)k_move_group<true, true> : (const void *)k_move_group<true, false>)
-                          : (ginv ? (const void *)k_move_group<false, true> : (const void *)k_move_group<false, false>);
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem);
+  cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, group_move_fn(extras, ginv, g->cbase >= 0), 32 * wpb, smem);
   if (e != cudaSuccess) return gfail(g, QMCB_E_CUDA, std::string("qmcb_group: occupancy: ") + cudaGetErrorString(e));
   if (per_sm < 1) return gfail(g, QMCB_E_LIMIT, "qmcb_group: a member's scratch does not fit one block");
   *grid = per_sm * g->n_sm;
@@ -1512,13 +1543,13 @@ static int bucket_grid(qmcb_group *g, bool extras, bool ginv, int stride, int wp
 
 // The configurations the tuner tries: members in runs of equal extras flag,
 // each run one bucket or cut into size classes whose per-warp scratch stays
-// within a factor 2 or 1.4 of the class's smallest; 4 or 2 warps per block
+// within a factor 2, 1.4 or 1.15 of the class's smallest; 4 or 2 warps per block
 // (fewer where one block could not hold them).
 static int build_candidates(qmcb_group *g)
 {
   const int n = (int)g->mem.size();
   std::vector<std::vector<int>> splits;
-  for (double ratio : {0.0, 2.0, 1.4}) {
+  for (double ratio : {0.0, 2.0, 1.4, 1.15}) {
     std::vector<int> c;
     int lo = 0;
     for (int i = 1; i < n; i++) {
@@ -1595,7 +1626,7 @@ static int group_enqueue(qmcb_group *g, int c, int n_steps, const int *first_ste
     const GroupMember *gm = g->d_gm + B.first;
     for (int t = 0; t < n_steps; t++) {
       GK(cudaMemsetAsync(g->d_counter + b, 0, sizeof(int), sb));
-      launch_group_move_any(B, sb, gm, t, g->d_counter + b);
+      GK(launch_group_move_any(B, sb, gm, t, g->d_counter + b, g->cbase >= 0 ? g->cbase + B.first : -1));
       if (dmc) {
         k_branch_group<<<B.count, 1024, 0, sb>>>(gm, t);
         k_copy_group<<<dim3(64, B.count), 256, 0, sb>>>(gm, t);
@@ -1664,8 +1695,9 @@ int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out)
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->fork_ev, cudaEventDisableTiming);
   // the group kernels hold the member prefix sums in static shared memory:
   // the dynamic part may use the rest of the opt-in maximum
-  const void *fns[4] = {(const void *)k_move_group<false, false>, (const void *)k_move_group<true, false>,
-                        (const void *)k_move_group<false, true>, (const void *)k_move_group<true, true>};
+  g->cbase = const_reserve(g->device, n);
+  const void *fns[8];
+  for (int k = 0; k < 8; k++) fns[k] = group_move_fn(k & 1, k & 2, k & 4);
   size_t stat = 0;
   for (const void *fn : fns) {
     cudaFuncAttributes fa{};
@@ -1692,6 +1724,7 @@ int qmcb_group_destroy(qmcb_group *g)
 {
   if (!g) return QMCB_OK;
   if (g->stream) cudaStreamSynchronize(g->stream);
+  const_release(g->device, g->cbase, (int)g->mem.size());
   if (g->gexec) cudaGraphExecDestroy(g->gexec);
   if (g->d_gm) cudaFree(g->d_gm);
   if (g->d_counter) cudaFree(g->d_counter);
@@ -1753,6 +1786,9 @@ int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmc
   // the members' own streams finish first (their last evaluate or copy)
   for (auto *h : g->mem) GK(cudaStreamSynchronize(h->stream));
   GK(cudaMemcpyAsync(g->d_gm, g->h_gm.data(), sizeof(GroupMember) * nm, cudaMemcpyHostToDevice, st));
+  if (g->cbase >= 0)
+    GK(cudaMemcpyToSymbolAsync(c_gm, g->h_gm.data(), sizeof(GroupMember) * nm, sizeof(GroupMember) * g->cbase,
+                               cudaMemcpyHostToDevice, st));
   for (auto *h : g->mem) GK(cudaMemsetAsync(h->d_stats, 0, sizeof(double) * ST_RUN_SUM_W, st));
   // configuration: the tuned one, else the next one not yet timed
   int c = g->chosen;
