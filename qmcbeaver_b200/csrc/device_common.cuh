@@ -658,6 +658,56 @@ __device__ __forceinline__ void basis_slots_warp(const DevSys &S, const double r
   }
 }
 
+// FP32 form of basis_slots_warp for the mixed-precision move: the slots'
+// exp(-a r^2) formed as in basis_shells_warp_f (argument in FP64, split
+// into a power of two and a fraction), the functions' sums in FP32.
+__device__ __forceinline__ void basis_slots_warp_f(const DevSys &S, const double r[3], float *chi, int ldc,
+                                                   float *ex)
+{
+  const int lane = lane_id();
+  for (int q = lane; q < S.nslot; q += 32) {
+    const int2 t = __ldg(&S.xsl[q]);
+    const double4 A = S.nuc[t.x];
+    const double x = r[0] - A.x, y = r[1] - A.y, z = r[2] - A.z;
+    const double a = -__ldg(&S.pexp[t.y]) * (x * x + y * y + z * z) * 1.4426950408889634;  // log2(e)
+    const double fl = floor(a);
+    ex[q] = fl < -150.0 ? 0.0f : ldexpf(exp2f((float)(a - fl)), (int)fl);
+  }
+  __syncwarp();
+  for (int k = lane; k < S.K; k += 32) {
+    const int4 fq = __ldg(&S.fq[k]);
+    const int2 f = __ldg(&S.fn[k]);
+    const double4 A = S.nuc[fq.x];
+    const float x = (float)(r[0] - A.x), y = (float)(r[1] - A.y), z = (float)(r[2] - A.z);
+    const float r2 = x * x + y * y + z * z;
+    const int a = f.x & 0xff, b = (f.x >> 8) & 0xff, c = (f.x >> 16) & 0xff;
+    const float Lf = 4.0f * fq.w + 6.0f, r2x4 = 4.0f * r2;
+    float E0 = 0.0f, E1 = 0.0f, El = 0.0f;
+    for (int i = 0; i < fq.z; i++) {
+      const float al = (float)__ldg(&S.pexp[f.y + i]);
+      const float e = (float)__ldg(&S.pcoef[f.y + i]) * ex[fq.y + i];
+      E0 += e;
+      E1 = fmaf(e, al, E1);
+      El = fmaf(e, al * fmaf(r2x4, al, -Lf), El);
+    }
+    const float xa = ipowf(x, a), yb = ipowf(y, b), zc = ipowf(z, c);
+    const float P = xa * yb * zc;
+    const float Px = a ? a * ipowf(x, a - 1) * yb * zc : 0.0f;
+    const float Py = b ? b * xa * ipowf(y, b - 1) * zc : 0.0f;
+    const float Pz = c ? c * xa * yb * ipowf(z, c - 1) : 0.0f;
+    float Pl = 0.0f;
+    if (a > 1) Pl += a * (a - 1.0f) * ipowf(x, a - 2) * yb * zc;
+    if (b > 1) Pl += b * (b - 1.0f) * xa * ipowf(y, b - 2) * zc;
+    if (c > 1) Pl += c * (c - 1.0f) * xa * yb * ipowf(z, c - 2);
+    const float PE1 = P * E1;
+    chi[0 * ldc + k] = E0 * P;
+    chi[1 * ldc + k] = fmaf(E0, Px, -2.0f * x * PE1);
+    chi[2 * ldc + k] = fmaf(E0, Py, -2.0f * y * PE1);
+    chi[3 * ldc + k] = fmaf(E0, Pz, -2.0f * z * PE1);
+    chi[4 * ldc + k] = fmaf(E0, Pl, P * El);
+  }
+}
+
 // FP64 tensor-core tile D(8x8) += A(8x4) B(4x8), mma.sync m8n8k4 (row.col).
 // Fragments: a = A[lane/4][lane%4], b = B[lane%4][lane/4],
 // d0,d1 = D[lane/4][2(lane%4)], D[lane/4][2(lane%4)+1].

@@ -1000,7 +1000,8 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
     __syncwarp();
     contract_dmma_warp((const double *)chi, ldc, S.ct[sp], n, K, (double *)Dn);
   } else {
-    basis_shells_warp_f(S, rn, (float *)chi, ldc);
+    // FP32 chi rows take half of region A; the slots follow them
+    basis_slots_warp_f(S, rn, (float *)chi, ldc, (float *)chi + 5 * ldc);
     __syncwarp();
     contract_slices_warp_f((const float *)chi, ldc, S.ctf[sp], n, K, (float *)Dn, (float *)cpart);
   }
