@@ -418,21 +418,24 @@ __device__ __forceinline__ int tb_func(const DevSys &S, int A, int i, int j)
   return S.tbp[3 * A + (ai != aj ? 0 : (ai ? 1 : 2))];
 }
 
-// Three-body changes when electron e moves from ro to rn, for the partners j
-// of this lane (j = lane + 32 k): U, laplacian and the gradient on e are
-// added to the lane's partial sums, U_x[j] is updated in place
-// (QMCThreeBodyJastrow::updateOne, QMcBeaver/src/QMCThreeBodyJastrow.cpp:43-178).
+// Three-body changes when electron e moves from ro to rn
+// (QMCThreeBodyJastrow::updateOne, QMcBeaver/src/QMCThreeBodyJastrow.cpp:43-178):
+// the lanes share out the (partner j, nucleus A) pairs, each adding U, the
+// laplacian and the gradient on e to its partial sums and leaving the
+// gradient change on j in pg[(j M + A)][3] (shared scratch, 3 N M doubles);
+// then U_x[j] takes those changes in nucleus order, as a loop over the
+// nuclei of one partner would.
 __device__ __noinline__ void tb_move_lane(const DevSys &S, const double *R, double *Ux, int e, const double *ro,
-                                          const double *rn, double *acc)
+                                          const double *rn, double *acc, double *pg)
 {
-  const int N = S.N;
-  for (int j = threadIdx.x & 31; j < N; j += 32) {
-    if (j == e) continue;
-    const double *rj = R + 3 * j;
-    const bool e_first = e > j;
-    for (int A = 0; A < S.M; A++) {
-      const int f = tb_func(S, A, e, j);
-      if (f < 0) continue;
+  const int N = S.N, M = S.M, lane = threadIdx.x & 31;
+  for (int q = lane; q < N * M; q += 32) {
+    const int j = q / M, A = q - j * M;
+    double gj[3] = {0.0, 0.0, 0.0};
+    const int f = j == e ? -1 : tb_func(S, A, e, j);
+    if (f >= 0) {
+      const double *rj = R + 3 * j;
+      const bool e_first = e > j;
       const double4 P = S.nuc[A];
       const double dj[3] = {rj[0] - P.x, rj[1] - P.y, rj[2] - P.z};
       double Uo, Lo, go1[3], go2[3], Un, Ln, gn1[3], gn2[3];
@@ -451,13 +454,19 @@ __device__ __noinline__ void tb_move_lane(const DevSys &S, const double *R, doub
       acc[0] += Un - Uo;
       acc[1] += Ln - Lo;
       for (int k = 0; k < 3; k++) {
-        const double ge = e_first ? gn1[k] - go1[k] : gn2[k] - go2[k];
-        const double gj = e_first ? gn2[k] - go2[k] : gn1[k] - go1[k];
-        acc[2 + k] += ge;
-        Ux[3 * j + k] += gj;
+        acc[2 + k] += e_first ? gn1[k] - go1[k] : gn2[k] - go2[k];
+        gj[k] = e_first ? gn2[k] - go2[k] : gn1[k] - go1[k];
       }
     }
+    for (int k = 0; k < 3; k++) pg[3 * q + k] = gj[k];
   }
+  __syncwarp();
+  for (int j = lane; j < N; j += 32) {
+    if (j == e) continue;
+    for (int A = 0; A < M; A++)
+      for (int k = 0; k < 3; k++) Ux[3 * j + k] += pg[3 * (j * M + A) + k];
+  }
+  __syncwarp();
 }
 
 // Three-body U, laplacian and gradients of all electrons from scratch

@@ -696,11 +696,12 @@ __device__ __forceinline__ void propose_move(const DevSys &S, const RunCfg &cfg,
 // QMCPotential_Energy::evaluate); lane j updates its own U_x[j] in place,
 // U_x[e] and the staged position of e are written last.  kTB: the system
 // may have three-body terms (a separate instantiation keeps them out of the
-// register allocation of the plain move).
+// register allocation of the plain move); tbs: 3 N M doubles of shared
+// scratch for them.
 template <bool kTB>
 __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR, double *Ux, int e, int sp,
                                                      const double ro[3], const double rn[3], double &dU,
-                                                     double &dUxx, double &dVee, double &dVen)
+                                                     double &dUxx, double &dVee, double &dVen, double *tbs)
 {
   const int lane = lane_id(), N = S.N;
   double ge[3] = {0, 0, 0};
@@ -756,7 +757,7 @@ __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR
   }
   if (kTB && S.ntb > 0) {
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    tb_move_lane(S, sR, Ux, e, ro, rn, acc);
+    tb_move_lane(S, sR, Ux, e, ro, rn, acc, tbs);
     dU += acc[0];
     dUxx += acc[1];
     ge[0] += acc[2];
@@ -990,7 +991,8 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
 
   // ---- incremental Jastrow + potential
   double dU, dUxx, dVee, dVen;
-  jastrow_pe_move_warp<kExtras>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
+  // (three-body partner gradients use region A, free until the basis)
+  jastrow_pe_move_warp<kExtras>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen, sm);
 
   // ---- basis at the new position and the new Slater / derivative rows
   if constexpr (sizeof(TS) == 8) {

@@ -31,15 +31,19 @@ __host__ __device__ inline int full_md_scratch_doubles(int N, int K, int nmax, i
 }
 // chi rows of the move kernel; the basis pass's exponential slots follow
 // them into the gr .. valc space (written only after the contraction)
-__host__ __device__ inline int move_md_chi_doubles(int N, int K, int nmax, int amax, int ndet, int nslot)
+// tbneed: doubles of three-body scratch (3 N M, or 0), also taken from the
+// chi .. valc space before the basis
+__host__ __device__ inline int move_md_chi_doubles(int N, int K, int nmax, int amax, int ndet, int nslot,
+                                                   int tbneed)
 {
   const int rest = 2 * even(3 * N) + even(5 * amax) + 2 * even(ndet) + even(nmax);
-  return even(max(5 * K, 5 * K + nslot - rest));
+  return even(max(max(5 * K, 5 * K + nslot - rest), tbneed - rest));
 }
-__host__ __device__ inline int move_md_scratch_doubles(int N, int K, int nmax, int amax, int ndet, int tail, int nslot)
+__host__ __device__ inline int move_md_scratch_doubles(int N, int K, int nmax, int amax, int ndet, int tail, int nslot,
+                                                       int tbneed)
 {
-  return move_md_chi_doubles(N, K, nmax, amax, ndet, nslot) + 2 * even(3 * N) + even(5 * amax) + 2 * even(ndet) +
-         even(nmax) + even(3 * N) + even(tail) + 2;
+  return move_md_chi_doubles(N, K, nmax, amax, ndet, nslot, tbneed) + 2 * even(3 * N) + even(5 * amax) +
+         2 * even(ndet) + even(nmax) + even(3 * N) + even(tail) + 2;
 }
 
 // One copy of spin sp's determinant block.
@@ -339,9 +343,10 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
   double *blk = state + (size_t)slot * L.stride;
   const int tail = L.sc + kScalars - L.gradD;
 
-  double *sm = smem + (size_t)warp * move_md_scratch_doubles(N, K, nmax, amax, nd, tail, S.nslot);
+  const int tbneed = S.ntb > 0 ? 3 * N * S.M : 0;
+  double *sm = smem + (size_t)warp * move_md_scratch_doubles(N, K, nmax, amax, nd, tail, S.nslot, tbneed);
   double *chi = sm;
-  double *gr = chi + move_md_chi_doubles(N, K, nmax, amax, nd, S.nslot);
+  double *gr = chi + move_md_chi_doubles(N, K, nmax, amax, nd, S.nslot, tbneed);
   double *mg = gr + even(3 * N);
   double *Dn = mg + even(3 * N);       // new rows of the active orbitals [5][a]
   double *rat = Dn + even(5 * amax);   // per-determinant ratios
@@ -364,7 +369,7 @@ __global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg,
   double rn[3], g_fwd, u_acc;
   propose_move<kMetropolis, true>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
   double dU, dUxx, dVee, dVen;
-  jastrow_pe_move_warp<true>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen);
+  jastrow_pe_move_warp<true>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen, chi);
 
   basis_slots_warp(S, rn, chi, K, chi + 5 * K);
   __syncwarp();

@@ -866,6 +866,8 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   // the basis pass keeps its exponential slots after the five chi rows,
   // reaching into the Dn / valc space
   L.mv_region_a = std::max(move_region_a(h->N, K), even(5 * K + (int)xsl.size() - L.mv_dn - L.mv_valc));
+  // three-body partner gradients (3 N M doubles) use region A before the basis
+  if (S.ntb > 0) L.mv_region_a = std::max(L.mv_region_a, even(3 * h->N * S.M));
   L.mv_r = even(3 * h->N);
   L.mv_tail = even(L.sc + kScalars - L.gradD);
   for (int sp = 0; sp < 2; sp++) {
@@ -902,7 +904,8 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   const int amax = std::max(nact[0], nact[1]);
   const size_t per_move =
-      sizeof(double) * (size_t)(md ? move_md_scratch_doubles(h->N, K, h->nmax, amax, S.ndet, L.sc + kScalars - L.gradD, S.nslot)
+      sizeof(double) * (size_t)(md ? move_md_scratch_doubles(h->N, K, h->nmax, amax, S.ndet, L.sc + kScalars - L.gradD, S.nslot,
+                                                           S.ntb > 0 ? 3 * h->N * S.M : 0)
                                    : L.mv_stride);
   const size_t per_full =
       sizeof(double) * (size_t)(md ? full_md_scratch_doubles(h->N, K, h->nmax, amax, S.ndet)
