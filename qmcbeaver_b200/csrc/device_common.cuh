@@ -332,6 +332,42 @@ __device__ __forceinline__ void pade_eval(const DevSys &S, int f, double r, doub
 }
 
 // ------------------------------------------------------------ three-body
+// The coefficient sums of one three-body term for fixed sizes (the
+// common NeN = Nee = 4), unrolled; the same operations in the same order
+// as the general loop in tb_term.
+template <int NEN, int NEE>
+__device__ __forceinline__ void tb_poly(const double *__restrict__ c, const double *x1, const double *x2,
+                                        const double *x12, double &P, double &Pl, double &Pm, double &Pn,
+                                        double &Pll, double &Pmm, double &Pnn, double &Pln, double &Pmn)
+{
+#pragma unroll
+  for (int l = 0; l < NEN; l++) {
+    const double xl = x1[l], xl1 = l > 0 ? l * x1[l - 1] : 0.0, xl2 = l > 1 ? l * (l - 1.0) * x1[l - 2] : 0.0;
+#pragma unroll
+    for (int m = 0; m < NEN; m++) {
+      const double xm = x2[m], xm1 = m > 0 ? m * x2[m - 1] : 0.0, xm2 = m > 1 ? m * (m - 1.0) * x2[m - 2] : 0.0;
+      const double lm = xl * xm, dlm = xl1 * xm, ldm = xl * xm1;
+      double s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+      for (int n = 0; n < NEE; n++) {
+        const double cc = __ldg(&c[(l * NEN + m) * NEE + n]);
+        s0 = fma(cc, x12[n], s0);
+        if (n > 0) s1 = fma(cc * n, x12[n - 1], s1);
+        if (n > 1) s2 = fma(cc * (n * (n - 1.0)), x12[n - 2], s2);
+      }
+      P = fma(lm, s0, P);
+      Pl = fma(dlm, s0, Pl);
+      Pm = fma(ldm, s0, Pm);
+      Pn = fma(lm, s1, Pn);
+      Pln = fma(dlm, s1, Pln);
+      Pmn = fma(ldm, s1, Pmn);
+      Pll = fma(xl2 * xm, s0, Pll);
+      Pmm = fma(xl * xm2, s0, Pmm);
+      Pnn = fma(lm, s2, Pnn);
+    }
+  }
+}
+
 // One Cambridge three-body term (CambridgeThreeBodyCorrelationFunction::
 // setElectron / evaluate / getLapPoly, QMcBeaver/src/CambridgeThreeBodyCorrelationFunction.cpp:
 // 150-470) of the electron pair (first, second) around one nucleus: d1, d2 the
@@ -370,6 +406,9 @@ __device__ inline bool tb_term(const DevSys &S, int f, const double d1[3], const
   // polynomial sums: value, d/dr1, d/dr2, d/dr12 and the second derivatives
   double P = 0, Pl = 0, Pm = 0, Pn = 0, Pll = 0, Pmm = 0, Pnn = 0, Pln = 0, Pmn = 0;
   const double *c = S.tbc + info.w;
+  if (Nen == 4 && Nee == 4)
+    tb_poly<4, 4>(c, x1, x2, x12, P, Pl, Pm, Pn, Pll, Pmm, Pnn, Pln, Pmn);
+  else
   for (int l = 0; l < Nen; l++) {
     const double xl = x1[l], xl1 = l > 0 ? l * x1[l - 1] : 0.0, xl2 = l > 1 ? l * (l - 1.0) * x1[l - 2] : 0.0;
     for (int m = 0; m < Nen; m++) {

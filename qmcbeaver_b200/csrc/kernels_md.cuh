@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(128) k_full_md(DevSys S, Layout L, RunCfg cfg,
 // ------------------------------------------------------------------------
 // One single-electron move of every walker in the list (see k_move).
 template <bool kMetropolis>
-__global__ void __launch_bounds__(128) k_move_md(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+__global__ void __launch_bounds__(128, 3) k_move_md(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                                  int num, const int *d_num, const double *R_in, MoveArgs mv,
                                                  const EnergyCtl *ectl, double *stats, EvalOut out)
 {
