@@ -255,11 +255,17 @@ def serving_section(args):
     ref = Server(max_active=1).run(seq)
     same = all(abs(a.energy - b.energy) <= 1e-9 * max(1.0, abs(b.energy)) for a, b in zip(mix, seq)
                if len(a.energies) == len(b.energies))
+    # the same arrivals with all active jobs stepped as one group per batch
+    # of 40 steps (the largest job's sweep)
+    grp = make_jobs(args.serve_jobs, rate=args.serve_rate, seed=11, **kw)
+    rg = Server(max_active=16, mode="group", batch_steps=40).run(grp)
     return {"jobs": res["jobs"], "arrival_rate_per_s": args.serve_rate, "target_error_ha": kw["target_error"],
             "latency_p50_s": res["latency_p50_s"], "latency_p99_s": res["latency_p99_s"],
             "walker_moves_per_s": res["walker_moves_per_s"],
             "sequential": {"latency_p50_s": ref["latency_p50_s"], "latency_p99_s": ref["latency_p99_s"],
                            "walker_moves_per_s": ref["walker_moves_per_s"]},
+            "group_mode": {"latency_p50_s": rg["latency_p50_s"], "latency_p99_s": rg["latency_p99_s"],
+                           "walker_moves_per_s": rg["walker_moves_per_s"], "jobs": rg["jobs"]},
             "same_results_alone_and_mixed": bool(same)}
 
 
