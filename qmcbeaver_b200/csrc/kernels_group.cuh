@@ -79,10 +79,11 @@ __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__rest
   const int lane = lane_id(), warp = threadIdx.x >> 5;
   double *sm = smem + (size_t)warp * stride;
   const int total = prefix[nm];
-  for (;;) {
-    int i = 0;
-    if (lane == 0) i = atomicAdd(counter, 1);
-    i = __shfl_sync(QMCB_FULL_MASK, i, 0);
+  // the first walker of every warp by its place in the grid, the rest from
+  // the counter (one atomic round trip fewer per warp)
+  const int nwarps = gridDim.x * (blockDim.x >> 5);
+  int i = blockIdx.x * (blockDim.x >> 5) + warp;
+  for (;; ) {
     if (i >= total) break;
     const int m = group_find(prefix, nm, i);
     const GroupMember &G = kConst ? c_gm[cbase + m] : gm[m];
@@ -95,6 +96,9 @@ __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__rest
     move_walker<true, double, double, kExtras, kGInv>(G.S, G.L, G.cfg, G.state, G.live, i - prefix[m], sm, nullptr, mv,
                                                G.ectl, G.stats, EvalOut{});
     __syncwarp();
+    int nx = 0;
+    if (lane == 0) nx = nwarps + atomicAdd(counter, 1);
+    i = __shfl_sync(QMCB_FULL_MASK, nx, 0);
   }
 }
 
