@@ -80,11 +80,14 @@ __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__rest
   double *sm = smem + (size_t)warp * stride;
   const int total = prefix[nm];
   // the first walker of every warp by its place in the grid, the rest from
-  // the counter (one atomic round trip fewer per warp)
+  // the counter; the next index is claimed when a walker starts, so the
+  // atomic's round trip overlaps the move
   const int nwarps = gridDim.x * (blockDim.x >> 5);
   int i = blockIdx.x * (blockDim.x >> 5) + warp;
   for (;; ) {
     if (i >= total) break;
+    int nx = 0;
+    if (lane == 0) nx = nwarps + atomicAdd(counter, 1);
     const int m = group_find(prefix, nm, i);
     const GroupMember &G = kConst ? c_gm[cbase + m] : gm[m];
     MoveArgs mv;
@@ -96,8 +99,6 @@ __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__rest
     move_walker<true, double, double, kExtras, kGInv>(G.S, G.L, G.cfg, G.state, G.live, i - prefix[m], sm, nullptr, mv,
                                                G.ectl, G.stats, EvalOut{});
     __syncwarp();
-    int nx = 0;
-    if (lane == 0) nx = nwarps + atomicAdd(counter, 1);
     i = __shfl_sync(QMCB_FULL_MASK, nx, 0);
   }
 }
