@@ -169,6 +169,15 @@ typedef struct qmcb_run_params {
   double rel_cutoff;         /* observables with |E - E_orig| / |E_orig| >= rel_cutoff are left out */
   int limit_branching;       /* QMCWalker::branchRecommended rules on splits (QMCWalker.cpp) */
   int energy_cutoff;         /* QMCB_ECUT_*: local energy used in the reweighting exponent */
+  /* 0 (the reference): the Green's functions of a single-electron
+   * importance-sampled move multiply in every unmoved electron's term
+   * (QMcBeaver/src/QMCWalker.cpp:383-388, 756-780, 540-583); their drifts
+   * differ before and after the move, so the acceptance ratio is not the
+   * proposal's and VMC samples a distribution slightly off |psi|^2 (h2o:
+   * 10 mHa high).  1: the moved electron's density only -- the exact
+   * Metropolis-Hastings ratio of a single-electron proposal.  No counterpart
+   * in the reference; all-electron moves are unaffected by the choice. */
+  int exact_single_electron_gf;
 } qmcb_run_params;
 
 /* energy_cutoff_type (QMCWalkerData::getModifiedLocalEnergy, QMcBeaver/src/QMCWalkerData.cpp:163-205) */

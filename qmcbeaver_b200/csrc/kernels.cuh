@@ -568,7 +568,8 @@ __device__ inline double umrigar_log_gf(const UmrigarFrame &F, const RunCfg &cfg
 }
 
 // Proposal of electron e and ln G(R -> R') over all electrons (the
-// unmoved ones contribute their stay-in-place density).
+// unmoved ones contribute their stay-in-place density; cfg.exact_gf: the
+// moved electron only).
 __device__ __noinline__ void umrigar_propose(const DevSys &S, const RunCfg &cfg, int slot, int step, int e, int N,
                                              const double *R, const double *mgo, double *rn, double *log_fwd,
                                              double *u_acc)
@@ -608,7 +609,7 @@ __device__ __noinline__ void umrigar_propose(const DevSys &S, const RunCfg &cfg,
     UmrigarFrame Fi;
     if (i == e) {
       part += umrigar_log_gf(F, cfg, rn);
-    } else {
+    } else if (!cfg.exact_gf) {
       umrigar_frame(S, cfg, R + 3 * i, mgo + 3 * i, Fi);
       part += umrigar_log_gf(Fi, cfg, R + 3 * i);
     }
@@ -623,6 +624,7 @@ __device__ __noinline__ double umrigar_log_reverse(const DevSys &S, const RunCfg
 {
   double part = 0.0;
   for (int i = threadIdx.x & 31; i < N; i += 32) {
+    if (cfg.exact_gf && i != e) continue;
     UmrigarFrame F;
     umrigar_frame(S, cfg, Rn + 3 * i, mg + 3 * i, F);
     part += umrigar_log_gf(F, cfg, i == e ? ro : Rn + 3 * i);
@@ -675,7 +677,7 @@ __device__ __forceinline__ void propose_move(const DevSys &S, const RunCfg &cfg,
       rn[d] = ro[d] + disp;
       g_fwd += drift * drift;
     }
-    if (cfg.sampling == 1) {
+    if (cfg.sampling == 1 && !cfg.exact_gf) {
       // G(R -> R') includes the drift of the electrons that do not move
       // (QMcBeaver/src/QMCWalker.cpp:383-388)
       double prt = 0.0;
@@ -798,6 +800,7 @@ __device__ __forceinline__ bool metropolis_reweight(const DevSys &S, const RunCf
   } else if (cfg.sampling == 1) {
     double pr = 0.0;
     for (int t = lane; t < 3 * N; t += 32) {
+      if (cfg.exact_gf && t / 3 != e) continue;
       const double tt = (t / 3 == e) ? (ro[t - 3 * e] - rn[t - 3 * e] - cfg.dt * mg[t]) : (cfg.dt * mg[t]);
       pr += tt * tt;
     }

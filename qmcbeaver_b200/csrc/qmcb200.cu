@@ -181,6 +181,7 @@ static RunCfg make_cfg(const qmcb_run_params &p)
   c.seed = p.seed;
   c.limit_branching = p.limit_branching;
   c.ecut = p.energy_cutoff;
+  c.exact_gf = p.exact_single_electron_gf;
   c.e_orig = p.energy_original != 0.0 ? p.energy_original : (p.energy_estimated != 0.0 ? p.energy_estimated : -1.0);
   c.rel_cutoff = p.rel_cutoff > 0 ? p.rel_cutoff : 1e300;
   return c;
@@ -964,7 +965,8 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: umrigar93_equalelectrons_parameter must be in (0, 1]");
   if (p->run_type < 0 || p->run_type > 1 || p->sampling < 0 || p->sampling > 2 || p->qf_modification < 0 ||
       p->qf_modification > 2 || p->energy_modification < 0 || p->energy_modification > 2 || p->reweighting < 0 ||
-      p->reweighting > 2 || p->energy_cutoff < 0 || p->energy_cutoff > 2)
+      p->reweighting > 2 || p->energy_cutoff < 0 || p->energy_cutoff > 2 || p->exact_single_electron_gf < 0 ||
+      p->exact_single_electron_gf > 1)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");
   if (p->precision != QMCB_PREC_FP64 && p->precision != QMCB_PREC_MIXED)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown precision");

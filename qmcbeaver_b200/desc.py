@@ -49,7 +49,7 @@ class RunParams(C.Structure):
         ("old_walker_acceptance", C.c_int), ("refresh_interval", C.c_int), ("precision", C.c_int),
         ("seed", C.c_uint64), ("population_control", C.c_double), ("target_walkers", C.c_int),
         ("reweight_start_step", C.c_int), ("energy_original", C.c_double), ("rel_cutoff", C.c_double),
-        ("limit_branching", C.c_int), ("energy_cutoff", C.c_int),
+        ("limit_branching", C.c_int), ("energy_cutoff", C.c_int), ("exact_single_electron_gf", C.c_int),
     ]
 
 
