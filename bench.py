@@ -476,9 +476,16 @@ def main():
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_moves = 0.0
+    # each step's E_T goes up before it is enqueued; its statistics come back
+    # while the next step runs (two batches in flight), so the host's trial
+    # energy follows the statistics one step behind
+    f.set_params(p)
+    f.run_steps_async(step0, 1)
     for s in range(args.e2e_steps):
-        f.set_params(p)
-        st2 = f.run_steps(step0 + s, 1)
+        if s + 1 < args.e2e_steps:
+            f.set_params(p)
+            f.run_steps_async(step0 + s + 1, 1)
+        st2 = f.steps_collect()
         e2e_moves += st2.n_moves
         if st2.sum_weight > 0:
             sw += st2.sum_weight
@@ -494,7 +501,8 @@ def main():
     e2e_s, e2e_moves = aggregate_timing(e2e_s, e2e_moves)
     e2e = {"value": e2e_moves / e2e_s, "unit": "walker-moves/s", "h2d_bytes_per_step": ctypes.sizeof(RunParams),
            "d2h_bytes_per_step": ctypes.sizeof(StepStats) + 16,
-           "api": "qmcb_set_params + qmcb_run_steps(step, 1) per step (host E_T in, step statistics out)"}
+           "api": "qmcb_set_params + qmcb_run_steps_async(step, 1) per step, statistics collected one step "
+                  "behind with qmcb_steps_collect (host E_T in, step statistics out)"}
 
     # reference-facing evaluate (QMCFunctions::evaluate shape) with host buffers
     slots = np.arange(min(W, 4096), dtype=np.int32)

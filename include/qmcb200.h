@@ -286,11 +286,13 @@ int qmcb_run_step_configs(qmcb_handle *h, int step, double *records, int capacit
                           qmcb_step_stats *stats);
 
 /* Asynchronous form for drivers that keep several handles busy at once
- * (one stream per handle; kernels of different handles overlap on the GPU):
+ * (one stream per handle; kernels of different handles overlap on the GPU)
+ * or that prepare a batch while the previous one runs:
  * qmcb_run_steps_async enqueues the steps and returns; qmcb_steps_done
- * returns 1 when they finished (0 while running, negative on error);
- * qmcb_steps_collect waits and returns the statistics.  One batch in
- * flight per handle. */
+ * returns 1 when the oldest batch in flight finished (0 while running,
+ * negative on error); qmcb_steps_collect waits for it and returns its
+ * statistics.  At most two batches in flight per handle, collected in the
+ * order they were enqueued; qmcb_run_steps needs none in flight. */
 int qmcb_run_steps_async(qmcb_handle *h, int first_step, int n_steps);
 int qmcb_steps_done(qmcb_handle *h);
 int qmcb_steps_collect(qmcb_handle *h, qmcb_step_stats *stats);

@@ -93,10 +93,15 @@ struct qmcb_handle {
   bool evaluated_once = false;
   int state_prec = -1;  // precision the stored walker state was written in
   // asynchronous step batches (qmcb_run_steps_async)
-  double *h_stats = nullptr;  // pinned
-  int *h_ctl = nullptr;       // pinned
-  cudaEvent_t done_ev = nullptr;
-  bool in_flight = false;
+  // up to two batches in flight, each with its own pinned statistics copy
+  double *h_stats = nullptr;  // pinned, [2][ST_COUNT]
+  int *h_ctl = nullptr;       // pinned, [2][4]
+  cudaEvent_t done_ev[2] = {nullptr, nullptr};
+  int n_flight = 0;           // batches enqueued and not yet collected
+  EnergyCtl *h_ectl = nullptr;  // pinned [4]: E_T / E_est uploads of qmcb_set_params
+  cudaEvent_t ectl_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // each slot's copy done
+  int ectl_next = 0;
+  int head = 0;               // slot of the oldest of them
   // kernel timing (qmcb_set_profiling)
   bool prof = false;
   std::vector<cudaEvent_t> prof_ev;
@@ -897,9 +902,12 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(cudaMalloc(&h->d_R, sizeof(double) * (size_t)max_walkers * 3 * h->N));
   CKC(cudaMalloc(&h->d_out, sizeof(double) * (size_t)max_walkers * (6 * h->N + 8)));
   CKC(cudaMalloc(&h->d_status, max_walkers));
-  CKC(cudaMallocHost(&h->h_stats, sizeof(double) * ST_COUNT));
-  CKC(cudaMallocHost(&h->h_ctl, sizeof(int) * 4));
-  CKC(cudaEventCreateWithFlags(&h->done_ev, cudaEventDisableTiming));
+  CKC(cudaMallocHost(&h->h_stats, sizeof(double) * 2 * ST_COUNT));
+  CKC(cudaMallocHost(&h->h_ctl, sizeof(int) * 2 * 4));
+  CKC(cudaMallocHost(&h->h_ectl, sizeof(EnergyCtl) * 4));
+  for (int k = 0; k < 4; k++) CKC(cudaEventCreateWithFlags(&h->ectl_ev[k], cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&h->done_ev[0], cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&h->done_ev[1], cudaEventDisableTiming));
 
   int max_optin = 0;
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
@@ -949,7 +957,11 @@ int qmcb_destroy(qmcb_handle *h)
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
-  if (h->done_ev) cudaEventDestroy(h->done_ev);
+  for (cudaEvent_t e : h->done_ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->ectl_ev)
+    if (e) cudaEventDestroy(e);
+  if (h->h_ectl) cudaFreeHost(h->h_ectl);
   if (h->h_stats) cudaFreeHost(h->h_stats);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -975,12 +987,19 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
   h->params = *p;
   if (h->n_live_host > 0) {
     // the host's E_T / E_est feed the next steps (QMCManager::updateTrialEnergy)
-    EnergyCtl ec{};
+    // from a pinned slot (a ring of four, so that slots still being read by
+    // copies in flight are not rewritten), asynchronous to the host
+    const int k = h->ectl_next;
+    h->ectl_next = (k + 1) & 3;
+    CK(cudaEventSynchronize(h->ectl_ev[k]));  // this slot's previous copy has left it
+    EnergyCtl &ec = h->h_ectl[k];
+    ec = EnergyCtl{};
     ec.e_trial = p->energy_trial;
     ec.e_est = p->energy_estimated;
     ec.target_weight = p->target_walkers > 0 ? p->target_walkers : h->target_weight;
     ec.pop_control = p->population_control;
     CK(cudaMemcpyAsync(h->d_ectl, &ec, sizeof(ec), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaEventRecord(h->ectl_ev[k], h->stream));
   }
   return QMCB_OK;
 }
@@ -1155,7 +1174,7 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps, double *du
   if (!h->evaluated_once) return fail(h, QMCB_E_STATE, "qmcb_run_steps: call qmcb_init_walkers first");
   if (h->state_prec != h->params.precision)
     return fail(h, QMCB_E_STATE, "qmcb_run_steps: walker state was written in another precision; call qmcb_init_walkers");
-  if (h->in_flight) return fail(h, QMCB_E_STATE, "qmcb_run_steps: a batch of steps is still in flight on this handle");
+  if (h->n_flight >= 2) return fail(h, QMCB_E_STATE, "qmcb_run_steps_async: two batches of steps are already in flight on this handle");
   if (h->n_live_host <= 0) return fail(h, QMCB_E_STATE, "qmcb_run_steps: no live walkers (population died out)");
   cudaStream_t st = h->stream;
   RunCfg cfg = make_cfg(h->params);
@@ -1214,22 +1233,26 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps, double *du
     }
   }
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(h->h_stats, h->d_stats, sizeof(double) * ST_COUNT, cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
-  CK(cudaEventRecord(h->done_ev, st));
-  h->in_flight = true;
+  const int slot = (h->head + h->n_flight) & 1;
+  CK(cudaMemcpyAsync(h->h_stats + slot * ST_COUNT, h->d_stats, sizeof(double) * ST_COUNT, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h->h_ctl + slot * 4, h->d_ctl, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(h->done_ev[slot], st));
+  h->n_flight++;
   return QMCB_OK;
 }
 
 // Waits for the batch in flight and converts the pinned statistics.
 static int finish_steps(qmcb_handle *h, qmcb_step_stats *stats)
 {
-  if (!h->in_flight) return fail(h, QMCB_E_STATE, "qmcb_steps_collect: no batch in flight");
-  CK(cudaEventSynchronize(h->done_ev));
-  h->in_flight = false;
+  if (h->n_flight == 0) return fail(h, QMCB_E_STATE, "qmcb_steps_collect: no batch in flight");
+  const int slot = h->head;
+  CK(cudaEventSynchronize(h->done_ev[slot]));
+  h->head ^= 1;
+  h->n_flight--;
   if (h->prof) prof_collect(h);
-  const double *sv = h->h_stats;
-  h->n_live_host = h->h_ctl[0];
+  const double *sv = h->h_stats + slot * ST_COUNT;
+  const int *cv = h->h_ctl + slot * 4;
+  h->n_live_host = cv[0];
   if (stats) {
     stats->sum_weight = sv[ST_SUM_W];
     stats->sum_weight_energy = sv[ST_SUM_WE];
@@ -1237,7 +1260,7 @@ static int finish_steps(qmcb_handle *h, qmcb_step_stats *stats)
     stats->sum_accept = sv[ST_SUM_ACC];
     stats->n_moves = sv[ST_MOVES];
     stats->final_weight = sv[ST_FINAL_W];
-    stats->n_walkers = h->h_ctl[0];
+    stats->n_walkers = cv[0];
     stats->n_singular = (int)sv[ST_SINGULAR];
   }
   return QMCB_OK;
@@ -1246,6 +1269,7 @@ static int finish_steps(qmcb_handle *h, qmcb_step_stats *stats)
 int qmcb_run_steps(qmcb_handle *h, int first_step, int n_steps, qmcb_step_stats *stats)
 {
   if (!h) return QMCB_E_ARG;
+  if (h->n_flight) return fail(h, QMCB_E_STATE, "qmcb_run_steps: collect the batches in flight first");
   int rc = enqueue_steps(h, first_step, n_steps);
   if (rc) return rc;
   return finish_steps(h, stats);
@@ -1259,6 +1283,7 @@ int qmcb_run_step_configs(qmcb_handle *h, int step, double *records, int capacit
   if (capacity < n) return fail(h, QMCB_E_ARG, "qmcb_run_step_configs: capacity below the live walker count");
   const size_t rec = (size_t)QMCB_CONFIG_RECORD(h->N);
   if (!h->d_dump) CK(cudaMalloc(&h->d_dump, sizeof(double) * 2 * rec * (size_t)h->max_walkers));
+  if (h->n_flight) return fail(h, QMCB_E_STATE, "qmcb_run_step_configs: collect the batches in flight first");
   int rc = enqueue_steps(h, step, 1, h->d_dump);
   if (rc) return rc;
   // the walkers that moved are the n live before the step, in list order
@@ -1278,8 +1303,8 @@ int qmcb_run_steps_async(qmcb_handle *h, int first_step, int n_steps)
 int qmcb_steps_done(qmcb_handle *h)
 {
   if (!h) return -QMCB_E_ARG;
-  if (!h->in_flight) return 1;
-  cudaError_t e = cudaEventQuery(h->done_ev);
+  if (h->n_flight == 0) return 1;
+  cudaError_t e = cudaEventQuery(h->done_ev[h->head]);
   if (e == cudaSuccess) return 1;
   if (e == cudaErrorNotReady) return 0;
   fail(h, QMCB_E_CUDA, std::string("qmcb_steps_done: ") + cudaGetErrorString(e));
@@ -1758,7 +1783,7 @@ int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmc
     const std::string who = "qmcb_group_run_steps: member " + std::to_string(g->user[i]);
     if (first_steps[g->user[i]] < 0) return gfail(g, QMCB_E_ARG, who + ": negative first step");
     if (!h->evaluated_once) return gfail(g, QMCB_E_STATE, who + ": call qmcb_init_walkers first");
-    if (h->in_flight) return gfail(g, QMCB_E_STATE, who + ": a batch of steps is in flight on its handle");
+    if (h->n_flight) return gfail(g, QMCB_E_STATE, who + ": a batch of steps is in flight on its handle");
     if (h->params.precision != QMCB_PREC_FP64 || h->state_prec != QMCB_PREC_FP64)
       return gfail(g, QMCB_E_ARG, who + ": groups step FP64 walkers only");
     refresh |= h->params.refresh_interval > 0;
