@@ -1,6 +1,6 @@
 """Times the reference QMcBeaver CPU program (oracle/_ref/QMcBeaver.x, built
-from the reference's own sources) on a synthetic workload -- TEST / BASELINE
-INFRASTRUCTURE: used only by bench.py's reference arm and cpu_baseline.
+from the reference's own sources) on a synthetic workload -- test and CPU-baseline
+infrastructure: used only by bench.py's reference arm and cpu_baseline.
 
 Runs P independent processes at once (the reference's manager_worker MPI
 mode is exactly independent walker populations plus a reduce), each on its
