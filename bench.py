@@ -200,7 +200,8 @@ def mixed_section(system, W, e0, rank, args):
 
 def rows_section(args, rank: int):
     """The widened rows on their own workloads: Cambridge2 two-body Jastrow,
-    a 12-determinant CI expansion and the three-body Jastrow (with Cambridge2),
+    a 12-determinant CI expansion, the three-body Jastrow (with Cambridge2)
+    and the reference's water input (cusps, three-body, Umrigar93 moves),
     VMC with drift on the device (timed
     with CUDA events on the library's stream), next to the reference CPU
     program on the same systems (all host cores, a bounded sample)."""
@@ -209,11 +210,21 @@ def rows_section(args, rank: int):
     from qmcbeaver_b200.desc import QMCB_IMPORTANCE_SAMPLING, QMCB_QF_UMRIGAR93_UNEQUAL, run_params
     from qmcbeaver_b200.replicas import aggregate_timing, replica_seed
     from qmcbeaver_b200.system import make_system
+    from qmcbeaver_b200.desc import QMCB_UMRIGAR93_IMPORTANCE_SAMPLING
+    from qmcbeaver_b200.system import system_from_arrays
     out = {}
-    for wl, W in (("vmc_cambridge2_16e", 8192), ("vmc_multidet_12e", 8192), ("vmc_threebody_16e", 8192)):
-        s = make_system(wl, seed=1)
+    # the reference's own water input as this repository's reader builds it
+    # (cusp replacement, Cambridge three-body Jastrow; tests/golden/inputs),
+    # with its own sampling method
+    h2o = np.load(os.path.join(ROOT, "tests", "golden", "inputs", "h2o.npz"))
+    h2o = system_from_arrays({k[4:]: h2o[k] for k in h2o.files if k.startswith("sys_")})
+    rows = [("vmc_cambridge2_16e", make_system("vmc_cambridge2_16e", seed=1), 8192, QMCB_IMPORTANCE_SAMPLING),
+            ("vmc_multidet_12e", make_system("vmc_multidet_12e", seed=1), 8192, QMCB_IMPORTANCE_SAMPLING),
+            ("vmc_threebody_16e", make_system("vmc_threebody_16e", seed=1), 8192, QMCB_IMPORTANCE_SAMPLING),
+            ("h2o_input_umrigar93", h2o, 8192, QMCB_UMRIGAR93_IMPORTANCE_SAMPLING)]
+    for wl, s, W, sampling in rows:
         N = s.n_electrons
-        p = run_params(sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01,
+        p = run_params(sampling=sampling, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01,
                        refresh_interval=50, seed=replica_seed(17, rank), rel_cutoff=0.0)
         f = QMCB200Functions(s, W, p)
         f.init_walkers(s.initial_positions(W, seed=300 + rank))
@@ -234,11 +245,12 @@ def rows_section(args, rank: int):
         if rank == 0 and not args.no_cpu_baseline:
             from oracle import refrun
             if refrun.available():
-                r = refrun.run_reference(s, "vmc_drift", 0.01, 32, 400, os.cpu_count() or 1)
+                mode = "vmc_umrigar93" if sampling == QMCB_UMRIGAR93_IMPORTANCE_SAMPLING else "vmc_drift"
+                r = refrun.run_reference(s, mode, 0.01, 32, 400, os.cpu_count() or 1)
                 if r["ok"]:
                     row["cpu_reference"] = {"value": r["moves_per_s"], "unit": "walker-moves/s", "cores": r["procs"],
                                             "sample": f"{r['procs']} processes x 32 walkers x 400 steps of the "
-                                                      "reference's drift-diffusion VMC"}
+                                                      f"reference's {mode} VMC"}
         out[wl] = row
     return out
 

@@ -30,6 +30,8 @@ RUN_FLAGS = {
     "vmc_drift": {"run_type": "variational", "sampling_method": "importance_sampling",
                   "QF_modification_type": "umrigar93_unequalelectrons"},
     "vmc": {"run_type": "variational", "sampling_method": "no_importance_sampling", "QF_modification_type": "none"},
+    "vmc_umrigar93": {"run_type": "variational", "sampling_method": "umrigar93_importance_sampling",
+                      "QF_modification_type": "umrigar93_unequalelectrons"},
 }
 
 
