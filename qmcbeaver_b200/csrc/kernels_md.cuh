@@ -37,7 +37,9 @@ __host__ __device__ inline int move_md_chi_doubles(int N, int K, int nmax, int a
                                                    int tbneed)
 {
   const int rest = 2 * even(3 * N) + even(5 * amax) + 2 * even(ndet) + even(nmax);
-  return even(max(max(5 * K, 5 * K + nslot - rest), tbneed - rest));
+  // after the contraction the chi rows hold every determinant's
+  // Sherman-Morrison factors, laplacian partial sums and 1 / ratio
+  return even(max(max(max(5 * K, 5 * K + nslot - rest), tbneed - rest), 2 * ndet * nmax + ndet));
 }
 __host__ __device__ inline int move_md_scratch_doubles(int N, int K, int nmax, int amax, int ndet, int tail, int nslot,
                                                        int tbneed)
@@ -390,16 +392,17 @@ __global__ void __launch_bounds__(128, 3) k_move_md(DevSys S, Layout L, RunCfg c
   bool bad;
   md_weights(S, sp == 0 ? src.dsc : (no > 0 ? oth.dsc : nullptr), sp == 1 ? src.dsc : (no > 0 ? oth.dsc : nullptr),
              tpr, logD0, sgnD0, bad);
+  // lane c takes determinant c's row ratio
   bool zero_ratio = false;
-  for (int c = 0; c < nd; c++) {
+  for (int c = lane; c < nd; c += 32) {
     const int *occ = S.docc[sp] + (size_t)c * n;
     const double *Inv = src.inv + (size_t)c * n * n;
-    double rp = 0.0;
-    for (int o = lane; o < n; o += 32) rp = fma(Dn[occ[o]], Inv[o * n + el], rp);
-    const double r = warp_sum(rp);
+    double r = 0.0;
+    for (int o = 0; o < n; o++) r = fma(Dn[occ[o]], Inv[o * n + el], r);
+    rat[c] = r;
     if (!(r != 0.0) || !isfinite(r)) zero_ratio = true;
-    if (lane == 0) rat[c] = r;
   }
+  zero_ratio = __any_sync(QMCB_FULL_MASK, zero_ratio);
   __syncwarp();
   double rpart = 0.0;
   for (int c = lane; c < nd; c += 32) rpart += tpr[c] * rat[c];
@@ -409,58 +412,68 @@ __global__ void __launch_bounds__(128, 3) k_move_md(DevSys S, Layout L, RunCfg c
 
   // ---- Sherman-Morrison row update of every determinant into the idle
   //      copy (Array2D::inverseUpdateOneRow, QMcBeaver/include/Array2D.h:1567-1610)
-  //      and its ratio sums with the new inverse
-  for (int c = 0; c < nd; c++) {
+  //      and its ratio sums with the new inverse; the lanes share out the
+  //      determinants' columns, elements and electrons (the chi rows, free
+  //      after the contraction, hold the factors and partial sums)
+  double *vall = chi;                    // [nd][n] factors
+  double *lpp = chi + nd * n;            // [nd][n] laplacian partial sums
+  double *qd = chi + 2 * nd * n;         // [nd] 1 / ratio
+  for (int c = lane; c < nd; c += 32) qd[c] = 1.0 / rat[c];
+  __syncwarp();
+  for (int t = lane; t < nd * n; t += 32) {
+    const int c = t / n, col = t - c * n;
     const int *occ = S.docc[sp] + (size_t)c * n;
     const double *Iv = src.inv + (size_t)c * n * n;
-    double *Iw = dst.inv + (size_t)c * n * n;
-    const double q = 1.0 / rat[c];
-    for (int col = lane; col < n; col += 32) {
-      double v = 0.0;
-      if (col != el)
-        for (int l = 0; l < n; l++) v = fma(Dn[occ[l]], Iv[l * n + col], v);
-      valc[col] = v * q;
-    }
-    __syncwarp();
-    for (int t = lane; t < n * n; t += 32) {
-      const int r = t / n, col = t - r * n;
-      Iw[t] = col == el ? Iv[r * n + el] * q : Iv[t] - valc[col] * Iv[r * n + el];
-    }
-    __syncwarp();
-    double lp = 0.0;
-    for (int e2 = lane; e2 < n; e2 += 32) {
-      double gx = 0, gy = 0, gz = 0;
-      for (int o = 0; o < n; o++) {
-        const int orb = occ[o];
-        const double iv = Iw[o * n + e2];
-        if (e2 == el) {
-          gx = fma(Dn[a + orb], iv, gx);
-          gy = fma(Dn[2 * a + orb], iv, gy);
-          gz = fma(Dn[3 * a + orb], iv, gz);
-          lp = fma(Dn[4 * a + orb], iv, lp);
-        } else {
-          gx = fma(DgT[(0 * a + orb) * n + e2], iv, gx);
-          gy = fma(DgT[(1 * a + orb) * n + e2], iv, gy);
-          gz = fma(DgT[(2 * a + orb) * n + e2], iv, gz);
-          lp = fma(DlT[orb * n + e2], iv, lp);
-        }
-      }
-      double *g = dst.g + ((size_t)c * n + e2) * 3;
-      g[0] = gx;
-      g[1] = gy;
-      g[2] = gz;
-    }
-    lp = warp_sum(lp);
-    if (lane == 0) {
-      const double *d0 = src.dsc + 4 * c;
-      double *d = dst.dsc + 4 * c;
-      d[0] = d0[0] + log(fabs(rat[c]));
-      d[1] = d0[1] * (rat[c] < 0 ? -1.0 : 1.0);
-      d[2] = lp;
-      d[3] = (!(rat[c] != 0.0) || !isfinite(rat[c])) ? 1.0 : d0[3];
-    }
-    __syncwarp();
+    double v = 0.0;
+    if (col != el)
+      for (int l = 0; l < n; l++) v = fma(Dn[occ[l]], Iv[l * n + col], v);
+    vall[t] = v * qd[c];
   }
+  __syncwarp();
+  for (int u = lane; u < nd * n * n; u += 32) {
+    const int c = u / (n * n), t = u - c * n * n, r = t / n, col = t - r * n;
+    const double *Iv = src.inv + (size_t)c * n * n;
+    dst.inv[u] = col == el ? Iv[r * n + el] * qd[c] : Iv[t] - vall[c * n + col] * Iv[r * n + el];
+  }
+  __syncwarp();
+  for (int t = lane; t < nd * n; t += 32) {
+    const int c = t / n, e2 = t - c * n;
+    const int *occ = S.docc[sp] + (size_t)c * n;
+    const double *Iw = dst.inv + (size_t)c * n * n;
+    double gx = 0, gy = 0, gz = 0, lp = 0;
+    for (int o = 0; o < n; o++) {
+      const int orb = occ[o];
+      const double iv = Iw[o * n + e2];
+      if (e2 == el) {
+        gx = fma(Dn[a + orb], iv, gx);
+        gy = fma(Dn[2 * a + orb], iv, gy);
+        gz = fma(Dn[3 * a + orb], iv, gz);
+        lp = fma(Dn[4 * a + orb], iv, lp);
+      } else {
+        gx = fma(DgT[(0 * a + orb) * n + e2], iv, gx);
+        gy = fma(DgT[(1 * a + orb) * n + e2], iv, gy);
+        gz = fma(DgT[(2 * a + orb) * n + e2], iv, gz);
+        lp = fma(DlT[orb * n + e2], iv, lp);
+      }
+    }
+    double *g = dst.g + ((size_t)c * n + e2) * 3;
+    g[0] = gx;
+    g[1] = gy;
+    g[2] = gz;
+    lpp[t] = lp;
+  }
+  __syncwarp();
+  for (int c = lane; c < nd; c += 32) {
+    double lp = 0.0;
+    for (int e2 = 0; e2 < n; e2++) lp += lpp[c * n + e2];
+    const double *d0 = src.dsc + 4 * c;
+    double *d = dst.dsc + 4 * c;
+    d[0] = d0[0] + log(fabs(rat[c]));
+    d[1] = d0[1] * (rat[c] < 0 ? -1.0 : 1.0);
+    d[2] = lp;
+    d[3] = (!(rat[c] != 0.0) || !isfinite(rat[c])) ? 1.0 : d0[3];
+  }
+  __syncwarp();
 
   // ---- new weights termPR'_c = termPR_c ratio_c / R_D and the combined ratios
   for (int c = lane; c < nd; c += 32) tpr[c] *= rat[c] * iRD;
