@@ -309,7 +309,7 @@ int qmcb_steps_collect(qmcb_handle *h, qmcb_step_stats *stats);
  * fastest; results do not depend on the configuration.  Batches without
  * refresh are captured as one CUDA graph and replayed while the batch length
  * and configuration stay the same.
- * Members: single-determinant FP64 handles on one device, each initialised
+ * Members: FP64 handles (one or several determinants) on one device, each initialised
  * (qmcb_init_walkers), none in flight; the caller does not use a member's
  * handle for steps while the group steps it.  At most 512 members.
  * qmcb_group_run_steps advances member i by n_steps steps from

@@ -61,9 +61,10 @@ __device__ __forceinline__ int group_find(const int *prefix, int nm, int i)
 // members gm[0..nm) (kConst: c_gm[cbase .. cbase + nm)); stride: doubles of
 // shared memory per warp (at least every member's L.mv_stride); *counter is
 // zero at launch.
-template <bool kExtras, bool kGInv, bool kConst>
-__global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__restrict__ gm, int nm, int t, int stride,
-                                                    int *counter, int cbase)
+// kMD: the members have several determinants (md_move_walker).
+template <bool kExtras, bool kGInv, bool kConst, bool kMD>
+__global__ void __launch_bounds__(128, kMD ? 3 : 5) k_move_group(const GroupMember *__restrict__ gm, int nm, int t,
+                                                              int stride, int *counter, int cbase)
 {
   extern __shared__ double smem[];
   __shared__ int prefix[kGroupMax + 1];
@@ -96,8 +97,12 @@ __global__ void __launch_bounds__(128, 5) k_move_group(const GroupMember *__rest
     mv.do_reweight = mv.e == 0;
     mv.reweight_on = mv.step >= G.reweight_start;
     mv.dump = nullptr;
-    move_walker<true, double, double, kExtras, kGInv>(G.S, G.L, G.cfg, G.state, G.live, i - prefix[m], sm, nullptr, mv,
-                                               G.ectl, G.stats, EvalOut{});
+    if constexpr (kMD)
+      md_move_walker<true>(G.S, G.L, G.cfg, G.state, G.live, i - prefix[m], sm, nullptr, mv, G.ectl, G.stats,
+                           EvalOut{});
+    else
+      move_walker<true, double, double, kExtras, kGInv>(G.S, G.L, G.cfg, G.state, G.live, i - prefix[m], sm, nullptr,
+                                                        mv, G.ectl, G.stats, EvalOut{});
     __syncwarp();
     i = __shfl_sync(QMCB_FULL_MASK, nx, 0);
   }

@@ -326,16 +326,16 @@ __global__ void __launch_bounds__(128) k_full_md(DevSys S, Layout L, RunCfg cfg,
 
 // ------------------------------------------------------------------------
 // One single-electron move of every walker in the list (see k_move).
+// md_move_walker: the work of one warp on walker wi (sm: its
+// move_md_scratch_doubles of shared memory); k_move_md runs it for one
+// system, k_move_group for the walkers of many.
 template <bool kMetropolis>
-__global__ void __launch_bounds__(128, 3) k_move_md(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
-                                                 int num, const int *d_num, const double *R_in, MoveArgs mv,
-                                                 const EnergyCtl *ectl, double *stats, EvalOut out)
+__device__ __forceinline__ void md_move_walker(const DevSys &S, const Layout &L, const RunCfg &cfg, double *state,
+                                               const int *slots, int wi, double *sm, const double *R_in,
+                                               const MoveArgs &mv, const EnergyCtl *ectl, double *stats,
+                                               const EvalOut &out)
 {
-  extern __shared__ double smem[];
-  const int lane = lane_id(), warp = threadIdx.x >> 5;
-  const int nw = d_num ? *d_num : num;
-  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (wi >= nw) return;
+  const int lane = lane_id();
   const int N = S.N, K = S.K, nd = S.ndet;
   const int nmax = max(S.na, S.nb), amax = max(S.nact[0], S.nact[1]);
   const int e = mv.e;
@@ -346,7 +346,6 @@ __global__ void __launch_bounds__(128, 3) k_move_md(DevSys S, Layout L, RunCfg c
   const int tail = L.sc + kScalars - L.gradD;
 
   const int tbneed = S.ntb > 0 ? 3 * N * S.M : 0;
-  double *sm = smem + (size_t)warp * move_md_scratch_doubles(N, K, nmax, amax, nd, tail, S.nslot, tbneed);
   double *chi = sm;
   double *gr = chi + move_md_chi_doubles(N, K, nmax, amax, nd, S.nslot, tbneed);
   double *mg = gr + even(3 * N);
@@ -537,6 +536,22 @@ __global__ void __launch_bounds__(128, 3) k_move_md(DevSys S, Layout L, RunCfg c
     }
   }
   if (!kMetropolis) write_eval_out(out, wi, N, logD_new + U_new, sgnD_new, lap, EL, PE, Ven, Vee, bad, gr, mg);
+}
+
+template <bool kMetropolis>
+__global__ void __launch_bounds__(128, 3) k_move_md(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+                                                 int num, const int *d_num, const double *R_in, MoveArgs mv,
+                                                 const EnergyCtl *ectl, double *stats, EvalOut out)
+{
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5;
+  const int nw = d_num ? *d_num : num;
+  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (wi >= nw) return;
+  const int nmax = max(S.na, S.nb), amax = max(S.nact[0], S.nact[1]);
+  const int tail = L.sc + kScalars - L.gradD, tbneed = S.ntb > 0 ? 3 * S.N * S.M : 0;
+  double *sm = smem + (size_t)warp * move_md_scratch_doubles(S.N, S.K, nmax, amax, S.ndet, tail, S.nslot, tbneed);
+  md_move_walker<kMetropolis>(S, L, cfg, state, slots, wi, sm, R_in, mv, ectl, stats, out);
 }
 
 }  // namespace qmcb

@@ -1473,7 +1473,7 @@ struct qmcb_group {
   int cbase = -1;            // first slot of the member table in c_gm (-1: table in global memory)
   struct Bucket {
     int first, count, stride, wpb, grid;
-    bool extras, ginv;
+    bool extras, ginv, md;
   };
   std::vector<std::vector<Bucket>> cands;  // launch configurations the tuner tries
   std::vector<double> cost;                // ms per walker-move of each (< 0: not yet timed)
@@ -1512,14 +1512,20 @@ static bool member_extras(const qmcb_handle *h)
 // Persistent grid of one bucket: as many blocks as fit on every SM at once.
 // The group move kernel for a bucket's flags; cbase >= 0: the group's
 // member table sits in c_gm from cbase on.
-static const void *group_move_fn(bool extras, bool ginv, bool cst)
+static const void *group_move_fn(bool extras, bool ginv, bool cst, bool md)
 {
-  const void *fns[8] = {(const void *)k_move_group<false, false, false>, (const void *)k_move_group<true, false, false>,
-                        (const void *)k_move_group<false, true, false>,  (const void *)k_move_group<true, true, false>,
-                        (const void *)k_move_group<false, false, true>,  (const void *)k_move_group<true, false, true>,
-                        (const void *)k_move_group<false, true, true>,   (const void *)k_move_group<true, true, true>};
+  const void *fns[10] = {
+      (const void *)k_move_group<false, false, false, false>, (const void *)k_move_group<true, false, false, false>,
+      (const void *)k_move_group<false, true, false, false>,  (const void *)k_move_group<true, true, false, false>,
+      (const void *)k_move_group<false, false, true, false>,  (const void *)k_move_group<true, false, true, false>,
+      (const void *)k_move_group<false, true, true, false>,   (const void *)k_move_group<true, true, true, false>,
+      (const void *)k_move_group<true, false, false, true>,   (const void *)k_move_group<true, false, true, true>};
+  if (md) return fns[8 + (cst ? 1 : 0)];
   return fns[(extras ? 1 : 0) + (ginv ? 2 : 0) + (cst ? 4 : 0)];
 }
+
+// Doubles of shared memory one warp of the member's move kernel uses.
+static int member_stride(const qmcb_handle *h) { return (int)(h->smem_move / sizeof(double) / h->wpb_move); }
 
 static cudaError_t launch_group_move_any(const qmcb_group::Bucket &B, cudaStream_t st, const GroupMember *gm, int t,
                                          int *counter, int cbase)
@@ -1527,7 +1533,8 @@ static cudaError_t launch_group_move_any(const qmcb_group::Bucket &B, cudaStream
   const size_t smem = sizeof(double) * (size_t)B.stride * B.wpb;
   int nm = B.count, stride = B.stride;
   void *args[] = {(void *)&gm, (void *)&nm, (void *)&t, (void *)&stride, (void *)&counter, (void *)&cbase};
-  return cudaLaunchKernel(group_move_fn(B.extras, B.ginv, cbase >= 0), dim3(B.grid), dim3(32 * B.wpb), args, smem, st);
+  return cudaLaunchKernel(group_move_fn(B.extras, B.ginv, cbase >= 0, B.md), dim3(B.grid), dim3(32 * B.wpb), args,
+                          smem, st);
 }
 
 // Slots of c_gm per device, handed out to groups at create.
@@ -1559,12 +1566,12 @@ static void const_release(int device, int base, int n)
   for (int i = base; i < base + n; i++) u[i] = 0;
 }
 
-static int bucket_grid(qmcb_group *g, bool extras, bool ginv, int stride, int wpb, int *grid)
+static int bucket_grid(qmcb_group *g, bool extras, bool ginv, bool md, int stride, int wpb, int *grid)
 {
   int per_sm = 0;
   const size_t smem = sizeof(double) * (size_t)stride * wpb;
-  cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, group_move_fn(extras, ginv, g->cbase >= 0), 32 * wpb, smem);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, group_move_fn(extras, ginv, g->cbase >= 0, md),
+                                                                32 * wpb, smem);
   if (e != cudaSuccess) return gfail(g, QMCB_E_CUDA, std::string("qmcb_group: occupancy: ") + cudaGetErrorString(e));
   if (per_sm < 1) return gfail(g, QMCB_E_LIMIT, "qmcb_group: a member's scratch does not fit one block");
   *grid = per_sm * g->n_sm;
@@ -1584,8 +1591,8 @@ static int build_candidates(qmcb_group *g)
     int lo = 0;
     for (int i = 1; i < n; i++) {
       const bool run_end = member_extras(g->mem[i]) != member_extras(g->mem[i - 1]) ||
-                           g->mem[i]->ginv != g->mem[i - 1]->ginv;
-      const bool class_end = ratio > 0 && g->mem[i]->lay.mv_stride > ratio * g->mem[lo]->lay.mv_stride;
+                           g->mem[i]->ginv != g->mem[i - 1]->ginv || g->mem[i]->md != g->mem[i - 1]->md;
+      const bool class_end = ratio > 0 && member_stride(g->mem[i]) > ratio * member_stride(g->mem[lo]);
       if (run_end || class_end) {
         c.push_back(i);
         lo = i;
@@ -1606,14 +1613,15 @@ static int build_candidates(qmcb_group *g)
         b.count = hi - lo;
         b.extras = member_extras(g->mem[lo]);
         b.ginv = g->mem[lo]->ginv;
+        b.md = g->mem[lo]->md;
         b.stride = 0;
         long long walkers = 0;
         for (int i = lo; i < hi; i++) {
-          b.stride = std::max(b.stride, g->mem[i]->lay.mv_stride);
+          b.stride = std::max(b.stride, member_stride(g->mem[i]));
           walkers += g->mem[i]->max_walkers;
         }
         b.wpb = std::max(1, std::min<int>(wpb, g->max_optin / (int)(sizeof(double) * b.stride)));
-        int rc = bucket_grid(g, b.extras, b.ginv, b.stride, b.wpb, &b.grid);
+        int rc = bucket_grid(g, b.extras, b.ginv, b.md, b.stride, b.wpb, &b.grid);
         if (rc) return rc;
         // no more warps than the bucket has walkers, so that concurrent
         // buckets leave each other room on the SMs
@@ -1669,7 +1677,12 @@ static int group_enqueue(qmcb_group *g, int c, int n_steps, const int *first_ste
           if (h->params.refresh_interval > 0 && (step + 1) % h->params.refresh_interval == 0) {
             EvalOut o2{};
             const int blocks_full = (h->max_walkers + h->wpb_full - 1) / h->wpb_full;
-            launch_full(h, blocks_full, sb, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, 0, o2);
+            if (h->md)
+              k_full_md<<<blocks_full, 32 * h->wpb_full, h->smem_full, sb>>>(h->sys, h->lay, make_cfg(h->params),
+                                                                              h->d_state, h->d_live, 0, h->d_ctl,
+                                                                              nullptr, 0, o2);
+            else
+              launch_full(h, blocks_full, sb, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, 0, o2);
           }
         }
       }
@@ -1691,9 +1704,6 @@ int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out)
   for (int i = 0; i < n; i++) {
     const qmcb_handle *h = members[i];
     if (!h) return gfail(nullptr, QMCB_E_ARG, "qmcb_group_create: null member");
-    if (h->md)
-      return gfail(nullptr, QMCB_E_ARG,
-                   "qmcb_group_create: member " + std::to_string(i) + " has several determinants; step it on its own");
     if (h->device != members[0]->device)
       return gfail(nullptr, QMCB_E_ARG, "qmcb_group_create: members on different devices");
     for (int j = 0; j < i; j++)
@@ -1707,10 +1717,11 @@ int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out)
   std::vector<int> idx(n);
   for (int i = 0; i < n; i++) idx[i] = i;
   std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
+    if (members[a]->md != members[b]->md) return !members[a]->md;
     const bool ea = member_extras(members[a]), eb = member_extras(members[b]);
     if (ea != eb) return !ea;
     if (members[a]->ginv != members[b]->ginv) return !members[a]->ginv;
-    return members[a]->lay.mv_stride < members[b]->lay.mv_stride;
+    return member_stride(members[a]) < member_stride(members[b]);
   });
   for (int i : idx) {
     g->mem.push_back(members[i]);
@@ -1726,8 +1737,10 @@ int qmcb_group_create(qmcb_handle *const *members, int n, qmcb_group **out)
   // the group kernels hold the member prefix sums in static shared memory:
   // the dynamic part may use the rest of the opt-in maximum
   g->cbase = const_reserve(g->device, n);
-  const void *fns[8];
-  for (int k = 0; k < 8; k++) fns[k] = group_move_fn(k & 1, k & 2, k & 4);
+  const void *fns[10];
+  for (int k = 0; k < 8; k++) fns[k] = group_move_fn(k & 1, k & 2, k & 4, false);
+  fns[8] = group_move_fn(true, false, false, true);
+  fns[9] = group_move_fn(true, false, true, true);
   size_t stat = 0;
   for (const void *fn : fns) {
     cudaFuncAttributes fa{};

@@ -24,6 +24,8 @@ def _systems(extra_threebody=False):
         s = make_random_molecule(ne, nn, nb, 5.0 + ne / 10, (1, 6, 7, 8), seed=10 + k)
         if extra_threebody and k == 2:
             s = with_three_body(s, seed=3)
+        if extra_threebody and k == 4:
+            s = with_determinants(s, 6, 3, seed=2)  # several determinants
         out.append((s, w))
     return out
 
@@ -136,11 +138,7 @@ def test_dmc_group_branches_like_members_alone():
 
 def test_group_refuses_unsupported_members():
     s = make_random_molecule(8, 2, 32, 5.0, (1, 6, 7, 8), seed=4)
-    md = with_determinants(s, 3, 2, seed=1)
     a = QMCB200Functions(s, 64, _params(0))
-    b = QMCB200Functions(md, 64, _params(1))
-    with pytest.raises(QMCBError, match="several determinants"):
-        QMCB200Group([a, b])
     c = QMCB200Functions(s, 64, run_params(precision=QMCB_PREC_MIXED, dt=0.01))
     c.init_walkers(s.initial_positions(32, seed=1))
     a.init_walkers(s.initial_positions(32, seed=2))
