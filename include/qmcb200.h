@@ -180,7 +180,11 @@ typedef struct qmcb_run_params {
   int exact_single_electron_gf;
 } qmcb_run_params;
 
-/* energy_cutoff_type (QMCWalkerData::getModifiedLocalEnergy, QMcBeaver/src/QMCWalkerData.cpp:163-205) */
+/* Energy cutoffs in the reweighting exponent.  The reference defines them
+ * (QMCWalkerData::getModifiedLocalEnergy, QMcBeaver/src/QMCWalkerData.cpp:163-205)
+ * but never calls that function, so its energy_cutoff_type changes nothing:
+ * QMCB_ECUT_NONE is the reference's behaviour, the other two are an opt-in
+ * stabiliser for poor trial functions (they bias the DMC energy). */
 #define QMCB_ECUT_NONE 0
 #define QMCB_ECUT_UMRIGAR93 1    /* E_L * |modified drift| / |drift| */
 #define QMCB_ECUT_BDJM_PUSH88 2  /* E_L clamped to E_orig +- 2 / sqrt(dt) */

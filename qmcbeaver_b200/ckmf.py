@@ -324,13 +324,18 @@ class CkmfInput:
                 raise CkmfError(f"{key} {v!r} is not supported by the walker path")
             return table[v]
 
+        ecut_input = pick("energy_cutoff", ecut, "energy_cutoff_type", "umrigar93")
+        ecut_run = ecut_input if "energy_cutoff" in overrides else D.QMCB_ECUT_NONE
         kw = dict(
             run_type=pick("run_type", run_type, "run_type", "variational"),
             sampling=pick("sampling", sampling, "sampling_method", "umrigar93_importance_sampling"),
             qf_modification=pick("qf_modification", qf, "QF_modification_type", "umrigar93_unequalelectrons"),
             energy_modification=pick("energy_modification", emod, "energy_modification_type", "umrigar93"),
             reweighting=pick("reweighting", rw, "walker_reweighting_method", "umrigar93_probability_weighted"),
-            energy_cutoff=pick("energy_cutoff", ecut, "energy_cutoff_type", "umrigar93"),
+            # the reference reads energy_cutoff_type but never applies it
+            # (QMCWalkerData::getModifiedLocalEnergy has no caller): an
+            # input's value is checked, and the run has no cutoff
+            energy_cutoff=ecut_run,
             dt=f("dt", 0.01, float),
             energy_trial=f("energy", 0.0, float),
             energy_estimated=f("energy", 0.0, float),

@@ -28,6 +28,9 @@ CASES = {
     "h2o_vmc": ("examples/h2o.ckmf", 16, 40, 8000, 1000, {}),
     # single-electron moves, as the device makes them
     "h2o_vmc_one_e": ("examples/h2o.ckmf", 16, 80, 16000, 2000, {"one_e_per_iter": 1}),
+    # diffusion Monte Carlo with the input's DMC settings, single-electron moves
+    "h2o_dmc_one_e": ("examples/h2o.ckmf", 16, 100, 30000, 5000,
+                      {"one_e_per_iter": 1, "run_type": "diffusion", "energy": -76.36}),
 }
 _ENERGY = re.compile(r"-+ Energy -+\s*\n\s*([-0-9.eE+]+)\s*\+/-\s*([0-9.eE+-]+)")
 

@@ -200,7 +200,8 @@ def test_run_params_from_flags():
                                    "energy_cutoff_type\n bdjm-push88\npopulation_control_parameter\n 100"))
     p = c.run_params()
     assert p.run_type == D.QMCB_DMC and p.sampling == D.QMCB_IMPORTANCE_SAMPLING
-    assert p.energy_cutoff == D.QMCB_ECUT_BDJM_PUSH88 and p.population_control == 100.0
+    # energy_cutoff_type is read (and checked) but the reference never applies it
+    assert p.energy_cutoff == D.QMCB_ECUT_NONE and p.population_control == 100.0
     assert p.dt == 0.02 and p.dt_effective == 0.02
     assert p.qf_modification == D.QMCB_QF_UMRIGAR93_UNEQUAL   # the reference's default
 

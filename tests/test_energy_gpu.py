@@ -20,7 +20,8 @@ import pytest
 from helpers import GOLDEN_DIR
 from inputs_common import load_input_case
 from qmcbeaver_b200.api import QMCB200Functions
-from qmcbeaver_b200.desc import (QMCB_NO_IMPORTANCE_SAMPLING, QMCB_QF_UMRIGAR93_UNEQUAL,
+from qmcbeaver_b200.desc import (QMCB_DMC, QMCB_ECUT_NONE, QMCB_EMOD_UMRIGAR93, QMCB_NO_IMPORTANCE_SAMPLING,
+                                 QMCB_QF_UMRIGAR93_UNEQUAL, QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED,
                                  QMCB_UMRIGAR93_IMPORTANCE_SAMPLING, run_params)
 
 pytestmark = pytest.mark.gpu
@@ -67,3 +68,37 @@ def test_exact_green_functions_match_reference_all_electron_runs():
     _agree(m, err, ref, "umrigar93, exact single-electron Green's functions")
     m, err = _device_vmc(QMCB_NO_IMPORTANCE_SAMPLING, 0.09, 0, seed=13)
     _agree(m, err, ref, "Metropolis, step sqrt(0.09)")
+
+
+def test_dmc_energy_agrees_with_reference_program():
+    """DMC with the input's settings (Umrigar93 moves and energy
+    modification, probability-weighted reweighting, dt 0.01, population
+    control 1 after an equilibration under the strong control 1 / dt the
+    reference applies while equilibrating, QMcBeaver/src/QMCManager.cpp:
+    2263-2310) against the reference's single-electron DMC runs; the
+    reference applies no energy cutoff."""
+    ref = _reference("h2o_dmc_one_e")
+    s, _ = load_input_case("h2o")
+    N, W, dt = s.n_electrons, 8192, 0.01
+
+    def params(pc, e):
+        return run_params(run_type=QMCB_DMC, sampling=QMCB_UMRIGAR93_IMPORTANCE_SAMPLING,
+                          qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=dt, energy_modification=QMCB_EMOD_UMRIGAR93,
+                          reweighting=QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED, energy_cutoff=QMCB_ECUT_NONE,
+                          population_control=pc, target_walkers=W, energy_trial=e, energy_estimated=e,
+                          energy_original=e, old_walker_acceptance=30, reweight_start_step=100, refresh_interval=50,
+                          seed=77, rel_cutoff=100.0)
+
+    f = QMCB200Functions(s, 3 * W, params(1.0 / dt, -76.36))
+    f.init_walkers(s.initial_positions(W, seed=3))
+    warm, sweeps = 500, 2000
+    f.run_steps(1, (warm - 100) * N)
+    st = f.run_steps(1 + (warm - 100) * N, 100 * N)
+    f.set_params(params(1.0, st.sum_weight_energy / st.sum_weight))
+    e = []
+    for k in range(sweeps):
+        st = f.run_steps(1 + (warm + k) * N, N)
+        e.append(st.sum_weight_energy / st.sum_weight)
+    assert 0.5 * W < st.n_walkers < 2 * W
+    blocks = np.array([b.mean() for b in np.array_split(np.array(e), 20)])
+    _agree(blocks.mean(), blocks.std(ddof=1) / np.sqrt(len(blocks)), ref, "DMC")
