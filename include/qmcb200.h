@@ -178,6 +178,11 @@ typedef struct qmcb_run_params {
    * Metropolis-Hastings ratio of a single-electron proposal.  No counterpart
    * in the reference; all-electron moves are unaffected by the choice. */
   int exact_single_electron_gf;
+  /* 1 (the reference): DMC reweights with the running effective time step
+   * dt <w p dR^2> / <w dR^2> over the moves sampled so far
+   * (QMCManager::updateEffectiveTimeStep, QMcBeaver/src/QMCManager.cpp:2312-2331,
+   * updated here with the trial energy); 0: dt_effective as given. */
+  int dynamic_time_step;
 } qmcb_run_params;
 
 /* Energy cutoffs in the reweighting exponent.  The reference defines them

@@ -336,6 +336,7 @@ class CkmfInput:
             # (QMCWalkerData::getModifiedLocalEnergy has no caller): an
             # input's value is checked, and the run has no cutoff
             energy_cutoff=ecut_run,
+            dynamic_time_step=1,  # the reference updates dt_effective as it runs
             dt=f("dt", 0.01, float),
             energy_trial=f("energy", 0.0, float),
             energy_estimated=f("energy", 0.0, float),

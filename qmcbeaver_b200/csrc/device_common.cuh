@@ -121,6 +121,7 @@ struct Layout {
 struct RunCfg {
   int run_type, sampling, qf_mod, emod, reweighting, old_walker_acceptance, limit_branching, ecut;
   int exact_gf;  // single-electron moves: Green's functions of the moved electron only
+  int dyn_dt;    // reweight with the running effective time step (EnergyCtl::dt_eff)
   double qf_a, dt, dt_eff;
   double branching_threshold, fusion_threshold;
   double e_orig, rel_cutoff;

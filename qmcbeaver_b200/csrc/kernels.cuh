@@ -38,6 +38,8 @@ enum StatIdx {
   ST_RUN_SUM_W,   // running sums for E_est (kept across calls)
   ST_RUN_SUM_WE,
   ST_RUN_COUNT,   // samples in the running sums
+  ST_RUN_SUM_WPD2,  // running sums of w p dR^2 and w dR^2 for the effective time step
+  ST_RUN_SUM_WD2,
   ST_COUNT
 };
 
@@ -45,6 +47,7 @@ enum StatIdx {
 // seen by the following launches without a host round trip).
 struct EnergyCtl {
   double e_trial, e_est, target_weight, pop_control;
+  double dt_eff;  // effective time step of the reweighting (RunCfg::dyn_dt)
 };
 
 // Shared-memory doubles needed by one warp.
@@ -858,7 +861,7 @@ __device__ __forceinline__ bool metropolis_reweight(const DevSys &S, const RunCf
         rw = accept ? 0.5 * (St + So) : So;
       else
         rw = p * 0.5 * (So + St) + (1.0 - p) * So;
-      const double dW = exp(rw * cfg.dt_eff);
+      const double dW = exp(rw * (cfg.dyn_dt ? ectl->dt_eff : cfg.dt_eff));
       if (new_age - cfg.old_walker_acceptance > 0)
         w *= 0.9;
       else
@@ -878,6 +881,14 @@ __device__ __forceinline__ bool metropolis_reweight(const DevSys &S, const RunCf
       atomicAdd(&stats[ST_RUN_SUM_W], w);
       atomicAdd(&stats[ST_RUN_SUM_WE], w * Eobs);
       atomicAdd(&stats[ST_RUN_COUNT], 1.0);
+      if (cfg.dyn_dt) {
+        // distance the moved electron was proposed to go, as
+        // QMCWalker::calculateObservables samples it (QMcBeaver/src/QMCWalker.cpp:2176-2178, 2376-2383)
+        const double d2 = (rn[0] - ro[0]) * (rn[0] - ro[0]) + (rn[1] - ro[1]) * (rn[1] - ro[1]) +
+                          (rn[2] - ro[2]) * (rn[2] - ro[2]);
+        atomicAdd(&stats[ST_RUN_SUM_WPD2], w * p * d2);
+        atomicAdd(&stats[ST_RUN_SUM_WD2], w * d2);
+      }
     }
   }
   if (lane == 0) {
@@ -1474,8 +1485,12 @@ __global__ void k_copy(double *state, Layout L, const int2 *copies, const int *c
 // E_est from the running weighted energy average and
 // E_T = E_est - c ln(W / W0) (QMCManager::updateEstimatedEnergy /
 // updateTrialEnergy, QMcBeaver/src/QMCManager.cpp:2247-2310).
-__device__ __forceinline__ void update_energy(EnergyCtl *ectl, const double *stats, int min_samples_ok)
+// dyn_dt: also the effective time step dt <w p dR^2> / <w dR^2>
+// (QMCDerivativeProperties::getEffectiveTimeStep, QMcBeaver/src/QMCDerivativeProperties.cpp:25-42).
+__device__ __forceinline__ void update_energy(EnergyCtl *ectl, const double *stats, int min_samples_ok, int dyn_dt,
+                                              double dt)
 {
+  if (dyn_dt && stats[ST_RUN_SUM_WD2] > 1e-20) ectl->dt_eff = dt * stats[ST_RUN_SUM_WPD2] / stats[ST_RUN_SUM_WD2];
   double sw = stats[ST_RUN_SUM_W];
   // E_est follows the running average once it holds 100 samples
   // (QMCManager::updateEstimatedEnergy, QMcBeaver/src/QMCManager.cpp:2247-2261)
@@ -1485,10 +1500,10 @@ __device__ __forceinline__ void update_energy(EnergyCtl *ectl, const double *sta
   ectl->e_trial = ectl->e_est - ectl->pop_control * lr;
 }
 
-__global__ void k_energy(EnergyCtl *ectl, const double *stats, int min_samples_ok)
+__global__ void k_energy(EnergyCtl *ectl, const double *stats, int min_samples_ok, int dyn_dt, double dt)
 {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  update_energy(ectl, stats, min_samples_ok);
+  update_energy(ectl, stats, min_samples_ok, dyn_dt, dt);
 }
 
 // Packs R, weight, E_L, log|psi|, sign of the first n live walkers into

@@ -133,7 +133,7 @@ __global__ void k_energy_group(const GroupMember *__restrict__ gm, int nm, int t
   if (m >= nm) return;
   const GroupMember &G = gm[m];
   if (!G.dmc || group_step(G, t) % G.S.N != 0) return;
-  update_energy(G.ectl, G.stats, 1);
+  update_energy(G.ectl, G.stats, 1, G.cfg.dyn_dt, G.cfg.dt);
 }
 
 }  // namespace qmcb

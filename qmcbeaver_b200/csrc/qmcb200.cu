@@ -187,6 +187,7 @@ static RunCfg make_cfg(const qmcb_run_params &p)
   c.limit_branching = p.limit_branching;
   c.ecut = p.energy_cutoff;
   c.exact_gf = p.exact_single_electron_gf;
+  c.dyn_dt = p.dynamic_time_step;
   c.e_orig = p.energy_original != 0.0 ? p.energy_original : (p.energy_estimated != 0.0 ? p.energy_estimated : -1.0);
   c.rel_cutoff = p.rel_cutoff > 0 ? p.rel_cutoff : 1e300;
   return c;
@@ -978,7 +979,7 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
   if (p->run_type < 0 || p->run_type > 1 || p->sampling < 0 || p->sampling > 2 || p->qf_modification < 0 ||
       p->qf_modification > 2 || p->energy_modification < 0 || p->energy_modification > 2 || p->reweighting < 0 ||
       p->reweighting > 2 || p->energy_cutoff < 0 || p->energy_cutoff > 2 || p->exact_single_electron_gf < 0 ||
-      p->exact_single_electron_gf > 1)
+      p->exact_single_electron_gf > 1 || p->dynamic_time_step < 0 || p->dynamic_time_step > 1)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");
   if (p->precision != QMCB_PREC_FP64 && p->precision != QMCB_PREC_MIXED)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown precision");
@@ -998,6 +999,7 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
     ec.e_est = p->energy_estimated;
     ec.target_weight = p->target_walkers > 0 ? p->target_walkers : h->target_weight;
     ec.pop_control = p->population_control;
+    ec.dt_eff = p->dt_effective;
     CK(cudaMemcpyAsync(h->d_ectl, &ec, sizeof(ec), cudaMemcpyHostToDevice, h->stream));
     CK(cudaEventRecord(h->ectl_ev[k], h->stream));
   }
@@ -1156,6 +1158,7 @@ int qmcb_init_walkers(qmcb_handle *h, int n, const double *R)
   ec.e_est = h->params.energy_estimated;
   ec.target_weight = h->params.target_walkers > 0 ? h->params.target_walkers : n;
   ec.pop_control = h->params.population_control;
+  ec.dt_eff = h->params.dt_effective;
   h->target_weight = ec.target_weight;
   CK(cudaMemcpyAsync(h->d_ectl, &ec, sizeof(ec), cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync(h->d_stats, 0, sizeof(double) * ST_COUNT, st));
@@ -1217,7 +1220,7 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps, double *du
       }
       {
         ProfScope ps(h, QMCB_KERNEL_ENERGY, st);
-        k_energy<<<1, 32, 0, st>>>(h->d_ectl, h->d_stats, 1);
+        k_energy<<<1, 32, 0, st>>>(h->d_ectl, h->d_stats, 1, cfg.dyn_dt, cfg.dt);
         ps.end(st);
       }
     }

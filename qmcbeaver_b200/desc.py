@@ -50,6 +50,7 @@ class RunParams(C.Structure):
         ("seed", C.c_uint64), ("population_control", C.c_double), ("target_walkers", C.c_int),
         ("reweight_start_step", C.c_int), ("energy_original", C.c_double), ("rel_cutoff", C.c_double),
         ("limit_branching", C.c_int), ("energy_cutoff", C.c_int), ("exact_single_electron_gf", C.c_int),
+        ("dynamic_time_step", C.c_int),
     ]
 
 

@@ -87,7 +87,7 @@ def test_dmc_energy_agrees_with_reference_program():
                           reweighting=QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED, energy_cutoff=QMCB_ECUT_NONE,
                           population_control=pc, target_walkers=W, energy_trial=e, energy_estimated=e,
                           energy_original=e, old_walker_acceptance=30, reweight_start_step=100, refresh_interval=50,
-                          seed=77, rel_cutoff=100.0)
+                          seed=77, rel_cutoff=100.0, dynamic_time_step=1)
 
     f = QMCB200Functions(s, 3 * W, params(1.0 / dt, -76.36))
     f.init_walkers(s.initial_positions(W, seed=3))
