@@ -383,6 +383,45 @@ def run_reference_arm(args, rank: int):
     print(json.dumps(out))
 
 
+def profile_case(name: str) -> None:
+    """Small fixed workloads for kernel captures (one GPU, a few hundred MB
+    on the device): "multidet_small" runs 4N importance-sampled VMC steps of
+    the 12-electron / 12-determinant system with 8,192 walkers (the
+    several-determinant move kernel); "group_small" runs three batches of 40
+    steps of 16 molecules of 4-40 electrons (256-2,048 walkers each) as one
+    group in configuration 0 (the group move kernel)."""
+    from qmcbeaver_b200.api import QMCB200Functions, QMCB200Group
+    from qmcbeaver_b200.desc import run_params
+    from qmcbeaver_b200.system import make_system
+    if name == "multidet_small":
+        s = make_system("vmc_multidet_12e", seed=1)
+        W = 8192
+        f = QMCB200Functions(s, W, run_params(sampling=1, qf_modification=2, dt=0.01, seed=3, rel_cutoff=0.0))
+        f.init_walkers(s.initial_positions(W, seed=1))
+        st = f.run_steps(0, 4 * s.n_electrons)
+        print("ok", st.n_moves)
+        f.close()
+    elif name == "group_small":
+        from qmcbeaver_b200.serving import make_jobs
+        jobs = make_jobs(16, rate=1.0, seed=29, electrons=(4, 40), walkers=(256, 2048), orbitals="random")
+        hs = []
+        for j in jobs:
+            f = QMCB200Functions(j.system, j.walkers, run_params(sampling=1, qf_modification=2, dt=0.01,
+                                                                 seed=j.seed, rel_cutoff=0.0))
+            f.init_walkers(j.system.initial_positions(j.walkers, seed=j.seed))
+            hs.append(f)
+        g = QMCB200Group(hs)
+        g.set_config(0)
+        for b in range(3):
+            st = g.run_steps(b * 40, 40)
+        print("ok", sum(x.n_moves for x in st), g.config())
+        g.close()
+        for f in hs:
+            f.close()
+    else:
+        raise SystemExit(f"unknown case {name}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,7 +434,12 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and serving sections")
     ap.add_argument("--serve-jobs", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=20.0)
+    ap.add_argument("--case", choices=["multidet_small", "group_small"],
+                    help="run one small profiling workload instead of the benchmark")
     args = ap.parse_args()
+    if args.case:
+        profile_case(args.case)
+        return
     if args.warmup < 3:
         args.warmup = 3
 
