@@ -9,7 +9,8 @@ Each fixture stores the system as this repository's reader builds it from
 the input (qmcbeaver_b200.ckmf; system arrays, not the input text), walker
 positions and, per call of a sequence -- a full evaluation, then
 single-electron moves with rollbacks (QMcBeaver/src/QMCWalker.cpp:254-266)
-and an electron placed near a nucleus every third move -- the reference's
+and an electron placed near a nucleus every third move; full evaluations
+at perturbed positions only, for the inputs of FULL_ONLY -- the reference's
 log|psi|, sign, grad psi / psi, modified drift, lap psi / psi, E_L,
 potentials and singular flag.
 
@@ -36,7 +37,14 @@ CASES = {
     "be_mcscf": ("examples/BeMCSCF.ckmf", 4, 16),   # 10 determinants, cusps
     "ne0p": ("examples/ne0P.ckmf", 4, 24),          # plain Slater-Jastrow
     "annulene": ("examples/10_Annulene-heart-DZd_CCSDT.HF_CC-PVDZ.DMC.ckmf", 3, 40),  # 70 electrons, cusps
+    # 28 atoms, 76 electrons, 516 basis functions, FixedCuspPade, cusps: full
+    # evaluations only -- the reference's one-electron path copies derivative
+    # rows with the full orbital-row width (QMcBeaver/src/QMCWalkerData.cpp:80-93,
+    # QMcBeaver/include/Array2D.h:986), wrong when more orbitals are listed
+    # than occupied (516 listed, 76 per spin occupied)
+    "hmx": ("test/hmx.ckmf", 3, 6),
 }
+FULL_ONLY = {"hmx"}
 QF, DT = 2, 0.01
 
 
@@ -48,7 +56,8 @@ def run_case(name: str) -> None:
     path = os.path.join(REF_INPUTS, rel)
     text = open(path).read()
     s = read_ckmf(path).to_system()
-    ref = ReferenceEvaluator(s, qf_mod=QF, dt=DT, ckmf_text=text, one_e_per_iter=1)
+    full_only = name in FULL_ONLY
+    ref = ReferenceEvaluator(s, qf_mod=QF, dt=DT, ckmf_text=text, one_e_per_iter=0 if full_only else 1)
     rng = np.random.default_rng(7)
     R = s.initial_positions(W, seed=13)
     N = s.n_electrons
@@ -63,7 +72,10 @@ def run_case(name: str) -> None:
 
     call(-1, R)
     prev = None
-    for m in range(moves):
+    for m in range(moves if full_only else 0):
+        R = R + 0.15 * rng.standard_normal(R.shape)
+        call(-1, R)
+    for m in range(0 if full_only else moves):
         e = (m * 5) % N  # both spins, not in order
         if m % 6 == 5 and prev is not None:
             pe, pr = prev
@@ -79,6 +91,10 @@ def run_case(name: str) -> None:
         call(e, R)
         prev = (e, old)
     keys = ["log_abs_psi", "sign", "grad", "mod_grad", "lap", "e_local", "potential", "ne", "ee", "singular"]
+    if full_only:
+        # the all-electron path leaves the per-spin determinants that log|psi|
+        # and the sign are read from unset
+        keys = [k for k in keys if k not in ("log_abs_psi", "sign")]
     data = {k: np.stack([o[k] for o in outs]) for k in keys}
     data.update(whichE=np.array(whichE), R=np.stack(Rseq), qf_mod=np.array(QF), dt=np.array(DT),
                 source=np.array(rel))

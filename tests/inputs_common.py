@@ -36,7 +36,7 @@ def replay_against_reference(s, d, evaluate, label):
         orc.evaluate(ws, R, e)
         worst = np.maximum(worst, slater_conditions(orc, ws, s))
         ref = {k: d[k][i] for k in ("log_abs_psi", "sign", "grad", "mod_grad", "lap", "e_local", "potential",
-                                     "singular")}
+                                     "singular") if k in d.files}
         amp = (np.abs(ref["lap"]) / 2 + np.abs(ref["potential"])) / np.maximum(np.abs(ref["e_local"]), 1.0)
         if s.n_det > 1:
             amp = amp * np.maximum(orc.kappa(ws), 1.0)

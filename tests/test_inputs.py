@@ -7,7 +7,7 @@ from inputs_common import INPUT_CASES, load_input_case, replay_against_reference
 
 
 def test_input_cases_present():
-    assert {"h2o", "oepi", "chkpnt", "det", "be_mcscf", "ne0p", "annulene"} <= set(INPUT_CASES)
+    assert {"h2o", "oepi", "chkpnt", "det", "be_mcscf", "ne0p", "annulene", "hmx"} <= set(INPUT_CASES)
 
 
 @pytest.mark.parametrize("case", INPUT_CASES)
