@@ -1209,8 +1209,21 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
     double *Rw = blk + L.R;
     if (lane < 3) Rw[3 * e + lane] = rn[lane];
     if (!kGInv) {
+      // the staged inverse goes back by one bulk (TMA) store of its 16-byte
+      // part, issued after every lane's shared-memory writes are fenced for
+      // the async proxy; its last odd element by plain store.  Both ends are
+      // 16-byte aligned (per-warp scratch offsets and walker-block arrays).
       TI *InvW = (TI *)(blk + L.Inv[sp]);
-      for (int t = lane; t < n * n; t += 32) InvW[t] = Inv[t];
+      const int bytes = n * n * (int)sizeof(TI), bulk = bytes & ~15;
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0 && bulk > 0) {
+        asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(InvW),
+                     "r"((unsigned)__cvta_generic_to_shared(Inv)), "r"(bulk)
+                     : "memory");
+        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+      }
+      for (int t = bulk / (int)sizeof(TI) + lane; t < n * n; t += 32) InvW[t] = Inv[t];
     } else if (lane == 0) {
       sc[SC_INVCUR_A + sp] = (double)(1 - icur);
     }
@@ -1244,6 +1257,12 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
       sc[SC_MODRATIO] = modratio;
       sc[SC_STATUS] = bad ? 1.0 : 0.0;
     }
+  }
+  if (!kGInv && accept) {
+    // the bulk store must have read the staged inverse before this warp's
+    // scratch is left (or reused for the next walker)
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+    __syncwarp();
   }
   if (!kMetropolis) {
     const double la = sp == 0 ? logdet_new : sc0[SC_LOGDET_A];
