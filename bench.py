@@ -6,16 +6,21 @@ branching, full LU refresh every 50 steps).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-One step = one single-electron move (propose, evaluate, accept/reject) of
-every live walker, plus the DMC reweight / branching on the steps that move
-electron 0.  Under torchrun each rank runs an independent walker population
-(walkers shard with no data-path collective; weak scaling); the timed region
-is bracketed by barriers and the max time over ranks is reported.
+One bench step = one whole DMC block of the workload: lcm(N, refresh
+interval) = 150 single-electron moves (propose, evaluate, accept/reject) of
+every live walker, i.e. 5 sweeps of the 30 electrons with their 5 reweight /
+branching passes (after each move of electron 0) and 3 full LU refreshes
+(every 50 moves), so every timed region, however short, holds the same
+share of each kind of work.  Under torchrun each rank runs an independent
+walker population (walkers shard with no data-path collective; weak
+scaling); the timed region is bracketed by barriers and the max time over
+ranks is reported.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -30,6 +35,25 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "dmc_6nuc_30e"
 DEFAULT_WALKERS = 16384
+REFRESH_INTERVAL = 50
+
+
+def block_moves(N: int) -> int:
+    """Single-electron moves per walker in one bench step: the least common
+    multiple of the sweep length N (a reweight / branching pass after every
+    move of electron 0) and the LU refresh interval."""
+    return N * REFRESH_INTERVAL // math.gcd(N, REFRESH_INTERVAL)
+
+
+def workload_config(system, walkers: int) -> dict:
+    """The workload's identity, printed the same way by both arms."""
+    N = system.n_electrons
+    return {"workload": WORKLOAD, "electrons": N, "nuclei": system.n_nuclei, "basis_functions": system.n_basis,
+            "walkers_per_gpu": walkers, "tau": 0.01, "refresh_interval": REFRESH_INTERVAL,
+            "moves_per_walker_per_step": block_moves(N),
+            "step": f"one DMC block: {block_moves(N)} single-electron moves of every walker "
+                    f"({block_moves(N) // N} sweeps with their reweight/branching passes, "
+                    f"{block_moves(N) // REFRESH_INTERVAL} LU refreshes)"}
 
 
 def bytes_per_move(n: int, N: int) -> int:
@@ -118,7 +142,7 @@ def dmc_params(seed: int, e0: float, reweight_start: int = 0):
     from qmcbeaver_b200.desc import (QMCB_DMC, QMCB_ECUT_BDJM_PUSH88, QMCB_EMOD_UMRIGAR93, QMCB_IMPORTANCE_SAMPLING,
                                      QMCB_QF_UMRIGAR93_UNEQUAL, run_params)
     return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
-                      energy_modification=QMCB_EMOD_UMRIGAR93, dt=0.01, refresh_interval=50,
+                      energy_modification=QMCB_EMOD_UMRIGAR93, dt=0.01, refresh_interval=REFRESH_INTERVAL,
                       reweight_start_step=reweight_start, energy_trial=e0, energy_estimated=e0, energy_original=e0,
                       seed=seed, energy_cutoff=QMCB_ECUT_BDJM_PUSH88, population_control=1.0 / 0.01)
 
@@ -161,13 +185,14 @@ def mixed_section(system, W, e0, rank, args):
     p.precision = QMCB_PREC_MIXED
     f.set_params(p)
     f.init_walkers(R_eq)
-    f.run_steps(0, args.warmup)
-    steps = max(args.steps // 4, 3 * N)
+    P = block_moves(N)
+    f.run_steps(0, args.warmup * P)
+    steps = max(args.steps // 4, 1) * P
     torch.cuda.synchronize()
     s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stream = torch.cuda.ExternalStream(f.stream)
     s_ev.record(stream)
-    st = f.run_steps(args.warmup, steps)
+    st = f.run_steps(args.warmup * P, steps)
     e_ev.record(stream)
     torch.cuda.synchronize()
     ms, moves = aggregate_timing(s_ev.elapsed_time(e_ev), st.n_moves)
@@ -357,6 +382,11 @@ def batching_section(args):
 
 
 def run_reference_arm(args, rank: int):
+    """The reference's own CPU program on the same workload and bench step:
+    every step is one run of the unmodified QMcBeaver.x per host core (64
+    walkers each, distinct seeds) over one DMC block of single-electron moves;
+    walker-moves/s from the reference's own "Entire Step" timer, summed over
+    the processes, averaged over the timed steps."""
     if rank != 0:
         return
     from qmcbeaver_b200.system import make_system
@@ -366,70 +396,37 @@ def run_reference_arm(args, rank: int):
     if not refrun.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/QMcBeaver.x not built (reference tree absent at build time)"}))
         return
-    # one short untimed warm-up run, then one bounded timed sample (~10 s of
-    # CPU work on every host core); the reference's own timers give us/move
-    cpu_reference_sample(system, walkers=4, steps=30, procs=procs, e0=E_GUESS)
-    last = cpu_reference_sample(system, walkers=64, steps=1500, procs=procs, e0=E_GUESS)
-    vals = [last["moves_per_s"]]
+    P = block_moves(system.n_electrons)
+    walkers = 64
+    for _ in range(args.warmup):
+        cpu_reference_sample(system, walkers=walkers, steps=P, procs=procs, e0=E_GUESS)
+    vals, last = [], None
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        last = cpu_reference_sample(system, walkers=walkers, steps=P, procs=procs, e0=E_GUESS)
+        vals.append(last["moves_per_s"])
+    wall = time.perf_counter() - t0
     v = float(np.mean(vals)) if vals else 0.0
-    sample = (f"{procs} processes x {last['walkers']} walkers x {last['steps']} steps of the reference's "
+    sample = (f"each step: {procs} processes x {walkers} walkers x {P} single-electron moves of the reference's "
               f"{last['mode']} ({last.get('note', 'full DMC')})")
     out = {"metric": "walker-moves/s", "value": v, "unit": "walker-moves/s", "impl": "reference", "n_gpus": args.gpus,
-           "steps": len(vals), "warmup": args.warmup, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "walkers_per_process": last["walkers"], "processes": procs},
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": dict(workload_config(system, args.walkers), parallelism="single"),
            "cpu_baseline": {"value": v, "unit": "walker-moves/s", "cores": procs, "kind": "reference",
                             "sample": sample},
            "e2e": {"value": v, "unit": "walker-moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
 
-def profile_case(name: str) -> None:
-    """Small fixed workloads for kernel captures (one GPU, a few hundred MB
-    on the device): "multidet_small" runs 4N importance-sampled VMC steps of
-    the 12-electron / 12-determinant system with 8,192 walkers (the
-    several-determinant move kernel); "group_small" runs three batches of 40
-    steps of 16 molecules of 4-40 electrons (256-2,048 walkers each) as one
-    group in configuration 0 (the group move kernel)."""
-    from qmcbeaver_b200.api import QMCB200Functions, QMCB200Group
-    from qmcbeaver_b200.desc import run_params
-    from qmcbeaver_b200.system import make_system
-    if name == "multidet_small":
-        s = make_system("vmc_multidet_12e", seed=1)
-        W = 8192
-        f = QMCB200Functions(s, W, run_params(sampling=1, qf_modification=2, dt=0.01, seed=3, rel_cutoff=0.0))
-        f.init_walkers(s.initial_positions(W, seed=1))
-        st = f.run_steps(0, 4 * s.n_electrons)
-        print("ok", st.n_moves)
-        f.close()
-    elif name == "group_small":
-        from qmcbeaver_b200.serving import make_jobs
-        jobs = make_jobs(16, rate=1.0, seed=29, electrons=(4, 40), walkers=(256, 2048), orbitals="random")
-        hs = []
-        for j in jobs:
-            f = QMCB200Functions(j.system, j.walkers, run_params(sampling=1, qf_modification=2, dt=0.01,
-                                                                 seed=j.seed, rel_cutoff=0.0))
-            f.init_walkers(j.system.initial_positions(j.walkers, seed=j.seed))
-            hs.append(f)
-        g = QMCB200Group(hs)
-        g.set_config(0)
-        for b in range(3):
-            st = g.run_steps(b * 40, 40)
-        print("ok", sum(x.n_moves for x in st), g.config())
-        g.close()
-        for f in hs:
-            f.close()
-    else:
-        raise SystemExit(f"unknown case {name}")
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=6000)
-    ap.add_argument("--warmup", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=40, help="timed bench steps (whole DMC blocks, 150 moves each)")
+    ap.add_argument("--warmup", type=int, default=3, help="untimed bench steps (whole DMC blocks)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--walkers", type=int, default=DEFAULT_WALKERS)
-    ap.add_argument("--e2e-steps", type=int, default=120)
+    ap.add_argument("--e2e-steps", type=int, default=2, help="bench steps timed end to end, one API call per move")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and serving sections")
     ap.add_argument("--serve-jobs", type=int, default=24)
@@ -483,8 +480,9 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    P = block_moves(N)
     # warm-up
-    f.run_steps(0, args.warmup)
+    f.run_steps(0, args.warmup * P)
     stream = torch.cuda.ExternalStream(f.stream)
     f.set_profiling(True)
     f.kernel_stats(reset=True)
@@ -494,7 +492,7 @@ def main():
     t_end = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         t_start.record(stream)
-        st = f.run_steps(args.warmup, args.steps)
+        st = f.run_steps(args.warmup * P, args.steps * P)
         t_end.record(stream)
         torch.cuda.synchronize()
     barrier()
@@ -528,7 +526,8 @@ def main():
     p = dmc_params(seed=replica_seed(77, rank), e0=e0)
     e_est = e0
     sw = swe = 0.0
-    step0 = args.warmup + args.steps
+    step0 = (args.warmup + args.steps) * P
+    e2e_moves_per_walker = args.e2e_steps * P
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_moves = 0.0
@@ -537,8 +536,8 @@ def main():
     # energy follows the statistics one step behind
     f.set_params(p)
     f.run_steps_async(step0, 1)
-    for s in range(args.e2e_steps):
-        if s + 1 < args.e2e_steps:
+    for s in range(e2e_moves_per_walker):
+        if s + 1 < e2e_moves_per_walker:
             f.set_params(p)
             f.run_steps_async(step0 + s + 1, 1)
         st2 = f.steps_collect()
@@ -555,10 +554,11 @@ def main():
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_s, e2e_moves = aggregate_timing(e2e_s, e2e_moves)
-    e2e = {"value": e2e_moves / e2e_s, "unit": "walker-moves/s", "h2d_bytes_per_step": ctypes.sizeof(RunParams),
-           "d2h_bytes_per_step": ctypes.sizeof(StepStats) + 16,
-           "api": "qmcb_set_params + qmcb_run_steps_async(step, 1) per step, statistics collected one step "
-                  "behind with qmcb_steps_collect (host E_T in, step statistics out)"}
+    e2e = {"value": e2e_moves / e2e_s, "unit": "walker-moves/s", "h2d_bytes_per_step": P * ctypes.sizeof(RunParams),
+           "d2h_bytes_per_step": P * (ctypes.sizeof(StepStats) + 16),
+           "steps": args.e2e_steps, "ms_per_step": 1e3 * e2e_s / max(args.e2e_steps, 1),
+           "api": "qmcb_set_params + qmcb_run_steps_async(step, 1) per single-electron move, statistics collected "
+                  "one move behind with qmcb_steps_collect (host E_T in, move statistics out); bytes per bench step"}
 
     # reference-facing evaluate (QMCFunctions::evaluate shape) with host buffers
     slots = np.arange(min(W, 4096), dtype=np.int32)
@@ -582,12 +582,10 @@ def main():
     out = {"metric": "walker-moves/s", "value": value, "unit": "walker-moves/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "walkers_per_gpu": W, "electrons": N, "nuclei": system.n_nuclei,
-                      "basis_functions": system.n_basis, "tau": 0.01, "refresh_interval": 50,
-                      "walker_moves": moves, "final_walkers": st.n_walkers,
-                      "parallelism": f"replicas{world}" if world > 1 else "single",
-                      "l2": "walker state > L2 (%.0f MB per GPU)" % (2 * W * f.lay_bytes() / 1e6)
-                      if hasattr(f, "lay_bytes") else "walker state larger than L2"},
+           "config": dict(workload_config(system, W), parallelism=f"replicas{world}" if world > 1 else "single",
+                          l2="inputs larger than L2: walker state %.0f MB per GPU" % (f.state_bytes() / 1e6)),
+           "run": {"walker_moves": moves, "final_walkers": st.n_walkers,
+                   "single_electron_steps": args.steps * P, "kernel_launches_by_kind": {k: v["launches"] for k, v in ks.items()}},
            "roofline": roofline, "gpu_launches": launches, "kernels": ks, "e2e": e2e, "e2e_evaluate_api": e2e_eval,
            "energy": {"mean_weighted_E_L": ensemble["energy"], "walkers_all_ranks": ensemble["walkers"],
                       "acceptance": st.sum_accept / max(st.n_moves, 1), "singular": st.n_singular}}

@@ -361,7 +361,10 @@ int qmcb_set_walker_weights(qmcb_handle *h, int n, const double *w);
 /* One nonunit-weight branching pass over the live walkers
  * (QMCRun::branchWalkers / nonunitWeightBranching,
  * QMcBeaver/src/QMCRun.cpp:89-127,740-814); `step` selects the random
- * stream of the fusion draws.  Returns the new live count in *n_live. */
+ * stream of the fusion draws, the draw of a fused pair is keyed by the live-list
+ * position of its first member, and a split is decided on the weight before
+ * fusion (a fused survivor does not split in the same pass, as in the
+ * reference's single loop).  Returns the new live count in *n_live. */
 int qmcb_branch(qmcb_handle *h, int step, int *n_live);
 
 /* Kernel timing: when enabled, qmcb_run_steps records CUDA events around
@@ -394,8 +397,10 @@ void *qmcb_stream(qmcb_handle *h);
  *
  * Same decisions as qmcb_branch on a plain list of n walker weights (split
  * above branching_threshold, die below 0.01, fuse pairs below
- * fusion_threshold in list order, the draw of a pair keyed by (seed, index of
- * its first member, step)), without the branch-recommendation rules.
+ * fusion_threshold in list order, the draw of a pair keyed by (seed, list
+ * position of its first member, step), the split test on the weight before
+ * fusion), without the branch-recommendation rules.  qmcb_branch keys its
+ * draws by live-list position as well, so the two agree for any list order.
  * Outputs: d_weight_out / d_parent_out (room for 2n entries each) receive the
  * new list -- survivors in order, split copies appended -- with each entry's
  * source index; *d_n_out the new count.  All pointers are device memory;

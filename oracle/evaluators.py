@@ -24,7 +24,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libqmcref.so")
 REF_EXE = os.path.join(HERE, "_ref", "QMcBeaver.x")
-REFERENCE_TREE = os.environ.get("QMCB_REFERENCE_TREE", "/root/reference/QMcBeaver")
+# The QMcBeaver source tree the checker builds and reads its input files from:
+# QMCB_REFERENCE_TREE, else the read-only mount of the build container.  Every
+# test and fixture script takes the location from here.
+REFERENCE_TREE = os.environ.get("QMCB_REFERENCE_TREE") or "/root/reference/QMcBeaver"
 
 SCALARS = ["e_local", "kinetic", "potential", "ne", "ee", "U", "U_xx", "D_xx", "det_a", "det_b", "singular",
            "log_abs_psi", "sign", "psi"]

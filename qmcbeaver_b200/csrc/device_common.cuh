@@ -45,6 +45,7 @@ enum Sc {
   SC_MDCUR_B,
   SC_INVCUR_A,     // inverse kept in HBM (large spins): current copy (0/1) of the spin's inverse
   SC_INVCUR_B,
+  SC_FUSED,        // branching pass: 1 on the survivor of a fused pair until the pass's split test
   SC_COUNT
 };
 constexpr int kScalars = 24;  // padded

@@ -1260,7 +1260,12 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   }
   if (!kGInv && accept) {
     // the bulk store must have read the staged inverse before this warp's
-    // scratch is left (or reused for the next walker)
+    // scratch is left (or reused for the next walker).  .read waits for the
+    // shared-memory source only, not for the global writes: correct because
+    // every launch of k_move / k_move_group moves each walker at most once,
+    // so the kernel boundary orders these writes before the next read of the
+    // inverse.  A kernel that re-reads a walker's inverse within one launch
+    // must wait with cp.async.bulk.wait_group 0 (full completion) instead.
     if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
     __syncwarp();
   }
@@ -1294,7 +1299,10 @@ __global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg,
 // half the weight each (the copy is appended to the list), walkers below
 // 0.01 die, walkers below the fusion threshold are paired in list order and
 // one of each pair survives with the sum of the weights (probability
-// w1 / (w1 + w2) for the first).  Dead slots go on the free stack; copies
+// w1 / (w1 + w2) for the first; the uniform draw of a pair is keyed by
+// (seed, position of its first member in the live list, step)).  The split
+// test uses the weight before fusion, so a fused survivor does not split in
+// the same pass.  Dead slots go on the free stack; copies
 // take slots from it and are written to the copy list for k_copy.
 // ctl: [0] n_live, [1] n_free, [2] n_copies.
 // QMCWalker::branchRecommended (limit_branching): no split for a walker that
@@ -1366,13 +1374,15 @@ __device__ __forceinline__ void branch_block(double *state, const Layout &L, int
     double *wb = &state[(size_t)sb * L.stride + L.sc + SC_WEIGHT];
     double w1 = *wa, w2 = *wb, w3 = w1 + w2;
     double u[4];
-    rng_uniform4(seed, (uint32_t)sa, (uint32_t)step, 7u, u);
+    rng_uniform4(seed, (uint32_t)ia, (uint32_t)step, 7u, u);
     if (u[0] < w1 / w3) {
       *wa = w3;
       *wb = -1.0;  // marked dead
+      wa[SC_FUSED - SC_WEIGHT] = 1.0;
     } else {
       *wb = w3;
       *wa = -1.0;
+      wb[SC_FUSED - SC_WEIGHT] = 1.0;
     }
   }
   __syncthreads();
@@ -1423,7 +1433,12 @@ __device__ __forceinline__ void branch_block(double *state, const Layout &L, int
     int slot = i < n_keep ? live_tmp[i] : -1;
     double *wp = slot >= 0 ? &state[(size_t)slot * L.stride + L.sc + SC_WEIGHT] : nullptr;
     double w = wp ? *wp : 0.0;
-    int sp = (slot >= 0 && w > thr_split &&
+    // the split test reads the weight before fusion, as the reference's single
+    // pass does: the survivor of a fused pair (weight below the fusion
+    // threshold before) never splits in the same pass
+    const bool fused = wp && wp[SC_FUSED - SC_WEIGHT] != 0.0;
+    if (fused) wp[SC_FUSED - SC_WEIGHT] = 0.0;
+    int sp = (slot >= 0 && !fused && w > thr_split &&
               branch_recommended(state + (size_t)slot * L.stride + L.sc, e_orig, limit_branching)) ? 1 : 0;
     unsigned bs = __ballot_sync(QMCB_FULL_MASK, sp);
     int ps = __popc(bs & ((1u << lane) - 1));

@@ -239,9 +239,10 @@ static __device__ __align__(256) double g_noalloc_weight[QMCB_NOALLOC_MAX_WALKER
 static __device__ __align__(256) int g_noalloc_index[QMCB_NOALLOC_MAX_WALKERS];
 
 // Same decisions as k_branch (nonunit-weight branching, fusion pairs in list
-// order, random stream of a pair keyed by its first member's list index),
-// on plain arrays: survivors keep their order, split copies are appended.
-// w_out / parent_out need room for 2 n entries.
+// order, random stream of a pair keyed by its first member's list index, the
+// split test on the weight before fusion), on plain arrays: survivors keep
+// their order, split copies are appended.  w_out / parent_out need room for
+// 2 n entries.
 __global__ void __launch_bounds__(1024) k_branch_list(const double *w_in, int n, double thr_split, double thr_fuse,
                                                       uint64_t seed, int step, double *w_work, int *idx,
                                                       double *w_out, int *parent_out, int *n_out)
@@ -314,7 +315,8 @@ __global__ void __launch_bounds__(1024) k_branch_list(const double *w_in, int n,
     int j = c0 + tid;
     int src = j < nk ? idx[j] : -1;
     double w = src >= 0 ? w_work[src] : 0.0;
-    int sp = (src >= 0 && w > thr_split) ? 1 : 0;
+    // w_in holds the weight before fusion: a fused survivor does not split
+    int sp = (src >= 0 && w_in[src] > thr_split) ? 1 : 0;
     int ex, tot;
     block_scan(sp, ex, tot);
     if (src >= 0) {

@@ -20,8 +20,8 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 OUT = os.path.join(HERE, "energies")
-REF_INPUTS = "/root/reference/QMcBeaver"
 sys.path.insert(0, ROOT)
+from oracle.evaluators import REFERENCE_TREE as REF_INPUTS  # noqa: E402
 
 CASES = {
     # name: (input, processes, walkers, steps, equilibration steps, extra flags)

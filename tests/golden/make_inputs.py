@@ -25,8 +25,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 OUT = os.path.join(HERE, "inputs")
-REF_INPUTS = "/root/reference/QMcBeaver"
 sys.path.insert(0, ROOT)
+from oracle.evaluators import REFERENCE_TREE as REF_INPUTS  # noqa: E402
 
 CASES = {
     # name: (input, walkers, moves)

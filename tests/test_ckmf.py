@@ -9,12 +9,12 @@ import sys
 import numpy as np
 import pytest
 
-from oracle.evaluators import reference_available
+from oracle.evaluators import REFERENCE_TREE, reference_available
 from qmcbeaver_b200.ckmf import CkmfError, patch_flags, read_ckmf, strip_three_body
 from qmcbeaver_b200.system import Cambridge2, Pade, make_system, with_cambridge2
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_INPUTS = "/root/reference/QMcBeaver"
+REF_INPUTS = REFERENCE_TREE
 
 
 def _same_tables(a, b):

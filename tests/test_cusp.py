@@ -11,12 +11,12 @@ import sys
 import numpy as np
 import pytest
 
-from oracle.evaluators import reference_available
+from oracle.evaluators import REFERENCE_TREE, reference_available
 from qmcbeaver_b200.api import fit_cusps
 from qmcbeaver_b200.system import make_system
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_INPUTS = "/root/reference/QMcBeaver"
+REF_INPUTS = REFERENCE_TREE
 HAVE_REF = reference_available() and os.path.isdir(REF_INPUTS)
 
 _SYSTEM = r"""

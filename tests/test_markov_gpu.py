@@ -79,37 +79,36 @@ def test_vmc_energy_agrees_with_oracle_chain():
     assert 0.2 < acc / (sweeps - warm) < 0.99
 
 
-def branch_restatement(w, slots, thr, fuse, seed, step):
-    """QMCRun::nonunitWeightBranching (QMcBeaver/src/QMCRun.cpp:740-814) over
-    the live list with the device's fusion draws."""
+def branch_restatement(w, thr, fuse, seed, step):
+    """QMCRun::nonunitWeightBranching (QMcBeaver/src/QMCRun.cpp:740-814): one
+    pass over the live list in which a walker above the threshold splits
+    (copy appended in list order), one below 0.01 dies and ones below the
+    fusion threshold fuse in pairs; the fusion draws are the device's, keyed
+    by the list position of a pair's first member."""
     w = list(w)
     keep = [True] * len(w)
+    adds = []
     pend = None
     for i in range(len(w)):
-        if w[i] > thr or w[i] < 0.01:
-            if w[i] < 0.01:
-                keep[i] = False
-            continue
-        if w[i] < fuse:
+        if w[i] > thr:
+            w[i] = w[i] / 2
+            adds.append(i)
+        elif w[i] < 0.01:
+            keep[i] = False
+        elif w[i] < fuse:
             if pend is None:
                 pend = i
             else:
                 w1, w2 = w[pend], w[i]
                 w3 = w1 + w2
-                if uniform4(seed, slots[pend], step, 7)[0] < w1 / w3:
+                if uniform4(seed, pend, step, 7)[0] < w1 / w3:
                     w[pend] = w3
                     keep[i] = False
                 else:
                     w[i] = w3
                     keep[pend] = False
                 pend = None
-    out = [w[i] for i in range(len(w)) if keep[i]]
-    adds = []
-    for j in range(len(out)):
-        if out[j] > thr:
-            out[j] = out[j] / 2
-            adds.append(out[j])
-    return out + adds
+    return [w[i] for i in range(len(w)) if keep[i]] + [w[i] for i in adds]
 
 
 def test_branching_matches_reference_rule():
@@ -122,11 +121,26 @@ def test_branching_matches_reference_rule():
     w[rng.random(W) < 0.05] = 0.005
     f.set_walker_weights(w)
     n = f.branch(step=77)
-    expect = branch_restatement(w, list(range(W)), 2.0, 0.45, 4242, 77)
+    expect = branch_restatement(w, 2.0, 0.45, 4242, 77)
     got = f.get_walkers()["weight"]
     assert n == len(expect)
     np.testing.assert_allclose(got, expect, rtol=0, atol=0)
     assert abs(got.sum() - sum(expect)) < 1e-9
+    # a second pass on the reordered list (deaths and appended copies), with a
+    # fusion threshold above half the branching threshold: fused survivors
+    # whose summed weight exceeds the branching threshold must not split
+    w2 = np.exp(rng.normal(0.0, 0.8, n))
+    w2[rng.random(n) < 0.3] = 1.3
+    w2[rng.random(n) < 0.05] = 0.005
+    f.set_params(run_params(run_type=QMCB_DMC, seed=4242, limit_branching=0, branching_threshold=2.0,
+                            fusion_threshold=1.5))
+    f.set_walker_weights(w2)
+    n2 = f.branch(step=78)
+    expect2 = branch_restatement(w2, 2.0, 1.5, 4242, 78)
+    got2 = f.get_walkers()["weight"]
+    assert n2 == len(expect2)
+    np.testing.assert_allclose(got2, expect2, rtol=0, atol=0)
+    assert np.sum(np.array(expect2) > 2.0) > 0  # fused survivors above the threshold stay whole
 
 
 def test_branching_copies_walker_state():

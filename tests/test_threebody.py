@@ -9,13 +9,13 @@ import sys
 import numpy as np
 import pytest
 
-from oracle.evaluators import reference_available
+from oracle.evaluators import REFERENCE_TREE, reference_available
 from qmcbeaver_b200.ckmf import read_ckmf
 from qmcbeaver_b200.system import make_system
 from qmcbeaver_b200.threebody import ThreeBody, constraint_matrix, dependency_matrix, file_order, random_three_body
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_INPUTS = "/root/reference/QMcBeaver"
+REF_INPUTS = REFERENCE_TREE
 HAVE_REF = reference_available() and os.path.isdir(REF_INPUTS)
 
 
