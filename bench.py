@@ -144,7 +144,8 @@ def dmc_params(seed: int, e0: float, reweight_start: int = 0):
     return run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
                       energy_modification=QMCB_EMOD_UMRIGAR93, dt=0.01, refresh_interval=REFRESH_INTERVAL,
                       reweight_start_step=reweight_start, energy_trial=e0, energy_estimated=e0, energy_original=e0,
-                      seed=seed, energy_cutoff=QMCB_ECUT_BDJM_PUSH88, population_control=1.0 / 0.01)
+                      seed=seed, energy_cutoff=QMCB_ECUT_BDJM_PUSH88, population_control=1.0 / 0.01,
+                      walker_deletion=1)
 
 
 EQUIL_SWEEPS = 5
@@ -166,61 +167,105 @@ def cpu_reference_sample(system, walkers: int, steps: int, procs: int, e0: float
     return r
 
 
-def mixed_section(system, W, e0, rank, args):
-    """The same DMC workload with the mixed-precision path (FP32 basis and
-    orbital rows, FP64 inverse / ratios / refresh / energies) and its local
-    energy error against the FP64 path on identical configurations."""
-    import torch
+def el_errors(system, prec, W=256, sweeps=1, seed=3, R=None):
+    """Per-walker |E_L - E_L(FP64)| of precision `prec` on identical
+    configurations: a full evaluation, then `sweeps` sweeps of
+    single-electron moves through the evaluate entry point."""
     from qmcbeaver_b200.api import QMCB200Functions
-    from qmcbeaver_b200.desc import QMCB_PREC_FP64, QMCB_PREC_MIXED, run_params
-    from qmcbeaver_b200.replicas import aggregate_timing, replica_seed
-    N = system.n_electrons
-    p = dmc_params(seed=replica_seed(91, rank), e0=-1.0, reweight_start=EQUIL_SWEEPS * N)
-    p.precision = QMCB_PREC_MIXED
-    f = QMCB200Functions(system, 2 * W, p)
-    f.init_walkers(system.initial_positions(W, seed=2000 + rank))
-    f.run_steps(0, EQUIL_SWEEPS * N)
-    R_eq = f.get_walkers()["R"]
-    p = dmc_params(seed=replica_seed(91, rank), e0=e0)
-    p.precision = QMCB_PREC_MIXED
-    f.set_params(p)
-    f.init_walkers(R_eq)
-    P = block_moves(N)
-    f.run_steps(0, args.warmup * P)
-    steps = max(args.steps // 4, 1) * P
-    torch.cuda.synchronize()
-    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stream = torch.cuda.ExternalStream(f.stream)
-    s_ev.record(stream)
-    st = f.run_steps(args.warmup * P, steps)
-    e_ev.record(stream)
-    torch.cuda.synchronize()
-    ms, moves = aggregate_timing(s_ev.elapsed_time(e_ev), st.n_moves)
-    f.close()
-    # local-energy error on identical configurations (256 walkers, 2 sweeps of moves)
-    Wc = 256
-    a = QMCB200Functions(system, Wc, run_params(precision=QMCB_PREC_FP64, qf_modification=2, dt=0.01))
-    b = QMCB200Functions(system, Wc, run_params(precision=QMCB_PREC_MIXED, qf_modification=2, dt=0.01))
-    R = np.ascontiguousarray(R_eq[:Wc])
-    sl = np.arange(Wc)
+    from qmcbeaver_b200.desc import QMCB_PREC_FP64, run_params
+    a = QMCB200Functions(system, W, run_params(precision=QMCB_PREC_FP64, qf_modification=2, dt=0.01))
+    b = QMCB200Functions(system, W, run_params(precision=prec, qf_modification=2, dt=0.01))
+    R = np.ascontiguousarray(R[:W] if R is not None else system.initial_positions(W, seed=seed))
+    sl = np.arange(W)
     a.evaluate(sl, R, -1)
     b.evaluate(sl, R, -1)
-    rng = np.random.default_rng(3)
+    rng = np.random.default_rng(seed)
     errs = []
-    for m in range(2 * N):
+    N = system.n_electrons
+    for m in range(sweeps * N):
         e = m % N
-        R[:, e] += 0.1 * rng.standard_normal((Wc, 3))
+        R[:, e] += 0.1 * rng.standard_normal((W, 3))
         x, y = a.evaluate(sl, R, e), b.evaluate(sl, R, e)
         ok = (x["status"] == 0) & (y["status"] == 0)
         errs.append(np.abs(x["e_local"] - y["e_local"])[ok])
     a.close()
     b.close()
     err = np.concatenate(errs)
-    return {"value": moves / (ms / 1e3), "unit": "walker-moves/s", "steps": steps,
-            "el_error_vs_fp64_ha": {"median": float(np.median(err)), "p90": float(np.percentile(err, 90)),
-                                    "p99": float(np.percentile(err, 99))},
-            "note": "FP32 basis and orbital rows (FP64 accumulation), FP64 inverse, determinant ratio, ratio sums, "
-                    "LU refresh and energies"}
+    return {"median": float(np.median(err)), "p99": float(np.percentile(err, 99)), "max": float(err.max()),
+            "samples": int(err.size), "within_1e-5_ha": float(np.mean(err <= 1e-5))}
+
+
+PREC_NAMES = {0: "fp64", 1: "mixed_fp32_rows", 2: "int8_slices_tcgen05"}
+
+
+def precision_section(args, rank: int):
+    """The 100-electron workload (20 nuclei, 400 basis functions, 65,536
+    walkers, DMC as the main workload) in the three arithmetic modes: plain
+    FP64 (one warp per walker, FP64 tensor-pipe contraction), FP32 basis and
+    orbital rows, and the batched tensor-core contraction of int8 digit
+    planes (tcgen05 kind::i8, FP64-equivalent rows), each timed with CUDA
+    events over two DMC blocks (200 moves per walker: 2 branching passes, 4
+    LU refreshes), with per-kernel times; then the per-walker local-energy
+    error of each mode against FP64 on identical configurations, on this
+    workload, the 30-electron one and the reference's water input."""
+    import torch
+    from qmcbeaver_b200.api import QMCB200Functions
+    from qmcbeaver_b200.desc import QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES, QMCB_PREC_MIXED
+    from qmcbeaver_b200.replicas import aggregate_timing, replica_seed
+    from qmcbeaver_b200.system import make_system, system_from_arrays
+    system = make_system("mixed_20nuc_100e", seed=1)
+    W = args.c3_walkers
+    N, n = system.n_electrons, system.n_alpha
+    out = {"workload": "mixed_20nuc_100e", "walkers": W, "electrons": N, "basis_functions": system.n_basis,
+           "modes": {}}
+    R_eq = None
+    for prec in (QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES, QMCB_PREC_MIXED):
+        p = dmc_params(seed=replica_seed(91, rank), e0=-1.0, reweight_start=10 ** 9)
+        p.precision = prec
+        f = QMCB200Functions(system, 2 * W, p)
+        f.init_walkers(system.initial_positions(W, seed=2000 + rank))
+        f.run_steps(0, 2 * N)
+        wk = f.get_walkers()
+        e0 = float(np.mean(wk["e_local"]))
+        if R_eq is None:
+            R_eq = wk["R"]
+        p = dmc_params(seed=replica_seed(91, rank), e0=e0)
+        p.precision = prec
+        f.set_params(p)
+        f.init_walkers(wk["R"])
+        f.run_steps(0, N)
+        f.set_profiling(True)
+        f.kernel_stats(reset=True)
+        steps = 2 * block_moves(N)
+        torch.cuda.synchronize()
+        s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream = torch.cuda.ExternalStream(f.stream)
+        s_ev.record(stream)
+        st = f.run_steps(N, steps)
+        e_ev.record(stream)
+        torch.cuda.synchronize()
+        ms, moves = aggregate_timing(s_ev.elapsed_time(e_ev), st.n_moves)
+        ks = f.kernel_stats(reset=True)
+        f.close()
+        out["modes"][PREC_NAMES[prec]] = {
+            "value": moves / (ms / 1e3), "unit": "walker-moves/s", "steps": steps, "ms": ms,
+            "kernels_ms": {k: round(v["ms"], 3) for k, v in ks.items() if v["launches"]},
+            "final_walkers": st.n_walkers}
+    fp = out["modes"]["fp64"]["value"]
+    for k, v in out["modes"].items():
+        v["vs_fp64"] = v["value"] / fp
+    h2o = np.load(os.path.join(ROOT, "tests", "golden", "inputs", "h2o.npz"))
+    h2o = system_from_arrays({k[4:]: h2o[k] for k in h2o.files if k.startswith("sys_")})
+    err = {}
+    for name, s, R in (("mixed_20nuc_100e", system, R_eq), ("dmc_6nuc_30e", make_system("dmc_6nuc_30e", seed=1), None),
+                       ("h2o_input", h2o, None)):
+        err[name] = {PREC_NAMES[p]: el_errors(s, p, R=R) for p in (QMCB_PREC_INT8_SLICES, QMCB_PREC_MIXED)}
+    out["el_error_vs_fp64_ha"] = err
+    out["note"] = ("int8_slices_tcgen05: basis values and MO coefficients cut into 7 int8 digit planes, "
+                   "tcgen05.mma kind::i8 with exact int32 accumulation, FP64 recombination; FP64 inverse, "
+                   "Sherman-Morrison update, ratio sums, refresh and energies. mixed_fp32_rows: FP32 basis and "
+                   "orbital rows, FP64 inverse and energies.")
+    return out
 
 
 def rows_section(args, rank: int):
@@ -281,29 +326,45 @@ def rows_section(args, rank: int):
 
 
 def serving_section(args):
-    """Poisson arrivals of VMC energy jobs (molecules drawn like the
-    uneven-batching workload, 4-40 electrons), run concurrently with
-    footprint admission, next to the same jobs solved one after another."""
-    from qmcbeaver_b200.serving import Server, make_jobs
-    kw = dict(electrons=(4, 40), walkers=(256, 2048), target_error=0.2, max_sweeps=200)
-    mix = make_jobs(args.serve_jobs, rate=args.serve_rate, seed=11, **kw)
-    res = Server(max_active=16).run(mix)
-    seq = make_jobs(args.serve_jobs, rate=args.serve_rate, seed=11, **kw)
-    ref = Server(max_active=1).run(seq)
-    same = all(abs(a.energy - b.energy) <= 1e-9 * max(1.0, abs(b.energy)) for a, b in zip(mix, seq)
-               if len(a.energies) == len(b.energies))
-    # the same arrivals with all active jobs stepped as one group per batch
-    # of 40 steps (the largest job's sweep)
-    grp = make_jobs(args.serve_jobs, rate=args.serve_rate, seed=11, **kw)
-    rg = Server(max_active=16, mode="group", batch_steps=40).run(grp)
-    return {"jobs": res["jobs"], "arrival_rate_per_s": args.serve_rate, "target_error_ha": kw["target_error"],
-            "latency_p50_s": res["latency_p50_s"], "latency_p99_s": res["latency_p99_s"],
-            "walker_moves_per_s": res["walker_moves_per_s"],
-            "sequential": {"latency_p50_s": ref["latency_p50_s"], "latency_p99_s": ref["latency_p99_s"],
-                           "walker_moves_per_s": ref["walker_moves_per_s"]},
-            "group_mode": {"latency_p50_s": rg["latency_p50_s"], "latency_p99_s": rg["latency_p99_s"],
-                           "walker_moves_per_s": rg["walker_moves_per_s"], "jobs": rg["jobs"]},
-            "same_results_alone_and_mixed": bool(same)}
+    """Serving: Poisson arrivals of VMC energy jobs at 1, 10, 30 and 100
+    jobs/s.  Synthetic molecules drawn like the uneven-batching workload
+    (4-200 electrons, basis 4N, N/5 nuclei, random orthonormal orbitals,
+    256-1,024 walkers) are run to 0.2 Ha or a sweep cap: their local-energy
+    spread (10-1,000 Ha) would need 1e9-1e12 samples for 1 mHa.  Each rate
+    runs with the jobs' handles on concurrent streams; at 10 jobs/s also as
+    one group per batch and one job at a time.  Then jobs on the reference's
+    water input (cusp replacement, three-body Jastrow), whose trial function
+    reaches the 1 mHa target of the serving workload in a few seconds of
+    device time, arrive at 1 job/s."""
+    from qmcbeaver_b200.serving import Server, make_input_jobs, make_jobs
+    from qmcbeaver_b200.system import system_from_arrays
+    kw = dict(electrons=(4, 200), walkers=(256, 1024), target_error=0.2, max_sweeps=24, orbitals="random")
+    out = {"jobs_per_rate": args.serve_jobs, "electrons": [4, 200], "target_error_ha": 0.2, "rates": {}}
+
+    def summary(r):
+        return {k: r[k] for k in ("jobs", "latency_p50_s", "latency_p99_s", "walker_moves_per_s", "wall_s")}
+
+    for rate in (1.0, 10.0, 30.0, 100.0):
+        r = Server(max_active=16).run(make_jobs(args.serve_jobs, rate=rate, seed=11, **kw))
+        out["rates"][str(rate)] = {"streams": summary(r)}
+    rate = 10.0
+    mix = make_jobs(args.serve_jobs, rate=rate, seed=11, **kw)
+    rg = Server(max_active=16, mode="group", batch_steps=50).run(make_jobs(args.serve_jobs, rate=rate, seed=11, **kw))
+    out["rates"][str(rate)]["group"] = summary(rg)
+    seq = make_jobs(args.serve_jobs, rate=rate, seed=11, **kw)
+    rs = Server(max_active=1).run(seq)
+    out["rates"][str(rate)]["one_at_a_time"] = summary(rs)
+    rm = Server(max_active=16).run(mix)
+    out["same_results_alone_and_mixed"] = bool(all(
+        abs(a.energy - b.energy) <= 1e-9 * max(1.0, abs(b.energy)) for a, b in zip(mix, seq)
+        if len(a.energies) == len(b.energies)))
+    h2o = np.load(os.path.join(ROOT, "tests", "golden", "inputs", "h2o.npz"))
+    h2o = system_from_arrays({k[4:]: h2o[k] for k in h2o.files if k.startswith("sys_")})
+    jobs = make_input_jobs(6, rate=1.0, system=h2o, seed=5, walkers=(2048, 8192), target_error=1e-3)
+    r = Server(max_active=8).run(jobs)
+    out["h2o_input_1mha"] = dict(summary(r), target_error_ha=1e-3,
+                                 errors_ha=[j.error for j in jobs], energies_ha=[j.energy for j in jobs])
+    return out
 
 
 def _batch_compare(jobs, B, timed):
@@ -419,6 +480,60 @@ def run_reference_arm(args, rank: int):
     print(json.dumps(out))
 
 
+def profile_case(name: str) -> None:
+    """Small fixed workloads for kernel captures (one GPU, a few hundred MB
+    on the device): "multidet_small" runs 4N importance-sampled VMC steps of
+    the 12-electron / 12-determinant system with 8,192 walkers (the
+    several-determinant move kernel); "group_small" runs three batches of 40
+    steps of 16 molecules of 4-40 electrons (256-2,048 walkers each) as one
+    group in configuration 0 (the group move kernel); "rows_small" runs 6
+    importance-sampled VMC steps of the 100-electron / 400-function system
+    with 16,384 walkers under QMCB_PREC_INT8_SLICES (the tensor-core
+    contraction k_rows_mma, its prep kernel and the move kernel on rows)."""
+    from qmcbeaver_b200.api import QMCB200Functions, QMCB200Group
+    from qmcbeaver_b200.desc import run_params
+    from qmcbeaver_b200.system import make_system
+    if name == "multidet_small":
+        s = make_system("vmc_multidet_12e", seed=1)
+        W = 8192
+        f = QMCB200Functions(s, W, run_params(sampling=1, qf_modification=2, dt=0.01, seed=3, rel_cutoff=0.0))
+        f.init_walkers(s.initial_positions(W, seed=1))
+        st = f.run_steps(0, 4 * s.n_electrons)
+        print("ok", st.n_moves)
+        f.close()
+    elif name == "group_small":
+        from qmcbeaver_b200.serving import make_jobs
+        jobs = make_jobs(16, rate=1.0, seed=29, electrons=(4, 40), walkers=(256, 2048), orbitals="random")
+        hs = []
+        for j in jobs:
+            f = QMCB200Functions(j.system, j.walkers, run_params(sampling=1, qf_modification=2, dt=0.01,
+                                                                 seed=j.seed, rel_cutoff=0.0))
+            f.init_walkers(j.system.initial_positions(j.walkers, seed=j.seed))
+            hs.append(f)
+        g = QMCB200Group(hs)
+        g.set_config(0)
+        for b in range(3):
+            st = g.run_steps(b * 40, 40)
+        print("ok", sum(x.n_moves for x in st), g.config())
+        g.close()
+        for f in hs:
+            f.close()
+    elif name == "rows_small":
+        from qmcbeaver_b200.desc import QMCB_PREC_INT8_SLICES
+        s = make_system("mixed_20nuc_100e", seed=1)
+        W = 16384  # 4.8 GB of walker state, 240 MB of A digits: larger than L2
+        f = QMCB200Functions(s, W, run_params(sampling=1, qf_modification=2, dt=0.01, seed=3, rel_cutoff=0.0,
+                                              precision=QMCB_PREC_INT8_SLICES))
+        f.init_walkers(s.initial_positions(W, seed=1))
+        st = f.run_steps(0, 6)
+        print("ok", st.n_moves)
+        f.close()
+    else:
+        raise SystemExit(f"unknown case {name}")
+
+
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -428,14 +543,24 @@ def main():
     ap.add_argument("--walkers", type=int, default=DEFAULT_WALKERS)
     ap.add_argument("--e2e-steps", type=int, default=2, help="bench steps timed end to end, one API call per move")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and serving sections")
-    ap.add_argument("--serve-jobs", type=int, default=24)
+    ap.add_argument("--no-extras", action="store_true", help="skip the precision, rows, serving and batching sections")
+    ap.add_argument("--c3-walkers", type=int, default=65536, help="walkers of the 100-electron precision workload")
+    ap.add_argument("--section", choices=["precision", "rows", "serving", "batching"],
+                    help="run one extra section alone and print it")
+    ap.add_argument("--serve-jobs", type=int, default=12)
     ap.add_argument("--serve-rate", type=float, default=20.0)
-    ap.add_argument("--case", choices=["multidet_small", "group_small"],
+    ap.add_argument("--case", choices=["multidet_small", "group_small", "rows_small"],
                     help="run one small profiling workload instead of the benchmark")
     args = ap.parse_args()
     if args.case:
         profile_case(args.case)
+        return
+    if args.section:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        fn = {"precision": precision_section, "rows": rows_section, "serving": lambda a, r: serving_section(a),
+              "batching": lambda a, r: batching_section(a)}[args.section]
+        print(json.dumps({args.section: fn(args, 0)}))
         return
     if args.warmup < 3:
         args.warmup = 3
@@ -560,24 +685,50 @@ def main():
            "api": "qmcb_set_params + qmcb_run_steps_async(step, 1) per single-electron move, statistics collected "
                   "one move behind with qmcb_steps_collect (host E_T in, move statistics out); bytes per bench step"}
 
-    # reference-facing evaluate (QMCFunctions::evaluate shape) with host buffers
+    # reference-facing evaluate (QMCFunctions::evaluate shape) with host
+    # buffers: qmcb_evaluate_moved sends the moved electron's position up and
+    # brings back what a Metropolis driver reads after the call (psi, the
+    # modified drift of every electron for the Green's functions, E_L, the
+    # kinetic and potential terms, the singular flag), into page-locked host
+    # arrays; next to it the all-positions qmcb_evaluate with every output
+    from qmcbeaver_b200.api import OUT_E_LOCAL, OUT_LAP, OUT_MOD_GRAD, OUT_PE, OUT_PSI, OUT_STATUS
     slots = np.arange(min(W, 4096), dtype=np.int32)
-    Rh = np.ascontiguousarray(R_eq[: len(slots)])
-    f2 = QMCB200Functions(system, len(slots), dmc_params(seed=1, e0=e0))
+    nW = len(slots)
+    Rh = np.ascontiguousarray(R_eq[:nW])
+    f2 = QMCB200Functions(system, nW, dmc_params(seed=1, e0=e0))
     f2.evaluate(slots, Rh, -1)
+    pin = {k: torch.zeros(shape, dtype=dt).pin_memory().numpy() for k, shape, dt in
+           (("log_abs_psi", (nW,), torch.float64), ("sign", (nW,), torch.float64),
+            ("grad", (nW, N, 3), torch.float64), ("mod_grad", (nW, N, 3), torch.float64),
+            ("lap", (nW,), torch.float64), ("e_local", (nW,), torch.float64), ("pe", (nW, 3), torch.float64),
+            ("status", (nW,), torch.uint8))}
+    r_up = torch.zeros((nW, 3), dtype=torch.float64).pin_memory().numpy()
+    mask = OUT_PSI | OUT_MOD_GRAD | OUT_LAP | OUT_E_LOCAL | OUT_PE | OUT_STATUS
     rng = np.random.default_rng(5)
-    t0 = time.perf_counter()
     n_eval = 2 * N
+    disp = 0.1 * rng.standard_normal((n_eval, nW, 3))
+    t0 = time.perf_counter()
     for s in range(n_eval):
         e = s % N
-        Rh[:, e] += 0.1 * rng.standard_normal((len(slots), 3))
-        f2.evaluate(slots, Rh, e)
+        r_up[:] = Rh[:, e] + disp[s]
+        f2.evaluate_moved(slots, r_up, e, mask, out=pin)
     ev_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for s in range(n_eval):
+        e = s % N
+        Rh[:, e] += disp[s]
+        f2.evaluate(slots, Rh, e)
+    full_s = time.perf_counter() - t0
     f2.close()
-    e2e_eval = {"value": len(slots) * n_eval / ev_s, "unit": "walker-moves/s", "walkers": len(slots),
-                "h2d_bytes_per_step": len(slots) * (3 * N * 8 + 4),
-                "d2h_bytes_per_step": len(slots) * (6 * N * 8 + 7 * 8 + 1),
-                "api": "qmcb_evaluate(which_e, host R[num][N][3]) per step, no Markov chain"}
+    e2e_eval = {"value": nW * n_eval / ev_s, "unit": "walker-moves/s", "walkers": nW,
+                "h2d_bytes_per_step": nW * (3 * 8 + 4),
+                "d2h_bytes_per_step": nW * (3 * N * 8 + 7 * 8 + 1),
+                "api": "qmcb_evaluate_moved(which_e, moved electron's position, outputs psi | mod_grad | lap | "
+                       "e_local | pe | status) per single-electron move into page-locked host arrays",
+                "all_positions_all_outputs": {
+                    "value": nW * n_eval / full_s, "unit": "walker-moves/s",
+                    "h2d_bytes_per_step": nW * (3 * N * 8 + 4), "d2h_bytes_per_step": nW * (6 * N * 8 + 7 * 8 + 1),
+                    "api": "qmcb_evaluate(which_e, host R[num][N][3]) with every output, pageable numpy arrays"}}
 
     out = {"metric": "walker-moves/s", "value": value, "unit": "walker-moves/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -594,7 +745,7 @@ def main():
         out["clocks"] = clocks
     f.close()
     if not args.no_extras:
-        out["mixed"] = mixed_section(system, W, e0, rank, args)
+        out["precision"] = precision_section(args, rank)
         out["rows"] = rows_section(args, rank)
         if world == 1:
             out["serving"] = serving_section(args)

@@ -71,6 +71,16 @@ extern "C" {
 /* arithmetic of the orbital contraction and Slater updates */
 #define QMCB_PREC_FP64 0  /* plain FP64 everywhere (parity path) */
 #define QMCB_PREC_MIXED 1 /* FP32 orbital rows / SM update, FP64 refresh and accumulators */
+/* FP64 walker state and updates; each single-electron move's orbital rows
+ * (QMCSlater::update_Ds -> Array2D::gemm, QMcBeaver/src/QMCSlater.cpp:856-862)
+ * come from one batched tensor-core contraction over all walkers of the step:
+ * basis values and MO coefficients cut into 7 int8 digit planes, int8 x int8
+ * products accumulated exactly in int32 (tcgen05 kind::i8), recombined in
+ * FP64.  The rows agree with FP64 dot products to FP64 rounding level (48 bits
+ * of every product kept), so results match QMCB_PREC_FP64 within the FP64
+ * parity bounds.  One determinant per system; the full evaluation and the LU
+ * refresh run in FP64. */
+#define QMCB_PREC_INT8_SLICES 2
 
 /*
  * Molecular system: what QMCInput reads from the .ckmf &geometry, &basis,
@@ -183,6 +193,17 @@ typedef struct qmcb_run_params {
    * (QMCManager::updateEffectiveTimeStep, QMcBeaver/src/QMCManager.cpp:2312-2331,
    * updated here with the trial energy); 0: dt_effective as given. */
   int dynamic_time_step;
+  /* 1: after each DMC reweight a walker is deleted (weight 0, removed at the
+   * next branching) by the reference's rules (QMCWalker::reweight_walker,
+   * QMcBeaver/src/QMCWalker.cpp:1196-1365), with iteration = step -
+   * equilibration_steps: while iteration < -100 (equilibrating) when its
+   * weight exceeds twice the branching threshold or falls below 0.1, dW is
+   * outside [0.5, 1.5] or NaN, |E_L - E_orig| / |E_orig| > rel_cutoff (after
+   * step 5) or its age reaches 30; afterwards when dW^(age+1) > 15 or dW is
+   * NaN, its weight exceeds 50, or |E_L - E_orig| / |E_orig| > rel_cutoff.
+   * E_L is the accepted configuration's.  0: no deletion. */
+  int walker_deletion;
+  int equilibration_steps;   /* equilibration_steps: steps before iteration 0 */
 } qmcb_run_params;
 
 /* Energy cutoffs in the reweighting exponent.  The reference defines them
@@ -254,6 +275,40 @@ int qmcb_max_walkers(const qmcb_handle *h);
 int qmcb_evaluate(qmcb_handle *h, int which_e, const int *slots, int num, const double *R,
                   double *log_abs_psi, double *sign, double *grad, double *mod_grad, double *lap,
                   double *e_local, double *pe, unsigned char *status);
+
+/*
+ * Single-electron form of qmcb_evaluate for drivers that keep the positions
+ * on the host (QMCWalker moves one electron, QMcBeaver/src/QMCWalker.cpp:
+ * 313-398, then QMCRun::propagateWalkers calls QMCFunctions::evaluate,
+ * QMcBeaver/src/QMCRun.cpp:43-55): the other electrons' positions are already
+ * in the walker state, so only r_moved[num][3], the new position of
+ * electron which_e, crosses the bus, and only the outputs selected in
+ * out_mask (QMCB_OUT_*) come back (their pointers must be non-NULL; the
+ * others may be NULL).  Same numbers as qmcb_evaluate.  Host buffers may be
+ * pageable; page-locked ones (cudaMallocHost / cudaHostRegister) copy at the
+ * bus's full rate.  Returns after the copies are done.
+ */
+#define QMCB_OUT_PSI 1        /* log_abs_psi[num], sign[num] */
+#define QMCB_OUT_GRAD 2       /* grad[num][N][3] */
+#define QMCB_OUT_MOD_GRAD 4   /* mod_grad[num][N][3] */
+#define QMCB_OUT_LAP 8        /* lap[num] */
+#define QMCB_OUT_E_LOCAL 16   /* e_local[num] */
+#define QMCB_OUT_PE 32        /* pe[num][3] */
+#define QMCB_OUT_STATUS 64    /* status[num] */
+#define QMCB_OUT_ALL 127
+int qmcb_evaluate_moved(qmcb_handle *h, int which_e, const int *slots, int num, const double *r_moved,
+                        unsigned out_mask, double *log_abs_psi, double *sign, double *grad, double *mod_grad,
+                        double *lap, double *e_local, double *pe, unsigned char *status);
+
+/* Walker slots for drivers that own their walkers one by one through the
+ * evaluate entry points (the reference keeps a std::list<QMCWalker>, adds
+ * copies and erases walkers in QMCRun::nonunitWeightBranching,
+ * QMcBeaver/src/QMCRun.cpp:740-814): qmcb_alloc_slot hands out a free slot,
+ * qmcb_free_slot returns one (QMCB_E_ARG if it was not handed out).  The
+ * walker list of qmcb_init_walkers / qmcb_run_steps is separate and is not
+ * touched.  Thread safe. */
+int qmcb_alloc_slot(qmcb_handle *h, int *slot);
+int qmcb_free_slot(qmcb_handle *h, int slot);
 
 /* Same as qmcb_evaluate with every pointer in device memory and no
  * host synchronisation; stream NULL = the handle's stream. */
@@ -375,7 +430,9 @@ int qmcb_branch(qmcb_handle *h, int step, int *n_live);
 #define QMCB_KERNEL_COPY 2
 #define QMCB_KERNEL_ENERGY 3
 #define QMCB_KERNEL_REFRESH 4
-#define QMCB_KERNEL_COUNT 5
+#define QMCB_KERNEL_ROWS_PREP 5 /* QMCB_PREC_INT8_SLICES: proposal, basis values and their digits */
+#define QMCB_KERNEL_ROWS_MMA 6  /* QMCB_PREC_INT8_SLICES: the tensor-core contraction */
+#define QMCB_KERNEL_COUNT 7
 int qmcb_set_profiling(qmcb_handle *h, int enable);
 int qmcb_get_kernel_stats(qmcb_handle *h, double *out, int reset);
 

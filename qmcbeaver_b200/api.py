@@ -31,10 +31,14 @@ EXPORTS = [
     "qmcb_branch_weights_noalloc", "qmcb_run_steps_async", "qmcb_steps_done", "qmcb_steps_collect",
     "qmcb_state_bytes", "qmcb_fit_cusps", "qmcb_run_step_configs",
     "qmcb_group_create", "qmcb_group_destroy", "qmcb_group_last_error", "qmcb_group_run_steps", "qmcb_group_config",
-    "qmcb_group_set_config",
+    "qmcb_group_set_config", "qmcb_evaluate_moved", "qmcb_alloc_slot", "qmcb_free_slot",
 ]
 
-KERNELS = ["move", "branch", "copy", "energy", "refresh"]
+# qmcb_evaluate_moved output selection (QMCB_OUT_*)
+OUT_PSI, OUT_GRAD, OUT_MOD_GRAD, OUT_LAP, OUT_E_LOCAL, OUT_PE, OUT_STATUS = 1, 2, 4, 8, 16, 32, 64
+OUT_ALL = 127
+
+KERNELS = ["move", "branch", "copy", "energy", "refresh", "rows_prep", "rows_mma"]
 
 _lib: Optional[C.CDLL] = None
 
@@ -64,6 +68,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.qmcb_max_walkers.argtypes = [vp]
     L.qmcb_evaluate.argtypes = [vp, C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.qmcb_evaluate_device.argtypes = [vp, C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.qmcb_evaluate_moved.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_uint, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.qmcb_alloc_slot.argtypes = [vp, C.POINTER(C.c_int)]
+    L.qmcb_free_slot.argtypes = [vp, C.c_int]
     L.qmcb_init_walkers.argtypes = [vp, C.c_int, vp]
     L.qmcb_run_steps.argtypes = [vp, C.c_int, C.c_int, vp]
     L.qmcb_num_walkers.argtypes = [vp]
@@ -158,6 +165,34 @@ class QMCB200Functions:
         out["ee"] = out["pe"][:, 2]
         out["kinetic"] = -0.5 * out["lap"]
         return out
+
+    def evaluate_moved(self, slots: Sequence[int], r_moved: np.ndarray, which_e: int, out_mask: int = OUT_ALL,
+                       out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        """qmcb_evaluate_moved: electron which_e of every walker in `slots`
+        moved to r_moved[num][3] (the other positions are the stored ones);
+        returns the outputs selected in out_mask.  `out` may hold
+        preallocated (for example page-locked) arrays to fill."""
+        slots_a = np.ascontiguousarray(slots, dtype=np.int32)
+        num = len(slots_a)
+        r = np.ascontiguousarray(r_moved, dtype=np.float64).reshape(num, 3)
+        if out is None:
+            out = dict(log_abs_psi=np.zeros(num), sign=np.zeros(num), grad=np.zeros((num, self.N, 3)),
+                       mod_grad=np.zeros((num, self.N, 3)), lap=np.zeros(num), e_local=np.zeros(num),
+                       pe=np.zeros((num, 3)), status=np.zeros(num, np.uint8))
+        rc = self.lib.qmcb_evaluate_moved(self.h, int(which_e), _ptr(slots_a), num, _ptr(r), int(out_mask),
+                                          _ptr(out["log_abs_psi"]), _ptr(out["sign"]), _ptr(out["grad"]),
+                                          _ptr(out["mod_grad"]), _ptr(out["lap"]), _ptr(out["e_local"]),
+                                          _ptr(out["pe"]), _ptr(out["status"]))
+        self._check(rc, "qmcb_evaluate_moved")
+        return out
+
+    def alloc_slot(self) -> int:
+        s = C.c_int()
+        self._check(self.lib.qmcb_alloc_slot(self.h, C.byref(s)), "qmcb_alloc_slot")
+        return s.value
+
+    def free_slot(self, slot: int) -> None:
+        self._check(self.lib.qmcb_free_slot(self.h, int(slot)), "qmcb_free_slot")
 
     # ------------------------------------------------------------ Markov chain
     def init_walkers(self, R: np.ndarray) -> None:

@@ -11,7 +11,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libqmcb200.so")
 SOURCES = ["qmcb200.cu", "cusp_fit.c"]
-HEADERS = ["device_common.cuh", "kernels.cuh", "kernels_md.cuh", "kernels_group.cuh", "cusp_fit.h"]
+HEADERS = ["device_common.cuh", "kernels.cuh", "kernels_md.cuh", "kernels_group.cuh", "kernels_rows.cuh", "cusp_fit.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 

@@ -348,6 +348,10 @@ class CkmfInput:
             rel_cutoff=f("rel_cutoff", 100.0, float),
             limit_branching=f("limit_branching", 1, int),
             target_walkers=f("number_of_walkers", 100, int),
+            # QMCWalker::reweight_walker deletes walkers by fixed rules after
+            # every reweight; iteration 0 follows the equilibration steps
+            walker_deletion=1,
+            equilibration_steps=f("equilibration_steps", 2000, int),
         )
         kw.update(overrides)
         return D.run_params(**kw)

@@ -123,6 +123,8 @@ struct RunCfg {
   int run_type, sampling, qf_mod, emod, reweighting, old_walker_acceptance, limit_branching, ecut;
   int exact_gf;  // single-electron moves: Green's functions of the moved electron only
   int dyn_dt;    // reweight with the running effective time step (EnergyCtl::dt_eff)
+  int deletion;  // the reference's walker deletion rules after a reweight
+  int equil_steps;  // step of iteration 0 (deletion rules: equilibrating while step - equil_steps < -100)
   double qf_a, dt, dt_eff;
   double branching_threshold, fusion_threshold;
   double e_orig, rel_cutoff;

@@ -459,6 +459,12 @@ struct MoveArgs {
   int do_reweight;   // this step reweights / collects observables (whichE == 0)
   int reweight_on;   // step >= reweight_start_step
   double *dump;      // configuration records of this step (null: none), see dump_configs
+  // orbital rows of the moved electron at the proposed position, [list
+  // index][5][n] (null: the move kernel evaluates the basis and contracts)
+  const double *rows = nullptr;
+  // evaluate entry points: R_in holds only the moved electron's position per
+  // walker ([num][3]) instead of all positions ([num][N][3])
+  int rin_moved = 0;
 };
 
 // Configuration records of one Metropolis step (print_configs:
@@ -645,7 +651,8 @@ __device__ __noinline__ double umrigar_log_reverse(const DevSys &S, const RunCfg
 template <bool kMetropolis, bool kUmr>
 __device__ __forceinline__ void propose_move(const DevSys &S, const RunCfg &cfg, int slot, int step, int e, int N,
                                              const double *R, const double ro[3], const double *mgo,
-                                             const double *R_in, int wi, double rn[3], double &g_fwd, double &u_acc)
+                                             const double *R_in, int wi, double rn[3], double &g_fwd, double &u_acc,
+                                             int rin_moved)
 {
   const int lane = lane_id();
   g_fwd = 0.0;
@@ -692,7 +699,9 @@ __device__ __forceinline__ void propose_move(const DevSys &S, const RunCfg &cfg,
       g_fwd += warp_sum(prt);
     }
   } else {
-    for (int d = 0; d < 3; d++) rn[d] = R_in[(size_t)wi * 3 * N + 3 * e + d];
+    // the caller's position of electron e: R_in[wi][N][3], or R_in[wi][3]
+    // when the caller sends the moved electron only
+    for (int d = 0; d < 3; d++) rn[d] = rin_moved ? R_in[(size_t)wi * 3 + d] : R_in[(size_t)wi * 3 * N + 3 * e + d];
   }
 }
 
@@ -867,6 +876,18 @@ __device__ __forceinline__ bool metropolis_reweight(const DevSys &S, const RunCf
       else
         w *= dW;
       if (lane == 0) sc[SC_DW] = dW;
+      if (cfg.deletion) {
+        // QMCWalker::reweight_walker's deletions (QMcBeaver/src/QMCWalker.cpp:1196-1365),
+        // on the accepted configuration's local energy
+        const double rel = fabs(((accept ? EL : sc0[SC_EL]) - cfg.e_orig) / cfg.e_orig);
+        bool del;
+        if (mv.step - cfg.equil_steps < -100)
+          del = w > 2.0 * cfg.branching_threshold || w < 0.1 || dW > 1.5 || dW < 0.5 || isnan(dW) ||
+                (rel > cfg.rel_cutoff && mv.step > 5) || new_age >= 30.0;
+        else
+          del = pow(dW, new_age + 1.0) > 15.0 || isnan(dW) || w > 50.0 || rel > cfg.rel_cutoff;
+        if (del) w = 0.0;
+      }
       // a non-finite weight (NaN energy or exp overflow) removes the walker
       // at the next branching instead of poisoning the ensemble sums
       if (!isfinite(w)) w = 0.0;
@@ -1001,7 +1022,8 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
 
   const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3], g_fwd, u_acc;
-  propose_move<kMetropolis, kExtras>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
+  propose_move<kMetropolis, kExtras>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc,
+                                     mv.rin_moved);
 
   // ---- incremental Jastrow + potential
   double dU, dUxx, dVee, dVen;
@@ -1009,7 +1031,12 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   jastrow_pe_move_warp<kExtras>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen, sm);
 
   // ---- basis at the new position and the new Slater / derivative rows
-  if constexpr (sizeof(TS) == 8) {
+  if (mv.rows) {
+    // computed for the whole step by the batched tensor-core contraction
+    const double *src = mv.rows + (size_t)wi * 5 * n;
+    for (int t = lane; t < 5 * n; t += 32) Dn[t] = (TS)src[t];
+    __syncwarp();
+  } else if constexpr (sizeof(TS) == 8) {
     // the exponential slots follow the five chi rows (into the Dn / valc
     // space, unused until the contraction)
     basis_slots_warp(S, rn, (double *)chi, ldc, sm + 5 * ldc);

@@ -368,7 +368,7 @@ __device__ __forceinline__ void md_move_walker(const DevSys &S, const Layout &L,
 
   const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3], g_fwd, u_acc;
-  propose_move<kMetropolis, true>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc);
+  propose_move<kMetropolis, true>(S, cfg, slot, mv.step, e, N, sR, ro, mgo, R_in, wi, rn, g_fwd, u_acc, mv.rin_moved);
   double dU, dUxx, dVee, dVen;
   jastrow_pe_move_warp<true>(S, sR, Ux, e, sp, ro, rn, dU, dUxx, dVee, dVen, chi);
 

@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 #include "kernels_md.cuh"
 #include "kernels_group.cuh"
+#include "kernels_rows.cuh"
 
 using namespace qmcb;
 
@@ -53,6 +54,16 @@ struct qmcb_handle {
   double2 *d_prim = nullptr;
   double *d_ct[2] = {nullptr, nullptr};
   float *d_ctf[2] = {nullptr, nullptr};
+  // batched orbital rows on the tensor cores (QMCB_PREC_INT8_SLICES), set up
+  // on first use: the transposed MO coefficients [K][n_s] kept for the digit
+  // tables, A digits of the step's basis rows, B digits per spin, row and
+  // orbital scales, the rows [walker][5][n]
+  std::vector<double> ct_host[2];
+  signed char *d_rows_A = nullptr, *d_rows_B[2] = {nullptr, nullptr};
+  double *d_rows_rs = nullptr, *d_rows_cs[2] = {nullptr, nullptr}, *d_rows_out = nullptr;
+  int rows_ksteps = 0, wpb_rows = 1, wpb_prep = 1;
+  size_t smem_rows = 0, smem_prep = 0;
+  Layout lay_rows{};  // move-kernel scratch without the basis rows
   double *d_pade = nullptr;
   int2 *d_pade_len = nullptr;
   double2 *d_pade_ab = nullptr;
@@ -109,6 +120,10 @@ struct qmcb_handle {
   size_t prof_used = 0;
   double prof_ms[QMCB_KERNEL_COUNT] = {0};
   double prof_n[QMCB_KERNEL_COUNT] = {0};
+  // slot allocator of the evaluate entry points (qmcb_alloc_slot / qmcb_free_slot)
+  std::mutex slot_mu;
+  std::vector<char> slot_used;
+  std::vector<int> slot_free;
   std::string err;
 };
 
@@ -188,6 +203,8 @@ static RunCfg make_cfg(const qmcb_run_params &p)
   c.ecut = p.energy_cutoff;
   c.exact_gf = p.exact_single_electron_gf;
   c.dyn_dt = p.dynamic_time_step;
+  c.deletion = p.walker_deletion;
+  c.equil_steps = p.equilibration_steps;
   c.e_orig = p.energy_original != 0.0 ? p.energy_original : (p.energy_estimated != 0.0 ? p.energy_estimated : -1.0);
   c.rel_cutoff = p.rel_cutoff > 0 ? p.rel_cutoff : 1e300;
   return c;
@@ -379,22 +396,59 @@ static void launch_move_g(qmcb_handle *h, const dim3 &g, const dim3 &b, size_t s
                           const int *slots, int num, const int *d_num, const double *R_in, const MoveArgs &mv,
                           const EvalOut &o)
 {
+  // with rows from the tensor cores the scratch has no basis rows
+  const Layout &L = mv.rows ? h->lay_rows : h->lay;
   if (h->ginv)
-    k_move<kMetropolis, TS, TI, kExtras, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+    k_move<kMetropolis, TS, TI, kExtras, true><<<g, b, sm, st>>>(h->sys, L, cfg, h->d_state, slots, num, d_num,
                                                                  R_in, mv, h->d_ectl, h->d_stats, o);
   else
-    k_move<kMetropolis, TS, TI, kExtras, false><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+    k_move<kMetropolis, TS, TI, kExtras, false><<<g, b, sm, st>>>(h->sys, L, cfg, h->d_state, slots, num, d_num,
                                                                   R_in, mv, h->d_ectl, h->d_stats, o);
 }
 
+// One single-electron move of list entries [0, num) (d_num: device count,
+// grids sized for `cap` entries).  Under QMCB_PREC_INT8_SLICES three
+// launches: proposal + basis digits, the tensor-core contraction, the move
+// kernel on the rows; else the move kernel alone.
 template <bool kMetropolis>
-static void launch_move(qmcb_handle *h, int blocks, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
+static void launch_move(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
                         const int *d_num, const double *R_in, MoveArgs mv, EvalOut o)
 {
-  const dim3 g(blocks), b(32 * h->wpb_move);
-  const size_t sm = h->smem_move;
   // the Umrigar93 move is compiled only into the extras instantiation
   const bool extras = h->extras || (kMetropolis && cfg.sampling == QMCB_UMRIGAR93_IMPORTANCE_SAMPLING);
+  if (h->params.precision == QMCB_PREC_INT8_SLICES) {
+    const int sp = mv.e < h->sys.na ? 0 : 1, n = sp ? h->sys.nb : h->sys.na;
+    {
+      ProfScope ps(h, QMCB_KERNEL_ROWS_PREP, st);
+      const int pb = (cap + h->wpb_prep - 1) / h->wpb_prep;
+      if (extras)
+        k_rows_prep<kMetropolis, true><<<pb, 32 * h->wpb_prep, h->smem_prep, st>>>(
+            h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, mv, h->rows_ksteps, h->d_rows_A, h->d_rows_rs);
+      else
+        k_rows_prep<kMetropolis, false><<<pb, 32 * h->wpb_prep, h->smem_prep, st>>>(
+            h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, mv, h->rows_ksteps, h->d_rows_A, h->d_rows_rs);
+      ps.end(st);
+    }
+    {
+      ProfScope ps(h, QMCB_KERNEL_ROWS_MMA, st);
+      const dim3 g((cap + kTileWalkers - 1) / kTileWalkers, (n + kNTile - 1) / kNTile);
+      k_rows_mma<<<g, 128, kRowsSmem, st>>>(h->d_rows_A, h->d_rows_B[sp], h->d_rows_rs, h->d_rows_cs[sp], n,
+                                            h->rows_ksteps, num, d_num, h->d_rows_out, h->d_ctl + 3);
+      ps.end(st);
+    }
+    mv.rows = h->d_rows_out;
+    const dim3 g((cap + h->wpb_rows - 1) / h->wpb_rows), b(32 * h->wpb_rows);
+    ProfScope ps(h, QMCB_KERNEL_MOVE, st);
+    if (extras)
+      launch_move_g<kMetropolis, double, double, true>(h, g, b, h->smem_rows, st, cfg, slots, num, d_num, R_in, mv, o);
+    else
+      launch_move_g<kMetropolis, double, double, false>(h, g, b, h->smem_rows, st, cfg, slots, num, d_num, R_in, mv, o);
+    ps.end(st);
+    return;
+  }
+  const dim3 g((cap + h->wpb_move - 1) / h->wpb_move), b(32 * h->wpb_move);
+  const size_t sm = h->smem_move;
+  ProfScope ps(h, QMCB_KERNEL_MOVE, st);
   if (h->params.precision == QMCB_PREC_MIXED) {
     if (extras)
       launch_move_g<kMetropolis, float, MIXED_TI, true>(h, g, b, sm, st, cfg, slots, num, d_num, R_in, mv, o);
@@ -406,6 +460,7 @@ static void launch_move(qmcb_handle *h, int blocks, cudaStream_t st, const RunCf
     else
       launch_move_g<kMetropolis, double, double, false>(h, g, b, sm, st, cfg, slots, num, d_num, R_in, mv, o);
   }
+  ps.end(st);
 }
 
 // The dynamic shared-memory limit of every move-kernel instantiation.
@@ -418,6 +473,94 @@ static cudaError_t move_smem_limits(int bytes)
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move<kMetropolis, TS, TI, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_move<kMetropolis, TS, TI, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e;
+}
+
+// ---------------------------------------------------------------------------
+// Batched orbital rows on the tensor cores (QMCB_PREC_INT8_SLICES,
+// kernels_rows.cuh).
+
+// Walker state written under QMCB_PREC_FP64 serves QMCB_PREC_INT8_SLICES too.
+static int state_kind(int prec) { return prec == QMCB_PREC_MIXED ? QMCB_PREC_MIXED : QMCB_PREC_FP64; }
+
+template <bool kMetropolis>
+static cudaError_t rows_prep_limits(int bytes)
+{
+  cudaError_t e = cudaFuncSetAttribute(k_rows_prep<kMetropolis, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_rows_prep<kMetropolis, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
+}
+
+// Digit tables of the MO coefficients, operand buffers, the move kernel's
+// smaller scratch layout; once per handle, on the first use of the mode.
+static int rows_setup(qmcb_handle *h)
+{
+  if (h->d_rows_A) return QMCB_OK;
+  const int K = h->K, N = h->N;
+  if (K > 8192) return fail(h, QMCB_E_LIMIT, "QMCB_PREC_INT8_SLICES: at most 8192 basis functions (int32 digit sums)");
+  const int ks = (K + kKStep - 1) / kKStep;
+  const size_t tiles = (size_t)(h->max_walkers + kTileWalkers - 1) / kTileWalkers;
+#define CKR(call)                                                                                    \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? QMCB_E_NOMEM : QMCB_E_CUDA,                   \
+                  std::string("QMCB_PREC_INT8_SLICES set-up: " #call ": ") + cudaGetErrorString(e_)); \
+  } while (0)
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? h->sys.nb : h->sys.na;
+    const int nt = std::max((n + kNTile - 1) / kNTile, 1);
+    std::vector<signed char> B((size_t)nt * ks * kSlices * kBBlock, 0);
+    std::vector<double> cs((size_t)nt * kNTile, 1.0);
+    const std::vector<double> &ct = h->ct_host[sp];
+    for (int o = 0; o < n; o++) {
+      double amax = 0.0;
+      for (int k = 0; k < K; k++) amax = std::max(amax, std::fabs(ct[(size_t)k * n + o]));
+      const double scale = rows_scale(amax), inv = 1.0 / scale;
+      cs[o] = scale;
+      for (int k = 0; k < K; k++) {
+        signed char dg[kSlices];
+        rows_digits(ct[(size_t)k * n + o] * inv, dg);
+        for (int q = 0; q < kSlices; q++)
+          B[(((size_t)(o / kNTile) * ks + k / kKStep) * kSlices + q) * kBBlock + rows_blk_off(o % kNTile, k % kKStep)] = dg[q];
+      }
+    }
+    CKR(cudaMalloc(&h->d_rows_B[sp], B.size()));
+    CKR(cudaMemcpy(h->d_rows_B[sp], B.data(), B.size(), cudaMemcpyHostToDevice));
+    CKR(cudaMalloc(&h->d_rows_cs[sp], sizeof(double) * cs.size()));
+    CKR(cudaMemcpy(h->d_rows_cs[sp], cs.data(), sizeof(double) * cs.size(), cudaMemcpyHostToDevice));
+  }
+  const size_t abytes = tiles * ks * kSlices * kABlock;
+  CKR(cudaMalloc(&h->d_rows_A, abytes));
+  CKR(cudaMemset(h->d_rows_A, 0, abytes));  // rows 125 .. 127 of every tile stay zero
+  CKR(cudaMalloc(&h->d_rows_rs, sizeof(double) * tiles * 5 * kTileWalkers));
+  CKR(cudaMalloc(&h->d_rows_out, sizeof(double) * (size_t)h->max_walkers * 5 * h->nmax));
+  // a wait inside the contraction kernel that gave up sets ctl[3], which
+  // returns with every batch's live count
+  CKR(cudaMemset(h->d_ctl + 3, 0, sizeof(int)));
+  h->rows_ksteps = ks;
+  // the move kernel without the basis rows: region A holds only the slice
+  // sums and the new drifts (and the three-body partner gradients)
+  Layout L = h->lay;
+  const int ra = even(std::max(kPart + 6 * N, h->sys.ntb > 0 ? 3 * N * h->sys.M : 0));
+  L.mv_stride += ra - L.mv_region_a;
+  L.mv_region_a = ra;
+  h->lay_rows = L;
+  int max_optin = 0;
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  const size_t per_move = sizeof(double) * (size_t)L.mv_stride;
+  const size_t per_prep = sizeof(double) * (size_t)rows_prep_doubles(N, K, h->sys.nslot);
+  if (per_move > (size_t)max_optin || per_prep > (size_t)max_optin || kRowsSmem > max_optin)
+    return fail(h, QMCB_E_LIMIT, "QMCB_PREC_INT8_SLICES: system too large for the per-walker shared-memory scratch");
+  h->wpb_rows = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_move);
+  h->smem_rows = per_move * h->wpb_rows;
+  h->wpb_prep = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_prep);
+  h->smem_prep = per_prep * h->wpb_prep;
+  CKR(rows_prep_limits<true>(max_optin));
+  CKR(rows_prep_limits<false>(max_optin));
+  CKR(cudaFuncSetAttribute(k_rows_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowsSmem));
+#undef CKR
+  return QMCB_OK;
 }
 
 extern "C" {
@@ -739,6 +882,8 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(upload(&h->d_pcoef, pcoef));
   CKC(upload(&h->d_ct[0], ct[0]));
   CKC(upload(&h->d_ct[1], ct[1]));
+  h->ct_host[0] = ct[0];
+  h->ct_host[1] = ct[1];
   for (int sp = 0; sp < 2; sp++) {
     std::vector<float> cf(ct[sp].begin(), ct[sp].end());
     CKC(upload(&h->d_ctf[sp], cf));
@@ -897,6 +1042,7 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(cudaMalloc(&h->d_live_tmp, sizeof(int) * max_walkers));
   CKC(cudaMalloc(&h->d_free, sizeof(int) * max_walkers));
   CKC(cudaMalloc(&h->d_ctl, sizeof(int) * 4));
+  CKC(cudaMemset(h->d_ctl, 0, sizeof(int) * 4));
   CKC(cudaMalloc(&h->d_copies, sizeof(int2) * max_walkers));
   CKC(cudaMalloc(&h->d_stats, sizeof(double) * ST_COUNT));
   CKC(cudaMemset(h->d_stats, 0, sizeof(double) * ST_COUNT));
@@ -956,7 +1102,9 @@ int qmcb_destroy(qmcb_handle *h)
   void *ptrs[] = {h->d_tbi, h->d_tbL, h->d_tbc, h->d_tbp, h->d_cns, h->d_csexp, h->d_cscoef[0], h->d_cscoef[1], h->d_cpar[0], h->d_cpar[1], h->d_crmax[0],
                   h->d_crmax[1], h->d_docc[0], h->d_docc[1], h->d_dswap[0], h->d_dswap[1], h->d_ci, h->d_ctype, h->d_cparam, h->d_ctf[0], h->d_ctf[1], h->d_pade_ab, h->d_shell, h->d_fn, h->d_xsl, h->d_fq, h->d_pexp, h->d_pcoef, h->d_nuc,   h->d_bf,   h->d_prim,     h->d_ct[0], h->d_ct[1], h->d_pade,   h->d_pade_len,
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
-                  h->d_copies, h->d_stats, h->d_dump, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status};
+                  h->d_copies, h->d_stats, h->d_dump, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status,
+                  h->d_rows_A, h->d_rows_B[0], h->d_rows_B[1], h->d_rows_rs, h->d_rows_cs[0], h->d_rows_cs[1],
+                  h->d_rows_out};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
@@ -981,12 +1129,17 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
   if (p->run_type < 0 || p->run_type > 1 || p->sampling < 0 || p->sampling > 2 || p->qf_modification < 0 ||
       p->qf_modification > 2 || p->energy_modification < 0 || p->energy_modification > 2 || p->reweighting < 0 ||
       p->reweighting > 2 || p->energy_cutoff < 0 || p->energy_cutoff > 2 || p->exact_single_electron_gf < 0 ||
-      p->exact_single_electron_gf > 1 || p->dynamic_time_step < 0 || p->dynamic_time_step > 1)
+      p->exact_single_electron_gf > 1 || p->dynamic_time_step < 0 || p->dynamic_time_step > 1 ||
+      p->walker_deletion < 0 || p->walker_deletion > 1)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");
-  if (p->precision != QMCB_PREC_FP64 && p->precision != QMCB_PREC_MIXED)
+  if (p->precision != QMCB_PREC_FP64 && p->precision != QMCB_PREC_MIXED && p->precision != QMCB_PREC_INT8_SLICES)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown precision");
   if (h->md && p->precision != QMCB_PREC_FP64)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: several determinants run in FP64 only");
+  if (p->precision == QMCB_PREC_INT8_SLICES) {
+    const int rc = rows_setup(h);
+    if (rc) return rc;
+  }
   h->params = *p;
   if (h->n_live_host > 0) {
     // the host's E_T / E_est feed the next steps (QMCManager::updateTrialEnergy)
@@ -1048,7 +1201,7 @@ static void launch_full(qmcb_handle *h, int blocks, cudaStream_t st, const RunCf
 }
 
 static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num, const double *d_R, EvalOut o,
-                       cudaStream_t st)
+                       cudaStream_t st, int rin_moved = 0)
 {
   RunCfg cfg = make_cfg(h->params);
   const bool mixed = h->params.precision == QMCB_PREC_MIXED;
@@ -1060,6 +1213,7 @@ static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num,
                                                                  nullptr, d_R, 1, o);
     } else {
       MoveArgs mv{which_e, 0, 0, 0};
+      mv.rin_moved = rin_moved;
       int blocks = (num + h->wpb_move - 1) / h->wpb_move;
       k_move_md<false><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, d_slots,
                                                                         num, nullptr, d_R, mv, h->d_ectl,
@@ -1073,14 +1227,14 @@ static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num,
     int blocks = (num + h->wpb_full - 1) / h->wpb_full;
     launch_full(h, blocks, st, cfg, d_slots, num, nullptr, d_R, 1, o);
   } else {
-    if (h->state_prec != h->params.precision)
+    if (h->state_prec != state_kind(h->params.precision))
       return fail(h, QMCB_E_STATE, "evaluate: walker state was written in another precision; evaluate all electrons first");
     MoveArgs mv{which_e, 0, 0, 0};
-    int blocks = (num + h->wpb_move - 1) / h->wpb_move;
-    launch_move<false>(h, blocks, st, cfg, d_slots, num, nullptr, d_R, mv, o);
+    mv.rin_moved = rin_moved;
+    launch_move<false>(h, num, st, cfg, d_slots, num, nullptr, d_R, mv, o);
   }
   CK(cudaGetLastError());
-  if (which_e < 0) h->state_prec = h->params.precision;
+  if (which_e < 0) h->state_prec = state_kind(h->params.precision);
   return QMCB_OK;
 }
 
@@ -1132,7 +1286,89 @@ int qmcb_evaluate(qmcb_handle *h, int which_e, const int *slots, int num, const 
   if (mod_grad)
     CK(cudaMemcpyAsync(mod_grad, o_mg, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
   if (status) CK(cudaMemcpyAsync(status, h->d_status, num, cudaMemcpyDeviceToHost, st));
+  int rows_err = 0;
+  if (h->params.precision == QMCB_PREC_INT8_SLICES && which_e >= 0)
+    CK(cudaMemcpyAsync(&rows_err, h->d_ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  if (rows_err) return fail(h, QMCB_E_CUDA, "qmcb_evaluate: the tensor-core contraction gave up waiting (rows not written)");
+  return QMCB_OK;
+}
+
+int qmcb_evaluate_moved(qmcb_handle *h, int which_e, const int *slots, int num, const double *r_moved,
+                        unsigned out_mask, double *log_abs_psi, double *sign, double *grad, double *mod_grad,
+                        double *lap, double *e_local, double *pe, unsigned char *status)
+{
+  if (!h) return QMCB_E_ARG;
+  if (num < 0 || num > h->max_walkers || which_e < 0 || which_e >= h->N || !r_moved || !slots)
+    return fail(h, QMCB_E_ARG, "qmcb_evaluate_moved: bad argument");
+  for (int i = 0; i < num; i++)
+    if (slots[i] < 0 || slots[i] >= h->max_walkers) return fail(h, QMCB_E_ARG, "qmcb_evaluate_moved: slot out of range");
+  if (!h->evaluated_once)
+    return fail(h, QMCB_E_STATE, "qmcb_evaluate_moved: one-electron update before any full evaluation");
+  if (((out_mask & QMCB_OUT_PSI) && (!log_abs_psi || !sign)) || ((out_mask & QMCB_OUT_GRAD) && !grad) ||
+      ((out_mask & QMCB_OUT_MOD_GRAD) && !mod_grad) || ((out_mask & QMCB_OUT_LAP) && !lap) ||
+      ((out_mask & QMCB_OUT_E_LOCAL) && !e_local) || ((out_mask & QMCB_OUT_PE) && !pe) ||
+      ((out_mask & QMCB_OUT_STATUS) && !status))
+    return fail(h, QMCB_E_ARG, "qmcb_evaluate_moved: an output selected in out_mask is NULL");
+  if (num == 0) return QMCB_OK;
+  const int N = h->N;
+  cudaStream_t st = h->stream;
+  CK(cudaMemcpyAsync(h->d_slots, slots, sizeof(int) * num, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->d_R, r_moved, sizeof(double) * 3 * (size_t)num, cudaMemcpyHostToDevice, st));
+  double *base = h->d_out;
+  double *o_lp = base, *o_sg = o_lp + num, *o_lap = o_sg + num, *o_el = o_lap + num, *o_pe = o_el + num;
+  double *o_g = o_pe + 3 * (size_t)num, *o_mg = o_g + 3 * (size_t)N * num;
+  // outputs not asked for are not written by the kernel either
+  EvalOut o{(out_mask & QMCB_OUT_PSI) ? o_lp : nullptr, (out_mask & QMCB_OUT_PSI) ? o_sg : nullptr,
+            (out_mask & QMCB_OUT_GRAD) ? o_g : nullptr, (out_mask & QMCB_OUT_MOD_GRAD) ? o_mg : nullptr,
+            (out_mask & QMCB_OUT_LAP) ? o_lap : nullptr, (out_mask & QMCB_OUT_E_LOCAL) ? o_el : nullptr,
+            (out_mask & QMCB_OUT_PE) ? o_pe : nullptr, (out_mask & QMCB_OUT_STATUS) ? h->d_status : nullptr};
+  int rc = launch_eval(h, which_e, h->d_slots, num, h->d_R, o, st, 1);
+  if (rc) return rc;
+  if (out_mask & QMCB_OUT_PSI) {
+    CK(cudaMemcpyAsync(log_abs_psi, o_lp, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(sign, o_sg, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
+  }
+  if (out_mask & QMCB_OUT_LAP) CK(cudaMemcpyAsync(lap, o_lap, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
+  if (out_mask & QMCB_OUT_E_LOCAL) CK(cudaMemcpyAsync(e_local, o_el, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
+  if (out_mask & QMCB_OUT_PE) CK(cudaMemcpyAsync(pe, o_pe, sizeof(double) * 3 * num, cudaMemcpyDeviceToHost, st));
+  if (out_mask & QMCB_OUT_GRAD)
+    CK(cudaMemcpyAsync(grad, o_g, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
+  if (out_mask & QMCB_OUT_MOD_GRAD)
+    CK(cudaMemcpyAsync(mod_grad, o_mg, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
+  if (out_mask & QMCB_OUT_STATUS) CK(cudaMemcpyAsync(status, h->d_status, num, cudaMemcpyDeviceToHost, st));
+  int rows_err = 0;
+  if (h->params.precision == QMCB_PREC_INT8_SLICES)
+    CK(cudaMemcpyAsync(&rows_err, h->d_ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (rows_err) return fail(h, QMCB_E_CUDA, "qmcb_evaluate_moved: the tensor-core contraction gave up waiting");
+  return QMCB_OK;
+}
+
+int qmcb_alloc_slot(qmcb_handle *h, int *slot)
+{
+  if (!h || !slot) return QMCB_E_ARG;
+  std::lock_guard<std::mutex> lock(h->slot_mu);
+  if (h->slot_used.empty()) {
+    h->slot_used.assign(h->max_walkers, 0);
+    h->slot_free.clear();
+    for (int s = h->max_walkers - 1; s >= 0; s--) h->slot_free.push_back(s);
+  }
+  if (h->slot_free.empty()) return fail(h, QMCB_E_LIMIT, "qmcb_alloc_slot: all max_walkers slots are in use");
+  *slot = h->slot_free.back();
+  h->slot_free.pop_back();
+  h->slot_used[*slot] = 1;
+  return QMCB_OK;
+}
+
+int qmcb_free_slot(qmcb_handle *h, int slot)
+{
+  if (!h) return QMCB_E_ARG;
+  std::lock_guard<std::mutex> lock(h->slot_mu);
+  if (slot < 0 || slot >= h->max_walkers || h->slot_used.empty() || !h->slot_used[slot])
+    return fail(h, QMCB_E_ARG, "qmcb_free_slot: slot was not handed out by qmcb_alloc_slot");
+  h->slot_used[slot] = 0;
+  h->slot_free.push_back(slot);
   return QMCB_OK;
 }
 
@@ -1177,7 +1413,7 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps, double *du
 {
   if (n_steps < 0 || first_step < 0) return fail(h, QMCB_E_ARG, "qmcb_run_steps: bad step range");
   if (!h->evaluated_once) return fail(h, QMCB_E_STATE, "qmcb_run_steps: call qmcb_init_walkers first");
-  if (h->state_prec != h->params.precision)
+  if (h->state_prec != state_kind(h->params.precision))
     return fail(h, QMCB_E_STATE, "qmcb_run_steps: walker state was written in another precision; call qmcb_init_walkers");
   if (h->n_flight >= 2) return fail(h, QMCB_E_STATE, "qmcb_run_steps_async: two batches of steps are already in flight on this handle");
   if (h->n_live_host <= 0) return fail(h, QMCB_E_STATE, "qmcb_run_steps: no live walkers (population died out)");
@@ -1197,15 +1433,13 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps, double *du
     mv.reweight_on = step >= h->params.reweight_start_step;
     mv.dump = dump;
     EvalOut o{};
-    {
+    if (h->md) {
       ProfScope ps(h, QMCB_KERNEL_MOVE, st);
-      if (h->md)
-        k_move_md<true><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state,
-                                                                         h->d_live, 0, h->d_ctl, nullptr, mv,
-                                                                         h->d_ectl, h->d_stats, o);
-      else
-        launch_move<true>(h, blocks, st, cfg, h->d_live, 0, h->d_ctl, nullptr, mv, o);
+      k_move_md<true><<<blocks, 32 * h->wpb_move, h->smem_move, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live, 0,
+                                                                       h->d_ctl, nullptr, mv, h->d_ectl, h->d_stats, o);
       ps.end(st);
+    } else {
+      launch_move<true>(h, h->max_walkers, st, cfg, h->d_live, 0, h->d_ctl, nullptr, mv, o);
     }
     if (dmc && mv.e == 0) {
       {
@@ -1258,6 +1492,7 @@ static int finish_steps(qmcb_handle *h, qmcb_step_stats *stats)
   const double *sv = h->h_stats + slot * ST_COUNT;
   const int *cv = h->h_ctl + slot * 4;
   h->n_live_host = cv[0];
+  if (cv[3]) return fail(h, QMCB_E_CUDA, "qmcb_run_steps: the tensor-core contraction gave up waiting (rows not written)");
   if (stats) {
     stats->sum_weight = sv[ST_SUM_W];
     stats->sum_weight_energy = sv[ST_SUM_WE];

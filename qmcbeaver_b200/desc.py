@@ -17,7 +17,7 @@ QMCB_NO_IMPORTANCE_SAMPLING, QMCB_IMPORTANCE_SAMPLING, QMCB_UMRIGAR93_IMPORTANCE
 QMCB_QF_NONE, QMCB_QF_UMRIGAR93_EQUAL, QMCB_QF_UMRIGAR93_UNEQUAL = 0, 1, 2
 QMCB_EMOD_NONE, QMCB_EMOD_UMRIGAR93, QMCB_EMOD_MODIFIED_UMRIGAR93 = 0, 1, 2
 QMCB_RW_SIMPLE_SYMMETRIC, QMCB_RW_SIMPLE_ASYMMETRIC, QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED = 0, 1, 2
-QMCB_PREC_FP64, QMCB_PREC_MIXED = 0, 1
+QMCB_PREC_FP64, QMCB_PREC_MIXED, QMCB_PREC_INT8_SLICES = 0, 1, 2
 QMCB_ST_SINGULAR, QMCB_ST_NAN = 1, 2
 QMCB_ECUT_NONE, QMCB_ECUT_UMRIGAR93, QMCB_ECUT_BDJM_PUSH88 = 0, 1, 2
 
@@ -50,7 +50,7 @@ class RunParams(C.Structure):
         ("seed", C.c_uint64), ("population_control", C.c_double), ("target_walkers", C.c_int),
         ("reweight_start_step", C.c_int), ("energy_original", C.c_double), ("rel_cutoff", C.c_double),
         ("limit_branching", C.c_int), ("energy_cutoff", C.c_int), ("exact_single_electron_gf", C.c_int),
-        ("dynamic_time_step", C.c_int),
+        ("dynamic_time_step", C.c_int), ("walker_deletion", C.c_int), ("equilibration_steps", C.c_int),
     ]
 
 
@@ -87,6 +87,8 @@ def run_params(**kw) -> RunParams:
     p.rel_cutoff = 100.0
     p.limit_branching = 1
     p.energy_cutoff = QMCB_ECUT_NONE
+    p.walker_deletion = 0
+    p.equilibration_steps = 0
     for k, v in kw.items():
         if not hasattr(p, k):
             raise AttributeError(k)

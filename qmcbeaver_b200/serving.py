@@ -88,25 +88,33 @@ def state_footprint(system: MolecularSystem, walkers: int) -> int:
     return 2 * walkers * words * 8
 
 
+def device_budget(fraction: float = 0.8) -> int:
+    """Bytes of device memory the server may hand to walker state: a
+    fraction of what the current device has free (cudaMemGetInfo)."""
+    import torch
+    free, _ = torch.cuda.mem_get_info()
+    return int(fraction * free)
+
+
 class Server:
     """Admits jobs in arrival order while the sum of their device footprints
-    stays under `hbm_budget` bytes and at most `max_active` run at once."""
+    stays under `hbm_budget` bytes (default: 80% of the device memory free
+    when the server starts) and at most `max_active` run at once."""
 
-    def __init__(self, hbm_budget: int = 40 << 30, max_active: int = 16, mode: str = "streams",
+    def __init__(self, hbm_budget: Optional[int] = None, max_active: int = 16, mode: str = "streams",
                  batch_steps: int = 64):
         if mode not in ("streams", "group"):
             raise ValueError(f"unknown serving mode {mode!r}")
-        self.hbm_budget = int(hbm_budget)
+        self.hbm_budget = int(hbm_budget) if hbm_budget is not None else device_budget()
         self.max_active = int(max_active)
         self.mode = mode
         self.batch_steps = int(batch_steps)
 
     def _handle(self, job: Job) -> QMCB200Functions:
-        # the group path steps FP64 walkers and needs no refresh (a refresh
-        # is a per-member launch outside the captured batch)
+        # both modes refresh every 50 moves (in group mode a batch that holds
+        # a refresh runs as launches instead of a captured graph)
         p = run_params(run_type=QMCB_VMC, sampling=QMCB_IMPORTANCE_SAMPLING,
-                       qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=job.dt,
-                       refresh_interval=50 if self.mode == "streams" else 0,
+                       qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=job.dt, refresh_interval=50,
                        seed=job.seed, precision=job.precision, rel_cutoff=0.0)
         f = QMCB200Functions(job.system, (2 if self.mode == "streams" else 1) * job.walkers, p)
         f.init_walkers(job.system.initial_positions(job.walkers, seed=job.seed))
@@ -275,3 +283,20 @@ def make_jobs(n_jobs: int, rate: float, seed: int = 1, electrons=(4, 40), walker
         jobs.append(Job(job_id=i, system=sysm, walkers=W, target_error=target_error, seed=seed * 7919 + i,
                         arrival=t, max_sweeps=max_sweeps, precision=precision))
     return jobs
+
+
+def make_input_jobs(n_jobs: int, rate: float, system: MolecularSystem, seed: int = 1, walkers=(1024, 4096),
+                    target_error: float = 1e-3, max_sweeps: int = 4000, min_blocks: int = 16) -> List[Job]:
+    """Poisson arrivals at `rate` jobs/s of VMC energy jobs on one given
+    system (for example one of the reference's input files), walkers uniform
+    in `walkers`, each run to `target_error` Hartree."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    jobs = []
+    for i in range(n_jobs):
+        t += rng.exponential(1.0 / rate)
+        W = int(rng.integers(walkers[0], walkers[1] + 1))
+        jobs.append(Job(job_id=i, system=system, walkers=W, target_error=target_error, seed=seed * 7919 + i,
+                        arrival=t, max_sweeps=max_sweeps, min_blocks=min_blocks))
+    return jobs
+

@@ -118,3 +118,43 @@ def place_near_nuclei(R, system, rng, radius=0.03):
         R[w, e] = system.coords[a] + radius * rng.random() * v / np.linalg.norm(v)
         es[w] = e
     return es
+
+
+def oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good=0.2, precision=0, electrons=None):
+    """Full evaluation, then single-electron moves of `electrons` (default:
+    `sweeps` sweeps of all) through the C ABI and the oracle on the same
+    positions, compared call by call at the condition-scaled parity bound."""
+    from oracle.evaluators import OracleEvaluator
+    from qmcbeaver_b200.api import QMCB200Functions
+    orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
+    f = QMCB200Functions(s, W + slots_offset, qf_modification=qf, dt=dt, precision=precision)
+    slots = np.arange(W) + slots_offset
+    ws = orc.new_walkers(W)
+    R = s.initial_positions(W, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    N = s.n_electrons
+    moved = list(electrons) if electrons is not None else [m % N for m in range(sweeps * N)]
+    calls = [(-1, None)] + [(e, None) for e in moved]
+    good = np.ones(W, bool)
+    worst_cond = np.zeros(W)
+    slope, limit = cond_bounds(s)
+    for i, (e, _) in enumerate(calls):
+        if e >= 0:
+            R[:, e] += sigma * rng.standard_normal((W, 3))
+        orc.evaluate(ws, R, e)
+        ref = orc.results(ws)
+        cond = slater_conditions(orc, ws, s)
+        worst_cond = np.maximum(worst_cond, cond)
+        good &= cond < limit
+        out = f.evaluate(slots, R, e)
+        kap = orc.kappa(ws)
+        compare(out, ref, PARITY_RTOL, f"{s.name} call {i} whichE={e}", mask=good, kappa=kap)
+        if (~good).any():
+            # ill-conditioned Slater matrices: rounding differences of two
+            # FP64 implementations grow as ~cond * 1e-15
+            tol = max(PARITY_RTOL, slope * float(worst_cond[~good].max()))
+            compare(out, ref, tol, f"{s.name} call {i} whichE={e} (cond {worst_cond[~good].max():.1e})", mask=~good,
+                    kappa=kap)
+    f.close()
+    assert good.mean() >= min_good, f"only {good.sum()} of {W} walkers stayed well conditioned"
+    return good.mean()

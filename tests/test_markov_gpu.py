@@ -75,7 +75,7 @@ def test_vmc_energy_agrees_with_oracle_chain():
     m1, e1 = block_stats(ref)
     m2, e2 = block_stats(gpu)
     z = abs(m1 - m2) / np.hypot(e1, e2)
-    assert z < 4.0, (m1, e1, m2, e2)
+    assert z < 2.0, (m1, e1, m2, e2)
     assert 0.2 < acc / (sweeps - warm) < 0.99
 
 
@@ -185,3 +185,59 @@ def test_dmc_population_stays_controlled():
     assert 0.7 * W < st.n_walkers < 1.5 * W
     assert np.isfinite(st.sum_weight_energy / st.sum_weight)
     assert st.n_singular < 0.01 * st.n_moves
+
+
+def _deletion_pair(s, W, e0, equil_steps, rel_cutoff, w0, step):
+    """One DMC step that reweights (electron 0 moves) with and without the
+    reference's deletion rules, splitting and fusion switched off so the only
+    deaths are deleted walkers; returns both walker lists (same draws)."""
+    out = []
+    for deletion in (0, 1):
+        p = run_params(run_type=QMCB_DMC, sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL,
+                       dt=0.01, energy_modification=1, energy_cutoff=2, energy_trial=e0, energy_estimated=e0,
+                       energy_original=e0, reweight_start_step=0, branching_threshold=1e300, fusion_threshold=0.0,
+                       limit_branching=0, rel_cutoff=rel_cutoff, seed=5, walker_deletion=deletion,
+                       equilibration_steps=equil_steps)
+        f = QMCB200Functions(s, W, p)
+        f.init_walkers(s.initial_positions(W, seed=4))
+        f.set_walker_weights(w0)
+        st = f.run_steps(step, 1)
+        out.append(f.get_walkers())
+        f.close()
+    return out
+
+
+@pytest.mark.parametrize("phase", ["production", "equilibration"])
+def test_walker_deletion_rules(phase):
+    """QMCWalker::reweight_walker's deletions (QMcBeaver/src/QMCWalker.cpp:
+    1196-1365): the walkers that survive with the rules on are exactly those
+    of the rules-off run that no rule deletes, with identical weights."""
+    s = make_system("dmc_6nuc_30e", seed=1)
+    W, N = 2000, s.n_electrons
+    f = QMCB200Functions(s, W, run_params(qf_modification=2, dt=0.01))
+    f.init_walkers(s.initial_positions(W, seed=4))
+    e0 = float(np.median(f.get_walkers()["e_local"]))
+    f.close()
+    rng = np.random.default_rng(8)
+    w0 = np.exp(rng.normal(0.0, 0.3, W))
+    heavy = rng.random(W) < 0.01
+    light = rng.random(W) < 0.02
+    w0[heavy] = 60.0   # above 50 (production) and 2 x 2.0 (equilibration)
+    w0[light] = 0.05   # below 0.1 (equilibration only)
+    step = 10 * N      # moves electron 0: reweights
+    equil = step + 1000 if phase == "equilibration" else 0
+    off, on = _deletion_pair(s, W, e0, equil, 0.3, w0, step)
+    assert len(off["weight"]) == W  # nothing dies without the rules (all weights >= 0.05)
+    rel = np.abs((off["e_local"] - e0) / e0)
+    dW = off["weight"] / w0
+    if phase == "production":
+        # dW^(age+1) stays far below 15 at dt 0.01 with the energy cutoff
+        keep = (off["weight"] <= 50.0) & (rel <= 0.3)
+        assert dW.max() < 2.0
+    else:
+        # (the heavy-walker rule, weight above twice the branching threshold,
+        # is off here with splitting)
+        keep = (off["weight"] >= 0.1) & (dW <= 1.5) & (dW >= 0.5) & (rel <= 0.3)
+    assert 0 < keep.sum() < W
+    np.testing.assert_array_equal(on["weight"], off["weight"][keep])
+    np.testing.assert_array_equal(on["R"], off["R"][keep])

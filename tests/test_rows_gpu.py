@@ -1,0 +1,108 @@
+"""The orbital rows of single-electron moves from the batched tensor-core
+contraction (QMCB_PREC_INT8_SLICES: basis values and MO coefficients cut into
+7 int8 digit planes, tcgen05 int8 products accumulated exactly in int32,
+recombined in FP64) against the reference and the oracle.
+
+The rows agree with FP64 dot products to FP64 rounding, so the same parity
+bounds as the plain FP64 path apply: 1e-10 relative on the golden cases
+recorded from the reference and on walkers whose Slater matrices stay below
+condition 5e4, 2e-15 x cond above.  The per-walker local-energy tolerance of
+the precision modes, 1e-5 Ha against the FP64 path on identical
+configurations, is gated on the 100-electron workload."""
+import numpy as np
+import pytest
+
+from helpers import GOLDEN_CASES, PARITY_RTOL, load_golden, oracle_sequence, replay
+from qmcbeaver_b200.api import QMCB200Functions
+from qmcbeaver_b200.desc import QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES, QMCB_IMPORTANCE_SAMPLING, run_params
+from qmcbeaver_b200.system import make_random_molecule, make_system
+
+pytestmark = pytest.mark.gpu
+
+# per-walker |E_L(tensor-core rows) - E_L(FP64)| on identical configurations
+EL_TOL_HA = 1e-5
+
+
+@pytest.mark.parametrize("case", [c for c in GOLDEN_CASES if "multidet" not in c])
+def test_rows_reproduce_reference_golden(case):
+    s, d = load_golden(case)
+    if s.n_det > 1:
+        pytest.skip("several determinants run the FP64 kernels")
+    W = d["R"].shape[1]
+    f = QMCB200Functions(s, W, qf_modification=int(d["qf_mod"]), dt=float(d["dt"]), precision=QMCB_PREC_INT8_SLICES)
+    slots = np.arange(W)
+    replay(lambda e, R: f.evaluate(slots, R, e), d, PARITY_RTOL, f"rows/{case}")
+    f.close()
+
+
+@pytest.mark.parametrize("wl,W,qf,dt,sweeps", [("vmc_water_10e", 100, 0, 0.09, 2),
+                                              ("dmc_6nuc_30e", 64, 2, 0.01, 2),
+                                              ("vmc_threebody_16e", 32, 2, 0.01, 1)])
+def test_rows_match_oracle_workloads(wl, W, qf, dt, sweeps):
+    oracle_sequence(make_system(wl, seed=3), W, qf, dt, sweeps, 3 * dt ** 0.5, seed=21, slots_offset=5,
+                    min_good=0.1, precision=QMCB_PREC_INT8_SLICES)
+
+
+@pytest.mark.parametrize("ne,nn,nb,W,seed", [(2, 1, 5, 3, 1), (7, 2, 20, 26, 3), (70, 8, 160, 51, 4)])
+def test_rows_match_oracle_shapes(ne, nn, nb, W, seed):
+    # one-electron spins, n_alpha != n_beta, walker counts that leave the
+    # last 25-walker tile partly empty
+    s = make_random_molecule(ne, nn, nb, 5.0, (1, 6, 7, 8), seed=seed)
+    oracle_sequence(s, W, 2, 0.02, 1, 0.2, seed=seed, min_good=0.0, precision=QMCB_PREC_INT8_SLICES)
+
+
+def test_rows_two_orbital_tiles():
+    # 66 electrons per spin: two 64-orbital tiles of the contraction
+    s = make_random_molecule(132, 14, 300, 7.0, (1, 6, 8), seed=6)
+    moved = [0, 1, 65, 66, 67, 131]
+    oracle_sequence(s, 3, 2, 0.02, 0, 0.2, seed=6, min_good=0.0, precision=QMCB_PREC_INT8_SLICES, electrons=moved)
+
+
+def _chain(s, W, prec, steps, seed=7):
+    p = run_params(sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=2, dt=0.01, seed=seed, rel_cutoff=0.0,
+                   precision=prec)
+    f = QMCB200Functions(s, W, p)
+    f.init_walkers(s.initial_positions(W, seed=seed))
+    st = f.run_steps(0, steps)
+    out = f.get_walkers()
+    f.close()
+    return st, out
+
+
+def test_rows_chain_follows_fp64_chain():
+    # the same proposals and draws: the tensor-core rows change the
+    # acceptance ratios by rounding only, so the chains stay together
+    s = make_system("dmc_6nuc_30e", seed=2)
+    W = 2000
+    a, wa = _chain(s, W, QMCB_PREC_FP64, 2 * s.n_electrons)
+    b, wb = _chain(s, W, QMCB_PREC_INT8_SLICES, 2 * s.n_electrons)
+    same = np.all(np.abs(wa["R"] - wb["R"]) < 1e-9, axis=(1, 2))
+    assert same.mean() > 0.995, same.mean()
+    assert abs(a.sum_accept - b.sum_accept) / a.sum_accept < 1e-3
+    el = np.abs(wa["e_local"] - wb["e_local"])[same]
+    assert np.max(el) < EL_TOL_HA, np.max(el)
+
+
+def test_rows_local_energy_error_100_electrons():
+    # the 100-electron / 400-function workload: per-walker E_L against the
+    # FP64 path on identical configurations over a sweep of moves
+    s = make_system("mixed_20nuc_100e", seed=1)
+    W = 250
+    a = QMCB200Functions(s, W, qf_modification=2, dt=0.01, precision=QMCB_PREC_FP64)
+    b = QMCB200Functions(s, W, qf_modification=2, dt=0.01, precision=QMCB_PREC_INT8_SLICES)
+    R = s.initial_positions(W, seed=4)
+    sl = np.arange(W)
+    a.evaluate(sl, R, -1)
+    b.evaluate(sl, R, -1)
+    rng = np.random.default_rng(9)
+    worst = 0.0
+    for e in range(s.n_electrons):
+        R[:, e] += 0.1 * rng.standard_normal((W, 3))
+        x, y = a.evaluate(sl, R, e), b.evaluate(sl, R, e)
+        ok = (x["status"] == 0) & (y["status"] == 0)
+        assert ok.mean() > 0.9
+        worst = max(worst, float(np.max(np.abs(x["e_local"] - y["e_local"])[ok])))
+        np.testing.assert_array_equal(x["status"], y["status"])
+    a.close()
+    b.close()
+    assert worst <= EL_TOL_HA, worst
