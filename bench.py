@@ -73,6 +73,15 @@ def read_peaks():
     return 6650.0, "fallback"
 
 
+def read_bf16_peak() -> float:
+    """Measured dense bf16 tensor throughput (TFLOP/s, burst), else the
+    pool's earlier measurement."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["bf16_tflops"])
+    return 1590.0
+
+
 def read_traffic(workload: str):
     """Per-walker-move DRAM bytes of the move kernel from the committed ncu
     summary (profiles/traffic.json), or None."""
@@ -247,10 +256,30 @@ def precision_section(args, rank: int):
         ms, moves = aggregate_timing(s_ev.elapsed_time(e_ev), st.n_moves)
         ks = f.kernel_stats(reset=True)
         f.close()
-        out["modes"][PREC_NAMES[prec]] = {
-            "value": moves / (ms / 1e3), "unit": "walker-moves/s", "steps": steps, "ms": ms,
-            "kernels_ms": {k: round(v["ms"], 3) for k, v in ks.items() if v["launches"]},
-            "final_walkers": st.n_walkers}
+        mode = {"value": moves / (ms / 1e3), "unit": "walker-moves/s", "steps": steps, "ms": ms,
+                "kernels_ms": {k: round(v["ms"], 3) for k, v in ks.items() if v["launches"]},
+                "final_walkers": st.n_walkers}
+        mv = ks["move"]
+        wpl = st.n_moves / max(mv["launches"], 1)  # walkers per move launch
+        mode["move_kernel_roofline"] = {
+            "bound": "hbm", "algorithmic_bytes_per_walker_move": bytes_per_move(n, N),
+            "achieved_gbs": bytes_per_move(n, N) * wpl / (mv["ms"] / mv["launches"] / 1e3) / 1e9,
+            "peak_gbs": read_peaks()[0]}
+        mode["move_kernel_roofline"]["frac"] = mode["move_kernel_roofline"]["achieved_gbs"] / read_peaks()[0]
+        if prec == QMCB_PREC_INT8_SLICES:
+            # tensor ops the contraction issues per launch: tiles of 25
+            # walkers x 64-orbital tiles x 32-byte K steps x 36 digit-pair
+            # MMAs (8 digit planes, pairs i + j < 8) of 128 x 64 x 32 int8
+            # multiply-adds
+            mm = ks["rows_mma"]
+            ops = (-(-wpl // 25)) * (-(-n // 64)) * (-(-system.n_basis // 32)) * 36 * 2 * 128 * 64 * 32
+            peak_tops = 2.0 * read_bf16_peak()
+            mode["contraction_roofline"] = {
+                "bound": "tensor", "kernel": "k_rows_mma", "achieved_tops": ops / (mm["ms"] / mm["launches"] / 1e3) / 1e12,
+                "peak_tops": peak_tops, "peak_kind": "int8 dense = 2 x measured bf16 dense burst",
+                "avg_launch_ms": mm["ms"] / mm["launches"]}
+            mode["contraction_roofline"]["frac"] = mode["contraction_roofline"]["achieved_tops"] / peak_tops
+        out["modes"][PREC_NAMES[prec]] = mode
     fp = out["modes"]["fp64"]["value"]
     for k, v in out["modes"].items():
         v["vs_fp64"] = v["value"] / fp
@@ -261,7 +290,7 @@ def precision_section(args, rank: int):
                        ("h2o_input", h2o, None)):
         err[name] = {PREC_NAMES[p]: el_errors(s, p, R=R) for p in (QMCB_PREC_INT8_SLICES, QMCB_PREC_MIXED)}
     out["el_error_vs_fp64_ha"] = err
-    out["note"] = ("int8_slices_tcgen05: basis values and MO coefficients cut into 7 int8 digit planes, "
+    out["note"] = ("int8_slices_tcgen05: basis values and MO coefficients cut into 8 int8 digit planes, "
                    "tcgen05.mma kind::i8 with exact int32 accumulation, FP64 recombination; FP64 inverse, "
                    "Sherman-Morrison update, ratio sums, refresh and energies. mixed_fp32_rows: FP32 basis and "
                    "orbital rows, FP64 inverse and energies.")
@@ -427,16 +456,24 @@ def _batch_compare(jobs, B, timed):
 def batching_section(args):
     """The uneven-batching workload: 64 synthetic molecules, even electron
     counts uniform in 4-200, basis 4N, N/5 nuclei with Z in {1, 6, 7, 8},
-    orthonormalised random orbital coefficients; walkers per molecule
-    uniform in 256-2048 (the workload's 256-8192 capped at 2048 so that all
-    64 walker populations fit in HBM together: this layout keeps every
-    walker's orbital rows, derivative rows and inverses resident).  VMC
-    importance-sampled steps, 100 per batch.  Next to it the same comparison
-    for 64 small molecules (4-40 electrons, the serving jobs' sizes), where
-    each molecule's step is a short kernel."""
-    from qmcbeaver_b200.serving import make_jobs
-    out = _batch_compare(make_jobs(64, rate=1.0, seed=23, electrons=(4, 200), walkers=(256, 2048),
-                                   orbitals="random"), B=100, timed=2)
+    orthonormalised random orbital coefficients, walkers per molecule uniform
+    in 256-8192 (every walker's orbital rows, derivative rows and inverses
+    resident: about 120 GB for the 64 populations; if the device has less
+    free memory the walker range is scaled down until they fit, and the
+    range used is reported).  VMC importance-sampled steps, 50 per batch.
+    Next to it the same comparison for 64 small molecules (4-40 electrons,
+    the serving jobs' sizes), where each molecule's step is a short kernel."""
+    from qmcbeaver_b200.serving import device_budget, make_jobs, state_footprint
+    hi = 8192
+    while True:
+        jobs = make_jobs(64, rate=1.0, seed=23, electrons=(4, 200), walkers=(256, hi), orbitals="random")
+        need = sum(state_footprint(j.system, j.walkers) // 2 for j in jobs)
+        if need <= 0.9 * device_budget(1.0) or hi <= 1024:
+            break
+        hi //= 2
+    out = _batch_compare(jobs, B=50, timed=2)
+    out["walker_range"] = [256, hi]
+    out["state_gb"] = need / 1e9
     out["small_molecules"] = _batch_compare(make_jobs(64, rate=1.0, seed=29, electrons=(4, 40), walkers=(256, 2048),
                                                       orbitals="random"), B=40, timed=5)
     return out

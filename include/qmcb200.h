@@ -74,9 +74,9 @@ extern "C" {
 /* FP64 walker state and updates; each single-electron move's orbital rows
  * (QMCSlater::update_Ds -> Array2D::gemm, QMcBeaver/src/QMCSlater.cpp:856-862)
  * come from one batched tensor-core contraction over all walkers of the step:
- * basis values and MO coefficients cut into 7 int8 digit planes, int8 x int8
+ * basis values and MO coefficients cut into 8 int8 digit planes, int8 x int8
  * products accumulated exactly in int32 (tcgen05 kind::i8), recombined in
- * FP64.  The rows agree with FP64 dot products to FP64 rounding level (48 bits
+ * FP64.  The rows agree with FP64 dot products to FP64 rounding level (56 bits
  * of every product kept), so results match QMCB_PREC_FP64 within the FP64
  * parity bounds.  One determinant per system; the full evaluation and the LU
  * refresh run in FP64. */

@@ -17,9 +17,9 @@
 // of two to |x| < 1 and cut into kSlices signed 7-bit digits,
 //   x = scale * sum_s d_s 2^-(6 + 7 s),  |d_s| <= 64,
 // the digit products sum_k a_i[r][k] b_j[k][o] are exact in int32
-// (|a b| <= 2^12, K <= 2^17 / kSlices), and the pairs with i + j = t share
+// (|a b| <= 2^12, K <= 2^19 / kSlices), and the pairs with i + j = t share
 // one TMEM accumulator (weight 2^-(12 + 7 t)).  The pairs with i + j < kSlices
-// keep 48 bits of every product: the rows agree with an FP64 dot product to
+// keep 56 bits of every product: the rows agree with an FP64 dot product to
 // its own rounding level, so the per-move Slater updates downstream stay in
 // the FP64 parity regime (Slater matrices of random 50 x 50 orbitals reach
 // condition numbers of 1e6, which amplify any FP32-class row error to 1e-1 Ha
@@ -43,7 +43,7 @@
 
 namespace qmcb {
 
-constexpr int kSlices = 7;       // int8 digits per operand value
+constexpr int kSlices = 8;       // int8 digits per operand value
 constexpr int kTileRows = 128;   // MMA M: TMEM lanes
 constexpr int kTileWalkers = 25; // walkers per tile: rows 0 .. 124 used
 constexpr int kNTile = 64;       // MMA N: orbitals per CTA
@@ -53,7 +53,8 @@ constexpr int kBBlock = kNTile * kKStep;     // the same for B
 constexpr int kRowsStages = 3;
 constexpr int kRowsStageBytes = kSlices * (kABlock + kBBlock);
 constexpr int kRowsSmem = kRowsStages * kRowsStageBytes + 1024;  // + barriers; > 113 KB: one CTA per SM
-constexpr uint32_t kRowsTmemCols = 512;  // kSlices accumulators of kNTile int32 columns, rounded to a power of two
+constexpr uint32_t kRowsTmemCols = 512;  // kSlices accumulators of kNTile int32 columns (all of TMEM)
+static_assert(kSlices * kNTile <= (int)kRowsTmemCols, "accumulators exceed the TMEM allocation");
 
 // Byte offset of (row r, k) in one K-step block of the no-swizzle K-major
 // operand layout: 8 x 16-byte core matrices, the two K halves 128 bytes

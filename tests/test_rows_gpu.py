@@ -1,6 +1,6 @@
 """The orbital rows of single-electron moves from the batched tensor-core
 contraction (QMCB_PREC_INT8_SLICES: basis values and MO coefficients cut into
-7 int8 digit planes, tcgen05 int8 products accumulated exactly in int32,
+8 int8 digit planes, tcgen05 int8 products accumulated exactly in int32,
 recombined in FP64) against the reference and the oracle.
 
 The rows agree with FP64 dot products to FP64 rounding, so the same parity
