@@ -145,3 +145,32 @@ def test_group_refuses_unsupported_members():
     g = QMCB200Group([a, c])
     with pytest.raises(QMCBError, match="FP64"):
         g.run_steps(0, 4)
+
+
+def test_group_members_match_the_oracle():
+    """Each member of a group, after a batch of group steps, holds the local
+    energy and log|psi| the oracle computes from scratch at the member's
+    current positions (to the drift of the Sherman-Morrison chain, 1e-8
+    relative, as for a single handle), on walkers whose Slater matrices are
+    well conditioned."""
+    from helpers import cond_bounds, slater_conditions
+    from oracle.evaluators import OracleEvaluator
+    systems = _systems(extra_threebody=True)
+    hs = _handles(systems, _params)
+    g = QMCB200Group(hs)
+    g.run_steps(_first_steps(systems), 40)
+    g.close()
+    for (s, w), f in zip(systems, hs):
+        got = f.get_walkers()
+        n = min(64, len(got["weight"]))
+        orc = OracleEvaluator(s, qf_mod=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01)
+        ws = orc.new_walkers(n)
+        orc.evaluate(ws, got["R"][:n], -1)
+        ref = orc.results(ws)
+        ok = (ref["singular"] == 0) & (slater_conditions(orc, ws, s) < cond_bounds(s)[1])
+        assert ok.sum() >= n // 4, (s.name, ok.sum())
+        kap = np.maximum(np.asarray(orc.kappa(ws), np.float64), 1.0)  # several determinants' mixing
+        for k in ("e_local", "log_abs_psi"):
+            err = np.abs(got[k][:n] - ref[k]) / np.maximum(np.abs(ref[k]), 1.0) / kap
+            assert np.max(err[ok]) < 1e-8, (s.name, k, float(np.max(err[ok])))
+        f.close()

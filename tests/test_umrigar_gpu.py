@@ -107,6 +107,6 @@ def test_vmc_energy_agrees_with_plain_metropolis():
     e1, a1 = chain(QMCB_UMRIGAR93_IMPORTANCE_SAMPLING, 0.09, 11)
     e2, a2 = chain(QMCB_NO_IMPORTANCE_SAMPLING, 0.09, 12)
     (m1, s1), (m2, s2) = stats(e1), stats(e2)
-    assert abs(m1 - m2) < 4.0 * np.hypot(s1, s2), (m1, s1, m2, s2)
+    assert abs(m1 - m2) < 2.0 * np.hypot(s1, s2), (m1, s1, m2, s2)
     # the importance-sampled move is accepted more often than the blind one
     assert a1 > a2 and 0.3 < a1 < 1.0, (a1, a2)
