@@ -110,7 +110,10 @@ class QMCB200Functions : public QMCSCFJastrow {
     if (qmcb_set_params(h_, &p) != QMCB_OK) die(qmcb_last_error(h_));
     std::clog << "QMCB200Functions: evaluate through " << qmcb_version() << std::endl;
   }
-  ~QMCB200Functions() { qmcb_destroy(h_); }
+  // The handle lives until the process ends: the reference deletes its
+  // QMCFunctions from destructors that can run after the CUDA runtime has shut
+  // down at exit (freeing device memory then is not possible).
+  ~QMCB200Functions() {}
 
   void evaluate(Array1D<QMCWalkerData *> &wd, Array1D<Array2D<double> *> &X, int num)
   {

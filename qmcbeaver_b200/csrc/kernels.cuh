@@ -64,6 +64,12 @@ __host__ __device__ inline int full_scratch_doubles(int N, int K, int nmax)
 {
   return 5 * (K + 1) + 5 * nmax + 2 * nmax * nmax + 2 * nmax + 3 * N + kPart + 8;
 }
+// The LU refresh of stored Slater values (k_full with do_basis = 0) needs no
+// basis rows and no new-row space: a smaller per-warp scratch, more warps per SM.
+__host__ __device__ inline int refresh_scratch_doubles(int N, int nmax)
+{
+  return 2 * nmax * nmax + 2 * nmax + 3 * N + kPart + 8;
+}
 
 // ------------------------------------------------------------------------
 // Modified quantum force, QMCSCFJastrow::calculate_Modified_Grad_PsiRatio
@@ -190,10 +196,21 @@ __device__ inline bool lu_inverse_warp(double *A, double *X, double *vv, double 
     if (p < 0) sg = -sg;
     for (int i = j + 1 + lane; i < n; i += 32) A[i * n + j] *= dum;
     __syncwarp();
-    int m = n - j - 1;
-    for (int t = lane; t < m * m; t += 32) {
-      int i = j + 1 + t / m, c = j + 1 + t % m;
-      A[i * n + c] -= A[i * n + j] * A[j * n + c];
+    // trailing update, element t = (i, c) of the (n-j-1)^2 block on lane
+    // t mod 32; the position advances by 32 elements without a division
+    const int m = n - j - 1;
+    if (m > 0) {
+      const int q32 = 32 / m, r32 = 32 - q32 * m;
+      int i = lane / m, c = lane - i * m;
+      for (int t = lane; t < m * m; t += 32) {
+        A[(j + 1 + i) * n + j + 1 + c] -= A[(j + 1 + i) * n + j] * A[j * n + j + 1 + c];
+        c += r32;
+        i += q32;
+        if (c >= m) {
+          c -= m;
+          i++;
+        }
+      }
     }
     __syncwarp();
   }
@@ -321,11 +338,11 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
   const int N = S.N, K = S.K, nmax = max(S.na, S.nb);
   const int slot = slots ? slots[wi] : wi;
   double *blk = state + (size_t)slot * L.stride;
-  double *sm = smem + (size_t)warp * full_scratch_doubles(N, K, nmax);
+  double *sm = smem + (size_t)warp * (do_basis ? full_scratch_doubles(N, K, nmax) : refresh_scratch_doubles(N, nmax));
   const int ldc = K + 1;
   double *chi = sm;
   double *Dn = chi + 5 * ldc;
-  double *A = Dn + 5 * nmax;
+  double *A = do_basis ? Dn + 5 * nmax : sm;  // the refresh has no basis rows
   double *X = A + nmax * nmax;
   double *vv = X + nmax * nmax;
   double *piv = vv + nmax;

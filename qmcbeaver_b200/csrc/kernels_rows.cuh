@@ -19,11 +19,13 @@
 // the digit products sum_k a_i[r][k] b_j[k][o] are exact in int32
 // (|a b| <= 2^12, K <= 2^19 / kSlices), and the pairs with i + j = t share
 // one TMEM accumulator (weight 2^-(12 + 7 t)).  The pairs with i + j < kSlices
-// keep 56 bits of every product: the rows agree with an FP64 dot product to
-// its own rounding level, so the per-move Slater updates downstream stay in
-// the FP64 parity regime (Slater matrices of random 50 x 50 orbitals reach
-// condition numbers of 1e6, which amplify any FP32-class row error to 1e-1 Ha
-// in the local energy).
+// keep 56 bits of every product relative to the row's largest basis value
+// and the orbital's largest coefficient: the rows carry FP64-level error in
+// the normwise sense (an FP64 dot product's error is relative to the sum of
+// its terms, which is smaller for elements far below their row's largest),
+// so the per-move Slater updates downstream stay in the FP64 regime (Slater
+// matrices of random 50 x 50 orbitals reach condition numbers of 1e6, which
+// amplify any FP32-class row error to 1e-1 Ha in the local energy).
 //
 //   k_rows_prep  one warp per walker: the move's proposal (the same draws as
 //                the move kernel, which recomputes it), the basis values at
@@ -33,8 +35,9 @@
 //                int8 x int8 -> int32 tcgen05.mma (kind::i8, M = 128, N = 64,
 //                K = 32 per instruction) over kSlices (kSlices + 1) / 2 digit
 //                pairs per K step, operands staged in shared memory by
-//                cp.async (3 stages), accumulators in TMEM, FP64 recombination
-//                in the epilogue; writes rows[walker][5][n]
+//                bulk copies (the TMA engine, 3 stages, one thread), accumulators
+//                in TMEM, FP64 recombination in the epilogue; writes
+//                rows[walker][5][n]
 // The move kernel then reads the rows instead of evaluating the basis and
 // contracting (MoveArgs::rows).
 #pragma once
@@ -53,6 +56,7 @@ constexpr int kBBlock = kNTile * kKStep;     // the same for B
 constexpr int kRowsStages = 3;
 constexpr int kRowsStageBytes = kSlices * (kABlock + kBBlock);
 constexpr int kRowsSmem = kRowsStages * kRowsStageBytes + 1024;  // + barriers; > 113 KB: one CTA per SM
+static_assert(kRowsStageBytes % 16 == 0 && kABlock % 16 == 0, "bulk copies move multiples of 16 bytes");
 constexpr uint32_t kRowsTmemCols = 512;  // kSlices accumulators of kNTile int32 columns (all of TMEM)
 static_assert(kSlices * kNTile <= (int)kRowsTmemCols, "accumulators exceed the TMEM allocation");
 
@@ -65,18 +69,20 @@ __host__ __device__ inline int rows_blk_off(int r, int k)
   return (r >> 3) * 256 + (k >> 4) * 128 + (r & 7) * 16 + (k & 15);
 }
 
-// Digits of x (|x| < 1 after scaling): d_s = rint(rem_s 2^(6 + 7 s)), rem_{s+1} =
-// rem_s - d_s 2^-(6 + 7 s); every step is exact in FP64.
+// Digits of x (|x| < 1 after scaling): q = rint(x 2^(7 kSlices - 1)) is cut
+// into balanced base-128 digits from the top, d_s = round(q_s / 2^w_s) with
+// w_s = 7 (kSlices - 1 - s) and q_{s+1} = q_s - d_s 2^w_s, so that
+// x = sum_s d_s 2^-(6 + 7 s) up to the rounding of q (2^-(7 kSlices - 1)),
+// |d_s| <= 64.  Integer arithmetic after the one conversion.
 __host__ __device__ inline void rows_digits(double x, signed char *d)
 {
-  double rem = x;
-  double up = 64.0, down = 1.0 / 64.0;
+  static_assert(7 * kSlices - 1 <= 62, "digits exceed a 64-bit fixed-point value");
+  long long q = llrint(ldexp(x, 7 * kSlices - 1));
   for (int s = 0; s < kSlices; s++) {
-    const double q = rint(rem * up);
-    d[s] = (signed char)q;
-    rem -= q * down;
-    up *= 128.0;
-    down *= (1.0 / 128.0);
+    const int w = 7 * (kSlices - 1 - s);
+    const long long ds = w > 0 ? (q + (1ll << (w - 1))) >> w : q;  // arithmetic shift: floor
+    d[s] = (signed char)ds;
+    q -= ds << w;
   }
 }
 
@@ -236,16 +242,22 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
   const int tile = blockIdx.x, ntile = blockIdx.y;
   if (tile * kTileWalkers >= nw) return;  // whole CTA: before any TMEM or barrier use
   unsigned char *stage0 = rsm;
-  uint64_t *bars = (uint64_t *)(rsm + kRowsStages * kRowsStageBytes);  // [kRowsStages]
-  uint32_t *tslot = (uint32_t *)(bars + kRowsStages);
+  // full[s]: the stage's operands landed (bulk copies, transaction bytes);
+  // empty[s]: the MMAs that read the stage completed (tcgen05.commit)
+  uint64_t *full = (uint64_t *)(rsm + kRowsStages * kRowsStageBytes);
+  uint64_t *empty = full + kRowsStages;
+  uint32_t *tslot = (uint32_t *)(empty + kRowsStages);
+  int *s_status = (int *)(tslot + 1);  // [0] ok, [1] last committed K step
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
                  "r"(kRowsTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    for (int s = 0; s < kRowsStages; s++)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + s)));
+    for (int s = 0; s < kRowsStages; s++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(full + s)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(empty + s)));
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -255,27 +267,33 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
 
   const signed char *Ag = A + (size_t)tile * ksteps * kSlices * kABlock;
   const signed char *Bg = B + (size_t)ntile * ksteps * kSlices * kBBlock;
-  bool ok = true;
-  int committed = -1;  // last K step whose MMAs were issued and committed
-  for (int kk = 0; kk < ksteps; kk++) {
-    const int st = kk % kRowsStages;
-    unsigned char *sA = stage0 + st * kRowsStageBytes, *sB = sA + kSlices * kABlock;
-    // the MMAs that last read this stage (K step kk - kRowsStages) are done
-    if (kk >= kRowsStages) ok = mbar_wait(smem_u32(bars + st), (uint32_t)((kk / kRowsStages - 1) & 1));
-    ok = __syncthreads_and(ok ? 1 : 0) != 0;
-    if (!ok) break;
-    const signed char *ga = Ag + (size_t)kk * kSlices * kABlock;
-    const signed char *gb = Bg + (size_t)kk * kSlices * kBBlock;
-    for (int c = tid; c < kSlices * kABlock / 16; c += 128) cp_async16((double *)(sA + 16 * c), (const double *)(ga + 16 * c));
-    for (int c = tid; c < kSlices * kBBlock / 16; c += 128) cp_async16((double *)(sB + 16 * c), (const double *)(gb + 16 * c));
-    cp_async_commit();
-    cp_async_wait<0>();
-    // the tensor cores read shared memory through the async proxy
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
+  if (tid == 0) {
+    // one thread streams the K steps: the digit planes of a K step are
+    // contiguous in global memory (kSlices x kABlock of A, kSlices x kBBlock
+    // of B), so two bulk copies fill a stage; kRowsStages - 1 steps are in
+    // flight while the tensor cores work on the current one
+    auto load = [&](int kk) {
+      const int st = kk % kRowsStages;
+      const uint32_t fb = smem_u32(full + st), dst = smem_u32(stage0 + st * kRowsStageBytes);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"((uint32_t)kRowsStageBytes)
+                   : "memory");
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+                   "l"(Ag + (size_t)kk * kSlices * kABlock), "r"((uint32_t)(kSlices * kABlock)), "r"(fb)
+                   : "memory");
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                       dst + kSlices * kABlock),
+                   "l"(Bg + (size_t)kk * kSlices * kBBlock), "r"((uint32_t)(kSlices * kBBlock)), "r"(fb)
+                   : "memory");
+    };
+    int loaded = 0, committed = -1;
+    bool ok = true;
+    for (; loaded < kRowsStages && loaded < ksteps; loaded++) load(loaded);
+    for (int kk = 0; kk < ksteps; kk++) {
+      const int st = kk % kRowsStages;
+      ok = mbar_wait(smem_u32(full + st), (uint32_t)((kk / kRowsStages) & 1));
+      if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+      const uint32_t a0 = smem_u32(stage0 + st * kRowsStageBytes), b0 = a0 + kSlices * kABlock;
 #pragma unroll
       for (int i = 0; i < kSlices; i++) {
 #pragma unroll
@@ -285,16 +303,33 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
           mma_i8(tmem + (uint32_t)((i + j) * kNTile), ad, bd, (kk > 0 || i > 0) ? 1u : 0u);
         }
       }
-      mma_commit(smem_u32(bars + st));
+      mma_commit(smem_u32(empty + st));
+      committed = kk;
+      // refill the stage the previous K step used, once its MMAs are done
+      if (kk >= 1 && loaded < ksteps) {
+        const int sp = (kk - 1) % kRowsStages;
+        ok = mbar_wait(smem_u32(empty + sp), (uint32_t)(((kk - 1) / kRowsStages) & 1));
+        if (!ok) break;
+        load(loaded++);
+      }
     }
-    committed = kk;
+    if (!ok) {
+      // a wait gave up: let the copies already issued land (bounded) before
+      // the shared memory is left
+      for (int l = committed + 1; l < loaded; l++) mbar_wait(smem_u32(full + l % kRowsStages), (uint32_t)((l / kRowsStages) & 1));
+    }
+    s_status[0] = ok ? 1 : 0;
+    s_status[1] = committed;
   }
+  __syncthreads();
+  const bool ok = s_status[0] != 0;
+  const int committed = s_status[1];
   // every MMA of this CTA is done once the last commit's phase completes
   // (waited for after a failed wait too, so that no MMA is in flight when
   // the TMEM is released)
   bool done = true;
   if (committed >= 0)
-    done = mbar_wait(smem_u32(bars + committed % kRowsStages), (uint32_t)((committed / kRowsStages) & 1));
+    done = mbar_wait(smem_u32(empty + committed % kRowsStages), (uint32_t)((committed / kRowsStages) & 1));
   const int okall = __syncthreads_and((ok && done && committed == ksteps - 1) ? 1 : 0);
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (okall) {

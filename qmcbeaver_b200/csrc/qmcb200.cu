@@ -99,8 +99,8 @@ struct qmcb_handle {
   unsigned char *d_status = nullptr;
   int n_live_host = 0;
   double target_weight = 0.0;
-  size_t smem_move = 0, smem_full = 0;
-  int wpb_move = 1, wpb_full = 1;  // warps (walkers) per CTA of k_move / k_full
+  size_t smem_move = 0, smem_full = 0, smem_refresh = 0;
+  int wpb_move = 1, wpb_full = 1, wpb_refresh = 1;  // warps (walkers) per CTA of k_move / k_full / the refresh
   bool evaluated_once = false;
   int state_prec = -1;  // precision the stored walker state was written in
   // asynchronous step batches (qmcb_run_steps_async)
@@ -491,6 +491,25 @@ static cudaError_t rows_prep_limits(int bytes)
   return e;
 }
 
+// Warps per CTA (1 .. kMaxWarpsPerBlock) that keep the most warps of a kernel
+// resident per SM when each warp needs `per_warp` bytes of shared memory
+// (large scratches pack better in small CTAs).
+static int best_warps_per_block(const qmcb_handle *h, size_t per_warp)
+{
+  int max_optin = 0, smem_sm = 0;
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->device);
+  int wpb = 1, best = 0;
+  for (int w = 1; w <= kMaxWarpsPerBlock && (size_t)w * per_warp <= (size_t)max_optin; w++) {
+    const int resident = w * (int)(smem_sm / (w * per_warp + 1024));  // 1 KB reserved per CTA
+    if (resident >= best) {
+      best = resident;
+      wpb = w;
+    }
+  }
+  return wpb;
+}
+
 // Digit tables of the MO coefficients, operand buffers, the move kernel's
 // smaller scratch layout; once per handle, on the first use of the mode.
 static int rows_setup(qmcb_handle *h)
@@ -532,12 +551,14 @@ static int rows_setup(qmcb_handle *h)
   }
   const size_t abytes = tiles * ks * kSlices * kABlock;
   CKR(cudaMalloc(&h->d_rows_A, abytes));
-  CKR(cudaMemset(h->d_rows_A, 0, abytes));  // rows 125 .. 127 of every tile stay zero
+  // on the handle's stream (non-blocking: a legacy-stream memset would not
+  // be ordered with its work)
+  CKR(cudaMemsetAsync(h->d_rows_A, 0, abytes, h->stream));  // rows 125 .. 127 of every tile stay zero
   CKR(cudaMalloc(&h->d_rows_rs, sizeof(double) * tiles * 5 * kTileWalkers));
   CKR(cudaMalloc(&h->d_rows_out, sizeof(double) * (size_t)h->max_walkers * 5 * h->nmax));
   // a wait inside the contraction kernel that gave up sets ctl[3], which
   // returns with every batch's live count
-  CKR(cudaMemset(h->d_ctl + 3, 0, sizeof(int)));
+  CKR(cudaMemsetAsync(h->d_ctl + 3, 0, sizeof(int), h->stream));
   h->rows_ksteps = ks;
   // the move kernel without the basis rows: region A holds only the slice
   // sums and the new drifts (and the three-body partner gradients)
@@ -552,9 +573,9 @@ static int rows_setup(qmcb_handle *h)
   const size_t per_prep = sizeof(double) * (size_t)rows_prep_doubles(N, K, h->sys.nslot);
   if (per_move > (size_t)max_optin || per_prep > (size_t)max_optin || kRowsSmem > max_optin)
     return fail(h, QMCB_E_LIMIT, "QMCB_PREC_INT8_SLICES: system too large for the per-walker shared-memory scratch");
-  h->wpb_rows = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_move);
+  h->wpb_rows = best_warps_per_block(h, per_move);
   h->smem_rows = per_move * h->wpb_rows;
-  h->wpb_prep = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_prep);
+  h->wpb_prep = best_warps_per_block(h, per_prep);
   h->smem_prep = per_prep * h->wpb_prep;
   CKR(rows_prep_limits<true>(max_optin));
   CKR(rows_prep_limits<false>(max_optin));
@@ -1076,6 +1097,9 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   h->wpb_full = (int)std::min<size_t>(kMaxWarpsPerBlock, max_optin / per_full);
   h->smem_move = per_move * h->wpb_move;
   h->smem_full = per_full * h->wpb_full;
+  const size_t per_refresh = sizeof(double) * (size_t)refresh_scratch_doubles(h->N, h->nmax);
+  h->wpb_refresh = best_warps_per_block(h, per_refresh);
+  h->smem_refresh = per_refresh * h->wpb_refresh;
   // the dynamic shared-memory limit is a per-kernel, process-wide attribute:
   // raise it to the device maximum once, so handles of different systems
   // (each launching with its own size) never undercut one another
@@ -1090,6 +1114,10 @@ int qmcb_create(const qmcb_system_desc *d, int max_walkers, qmcb_handle **out)
   CKC(cudaFuncSetAttribute(k_full_md, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_move_md<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
   CKC(cudaFuncSetAttribute(k_move_md<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin));
+  // the memsets above ran on the legacy default stream, which does not order
+  // against the handle's non-blocking stream: finish them before any work is
+  // queued there (a late memset of the control words would zero the live count)
+  CKC(cudaStreamSynchronize(0));
 #undef CKC
   *out = h;
   return QMCB_OK;
@@ -1180,11 +1208,14 @@ int qmcb_synchronize(qmcb_handle *h)
 }
 
 // One launch of the single-determinant full-evaluation / refresh kernel.
-static void launch_full(qmcb_handle *h, int blocks, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
+static void launch_full(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
                         const int *d_num, const double *R_in, int do_basis, EvalOut o)
 {
-  const dim3 g(blocks), b(32 * h->wpb_full);
-  const size_t sm = h->smem_full;
+  // list entries [0, num) (d_num: device count), grid sized for `cap`;
+  // the refresh (do_basis = 0) runs with its smaller per-warp scratch
+  const int wpb = do_basis ? h->wpb_full : h->wpb_refresh;
+  const dim3 g((cap + wpb - 1) / wpb), b(32 * wpb);
+  const size_t sm = do_basis ? h->smem_full : h->smem_refresh;
   if (h->params.precision == QMCB_PREC_MIXED) {
     if (h->extras)
       k_full<float, MIXED_TI, true><<<g, b, sm, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, do_basis, o);
@@ -1224,8 +1255,7 @@ static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num,
     return QMCB_OK;
   }
   if (which_e < 0) {
-    int blocks = (num + h->wpb_full - 1) / h->wpb_full;
-    launch_full(h, blocks, st, cfg, d_slots, num, nullptr, d_R, 1, o);
+    launch_full(h, num, st, cfg, d_slots, num, nullptr, d_R, 1, o);
   } else {
     if (h->state_prec != state_kind(h->params.precision))
       return fail(h, QMCB_E_STATE, "evaluate: walker state was written in another precision; evaluate all electrons first");
@@ -1467,7 +1497,7 @@ static int enqueue_steps(qmcb_handle *h, int first_step, int n_steps, double *du
         k_full_md<<<blocks_full, 32 * h->wpb_full, h->smem_full, st>>>(h->sys, h->lay, cfg, h->d_state, h->d_live, 0,
                                                                         h->d_ctl, nullptr, 0, o2);
       else
-        launch_full(h, blocks_full, st, cfg, h->d_live, 0, h->d_ctl, nullptr, 0, o2);
+        launch_full(h, h->max_walkers, st, cfg, h->d_live, 0, h->d_ctl, nullptr, 0, o2);
       ps.end(st);
     }
   }
@@ -1922,7 +1952,7 @@ static int group_enqueue(qmcb_group *g, int c, int n_steps, const int *first_ste
                                                                               h->d_state, h->d_live, 0, h->d_ctl,
                                                                               nullptr, 0, o2);
             else
-              launch_full(h, blocks_full, sb, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, 0, o2);
+              launch_full(h, h->max_walkers, sb, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, 0, o2);
           }
         }
       }

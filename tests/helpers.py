@@ -120,10 +120,12 @@ def place_near_nuclei(R, system, rng, radius=0.03):
     return es
 
 
-def oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good=0.2, precision=0, electrons=None):
+def oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good=0.2, precision=0, electrons=None,
+                    rtol=PARITY_RTOL, slope_factor=1.0):
     """Full evaluation, then single-electron moves of `electrons` (default:
     `sweeps` sweeps of all) through the C ABI and the oracle on the same
-    positions, compared call by call at the condition-scaled parity bound."""
+    positions, compared call by call at the condition-scaled parity bound
+    (rtol below the condition limit, slope_factor x the FP64 slope above)."""
     from oracle.evaluators import OracleEvaluator
     from qmcbeaver_b200.api import QMCB200Functions
     orc = OracleEvaluator(s, qf_mod=qf, dt=dt)
@@ -148,11 +150,11 @@ def oracle_sequence(s, W, qf, dt, sweeps, sigma, seed, slots_offset=0, min_good=
         good &= cond < limit
         out = f.evaluate(slots, R, e)
         kap = orc.kappa(ws)
-        compare(out, ref, PARITY_RTOL, f"{s.name} call {i} whichE={e}", mask=good, kappa=kap)
+        compare(out, ref, rtol, f"{s.name} call {i} whichE={e}", mask=good, kappa=kap)
         if (~good).any():
             # ill-conditioned Slater matrices: rounding differences of two
             # FP64 implementations grow as ~cond * 1e-15
-            tol = max(PARITY_RTOL, slope * float(worst_cond[~good].max()))
+            tol = max(rtol, slope_factor * slope * float(worst_cond[~good].max()))
             compare(out, ref, tol, f"{s.name} call {i} whichE={e} (cond {worst_cond[~good].max():.1e})", mask=~good,
                     kappa=kap)
     f.close()
