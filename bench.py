@@ -268,11 +268,11 @@ def precision_section(args, rank: int):
         mode["move_kernel_roofline"]["frac"] = mode["move_kernel_roofline"]["achieved_gbs"] / read_peaks()[0]
         if prec == QMCB_PREC_INT8_SLICES:
             # tensor ops the contraction issues per launch: tiles of 25
-            # walkers x 64-orbital tiles x 32-byte K steps x 36 digit-pair
-            # MMAs (8 digit planes, pairs i + j < 8) of 128 x 64 x 32 int8
+            # walkers x 32-orbital tiles x 32-byte K steps x 36 digit-pair
+            # MMAs (8 digit planes, pairs i + j < 8) of 128 x 32 x 32 int8
             # multiply-adds
             mm = ks["rows_mma"]
-            ops = (-(-wpl // 25)) * (-(-n // 64)) * (-(-system.n_basis // 32)) * 36 * 2 * 128 * 64 * 32
+            ops = (-(-wpl // 25)) * (-(-n // 32)) * (-(-system.n_basis // 32)) * 36 * 2 * 128 * 32 * 32
             peak_tops = 2.0 * read_bf16_peak()
             mode["contraction_roofline"] = {
                 "bound": "tensor", "kernel": "k_rows_mma", "achieved_tops": ops / (mm["ms"] / mm["launches"] / 1e3) / 1e12,
@@ -290,7 +290,8 @@ def precision_section(args, rank: int):
                        ("h2o_input", h2o, None)):
         err[name] = {PREC_NAMES[p]: el_errors(s, p, R=R) for p in (QMCB_PREC_INT8_SLICES, QMCB_PREC_MIXED)}
     out["el_error_vs_fp64_ha"] = err
-    out["note"] = ("int8_slices_tcgen05: basis values and MO coefficients cut into 8 int8 digit planes, "
+    out["note"] = ("int8_slices_tcgen05: basis values and MO coefficients scaled per 32-function block and cut into 8 int8 "
+                   "digit planes, "
                    "tcgen05.mma kind::i8 with exact int32 accumulation, FP64 recombination; FP64 inverse, "
                    "Sherman-Morrison update, ratio sums, refresh and energies. mixed_fp32_rows: FP32 basis and "
                    "orbital rows, FP64 inverse and energies.")
@@ -389,9 +390,13 @@ def serving_section(args):
         if len(a.energies) == len(b.energies)))
     h2o = np.load(os.path.join(ROOT, "tests", "golden", "inputs", "h2o.npz"))
     h2o = system_from_arrays({k[4:]: h2o[k] for k in h2o.files if k.startswith("sys_")})
-    jobs = make_input_jobs(6, rate=1.0, system=h2o, seed=5, walkers=(2048, 8192), target_error=1e-3)
+    # the input's own time step; 500 equilibration sweeps (the blocked error
+    # of a drifting series overstates the error), 8,192-16,384 walkers
+    jobs = make_input_jobs(3, rate=1.0, system=h2o, seed=5, walkers=(8192, 16384), target_error=1e-3,
+                           max_sweeps=6000, equil_sweeps=500, dt=0.01)
     r = Server(max_active=8).run(jobs)
-    out["h2o_input_1mha"] = dict(summary(r), target_error_ha=1e-3,
+    out["h2o_input_1mha"] = dict(summary(r), target_error_ha=1e-3, equil_sweeps=500,
+                                 sweeps=[int(len(j.energies)) for j in jobs],
                                  errors_ha=[j.error for j in jobs], energies_ha=[j.energy for j in jobs])
     return out
 
@@ -526,7 +531,10 @@ def profile_case(name: str) -> None:
     group in configuration 0 (the group move kernel); "rows_small" runs 6
     importance-sampled VMC steps of the 100-electron / 400-function system
     with 16,384 walkers under QMCB_PREC_INT8_SLICES (the tensor-core
-    contraction k_rows_mma, its prep kernel and the move kernel on rows)."""
+    contraction k_rows_mma, its prep kernel and the move kernel on rows);
+    "refresh_100e" sets up 16,384 walkers of the 100-electron system (one
+    full evaluation) and runs 50 FP64 steps, the last of which refreshes
+    every walker's inverses (the second k_full launch)."""
     from qmcbeaver_b200.api import QMCB200Functions, QMCB200Group
     from qmcbeaver_b200.desc import run_params
     from qmcbeaver_b200.system import make_system
@@ -565,6 +573,15 @@ def profile_case(name: str) -> None:
         st = f.run_steps(0, 6)
         print("ok", st.n_moves)
         f.close()
+    elif name == "refresh_100e":
+        s = make_system("mixed_20nuc_100e", seed=1)
+        W = 16384
+        f = QMCB200Functions(s, W, run_params(sampling=1, qf_modification=2, dt=0.01, seed=3, rel_cutoff=0.0,
+                                              refresh_interval=50))
+        f.init_walkers(s.initial_positions(W, seed=1))
+        st = f.run_steps(0, 50)
+        print("ok", st.n_moves)
+        f.close()
     else:
         raise SystemExit(f"unknown case {name}")
 
@@ -586,7 +603,7 @@ def main():
                     help="run one extra section alone and print it")
     ap.add_argument("--serve-jobs", type=int, default=12)
     ap.add_argument("--serve-rate", type=float, default=20.0)
-    ap.add_argument("--case", choices=["multidet_small", "group_small", "rows_small"],
+    ap.add_argument("--case", choices=["multidet_small", "group_small", "rows_small", "refresh_100e"],
                     help="run one small profiling workload instead of the benchmark")
     args = ap.parse_args()
     if args.case:

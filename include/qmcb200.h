@@ -74,13 +74,14 @@ extern "C" {
 /* FP64 walker state and updates; each single-electron move's orbital rows
  * (QMCSlater::update_Ds -> Array2D::gemm, QMcBeaver/src/QMCSlater.cpp:856-862)
  * come from one batched tensor-core contraction over all walkers of the step:
- * basis values and MO coefficients cut into 8 int8 digit planes, int8 x int8
- * products accumulated exactly in int32 (tcgen05 kind::i8), recombined in
- * FP64.  56 bits of every product are kept relative to the row's largest
- * basis value and the orbital's largest coefficient (FP64-level error in the
- * normwise sense), so results match QMCB_PREC_FP64 to ~1e-15 relative on
- * well-conditioned walkers (parity bound of this mode: 1e-9).  One determinant per system; the full evaluation and the LU
- * refresh run in FP64. */
+ * basis values and MO coefficients scaled per 32-function block and cut
+ * into 8 int8 digit planes, int8 x int8 products accumulated exactly in int32
+ * (tcgen05 kind::i8), every block recombined in FP64.  56 bits of every
+ * product are kept relative to its block's largest basis value and largest
+ * coefficient, so results match QMCB_PREC_FP64 to ~1e-15 relative on
+ * well-conditioned walkers (parity bound of this mode: 1e-9).  One
+ * determinant per system; the full evaluation and the LU refresh run in
+ * FP64. */
 #define QMCB_PREC_INT8_SLICES 2
 
 /*

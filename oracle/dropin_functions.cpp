@@ -35,6 +35,10 @@
 //
 // Private members of the reference classes are opened to read the tables
 // the reference keeps there (a maintainer would add accessors instead).
+#include <execinfo.h>
+#include <signal.h>
+#include <unistd.h>
+
 #include <cmath>
 #include <cstdlib>
 #include <iostream>
@@ -89,12 +93,33 @@ bool pade_tables(QMCCorrelationFunctionParameters *cp, std::vector<double> &num,
   return true;
 }
 
+// A fatal signal prints the call stack (module + offset per frame, for
+// addr2line) before the default action ends the process.
+void fatal_signal(int sig)
+{
+  const char msg[] = "QMCB200Functions: fatal signal, call stack:\n";
+  (void)!write(2, msg, sizeof(msg) - 1);
+  void *frames[64];
+  backtrace_symbols_fd(frames, backtrace(frames, 64), 2);
+  signal(sig, SIG_DFL);
+  raise(sig);
+}
+
 }  // namespace
+
+// Handles of every QMCB200Functions created (released at exit).
+static std::vector<qmcb_handle *> &live_handles()
+{
+  static std::vector<qmcb_handle *> v;
+  return v;
+}
 
 class QMCB200Functions : public QMCSCFJastrow {
  public:
   explicit QMCB200Functions(QMCInput *in) : in_(in)
   {
+    signal(SIGBUS, fatal_signal);
+    signal(SIGSEGV, fatal_signal);
     build_desc();
     // one scratch slot per walker of a pass, twice for the reference's
     // second evaluation of a rejected move
@@ -108,12 +133,34 @@ class QMCB200Functions : public QMCSCFJastrow {
                                                                                           : QMCB_QF_NONE;
     p.qf_equal_a = in->flags.umrigar93_equalelectrons_parameter;
     if (qmcb_set_params(h_, &p) != QMCB_OK) die(qmcb_last_error(h_));
+    live_handles().push_back(h_);
+    static bool registered = false;
+    if (!registered) {
+      std::atexit([] {
+        for (qmcb_handle *x : live_handles()) qmcb_destroy(x);
+        live_handles().clear();
+      });
+      registered = true;
+    }
     std::clog << "QMCB200Functions: evaluate through " << qmcb_version() << std::endl;
   }
-  // The handle lives until the process ends: the reference deletes its
-  // QMCFunctions from destructors that can run after the CUDA runtime has shut
-  // down at exit (freeing device memory then is not possible).
-  ~QMCB200Functions() {}
+  // The handle lives until the process ends and is released by an exit
+  // handler registered after the library's first CUDA call, so that it runs
+  // before the CUDA runtime's own exit handler (handlers run in reverse
+  // order); the reference deletes its QMCFunctions from destructors whose
+  // order against the runtime's shutdown is not fixed.
+  ~QMCB200Functions()
+  {
+    // QMCSlater::ciDet is set only for several determinants at allocation
+    // (QMcBeaver/src/QMCSlater.cpp:113-116) and otherwise pointed at a
+    // Slater matrix by QMCSlater's own evaluation (:669), which this class
+    // never runs; its destructor deletes it when nonzero (:299-300), so the
+    // uninitialised pointer is cleared here, before ~QMCSCFJastrow runs.
+    if (in_->WF.getNumberDeterminants() == 1) {
+      Alpha.ciDet = nullptr;
+      Beta.ciDet = nullptr;
+    }
+  }
 
   void evaluate(Array1D<QMCWalkerData *> &wd, Array1D<Array2D<double> *> &X, int num)
   {

@@ -13,30 +13,33 @@
 // multiplication by using fast routines of matrix multiplication and its
 // applications", Numer. Algorithms 59 (2012), in its integer form of
 // Ootomo, Ozaki, Yokota, "DGEMM on integer matrix multiplication unit",
-// IJHPCA 2024): every row of chi and every orbital of C is scaled by a power
-// of two to |x| < 1 and cut into kSlices signed 7-bit digits,
+// IJHPCA 2024): every 32-function block of a row of chi and of an orbital of
+// C is scaled by a power of two to |x| < 1 and cut into kSlices signed 7-bit
+// digits,
 //   x = scale * sum_s d_s 2^-(6 + 7 s),  |d_s| <= 64,
-// the digit products sum_k a_i[r][k] b_j[k][o] are exact in int32
-// (|a b| <= 2^12, K <= 2^19 / kSlices), and the pairs with i + j = t share
-// one TMEM accumulator (weight 2^-(12 + 7 t)).  The pairs with i + j < kSlices
-// keep 56 bits of every product relative to the row's largest basis value
-// and the orbital's largest coefficient: the rows carry FP64-level error in
-// the normwise sense (an FP64 dot product's error is relative to the sum of
-// its terms, which is smaller for elements far below their row's largest),
-// so the per-move Slater updates downstream stay in the FP64 regime (Slater
-// matrices of random 50 x 50 orbitals reach condition numbers of 1e6, which
-// amplify any FP32-class row error to 1e-1 Ha in the local energy).
+// the digit products of a block, sum_k a_i[r][k] b_j[k][o] over 32 k, are
+// exact in int32 (|a b| <= 2^12), and the pairs with i + j = t share one TMEM
+// accumulator (weight 2^-(12 + 7 t)).  The pairs with i + j < kSlices keep
+// 56 bits of every product relative to the block's largest basis value and
+// largest coefficient, and every block is rescaled and added in FP64: the
+// rows carry the error of an FP64 dot product over the blocks' magnitudes.
+// Per-row scales (one per row over all of K) are not enough: basis values of
+// distant centres sit many orders below the row's largest, and their terms
+// then lose the bits the Slater updates need (Slater matrices of random
+// 50 x 50 orbitals reach condition numbers of 1e6, which amplify any
+// FP32-class row error to 1e-1 Ha in the local energy).
 //
 //   k_rows_prep  one warp per walker: the move's proposal (the same draws as
 //                the move kernel, which recomputes it), the basis values at
 //                the proposed position, their per-row scales and int8 digits
 //                in the tensor-core operand layout
-//   k_rows_mma   one CTA per tile of 25 walkers (125 rows) and 64 orbitals:
-//                int8 x int8 -> int32 tcgen05.mma (kind::i8, M = 128, N = 64,
+//   k_rows_mma   one CTA per tile of 25 walkers (125 rows) and 32 orbitals:
+//                int8 x int8 -> int32 tcgen05.mma (kind::i8, M = 128, N = 32,
 //                K = 32 per instruction) over kSlices (kSlices + 1) / 2 digit
 //                pairs per K step, operands staged in shared memory by
-//                bulk copies (the TMA engine, 3 stages, one thread), accumulators
-//                in TMEM, FP64 recombination in the epilogue; writes
+//                bulk copies (the TMA engine, 3 stages, one thread), two TMEM
+//                accumulator buffers (one K step fills one while the four
+//                warps drain the other into FP64 registers); writes
 //                rows[walker][5][n]
 // The move kernel then reads the rows instead of evaluating the basis and
 // contracting (MoveArgs::rows).
@@ -49,16 +52,19 @@ namespace qmcb {
 constexpr int kSlices = 8;       // int8 digits per operand value
 constexpr int kTileRows = 128;   // MMA M: TMEM lanes
 constexpr int kTileWalkers = 25; // walkers per tile: rows 0 .. 124 used
-constexpr int kNTile = 64;       // MMA N: orbitals per CTA
-constexpr int kKStep = 32;       // int8 K of one MMA (bytes)
+constexpr int kNTile = 32;       // MMA N: orbitals per CTA
+constexpr int kKStep = 32;       // int8 K of one MMA (bytes); also the block of K sharing a scale
 constexpr int kABlock = kTileRows * kKStep;  // one digit plane of one K step of an A tile
 constexpr int kBBlock = kNTile * kKStep;     // the same for B
 constexpr int kRowsStages = 3;
 constexpr int kRowsStageBytes = kSlices * (kABlock + kBBlock);
 constexpr int kRowsSmem = kRowsStages * kRowsStageBytes + 1024;  // + barriers; > 113 KB: one CTA per SM
 static_assert(kRowsStageBytes % 16 == 0 && kABlock % 16 == 0, "bulk copies move multiples of 16 bytes");
-constexpr uint32_t kRowsTmemCols = 512;  // kSlices accumulators of kNTile int32 columns (all of TMEM)
-static_assert(kSlices * kNTile <= (int)kRowsTmemCols, "accumulators exceed the TMEM allocation");
+// two buffers of kSlices accumulators of kNTile int32 columns: the MMAs of
+// one K step fill one buffer while the epilogue drains the other
+constexpr uint32_t kRowsTmemCols = 512;
+constexpr int kAccCols = kSlices * kNTile;  // columns of one buffer
+static_assert(2 * kAccCols <= (int)kRowsTmemCols, "accumulators exceed the TMEM allocation");
 
 // Byte offset of (row r, k) in one K-step block of the no-swizzle K-major
 // operand layout: 8 x 16-byte core matrices, the two K halves 128 bytes
@@ -130,27 +136,35 @@ __global__ void __launch_bounds__(128) k_rows_prep(DevSys S, Layout L, RunCfg cf
   __syncwarp();  // chi overwrites the staged arrays
   basis_slots_warp(S, rn, chi, K, ex);
   __syncwarp();
-  // rows 5 wi .. 5 wi + 4 of the GEMM: tile, row in tile
+  // rows 5 wi .. 5 wi + 4 of the GEMM: tile, row in tile; every K step (32
+  // functions, covered by 8 lanes with 4 functions each) has its own scale
+  const unsigned gmask = 0xFFu << (8 * (lane >> 3));
   for (int d = 0; d < 5; d++) {
     const int row = 5 * wi + d, tile = row / (5 * kTileWalkers), r = row - tile * 5 * kTileWalkers;
-    double m = 0.0;
-    for (int k = lane; k < K; k += 32) m = fmax(m, fabs(chi[d * K + k]));
-    const double scale = rows_scale(warp_max(m)), inv = 1.0 / scale;  // exact: a power of two
-    if (lane == 0) rscale[row] = scale;
-    // four consecutive k per lane: one 4-byte store per digit plane
     for (int k0 = 4 * lane; k0 < ksteps * kKStep; k0 += 128) {
+      double x[4], m = 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        x[u] = k0 + u < K ? chi[d * K + k0 + u] : 0.0;
+        m = fmax(m, fabs(x[u]));
+      }
+      m = fmax(m, __shfl_xor_sync(gmask, m, 4));
+      m = fmax(m, __shfl_xor_sync(gmask, m, 2));
+      m = fmax(m, __shfl_xor_sync(gmask, m, 1));
+      const double scale = rows_scale(m), inv = 1.0 / scale;  // exact: a power of two
+      const int kk = k0 / kKStep;
+      if ((lane & 7) == 0) rscale[(size_t)row * ksteps + kk] = scale;
+      // four consecutive k per lane: one 4-byte store per digit plane
       uint32_t w[kSlices];
 #pragma unroll
       for (int s = 0; s < kSlices; s++) w[s] = 0u;
 #pragma unroll
       for (int u = 0; u < 4; u++) {
-        const int k = k0 + u;
         signed char dg[kSlices];
-        rows_digits(k < K ? chi[d * K + k] * inv : 0.0, dg);
+        rows_digits(x[u] * inv, dg);
 #pragma unroll
         for (int s = 0; s < kSlices; s++) w[s] |= (uint32_t)(unsigned char)dg[s] << (8 * u);
       }
-      const int kk = k0 / kKStep;
       const size_t base = ((size_t)tile * ksteps + kk) * kSlices * kABlock + rows_blk_off(r, k0 % kKStep);
 #pragma unroll
       for (int s = 0; s < kSlices; s++) *(uint32_t *)(A + base + (size_t)s * kABlock) = w[s];
@@ -222,13 +236,43 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *v)
       : "r"(taddr));
 }
 
+// Bounded wait that also gives up once *abort is set (another thread of the
+// CTA gave up first): false then, or after ~0.5 s (2^30 cycles).
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t mbar, uint32_t parity, const volatile int *abort)
+{
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (*abort || clock64() - t0 > (1ll << 30)) return false;
+  }
+}
+
 // ------------------------------------------------------------------------
 // k_rows_mma: grid (tiles, orbital tiles), 128 threads.  A: [tile][kstep]
 // [slice] blocks of kABlock bytes; B: [orbital tile][kstep][slice] blocks of
 // kBBlock bytes (the spin's MO coefficients, digits made at set-up);
-// rscale [rows], cscale [orbital tiles x kNTile]; rows [nrows][n] FP64 with
-// nrows = 5 x walkers.  err: set to 1 when a wait gave up (the rows are then
-// not written).
+// rscale [rows][ksteps], cscale [orbital tiles][ksteps][kNTile]: every
+// 32-function block of K has its own power-of-two scale on both sides, so
+// the digits keep 56 bits relative to the block's largest values and the
+// rows carry the error of an FP64 dot product of 32-term blocks.  rows
+// [nrows][n] FP64 with nrows = 5 x walkers.  err: set to 1 when a wait gave
+// up (the rows are then not written).
+//
+// Per K step, thread 0 issues the kSlices (kSlices + 1) / 2 digit-pair MMAs
+// into one of two TMEM buffers (the K step's parity) and commits them; the
+// four warps drain the other buffer meanwhile: the eight int32 accumulators
+// of a K step are below 2^20 in magnitude (32 products of digits <= 2^6 in
+// magnitude, at most 8 pairs), so neighbouring accumulators combine exactly
+// in int32 (a_t 2^7 + a_{t+1} < 2^28) and four exact FP64 conversions give
+// the K step's scaled sum, which is added to the FP64 result in registers.
 __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restrict__ A,
                                                      const signed char *__restrict__ B,
                                                      const double *__restrict__ rscale,
@@ -236,6 +280,7 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
                                                      int num, const int *d_num, double *__restrict__ rows,
                                                      int *err)
 {
+  static_assert(kSlices == 8, "the drain combines accumulators in four pairs");
   extern __shared__ __align__(1024) unsigned char rsm[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nw = d_num ? *d_num : num;
@@ -243,11 +288,16 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
   if (tile * kTileWalkers >= nw) return;  // whole CTA: before any TMEM or barrier use
   unsigned char *stage0 = rsm;
   // full[s]: the stage's operands landed (bulk copies, transaction bytes);
-  // empty[s]: the MMAs that read the stage completed (tcgen05.commit)
+  // empty[s]: the MMAs that read the stage completed (tcgen05.commit);
+  // done[b]: the MMAs of TMEM buffer b completed (tcgen05.commit);
+  // drained[b]: the 128 threads read buffer b (one arrival each)
   uint64_t *full = (uint64_t *)(rsm + kRowsStages * kRowsStageBytes);
   uint64_t *empty = full + kRowsStages;
-  uint32_t *tslot = (uint32_t *)(empty + kRowsStages);
-  int *s_status = (int *)(tslot + 1);  // [0] ok, [1] last committed K step
+  uint64_t *done = empty + kRowsStages;
+  uint64_t *drained = done + 2;
+  uint32_t *tslot = (uint32_t *)(drained + 2);
+  volatile int *s_abort = (volatile int *)(tslot + 1);
+  int *s_last = (int *)(tslot + 2);  // last committed K step (thread 0)
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
                  "r"(kRowsTmemCols));
@@ -258,6 +308,12 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(full + s)));
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(empty + s)));
     }
+    for (int b = 0; b < 2; b++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(done + b)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(smem_u32(drained + b)));
+    }
+    *s_abort = 0;
+    *s_last = -1;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -267,104 +323,129 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
 
   const signed char *Ag = A + (size_t)tile * ksteps * kSlices * kABlock;
   const signed char *Bg = B + (size_t)ntile * ksteps * kSlices * kBBlock;
-  if (tid == 0) {
-    // one thread streams the K steps: the digit planes of a K step are
-    // contiguous in global memory (kSlices x kABlock of A, kSlices x kBBlock
-    // of B), so two bulk copies fill a stage; kRowsStages - 1 steps are in
-    // flight while the tensor cores work on the current one
-    auto load = [&](int kk) {
-      const int st = kk % kRowsStages;
-      const uint32_t fb = smem_u32(full + st), dst = smem_u32(stage0 + st * kRowsStageBytes);
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"((uint32_t)kRowsStageBytes)
-                   : "memory");
-      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-                   "l"(Ag + (size_t)kk * kSlices * kABlock), "r"((uint32_t)(kSlices * kABlock)), "r"(fb)
-                   : "memory");
-      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                       dst + kSlices * kABlock),
-                   "l"(Bg + (size_t)kk * kSlices * kBBlock), "r"((uint32_t)(kSlices * kBBlock)), "r"(fb)
-                   : "memory");
-    };
-    int loaded = 0, committed = -1;
-    bool ok = true;
+  // one thread streams the K steps: the digit planes of a K step are
+  // contiguous in global memory (kSlices x kABlock of A, kSlices x kBBlock of
+  // B), so two bulk copies fill a stage; kRowsStages - 1 steps are in flight
+  // while the tensor cores work on the current one
+  auto load = [&](int kk) {
+    const int st = kk % kRowsStages;
+    const uint32_t fb = smem_u32(full + st), dst = smem_u32(stage0 + st * kRowsStageBytes);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"((uint32_t)kRowsStageBytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+                 "l"(Ag + (size_t)kk * kSlices * kABlock), "r"((uint32_t)(kSlices * kABlock)), "r"(fb)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     dst + kSlices * kABlock),
+                 "l"(Bg + (size_t)kk * kSlices * kBBlock), "r"((uint32_t)(kSlices * kBBlock)), "r"(fb)
+                 : "memory");
+  };
+  int loaded = 0;  // thread 0 only
+  if (tid == 0)
     for (; loaded < kRowsStages && loaded < ksteps; loaded++) load(loaded);
-    for (int kk = 0; kk < ksteps; kk++) {
-      const int st = kk % kRowsStages;
-      ok = mbar_wait(smem_u32(full + st), (uint32_t)((kk / kRowsStages) & 1));
-      if (!ok) break;
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t a0 = smem_u32(stage0 + st * kRowsStageBytes), b0 = a0 + kSlices * kABlock;
+
+  // the FP64 result of this thread's row (TMEM lane) and the CTA's orbitals
+  const int r = 32 * warp + lane;
+  const int row = tile * 5 * kTileWalkers + r;
+  const bool live = r < 5 * kTileWalkers && row < 5 * nw;
+  double out[kNTile];
 #pragma unroll
-      for (int i = 0; i < kSlices; i++) {
+  for (int q = 0; q < kNTile; q++) out[q] = 0.0;
+  const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+
+  // drain K step kk from buffer kk & 1; false when a wait gave up
+  auto drain = [&](int kk) -> bool {
+    const int b = kk & 1;
+    // warp-uniform: tcgen05.ld is .sync.aligned
+    if (!__all_sync(0xFFFFFFFFu, mbar_wait_or_abort(smem_u32(done + b), (uint32_t)((kk >> 1) & 1), s_abort)))
+      return false;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const double rs = live ? rscale[(size_t)row * ksteps + kk] : 0.0;
+    const double *cs = cscale + ((size_t)ntile * ksteps + kk) * kNTile;
 #pragma unroll
-        for (int j = 0; j + i < kSlices; j++) {
-          const uint64_t ad = umma_desc(a0 + i * kABlock, 128, 256);
-          const uint64_t bd = umma_desc(b0 + j * kBBlock, 128, 256);
-          mma_i8(tmem + (uint32_t)((i + j) * kNTile), ad, bd, (kk > 0 || i > 0) ? 1u : 0u);
+    for (int c = 0; c < kNTile / 16; c++) {
+      double part[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) part[q] = 0.0;
+#pragma unroll
+      for (int p = 0; p < kSlices / 2; p++) {
+        uint32_t v0[16], v1[16];
+        const uint32_t col = (uint32_t)(b * kAccCols + 2 * p * kNTile + 16 * c);
+        tmem_ld16(lane_base + col, v0);
+        tmem_ld16(lane_base + col + kNTile, v1);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        // pair p holds weights 2^-(12 + 14 p) (accumulator 2p) and
+        // 2^-(19 + 14 p) (accumulator 2p + 1): a_2p 2^7 + a_2p+1 at 2^-(19 + 14 p)
+        const double w = ldexp(1.0, -19 - 14 * p);
+#pragma unroll
+        for (int q = 0; q < 16; q++) part[q] = fma((double)((int)v0[q] * 128 + (int)v1[q]), w, part[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 16; q++) out[16 * c + q] = fma(part[q], rs * cs[16 * c + q], out[16 * c + q]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(drained + b)) : "memory");
+    return true;
+  };
+
+  bool ok = true;
+  for (int kk = 0; kk < ksteps && ok; kk++) {
+    if (tid == 0 && !*s_abort) {
+      const int st = kk % kRowsStages, b = kk & 1;
+      bool w = mbar_wait_or_abort(smem_u32(full + st), (uint32_t)((kk / kRowsStages) & 1), s_abort);
+      // the buffer's previous K step (kk - 2) has been read by every thread
+      if (w && kk >= 2) w = mbar_wait_or_abort(smem_u32(drained + b), (uint32_t)(((kk - 2) >> 1) & 1), s_abort);
+      if (w) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t a0 = smem_u32(stage0 + st * kRowsStageBytes), b0 = a0 + kSlices * kABlock;
+#pragma unroll
+        for (int i = 0; i < kSlices; i++) {
+#pragma unroll
+          for (int j = 0; j + i < kSlices; j++) {
+            const uint64_t ad = umma_desc(a0 + i * kABlock, 128, 256);
+            const uint64_t bd = umma_desc(b0 + j * kBBlock, 128, 256);
+            // the first pair of accumulator t = i + j in this K step is (0, t)
+            mma_i8(tmem + (uint32_t)(b * kAccCols + (i + j) * kNTile), ad, bd, i > 0 ? 1u : 0u);
+          }
+        }
+        mma_commit(smem_u32(empty + st));
+        mma_commit(smem_u32(done + b));
+        *s_last = kk;
+        // refill the stage the previous K step used, once its MMAs are done
+        if (kk >= 1 && loaded < ksteps) {
+          const int sp = (kk - 1) % kRowsStages;
+          w = mbar_wait_or_abort(smem_u32(empty + sp), (uint32_t)(((kk - 1) / kRowsStages) & 1), s_abort);
+          if (w) load(loaded++);
         }
       }
-      mma_commit(smem_u32(empty + st));
-      committed = kk;
-      // refill the stage the previous K step used, once its MMAs are done
-      if (kk >= 1 && loaded < ksteps) {
-        const int sp = (kk - 1) % kRowsStages;
-        ok = mbar_wait(smem_u32(empty + sp), (uint32_t)(((kk - 1) / kRowsStages) & 1));
-        if (!ok) break;
-        load(loaded++);
-      }
+      if (!w) *s_abort = 1;
     }
-    if (!ok) {
-      // a wait gave up: let the copies already issued land (bounded) before
-      // the shared memory is left
-      for (int l = committed + 1; l < loaded; l++) mbar_wait(smem_u32(full + l % kRowsStages), (uint32_t)((l / kRowsStages) & 1));
-    }
-    s_status[0] = ok ? 1 : 0;
-    s_status[1] = committed;
+    __syncwarp();
+    if (kk >= 1) ok = drain(kk - 1);
+    if (!ok) *s_abort = 1;
   }
+  if (ok && ksteps > 0) ok = drain(ksteps - 1);
+  if (!ok) *s_abort = 1;
   __syncthreads();
-  const bool ok = s_status[0] != 0;
-  const int committed = s_status[1];
-  // every MMA of this CTA is done once the last commit's phase completes
-  // (waited for after a failed wait too, so that no MMA is in flight when
-  // the TMEM is released)
-  bool done = true;
-  if (committed >= 0)
-    done = mbar_wait(smem_u32(empty + committed % kRowsStages), (uint32_t)((committed / kRowsStages) & 1));
-  const int okall = __syncthreads_and((ok && done && committed == ksteps - 1) ? 1 : 0);
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  if (okall) {
-    // epilogue: warp w holds rows 32 w .. 32 w + 31 (TMEM lanes)
-    const int r = 32 * warp + lane;
-    const int row = tile * 5 * kTileWalkers + r;
-    const bool live = r < 5 * kTileWalkers && row < 5 * nw;
-    const double rs = live ? rscale[row] : 0.0;
-    for (int c = 0; c < kNTile / 16; c++) {
-      double acc[16];
-#pragma unroll
-      for (int q = 0; q < 16; q++) acc[q] = 0.0;
-      double w = 1.0 / 4096.0;  // 2^-(12 + 7 t)
-#pragma unroll
-      for (int t = 0; t < kSlices; t++) {
-        uint32_t v[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(t * kNTile + 16 * c), v);
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-        for (int q = 0; q < 16; q++) acc[q] = fma((double)(int)v[q], w, acc[q]);
-        w *= 1.0 / 128.0;
-      }
-      if (live) {
-        const int o0 = ntile * kNTile + 16 * c;
-#pragma unroll
-        for (int q = 0; q < 16; q++)
-          if (o0 + q < n) rows[(size_t)row * n + o0 + q] = acc[q] * (rs * cscale[o0 + q]);
-      }
-    }
-  } else if (tid == 0) {
-    atomicExch(err, 1);
+  const bool okall = !*s_abort;
+  if (tid == 0) {
+    // leave no copy or MMA in flight: the copies issued but not consumed
+    // land (bounded waits), then the last commit's phase covers every MMA
+    const int last = *s_last;
+    for (int l = last + 1; l < loaded; l++)
+      mbar_wait(smem_u32(full + l % kRowsStages), (uint32_t)((l / kRowsStages) & 1));
+    if (last >= 0) mbar_wait(smem_u32(done + (last & 1)), (uint32_t)((last >> 1) & 1));
+    if (!okall) atomicExch(err, 1);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kRowsTmemCols));
+  if (okall && live) {
+    const int o0 = ntile * kNTile;
+#pragma unroll
+    for (int q = 0; q < kNTile; q++)
+      if (o0 + q < n) rows[(size_t)row * n + o0 + q] = out[q];
+  }
 }
 
 }  // namespace qmcb

@@ -516,7 +516,6 @@ static int rows_setup(qmcb_handle *h)
 {
   if (h->d_rows_A) return QMCB_OK;
   const int K = h->K, N = h->N;
-  if (K > 8192) return fail(h, QMCB_E_LIMIT, "QMCB_PREC_INT8_SLICES: at most 8192 basis functions (int32 digit sums)");
   const int ks = (K + kKStep - 1) / kKStep;
   const size_t tiles = (size_t)(h->max_walkers + kTileWalkers - 1) / kTileWalkers;
 #define CKR(call)                                                                                    \
@@ -530,18 +529,22 @@ static int rows_setup(qmcb_handle *h)
     const int n = sp ? h->sys.nb : h->sys.na;
     const int nt = std::max((n + kNTile - 1) / kNTile, 1);
     std::vector<signed char> B((size_t)nt * ks * kSlices * kBBlock, 0);
-    std::vector<double> cs((size_t)nt * kNTile, 1.0);
+    // one scale per (orbital, K step): cs[(orbital tile x ks + K step) x kNTile + orbital in tile]
+    std::vector<double> cs((size_t)nt * ks * kNTile, 1.0);
     const std::vector<double> &ct = h->ct_host[sp];
     for (int o = 0; o < n; o++) {
-      double amax = 0.0;
-      for (int k = 0; k < K; k++) amax = std::max(amax, std::fabs(ct[(size_t)k * n + o]));
-      const double scale = rows_scale(amax), inv = 1.0 / scale;
-      cs[o] = scale;
-      for (int k = 0; k < K; k++) {
-        signed char dg[kSlices];
-        rows_digits(ct[(size_t)k * n + o] * inv, dg);
-        for (int q = 0; q < kSlices; q++)
-          B[(((size_t)(o / kNTile) * ks + k / kKStep) * kSlices + q) * kBBlock + rows_blk_off(o % kNTile, k % kKStep)] = dg[q];
+      for (int kk = 0; kk < ks; kk++) {
+        const int k1 = std::min(K, (kk + 1) * kKStep);
+        double amax = 0.0;
+        for (int k = kk * kKStep; k < k1; k++) amax = std::max(amax, std::fabs(ct[(size_t)k * n + o]));
+        const double scale = rows_scale(amax), inv = 1.0 / scale;
+        cs[((size_t)(o / kNTile) * ks + kk) * kNTile + o % kNTile] = scale;
+        for (int k = kk * kKStep; k < k1; k++) {
+          signed char dg[kSlices];
+          rows_digits(ct[(size_t)k * n + o] * inv, dg);
+          for (int q = 0; q < kSlices; q++)
+            B[(((size_t)(o / kNTile) * ks + kk) * kSlices + q) * kBBlock + rows_blk_off(o % kNTile, k % kKStep)] = dg[q];
+        }
       }
     }
     CKR(cudaMalloc(&h->d_rows_B[sp], B.size()));
@@ -554,7 +557,7 @@ static int rows_setup(qmcb_handle *h)
   // on the handle's stream (non-blocking: a legacy-stream memset would not
   // be ordered with its work)
   CKR(cudaMemsetAsync(h->d_rows_A, 0, abytes, h->stream));  // rows 125 .. 127 of every tile stay zero
-  CKR(cudaMalloc(&h->d_rows_rs, sizeof(double) * tiles * 5 * kTileWalkers));
+  CKR(cudaMalloc(&h->d_rows_rs, sizeof(double) * tiles * 5 * kTileWalkers * ks));
   CKR(cudaMalloc(&h->d_rows_out, sizeof(double) * (size_t)h->max_walkers * 5 * h->nmax));
   // a wait inside the contraction kernel that gave up sets ctl[3], which
   // returns with every batch's live count

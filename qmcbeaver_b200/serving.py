@@ -286,10 +286,12 @@ def make_jobs(n_jobs: int, rate: float, seed: int = 1, electrons=(4, 40), walker
 
 
 def make_input_jobs(n_jobs: int, rate: float, system: MolecularSystem, seed: int = 1, walkers=(1024, 4096),
-                    target_error: float = 1e-3, max_sweeps: int = 4000, min_blocks: int = 16) -> List[Job]:
+                    target_error: float = 1e-3, max_sweeps: int = 4000, min_blocks: int = 16,
+                    equil_sweeps: int = 5, dt: float = 0.01) -> List[Job]:
     """Poisson arrivals at `rate` jobs/s of VMC energy jobs on one given
     system (for example one of the reference's input files), walkers uniform
-    in `walkers`, each run to `target_error` Hartree."""
+    in `walkers`, each equilibrated for `equil_sweeps` all-electron sweeps
+    (samples not kept) and run to `target_error` Hartree."""
     rng = np.random.default_rng(seed)
     t = 0.0
     jobs = []
@@ -297,6 +299,7 @@ def make_input_jobs(n_jobs: int, rate: float, system: MolecularSystem, seed: int
         t += rng.exponential(1.0 / rate)
         W = int(rng.integers(walkers[0], walkers[1] + 1))
         jobs.append(Job(job_id=i, system=system, walkers=W, target_error=target_error, seed=seed * 7919 + i,
-                        arrival=t, max_sweeps=max_sweeps, min_blocks=min_blocks))
+                        arrival=t, max_sweeps=max_sweeps, min_blocks=min_blocks, equil_sweeps=equil_sweeps,
+                        dt=dt))
     return jobs
 

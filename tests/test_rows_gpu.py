@@ -3,10 +3,10 @@ contraction (QMCB_PREC_INT8_SLICES: basis values and MO coefficients cut into
 8 int8 digit planes, tcgen05 int8 products accumulated exactly in int32,
 recombined in FP64) against the reference and the oracle.
 
-Every row keeps 56 bits relative to its largest basis value and every
-orbital 56 bits relative to its largest coefficient (the FP64 dot product's
-error is instead relative to the sum of its terms), so elements much smaller
-than their row's largest carry a few times FP64's rounding: the parity bounds
+Every 32-function block of a row keeps 56 bits relative to its largest
+basis value and largest coefficient (the FP64 dot product's error is instead
+relative to the sum of its terms), so elements much smaller than their
+block's largest carry a few times FP64's rounding: the parity bounds
 of this mode are 1e-9 relative on the golden cases recorded from the reference
 and on walkers whose Slater matrices stay below condition 5e4, 2e-14 x cond
 above (ten times the plain FP64 path's).  The per-walker local-energy
@@ -58,9 +58,10 @@ def test_rows_match_oracle_shapes(ne, nn, nb, W, seed):
 
 
 def test_rows_two_orbital_tiles():
-    # 66 electrons per spin: two 64-orbital tiles of the contraction
+    # 66 electrons per spin: three 32-orbital tiles of the contraction, the last
+    # with two orbitals
     s = make_random_molecule(132, 14, 300, 7.0, (1, 6, 8), seed=6)
-    moved = [0, 1, 65, 66, 67, 131]
+    moved = [0, 1, 31, 32, 65, 66, 67, 98, 131]
     oracle_sequence(s, 3, 2, 0.02, 0, 0.2, seed=6, min_good=0.0, precision=QMCB_PREC_INT8_SLICES, electrons=moved,
                     rtol=ROWS_RTOL, slope_factor=10.0)
 
