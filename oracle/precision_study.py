@@ -7,7 +7,8 @@ gradients, Laplacians) contracted in FP64 and in reduced-precision forms:
 FP64 rows stored as FP32, FP32 operands and accumulation, TF32, BF16,
 3xTF32 and 3xBF16 split products with FP32 accumulation, and the int8
 digit-plane scheme with exact integer sums (Ozaki et al. 2012; Ootomo,
-Ozaki, Yokota 2024) with 3-8 digit planes.  The inverse is FP64 in every
+Ozaki, Yokota 2024) with 3-8 digit planes, scaled per row / orbital over
+all of K or per 32-wide block of K (ozakiblk).  The inverse is FP64 in every
 case.  Printed per mode: the per-walker error of the Laplacian term and of
 the gradient ratios against FP64 (median, p90, max), and the Slater
 matrices' condition numbers.
@@ -96,6 +97,9 @@ def contract(rows, C, mode):
         elif mode.startswith("fp64x32"):
             # fp64 chi, fp64 C, but output rounded to fp32 (storage)
             out.append((X @ C.T).astype(np.float32).astype(np.float64))
+        elif mode.startswith("ozakiblk"):
+            S = int(mode[8:])
+            out.append(ozaki_blocked(X, C.T, S))
         elif mode.startswith("ozaki"):
             S = int(mode[5:])
             out.append(ozaki(X, C.T, S))
@@ -128,6 +132,17 @@ def ozaki(A, B, S):
     return acc * sa * sb
 
 
+def ozaki_blocked(A, B, S, block=32):
+    """The same digits with one scale per 32-wide block of K on both sides
+    (the layout of the tensor-core kernel): every block's pairs recombined
+    and rescaled in FP64, the blocks summed in FP64."""
+    K = A.shape[1]
+    acc = np.zeros((A.shape[0], B.shape[1]))
+    for k0 in range(0, K, block):
+        acc += ozaki(A[:, k0:k0 + block], B[k0:k0 + block, :], S)
+    return acc
+
+
 def slater_lap(s, R, mode):
     N = s.n_electrons
     na = s.n_alpha
@@ -155,7 +170,8 @@ def main():
     s = make_system(wl, seed=1)
     R = s.initial_positions(W, seed=5)
     base = slater_lap(s, R, "fp64")
-    for mode in (sys.argv[3].split(",") if len(sys.argv) > 3 else ["fp64x32", "fp32", "3xtf32", "ozaki5", "ozaki6", "ozaki7", "ozaki8"]):
+    for mode in (sys.argv[3].split(",") if len(sys.argv) > 3 else ["fp64x32", "fp32", "3xtf32", "ozaki5", "ozaki6", "ozaki7", "ozaki8",
+                                                                   "ozakiblk7", "ozakiblk8"]):
         res = slater_lap(s, R, mode)
         errs, gerr = [], []
         for sp in range(2):

@@ -666,48 +666,65 @@ __device__ __forceinline__ void basis_shells_warp(const DevSys &S, const double 
 // exponentials with their own coefficients (E0, E1, El as in shell_members).
 // Both passes spread the work evenly over the lanes, where one lane per
 // shell leaves the lanes of s shells idle while d shells run six members.
-__device__ __forceinline__ void basis_slots_warp(const DevSys &S, const double r[3], double *chi, int ldc,
-                                                 double *ex)
+// The exponential slots exp(-a |r - A|^2) of every (nucleus, primitive
+// exponent) pair at r, lanes over slots.
+__device__ __forceinline__ void basis_slot_exps_warp(const DevSys &S, const double r[3], double *ex)
 {
-  const int lane = lane_id();
-  for (int q = lane; q < S.nslot; q += 32) {
+  for (int q = lane_id(); q < S.nslot; q += 32) {
     const int2 t = __ldg(&S.xsl[q]);
     const double4 A = S.nuc[t.x];
     const double x = r[0] - A.x, y = r[1] - A.y, z = r[2] - A.z;
     ex[q] = exp(-__ldg(&S.pexp[t.y]) * (x * x + y * y + z * z));
   }
+}
+
+// Basis function k at r from the slot exponentials: value, gradient,
+// Laplacian into v[0..4].
+__device__ __forceinline__ void basis_function_rows(const DevSys &S, const double r[3], int k, const double *ex,
+                                                    double v[5])
+{
+  const int4 fq = __ldg(&S.fq[k]);
+  const int2 f = __ldg(&S.fn[k]);
+  const double4 A = S.nuc[fq.x];
+  const double x = r[0] - A.x, y = r[1] - A.y, z = r[2] - A.z;
+  const double r2 = x * x + y * y + z * z;
+  const int a = f.x & 0xff, b = (f.x >> 8) & 0xff, c = (f.x >> 16) & 0xff;
+  const double Lf = 4.0 * fq.w + 6.0, r2x4 = 4.0 * r2;
+  double E0 = 0.0, E1 = 0.0, El = 0.0;
+  for (int i = 0; i < fq.z; i++) {
+    const double al = __ldg(&S.pexp[f.y + i]);
+    const double e = __ldg(&S.pcoef[f.y + i]) * ex[fq.y + i];
+    E0 += e;
+    E1 = fma(e, al, E1);
+    El = fma(e, al * fma(r2x4, al, -Lf), El);
+  }
+  const double xa = ipow(x, a), yb = ipow(y, b), zc = ipow(z, c);
+  const double P = xa * yb * zc;
+  const double Px = a ? a * ipow(x, a - 1) * yb * zc : 0.0;
+  const double Py = b ? b * xa * ipow(y, b - 1) * zc : 0.0;
+  const double Pz = c ? c * xa * yb * ipow(z, c - 1) : 0.0;
+  double Pl = 0.0;
+  if (a > 1) Pl += a * (a - 1.0) * ipow(x, a - 2) * yb * zc;
+  if (b > 1) Pl += b * (b - 1.0) * xa * ipow(y, b - 2) * zc;
+  if (c > 1) Pl += c * (c - 1.0) * xa * yb * ipow(z, c - 2);
+  const double PE1 = P * E1;
+  v[0] = E0 * P;
+  v[1] = fma(E0, Px, -2.0 * x * PE1);
+  v[2] = fma(E0, Py, -2.0 * y * PE1);
+  v[3] = fma(E0, Pz, -2.0 * z * PE1);
+  v[4] = fma(E0, Pl, P * El);
+}
+
+__device__ __forceinline__ void basis_slots_warp(const DevSys &S, const double r[3], double *chi, int ldc,
+                                                 double *ex)
+{
+  basis_slot_exps_warp(S, r, ex);
   __syncwarp();
-  for (int k = lane; k < S.K; k += 32) {
-    const int4 fq = __ldg(&S.fq[k]);
-    const int2 f = __ldg(&S.fn[k]);
-    const double4 A = S.nuc[fq.x];
-    const double x = r[0] - A.x, y = r[1] - A.y, z = r[2] - A.z;
-    const double r2 = x * x + y * y + z * z;
-    const int a = f.x & 0xff, b = (f.x >> 8) & 0xff, c = (f.x >> 16) & 0xff;
-    const double Lf = 4.0 * fq.w + 6.0, r2x4 = 4.0 * r2;
-    double E0 = 0.0, E1 = 0.0, El = 0.0;
-    for (int i = 0; i < fq.z; i++) {
-      const double al = __ldg(&S.pexp[f.y + i]);
-      const double e = __ldg(&S.pcoef[f.y + i]) * ex[fq.y + i];
-      E0 += e;
-      E1 = fma(e, al, E1);
-      El = fma(e, al * fma(r2x4, al, -Lf), El);
-    }
-    const double xa = ipow(x, a), yb = ipow(y, b), zc = ipow(z, c);
-    const double P = xa * yb * zc;
-    const double Px = a ? a * ipow(x, a - 1) * yb * zc : 0.0;
-    const double Py = b ? b * xa * ipow(y, b - 1) * zc : 0.0;
-    const double Pz = c ? c * xa * yb * ipow(z, c - 1) : 0.0;
-    double Pl = 0.0;
-    if (a > 1) Pl += a * (a - 1.0) * ipow(x, a - 2) * yb * zc;
-    if (b > 1) Pl += b * (b - 1.0) * xa * ipow(y, b - 2) * zc;
-    if (c > 1) Pl += c * (c - 1.0) * xa * yb * ipow(z, c - 2);
-    const double PE1 = P * E1;
-    chi[0 * ldc + k] = E0 * P;
-    chi[1 * ldc + k] = fma(E0, Px, -2.0 * x * PE1);
-    chi[2 * ldc + k] = fma(E0, Py, -2.0 * y * PE1);
-    chi[3 * ldc + k] = fma(E0, Pz, -2.0 * z * PE1);
-    chi[4 * ldc + k] = fma(E0, Pl, P * El);
+  for (int k = lane_id(); k < S.K; k += 32) {
+    double v[5];
+    basis_function_rows(S, r, k, ex, v);
+#pragma unroll
+    for (int d = 0; d < 5; d++) chi[d * ldc + k] = v[d];
   }
 }
 

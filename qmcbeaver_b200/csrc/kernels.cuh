@@ -60,15 +60,18 @@ constexpr int kPart = 160;  // 5 quantities x 32 lanes of slice partial sums
 // spin's derivative rows and inverse.
 __host__ __device__ inline int even(int x) { return (x + 1) & ~1; }
 __host__ __device__ inline int move_region_a(int N, int K) { return even(max(5 * K, kPart + 6 * N)); }
+// k_full: chi [5][K + 1], new rows [5][nmax], the matrix inverted in place
+// [nmax][nmax], pivot scales, pivot rows, saved pivot column [nmax] each,
+// positions [3N].
 __host__ __device__ inline int full_scratch_doubles(int N, int K, int nmax)
 {
-  return 5 * (K + 1) + 5 * nmax + 2 * nmax * nmax + 2 * nmax + 3 * N + kPart + 8;
+  return even(5 * (K + 1) + 5 * nmax + nmax * nmax + 3 * nmax + 3 * N + kPart + 8);
 }
-// The LU refresh of stored Slater values (k_full with do_basis = 0) needs no
+// The refresh of stored Slater values (k_full with do_basis = 0) needs no
 // basis rows and no new-row space: a smaller per-warp scratch, more warps per SM.
 __host__ __device__ inline int refresh_scratch_doubles(int N, int nmax)
 {
-  return 2 * nmax * nmax + 2 * nmax + 3 * N + kPart + 8;
+  return even(nmax * nmax + 3 * nmax + 3 * N + kPart + 8);
 }
 
 // ------------------------------------------------------------------------
@@ -241,6 +244,122 @@ __device__ inline bool lu_inverse_warp(double *A, double *X, double *vv, double 
   return true;
 }
 
+// Warp Gauss-Jordan inverse in place, with the pivot rule of the
+// reference's LU (implicitly scaled partial pivoting, Array2D::ludcmp,
+// QMcBeaver/include/Array2D.h:1204-1340): the rows below the diagonal of
+// column j hold the same Schur complement in both eliminations, so the
+// pivots, ln|det| and the sign are the LU's.  Every step updates all rows
+// (lanes own columns, rows streamed with independent FMAs) instead of the
+// LU's two triangular solves per column, whose FMAs form one dependent
+// chain per lane; one n x n array instead of two.  A: [n][n] row-major,
+// receives A^-1 in A[o][e] (the layout of lu_inverse_warp's X); vv, piv,
+// col: n doubles of scratch each.  Returns false when singular.
+__device__ inline bool gj_inverse_warp(double *A, double *vv, double *piv, double *col, int n, double &logdet,
+                                       double &sign)
+{
+  const int lane = lane_id();
+  bool sing = false;
+  for (int i = lane; i < n; i += 32) {
+    double big = 0.0;
+    for (int j = 0; j < n; j++) big = fmax(big, fabs(A[i * n + j]));
+    if (big == 0.0) sing = true;
+    vv[i] = big == 0.0 ? 0.0 : 1.0 / big;
+  }
+  sing = __any_sync(QMCB_FULL_MASK, sing);
+  __syncwarp();
+  if (sing) {
+    logdet = -INFINITY;
+    sign = 0.0;
+    return false;
+  }
+  double sg = 1.0, ld = 0.0;
+  for (int j = 0; j < n; j++) {
+    double best = -1.0;
+    int bi = -1;
+    for (int i = j + lane; i < n; i += 32) {
+      double v = vv[i] * fabs(A[i * n + j]);
+      if (v >= best) {
+        best = v;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(QMCB_FULL_MASK, best, o);
+      int oi = __shfl_xor_sync(QMCB_FULL_MASK, bi, o);
+      if (ob > best || (ob == best && oi > bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (bi != j) {
+      for (int k = lane; k < n; k += 32) {
+        double t = A[bi * n + k];
+        A[bi * n + k] = A[j * n + k];
+        A[j * n + k] = t;
+      }
+      if (lane == 0) vv[bi] = vv[j];
+      sg = -sg;
+    }
+    if (lane == 0) piv[j] = (double)bi;
+    __syncwarp();
+    const double p = A[j * n + j];
+    if (p == 0.0) {
+      sing = true;
+      break;
+    }
+    ld += log(fabs(p));
+    if (p < 0) sg = -sg;
+    // column j is saved and replaced by the identity's column j, whose
+    // image under the step's row operations is column j of the inverse
+    for (int i = lane; i < n; i += 32) {
+      col[i] = A[i * n + j];
+      A[i * n + j] = i == j ? 1.0 : 0.0;
+    }
+    __syncwarp();
+    const double pinv = 1.0 / p;
+    for (int k = lane; k < n; k += 32) A[j * n + k] *= pinv;
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) {
+      const double rj = A[j * n + k];
+      int i = 0;
+      for (; i + 4 <= n; i += 4) {
+        double c[4], a[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          c[u] = col[i + u];
+          a[u] = A[(i + u) * n + k];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (i + u != j) A[(i + u) * n + k] = fma(-c[u], rj, a[u]);
+      }
+      for (; i < n; i++)
+        if (i != j) A[i * n + k] = fma(-col[i], rj, A[i * n + k]);
+    }
+    __syncwarp();
+  }
+  if (sing) {
+    logdet = -INFINITY;
+    sign = 0.0;
+    return false;
+  }
+  logdet = ld;
+  sign = sg;
+  // the row interchanges, undone as column interchanges, last first
+  for (int j = n - 1; j >= 0; j--) {
+    const int bi = (int)piv[j];
+    if (bi != j)
+      for (int i = lane; i < n; i += 32) {
+        const double t = A[i * n + j];
+        A[i * n + j] = A[i * n + bi];
+        A[i * n + bi] = t;
+      }
+  }
+  __syncwarp();
+  return true;
+}
+
 // ------------------------------------------------------------------------
 // Jastrow and potential from scratch for all electrons (updateAll order of
 // pairs is irrelevant here: totals are summed fresh, not incrementally).
@@ -343,10 +462,11 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
   double *chi = sm;
   double *Dn = chi + 5 * ldc;
   double *A = do_basis ? Dn + 5 * nmax : sm;  // the refresh has no basis rows
-  double *X = A + nmax * nmax;
-  double *vv = X + nmax * nmax;
+  double *X = A;                              // inverted in place
+  double *vv = A + nmax * nmax;
   double *piv = vv + nmax;
-  double *Rs = piv + nmax;
+  double *col = piv + nmax;
+  double *Rs = col + nmax;
   double *R = blk + L.R;
   double *sc = blk + L.sc;
 
@@ -392,7 +512,7 @@ __global__ void __launch_bounds__(128) k_full(DevSys S, Layout L, RunCfg cfg, do
     for (int t = lane; t < n * n; t += 32) A[t] = (double)Dv[t];
     __syncwarp();
     double logdet, sign;
-    bool ok = lu_inverse_warp(A, X, vv, piv, n, logdet, sign);
+    bool ok = gj_inverse_warp(A, vv, piv, col, n, logdet, sign);
     if (!ok) bad = true;
     TI *Inv = (TI *)(blk + L.Inv[sp]);
     for (int t = lane; t < n * n; t += 32) Inv[t] = (TI)X[t];

@@ -37,8 +37,8 @@
 //                int8 x int8 -> int32 tcgen05.mma (kind::i8, M = 128, N = 32,
 //                K = 32 per instruction) over kSlices (kSlices + 1) / 2 digit
 //                pairs per K step, operands staged in shared memory by
-//                bulk copies (the TMA engine, 3 stages, one thread), two TMEM
-//                accumulator buffers (one K step fills one while the four
+//                bulk copies (the TMA engine, 4 stages, one thread), two TMEM
+//                accumulator buffers (one K step fills one while the eight
 //                warps drain the other into FP64 registers); writes
 //                rows[walker][5][n]
 // The move kernel then reads the rows instead of evaluating the basis and
@@ -56,9 +56,10 @@ constexpr int kNTile = 32;       // MMA N: orbitals per CTA
 constexpr int kKStep = 32;       // int8 K of one MMA (bytes); also the block of K sharing a scale
 constexpr int kABlock = kTileRows * kKStep;  // one digit plane of one K step of an A tile
 constexpr int kBBlock = kNTile * kKStep;     // the same for B
-constexpr int kRowsStages = 3;
+constexpr int kRowsStages = 4;
 constexpr int kRowsStageBytes = kSlices * (kABlock + kBBlock);
 constexpr int kRowsSmem = kRowsStages * kRowsStageBytes + 1024;  // + barriers; > 113 KB: one CTA per SM
+constexpr int kRowsThreads = 256;  // two warps per TMEM lane quarter, each draining half the columns
 static_assert(kRowsStageBytes % 16 == 0 && kABlock % 16 == 0, "bulk copies move multiples of 16 bytes");
 // two buffers of kSlices accumulators of kNTile int32 columns: the MMAs of
 // one K step fill one buffer while the epilogue drains the other
@@ -79,16 +80,26 @@ __host__ __device__ inline int rows_blk_off(int r, int k)
 // into balanced base-128 digits from the top, d_s = round(q_s / 2^w_s) with
 // w_s = 7 (kSlices - 1 - s) and q_{s+1} = q_s - d_s 2^w_s, so that
 // x = sum_s d_s 2^-(6 + 7 s) up to the rounding of q (2^-(7 kSlices - 1)),
-// |d_s| <= 64.  Integer arithmetic after the one conversion.
+// |d_s| <= 64.  q = hi 2^28 + lo with hi = rint(x 2^27) and lo =
+// rint((x 2^27 - hi) 2^28) (the subtraction is exact), |hi|, |lo| <= 2^27:
+// each half gives four digits in 32-bit integer arithmetic.
 __host__ __device__ inline void rows_digits(double x, signed char *d)
 {
-  static_assert(7 * kSlices - 1 <= 62, "digits exceed a 64-bit fixed-point value");
-  long long q = llrint(ldexp(x, 7 * kSlices - 1));
-  for (int s = 0; s < kSlices; s++) {
-    const int w = 7 * (kSlices - 1 - s);
-    const long long ds = w > 0 ? (q + (1ll << (w - 1))) >> w : q;  // arithmetic shift: floor
-    d[s] = (signed char)ds;
-    q -= ds << w;
+  static_assert(kSlices == 8, "two halves of four digits");
+  const double xs = x * 134217728.0;  // 2^27: exact
+  const double h = rint(xs);
+  const int half[2] = {(int)h, (int)rint((xs - h) * 268435456.0)};  // 2^28: exact
+#pragma unroll
+  for (int p = 0; p < 2; p++) {
+    int q = half[p];
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      const int w = 21 - 7 * t;
+      const int ds = (q + (1 << (w - 1))) >> w;  // arithmetic shift: floor
+      d[4 * p + t] = (signed char)ds;
+      q -= ds * (1 << w);
+    }
+    d[4 * p + 3] = (signed char)q;
   }
 }
 
@@ -104,10 +115,14 @@ __host__ __device__ inline double rows_scale(double amax)
 // ------------------------------------------------------------------------
 // k_rows_prep: list entries [0, num) (d_num: device count); warp scratch:
 // the staged positions and modified drift (2 x 3N, read by the proposal),
-// then, in the same space, chi [5][K]; the exponential slots after both.
+// then, in the same space, the exponential slots.  The basis rows stay in
+// registers: lane l evaluates the four consecutive functions 4 l .. 4 l + 3
+// of every 128 (the eight lanes of a 32-function K block are one shuffle
+// group for its scale), so no [5][K] row array occupies shared memory.
 __host__ __device__ inline int rows_prep_doubles(int N, int K, int nslot)
 {
-  return max(2 * even(3 * N), even(5 * K)) + even(nslot);
+  (void)K;
+  return max(2 * even(3 * N), even(nslot));
 }
 
 template <bool kMetropolis, bool kExtras>
@@ -122,7 +137,7 @@ __global__ void __launch_bounds__(128) k_rows_prep(DevSys S, Layout L, RunCfg cf
   if (wi >= nw) return;
   const int N = S.N, K = S.K, e = mv.e;
   double *sm = smem + (size_t)warp * rows_prep_doubles(N, K, S.nslot);
-  double *sR = sm, *smg = sm + even(3 * N), *chi = sm, *ex = sm + max(2 * even(3 * N), even(5 * K));
+  double *sR = sm, *smg = sm + even(3 * N), *ex = sm;
   const int slot = slots ? slots[wi] : wi;
   const double *blk = state + (size_t)slot * L.stride;
   for (int t = lane; t < 3 * N; t += 32) {
@@ -133,27 +148,35 @@ __global__ void __launch_bounds__(128) k_rows_prep(DevSys S, Layout L, RunCfg cf
   const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
   double rn[3], g_fwd, u_acc;
   propose_move<kMetropolis, kExtras>(S, cfg, slot, mv.step, e, N, sR, ro, smg, R_in, wi, rn, g_fwd, u_acc, mv.rin_moved);
-  __syncwarp();  // chi overwrites the staged arrays
-  basis_slots_warp(S, rn, chi, K, ex);
+  __syncwarp();  // the slots overwrite the staged arrays
+  basis_slot_exps_warp(S, rn, ex);
   __syncwarp();
-  // rows 5 wi .. 5 wi + 4 of the GEMM: tile, row in tile; every K step (32
-  // functions, covered by 8 lanes with 4 functions each) has its own scale
+  // rows 5 wi .. 5 wi + 4 of the GEMM
+  const int row0 = 5 * wi, tile = row0 / (5 * kTileWalkers), r0 = row0 - tile * 5 * kTileWalkers;
   const unsigned gmask = 0xFFu << (8 * (lane >> 3));
-  for (int d = 0; d < 5; d++) {
-    const int row = 5 * wi + d, tile = row / (5 * kTileWalkers), r = row - tile * 5 * kTileWalkers;
-    for (int k0 = 4 * lane; k0 < ksteps * kKStep; k0 += 128) {
-      double x[4], m = 0.0;
+  for (int k0 = 4 * lane; k0 < ksteps * kKStep; k0 += 128) {
+    double v[4][5];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        x[u] = k0 + u < K ? chi[d * K + k0 + u] : 0.0;
-        m = fmax(m, fabs(x[u]));
+    for (int u = 0; u < 4; u++) {
+      if (k0 + u < K) {
+        basis_function_rows(S, rn, k0 + u, ex, v[u]);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 5; d++) v[u][d] = 0.0;
       }
+    }
+    const int kk = k0 / kKStep;
+#pragma unroll
+    for (int d = 0; d < 5; d++) {
+      // the K block's scale of row d: the largest of the eight lanes' values
+      double m = fmax(fmax(fabs(v[0][d]), fabs(v[1][d])), fmax(fabs(v[2][d]), fabs(v[3][d])));
       m = fmax(m, __shfl_xor_sync(gmask, m, 4));
       m = fmax(m, __shfl_xor_sync(gmask, m, 2));
       m = fmax(m, __shfl_xor_sync(gmask, m, 1));
       const double scale = rows_scale(m), inv = 1.0 / scale;  // exact: a power of two
-      const int kk = k0 / kKStep;
-      if ((lane & 7) == 0) rscale[(size_t)row * ksteps + kk] = scale;
+      // a walker's five rows lie in one tile (25 walkers = 125 rows)
+      const int r = r0 + d;
+      if ((lane & 7) == 0) rscale[(size_t)(row0 + d) * ksteps + kk] = scale;
       // four consecutive k per lane: one 4-byte store per digit plane
       uint32_t w[kSlices];
 #pragma unroll
@@ -161,7 +184,7 @@ __global__ void __launch_bounds__(128) k_rows_prep(DevSys S, Layout L, RunCfg cf
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         signed char dg[kSlices];
-        rows_digits(x[u] * inv, dg);
+        rows_digits(v[u][d] * inv, dg);
 #pragma unroll
         for (int s = 0; s < kSlices; s++) w[s] |= (uint32_t)(unsigned char)dg[s] << (8 * u);
       }
@@ -256,10 +279,13 @@ __device__ __forceinline__ bool mbar_wait_or_abort(uint32_t mbar, uint32_t parit
 }
 
 // ------------------------------------------------------------------------
-// k_rows_mma: grid (tiles, orbital tiles), 128 threads.  A: [tile][kstep]
-// [slice] blocks of kABlock bytes; B: [orbital tile][kstep][slice] blocks of
-// kBBlock bytes (the spin's MO coefficients, digits made at set-up);
-// rscale [rows][ksteps], cscale [orbital tiles][ksteps][kNTile]: every
+// k_rows_mma: one CTA per (tile, orbital tile), the orbital tiles of a tile
+// adjacent in the 1-D grid (they read the same A blocks, once from HBM and
+// then from L2), kRowsThreads threads.  A: [tile][kstep][slice] blocks of
+// kABlock bytes; B: [orbital tile][kstep][slice] blocks of kBBlock bytes (the
+// spin's MO coefficients, digits made at set-up); rscale [rows][ksteps]
+// (one walker's scales contiguous for the prep kernel's stores), cscale
+// [orbital tiles][ksteps][kNTile]: every
 // 32-function block of K has its own power-of-two scale on both sides, so
 // the digits keep 56 bits relative to the block's largest values and the
 // rows carry the error of an FP64 dot product of 32-term blocks.  rows
@@ -268,29 +294,31 @@ __device__ __forceinline__ bool mbar_wait_or_abort(uint32_t mbar, uint32_t parit
 //
 // Per K step, thread 0 issues the kSlices (kSlices + 1) / 2 digit-pair MMAs
 // into one of two TMEM buffers (the K step's parity) and commits them; the
-// four warps drain the other buffer meanwhile: the eight int32 accumulators
+// eight warps drain the other buffer meanwhile (warps w and w + 4 read TMEM
+// lanes 32 (w mod 4) .. + 31, columns 16 (w / 4) .. + 15 of every
+// accumulator): the eight int32 accumulators
 // of a K step are below 2^20 in magnitude (32 products of digits <= 2^6 in
 // magnitude, at most 8 pairs), so neighbouring accumulators combine exactly
 // in int32 (a_t 2^7 + a_{t+1} < 2^28) and four exact FP64 conversions give
 // the K step's scaled sum, which is added to the FP64 result in registers.
-__global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restrict__ A,
-                                                     const signed char *__restrict__ B,
-                                                     const double *__restrict__ rscale,
-                                                     const double *__restrict__ cscale, int n, int ksteps,
-                                                     int num, const int *d_num, double *__restrict__ rows,
-                                                     int *err)
+__global__ void __launch_bounds__(kRowsThreads, 1) k_rows_mma(const signed char *__restrict__ A,
+                                                              const signed char *__restrict__ B,
+                                                              const double *__restrict__ rscale,
+                                                              const double *__restrict__ cscale, int n, int ntiles,
+                                                              int ksteps, int num, const int *d_num,
+                                                              double *__restrict__ rows, int *err)
 {
   static_assert(kSlices == 8, "the drain combines accumulators in four pairs");
   extern __shared__ __align__(1024) unsigned char rsm[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nw = d_num ? *d_num : num;
-  const int tile = blockIdx.x, ntile = blockIdx.y;
+  const int tile = blockIdx.x / ntiles, ntile = blockIdx.x - tile * ntiles;
   if (tile * kTileWalkers >= nw) return;  // whole CTA: before any TMEM or barrier use
   unsigned char *stage0 = rsm;
   // full[s]: the stage's operands landed (bulk copies, transaction bytes);
   // empty[s]: the MMAs that read the stage completed (tcgen05.commit);
   // done[b]: the MMAs of TMEM buffer b completed (tcgen05.commit);
-  // drained[b]: the 128 threads read buffer b (one arrival each)
+  // drained[b]: the kRowsThreads threads read buffer b (one arrival each)
   uint64_t *full = (uint64_t *)(rsm + kRowsStages * kRowsStageBytes);
   uint64_t *empty = full + kRowsStages;
   uint64_t *done = empty + kRowsStages;
@@ -310,7 +338,7 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
     }
     for (int b = 0; b < 2; b++) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(done + b)));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(smem_u32(drained + b)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(drained + b)), "r"(kRowsThreads));
     }
     *s_abort = 0;
     *s_last = -1;
@@ -344,45 +372,57 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
   if (tid == 0)
     for (; loaded < kRowsStages && loaded < ksteps; loaded++) load(loaded);
 
-  // the FP64 result of this thread's row (TMEM lane) and the CTA's orbitals
-  const int r = 32 * warp + lane;
+  // the FP64 result of this thread's row (TMEM lane) and its half of the
+  // CTA's orbitals
+  const int quarter = warp & 3, half = warp >> 2;
+  const int r = 32 * quarter + lane;
   const int row = tile * 5 * kTileWalkers + r;
   const bool live = r < 5 * kTileWalkers && row < 5 * nw;
-  double out[kNTile];
+  double out[16];
 #pragma unroll
-  for (int q = 0; q < kNTile; q++) out[q] = 0.0;
-  const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+  for (int q = 0; q < 16; q++) out[q] = 0.0;
+  const uint32_t lane_base = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(16 * half);
 
   // drain K step kk from buffer kk & 1; false when a wait gave up
   auto drain = [&](int kk) -> bool {
     const int b = kk & 1;
+    // the scales first: their loads overlap the wait for the MMAs
+    const double rs = live ? rscale[(size_t)row * ksteps + kk] : 0.0;
+    const double *csp = cscale + ((size_t)ntile * ksteps + kk) * kNTile + 16 * half;
+    double cs[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) cs[q] = csp[q];
     // warp-uniform: tcgen05.ld is .sync.aligned
     if (!__all_sync(0xFFFFFFFFu, mbar_wait_or_abort(smem_u32(done + b), (uint32_t)((kk >> 1) & 1), s_abort)))
       return false;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    const double rs = live ? rscale[(size_t)row * ksteps + kk] : 0.0;
-    const double *cs = cscale + ((size_t)ntile * ksteps + kk) * kNTile;
+    double part[16];
 #pragma unroll
-    for (int c = 0; c < kNTile / 16; c++) {
-      double part[16];
+    for (int q = 0; q < 16; q++) part[q] = 0.0;
+    // two pairs of accumulators per wait: pair p holds weights
+    // 2^-(12 + 14 p) (accumulator 2p) and 2^-(19 + 14 p) (accumulator
+    // 2p + 1), so a_2p 2^7 + a_2p+1 (below 2^28) carries 2^-(19 + 14 p); it
+    // becomes a double exactly as (2^52 + 2^31 + v) - (2^52 + 2^31), the
+    // first term assembled from its bits (one FP64 add, no conversion)
 #pragma unroll
-      for (int q = 0; q < 16; q++) part[q] = 0.0;
+    for (int pp = 0; pp < kSlices / 2; pp += 2) {
+      uint32_t v[4][16];
 #pragma unroll
-      for (int p = 0; p < kSlices / 2; p++) {
-        uint32_t v0[16], v1[16];
-        const uint32_t col = (uint32_t)(b * kAccCols + 2 * p * kNTile + 16 * c);
-        tmem_ld16(lane_base + col, v0);
-        tmem_ld16(lane_base + col + kNTile, v1);
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-        // pair p holds weights 2^-(12 + 14 p) (accumulator 2p) and
-        // 2^-(19 + 14 p) (accumulator 2p + 1): a_2p 2^7 + a_2p+1 at 2^-(19 + 14 p)
-        const double w = ldexp(1.0, -19 - 14 * p);
+      for (int u = 0; u < 4; u++) tmem_ld16(lane_base + (uint32_t)(b * kAccCols + (2 * pp + u) * kNTile), v[u]);
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-        for (int q = 0; q < 16; q++) part[q] = fma((double)((int)v0[q] * 128 + (int)v1[q]), w, part[q]);
+      for (int u = 0; u < 2; u++) {
+        const double w = ldexp(1.0, -19 - 14 * (pp + u));
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+          const int c = (int)v[2 * u][q] * 128 + (int)v[2 * u + 1][q];
+          const double x = __hiloint2double(0x43300000, c ^ (int)0x80000000) - 4503601774854144.0;
+          part[q] = fma(x, w, part[q]);
+        }
       }
-#pragma unroll
-      for (int q = 0; q < 16; q++) out[16 * c + q] = fma(part[q], rs * cs[16 * c + q], out[16 * c + q]);
     }
+#pragma unroll
+    for (int q = 0; q < 16; q++) out[q] = fma(part[q], rs * cs[q], out[q]);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(drained + b)) : "memory");
     return true;
@@ -441,9 +481,9 @@ __global__ void __launch_bounds__(128, 1) k_rows_mma(const signed char *__restri
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kRowsTmemCols));
   if (okall && live) {
-    const int o0 = ntile * kNTile;
+    const int o0 = ntile * kNTile + 16 * half;
 #pragma unroll
-    for (int q = 0; q < kNTile; q++)
+    for (int q = 0; q < 16; q++)
       if (o0 + q < n) rows[(size_t)row * n + o0 + q] = out[q];
   }
 }

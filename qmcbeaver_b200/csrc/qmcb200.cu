@@ -431,9 +431,12 @@ static void launch_move(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &
     }
     {
       ProfScope ps(h, QMCB_KERNEL_ROWS_MMA, st);
-      const dim3 g((cap + kTileWalkers - 1) / kTileWalkers, (n + kNTile - 1) / kNTile);
-      k_rows_mma<<<g, 128, kRowsSmem, st>>>(h->d_rows_A, h->d_rows_B[sp], h->d_rows_rs, h->d_rows_cs[sp], n,
-                                            h->rows_ksteps, num, d_num, h->d_rows_out, h->d_ctl + 3);
+      // the orbital tiles of a tile adjacent in the grid (A read once from HBM)
+      const int ntiles = (n + kNTile - 1) / kNTile;
+      const unsigned g = (unsigned)((cap + kTileWalkers - 1) / kTileWalkers) * (unsigned)ntiles;
+      k_rows_mma<<<g, kRowsThreads, kRowsSmem, st>>>(h->d_rows_A, h->d_rows_B[sp], h->d_rows_rs, h->d_rows_cs[sp],
+                                                     n, ntiles, h->rows_ksteps, num, d_num, h->d_rows_out,
+                                                     h->d_ctl + 3);
       ps.end(st);
     }
     mv.rows = h->d_rows_out;
@@ -557,7 +560,7 @@ static int rows_setup(qmcb_handle *h)
   // on the handle's stream (non-blocking: a legacy-stream memset would not
   // be ordered with its work)
   CKR(cudaMemsetAsync(h->d_rows_A, 0, abytes, h->stream));  // rows 125 .. 127 of every tile stay zero
-  CKR(cudaMalloc(&h->d_rows_rs, sizeof(double) * tiles * 5 * kTileWalkers * ks));
+  CKR(cudaMalloc(&h->d_rows_rs, sizeof(double) * tiles * kTileRows * ks));  // [row][K step], 128 rows a tile
   CKR(cudaMalloc(&h->d_rows_out, sizeof(double) * (size_t)h->max_walkers * 5 * h->nmax));
   // a wait inside the contraction kernel that gave up sets ctl[3], which
   // returns with every batch's live count
