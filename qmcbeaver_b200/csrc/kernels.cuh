@@ -1207,14 +1207,14 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
     if (c == el) continue;
     TI val = (TI)0;
     if (kGInv) {
-      // HBM / L2 operands: four loads in flight before their FMAs
+      // HBM / L2 operands: eight loads in flight before their FMAs
       int l = 0;
-      for (; l + 4 <= n; l += 4) {
-        TI v[4];
+      for (; l + 8 <= n; l += 8) {
+        TI v[8];
 #pragma unroll
-        for (int u = 0; u < 4; u++) v[u] = InvO[(l + u) * n + c];
+        for (int u = 0; u < 8; u++) v[u] = InvO[(l + u) * n + c];
 #pragma unroll
-        for (int u = 0; u < 4; u++) val = fma((TI)Dn[l + u], v[u], val);
+        for (int u = 0; u < 8; u++) val = fma((TI)Dn[l + u], v[u], val);
       }
       for (; l < n; l++) val = fma((TI)Dn[l], InvO[l * n + c], val);
     } else {
@@ -1223,26 +1223,70 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
     valc[c] = (TI)(val * q);
   }
   __syncwarp();
+  double lp = 0.0;
   if (kGInv) {
     // the same element formulas as the in-place update, old copy -> new
-    // copy, four rows' loads in flight at a time
+    // copy, fused with the ratio sums of the moved spin
+    // (QMcBeaver/src/QMCSlater.cpp:741-762): lane = electron column c, the
+    // new inverse elements feed the sums as they are made (never read back)
+    // and the walker's derivative rows stream from HBM alongside, six
+    // orbitals' loads (36) in flight at a time, evict-first
+    constexpr int kB = 6;
     for (int c = lane; c < n; c += 32) {
       const TI vc = c == el ? (TI)0 : valc[c];
+      double gx = 0, gy = 0, gz = 0, ll = 0;
       int r = 0;
-      for (; r + 4 <= n; r += 4) {
-        TI ie[4], x[4];
+      for (; r + kB <= n; r += kB) {
+        TI ie[kB], x[kB];
+        TS g0[kB], g1[kB], g2[kB], gl[kB];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < kB; u++) {
           ie[u] = InvO[(r + u) * n + el];
           x[u] = InvO[(r + u) * n + c];
+          if (c == el) {
+            g0[u] = Dn[n + r + u];
+            g1[u] = Dn[2 * n + r + u];
+            g2[u] = Dn[3 * n + r + u];
+            gl[u] = Dn[4 * n + r + u];
+          } else {
+            g0[u] = __ldcs(&DgT[(0 * n + r + u) * n + c]);
+            g1[u] = __ldcs(&DgT[(1 * n + r + u) * n + c]);
+            g2[u] = __ldcs(&DgT[(2 * n + r + u) * n + c]);
+            gl[u] = __ldcs(&DlT[(r + u) * n + c]);
+          }
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) Inv[(r + u) * n + c] = c == el ? (TI)(ie[u] * q) : x[u] - vc * ie[u];
+        for (int u = 0; u < kB; u++) {
+          const TI nv = c == el ? (TI)(ie[u] * q) : x[u] - vc * ie[u];
+          Inv[(r + u) * n + c] = nv;
+          const double iv = (double)nv;
+          gx = fma((double)g0[u], iv, gx);
+          gy = fma((double)g1[u], iv, gy);
+          gz = fma((double)g2[u], iv, gz);
+          ll = fma((double)gl[u], iv, ll);
+        }
       }
       for (; r < n; r++) {
         const TI ie = InvO[r * n + el];
-        Inv[r * n + c] = c == el ? (TI)(ie * q) : InvO[r * n + c] - vc * ie;
+        const TI nv = c == el ? (TI)(ie * q) : InvO[r * n + c] - vc * ie;
+        Inv[r * n + c] = nv;
+        const double iv = (double)nv;
+        if (c == el) {
+          gx = fma((double)Dn[n + r], iv, gx);
+          gy = fma((double)Dn[2 * n + r], iv, gy);
+          gz = fma((double)Dn[3 * n + r], iv, gz);
+          ll = fma((double)Dn[4 * n + r], iv, ll);
+        } else {
+          gx = fma((double)__ldcs(&DgT[(0 * n + r) * n + c]), iv, gx);
+          gy = fma((double)__ldcs(&DgT[(1 * n + r) * n + c]), iv, gy);
+          gz = fma((double)__ldcs(&DgT[(2 * n + r) * n + c]), iv, gz);
+          ll = fma((double)__ldcs(&DlT[r * n + c]), iv, ll);
+        }
       }
+      lp += ll;
+      gD[3 * (base + c)] = gx;
+      gD[3 * (base + c) + 1] = gy;
+      gD[3 * (base + c) + 2] = gz;
     }
   } else if (n <= 32) {
     const int rpp = 32 / n, r0 = lane / n, c = lane - r0 * n;
@@ -1263,9 +1307,9 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   __syncwarp();
 
   // ---- ratio sums of the moved spin (QMcBeaver/src/QMCSlater.cpp:741-762)
-  //      lanes = (orbital slice, electron) for n <= 16
-  double lp = 0.0;
-  {
+  //      lanes = (orbital slice, electron) for n <= 16 (the inverse in HBM:
+  //      fused with its update above)
+  if (!kGInv) {
     const int S2 = n <= 32 ? 32 / n : 1;
     const int s2 = n <= 32 ? lane / n : 0;
     const int oa = n <= 32 ? (n * s2) / S2 : 0, ob = n <= 32 ? (n * (s2 + 1)) / S2 : n;
@@ -1443,7 +1487,7 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
 }
 
 template <bool kMetropolis, typename TS, typename TI, bool kExtras, bool kGInv>
-__global__ void __launch_bounds__(128, 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
+__global__ void __launch_bounds__(128, kGInv ? 3 : 5) k_move(DevSys S, Layout L, RunCfg cfg, double *state, const int *slots,
                                               int num, const int *d_num, const double *R_in, MoveArgs mv,
                                               const EnergyCtl *ectl, double *stats, EvalOut out)
 {

@@ -63,7 +63,7 @@ __device__ __forceinline__ int group_find(const int *prefix, int nm, int i)
 // zero at launch.
 // kMD: the members have several determinants (md_move_walker).
 template <bool kExtras, bool kGInv, bool kConst, bool kMD>
-__global__ void __launch_bounds__(128, kMD ? 3 : 5) k_move_group(const GroupMember *__restrict__ gm, int nm, int t,
+__global__ void __launch_bounds__(128, (kMD || kGInv) ? 3 : 5) k_move_group(const GroupMember *__restrict__ gm, int nm, int t,
                                                               int stride, int *counter, int cbase)
 {
   extern __shared__ double smem[];
