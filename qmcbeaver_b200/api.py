@@ -103,7 +103,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
 
 
 def _ptr(a: Optional[np.ndarray]):
-    return None if a is None else a.ctypes.data_as(C.c_void_p)
+    # the address as an int: ctypes.data_as builds a pointer object per call
+    # (microseconds each, a tenth of a single-electron evaluate at 4,096
+    # walkers); the caller keeps the array alive across the call
+    return None if a is None else a.ctypes.data
 
 
 class QMCB200Functions:

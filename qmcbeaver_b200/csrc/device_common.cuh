@@ -51,6 +51,7 @@ enum Sc {
 constexpr int kScalars = 24;  // padded
 
 constexpr int kShellPrim = 6;  // primitives kept in registers per shell
+constexpr int kFnPrim = 3;      // primitives per function in the fixed-count loop of basis_function_rows
 constexpr int kTbMax = 8;      // largest NeN / Nee of a three-body function
 
 struct DevSys {
@@ -570,6 +571,24 @@ __device__ __forceinline__ double ipow(double x, int a)
   return r;
 }
 
+// x^a, x^(a-1), x^(a-2) (1 for negative powers) with the products of ipow
+// in its order (x, x*x, (x*x)*x, ...), picked by selects for a <= 4 so that
+// the lanes of a warp run one instruction stream whatever their functions'
+// powers; larger powers take the loop.
+__device__ __forceinline__ void ipow3(double x, int a, double &pa, double &pa1, double &pa2)
+{
+  if (a > 4) {
+    pa = ipow(x, a);
+    pa1 = ipow(x, a - 1);
+    pa2 = ipow(x, a - 2);
+    return;
+  }
+  const double p2 = x * x, p3 = p2 * x, p4 = p3 * x;
+  pa = a == 0 ? 1.0 : a == 1 ? x : a == 2 ? p2 : a == 3 ? p3 : p4;
+  pa1 = a <= 1 ? 1.0 : a == 2 ? x : a == 3 ? p2 : p3;
+  pa2 = a <= 2 ? 1.0 : a == 3 ? x : p2;
+}
+
 __device__ __forceinline__ float ipowf(float x, int a)
 {
   float r = 1.0f;
@@ -691,22 +710,40 @@ __device__ __forceinline__ void basis_function_rows(const DevSys &S, const doubl
   const int a = f.x & 0xff, b = (f.x >> 8) & 0xff, c = (f.x >> 16) & 0xff;
   const double Lf = 4.0 * fq.w + 6.0, r2x4 = 4.0 * r2;
   double E0 = 0.0, E1 = 0.0, El = 0.0;
-  for (int i = 0; i < fq.z; i++) {
-    const double al = __ldg(&S.pexp[f.y + i]);
-    const double e = __ldg(&S.pcoef[f.y + i]) * ex[fq.y + i];
-    E0 += e;
-    E1 = fma(e, al, E1);
-    El = fma(e, al * fma(r2x4, al, -Lf), El);
+  if (fq.z <= kFnPrim) {
+    // fixed trip count (predicated): no data-dependent loop branch, the
+    // loads of all primitives in flight together
+#pragma unroll
+    for (int i = 0; i < kFnPrim; i++) {
+      if (i < fq.z) {
+        const double al = __ldg(&S.pexp[f.y + i]);
+        const double e = __ldg(&S.pcoef[f.y + i]) * ex[fq.y + i];
+        E0 += e;
+        E1 = fma(e, al, E1);
+        El = fma(e, al * fma(r2x4, al, -Lf), El);
+      }
+    }
+  } else {
+    for (int i = 0; i < fq.z; i++) {
+      const double al = __ldg(&S.pexp[f.y + i]);
+      const double e = __ldg(&S.pcoef[f.y + i]) * ex[fq.y + i];
+      E0 += e;
+      E1 = fma(e, al, E1);
+      El = fma(e, al * fma(r2x4, al, -Lf), El);
+    }
   }
-  const double xa = ipow(x, a), yb = ipow(y, b), zc = ipow(z, c);
+  double xa, xa1, xa2, yb, yb1, yb2, zc, zc1, zc2;
+  ipow3(x, a, xa, xa1, xa2);
+  ipow3(y, b, yb, yb1, yb2);
+  ipow3(z, c, zc, zc1, zc2);
   const double P = xa * yb * zc;
-  const double Px = a ? a * ipow(x, a - 1) * yb * zc : 0.0;
-  const double Py = b ? b * xa * ipow(y, b - 1) * zc : 0.0;
-  const double Pz = c ? c * xa * yb * ipow(z, c - 1) : 0.0;
+  const double Px = a ? a * xa1 * yb * zc : 0.0;
+  const double Py = b ? b * xa * yb1 * zc : 0.0;
+  const double Pz = c ? c * xa * yb * zc1 : 0.0;
   double Pl = 0.0;
-  if (a > 1) Pl += a * (a - 1.0) * ipow(x, a - 2) * yb * zc;
-  if (b > 1) Pl += b * (b - 1.0) * xa * ipow(y, b - 2) * zc;
-  if (c > 1) Pl += c * (c - 1.0) * xa * yb * ipow(z, c - 2);
+  if (a > 1) Pl += a * (a - 1.0) * xa2 * yb * zc;
+  if (b > 1) Pl += b * (b - 1.0) * xa * yb2 * zc;
+  if (c > 1) Pl += c * (c - 1.0) * xa * yb * zc2;
   const double PE1 = P * E1;
   v[0] = E0 * P;
   v[1] = fma(E0, Px, -2.0 * x * PE1);

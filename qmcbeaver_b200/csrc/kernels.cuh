@@ -1773,4 +1773,32 @@ __global__ void k_set_weights(double *state, Layout L, const int *live, int n, c
     state[(size_t)live[i] * L.stride + L.sc + SC_WEIGHT] = w[i];
 }
 
+// Per-walker evaluate outputs moved from the device buffer into mapped
+// page-locked host arrays with consecutive threads on consecutive elements,
+// so the stores cross the bus as full packets (the evaluate kernels store a
+// walker's scalars from one lane, one 8-byte packet each).  Segment
+// blockIdx.y: bytes[y] bytes from src[y] to dst[y]; whole 8-byte words when
+// both ends and the length allow it, bytes otherwise.
+struct PutList {
+  const void *src[8];
+  void *dst[8];
+  size_t bytes[8];
+};
+
+__global__ void k_put_outputs(PutList P)
+{
+  const int y = blockIdx.y;
+  const size_t n = P.bytes[y];
+  const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, di = (size_t)gridDim.x * blockDim.x;
+  if (((uintptr_t)P.src[y] | (uintptr_t)P.dst[y] | n) % 8 == 0) {
+    const unsigned long long *s = (const unsigned long long *)P.src[y];
+    unsigned long long *d = (unsigned long long *)P.dst[y];
+    for (size_t i = i0; i < n / 8; i += di) d[i] = s[i];
+  } else {
+    const unsigned char *s = (const unsigned char *)P.src[y];
+    unsigned char *d = (unsigned char *)P.dst[y];
+    for (size_t i = i0; i < n; i += di) d[i] = s[i];
+  }
+}
+
 }  // namespace qmcb

@@ -1237,6 +1237,95 @@ static void launch_full(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &
   }
 }
 
+// Device address of a host array that kernels can store into directly:
+// page-locked memory mapped into the device's address space (every
+// cudaMallocHost / cudaHostAlloc allocation under unified addressing, and
+// cudaHostRegister'd ranges that are mapped); null for pageable memory.
+static void *mapped_device_ptr(void *p)
+{
+  if (!p) return nullptr;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // not a pointer the runtime knows: pageable
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
+// Destinations of the evaluate outputs.  The per-electron arrays (grad,
+// mod_grad) go straight into the caller's array when that array is
+// page-locked and mapped: the kernel's stores of a walker's 3N values cross
+// the bus while it runs.  The per-walker values (psi, sign, lap, E_L,
+// potentials, status) always go to the handle's device buffer first; after
+// the kernel, one k_put_outputs launch moves the ones whose host arrays are
+// mapped in full packets, and one copy each brings back the rest (pageable
+// arrays).  Outputs not selected are not written at all.
+struct EvalDst {
+  void *host[8], *dev[8], *kernel[8];
+  size_t bytes[8];
+  bool mapped[8];
+};
+
+static EvalOut eval_destinations(qmcb_handle *h, int num, unsigned mask, double *log_abs_psi, double *sign,
+                                 double *grad, double *mod_grad, double *lap, double *e_local, double *pe,
+                                 unsigned char *status, EvalDst &d)
+{
+  const size_t N = h->N;
+  double *o_lp = h->d_out, *o_sg = o_lp + num, *o_lap = o_sg + num, *o_el = o_lap + num, *o_pe = o_el + num;
+  double *o_g = o_pe + 3 * (size_t)num, *o_mg = o_g + 3 * N * num;
+  const unsigned bit[8] = {QMCB_OUT_PSI, QMCB_OUT_PSI, QMCB_OUT_GRAD, QMCB_OUT_MOD_GRAD,
+                           QMCB_OUT_LAP, QMCB_OUT_E_LOCAL, QMCB_OUT_PE, QMCB_OUT_STATUS};
+  void *host[8] = {log_abs_psi, sign, grad, mod_grad, lap, e_local, pe, status};
+  void *dev[8] = {o_lp, o_sg, o_g, o_mg, o_lap, o_el, o_pe, h->d_status};
+  const size_t bytes[8] = {sizeof(double) * num, sizeof(double) * num, sizeof(double) * 3 * N * num,
+                           sizeof(double) * 3 * N * num, sizeof(double) * num, sizeof(double) * num,
+                           sizeof(double) * 3 * num, (size_t)num};
+  for (int i = 0; i < 8; i++) {
+    d.host[i] = host[i];
+    d.dev[i] = dev[i];
+    d.bytes[i] = bytes[i];
+    d.kernel[i] = nullptr;
+    d.mapped[i] = false;
+    if ((mask & bit[i]) && host[i]) {
+      void *m = mapped_device_ptr(host[i]);
+      d.mapped[i] = m != nullptr;
+      if (m) d.host[i] = m;
+      const bool per_electron = i == 2 || i == 3;
+      d.kernel[i] = (m && per_electron) ? m : dev[i];
+    }
+  }
+  return EvalOut{(double *)d.kernel[0], (double *)d.kernel[1], (double *)d.kernel[2], (double *)d.kernel[3],
+                 (double *)d.kernel[4], (double *)d.kernel[5], (double *)d.kernel[6], (unsigned char *)d.kernel[7]};
+}
+
+// After the kernel (enqueued on st): the mapped per-walker outputs by one
+// k_put_outputs launch, the pageable ones by one copy each.
+static cudaError_t eval_deliver(const EvalDst &d, cudaStream_t st)
+{
+  PutList P{};
+  int nput = 0;
+  size_t most = 0;
+  for (int i = 0; i < 8; i++) {
+    if (!d.kernel[i] || d.kernel[i] != d.dev[i]) continue;  // not selected, or stored by the kernel
+    if (d.mapped[i]) {
+      P.src[nput] = d.dev[i];
+      P.dst[nput] = d.host[i];
+      P.bytes[nput] = d.bytes[i];
+      most = std::max(most, d.bytes[i]);
+      nput++;
+    } else {
+      const cudaError_t e = cudaMemcpyAsync(d.host[i], d.dev[i], d.bytes[i], cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (nput > 0) {
+    const int blocks = (int)std::min<size_t>((most / 8 + 255) / 256, 64);
+    k_put_outputs<<<dim3(std::max(blocks, 1), nput), 256, 0, st>>>(P);
+    return cudaGetLastError();
+  }
+  return cudaSuccess;
+}
+
 static int launch_eval(qmcb_handle *h, int which_e, const int *d_slots, int num, const double *d_R, EvalOut o,
                        cudaStream_t st, int rin_moved = 0)
 {
@@ -1306,22 +1395,14 @@ int qmcb_evaluate(qmcb_handle *h, int which_e, const int *slots, int num, const 
   cudaStream_t st = h->stream;
   CK(cudaMemcpyAsync(h->d_slots, slots, sizeof(int) * num, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(h->d_R, R, sizeof(double) * (size_t)num * 3 * N, cudaMemcpyHostToDevice, st));
-  double *base = h->d_out;
-  double *o_lp = base, *o_sg = o_lp + num, *o_lap = o_sg + num, *o_el = o_lap + num, *o_pe = o_el + num;
-  double *o_g = o_pe + 3 * (size_t)num, *o_mg = o_g + 3 * (size_t)N * num;
-  EvalOut o{o_lp, o_sg, o_g, o_mg, o_lap, o_el, o_pe, h->d_status};
+  // every non-NULL output is returned
+  EvalDst dst;
+  const EvalOut o = eval_destinations(h, num, QMCB_OUT_ALL, log_abs_psi, sign, grad, mod_grad, lap, e_local, pe,
+                                      status, dst);
   int rc = launch_eval(h, which_e, h->d_slots, num, h->d_R, o, st);
   if (rc) return rc;
   if (which_e < 0) h->evaluated_once = true;
-  if (log_abs_psi) CK(cudaMemcpyAsync(log_abs_psi, o_lp, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
-  if (sign) CK(cudaMemcpyAsync(sign, o_sg, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
-  if (lap) CK(cudaMemcpyAsync(lap, o_lap, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
-  if (e_local) CK(cudaMemcpyAsync(e_local, o_el, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
-  if (pe) CK(cudaMemcpyAsync(pe, o_pe, sizeof(double) * 3 * num, cudaMemcpyDeviceToHost, st));
-  if (grad) CK(cudaMemcpyAsync(grad, o_g, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
-  if (mod_grad)
-    CK(cudaMemcpyAsync(mod_grad, o_mg, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
-  if (status) CK(cudaMemcpyAsync(status, h->d_status, num, cudaMemcpyDeviceToHost, st));
+  CK(eval_deliver(dst, st));
   int rows_err = 0;
   if (h->params.precision == QMCB_PREC_INT8_SLICES && which_e >= 0)
     CK(cudaMemcpyAsync(&rows_err, h->d_ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1347,32 +1428,15 @@ int qmcb_evaluate_moved(qmcb_handle *h, int which_e, const int *slots, int num, 
       ((out_mask & QMCB_OUT_STATUS) && !status))
     return fail(h, QMCB_E_ARG, "qmcb_evaluate_moved: an output selected in out_mask is NULL");
   if (num == 0) return QMCB_OK;
-  const int N = h->N;
   cudaStream_t st = h->stream;
   CK(cudaMemcpyAsync(h->d_slots, slots, sizeof(int) * num, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(h->d_R, r_moved, sizeof(double) * 3 * (size_t)num, cudaMemcpyHostToDevice, st));
-  double *base = h->d_out;
-  double *o_lp = base, *o_sg = o_lp + num, *o_lap = o_sg + num, *o_el = o_lap + num, *o_pe = o_el + num;
-  double *o_g = o_pe + 3 * (size_t)num, *o_mg = o_g + 3 * (size_t)N * num;
-  // outputs not asked for are not written by the kernel either
-  EvalOut o{(out_mask & QMCB_OUT_PSI) ? o_lp : nullptr, (out_mask & QMCB_OUT_PSI) ? o_sg : nullptr,
-            (out_mask & QMCB_OUT_GRAD) ? o_g : nullptr, (out_mask & QMCB_OUT_MOD_GRAD) ? o_mg : nullptr,
-            (out_mask & QMCB_OUT_LAP) ? o_lap : nullptr, (out_mask & QMCB_OUT_E_LOCAL) ? o_el : nullptr,
-            (out_mask & QMCB_OUT_PE) ? o_pe : nullptr, (out_mask & QMCB_OUT_STATUS) ? h->d_status : nullptr};
+  EvalDst dst;
+  const EvalOut o = eval_destinations(h, num, out_mask, log_abs_psi, sign, grad, mod_grad, lap, e_local, pe,
+                                      status, dst);
   int rc = launch_eval(h, which_e, h->d_slots, num, h->d_R, o, st, 1);
   if (rc) return rc;
-  if (out_mask & QMCB_OUT_PSI) {
-    CK(cudaMemcpyAsync(log_abs_psi, o_lp, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(sign, o_sg, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
-  }
-  if (out_mask & QMCB_OUT_LAP) CK(cudaMemcpyAsync(lap, o_lap, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
-  if (out_mask & QMCB_OUT_E_LOCAL) CK(cudaMemcpyAsync(e_local, o_el, sizeof(double) * num, cudaMemcpyDeviceToHost, st));
-  if (out_mask & QMCB_OUT_PE) CK(cudaMemcpyAsync(pe, o_pe, sizeof(double) * 3 * num, cudaMemcpyDeviceToHost, st));
-  if (out_mask & QMCB_OUT_GRAD)
-    CK(cudaMemcpyAsync(grad, o_g, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
-  if (out_mask & QMCB_OUT_MOD_GRAD)
-    CK(cudaMemcpyAsync(mod_grad, o_mg, sizeof(double) * 3 * (size_t)N * num, cudaMemcpyDeviceToHost, st));
-  if (out_mask & QMCB_OUT_STATUS) CK(cudaMemcpyAsync(status, h->d_status, num, cudaMemcpyDeviceToHost, st));
+  CK(eval_deliver(dst, st));
   int rows_err = 0;
   if (h->params.precision == QMCB_PREC_INT8_SLICES)
     CK(cudaMemcpyAsync(&rows_err, h->d_ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, st));

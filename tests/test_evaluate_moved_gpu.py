@@ -59,6 +59,51 @@ def test_moved_writes_only_selected_outputs():
     assert np.isfinite(full["e_local"]).all()
 
 
+@pytest.mark.parametrize("entry", ["moved", "all_positions"])
+def test_page_locked_outputs_equal_copied_outputs(entry):
+    """Outputs in mapped page-locked host memory are stored by the kernel
+    over the bus; they must equal the outputs copied back into pageable
+    arrays, and outputs not selected stay untouched."""
+    import torch
+    torch.cuda.set_device(0)
+    s = make_system("dmc_6nuc_30e", seed=2)
+    W, N = 200, s.n_electrons
+    a = QMCB200Functions(s, W, qf_modification=2, dt=0.01)
+    b = QMCB200Functions(s, W, qf_modification=2, dt=0.01)
+    R = s.initial_positions(W, seed=3)
+    sl = np.arange(W)
+    a.evaluate(sl, R, -1)
+    b.evaluate(sl, R, -1)
+    shapes = (("log_abs_psi", (W,), torch.float64), ("sign", (W,), torch.float64),
+              ("grad", (W, N, 3), torch.float64), ("mod_grad", (W, N, 3), torch.float64),
+              ("lap", (W,), torch.float64), ("e_local", (W,), torch.float64), ("pe", (W, 3), torch.float64),
+              ("status", (W,), torch.uint8))
+    pin = {k: torch.full(shp, 7, dtype=dt).pin_memory().numpy() for k, shp, dt in shapes}
+    mask = OUT_PSI | OUT_MOD_GRAD | OUT_E_LOCAL | OUT_STATUS
+    rng = np.random.default_rng(4)
+    for m in range(N + 3):
+        e = m % N
+        R[:, e] += 0.15 * rng.standard_normal((W, 3))
+        if entry == "moved":
+            x = a.evaluate_moved(sl, R[:, e], e, mask)
+            y = b.evaluate_moved(sl, R[:, e], e, mask, out=pin)
+            keys = ("log_abs_psi", "sign", "mod_grad", "e_local", "status")
+            for k in ("grad", "lap", "pe"):
+                assert np.all(pin[k] == 7), (m, k)
+        else:
+            x = a.evaluate(sl, R, e)
+            rc = b.lib.qmcb_evaluate(b.h, e, np.ascontiguousarray(sl, dtype=np.int32).ctypes.data, W,
+                                     np.ascontiguousarray(R).ctypes.data,
+                                     *[pin[k].ctypes.data for k, _, _ in shapes])
+            assert rc == 0, b.lib.qmcb_last_error(b.h)
+            y = pin
+            keys = [k for k, _, _ in shapes]
+        for k in keys:
+            np.testing.assert_array_equal(x[k], y[k], err_msg=f"{entry} move {m} {k}")
+    a.close()
+    b.close()
+
+
 def test_slot_allocator():
     s = make_system("vmc_water_10e", seed=1)
     f = QMCB200Functions(s, 5)
