@@ -204,22 +204,25 @@ def el_errors(system, prec, W=256, sweeps=1, seed=3, R=None):
             "samples": int(err.size), "within_1e-5_ha": float(np.mean(err <= 1e-5))}
 
 
-PREC_NAMES = {0: "fp64", 1: "mixed_fp32_rows", 2: "int8_slices_tcgen05"}
+PREC_NAMES = {0: "fp64", 1: "mixed_fp32_rows", 2: "int8_slices_tcgen05", 3: "bf16_tcgen05", 4: "bf16x3_tcgen05"}
 
 
 def precision_section(args, rank: int):
     """The 100-electron workload (20 nuclei, 400 basis functions, 65,536
-    walkers, DMC as the main workload) in the three arithmetic modes: plain
+    walkers, DMC as the main workload) in five arithmetic modes: plain
     FP64 (one warp per walker, FP64 tensor-pipe contraction), FP32 basis and
-    orbital rows, and the batched tensor-core contraction of int8 digit
-    planes (tcgen05 kind::i8, FP64-equivalent rows), each timed with CUDA
+    orbital rows, the batched tensor-core contraction of int8 digit
+    planes (tcgen05 kind::i8, FP64-equivalent rows), and the same batched
+    contraction with BF16 operands and FP32 accumulation (tcgen05 kind::f16),
+    plain and split into hi + lo with three products, each timed with CUDA
     events over two DMC blocks (200 moves per walker: 2 branching passes, 4
     LU refreshes), with per-kernel times; then the per-walker local-energy
     error of each mode against FP64 on identical configurations, on this
     workload, the 30-electron one and the reference's water input."""
     import torch
     from qmcbeaver_b200.api import QMCB200Functions
-    from qmcbeaver_b200.desc import QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES, QMCB_PREC_MIXED
+    from qmcbeaver_b200.desc import (QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC, QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES,
+                                     QMCB_PREC_MIXED)
     from qmcbeaver_b200.replicas import aggregate_timing, replica_seed
     from qmcbeaver_b200.system import make_system, system_from_arrays
     system = make_system("mixed_20nuc_100e", seed=1)
@@ -228,7 +231,8 @@ def precision_section(args, rank: int):
     out = {"workload": "mixed_20nuc_100e", "walkers": W, "electrons": N, "basis_functions": system.n_basis,
            "modes": {}}
     R_eq = None
-    for prec in (QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES, QMCB_PREC_MIXED):
+    reduced = (QMCB_PREC_INT8_SLICES, QMCB_PREC_BF16X3_TC, QMCB_PREC_BF16_TC, QMCB_PREC_MIXED)
+    for prec in (QMCB_PREC_FP64,) + reduced:
         p = dmc_params(seed=replica_seed(91, rank), e0=-1.0, reweight_start=10 ** 9)
         p.precision = prec
         f = QMCB200Functions(system, 2 * W, p)
@@ -279,6 +283,18 @@ def precision_section(args, rank: int):
                 "peak_tops": peak_tops, "peak_kind": "int8 dense = 2 x measured bf16 dense burst",
                 "avg_launch_ms": mm["ms"] / mm["launches"]}
             mode["contraction_roofline"]["frac"] = mode["contraction_roofline"]["achieved_tops"] / peak_tops
+        if prec in (QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC):
+            # tiles of 25 walkers x 32-orbital tiles x 16-function K steps x
+            # 1 or 3 MMAs of 128 x 32 x 16 BF16 multiply-adds
+            mm = ks["rows_mma"]
+            per = 3 if prec == QMCB_PREC_BF16X3_TC else 1
+            ops = (-(-wpl // 25)) * (-(-n // 32)) * (-(-system.n_basis // 16)) * per * 2 * 128 * 32 * 16
+            peak_tf = read_bf16_peak()
+            mode["contraction_roofline"] = {
+                "bound": "tensor", "kernel": "k_rows_mma_bf", "achieved_tflops": ops / (mm["ms"] / mm["launches"] / 1e3) / 1e12,
+                "peak_tflops": peak_tf, "peak_kind": "measured bf16 dense burst",
+                "avg_launch_ms": mm["ms"] / mm["launches"]}
+            mode["contraction_roofline"]["frac"] = mode["contraction_roofline"]["achieved_tflops"] / peak_tf
         out["modes"][PREC_NAMES[prec]] = mode
     fp = out["modes"]["fp64"]["value"]
     for k, v in out["modes"].items():
@@ -288,13 +304,16 @@ def precision_section(args, rank: int):
     err = {}
     for name, s, R in (("mixed_20nuc_100e", system, R_eq), ("dmc_6nuc_30e", make_system("dmc_6nuc_30e", seed=1), None),
                        ("h2o_input", h2o, None)):
-        err[name] = {PREC_NAMES[p]: el_errors(s, p, R=R) for p in (QMCB_PREC_INT8_SLICES, QMCB_PREC_MIXED)}
+        err[name] = {PREC_NAMES[p]: el_errors(s, p, R=R) for p in reduced}
     out["el_error_vs_fp64_ha"] = err
     out["note"] = ("int8_slices_tcgen05: basis values and MO coefficients scaled per 32-function block and cut into 8 int8 "
                    "digit planes, "
                    "tcgen05.mma kind::i8 with exact int32 accumulation, FP64 recombination; FP64 inverse, "
-                   "Sherman-Morrison update, ratio sums, refresh and energies. mixed_fp32_rows: FP32 basis and "
-                   "orbital rows, FP64 inverse and energies.")
+                   "Sherman-Morrison update, ratio sums, refresh and energies. bf16_tcgen05: basis values and MO "
+                   "coefficients rounded to BF16, tcgen05.mma kind::f16 with FP32 accumulation in TMEM over all "
+                   "of K. bf16x3_tcgen05: the split-precision variant, hi + lo BF16 per value, hi.hi + hi.lo + "
+                   "lo.hi accumulated in FP32. mixed_fp32_rows: FP32 basis and orbital rows, FP64 inverse and "
+                   "energies.")
     return out
 
 

@@ -83,6 +83,23 @@ extern "C" {
  * determinant per system; the full evaluation and the LU refresh run in
  * FP64. */
 #define QMCB_PREC_INT8_SLICES 2
+/* FP64 walker state and updates; each move's orbital rows from the same
+ * batched contraction with BF16 operands and FP32 accumulation in the tensor
+ * memory (tcgen05 kind::f16, M = 128, N = 32, K = 16 per instruction):
+ *   QMCB_PREC_BF16_TC    basis values and MO coefficients rounded to BF16
+ *                        (8 significant bits), one product per pair;
+ *   QMCB_PREC_BF16X3_TC  the split-precision variant: each value split as
+ *                        hi + lo (two BF16 values, 16 significant bits) and
+ *                        the products hi.hi + hi.lo + lo.hi accumulated in
+ *                        FP32 (compensated products, FP32-class rows).
+ * The reference's own reduced-precision option keeps float orbitals with a
+ * double inverse (qmcfloat, QMcBeaver/include/Array2D.h:79-84,
+ * QMcBeaver/src/QMCSlater.cpp:526-532).  These rows carry FP32-class or
+ * BF16-class errors that the Slater matrices' conditioning amplifies in the
+ * local energy; one determinant per system, FP64 full evaluation and LU
+ * refresh. */
+#define QMCB_PREC_BF16_TC 3
+#define QMCB_PREC_BF16X3_TC 4
 
 /*
  * Molecular system: what QMCInput reads from the .ckmf &geometry, &basis,
@@ -437,8 +454,8 @@ int qmcb_branch(qmcb_handle *h, int step, int *n_live);
 #define QMCB_KERNEL_COPY 2
 #define QMCB_KERNEL_ENERGY 3
 #define QMCB_KERNEL_REFRESH 4
-#define QMCB_KERNEL_ROWS_PREP 5 /* QMCB_PREC_INT8_SLICES: proposal, basis values and their digits */
-#define QMCB_KERNEL_ROWS_MMA 6  /* QMCB_PREC_INT8_SLICES: the tensor-core contraction */
+#define QMCB_KERNEL_ROWS_PREP 5 /* tensor-core rows modes: proposal, basis values and their operand planes */
+#define QMCB_KERNEL_ROWS_MMA 6  /* tensor-core rows modes: the tensor-core contraction */
 #define QMCB_KERNEL_COUNT 7
 int qmcb_set_profiling(qmcb_handle *h, int enable);
 int qmcb_get_kernel_stats(qmcb_handle *h, double *out, int reset);
@@ -448,6 +465,15 @@ int qmcb_synchronize(qmcb_handle *h);
 
 /* The CUDA stream of the handle (cudaStream_t as void*). */
 void *qmcb_stream(qmcb_handle *h);
+
+/* Diagnostic, no counterpart in the reference: the orbital rows the last
+ * single-electron move of a tensor-core rows mode (QMCB_PREC_INT8_SLICES,
+ * QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC) used, rows[num][5][*n] in the
+ * order of that move's walker list (value, d/dx, d/dy, d/dz, Laplacian rows
+ * of the moved electron at its proposed position times the spin's MO
+ * coefficients; *n = orbitals of the moved spin).  QMCB_E_STATE before any
+ * such move. */
+int qmcb_get_rows(qmcb_handle *h, int num, int *n, double *rows);
 
 /*
  * Allocation-free branching pass (no counterpart in the reference).

@@ -31,7 +31,7 @@ EXPORTS = [
     "qmcb_branch_weights_noalloc", "qmcb_run_steps_async", "qmcb_steps_done", "qmcb_steps_collect",
     "qmcb_state_bytes", "qmcb_fit_cusps", "qmcb_run_step_configs",
     "qmcb_group_create", "qmcb_group_destroy", "qmcb_group_last_error", "qmcb_group_run_steps", "qmcb_group_config",
-    "qmcb_group_set_config", "qmcb_evaluate_moved", "qmcb_alloc_slot", "qmcb_free_slot",
+    "qmcb_group_set_config", "qmcb_evaluate_moved", "qmcb_alloc_slot", "qmcb_free_slot", "qmcb_get_rows",
 ]
 
 # qmcb_evaluate_moved output selection (QMCB_OUT_*)
@@ -70,6 +70,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     L.qmcb_evaluate_device.argtypes = [vp, C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.qmcb_evaluate_moved.argtypes = [vp, C.c_int, vp, C.c_int, vp, C.c_uint, vp, vp, vp, vp, vp, vp, vp, vp]
     L.qmcb_alloc_slot.argtypes = [vp, C.POINTER(C.c_int)]
+    L.qmcb_get_rows.argtypes = [vp, C.c_int, C.POINTER(C.c_int), vp]
     L.qmcb_free_slot.argtypes = [vp, C.c_int]
     L.qmcb_init_walkers.argtypes = [vp, C.c_int, vp]
     L.qmcb_run_steps.argtypes = [vp, C.c_int, C.c_int, vp]
@@ -187,6 +188,15 @@ class QMCB200Functions:
                                           _ptr(out["mod_grad"]), _ptr(out["lap"]), _ptr(out["e_local"]),
                                           _ptr(out["pe"]), _ptr(out["status"]))
         self._check(rc, "qmcb_evaluate_moved")
+        return out
+
+    def get_rows(self, num: int) -> np.ndarray:
+        """qmcb_get_rows: the orbital rows [num][5][n] of the last
+        single-electron move made in a tensor-core rows mode."""
+        n = C.c_int()
+        self._check(self.lib.qmcb_get_rows(self.h, 0, C.byref(n), None), "qmcb_get_rows")
+        out = np.zeros((num, 5, n.value))
+        self._check(self.lib.qmcb_get_rows(self.h, int(num), C.byref(n), _ptr(out)), "qmcb_get_rows")
         return out
 
     def alloc_slot(self) -> int:

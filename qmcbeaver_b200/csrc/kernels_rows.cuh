@@ -45,6 +45,8 @@
 // contracting (MoveArgs::rows).
 #pragma once
 
+#include <cstring>
+
 #include "kernels.cuh"
 
 namespace qmcb {
@@ -485,6 +487,281 @@ __global__ void __launch_bounds__(kRowsThreads, 1) k_rows_mma(const signed char 
 #pragma unroll
     for (int q = 0; q < 16; q++)
       if (o0 + q < n) rows[(size_t)row * n + o0 + q] = out[q];
+  }
+}
+
+// ------------------------------------------------------------------------
+// BF16 tensor-core rows with FP32 accumulation (QMCB_PREC_BF16_TC,
+// QMCB_PREC_BF16X3_TC): the same batched GEMM, rows[5 x walker][o] =
+// sum_k chi[r][k] C[o][k], with BF16 operands and FP32 accumulation in TMEM
+// over all of K.  QMCB_PREC_BF16_TC rounds each operand value to BF16 (8
+// significant bits) once; QMCB_PREC_BF16X3_TC splits it as x = hi + lo
+// (hi = x rounded to 8 bits, lo = x - hi rounded to 8 bits, so hi + lo
+// keeps 16 bits) and accumulates the three products hi.hi + hi.lo + lo.hi
+// (the split-precision compensated product; lo.lo, below 2^-16 of the
+// product, is left out).  Floating-point operands need no block scales, so
+// the accumulator is read once per tile, after the last K step.
+//
+//   k_rows_prep_bf   one warp per walker: proposal and basis values as
+//                    k_rows_prep, written as kPlanes BF16 planes (hi, lo)
+//                    in the K-major core-matrix layout, 16 functions (32
+//                    bytes) per K step
+//   k_rows_mma_bf    one CTA of 128 threads per tile of 25 walkers and 32
+//                    orbitals: kPlanes == 1 one, kPlanes == 2 three
+//                    tcgen05.mma kind::f16 (BF16 x BF16 -> FP32, M = 128,
+//                    N = 32, K = 16) per K step into one 32-column TMEM
+//                    accumulator, operands staged by bulk copies in
+//                    kBfStages stages; writes rows[walker][5][n]
+constexpr int kBfKStep = 16;  // BF16 K of one MMA (32 bytes per row)
+constexpr int kBfStages = 6;
+constexpr int kBfThreads = 128;  // one warp per TMEM lane quarter
+constexpr uint32_t kBfTmemCols = 32;
+__host__ __device__ inline int bf_stage_bytes(int planes) { return planes * (kABlock + kBBlock); }
+__host__ __device__ inline int bf_smem_bytes(int planes) { return kBfStages * bf_stage_bytes(planes) + 256; }
+// Instruction descriptor of kind::f16: D F32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9 and 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kNTile >> 3) << 17) |
+                                ((uint32_t)(kTileRows >> 4) << 24);
+
+// x rounded to 8 significant bits (round to nearest by Veltkamp's split with
+// the factor 2^45 + 1; ties are not necessarily even), flushed to zero below
+// 2^-126 (BF16 normal range); the result is exactly a BF16 value.
+__host__ __device__ inline double bf16_round(double x)
+{
+  // the product rounded on its own (never fused with the subtraction)
+#ifdef __CUDA_ARCH__
+  const double c = __dmul_rn(x, 35184372088833.0);  // 2^45 + 1
+#else
+  const double c = x * 35184372088833.0;
+#endif
+  const double h = c - (c - x);
+  return fabs(h) < 1.1754943508222875e-38 ? 0.0 : h;
+}
+
+// Bits of a value that bf16_round produced (its FP32 form's upper half).
+__host__ __device__ inline uint32_t bf16_bits(double v)
+{
+  const float f = (float)v;  // exact: 8 significant bits in FP32 range
+#ifdef __CUDA_ARCH__
+  return __float_as_uint(f) >> 16;
+#else
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  return u >> 16;
+#endif
+}
+
+template <bool kMetropolis, bool kExtras, int kPlanes>
+__global__ void __launch_bounds__(128) k_rows_prep_bf(DevSys S, Layout L, RunCfg cfg, const double *state,
+                                                       const int *slots, int num, const int *d_num,
+                                                       const double *R_in, MoveArgs mv, int ksteps,
+                                                       unsigned char *A)
+{
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5, lane = lane_id();
+  const int nw = d_num ? *d_num : num;
+  const int wi = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (wi >= nw) return;
+  const int N = S.N, K = S.K, e = mv.e;
+  double *sm = smem + (size_t)warp * rows_prep_doubles(N, K, S.nslot);
+  double *sR = sm, *smg = sm + even(3 * N), *ex = sm;
+  const int slot = slots ? slots[wi] : wi;
+  const double *blk = state + (size_t)slot * L.stride;
+  for (int t = lane; t < 3 * N; t += 32) {
+    sR[t] = blk[L.R + t];
+    smg[t] = blk[L.mgrad + t];
+  }
+  __syncwarp();
+  const double ro[3] = {sR[3 * e], sR[3 * e + 1], sR[3 * e + 2]};
+  double rn[3], g_fwd, u_acc;
+  propose_move<kMetropolis, kExtras>(S, cfg, slot, mv.step, e, N, sR, ro, smg, R_in, wi, rn, g_fwd, u_acc, mv.rin_moved);
+  __syncwarp();  // the slots overwrite the staged arrays
+  basis_slot_exps_warp(S, rn, ex);
+  __syncwarp();
+  const int row0 = 5 * wi, tile = row0 / (5 * kTileWalkers), r0 = row0 - tile * 5 * kTileWalkers;
+  for (int k0 = 4 * lane; k0 < ksteps * kBfKStep; k0 += 128) {
+    double v[4][5];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (k0 + u < K) {
+        basis_function_rows(S, rn, k0 + u, ex, v[u]);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 5; d++) v[u][d] = 0.0;
+      }
+    }
+    // four consecutive functions: 8 bytes of a row in one 16-byte core-matrix row
+    const int kk = k0 / kBfKStep, kb = 2 * (k0 % kBfKStep);
+#pragma unroll
+    for (int d = 0; d < 5; d++) {
+      uint32_t hb[4], lb[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const double h = bf16_round(v[u][d]);
+        hb[u] = bf16_bits(h);
+        lb[u] = kPlanes > 1 ? bf16_bits(bf16_round(v[u][d] - h)) : 0u;
+      }
+      const size_t base = ((size_t)tile * ksteps + kk) * kPlanes * kABlock + rows_blk_off(r0 + d, kb);
+      *(uint2 *)(A + base) = make_uint2(hb[0] | (hb[1] << 16), hb[2] | (hb[3] << 16));
+      if (kPlanes > 1) *(uint2 *)(A + base + kABlock) = make_uint2(lb[0] | (lb[1] << 16), lb[2] | (lb[3] << 16));
+    }
+  }
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kIdescBf16), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v)
+{
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+
+// A: [tile][K step][plane] blocks of kABlock bytes (BF16, 16 functions per
+// K step); B: [orbital tile][K step][2 planes] blocks of kBBlock bytes (hi,
+// lo of the spin's MO coefficients, made at set-up; kPlanes == 1 reads the
+// hi plane).  Thread 0 streams the stages (bulk copies, one mbarrier per
+// stage) and issues the MMAs; the four warps read the accumulator once at
+// the end.  err: set to 1 when a wait gave up (the rows are then not
+// written).  Every wait is bounded; the kernel leaves no copy or MMA in
+// flight and frees its TMEM on every path.
+template <int kPlanes>
+__global__ void __launch_bounds__(kBfThreads) k_rows_mma_bf(const unsigned char *__restrict__ A,
+                                                           const unsigned char *__restrict__ B, int n, int ntiles,
+                                                           int ksteps, int num, const int *d_num,
+                                                           double *__restrict__ rows, int *err)
+{
+  extern __shared__ __align__(1024) unsigned char rsm[];
+  constexpr int kStage = kPlanes * (kABlock + kBBlock);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nw = d_num ? *d_num : num;
+  const int tile = blockIdx.x / ntiles, ntile = blockIdx.x - tile * ntiles;
+  if (tile * kTileWalkers >= nw) return;  // whole CTA: before any TMEM or barrier use
+  uint64_t *full = (uint64_t *)(rsm + kBfStages * kStage);
+  uint64_t *empty = full + kBfStages;
+  uint64_t *done = empty + kBfStages;
+  uint32_t *tslot = (uint32_t *)(done + 1);
+  volatile int *s_abort = (volatile int *)(tslot + 1);
+  int *s_last = (int *)(tslot + 2);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                 "r"(kBfTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kBfStages; s++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(full + s)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(empty + s)));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(done)));
+    *s_abort = 0;
+    *s_last = -1;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const unsigned char *Ag = A + (size_t)tile * ksteps * kPlanes * kABlock;
+  const unsigned char *Bg = B + (size_t)ntile * ksteps * 2 * kBBlock;
+  auto load = [&](int kk) {
+    const int st = kk % kBfStages;
+    const uint32_t fb = smem_u32(full + st), dst = smem_u32(rsm + st * kStage);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"((uint32_t)kStage)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+                 "l"(Ag + (size_t)kk * kPlanes * kABlock), "r"((uint32_t)(kPlanes * kABlock)), "r"(fb)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     dst + kPlanes * kABlock),
+                 "l"(Bg + (size_t)kk * 2 * kBBlock), "r"((uint32_t)(kPlanes * kBBlock)), "r"(fb)
+                 : "memory");
+  };
+  bool committed = false;  // thread 0: the final commit onto `done` was issued
+  if (tid == 0) {
+    int loaded = 0;
+    for (; loaded < kBfStages && loaded < ksteps; loaded++) load(loaded);
+    bool w = true;
+    for (int kk = 0; kk < ksteps && w; kk++) {
+      const int st = kk % kBfStages;
+      w = mbar_wait(smem_u32(full + st), (uint32_t)((kk / kBfStages) & 1));
+      if (!w) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t a0 = smem_u32(rsm + st * kStage), b0 = a0 + kPlanes * kABlock;
+      const uint64_t ah = umma_desc(a0, 128, 256), bh = umma_desc(b0, 128, 256);
+      mma_bf16(tmem, ah, bh, kk > 0 ? 1u : 0u);
+      if (kPlanes > 1) {
+        const uint64_t al = umma_desc(a0 + kABlock, 128, 256), bl = umma_desc(b0 + kBBlock, 128, 256);
+        mma_bf16(tmem, ah, bl, 1u);
+        mma_bf16(tmem, al, bh, 1u);
+      }
+      mma_commit(smem_u32(empty + st));
+      *s_last = kk;
+      // refill the stage the previous K step used once its MMAs have read
+      // it (this step's MMAs are queued meanwhile)
+      if (kk >= 1 && loaded < ksteps) {
+        const int sp = (kk - 1) % kBfStages;
+        w = mbar_wait(smem_u32(empty + sp), (uint32_t)(((kk - 1) / kBfStages) & 1));
+        if (w) load(loaded++);
+      }
+    }
+    if (w) {
+      mma_commit(smem_u32(done));
+      committed = true;
+    } else {
+      *s_abort = 1;
+      // leave no copy or MMA in flight: the copies issued but not consumed
+      // land, then the last step's MMAs complete (bounded waits)
+      const int last = *s_last;
+      for (int l = last + 1; l < loaded; l++)
+        mbar_wait(smem_u32(full + l % kBfStages), (uint32_t)((l / kBfStages) & 1));
+      if (last >= 0) mbar_wait(smem_u32(empty + last % kBfStages), (uint32_t)((last / kBfStages) & 1));
+    }
+  }
+  __syncwarp();
+  __syncthreads();
+  bool ok = !*s_abort;
+  if (ok) ok = __all_sync(0xFFFFFFFFu, mbar_wait_or_abort(smem_u32(done), 0u, s_abort));
+  if (!ok) *s_abort = 1;
+  float acc[32];
+  if (ok) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    uint32_t v[32];
+    tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16), v);
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 32; q++) acc[q] = __uint_as_float(v[q]);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  const bool okall = !*s_abort;
+  if (tid == 0 && !okall) {
+    // a warp gave up on `done`: the MMAs must still finish before the TMEM is freed
+    if (committed) mbar_wait(smem_u32(done), 0u);
+    atomicExch(err, 1);
+  }
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kBfTmemCols));
+  const int r = 32 * warp + lane;
+  const int row = tile * 5 * kTileWalkers + r;
+  if (okall && r < 5 * kTileWalkers && row < 5 * nw) {
+    const int o0 = ntile * kNTile;
+#pragma unroll
+    for (int q = 0; q < 32; q++)
+      if (o0 + q < n) rows[(size_t)row * n + o0 + q] = (double)acc[q];
   }
 }
 

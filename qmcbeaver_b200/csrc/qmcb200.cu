@@ -62,6 +62,11 @@ struct qmcb_handle {
   signed char *d_rows_A = nullptr, *d_rows_B[2] = {nullptr, nullptr};
   double *d_rows_rs = nullptr, *d_rows_cs[2] = {nullptr, nullptr}, *d_rows_out = nullptr;
   int rows_ksteps = 0, wpb_rows = 1, wpb_prep = 1;
+  // the BF16 forms (QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC): A planes of the
+  // step's basis rows (room for two), hi / lo planes of the MO coefficients
+  unsigned char *d_bf_A = nullptr, *d_bf_B[2] = {nullptr, nullptr};
+  int bf_ksteps = 0;
+  int rows_n = 0, rows_num = 0;  // the last tensor-core rows launch: orbitals per row, list capacity
   size_t smem_rows = 0, smem_prep = 0;
   Layout lay_rows{};  // move-kernel scratch without the basis rows
   double *d_pade = nullptr;
@@ -416,7 +421,53 @@ static void launch_move(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &
 {
   // the Umrigar93 move is compiled only into the extras instantiation
   const bool extras = h->extras || (kMetropolis && cfg.sampling == QMCB_UMRIGAR93_IMPORTANCE_SAMPLING);
-  if (h->params.precision == QMCB_PREC_INT8_SLICES) {
+  const int prec = h->params.precision;
+  if (prec == QMCB_PREC_BF16_TC || prec == QMCB_PREC_BF16X3_TC) {
+    const int sp = mv.e < h->sys.na ? 0 : 1, n = sp ? h->sys.nb : h->sys.na;
+    const bool x3 = prec == QMCB_PREC_BF16X3_TC;
+    {
+      ProfScope ps(h, QMCB_KERNEL_ROWS_PREP, st);
+      const int pb = (cap + h->wpb_prep - 1) / h->wpb_prep;
+      const unsigned th = 32 * h->wpb_prep;
+      if (extras && x3)
+        k_rows_prep_bf<kMetropolis, true, 2><<<pb, th, h->smem_prep, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num,
+                                                                            d_num, R_in, mv, h->bf_ksteps, h->d_bf_A);
+      else if (extras)
+        k_rows_prep_bf<kMetropolis, true, 1><<<pb, th, h->smem_prep, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num,
+                                                                            d_num, R_in, mv, h->bf_ksteps, h->d_bf_A);
+      else if (x3)
+        k_rows_prep_bf<kMetropolis, false, 2><<<pb, th, h->smem_prep, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num,
+                                                                             d_num, R_in, mv, h->bf_ksteps, h->d_bf_A);
+      else
+        k_rows_prep_bf<kMetropolis, false, 1><<<pb, th, h->smem_prep, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num,
+                                                                             d_num, R_in, mv, h->bf_ksteps, h->d_bf_A);
+      ps.end(st);
+    }
+    {
+      ProfScope ps(h, QMCB_KERNEL_ROWS_MMA, st);
+      const int ntiles = (n + kNTile - 1) / kNTile;
+      const unsigned g = (unsigned)((cap + kTileWalkers - 1) / kTileWalkers) * (unsigned)ntiles;
+      if (x3)
+        k_rows_mma_bf<2><<<g, kBfThreads, bf_smem_bytes(2), st>>>(h->d_bf_A, h->d_bf_B[sp], n, ntiles, h->bf_ksteps,
+                                                                  num, d_num, h->d_rows_out, h->d_ctl + 3);
+      else
+        k_rows_mma_bf<1><<<g, kBfThreads, bf_smem_bytes(1), st>>>(h->d_bf_A, h->d_bf_B[sp], n, ntiles, h->bf_ksteps,
+                                                                  num, d_num, h->d_rows_out, h->d_ctl + 3);
+      ps.end(st);
+    }
+    mv.rows = h->d_rows_out;
+    h->rows_n = n;
+    h->rows_num = cap;
+    const dim3 g((cap + h->wpb_rows - 1) / h->wpb_rows), b(32 * h->wpb_rows);
+    ProfScope ps(h, QMCB_KERNEL_MOVE, st);
+    if (extras)
+      launch_move_g<kMetropolis, double, double, true>(h, g, b, h->smem_rows, st, cfg, slots, num, d_num, R_in, mv, o);
+    else
+      launch_move_g<kMetropolis, double, double, false>(h, g, b, h->smem_rows, st, cfg, slots, num, d_num, R_in, mv, o);
+    ps.end(st);
+    return;
+  }
+  if (prec == QMCB_PREC_INT8_SLICES) {
     const int sp = mv.e < h->sys.na ? 0 : 1, n = sp ? h->sys.nb : h->sys.na;
     {
       ProfScope ps(h, QMCB_KERNEL_ROWS_PREP, st);
@@ -440,6 +491,8 @@ static void launch_move(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &
       ps.end(st);
     }
     mv.rows = h->d_rows_out;
+    h->rows_n = n;
+    h->rows_num = cap;
     const dim3 g((cap + h->wpb_rows - 1) / h->wpb_rows), b(32 * h->wpb_rows);
     ProfScope ps(h, QMCB_KERNEL_MOVE, st);
     if (extras)
@@ -482,8 +535,14 @@ static cudaError_t move_smem_limits(int bytes)
 // Batched orbital rows on the tensor cores (QMCB_PREC_INT8_SLICES,
 // kernels_rows.cuh).
 
-// Walker state written under QMCB_PREC_FP64 serves QMCB_PREC_INT8_SLICES too.
+// Walker state written under QMCB_PREC_FP64 serves the tensor-core rows modes too.
 static int state_kind(int prec) { return prec == QMCB_PREC_MIXED ? QMCB_PREC_MIXED : QMCB_PREC_FP64; }
+
+// The modes whose orbital rows come from a batched tensor-core contraction.
+static bool rows_mode(int prec)
+{
+  return prec == QMCB_PREC_INT8_SLICES || prec == QMCB_PREC_BF16_TC || prec == QMCB_PREC_BF16X3_TC;
+}
 
 template <bool kMetropolis>
 static cudaError_t rows_prep_limits(int bytes)
@@ -513,21 +572,76 @@ static int best_warps_per_block(const qmcb_handle *h, size_t per_warp)
   return wpb;
 }
 
-// Digit tables of the MO coefficients, operand buffers, the move kernel's
-// smaller scratch layout; once per handle, on the first use of the mode.
-static int rows_setup(qmcb_handle *h)
-{
-  if (h->d_rows_A) return QMCB_OK;
-  const int K = h->K, N = h->N;
-  const int ks = (K + kKStep - 1) / kKStep;
-  const size_t tiles = (size_t)(h->max_walkers + kTileWalkers - 1) / kTileWalkers;
 #define CKR(call)                                                                                    \
   do {                                                                                               \
     cudaError_t e_ = (call);                                                                         \
     if (e_ != cudaSuccess)                                                                           \
       return fail(h, e_ == cudaErrorMemoryAllocation ? QMCB_E_NOMEM : QMCB_E_CUDA,                   \
-                  std::string("QMCB_PREC_INT8_SLICES set-up: " #call ": ") + cudaGetErrorString(e_)); \
+                  std::string("tensor-core rows set-up: " #call ": ") + cudaGetErrorString(e_));     \
   } while (0)
+
+template <bool kMetropolis>
+static cudaError_t rows_prep_bf_limits(int bytes)
+{
+  cudaError_t e = cudaFuncSetAttribute(k_rows_prep_bf<kMetropolis, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_rows_prep_bf<kMetropolis, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_rows_prep_bf<kMetropolis, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_rows_prep_bf<kMetropolis, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
+}
+
+// What every tensor-core rows mode shares, once per handle: the rows
+// buffer, the move kernel's smaller scratch layout (no basis rows), the
+// prep kernels' CTA shapes and shared-memory limits.
+static int rows_common_setup(qmcb_handle *h)
+{
+  if (h->d_rows_out) return QMCB_OK;
+  const int K = h->K, N = h->N;
+  // the move kernel without the basis rows: region A holds only the slice
+  // sums and the new drifts (and the three-body partner gradients)
+  Layout L = h->lay;
+  const int ra = even(std::max(kPart + 6 * N, h->sys.ntb > 0 ? 3 * N * h->sys.M : 0));
+  L.mv_stride += ra - L.mv_region_a;
+  L.mv_region_a = ra;
+  int max_optin = 0;
+  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  const size_t per_move = sizeof(double) * (size_t)L.mv_stride;
+  const size_t per_prep = sizeof(double) * (size_t)rows_prep_doubles(N, K, h->sys.nslot);
+  if (per_move > (size_t)max_optin || per_prep > (size_t)max_optin || kRowsSmem > max_optin ||
+      bf_smem_bytes(2) > max_optin)
+    return fail(h, QMCB_E_LIMIT, "tensor-core rows: system too large for the per-walker shared-memory scratch");
+  CKR(cudaMalloc(&h->d_rows_out, sizeof(double) * (size_t)h->max_walkers * 5 * h->nmax));
+  // a wait inside a contraction kernel that gave up sets ctl[3], which
+  // returns with every batch's live count
+  CKR(cudaMemsetAsync(h->d_ctl + 3, 0, sizeof(int), h->stream));
+  h->lay_rows = L;
+  h->wpb_rows = best_warps_per_block(h, per_move);
+  h->smem_rows = per_move * h->wpb_rows;
+  h->wpb_prep = best_warps_per_block(h, per_prep);
+  h->smem_prep = per_prep * h->wpb_prep;
+  CKR(rows_prep_limits<true>(max_optin));
+  CKR(rows_prep_limits<false>(max_optin));
+  CKR(rows_prep_bf_limits<true>(max_optin));
+  CKR(rows_prep_bf_limits<false>(max_optin));
+  CKR(cudaFuncSetAttribute(k_rows_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowsSmem));
+  CKR(cudaFuncSetAttribute(k_rows_mma_bf<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bf_smem_bytes(1)));
+  CKR(cudaFuncSetAttribute(k_rows_mma_bf<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bf_smem_bytes(2)));
+  return QMCB_OK;
+}
+
+// QMCB_PREC_INT8_SLICES: digit tables of the MO coefficients and the
+// operand buffers; once per handle, on the first use of the mode.
+static int rows_setup(qmcb_handle *h)
+{
+  const int rc = rows_common_setup(h);
+  if (rc) return rc;
+  if (h->d_rows_A) return QMCB_OK;
+  const int K = h->K;
+  const int ks = (K + kKStep - 1) / kKStep;
+  const size_t tiles = (size_t)(h->max_walkers + kTileWalkers - 1) / kTileWalkers;
   for (int sp = 0; sp < 2; sp++) {
     const int n = sp ? h->sys.nb : h->sys.na;
     const int nt = std::max((n + kNTile - 1) / kNTile, 1);
@@ -561,34 +675,47 @@ static int rows_setup(qmcb_handle *h)
   // be ordered with its work)
   CKR(cudaMemsetAsync(h->d_rows_A, 0, abytes, h->stream));  // rows 125 .. 127 of every tile stay zero
   CKR(cudaMalloc(&h->d_rows_rs, sizeof(double) * tiles * kTileRows * ks));  // [row][K step], 128 rows a tile
-  CKR(cudaMalloc(&h->d_rows_out, sizeof(double) * (size_t)h->max_walkers * 5 * h->nmax));
-  // a wait inside the contraction kernel that gave up sets ctl[3], which
-  // returns with every batch's live count
-  CKR(cudaMemsetAsync(h->d_ctl + 3, 0, sizeof(int), h->stream));
   h->rows_ksteps = ks;
-  // the move kernel without the basis rows: region A holds only the slice
-  // sums and the new drifts (and the three-body partner gradients)
-  Layout L = h->lay;
-  const int ra = even(std::max(kPart + 6 * N, h->sys.ntb > 0 ? 3 * N * h->sys.M : 0));
-  L.mv_stride += ra - L.mv_region_a;
-  L.mv_region_a = ra;
-  h->lay_rows = L;
-  int max_optin = 0;
-  cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-  const size_t per_move = sizeof(double) * (size_t)L.mv_stride;
-  const size_t per_prep = sizeof(double) * (size_t)rows_prep_doubles(N, K, h->sys.nslot);
-  if (per_move > (size_t)max_optin || per_prep > (size_t)max_optin || kRowsSmem > max_optin)
-    return fail(h, QMCB_E_LIMIT, "QMCB_PREC_INT8_SLICES: system too large for the per-walker shared-memory scratch");
-  h->wpb_rows = best_warps_per_block(h, per_move);
-  h->smem_rows = per_move * h->wpb_rows;
-  h->wpb_prep = best_warps_per_block(h, per_prep);
-  h->smem_prep = per_prep * h->wpb_prep;
-  CKR(rows_prep_limits<true>(max_optin));
-  CKR(rows_prep_limits<false>(max_optin));
-  CKR(cudaFuncSetAttribute(k_rows_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowsSmem));
-#undef CKR
   return QMCB_OK;
 }
+
+// QMCB_PREC_BF16_TC / QMCB_PREC_BF16X3_TC: hi and lo BF16 planes of the MO
+// coefficients ([orbital tile][K step][plane] blocks) and the A buffer
+// (room for two planes); once per handle, on the first use of either mode.
+static int rows_bf_setup(qmcb_handle *h)
+{
+  const int rc = rows_common_setup(h);
+  if (rc) return rc;
+  if (h->d_bf_A) return QMCB_OK;
+  const int K = h->K;
+  const int ks = (K + kBfKStep - 1) / kBfKStep;
+  const size_t tiles = (size_t)(h->max_walkers + kTileWalkers - 1) / kTileWalkers;
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? h->sys.nb : h->sys.na;
+    const int nt = std::max((n + kNTile - 1) / kNTile, 1);
+    std::vector<unsigned char> B((size_t)nt * ks * 2 * kBBlock, 0);
+    const std::vector<double> &ct = h->ct_host[sp];
+    for (int o = 0; o < n; o++)
+      for (int k = 0; k < K; k++) {
+        const double c = ct[(size_t)k * n + o], hi = bf16_round(c), lo = bf16_round(c - hi);
+        const size_t blk = ((size_t)(o / kNTile) * ks + k / kBfKStep) * 2;
+        const int off = rows_blk_off(o % kNTile, 2 * (k % kBfKStep));
+        const uint32_t hb = bf16_bits(hi), lb = bf16_bits(lo);
+        B[blk * kBBlock + off] = (unsigned char)(hb & 0xff);
+        B[blk * kBBlock + off + 1] = (unsigned char)(hb >> 8);
+        B[(blk + 1) * kBBlock + off] = (unsigned char)(lb & 0xff);
+        B[(blk + 1) * kBBlock + off + 1] = (unsigned char)(lb >> 8);
+      }
+    CKR(cudaMalloc(&h->d_bf_B[sp], B.size()));
+    CKR(cudaMemcpy(h->d_bf_B[sp], B.data(), B.size(), cudaMemcpyHostToDevice));
+  }
+  const size_t abytes = tiles * ks * 2 * kABlock;
+  CKR(cudaMalloc(&h->d_bf_A, abytes));
+  CKR(cudaMemsetAsync(h->d_bf_A, 0, abytes, h->stream));  // rows 125 .. 127 of every tile stay zero
+  h->bf_ksteps = ks;
+  return QMCB_OK;
+}
+#undef CKR
 
 extern "C" {
 
@@ -1138,7 +1265,7 @@ int qmcb_destroy(qmcb_handle *h)
                   h->d_en[0], h->d_en[1], h->d_state,   h->d_live,  h->d_live_tmp, h->d_free, h->d_ctl,
                   h->d_copies, h->d_stats, h->d_dump, h->d_ectl,   h->d_slots, h->d_R,     h->d_out,    h->d_status,
                   h->d_rows_A, h->d_rows_B[0], h->d_rows_B[1], h->d_rows_rs, h->d_rows_cs[0], h->d_rows_cs[1],
-                  h->d_rows_out};
+                  h->d_rows_out, h->d_bf_A, h->d_bf_B[0], h->d_bf_B[1]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
@@ -1166,12 +1293,16 @@ int qmcb_set_params(qmcb_handle *h, const qmcb_run_params *p)
       p->exact_single_electron_gf > 1 || p->dynamic_time_step < 0 || p->dynamic_time_step > 1 ||
       p->walker_deletion < 0 || p->walker_deletion > 1)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown method selector");
-  if (p->precision != QMCB_PREC_FP64 && p->precision != QMCB_PREC_MIXED && p->precision != QMCB_PREC_INT8_SLICES)
+  if (p->precision < QMCB_PREC_FP64 || p->precision > QMCB_PREC_BF16X3_TC)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: unknown precision");
   if (h->md && p->precision != QMCB_PREC_FP64)
     return fail(h, QMCB_E_ARG, "qmcb_set_params: several determinants run in FP64 only");
   if (p->precision == QMCB_PREC_INT8_SLICES) {
     const int rc = rows_setup(h);
+    if (rc) return rc;
+  }
+  if (p->precision == QMCB_PREC_BF16_TC || p->precision == QMCB_PREC_BF16X3_TC) {
+    const int rc = rows_bf_setup(h);
     if (rc) return rc;
   }
   h->params = *p;
@@ -1205,6 +1336,19 @@ int qmcb_get_params(const qmcb_handle *h, qmcb_run_params *p)
 int qmcb_num_electrons(const qmcb_handle *h) { return h ? h->N : -1; }
 int qmcb_max_walkers(const qmcb_handle *h) { return h ? h->max_walkers : -1; }
 void *qmcb_stream(qmcb_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int qmcb_get_rows(qmcb_handle *h, int num, int *n, double *rows)
+{
+  if (!h || !n) return QMCB_E_ARG;
+  if (h->rows_n == 0) return fail(h, QMCB_E_STATE, "qmcb_get_rows: no single-electron move in a tensor-core rows mode yet");
+  *n = h->rows_n;
+  if (num < 0 || num > h->rows_num || (num > 0 && !rows)) return fail(h, QMCB_E_ARG, "qmcb_get_rows: bad argument");
+  if (num == 0) return QMCB_OK;
+  CK(cudaMemcpyAsync(rows, h->d_rows_out, sizeof(double) * 5 * (size_t)h->rows_n * num, cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return QMCB_OK;
+}
 
 int qmcb_synchronize(qmcb_handle *h)
 {
@@ -1404,7 +1548,7 @@ int qmcb_evaluate(qmcb_handle *h, int which_e, const int *slots, int num, const 
   if (which_e < 0) h->evaluated_once = true;
   CK(eval_deliver(dst, st));
   int rows_err = 0;
-  if (h->params.precision == QMCB_PREC_INT8_SLICES && which_e >= 0)
+  if (rows_mode(h->params.precision) && which_e >= 0)
     CK(cudaMemcpyAsync(&rows_err, h->d_ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   if (rows_err) return fail(h, QMCB_E_CUDA, "qmcb_evaluate: the tensor-core contraction gave up waiting (rows not written)");
@@ -1438,7 +1582,7 @@ int qmcb_evaluate_moved(qmcb_handle *h, int which_e, const int *slots, int num, 
   if (rc) return rc;
   CK(eval_deliver(dst, st));
   int rows_err = 0;
-  if (h->params.precision == QMCB_PREC_INT8_SLICES)
+  if (rows_mode(h->params.precision))
     CK(cudaMemcpyAsync(&rows_err, h->d_ctl + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   if (rows_err) return fail(h, QMCB_E_CUDA, "qmcb_evaluate_moved: the tensor-core contraction gave up waiting");

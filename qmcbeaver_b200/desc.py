@@ -17,7 +17,7 @@ QMCB_NO_IMPORTANCE_SAMPLING, QMCB_IMPORTANCE_SAMPLING, QMCB_UMRIGAR93_IMPORTANCE
 QMCB_QF_NONE, QMCB_QF_UMRIGAR93_EQUAL, QMCB_QF_UMRIGAR93_UNEQUAL = 0, 1, 2
 QMCB_EMOD_NONE, QMCB_EMOD_UMRIGAR93, QMCB_EMOD_MODIFIED_UMRIGAR93 = 0, 1, 2
 QMCB_RW_SIMPLE_SYMMETRIC, QMCB_RW_SIMPLE_ASYMMETRIC, QMCB_RW_UMRIGAR93_PROBABILITY_WEIGHTED = 0, 1, 2
-QMCB_PREC_FP64, QMCB_PREC_MIXED, QMCB_PREC_INT8_SLICES = 0, 1, 2
+QMCB_PREC_FP64, QMCB_PREC_MIXED, QMCB_PREC_INT8_SLICES, QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC = 0, 1, 2, 3, 4
 QMCB_ST_SINGULAR, QMCB_ST_NAN = 1, 2
 QMCB_ECUT_NONE, QMCB_ECUT_UMRIGAR93, QMCB_ECUT_BDJM_PUSH88 = 0, 1, 2
 
