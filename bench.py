@@ -550,7 +550,8 @@ def profile_case(name: str) -> None:
     group in configuration 0 (the group move kernel); "rows_small" runs 6
     importance-sampled VMC steps of the 100-electron / 400-function system
     with 16,384 walkers under QMCB_PREC_INT8_SLICES (the tensor-core
-    contraction k_rows_mma, its prep kernel and the move kernel on rows);
+    contraction k_rows_mma, its prep kernel and the move kernel on rows),
+    "rows_bf16x3_small" the same under QMCB_PREC_BF16X3_TC (k_rows_mma_bf);
     "refresh_100e" sets up 16,384 walkers of the 100-electron system (one
     full evaluation) and runs 50 FP64 steps, the last of which refreshes
     every walker's inverses (the second k_full launch)."""
@@ -582,12 +583,13 @@ def profile_case(name: str) -> None:
         g.close()
         for f in hs:
             f.close()
-    elif name == "rows_small":
-        from qmcbeaver_b200.desc import QMCB_PREC_INT8_SLICES
+    elif name in ("rows_small", "rows_bf16x3_small"):
+        from qmcbeaver_b200.desc import QMCB_PREC_BF16X3_TC, QMCB_PREC_INT8_SLICES
         s = make_system("mixed_20nuc_100e", seed=1)
-        W = 16384  # 4.8 GB of walker state, 240 MB of A digits: larger than L2
+        W = 16384  # 4.8 GB of walker state, 240 / 134 MB of operand planes: larger than L2
+        prec = QMCB_PREC_INT8_SLICES if name == "rows_small" else QMCB_PREC_BF16X3_TC
         f = QMCB200Functions(s, W, run_params(sampling=1, qf_modification=2, dt=0.01, seed=3, rel_cutoff=0.0,
-                                              precision=QMCB_PREC_INT8_SLICES))
+                                              precision=prec))
         f.init_walkers(s.initial_positions(W, seed=1))
         st = f.run_steps(0, 6)
         print("ok", st.n_moves)
@@ -622,7 +624,8 @@ def main():
                     help="run one extra section alone and print it")
     ap.add_argument("--serve-jobs", type=int, default=12)
     ap.add_argument("--serve-rate", type=float, default=20.0)
-    ap.add_argument("--case", choices=["multidet_small", "group_small", "rows_small", "refresh_100e"],
+    ap.add_argument("--case", choices=["multidet_small", "group_small", "rows_small", "rows_bf16x3_small",
+                                       "refresh_100e"],
                     help="run one small profiling workload instead of the benchmark")
     args = ap.parse_args()
     if args.case:

@@ -558,6 +558,37 @@ __device__ __forceinline__ int ee_func(const DevSys &S, int i, int j)
 }
 
 // ------------------------------------------------------------------ basis
+// L2 eviction policies and FP64 loads / stores that carry one: the HBM-kept
+// inverse of a large spin is read twice per move (Sherman-Morrison factors,
+// then the update), so its first read asks L2 to keep the lines and the
+// second read, the streamed derivative rows and the new inverse's stores ask
+// L2 to drop theirs first.
+__device__ __forceinline__ uint64_t l2_evict_last_policy()
+{
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint64_t l2_evict_first_policy()
+{
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ double ld_l2hint(const double *p, uint64_t pol)
+{
+  double v;
+  asm("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+__device__ __forceinline__ void st_l2hint(double *p, double v, uint64_t pol)
+{
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+
 // Contracted Cartesian Gaussian k with value, gradient and Laplacian, the
 // formulas of QMCBasisFunction::evaluateBasisFunctions
 // (QMcBeaver/src/QMCBasisFunction.cpp:287-403):

@@ -52,6 +52,24 @@ struct EnergyCtl {
 
 // Shared-memory doubles needed by one warp.
 constexpr int kPart = 160;  // 5 quantities x 32 lanes of slice partial sums
+// rows of the HBM-kept inverse per load batch of its update (eight orbitals'
+// 48 loads in flight per lane; 168 registers, no spills)
+constexpr int kGInvBatch = 8;
+
+// Loads and stores of the HBM-kept inverse with an L2 eviction policy (FP64
+// elements; other element types plain).
+template <typename T>
+__device__ __forceinline__ T ginv_ld(const T *p, uint64_t pol)
+{
+  if constexpr (sizeof(T) == 8) return ld_l2hint((const double *)p, pol);
+  else return *p;
+}
+template <typename T>
+__device__ __forceinline__ void ginv_st(T *p, T v, uint64_t pol)
+{
+  if constexpr (sizeof(T) == 8) st_l2hint((double *)p, v, pol);
+  else *p = v;
+}
 // Move-kernel scratch per warp (sizes in Layout::mv_*, set by the host):
 // region A holds the basis values chi[5][K]; once the contraction has
 // consumed them it is reused for the slice partial sums and the new drift /
@@ -1140,6 +1158,8 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
   const TS *DlT = (const TS *)(blk + L.DlT[sp]);
   double *sc = blk + L.sc;
   const int inv_d = even((n * n * (int)sizeof(TI) + 7) / 8);
+  // L2 policies of the HBM-kept inverse (kGInv): kept between its two reads
+  const uint64_t keep = kGInv ? l2_evict_last_policy() : 0, drop = kGInv ? l2_evict_first_policy() : 0;
 
   // ---- stage the walker's state: positions and the per-electron arrays
   //      first, the moved spin's inverse as a second group that lands while
@@ -1212,11 +1232,11 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
       for (; l + 8 <= n; l += 8) {
         TI v[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) v[u] = InvO[(l + u) * n + c];
+        for (int u = 0; u < 8; u++) v[u] = ginv_ld(&InvO[(l + u) * n + c], keep);
 #pragma unroll
         for (int u = 0; u < 8; u++) val = fma((TI)Dn[l + u], v[u], val);
       }
-      for (; l < n; l++) val = fma((TI)Dn[l], InvO[l * n + c], val);
+      for (; l < n; l++) val = fma((TI)Dn[l], ginv_ld(&InvO[l * n + c], keep), val);
     } else {
       for (int l = 0; l < n; l++) val = fma((TI)Dn[l], Inv[l * n + c], val);
     }
@@ -1229,9 +1249,9 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
     // copy, fused with the ratio sums of the moved spin
     // (QMcBeaver/src/QMCSlater.cpp:741-762): lane = electron column c, the
     // new inverse elements feed the sums as they are made (never read back)
-    // and the walker's derivative rows stream from HBM alongside, six
-    // orbitals' loads (36) in flight at a time, evict-first
-    constexpr int kB = 6;
+    // and the walker's derivative rows stream from HBM alongside, kGInvBatch
+    // orbitals' loads in flight at a time, evict-first
+    constexpr int kB = kGInvBatch;
     for (int c = lane; c < n; c += 32) {
       const TI vc = c == el ? (TI)0 : valc[c];
       double gx = 0, gy = 0, gz = 0, ll = 0;
@@ -1241,8 +1261,8 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
         TS g0[kB], g1[kB], g2[kB], gl[kB];
 #pragma unroll
         for (int u = 0; u < kB; u++) {
-          ie[u] = InvO[(r + u) * n + el];
-          x[u] = InvO[(r + u) * n + c];
+          ie[u] = ginv_ld(&InvO[(r + u) * n + el], drop);
+          x[u] = ginv_ld(&InvO[(r + u) * n + c], drop);
           if (c == el) {
             g0[u] = Dn[n + r + u];
             g1[u] = Dn[2 * n + r + u];
@@ -1258,7 +1278,7 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
 #pragma unroll
         for (int u = 0; u < kB; u++) {
           const TI nv = c == el ? (TI)(ie[u] * q) : x[u] - vc * ie[u];
-          Inv[(r + u) * n + c] = nv;
+          ginv_st(&Inv[(r + u) * n + c], nv, drop);
           const double iv = (double)nv;
           gx = fma((double)g0[u], iv, gx);
           gy = fma((double)g1[u], iv, gy);
@@ -1267,9 +1287,9 @@ __device__ __forceinline__ void move_walker(const DevSys &S, const Layout &L, co
         }
       }
       for (; r < n; r++) {
-        const TI ie = InvO[r * n + el];
-        const TI nv = c == el ? (TI)(ie * q) : InvO[r * n + c] - vc * ie;
-        Inv[r * n + c] = nv;
+        const TI ie = ginv_ld(&InvO[r * n + el], drop);
+        const TI nv = c == el ? (TI)(ie * q) : ginv_ld(&InvO[r * n + c], drop) - vc * ie;
+        ginv_st(&Inv[r * n + c], nv, drop);
         const double iv = (double)nv;
         if (c == el) {
           gx = fma((double)Dn[n + r], iv, gx);
