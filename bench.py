@@ -420,16 +420,18 @@ def serving_section(args):
     return out
 
 
-def _batch_compare(jobs, B, timed):
+def _batch_compare(jobs, B, timed, precision=0, refresh_interval=0):
     """One group over the jobs' handles (tuned first) against the same steps
     run handle after handle and on all handles' streams at once; wall-clock
-    walker-moves/s around synchronous batches of B steps."""
+    walker-moves/s around synchronous batches of B steps.  precision: the
+    orbital rows' arithmetic (QMCB_PREC_*); refresh_interval: the FP64
+    inverse refresh (0: none)."""
     from qmcbeaver_b200.api import QMCB200Functions, QMCB200Group
     from qmcbeaver_b200.desc import QMCB_IMPORTANCE_SAMPLING, QMCB_QF_UMRIGAR93_UNEQUAL, run_params
     hs = []
     for j in jobs:
         p = run_params(sampling=QMCB_IMPORTANCE_SAMPLING, qf_modification=QMCB_QF_UMRIGAR93_UNEQUAL, dt=0.01,
-                       seed=j.seed, rel_cutoff=0.0)
+                       seed=j.seed, rel_cutoff=0.0, precision=precision, refresh_interval=refresh_interval)
         f = QMCB200Functions(j.system, j.walkers, p)
         f.init_walkers(j.system.initial_positions(j.walkers, seed=j.seed))
         hs.append(f)
@@ -486,7 +488,9 @@ def batching_section(args):
     free memory the walker range is scaled down until they fit, and the
     range used is reported).  VMC importance-sampled steps, 50 per batch.
     Next to it the same comparison for 64 small molecules (4-40 electrons,
-    the serving jobs' sizes), where each molecule's step is a short kernel."""
+    the serving jobs' sizes), where each molecule's step is a short kernel,
+    and both workloads again on the split-BF16 tensor-core orbital rows with
+    an FP64 refresh every 50 moves."""
     from qmcbeaver_b200.serving import device_budget, make_jobs, state_footprint
     hi = 8192
     while True:
@@ -498,8 +502,17 @@ def batching_section(args):
     out = _batch_compare(jobs, B=50, timed=2)
     out["walker_range"] = [256, hi]
     out["state_gb"] = need / 1e9
-    out["small_molecules"] = _batch_compare(make_jobs(64, rate=1.0, seed=29, electrons=(4, 40), walkers=(256, 2048),
-                                                      orbitals="random"), B=40, timed=5)
+    small = make_jobs(64, rate=1.0, seed=29, electrons=(4, 40), walkers=(256, 2048), orbitals="random")
+    out["small_molecules"] = _batch_compare(small, B=40, timed=5)
+    # the configuration's FP32/BF16 orbital path with an FP64 refresh: every
+    # member's rows from the split-BF16 tensor-core contraction with FP32
+    # accumulation (FP32-class rows), the inverse refreshed in FP64 every 50 moves
+    from qmcbeaver_b200.desc import QMCB_PREC_BF16X3_TC
+    out["bf16x3_rows_fp64_refresh"] = _batch_compare(jobs, B=50, timed=2, precision=QMCB_PREC_BF16X3_TC,
+                                                     refresh_interval=50)
+    out["small_molecules"]["bf16x3_rows_fp64_refresh"] = _batch_compare(small, B=40, timed=5,
+                                                                        precision=QMCB_PREC_BF16X3_TC,
+                                                                        refresh_interval=50)
     return out
 
 

@@ -32,6 +32,7 @@ struct GroupMember {
   int dmc;
   int limit_branching;
   double thr_split, thr_fuse;
+  const double *rows;  // tensor-core rows modes: the step's orbital rows (null: FP64 basis and contraction)
 };
 
 // Member tables of groups that fit (kConst launches): read through the
@@ -97,6 +98,7 @@ __global__ void __launch_bounds__(128, (kMD || kGInv) ? 3 : 5) k_move_group(cons
     mv.do_reweight = mv.e == 0;
     mv.reweight_on = mv.step >= G.reweight_start;
     mv.dump = nullptr;
+    mv.rows = G.rows;
     if constexpr (kMD)
       md_move_walker<true>(G.S, G.L, G.cfg, G.state, G.live, i - prefix[m], sm, nullptr, mv, G.ectl, G.stats,
                            EvalOut{});

@@ -136,9 +136,9 @@ struct qmcb_handle {
 struct ProfScope {
   qmcb_handle *h;
   size_t idx;
-  ProfScope(qmcb_handle *hh, int kind, cudaStream_t st) : h(hh), idx((size_t)-1)
+  ProfScope(qmcb_handle *hh, int kind, cudaStream_t st, bool on = true) : h(hh), idx((size_t)-1)
   {
-    if (!h->prof) return;
+    if (!h->prof || !on) return;
     if (h->prof_used + 2 > h->prof_ev.size()) {
       size_t grow = std::max<size_t>(256, h->prof_ev.size());
       for (size_t i = 0; i < grow; i++) {
@@ -411,24 +411,32 @@ static void launch_move_g(qmcb_handle *h, const dim3 &g, const dim3 &b, size_t s
                                                                   R_in, mv, h->d_ectl, h->d_stats, o);
 }
 
-// One single-electron move of list entries [0, num) (d_num: device count,
-// grids sized for `cap` entries).  Under QMCB_PREC_INT8_SLICES three
-// launches: proposal + basis digits, the tensor-core contraction, the move
-// kernel on the rows; else the move kernel alone.
-template <bool kMetropolis>
-static void launch_move(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
-                        const int *d_num, const double *R_in, MoveArgs mv, EvalOut o)
+// Walker state written under QMCB_PREC_FP64 serves the tensor-core rows modes too.
+static int state_kind(int prec) { return prec == QMCB_PREC_MIXED ? QMCB_PREC_MIXED : QMCB_PREC_FP64; }
+
+// The modes whose orbital rows come from a batched tensor-core contraction.
+static bool rows_mode(int prec)
 {
-  // the Umrigar93 move is compiled only into the extras instantiation
-  const bool extras = h->extras || (kMetropolis && cfg.sampling == QMCB_UMRIGAR93_IMPORTANCE_SAMPLING);
+  return prec == QMCB_PREC_INT8_SLICES || prec == QMCB_PREC_BF16_TC || prec == QMCB_PREC_BF16X3_TC;
+}
+
+// The batched orbital rows of one single-electron step (the tensor-core
+// rows modes) into h->d_rows_out: proposal + basis operand planes, then the
+// contraction; prof: record the two kernels' times (not under stream capture).
+template <bool kMetropolis>
+static void launch_rows(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
+                        const int *d_num, const double *R_in, const MoveArgs &mv, bool extras, bool prof)
+{
   const int prec = h->params.precision;
+  const int sp = mv.e < h->sys.na ? 0 : 1, n = sp ? h->sys.nb : h->sys.na;
+  const int pb = (cap + h->wpb_prep - 1) / h->wpb_prep;
+  const unsigned th = 32 * h->wpb_prep;
+  const int ntiles = (n + kNTile - 1) / kNTile;
+  const unsigned g = (unsigned)((cap + kTileWalkers - 1) / kTileWalkers) * (unsigned)ntiles;
   if (prec == QMCB_PREC_BF16_TC || prec == QMCB_PREC_BF16X3_TC) {
-    const int sp = mv.e < h->sys.na ? 0 : 1, n = sp ? h->sys.nb : h->sys.na;
     const bool x3 = prec == QMCB_PREC_BF16X3_TC;
     {
-      ProfScope ps(h, QMCB_KERNEL_ROWS_PREP, st);
-      const int pb = (cap + h->wpb_prep - 1) / h->wpb_prep;
-      const unsigned th = 32 * h->wpb_prep;
+      ProfScope ps(h, QMCB_KERNEL_ROWS_PREP, st, prof);
       if (extras && x3)
         k_rows_prep_bf<kMetropolis, true, 2><<<pb, th, h->smem_prep, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num,
                                                                             d_num, R_in, mv, h->bf_ksteps, h->d_bf_A);
@@ -443,56 +451,48 @@ static void launch_move(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &
                                                                              d_num, R_in, mv, h->bf_ksteps, h->d_bf_A);
       ps.end(st);
     }
-    {
-      ProfScope ps(h, QMCB_KERNEL_ROWS_MMA, st);
-      const int ntiles = (n + kNTile - 1) / kNTile;
-      const unsigned g = (unsigned)((cap + kTileWalkers - 1) / kTileWalkers) * (unsigned)ntiles;
-      if (x3)
-        k_rows_mma_bf<2><<<g, kBfThreads, bf_smem_bytes(2), st>>>(h->d_bf_A, h->d_bf_B[sp], n, ntiles, h->bf_ksteps,
-                                                                  num, d_num, h->d_rows_out, h->d_ctl + 3);
-      else
-        k_rows_mma_bf<1><<<g, kBfThreads, bf_smem_bytes(1), st>>>(h->d_bf_A, h->d_bf_B[sp], n, ntiles, h->bf_ksteps,
-                                                                  num, d_num, h->d_rows_out, h->d_ctl + 3);
-      ps.end(st);
-    }
-    mv.rows = h->d_rows_out;
-    h->rows_n = n;
-    h->rows_num = cap;
-    const dim3 g((cap + h->wpb_rows - 1) / h->wpb_rows), b(32 * h->wpb_rows);
-    ProfScope ps(h, QMCB_KERNEL_MOVE, st);
-    if (extras)
-      launch_move_g<kMetropolis, double, double, true>(h, g, b, h->smem_rows, st, cfg, slots, num, d_num, R_in, mv, o);
+    ProfScope ps(h, QMCB_KERNEL_ROWS_MMA, st, prof);
+    if (x3)
+      k_rows_mma_bf<2><<<g, kBfThreads, bf_smem_bytes(2), st>>>(h->d_bf_A, h->d_bf_B[sp], n, ntiles, h->bf_ksteps, num,
+                                                                d_num, h->d_rows_out, h->d_ctl + 3);
     else
-      launch_move_g<kMetropolis, double, double, false>(h, g, b, h->smem_rows, st, cfg, slots, num, d_num, R_in, mv, o);
+      k_rows_mma_bf<1><<<g, kBfThreads, bf_smem_bytes(1), st>>>(h->d_bf_A, h->d_bf_B[sp], n, ntiles, h->bf_ksteps, num,
+                                                                d_num, h->d_rows_out, h->d_ctl + 3);
     ps.end(st);
-    return;
-  }
-  if (prec == QMCB_PREC_INT8_SLICES) {
-    const int sp = mv.e < h->sys.na ? 0 : 1, n = sp ? h->sys.nb : h->sys.na;
+  } else {
     {
-      ProfScope ps(h, QMCB_KERNEL_ROWS_PREP, st);
-      const int pb = (cap + h->wpb_prep - 1) / h->wpb_prep;
+      ProfScope ps(h, QMCB_KERNEL_ROWS_PREP, st, prof);
       if (extras)
-        k_rows_prep<kMetropolis, true><<<pb, 32 * h->wpb_prep, h->smem_prep, st>>>(
-            h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, mv, h->rows_ksteps, h->d_rows_A, h->d_rows_rs);
+        k_rows_prep<kMetropolis, true><<<pb, th, h->smem_prep, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+                                                                      R_in, mv, h->rows_ksteps, h->d_rows_A, h->d_rows_rs);
       else
-        k_rows_prep<kMetropolis, false><<<pb, 32 * h->wpb_prep, h->smem_prep, st>>>(
-            h->sys, h->lay, cfg, h->d_state, slots, num, d_num, R_in, mv, h->rows_ksteps, h->d_rows_A, h->d_rows_rs);
+        k_rows_prep<kMetropolis, false><<<pb, th, h->smem_prep, st>>>(h->sys, h->lay, cfg, h->d_state, slots, num, d_num,
+                                                                       R_in, mv, h->rows_ksteps, h->d_rows_A, h->d_rows_rs);
       ps.end(st);
     }
-    {
-      ProfScope ps(h, QMCB_KERNEL_ROWS_MMA, st);
-      // the orbital tiles of a tile adjacent in the grid (A read once from HBM)
-      const int ntiles = (n + kNTile - 1) / kNTile;
-      const unsigned g = (unsigned)((cap + kTileWalkers - 1) / kTileWalkers) * (unsigned)ntiles;
-      k_rows_mma<<<g, kRowsThreads, kRowsSmem, st>>>(h->d_rows_A, h->d_rows_B[sp], h->d_rows_rs, h->d_rows_cs[sp],
-                                                     n, ntiles, h->rows_ksteps, num, d_num, h->d_rows_out,
-                                                     h->d_ctl + 3);
-      ps.end(st);
-    }
+    // the orbital tiles of a tile adjacent in the grid (A read once from HBM)
+    ProfScope ps(h, QMCB_KERNEL_ROWS_MMA, st, prof);
+    k_rows_mma<<<g, kRowsThreads, kRowsSmem, st>>>(h->d_rows_A, h->d_rows_B[sp], h->d_rows_rs, h->d_rows_cs[sp], n,
+                                                   ntiles, h->rows_ksteps, num, d_num, h->d_rows_out, h->d_ctl + 3);
+    ps.end(st);
+  }
+  h->rows_n = n;
+  h->rows_num = cap;
+}
+
+// One single-electron move of list entries [0, num) (d_num: device count,
+// grids sized for `cap` entries).  Under QMCB_PREC_INT8_SLICES three
+// launches: proposal + basis digits, the tensor-core contraction, the move
+// kernel on the rows; else the move kernel alone.
+template <bool kMetropolis>
+static void launch_move(qmcb_handle *h, int cap, cudaStream_t st, const RunCfg &cfg, const int *slots, int num,
+                        const int *d_num, const double *R_in, MoveArgs mv, EvalOut o)
+{
+  // the Umrigar93 move is compiled only into the extras instantiation
+  const bool extras = h->extras || (kMetropolis && cfg.sampling == QMCB_UMRIGAR93_IMPORTANCE_SAMPLING);
+  if (rows_mode(h->params.precision)) {
+    launch_rows<kMetropolis>(h, cap, st, cfg, slots, num, d_num, R_in, mv, extras, true);
     mv.rows = h->d_rows_out;
-    h->rows_n = n;
-    h->rows_num = cap;
     const dim3 g((cap + h->wpb_rows - 1) / h->wpb_rows), b(32 * h->wpb_rows);
     ProfScope ps(h, QMCB_KERNEL_MOVE, st);
     if (extras)
@@ -535,14 +535,6 @@ static cudaError_t move_smem_limits(int bytes)
 // Batched orbital rows on the tensor cores (QMCB_PREC_INT8_SLICES,
 // kernels_rows.cuh).
 
-// Walker state written under QMCB_PREC_FP64 serves the tensor-core rows modes too.
-static int state_kind(int prec) { return prec == QMCB_PREC_MIXED ? QMCB_PREC_MIXED : QMCB_PREC_FP64; }
-
-// The modes whose orbital rows come from a batched tensor-core contraction.
-static bool rows_mode(int prec)
-{
-  return prec == QMCB_PREC_INT8_SLICES || prec == QMCB_PREC_BF16_TC || prec == QMCB_PREC_BF16X3_TC;
-}
 
 template <bool kMetropolis>
 static cudaError_t rows_prep_limits(int bytes)
@@ -2147,6 +2139,20 @@ static int group_enqueue(qmcb_group *g, int c, int n_steps, const int *first_ste
     for (int i = B.first; i < B.first + B.count; i++) dmc |= g->mem[i]->params.run_type == QMCB_DMC;
     const GroupMember *gm = g->d_gm + B.first;
     for (int t = 0; t < n_steps; t++) {
+      // members on tensor-core rows: their step's rows first (one prep and
+      // one contraction launch per member, on the bucket's stream)
+      for (int i = B.first; i < B.first + B.count; i++) {
+        qmcb_handle *h = g->mem[i];
+        if (!rows_mode(h->params.precision)) continue;
+        MoveArgs mv;
+        mv.step = first_steps[g->user[i]] + t;
+        mv.e = mv.step % h->N;
+        mv.do_reweight = mv.e == 0;
+        mv.reweight_on = mv.step >= h->params.reweight_start_step;
+        mv.dump = nullptr;
+        launch_rows<true>(h, h->max_walkers, sb, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, mv,
+                          member_extras(h), false);
+      }
       GK(cudaMemsetAsync(g->d_counter + b, 0, sizeof(int), sb));
       GK(launch_group_move_any(B, sb, gm, t, g->d_counter + b, g->cbase >= 0 ? g->cbase + B.first : -1));
       if (dmc) {
@@ -2274,16 +2280,20 @@ int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmc
 {
   if (!g || !first_steps || n_steps < 0) return gfail(g, QMCB_E_ARG, "qmcb_group_run_steps: bad argument");
   const int nm = (int)g->mem.size();
-  bool refresh = false;
+  bool refresh = false, rows_members = false;
   for (int i = 0; i < nm; i++) {
     qmcb_handle *h = g->mem[i];
     const std::string who = "qmcb_group_run_steps: member " + std::to_string(g->user[i]);
     if (first_steps[g->user[i]] < 0) return gfail(g, QMCB_E_ARG, who + ": negative first step");
     if (!h->evaluated_once) return gfail(g, QMCB_E_STATE, who + ": call qmcb_init_walkers first");
     if (h->n_flight) return gfail(g, QMCB_E_STATE, who + ": a batch of steps is in flight on its handle");
-    if (h->params.precision != QMCB_PREC_FP64 || h->state_prec != QMCB_PREC_FP64)
-      return gfail(g, QMCB_E_ARG, who + ": groups step FP64 walkers only");
+    if ((h->params.precision != QMCB_PREC_FP64 && !rows_mode(h->params.precision)) || h->state_prec != QMCB_PREC_FP64)
+      return gfail(g, QMCB_E_ARG, who + ": groups step FP64 walkers (FP64 or tensor-core orbital rows) only");
+    if (h->md && h->params.precision != QMCB_PREC_FP64)
+      return gfail(g, QMCB_E_ARG, who + ": several determinants run in FP64 only");
     refresh |= h->params.refresh_interval > 0;
+    // the rows kernels take the step number as an argument: no graph replay
+    rows_members |= rows_mode(h->params.precision);
   }
   cudaSetDevice(g->device);
   // members' tables, parameters and step numbers
@@ -2291,8 +2301,10 @@ int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmc
   for (int i = 0; i < nm; i++) {
     qmcb_handle *h = g->mem[i];
     GroupMember &G = g->h_gm[i];
+    const bool rows = rows_mode(h->params.precision);
     G.S = h->sys;
-    G.L = h->lay;
+    G.L = rows ? h->lay_rows : h->lay;  // the move kernel on rows needs no basis scratch
+    G.rows = rows ? h->d_rows_out : nullptr;
     G.cfg = make_cfg(h->params);
     G.state = h->d_state;
     G.live = h->d_live;
@@ -2326,7 +2338,7 @@ int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmc
         break;
       }
   GK(cudaEventRecord(g->ev0, st));
-  if (!refresh && n_steps > 0) {
+  if (!refresh && !rows_members && n_steps > 0) {
     if (!(g->gexec && g->g_steps == n_steps && g->g_config == c)) {
       if (g->gexec) {
         cudaGraphExecDestroy(g->gexec);
@@ -2362,6 +2374,10 @@ int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmc
   }
   GK(cudaStreamSynchronize(st));
   g->last = c;
+  for (int i = 0; i < nm; i++)
+    if (g->mem[i]->h_ctl[3])
+      return gfail(g, QMCB_E_CUDA, "qmcb_group_run_steps: member " + std::to_string(g->user[i]) +
+                                       ": the tensor-core contraction gave up waiting (rows not written)");
   double moves = 0.0;
   for (int i = 0; i < nm; i++) {
     qmcb_handle *h = g->mem[i];

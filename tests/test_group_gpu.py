@@ -89,6 +89,39 @@ def test_vmc_group_matches_members_alone(extras):
         assert np.allclose(wa["e_local"], wb["e_local"], rtol=1e-12, atol=1e-12)
 
 
+def test_group_members_on_tensor_core_rows_match_members_alone():
+    """Members whose orbital rows come from the batched tensor-core
+    contraction (int8 digit planes at FP64 accuracy, BF16 and split BF16 with
+    FP32 accumulation) next to FP64 members: the group launches each rows
+    member's prep and contraction before the persistent move kernel, and every
+    member follows exactly its own handle's chain."""
+    from qmcbeaver_b200.desc import QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC, QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES
+    systems = _systems()
+    precs = [QMCB_PREC_BF16X3_TC, QMCB_PREC_INT8_SLICES, QMCB_PREC_FP64, QMCB_PREC_BF16_TC, QMCB_PREC_INT8_SLICES]
+
+    def params(k):
+        p = _params(k)
+        p.precision = precs[k]
+        return p
+
+    solo, grouped = _handles(systems, params), _handles(systems, params)
+    g = QMCB200Group(grouped)
+    fs = _first_steps(systems)
+    n_steps = 11
+    for b in range(4):
+        st_g = g.run_steps([f + b * n_steps for f in fs], n_steps)
+        for k, f in enumerate(solo):
+            st = f.run_steps(fs[k] + b * n_steps, n_steps)
+            assert st.n_moves == st_g[k].n_moves
+            assert st_g[k].sum_accept == pytest.approx(st.sum_accept, rel=1e-12)
+    for a, b in zip(solo, grouped):
+        wa, wb = a.get_walkers(), b.get_walkers()
+        assert np.isfinite(wa["R"]).all()
+        assert np.array_equal(wa["R"], wb["R"])
+        assert np.allclose(wa["e_local"], wb["e_local"], rtol=1e-12, atol=1e-12)
+    g.close()
+
+
 def test_every_configuration_gives_the_same_chain():
     systems = _systems()
     ref = _handles(systems, _params)
