@@ -384,7 +384,9 @@ def serving_section(args):
     one group per batch and one job at a time.  Then jobs on the reference's
     water input (cusp replacement, three-body Jastrow), whose trial function
     reaches the 1 mHa target of the serving workload in a few seconds of
-    device time, arrive at 1 job/s."""
+    device time, arrive at 1 job/s.  At 10 jobs/s the arrivals also run with
+    every job on split-BF16 tensor-core orbital rows, and the water jobs also
+    on tensor-core rows at FP64 accuracy."""
     from qmcbeaver_b200.serving import Server, make_input_jobs, make_jobs
     from qmcbeaver_b200.system import system_from_arrays
     kw = dict(electrons=(4, 200), walkers=(256, 1024), target_error=0.2, max_sweeps=24, orbitals="random")
@@ -403,6 +405,12 @@ def serving_section(args):
     seq = make_jobs(args.serve_jobs, rate=rate, seed=11, **kw)
     rs = Server(max_active=1).run(seq)
     out["rates"][str(rate)]["one_at_a_time"] = summary(rs)
+    # the same arrivals with every job on split-BF16 tensor-core orbital rows
+    # (FP32 accumulation, FP64 inverse, refresh and energies)
+    from qmcbeaver_b200.desc import QMCB_PREC_BF16X3_TC, QMCB_PREC_INT8_SLICES
+    rb = Server(max_active=16).run(make_jobs(args.serve_jobs, rate=rate, seed=11, precision=QMCB_PREC_BF16X3_TC,
+                                             **kw))
+    out["rates"][str(rate)]["streams_bf16x3_rows"] = summary(rb)
     rm = Server(max_active=16).run(mix)
     out["same_results_alone_and_mixed"] = bool(all(
         abs(a.energy - b.energy) <= 1e-9 * max(1.0, abs(b.energy)) for a, b in zip(mix, seq)
@@ -417,6 +425,15 @@ def serving_section(args):
     out["h2o_input_1mha"] = dict(summary(r), target_error_ha=1e-3, equil_sweeps=500,
                                  sweeps=[int(len(j.energies)) for j in jobs],
                                  errors_ha=[j.error for j in jobs], energies_ha=[j.energy for j in jobs])
+    # the same 1 mHa jobs on tensor-core rows at FP64 accuracy (int8 digit planes)
+    jobs = make_input_jobs(3, rate=1.0, system=h2o, seed=5, walkers=(8192, 16384), target_error=1e-3,
+                           max_sweeps=6000, equil_sweeps=500, dt=0.01)
+    for j in jobs:
+        j.precision = QMCB_PREC_INT8_SLICES
+    r = Server(max_active=8).run(jobs)
+    out["h2o_input_1mha_int8_rows"] = dict(summary(r), target_error_ha=1e-3, equil_sweeps=500,
+                                           sweeps=[int(len(j.energies)) for j in jobs],
+                                           errors_ha=[j.error for j in jobs], energies_ha=[j.energy for j in jobs])
     return out
 
 

@@ -421,7 +421,9 @@ int qmcb_group_set_config(qmcb_group *g, int config);
  * QMCB_STAGED_INVERSE_MAX, read by qmcb_create, moves that threshold.  Both
  * layouts compute the same numbers. */
 
-/* Device bytes of the walker state of a handle (admission control). */
+/* Device bytes of the walker state of a handle (admission control), plus the
+ * operand and row buffers of the tensor-core rows modes once one of them
+ * has been set up on the handle. */
 size_t qmcb_state_bytes(const qmcb_handle *h);
 
 /* Live walker count and per-walker read back (host buffers, any may be NULL). */

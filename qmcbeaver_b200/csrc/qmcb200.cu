@@ -1795,7 +1795,20 @@ int qmcb_steps_collect(qmcb_handle *h, qmcb_step_stats *stats)
 
 size_t qmcb_state_bytes(const qmcb_handle *h)
 {
-  return h ? (size_t)h->max_walkers * h->lay.stride * sizeof(double) : 0;
+  if (!h) return 0;
+  size_t b = (size_t)h->max_walkers * h->lay.stride * sizeof(double);
+  // the tensor-core rows modes' buffers, once a mode has set them up
+  const size_t tiles = (size_t)(h->max_walkers + kTileWalkers - 1) / kTileWalkers;
+  if (h->d_rows_out) b += sizeof(double) * (size_t)h->max_walkers * 5 * h->nmax;
+  for (int sp = 0; sp < 2; sp++) {
+    const int n = sp ? h->sys.nb : h->sys.na;
+    const size_t nt = (size_t)std::max((n + kNTile - 1) / kNTile, 1);
+    if (h->d_rows_A) b += nt * h->rows_ksteps * (kSlices * kBBlock + kNTile * sizeof(double));
+    if (h->d_bf_A) b += nt * h->bf_ksteps * 2 * kBBlock;
+  }
+  if (h->d_rows_A) b += tiles * h->rows_ksteps * (kSlices * kABlock + kTileRows * sizeof(double));
+  if (h->d_bf_A) b += tiles * h->bf_ksteps * 2 * kABlock;
+  return b;
 }
 
 int qmcb_num_walkers(const qmcb_handle *h) { return h ? h->n_live_host : -1; }

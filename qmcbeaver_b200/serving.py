@@ -30,7 +30,8 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 from .api import QMCB200Functions, QMCB200Group
-from .desc import QMCB_IMPORTANCE_SAMPLING, QMCB_PREC_FP64, QMCB_QF_UMRIGAR93_UNEQUAL, QMCB_VMC, run_params
+from .desc import (QMCB_IMPORTANCE_SAMPLING, QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC, QMCB_PREC_FP64,
+                   QMCB_PREC_INT8_SLICES, QMCB_QF_UMRIGAR93_UNEQUAL, QMCB_VMC, run_params)
 from .system import MolecularSystem, make_random_molecule
 
 
@@ -70,12 +71,13 @@ def blocked_error(samples: Sequence[float], nblocks: int = 8) -> float:
     return float(m.std(ddof=1) / math.sqrt(len(m)))
 
 
-def state_footprint(system: MolecularSystem, walkers: int) -> int:
+def state_footprint(system: MolecularSystem, walkers: int, precision: int = QMCB_PREC_FP64) -> int:
     """Device bytes a job's handle allocates for its walker state
     (the per-walker block of the library, 2x walker capacity, 256-byte
     blocks): positions, Slater rows / derivatives / inverse per spin (two
     inverse copies for spins above 16 electrons), per-electron arrays,
-    scalars."""
+    scalars; for the tensor-core rows modes also their operand planes, block
+    scales and the step's rows (the library's qmcb_state_bytes)."""
     def pad4(x):
         return (x + 3) & ~3
     N, na, nb = system.n_electrons, system.n_alpha, system.n_beta
@@ -85,7 +87,20 @@ def state_footprint(system: MolecularSystem, walkers: int) -> int:
         words += pad4(n * n) + pad4(3 * n * n) + pad4(n * n) + (2 * pad4(n * n) if ginv else pad4(n * n))
     words += 4 * pad4(3 * N) + pad4(24)
     words = (words + 31) & ~31
-    return 2 * walkers * words * 8
+    cap = 2 * walkers
+    total = cap * words * 8
+    if precision in (QMCB_PREC_INT8_SLICES, QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC):
+        K = system.n_basis
+        tiles = -(-cap // 25)                      # 25 walkers (125 of 128 rows) per tile
+        total += 8 * cap * 5 * max(na, nb)         # the step's rows
+        nt = [max(-(-n // 32), 1) for n in (na, nb)]  # 32-orbital tiles per spin
+        if precision == QMCB_PREC_INT8_SLICES:
+            ks = -(-K // 32)                       # 8 int8 digit planes, a scale per 32-function block
+            total += sum(t * ks * (8 * 1024 + 32 * 8) for t in nt) + tiles * ks * (8 * 4096 + 128 * 8)
+        else:
+            ks = -(-K // 16)                       # hi / lo BF16 planes, 16 functions per K step
+            total += sum(t * ks * 2 * 1024 for t in nt) + tiles * ks * 2 * 4096
+    return total
 
 
 def device_budget(fraction: float = 0.8) -> int:
@@ -152,7 +167,7 @@ class Server:
             # admission by device footprint (walkers + inverses + rows)
             while queue and len(active) < self.max_active:
                 j = queue[0]
-                need = state_footprint(j.system, j.walkers)
+                need = state_footprint(j.system, j.walkers, j.precision)
                 if active and used + need > self.hbm_budget:
                     break
                 queue.pop(0)
@@ -206,7 +221,7 @@ class Server:
             changed = False
             while queue and len(active) < self.max_active:
                 j = queue[0]
-                need = state_footprint(j.system, j.walkers) // 2
+                need = state_footprint(j.system, j.walkers, j.precision) // 2
                 if active and used + need > self.hbm_budget:
                     break
                 queue.pop(0)

@@ -51,8 +51,31 @@ def test_footprint_matches_library():
     from qmcbeaver_b200.api import QMCB200Functions
     from qmcbeaver_b200.system import make_system
     from qmcbeaver_b200.system import make_random_molecule
+    from qmcbeaver_b200.desc import QMCB_PREC_BF16X3_TC, QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES
     for s in (make_system("vmc_water_10e"), make_system("dmc_6nuc_30e"),
               make_random_molecule(60, 8, 120, 8.0, (1, 6, 7, 8), seed=2)):
-        f = QMCB200Functions(s, 2 * 300)
-        assert f.state_bytes() == state_footprint(s, 300)
-        f.close()
+        for prec in (QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES, QMCB_PREC_BF16X3_TC):
+            f = QMCB200Functions(s, 2 * 300, precision=prec)
+            assert f.state_bytes() == state_footprint(s, 300, prec), prec
+            f.close()
+
+
+def test_tensor_core_rows_jobs_same_alone_and_in_mix():
+    """Jobs on split-BF16 tensor-core rows next to FP64 jobs: each job's
+    energies are the same alone and in the mix."""
+    from qmcbeaver_b200.desc import QMCB_PREC_BF16X3_TC
+
+    def fresh():
+        js = make_jobs(4, rate=1e3, seed=9, electrons=(6, 40), walkers=(256, 512), target_error=0.0, max_sweeps=16)
+        for k, j in enumerate(js):
+            j.arrival = 0.0
+            if k % 2 == 0:
+                j.precision = QMCB_PREC_BF16X3_TC
+        return js
+    mix = fresh()
+    Server(max_active=4, mode="streams").run(mix)
+    for k in (0, 1):
+        alone = fresh()[k]
+        Server(max_active=1, mode="streams").run([alone])
+        assert len(alone.energies) == len(mix[k].energies) == 16
+        np.testing.assert_allclose(alone.energies, mix[k].energies, rtol=1e-10, atol=0)
