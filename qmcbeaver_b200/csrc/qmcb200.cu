@@ -1972,6 +1972,10 @@ struct qmcb_group {
   cudaEvent_t fork_ev = nullptr;
   std::vector<cudaStream_t> side;  // one stream per bucket
   std::vector<cudaEvent_t> side_ev;
+  // members on tensor-core rows: a step's rows kernels run on the member's
+  // own stream, forked from its bucket's stream (step_ev[bucket]) and joined
+  // back before the bucket's move kernel (rows_ev[member])
+  std::vector<cudaEvent_t> step_ev, rows_ev;
   cudaGraphExec_t gexec = nullptr;  // the last batch's launch sequence
   int g_steps = -1, g_config = -1;
   std::string err;
@@ -2153,18 +2157,28 @@ static int group_enqueue(qmcb_group *g, int c, int n_steps, const int *first_ste
     const GroupMember *gm = g->d_gm + B.first;
     for (int t = 0; t < n_steps; t++) {
       // members on tensor-core rows: their step's rows first (one prep and
-      // one contraction launch per member, on the bucket's stream)
+      // one contraction launch per member), each member's on its own stream
+      // so that the members' small kernels overlap, joined back into the
+      // bucket's stream before its move kernel
+      bool forked = false;
       for (int i = B.first; i < B.first + B.count; i++) {
         qmcb_handle *h = g->mem[i];
         if (!rows_mode(h->params.precision)) continue;
+        if (!forked) {
+          GK(cudaEventRecord(g->step_ev[b], sb));
+          forked = true;
+        }
+        GK(cudaStreamWaitEvent(h->stream, g->step_ev[b], 0));
         MoveArgs mv;
         mv.step = first_steps[g->user[i]] + t;
         mv.e = mv.step % h->N;
         mv.do_reweight = mv.e == 0;
         mv.reweight_on = mv.step >= h->params.reweight_start_step;
         mv.dump = nullptr;
-        launch_rows<true>(h, h->max_walkers, sb, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, mv,
+        launch_rows<true>(h, h->max_walkers, h->stream, make_cfg(h->params), h->d_live, 0, h->d_ctl, nullptr, mv,
                           member_extras(h), false);
+        GK(cudaEventRecord(g->rows_ev[i], h->stream));
+        GK(cudaStreamWaitEvent(sb, g->rows_ev[i], 0));
       }
       GK(cudaMemsetAsync(g->d_counter + b, 0, sizeof(int), sb));
       GK(launch_group_move_any(B, sb, gm, t, g->d_counter + b, g->cbase >= 0 ? g->cbase + B.first : -1));
@@ -2278,6 +2292,8 @@ int qmcb_group_destroy(qmcb_group *g)
   if (g->ev1) cudaEventDestroy(g->ev1);
   if (g->fork_ev) cudaEventDestroy(g->fork_ev);
   for (cudaEvent_t e : g->side_ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : g->step_ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : g->rows_ev) cudaEventDestroy(e);
   for (cudaStream_t s2 : g->side) {
     cudaStreamSynchronize(s2);
     cudaStreamDestroy(s2);
@@ -2335,6 +2351,14 @@ int qmcb_group_run_steps(qmcb_group *g, const int *first_steps, int n_steps, qmc
     G.thr_fuse = h->params.fusion_threshold;
   }
   cudaStream_t st = g->stream;
+  if (rows_members && g->rows_ev.empty()) {
+    size_t nb = 0;
+    for (const auto &cand : g->cands) nb = std::max(nb, cand.size());
+    g->step_ev.assign(nb, nullptr);
+    g->rows_ev.assign(nm, nullptr);
+    for (auto &e : g->step_ev) GK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : g->rows_ev) GK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
   // the members' own streams finish first (their last evaluate or copy)
   for (auto *h : g->mem) GK(cudaStreamSynchronize(h->stream));
   GK(cudaMemcpyAsync(g->d_gm, g->h_gm.data(), sizeof(GroupMember) * nm, cudaMemcpyHostToDevice, st));
