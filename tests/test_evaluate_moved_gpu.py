@@ -59,6 +59,35 @@ def test_moved_writes_only_selected_outputs():
     assert np.isfinite(full["e_local"]).all()
 
 
+def test_page_locked_inputs_equal_copied_inputs():
+    """Slots and moved positions in page-locked host memory (copied by DMA
+    straight from the caller's buffers): the same results as pageable inputs,
+    call after call, with a permuted slot list."""
+    import torch
+    torch.cuda.set_device(0)
+    s = make_system("dmc_6nuc_30e", seed=2)
+    W, N = 150, s.n_electrons
+    a = QMCB200Functions(s, W, qf_modification=2, dt=0.01)
+    b = QMCB200Functions(s, W, qf_modification=2, dt=0.01)
+    R = s.initial_positions(W, seed=3)
+    sl = np.arange(W)[::-1].copy()  # a permuted slot list
+    a.evaluate(sl, R, -1)
+    b.evaluate(sl, R, -1)
+    sl_pin = torch.tensor(sl, dtype=torch.int32).pin_memory().numpy()
+    r_pin = torch.zeros((W, 3), dtype=torch.float64).pin_memory().numpy()
+    rng = np.random.default_rng(6)
+    for m in range(N + 2):
+        e = m % N
+        R[:, e] += 0.15 * rng.standard_normal((W, 3))
+        r_pin[:] = R[:, e]
+        x = a.evaluate_moved(sl, np.ascontiguousarray(R[:, e]), e)
+        y = b.evaluate_moved(sl_pin, r_pin, e)
+        for k in ("log_abs_psi", "sign", "mod_grad", "e_local", "pe", "status"):
+            np.testing.assert_array_equal(x[k], y[k], err_msg=f"move {m} {k}")
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("entry", ["moved", "all_positions"])
 def test_page_locked_outputs_equal_copied_outputs(entry):
     """Outputs in mapped page-locked host memory are stored by the kernel
