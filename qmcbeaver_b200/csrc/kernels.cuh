@@ -125,10 +125,10 @@ __device__ inline double qf_modify_warp(const DevSys &S, const RunCfg &cfg, cons
       double4 P = S.nuc[cn];
       double nv[3] = {R[3 * i] - P.x, R[3 * i + 1] - P.y, R[3 * i + 2] - P.z};
       double d2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
-      double il = 1.0 / sqrt(d2);
+      double il = rsqrt(d2);
       double ev[3] = {gr[3 * i], gr[3 * i + 1], gr[3 * i + 2]};
       double ev2 = ev[0] * ev[0] + ev[1] * ev[1] + ev[2] * ev[2];
-      double sc = fabs(ev2) < 1e-10 ? 0.0 : 1.0 / sqrt(ev2);
+      double sc = fabs(ev2) < 1e-10 ? 0.0 : rsqrt(ev2);
       double dotp = 0.0;
       for (int x = 0; x < 3; x++) dotp += (nv[x] * il) * (ev[x] * sc);
       double temp = P.w * P.w * d2;
@@ -394,35 +394,37 @@ __device__ inline void jastrow_pe_full_warp(const DevSys &S, const double *R, do
     for (int j = 0; j < N; j++) {
       if (j == i) continue;
       double dx = xi - R[3 * j], dy = yi - R[3 * j + 1], dz = zi - R[3 * j + 2];
-      double r = sqrt(dx * dx + dy * dy + dz * dz);
-      if (j < i) pee += 1.0 / r;
+      // 1 / r from one reciprocal square root (ulp-level differences from
+      // sqrt and divisions, far inside the parity bound)
+      const double r2 = dx * dx + dy * dy + dz * dz, ir = rsqrt(r2), r = r2 * ir;
+      if (j < i) pee += ir;
       int f = ee_func(S, i, j);
       if (f < 0) continue;
       double u, du, d2u;
       pade_eval(S, f, r, u, du, d2u);
-      gx += du * (dx / r);
-      gy += du * (dy / r);
-      gz += du * (dz / r);
+      gx += du * (dx * ir);
+      gy += du * (dy * ir);
+      gz += du * (dz * ir);
       if (j < i) {
         pu += u;
-        pxx += 2.0 * (2.0 / r * du + d2u);
+        pxx += 2.0 * (2.0 * ir * du + d2u);
       }
     }
     int sp = i < S.na ? 0 : 1;
     for (int A = 0; A < S.M; A++) {
       double4 P = S.nuc[A];
       double dx = xi - P.x, dy = yi - P.y, dz = zi - P.z;
-      double r = sqrt(dx * dx + dy * dy + dz * dz);
-      pen -= P.w / r;
+      const double r2 = dx * dx + dy * dy + dz * dz, ir = rsqrt(r2), r = r2 * ir;
+      pen -= P.w * ir;
       int f = S.en[sp][A];
       if (f < 0) continue;
       double u, du, d2u;
       pade_eval(S, f, r, u, du, d2u);
-      gx += du * (dx / r);
-      gy += du * (dy / r);
-      gz += du * (dz / r);
+      gx += du * (dx * ir);
+      gy += du * (dy * ir);
+      gz += du * (dz * ir);
       pu += u;
-      pxx += 2.0 / r * du + d2u;
+      pxx += 2.0 * ir * du + d2u;
     }
     ux[3 * i] = gx;
     ux[3 * i + 1] = gy;
@@ -882,9 +884,11 @@ __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR
     const double Rj[3] = {sR[3 * j], sR[3 * j + 1], sR[3 * j + 2]};
     const double dxo = ro[0] - Rj[0], dyo = ro[1] - Rj[1], dzo = ro[2] - Rj[2];
     const double dxn = rn[0] - Rj[0], dyn = rn[1] - Rj[1], dzn = rn[2] - Rj[2];
-    const double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
-    const double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
-    const double io = 1.0 / r_o, in_ = 1.0 / r_n;
+    // 1 / r from one reciprocal square root, r = r^2 / r (ulp-level
+    // differences from sqrt and a division, far inside the parity bound)
+    const double r2o = dxo * dxo + dyo * dyo + dzo * dzo, r2n = dxn * dxn + dyn * dyn + dzn * dzn;
+    const double io = rsqrt(r2o), in_ = rsqrt(r2n);
+    const double r_o = r2o * io, r_n = r2n * in_;
     dVee += in_ - io;
     const int f = ee_func(S, e, j);
     if (f >= 0) {
@@ -907,9 +911,11 @@ __device__ __forceinline__ void jastrow_pe_move_warp(const DevSys &S, double *sR
     const double4 P = S.nuc[A];
     const double dxo = ro[0] - P.x, dyo = ro[1] - P.y, dzo = ro[2] - P.z;
     const double dxn = rn[0] - P.x, dyn = rn[1] - P.y, dzn = rn[2] - P.z;
-    const double r_o = sqrt(dxo * dxo + dyo * dyo + dzo * dzo);
-    const double r_n = sqrt(dxn * dxn + dyn * dyn + dzn * dzn);
-    const double io = 1.0 / r_o, in_ = 1.0 / r_n;
+    // 1 / r from one reciprocal square root, r = r^2 / r (ulp-level
+    // differences from sqrt and a division, far inside the parity bound)
+    const double r2o = dxo * dxo + dyo * dyo + dzo * dzo, r2n = dxn * dxn + dyn * dyn + dzn * dzn;
+    const double io = rsqrt(r2o), in_ = rsqrt(r2n);
+    const double r_o = r2o * io, r_n = r2n * in_;
     dVen -= P.w * (in_ - io);
     const int f = S.en[sp][A];
     if (f >= 0) {
