@@ -92,9 +92,10 @@ def test_vmc_group_matches_members_alone(extras):
 def test_group_members_on_tensor_core_rows_match_members_alone():
     """Members whose orbital rows come from the batched tensor-core
     contraction (int8 digit planes at FP64 accuracy, BF16 and split BF16 with
-    FP32 accumulation) next to FP64 members: the group launches each rows
-    member's prep and contraction before the persistent move kernel, and every
-    member follows exactly its own handle's chain."""
+    FP32 accumulation) next to FP64 members, all refreshing their inverses in
+    FP64 every 7 steps: the group launches each rows member's prep and
+    contraction before the persistent move kernel, and every member follows
+    exactly its own handle's chain."""
     from qmcbeaver_b200.desc import QMCB_PREC_BF16_TC, QMCB_PREC_BF16X3_TC, QMCB_PREC_FP64, QMCB_PREC_INT8_SLICES
     systems = _systems()
     precs = [QMCB_PREC_BF16X3_TC, QMCB_PREC_INT8_SLICES, QMCB_PREC_FP64, QMCB_PREC_BF16_TC, QMCB_PREC_INT8_SLICES]
@@ -102,6 +103,7 @@ def test_group_members_on_tensor_core_rows_match_members_alone():
     def params(k):
         p = _params(k)
         p.precision = precs[k]
+        p.refresh_interval = 7  # FP64 refreshes of the inverses inside the group's batches
         return p
 
     solo, grouped = _handles(systems, params), _handles(systems, params)
